@@ -1,0 +1,344 @@
+#!/usr/bin/env python
+"""Throughput of the Wick (H, S) pair evaluator on B200: pair-elements per second.
+
+Workload (default ``config2``): the linear-H6/cc-pVDZ NOCISD(3) space of noci-rs, as a seeded
+synthetic stand-in with the same dimensions (PySCF integrals are not available): n = 30
+orbitals, 3 + 3 electrons, an RHF-like and two spin-polarised references, every single and
+double excitation of each (26490 determinants), and 10^7 determinant pairs sampled uniformly
+among pairs whose parents differ (seed 12345).  A step evaluates (H, S) for the whole batch.
+
+* ``value``   device-resident throughput: pairs and results already in HBM.
+* ``e2e``     through the host-buffer C ABI call (nw_eval_hs_pairs): pinned host pairs are
+              copied in and (H, S) copied out inside every timed step.
+* ``roofline`` the evaluator phase (all contraction-rank class kernels) against the measured
+              HBM copy bandwidth, with algorithmic bytes per pair
+              B(La, Lb) = 8 [2 (La^2 + Lb^2) + 2 C(La,2)^2 + 2 C(Lb,2)^2 + La^2 Lb^2] + 60.
+* ``cpu_baseline`` the FP64 CPU restatement of the reference path on all host cores, on a
+              bounded sample of the same pairs.
+
+``--impl reference`` times that CPU restatement alone (the reference is Rust and cannot be
+built here; the restatement is the only runnable form of its algorithm).
+
+Multi-GPU: one process per GPU under torchrun; each rank evaluates its own 10^7-pair batch
+(no data-path collective, weak scaling); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "noci-rs_b200"))
+
+METRIC = "Wick H/S pair-elements/s"
+UNIT = "pair-elements/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["config2", "config3"], default="config2")
+    ap.add_argument("--npairs", type=int, default=10_000_000)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(name: str, npairs: int, rank: int):
+    from nociwick import synthetic as sy
+    if name == "config2":
+        system = sy.config2_system()
+        basis = sy.sd_basis(30, 3, 3, 3)
+        pairs = sy.sample_pairs(basis, npairs, seed=12345 + rank)
+        cfg = {"workload": "H6/cc-pVDZ NOCISD(3) stand-in: n=30, 3a+3b electrons, RHF+2 UHF refs, "
+                           "26490 SD determinants, uniform pairs across parents",
+               "nmo": 30, "nocc": [3, 3], "nref": 3, "ndet": int(basis.shape[0]), "npairs_per_gpu": npairs}
+    else:
+        system = sy.config3_system()
+        basis = sy.sd_basis(64, 6, 6, 8)
+        pairs = sy.sample_pairs_by_rank(basis, npairs, seed=3 + rank)
+        cfg = {"workload": "synthetic stress: n=64, 6a+6b electrons, naux=256, 8 refs, 6/64 ordered ref "
+                           "pairs with zero-overlap orbitals, contraction rank 0-4 uniform",
+               "nmo": 64, "nocc": [6, 6], "nref": 8, "ndet": int(basis.shape[0]), "npairs_per_gpu": npairs}
+    return system, basis, pairs.astype(np.uint32), cfg
+
+
+def algorithmic_bytes(basis, pairs) -> float:
+    ra = basis["rank_a"].astype(np.int64)
+    rb = basis["rank_b"].astype(np.int64)
+    la = ra[pairs[:, 0]] + ra[pairs[:, 1]]
+    lb = rb[pairs[:, 0]] + rb[pairs[:, 1]]
+    c2 = lambda l: l * (l - 1) // 2  # noqa: E731
+    b = 8 * (2 * (la * la + lb * lb) + 2 * c2(la) ** 2 + 2 * c2(lb) ** 2 + la * la * lb * lb) + 60
+    return float(b.sum())
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.flush()
+        with open(self.file.name) as f:
+            rows = [r.strip().split(",") for r in f if r.strip()]
+        os.unlink(self.file.name)
+        sm, smax, reasons = [], [], set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names[1:], start=5):
+                if r[k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(system, basis, pairs, seconds: float, gpu_hs=None):
+    """The FP64 CPU restatement of the reference path on every host core, on a bounded sample."""
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import Oracle
+    orc = Oracle.from_system(system, tol=1e-8, with_mo_cache=False)
+    ob = orc.oracle_basis(basis)
+    cores = os.cpu_count() or 1
+    cal = pairs[:min(pairs.shape[0], 100_000)].astype(np.int64)
+    t0 = time.perf_counter()
+    orc.eval_pairs(ob, cal, nthreads=cores)
+    rate = cal.shape[0] / max(time.perf_counter() - t0, 1e-6)
+    nsample = int(min(pairs.shape[0], max(cal.shape[0], rate * seconds)))
+    sample = pairs[:nsample].astype(np.int64)
+    t0 = time.perf_counter()
+    h, s = orc.eval_pairs(ob, sample, nthreads=cores)
+    dt = time.perf_counter() - t0
+    out = {"value": nsample / dt, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"first {nsample} pairs of the same batch ({dt:.1f} s of CPU work, C++ FP64 restatement "
+                     f"of the reference evaluator, {cores} threads)"}
+    if gpu_hs is not None:
+        err = max(float(np.max(np.abs(gpu_hs[:nsample, 0] - h))), float(np.max(np.abs(gpu_hs[:nsample, 1] - s))))
+        out["max_abs_err_gpu_vs_cpu"] = err
+    return out
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    system, basis, pairs, cfg = workload(args.workload, args.npairs, 0)
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import Oracle
+    orc = Oracle.from_system(system, tol=1e-8, with_mo_cache=False)
+    ob = orc.oracle_basis(basis)
+    cores = os.cpu_count() or 1
+    cal = pairs[:100_000].astype(np.int64)
+    t0 = time.perf_counter()
+    orc.eval_pairs(ob, cal, nthreads=cores)
+    rate = cal.shape[0] / max(time.perf_counter() - t0, 1e-6)
+    # each step is a bounded sample sized so warmup + steps take about two minutes
+    per_step = int(max(10_000, min(pairs.shape[0], rate * 120.0 / max(1, args.steps + args.warmup))))
+    sample = pairs[:per_step].astype(np.int64)
+    for _ in range(args.warmup):
+        orc.eval_pairs(ob, sample, nthreads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        orc.eval_pairs(ob, sample, nthreads=cores)
+    dt = time.perf_counter() - t0
+    value = per_step * args.steps / dt
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": dict(cfg, sample_pairs_per_step=per_step),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{per_step} pairs per step, C++ FP64 restatement of the reference "
+                                       f"evaluator (the Rust reference cannot be built here), {cores} threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import nociwick
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+    torch.cuda.set_device(local_rank)
+    system, basis, pairs, cfg = workload(args.workload, args.npairs, rank)
+    npairs = pairs.shape[0]
+    eng = nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8,
+                               device=local_rank)
+    t0 = time.perf_counter()
+    eng.build()
+    build_s = time.perf_counter() - t0
+    eng.set_basis(basis)
+    info = eng.info()
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    dpairs = torch.from_numpy(pairs.view(np.int32)).to(f"cuda:{local_rank}")
+    dout = torch.empty((npairs, 2), dtype=torch.float64, device=f"cuda:{local_rank}")
+    hpairs = torch.from_numpy(pairs.view(np.int32)).pin_memory()
+    hout = torch.empty((npairs, 2), dtype=torch.float64).pin_memory()
+    hp_ptr, ho_ptr = hpairs.data_ptr(), hout.data_ptr()
+
+    def step_device():
+        eng.eval_pairs_device(dpairs.data_ptr(), npairs, dout.data_ptr(), sh)
+
+    def step_e2e():
+        # the public host-buffer C ABI call: H2D pairs, evaluate, D2H (H, S), synchronise
+        st = eng._lib.nw_eval_hs_pairs(eng._ctx, hp_ptr, npairs, ho_ptr, __import__("ctypes").c_void_p(sh))
+        eng._check(st, "nw_eval_hs_pairs")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(max(3, args.warmup)):
+        step_device()
+    eng.sync(sh)
+    # device-resident throughput
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step_device()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    t_dev = ev0.elapsed_time(ev1)
+    eng.sync(sh)
+    # evaluator-phase timing for the roofline (CUDA events recorded inside the library on the
+    # launching stream)
+    eng.set_timing(True)
+    phases = []
+    for _ in range(min(args.steps, 10)):
+        step_device()
+        phases.append(eng.last_timings())
+    eng.set_timing(False)
+    # end to end through the host-buffer entry point
+    for _ in range(2):
+        step_e2e()
+    barrier()
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    for _ in range(args.steps):
+        step_e2e()
+    ev3.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    t_e2e = ev2.elapsed_time(ev3)
+    if dist is not None:
+        t = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_dev, t_e2e = float(t[0]), float(t[1])
+    if rank != 0:
+        return
+    total_pairs = npairs * world
+    value = total_pairs * args.steps / (t_dev / 1e3)
+    e2e = total_pairs * args.steps / (t_e2e / 1e3)
+    ev_ms = statistics.median([p["eval_m0"] + p["eval_gen"] for p in phases])
+    phase_ms = {k: statistics.median([p[k] for p in phases]) for k in phases[0]}
+    alg_bytes = algorithmic_bytes(basis, pairs)
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ev_ms / 1e3) / 1e9
+    clocks = clk.summary()
+    kernels_per_step = 3 + 25 + 1 + (1 if info["ngeneric"] > 0 else 0)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": t_dev / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(cfg, l2="inputs larger than L2: pairs %d MB + results %d MB + intermediates %d MB per step"
+                       % (npairs * 8 >> 20, npairs * 16 >> 20, info["slab_bytes"] >> 20),
+                       build_seconds=round(build_s, 3), parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": npairs * 8, "d2h_bytes_per_step": npairs * 16},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "evaluator phase (25 rank-class kernels + runtime-rank kernel)",
+                     "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_step": alg_bytes,
+                     "eval_ms": ev_ms, "phase_ms": phase_ms},
+        "clocks": clocks,
+        "gpu_launches": kernels_per_step * args.steps,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(system, basis, pairs, args.cpu_seconds, gpu_hs=dout.cpu().numpy())
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device(f"cuda:{local_rank}"))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

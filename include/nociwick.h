@@ -1,0 +1,164 @@
+/*
+ * nociwick.h - C ABI of the B200 nonorthogonal Wick matrix-element engine.
+ *
+ * The engine evaluates overlap and Hamiltonian matrix elements (H_ij, S_ij) between
+ * nonorthogonal determinants by the extended nonorthogonal Wick theorem, on one NVIDIA
+ * B200 (sm_100a), with the per-reference-pair intermediates resident in HBM.  It replaces
+ * the hot path of dy-cl/noci-rs, src/nonorthogonalwicks (Wick build + evaluators) and
+ * src/noci/hs.rs (batched pair dispatch); each entry point names the reference interface it
+ * stands in for.
+ *
+ * Conventions
+ *  - Matrices are row-major FP64.  AO integrals are chemists' (mu nu|lam sig) stored as
+ *    eri[((mu*n + nu)*n + lam)*n + sig], the PySCF int2e s1 order read by noci-rs.
+ *  - Orbital coefficients C[mu][p] (nao x nmo).  A reference's occupied orbitals are the
+ *    first nocc columns (noci-rs contraction_orbitals assumes the same).
+ *  - A determinant is an nw_det record: parent reference, per-spin excitation rank and the
+ *    first four hole then particle orbital indices (noci-rs ExcitationSpinCache), and the
+ *    product of both spins' fermionic excitation phases (ReducedTwoSpinDetState.phase).
+ *  - Pair (a, b) puts determinant a in the bra and b in the ket; results are written as
+ *    hs[2*i] = H, hs[2*i + 1] = S.
+ *  - Every call returns an nw_status; NW_OK is 0.  Nothing aborts the process.
+ *  - A context owns its device memory and is not thread-safe; calls on one context must be
+ *    serialised by the caller (different contexts are independent).
+ */
+#ifndef NOCIWICK_H
+#define NOCIWICK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__) || defined(__clang__)
+#define NW_API __attribute__((visibility("default")))
+#else
+#define NW_API
+#endif
+
+typedef enum {
+    NW_OK = 0,
+    NW_ERR_INVALID = 1,      /* bad argument or inconsistent input data            */
+    NW_ERR_CUDA = 2,         /* a CUDA runtime or cuBLAS call failed               */
+    NW_ERR_ALLOC = 3,        /* device or pinned host allocation failed            */
+    NW_ERR_UNSUPPORTED = 4,  /* input outside what this build supports             */
+    NW_ERR_STATE = 5,        /* call out of order (e.g. evaluate before build)     */
+    NW_ERR_NO_DEVICE = 6     /* no usable CUDA device                              */
+} nw_status;
+
+/* Matrix-element conventions for reference pairs with zero-overlap orbital pairs (m > 0).
+ * NW_CONVENTION_REFERENCE reproduces noci-rs xw_hamiltonian_overlap_gen_prepared
+ * (src/nonorthogonalwicks/eval/preparehamiltonianoverlap.rs:20550-20966) including its
+ * treatment of singular mixed determinants, its (0,1)+(1,0) scalar term and the omitted
+ * E_nuc*S.  NW_CONVENTION_EXACT returns the exact matrix element (checked against a
+ * brute-force Fock-space evaluation).  Pairs without zero-overlap orbitals agree in both. */
+typedef enum { NW_CONVENTION_REFERENCE = 0, NW_CONVENTION_EXACT = 1 } nw_convention;
+
+/* One determinant (32 bytes).  Replaces noci-rs ExcitationCache + ReducedTwoSpinDetState
+ * (src/lib.rs:136-167, :230-266) as the per-determinant input of the batched evaluator. */
+typedef struct {
+    uint32_t parent;     /* reference index                                          */
+    uint8_t rank_a;      /* alpha excitation rank (0..4)                             */
+    uint8_t idx_a[8];    /* alpha holes [0..3] then particles [4..7], ascending      */
+    uint8_t rank_b;      /* beta excitation rank (0..4)                              */
+    uint8_t idx_b[8];    /* beta holes then particles                                */
+    uint8_t pad[2];
+    double phase;        /* alpha phase * beta phase relative to the parent          */
+} nw_det;
+
+/* AO data (noci-rs AoData, src/lib.rs:52-76): only the fields the Wick path reads. */
+typedef struct {
+    int32_t nao;         /* AO basis size                                            */
+    int32_t nmo;         /* orbitals per spin per reference (== nao in noci-rs)      */
+    double enuc;         /* nuclear repulsion energy                                 */
+    const double* s;     /* nao x nao overlap                                        */
+    const double* h;     /* nao x nao core Hamiltonian                               */
+    const double* eri;   /* nao^4 Coulomb integrals (mu nu|lam sig)                  */
+} nw_system;
+
+/* Reference determinants (noci-rs DetState ca/cb/oa/ob, src/scalar.rs:30-61). */
+typedef struct {
+    int32_t nref;
+    int32_t nocc_a;      /* occupied alpha orbitals per reference (first nocc_a)     */
+    int32_t nocc_b;
+    const double* c_alpha;  /* nref x nao x nmo                                      */
+    const double* c_beta;   /* nref x nao x nmo                                      */
+} nw_refs;
+
+typedef struct {
+    double tol;          /* singular values |s| <= tol are zero-overlap pairs (noci-rs tol) */
+    int32_t convention;  /* nw_convention                                           */
+    int32_t device;      /* CUDA device ordinal                                     */
+} nw_opts;
+
+typedef struct {
+    int32_t nref;
+    int32_t nmo;
+    int32_t ngeneric;            /* ordered reference pairs with m_alpha + m_beta > 0   */
+    int32_t pad;
+    uint64_t slab_bytes;         /* device bytes held for intermediates                 */
+    uint64_t ndet;               /* determinants in the resident basis                  */
+} nw_info;
+
+typedef struct nw_ctx nw_ctx;
+
+/* Create a context: copies the AO data and reference orbitals to the device.
+ * Replaces the inputs of noci-rs build_wicks_shared (src/noci/wicks.rs:133-139). */
+NW_API nw_status nw_ctx_create(const nw_system* sys, const nw_refs* refs, const nw_opts* opts, nw_ctx** out);
+
+/* Build every ordered reference-pair intermediate on the GPU (Loewdin pairing by an FP64
+ * Jacobi SVD, M^(0)/M^(1), X/Y, F, V, J and II tensors).
+ * Replaces build_wicks_shared / build_wicks_pair (src/noci/wicks.rs:37-279) and
+ * SameSpinBuild::new / DiffSpinBuild::new (src/nonorthogonalwicks/build.rs:86-926). */
+NW_API nw_status nw_build_intermediates(nw_ctx* ctx);
+
+/* Zero-overlap counts (m_alpha, m_beta) of ordered pair x*nref + w, as planned by
+ * plan_wicks_pairs (src/noci/wicks.rs:90-121).  m must hold 2*nref*nref ints. */
+NW_API nw_status nw_pair_zero_counts(const nw_ctx* ctx, int32_t* m);
+
+/* Upload the determinant basis once (host array of ndet records); it stays resident.
+ * Replaces the reduced_basis argument of calculate_hs_pairs_wicks_batched (src/noci/hs.rs:72-78). */
+NW_API nw_status nw_set_basis(nw_ctx* ctx, const nw_det* basis, uint64_t ndet);
+
+/* (H, S) for npairs requests (a_i, b_i) = pairs[2i], pairs[2i+1] into the resident basis,
+ * with device-resident pairs and output.  Same-parent pairs more than a double excitation
+ * apart give exactly (0, 0); every other pair goes through the Wick path.  The call is
+ * asynchronous on `stream` (a cudaStream_t, or NULL for the legacy stream).
+ * Replaces calculate_hs_pairs_wicks_batched (src/noci/hs.rs:72-130) and
+ * xw_hamiltonian_overlap_prepared_batched (preparehamiltonianoverlap.rs:121-362). */
+NW_API nw_status nw_eval_hs_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs,
+                                  double* hs_dev, void* stream);
+
+/* The same with host buffers: copies pairs in, evaluates, copies (H, S) out, and returns
+ * when the results are in hs_host.  Pinned host memory gives the full transfer rate. */
+NW_API nw_status nw_eval_hs_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* hs_host,
+                           void* stream);
+
+/* Overlap only, S for each pair (hs_dev[i]), device buffers.
+ * Replaces xw_overlap (src/nonorthogonalwicks/eval/overlap.rs:42-65) times the phases. */
+NW_API nw_status nw_eval_s_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* s_dev,
+                                 void* stream);
+
+/* Wait for the work queued on `stream` and report pair indices that were out of range in an
+ * earlier device-buffer call (those outputs are NaN). */
+NW_API nw_status nw_sync(nw_ctx* ctx, void* stream);
+
+/* Per-phase device times of the most recent nw_eval_hs_pairs* call, measured with CUDA events
+ * recorded on its stream while timing is enabled: ms[0] classify, ms[1] scan, ms[2] scatter,
+ * ms[3] m = 0 evaluator, ms[4] m > 0 evaluator.  nw_last_timings waits for that call. */
+NW_API nw_status nw_set_timing(nw_ctx* ctx, int enable);
+NW_API nw_status nw_last_timings(nw_ctx* ctx, float* ms);
+
+NW_API nw_status nw_ctx_info(const nw_ctx* ctx, nw_info* out);
+NW_API nw_status nw_ctx_destroy(nw_ctx* ctx);
+NW_API const char* nw_status_string(nw_status st);
+/* Text of the last error recorded on ctx (empty string if none). */
+NW_API const char* nw_last_error(const nw_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NOCIWICK_H */

@@ -1,0 +1,282 @@
+// C ABI of the engine (declared in include/nociwick.h): context lifetime, input validation,
+// and the host/device entry points.
+#include <cuda_runtime.h>
+#include <cublas_v2.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace nw {
+
+nw_status fail(nw_ctx* ctx, nw_status st, const std::string& msg) {
+  if (ctx) ctx->last_error = msg;
+  return st;
+}
+
+nw_status cuda_fail(nw_ctx* ctx, cudaError_t e, const char* what) {
+  return fail(ctx, NW_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+nw_status ensure(nw_ctx* ctx, DevBuf& b, size_t bytes) {
+  if (b.bytes >= bytes) return NW_OK;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  size_t want = bytes + bytes / 4 + 256;
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e != cudaSuccess) {
+    b.p = nullptr;
+    return fail(ctx, NW_ERR_ALLOC, std::string("scratch allocation failed: ") + cudaGetErrorString(e));
+  }
+  b.bytes = want;
+  return NW_OK;
+}
+
+}  // namespace nw
+
+namespace {
+
+void free_buf(nw::DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+nw_status upload(nw_ctx* ctx, double** dst, const double* src, size_t count) {
+  if (cudaMalloc(dst, count * sizeof(double)) != cudaSuccess)
+    return nw::fail(ctx, NW_ERR_ALLOC, "device allocation for inputs failed");
+  NW_CUDA(ctx, cudaMemcpy(*dst, src, count * sizeof(double), cudaMemcpyHostToDevice));
+  return NW_OK;
+}
+
+bool finite_all(const double* p, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(p[i])) return false;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* nw_status_string(nw_status st) {
+  switch (st) {
+    case NW_OK:
+      return "ok";
+    case NW_ERR_INVALID:
+      return "invalid argument";
+    case NW_ERR_CUDA:
+      return "CUDA error";
+    case NW_ERR_ALLOC:
+      return "allocation failed";
+    case NW_ERR_UNSUPPORTED:
+      return "unsupported input";
+    case NW_ERR_STATE:
+      return "call out of order";
+    case NW_ERR_NO_DEVICE:
+      return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+const char* nw_last_error(const nw_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+nw_status nw_ctx_create(const nw_system* sys, const nw_refs* refs, const nw_opts* opts, nw_ctx** out) {
+  if (!out) return NW_ERR_INVALID;
+  *out = nullptr;
+  if (!sys || !refs || !opts || !sys->s || !sys->h || !sys->eri || !refs->c_alpha || !refs->c_beta)
+    return NW_ERR_INVALID;
+  const int nao = sys->nao, nmo = sys->nmo, nref = refs->nref;
+  if (nao <= 0 || nmo <= 0 || nmo > 128 || nref <= 0 || nref > 256) return NW_ERR_UNSUPPORTED;
+  if (refs->nocc_a < 0 || refs->nocc_b < 0 || refs->nocc_a > nmo || refs->nocc_b > nmo) return NW_ERR_INVALID;
+  if (refs->nocc_a > 64 || refs->nocc_b > 64) return NW_ERR_UNSUPPORTED;
+  if (!(opts->tol >= 0.0) || !std::isfinite(opts->tol) || !std::isfinite(sys->enuc)) return NW_ERR_INVALID;
+  if (opts->convention != NW_CONVENTION_REFERENCE && opts->convention != NW_CONVENTION_EXACT) return NW_ERR_INVALID;
+  const size_t n2 = (size_t)nao * nao, n4 = n2 * n2;
+  if (!finite_all(sys->s, n2) || !finite_all(sys->h, n2) || !finite_all(sys->eri, n4) ||
+      !finite_all(refs->c_alpha, (size_t)nref * nao * nmo) || !finite_all(refs->c_beta, (size_t)nref * nao * nmo))
+    return NW_ERR_INVALID;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return NW_ERR_NO_DEVICE;
+  if (opts->device < 0 || opts->device >= ndev) return NW_ERR_INVALID;
+  nw_ctx* ctx = new (std::nothrow) nw_ctx();
+  if (!ctx) return NW_ERR_ALLOC;
+  ctx->device = opts->device;
+  ctx->nao = nao;
+  ctx->nmo = nmo;
+  ctx->nref = nref;
+  ctx->nocc_a = refs->nocc_a;
+  ctx->nocc_b = refs->nocc_b;
+  ctx->enuc = sys->enuc;
+  ctx->tol = opts->tol;
+  ctx->convention = opts->convention;
+  nw_status st = NW_OK;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) st = NW_ERR_CUDA;
+  if (st == NW_OK && cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) st = NW_ERR_CUDA;
+  if (st == NW_OK) st = upload(ctx, &ctx->d_s, sys->s, n2);
+  if (st == NW_OK) st = upload(ctx, &ctx->d_h, sys->h, n2);
+  if (st == NW_OK) st = upload(ctx, &ctx->d_eri, sys->eri, n4);
+  if (st == NW_OK) st = upload(ctx, &ctx->d_ca, refs->c_alpha, (size_t)nref * nao * nmo);
+  if (st == NW_OK) st = upload(ctx, &ctx->d_cb, refs->c_beta, (size_t)nref * nao * nmo);
+  if (st == NW_OK && cudaMallocHost(&ctx->h_flag, sizeof(uint32_t)) != cudaSuccess) st = NW_ERR_ALLOC;
+  if (st != NW_OK) {
+    nw_ctx_destroy(ctx);
+    return st;
+  }
+  *out = ctx;
+  return NW_OK;
+}
+
+nw_status nw_build_intermediates(nw_ctx* ctx) {
+  if (!ctx) return NW_ERR_INVALID;
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  return nw::build_all(ctx);
+}
+
+nw_status nw_pair_zero_counts(const nw_ctx* ctx, int32_t* m) {
+  if (!ctx || !m) return NW_ERR_INVALID;
+  if (!ctx->built) return NW_ERR_STATE;
+  std::memcpy(m, ctx->m_counts.data(), sizeof(int32_t) * ctx->m_counts.size());
+  return NW_OK;
+}
+
+nw_status nw_set_basis(nw_ctx* ctx, const nw_det* basis, uint64_t ndet) {
+  if (!ctx || (!basis && ndet)) return NW_ERR_INVALID;
+  if (ndet >= 0xFFFFFFFFull) return nw::fail(ctx, NW_ERR_UNSUPPORTED, "at most 2^32 - 2 determinants");
+  // Validate every record: parent in range, ranks <= 4, holes ascending in the occupied
+  // block, particles ascending in the virtual block.
+  for (uint64_t i = 0; i < ndet; ++i) {
+    const nw_det& d = basis[i];
+    if (d.parent >= (uint32_t)ctx->nref) return nw::fail(ctx, NW_ERR_INVALID, "determinant parent out of range");
+    if (!std::isfinite(d.phase)) return nw::fail(ctx, NW_ERR_INVALID, "non-finite determinant phase");
+    for (int spin = 0; spin < 2; ++spin) {
+      const int r = spin ? d.rank_b : d.rank_a;
+      const uint8_t* idx = spin ? d.idx_b : d.idx_a;
+      const int nocc = spin ? ctx->nocc_b : ctx->nocc_a;
+      if (r > 4) return nw::fail(ctx, NW_ERR_UNSUPPORTED, "excitation rank above 4 per spin");
+      for (int k = 0; k < r; ++k) {
+        if (idx[k] >= nocc) return nw::fail(ctx, NW_ERR_INVALID, "hole index not occupied in the parent");
+        if (idx[4 + k] < nocc || idx[4 + k] >= ctx->nmo)
+          return nw::fail(ctx, NW_ERR_INVALID, "particle index not virtual in the parent");
+        if (k > 0 && (idx[k] <= idx[k - 1] || idx[4 + k] <= idx[3 + k]))
+          return nw::fail(ctx, NW_ERR_INVALID, "hole/particle indices must be strictly ascending");
+      }
+    }
+  }
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (ctx->d_dets) cudaFree(ctx->d_dets);
+  ctx->d_dets = nullptr;
+  ctx->ndet = 0;
+  if (ndet == 0) return NW_OK;
+  if (cudaMalloc(&ctx->d_dets, ndet * sizeof(nw_det)) != cudaSuccess)
+    return nw::fail(ctx, NW_ERR_ALLOC, "basis allocation failed");
+  NW_CUDA(ctx, cudaMemcpy(ctx->d_dets, basis, ndet * sizeof(nw_det), cudaMemcpyHostToDevice));
+  ctx->ndet = ndet;
+  return NW_OK;
+}
+
+nw_status nw_eval_hs_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* hs_dev,
+                                  void* stream) {
+  if (!ctx || (npairs && (!pairs_dev || !hs_dev))) return NW_ERR_INVALID;
+  return nw::eval_pairs(ctx, pairs_dev, npairs, hs_dev, false, static_cast<cudaStream_t>(stream));
+}
+
+nw_status nw_eval_s_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* s_dev,
+                                 void* stream) {
+  if (!ctx || (npairs && (!pairs_dev || !s_dev))) return NW_ERR_INVALID;
+  return nw::eval_pairs(ctx, pairs_dev, npairs, s_dev, true, static_cast<cudaStream_t>(stream));
+}
+
+nw_status nw_eval_hs_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* hs_host, void* stream) {
+  if (!ctx || (npairs && (!pairs_host || !hs_host))) return NW_ERR_INVALID;
+  if (npairs == 0) return NW_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  nw_status st = nw::ensure(ctx, ctx->io_pairs, npairs * 2 * sizeof(uint32_t));
+  if (st != NW_OK) return st;
+  if ((st = nw::ensure(ctx, ctx->io_hs, npairs * 2 * sizeof(double))) != NW_OK) return st;
+  uint32_t* dp = static_cast<uint32_t*>(ctx->io_pairs.p);
+  double* dh = static_cast<double*>(ctx->io_hs.p);
+  NW_CUDA(ctx, cudaMemcpyAsync(dp, pairs_host, npairs * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  if ((st = nw::eval_pairs(ctx, dp, npairs, dh, false, s)) != NW_OK) return st;
+  NW_CUDA(ctx, cudaMemcpyAsync(hs_host, dh, npairs * 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  NW_CUDA(ctx, cudaMemcpyAsync(ctx->h_flag, ctx->flag.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  NW_CUDA(ctx, cudaStreamSynchronize(s));
+  if (*ctx->h_flag) return nw::fail(ctx, NW_ERR_INVALID, "pair index out of range of the determinant basis");
+  return NW_OK;
+}
+
+nw_status nw_sync(nw_ctx* ctx, void* stream) {
+  if (!ctx) return NW_ERR_INVALID;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (ctx->flag.p) {
+    NW_CUDA(ctx, cudaMemcpyAsync(ctx->h_flag, ctx->flag.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  }
+  NW_CUDA(ctx, cudaStreamSynchronize(s));
+  if (ctx->flag.p && *ctx->h_flag) return nw::fail(ctx, NW_ERR_INVALID, "pair index out of range of the determinant basis");
+  return NW_OK;
+}
+
+nw_status nw_set_timing(nw_ctx* ctx, int enable) {
+  if (!ctx) return NW_ERR_INVALID;
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (enable && !ctx->ev[0]) {
+    for (int i = 0; i < 6; ++i) NW_CUDA(ctx, cudaEventCreate(&ctx->ev[i]));
+  }
+  ctx->timing = enable != 0;
+  ctx->timed_valid = false;
+  return NW_OK;
+}
+
+nw_status nw_last_timings(nw_ctx* ctx, float* ms) {
+  if (!ctx || !ms) return NW_ERR_INVALID;
+  if (!ctx->timed_valid) return nw::fail(ctx, NW_ERR_STATE, "no timed evaluation recorded");
+  NW_CUDA(ctx, cudaEventSynchronize(ctx->ev[5]));
+  for (int i = 0; i < 5; ++i) NW_CUDA(ctx, cudaEventElapsedTime(&ms[i], ctx->ev[i], ctx->ev[i + 1]));
+  return NW_OK;
+}
+
+nw_status nw_ctx_info(const nw_ctx* ctx, nw_info* out) {
+  if (!ctx || !out) return NW_ERR_INVALID;
+  std::memset(out, 0, sizeof(*out));
+  out->nref = ctx->nref;
+  out->nmo = ctx->nmo;
+  out->ngeneric = ctx->built ? ctx->nref * ctx->nref - ctx->nfast : 0;
+  out->slab_bytes = ctx->slab_bytes;
+  out->ndet = ctx->ndet;
+  return NW_OK;
+}
+
+nw_status nw_ctx_destroy(nw_ctx* ctx) {
+  if (!ctx) return NW_OK;
+  cudaSetDevice(ctx->device);
+  cudaDeviceSynchronize();
+  double* bufs[] = {ctx->d_s, ctx->d_h, ctx->d_eri, ctx->d_ca, ctx->d_cb, ctx->d_slab};
+  for (double* b : bufs)
+    if (b) cudaFree(b);
+  if (ctx->d_fast) cudaFree(ctx->d_fast);
+  if (ctx->d_gen) cudaFree(ctx->d_gen);
+  if (ctx->d_order) cudaFree(ctx->d_order);
+  if (ctx->d_dets) cudaFree(ctx->d_dets);
+  free_buf(ctx->keys);
+  free_buf(ctx->perm);
+  free_buf(ctx->counts);
+  free_buf(ctx->offsets);
+  free_buf(ctx->flag);
+  free_buf(ctx->io_pairs);
+  free_buf(ctx->io_hs);
+  if (ctx->h_flag) cudaFreeHost(ctx->h_flag);
+  for (int i = 0; i < 6; ++i)
+    if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+  if (ctx->blas) cublasDestroy(ctx->blas);
+  delete ctx;
+  return NW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,105 @@
+// Internal types of the B200 Wick engine: device-side pair tables, the context, and the
+// small dense linear algebra used by the pair evaluators.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cublas_v2.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/nociwick.h"
+#include "wick_math.cuh"
+
+namespace nw {
+
+constexpr int kMaxL = 8;          // largest contraction-determinant dimension per spin
+constexpr int kClasses = 26;      // (L_alpha, L_beta) in 0..4 x 0..4, plus one "other" class
+constexpr uint32_t kSkipKey = 0xFFFFFFFFu;
+
+struct EvalParams {
+  const nw_det* dets;
+  uint64_t ndet;
+  const FastPair* fast;    // indexed by ordered pair x*nref + w
+  const GenPair* gen;      // indexed by ordered pair x*nref + w
+  const int32_t* order;    // ordered pair -> sort position (fast pairs first)
+  int32_t nref, n, nocc_a, nocc_b;
+  int32_t nfast;           // number of fast ordered pairs (sort positions 0..nfast-1)
+  int32_t exact;
+  double enuc, tol;
+};
+
+// ---------------------------------------------------------------------------------------
+// Context.
+// ---------------------------------------------------------------------------------------
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace nw
+
+struct nw_ctx {
+  int device = 0;
+  int nao = 0, nmo = 0, nref = 0, nocc_a = 0, nocc_b = 0;
+  double enuc = 0.0, tol = 1e-8;
+  int convention = NW_CONVENTION_REFERENCE;
+  bool built = false;
+
+  // inputs on the device
+  double* d_s = nullptr;
+  double* d_h = nullptr;
+  double* d_eri = nullptr;
+  double* d_ca = nullptr;   // nref x nao x nmo
+  double* d_cb = nullptr;
+
+  // intermediates
+  double* d_slab = nullptr;
+  size_t slab_bytes = 0;
+  nw::FastPair* d_fast = nullptr;
+  nw::GenPair* d_gen = nullptr;
+  int32_t* d_order = nullptr;
+  int nfast = 0;
+  std::vector<int32_t> m_counts;   // 2 per ordered pair
+  std::vector<int32_t> order_host; // ordered pair -> sort position
+
+  // resident basis
+  nw_det* d_dets = nullptr;
+  uint64_t ndet = 0;
+
+  // evaluation scratch (grown on demand)
+  nw::DevBuf keys, perm, counts, offsets, flag;
+  uint32_t* h_flag = nullptr;      // pinned mirror of the device error flag
+  nw::DevBuf io_pairs, io_hs;      // staging for the host-buffer entry point
+
+  cublasHandle_t blas = nullptr;
+  std::string last_error;
+
+  // optional per-phase timing of the evaluation pipeline
+  bool timing = false;
+  bool timed_valid = false;
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace nw {
+
+// Records an error on the context and returns the status.
+nw_status fail(nw_ctx* ctx, nw_status st, const std::string& msg);
+nw_status cuda_fail(nw_ctx* ctx, cudaError_t e, const char* what);
+nw_status ensure(nw_ctx* ctx, DevBuf& b, size_t bytes);
+
+// Build (build.cu).
+nw_status build_all(nw_ctx* ctx);
+
+// Evaluation (eval.cu).
+nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, bool overlap_only,
+                     cudaStream_t stream);
+
+}  // namespace nw
+
+#define NW_CUDA(ctx, call)                                  \
+  do {                                                      \
+    cudaError_t e_ = (call);                                \
+    if (e_ != cudaSuccess) return nw::cuda_fail(ctx, e_, #call); \
+  } while (0)

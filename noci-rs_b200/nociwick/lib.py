@@ -1,0 +1,232 @@
+"""ctypes binding of libnociwick.so (the sm_100a engine) and a Python mirror of the noci-rs
+interface for the Wick (H, S) path.
+
+The mirror keeps the reference's names so a caller of noci-rs finds the same entry points:
+
+* ``build_wicks_shared``  -> src/noci/wicks.rs:133-279 (intermediates for all reference pairs)
+* ``WicksShared``         -> src/nonorthogonalwicks/storage.rs:35-150 (owner of the device slab)
+* ``calculate_hs_pairs_wicks_batched`` -> src/noci/hs.rs:72-130 (batched (H, S) for pairs)
+
+There is no CPU evaluation path: if the CUDA library cannot be loaded, or no GPU is present,
+the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+from .synthetic import NW_DET_DTYPE
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnociwick.so")
+_lib = None
+
+NW_OK = 0
+_STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "allocation failed", 4: "unsupported input",
+           5: "call out of order", 6: "no CUDA device"}
+CONVENTIONS = {"reference": 0, "exact": 1}
+
+
+class NwError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        super().__init__(f"{where}: {_STATUS.get(status, status)}" + (f" ({detail})" if detail else ""))
+        self.status = status
+
+
+class NwSystem(ctypes.Structure):
+    _fields_ = [("nao", ctypes.c_int32), ("nmo", ctypes.c_int32), ("enuc", ctypes.c_double),
+                ("s", ctypes.POINTER(ctypes.c_double)), ("h", ctypes.POINTER(ctypes.c_double)),
+                ("eri", ctypes.POINTER(ctypes.c_double))]
+
+
+class NwRefs(ctypes.Structure):
+    _fields_ = [("nref", ctypes.c_int32), ("nocc_a", ctypes.c_int32), ("nocc_b", ctypes.c_int32),
+                ("c_alpha", ctypes.POINTER(ctypes.c_double)), ("c_beta", ctypes.POINTER(ctypes.c_double))]
+
+
+class NwOpts(ctypes.Structure):
+    _fields_ = [("tol", ctypes.c_double), ("convention", ctypes.c_int32), ("device", ctypes.c_int32)]
+
+
+class NwInfo(ctypes.Structure):
+    _fields_ = [("nref", ctypes.c_int32), ("nmo", ctypes.c_int32), ("ngeneric", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("slab_bytes", ctypes.c_uint64), ("ndet", ctypes.c_uint64)]
+
+
+EXPORTED = ("nw_ctx_create", "nw_build_intermediates", "nw_pair_zero_counts", "nw_set_basis",
+            "nw_eval_hs_pairs_device", "nw_eval_hs_pairs", "nw_eval_s_pairs_device", "nw_sync",
+            "nw_set_timing", "nw_last_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
+            "nw_last_error")
+
+
+def load(path: Optional[str] = None):
+    """Load libnociwick.so; raises if it is missing (there is no fallback)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"CUDA engine library not found at {p}; build it with `make -C noci-rs_b200` "
+                           "(or __graft_entry__.build()).")
+    L = ctypes.CDLL(p)
+    vp = ctypes.c_void_p
+    L.nw_ctx_create.argtypes = [ctypes.POINTER(NwSystem), ctypes.POINTER(NwRefs), ctypes.POINTER(NwOpts),
+                                ctypes.POINTER(vp)]
+    L.nw_build_intermediates.argtypes = [vp]
+    L.nw_pair_zero_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+    L.nw_set_basis.argtypes = [vp, vp, ctypes.c_uint64]
+    L.nw_eval_hs_pairs_device.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
+    L.nw_eval_hs_pairs.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
+    L.nw_eval_s_pairs_device.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
+    L.nw_sync.argtypes = [vp, vp]
+    L.nw_set_timing.argtypes = [vp, ctypes.c_int]
+    L.nw_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    L.nw_ctx_info.argtypes = [vp, ctypes.POINTER(NwInfo)]
+    L.nw_ctx_destroy.argtypes = [vp]
+    L.nw_status_string.argtypes = [ctypes.c_int]
+    L.nw_status_string.restype = ctypes.c_char_p
+    L.nw_last_error.argtypes = [vp]
+    L.nw_last_error.restype = ctypes.c_char_p
+    for name in EXPORTED:
+        if name not in ("nw_status_string", "nw_last_error"):
+            getattr(L, name).restype = ctypes.c_int
+    if path is None:
+        _lib = L
+    return L
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class WicksShared:
+    """Device-resident Wick intermediates for every ordered reference pair, plus the resident
+    determinant basis.  Mirrors noci-rs WicksShared/WicksView (storage.rs:35-150, view.rs:20-147)."""
+
+    def __init__(self, s, h, eri, enuc: float, refs: Sequence[Tuple[np.ndarray, int, np.ndarray, int]],
+                 tol: float = 1e-8, convention: str = "reference", device: int = 0):
+        self._lib = load()
+        self._ctx = ctypes.c_void_p()
+        nmo = refs[0][0].shape[1]
+        nao = refs[0][0].shape[0]
+        nocc_a = bin(refs[0][1]).count("1")
+        nocc_b = bin(refs[0][3]).count("1")
+        for (ca, oa, cb, ob) in refs:
+            if oa != (1 << nocc_a) - 1 or ob != (1 << nocc_b) - 1:
+                raise ValueError("reference occupations must be the first nocc orbitals (aufbau order)")
+        self._s = np.ascontiguousarray(s, dtype=np.float64)
+        self._h = np.ascontiguousarray(h, dtype=np.float64)
+        self._eri = np.ascontiguousarray(eri, dtype=np.float64)
+        self._ca = np.ascontiguousarray(np.stack([r[0] for r in refs]), dtype=np.float64)
+        self._cb = np.ascontiguousarray(np.stack([r[2] for r in refs]), dtype=np.float64)
+        sysd = NwSystem(nao, nmo, float(enuc), _dp(self._s), _dp(self._h), _dp(self._eri))
+        rd = NwRefs(len(refs), nocc_a, nocc_b, _dp(self._ca), _dp(self._cb))
+        od = NwOpts(float(tol), CONVENTIONS[convention], int(device))
+        st = self._lib.nw_ctx_create(ctypes.byref(sysd), ctypes.byref(rd), ctypes.byref(od), ctypes.byref(self._ctx))
+        if st != NW_OK:
+            raise NwError(st, "nw_ctx_create")
+        self.nref, self.nmo, self.nocc_a, self.nocc_b = len(refs), nmo, nocc_a, nocc_b
+        self.tol, self.convention = tol, convention
+        self._basis = None
+
+    # -- lifetime --------------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_ctx", None) and self._ctx.value:
+            self._lib.nw_ctx_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int, where: str):
+        if st != NW_OK:
+            detail = self._lib.nw_last_error(self._ctx)
+            raise NwError(st, where, detail.decode() if detail else "")
+
+    # -- build / basis ---------------------------------------------------------------------
+    def build(self):
+        self._check(self._lib.nw_build_intermediates(self._ctx), "nw_build_intermediates")
+        return self
+
+    def zero_counts(self) -> np.ndarray:
+        m = np.zeros(2 * self.nref * self.nref, np.int32)
+        self._check(self._lib.nw_pair_zero_counts(self._ctx, m.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))),
+                    "nw_pair_zero_counts")
+        return m.reshape(self.nref, self.nref, 2)
+
+    def set_basis(self, dets: np.ndarray):
+        dets = np.ascontiguousarray(dets)
+        if dets.dtype != NW_DET_DTYPE:
+            raise TypeError("basis must use the nw_det record dtype")
+        self._check(self._lib.nw_set_basis(self._ctx, dets.ctypes.data, dets.shape[0]), "nw_set_basis")
+        self._basis = dets
+        return self
+
+    def info(self) -> dict:
+        inf = NwInfo()
+        self._check(self._lib.nw_ctx_info(self._ctx, ctypes.byref(inf)), "nw_ctx_info")
+        return {"nref": inf.nref, "nmo": inf.nmo, "ngeneric": inf.ngeneric, "slab_bytes": inf.slab_bytes,
+                "ndet": inf.ndet}
+
+    # -- evaluation ------------------------------------------------------------------------
+    def eval_pairs(self, pairs: np.ndarray, out: Optional[np.ndarray] = None, stream: int = 0):
+        """(H, S) for host pairs (n, 2) -> host array (n, 2); copies in and out inside the call."""
+        pairs = np.ascontiguousarray(pairs, dtype=np.uint32)
+        n = pairs.shape[0]
+        if out is None:
+            out = np.empty((n, 2), np.float64)
+        self._check(self._lib.nw_eval_hs_pairs(self._ctx, pairs.ctypes.data, n, out.ctypes.data,
+                                               ctypes.c_void_p(stream)), "nw_eval_hs_pairs")
+        return out
+
+    def eval_pairs_device(self, pairs_ptr: int, npairs: int, out_ptr: int, stream: int = 0):
+        self._check(self._lib.nw_eval_hs_pairs_device(self._ctx, ctypes.c_void_p(pairs_ptr), npairs,
+                                                      ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream)),
+                    "nw_eval_hs_pairs_device")
+
+    def eval_overlap_device(self, pairs_ptr: int, npairs: int, out_ptr: int, stream: int = 0):
+        self._check(self._lib.nw_eval_s_pairs_device(self._ctx, ctypes.c_void_p(pairs_ptr), npairs,
+                                                     ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream)),
+                    "nw_eval_s_pairs_device")
+
+    def set_timing(self, enable: bool = True):
+        self._check(self._lib.nw_set_timing(self._ctx, 1 if enable else 0), "nw_set_timing")
+
+    def last_timings(self) -> dict:
+        """Device ms of the phases of the last evaluation (CUDA events on its stream)."""
+        ms = (ctypes.c_float * 5)()
+        self._check(self._lib.nw_last_timings(self._ctx, ms), "nw_last_timings")
+        return dict(zip(("classify", "scan", "scatter", "eval_m0", "eval_gen"), [float(v) for v in ms]))
+
+    def sync(self, stream: int = 0):
+        self._check(self._lib.nw_sync(self._ctx, ctypes.c_void_p(stream)), "nw_sync")
+
+
+def build_wicks_shared(ao, refs, tol: float = 1e-8, convention: str = "reference", device: int = 0) -> WicksShared:
+    """noci-rs build_wicks_shared (src/noci/wicks.rs:133-279): intermediates for all ordered
+    reference pairs, built on the GPU.  ``ao`` has attributes s, h, eri, enuc."""
+    return WicksShared(ao.s, ao.h, ao.eri, ao.enuc, refs, tol, convention, device).build()
+
+
+def calculate_hs_pairs_wicks_batched(wicks: WicksShared, pairs: np.ndarray,
+                                     reduced_basis: Optional[np.ndarray] = None) -> np.ndarray:
+    """noci-rs calculate_hs_pairs_wicks_batched (src/noci/hs.rs:72-130): (H, S) per pair.
+
+    ``pairs`` is (n, 2) determinant indices; ``reduced_basis`` (nw_det records) replaces the
+    resident basis when given.  Returns an (n, 2) array of (H, S).
+    """
+    if reduced_basis is not None:
+        wicks.set_basis(reduced_basis)
+    return wicks.eval_pairs(pairs)

@@ -60,23 +60,41 @@ def canonical_null_gauge(u: np.ndarray, v: np.ndarray, s: np.ndarray, tol: float
     """Fix the free rotation of the zero-singular-value columns of U and V.
 
     The SVD leaves the columns of U and V that belong to zero singular values determined only
-    up to independent orthogonal rotations.  The exact matrix elements do not depend on that
-    choice, but the reference evaluator's handling of zero-overlap pairs does once m >= 2, so
-    the choice is fixed here by a rule any SVD implementation can reproduce: with U0 the null
-    columns, U0^T = Q R (QR with a positive diagonal) and U0 is replaced by U0 Q = R^T; the
-    same for V.  Returns the new (u, v) and the factor det(Q_U) det(Q_V) for the phase.
+    up to independent orthogonal transformations (for one zero, independent signs).  The exact
+    matrix elements do not depend on that choice, but the reference evaluator's handling of
+    zero-overlap pairs does, so the choice is fixed here by a rule any SVD routine can
+    reproduce: with U0 the null columns, B = U0^T is factored B = Q R by modified Gram-Schmidt
+    over its columns (a column whose residual norm is <= 1e-10 is skipped) with R's diagonal
+    positive, and U0 is replaced by U0 Q; the same for V.  The CUDA build applies the same
+    rule (canonical_null_columns in noci-rs_b200/csrc/wick_math.cuh).
+    Returns the new (u, v) and the factor det(Q_U) det(Q_V).
     """
     zeros = [k for k, val in enumerate(s) if abs(val) <= tol]
-    if len(zeros) < 2:
+    m = len(zeros)
+    if m < 1:
         return u, v, 1.0
     fac = 1.0
     out = []
     for mat in (u, v):
         m0 = mat[:, zeros]
-        q, r = np.linalg.qr(m0.T)
-        d = np.sign(np.diag(r))
-        d[d == 0] = 1.0
-        q = q * d[None, :]
+        bt = m0.T                      # m x o; its columns are the rows of U0
+        q = np.zeros((m, m))
+        found = 0
+        for col in range(bt.shape[1]):
+            if found == m:
+                break
+            w = bt[:, col].copy()
+            for _ in range(2):
+                for f in range(found):
+                    w -= q[:, f] * (q[:, f] @ w)
+            nrm = float(np.sqrt(w @ w))
+            if nrm <= 1e-10:
+                continue
+            q[:, found] = w / nrm
+            found += 1
+        if found < m:
+            out.append(mat)
+            continue
         fac *= float(np.linalg.det(q))
         mat = mat.copy()
         mat[:, zeros] = m0 @ q
@@ -89,7 +107,7 @@ def ortho_svd_rotate(s_ao: np.ndarray, cx_occ: np.ndarray, cw_occ: np.ndarray,
                      canonical: bool = True):
     """Loewdin pairing: S_occ = U s V^T, rotated occupied sets and phase det(U) det(V).
 
-    Follows build.rs:401-424; with two or more zero singular values the null-space gauge is
+    Follows build.rs:401-424; when zero singular values are present the null-space gauge is
     fixed by ``canonical_null_gauge``.  ``null_gauge`` (tests only) first applies random
     independent rotations to the null columns of U and V, as a different SVD routine might.
     """
@@ -101,6 +119,8 @@ def ortho_svd_rotate(s_ao: np.ndarray, cx_occ: np.ndarray, cw_occ: np.ndarray,
         u, v = u.copy(), v.copy()
         for mat in (u, v):
             q, _ = np.linalg.qr(null_gauge.standard_normal((len(zeros), len(zeros))))
+            if null_gauge.random() < 0.5:
+                q[:, 0] *= -1.0            # include reflections (one-sided sign flips)
             mat[:, zeros] = mat[:, zeros] @ q
     if canonical:
         u, v, _ = canonical_null_gauge(u, v, s, tol)

@@ -1,0 +1,100 @@
+"""The C ABI (include/nociwick.h) without a GPU: exports, struct layouts, error paths."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import nociwick
+from nociwick import lib as L
+from nociwick.synthetic import NW_DET_DTYPE
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "nociwick.h")
+
+
+def header_functions():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"NW_API\s+(?:const\s+)?\w+\*?\s+(nw_\w+)\s*\(", text)))
+
+
+def test_every_declared_symbol_is_exported():
+    names = header_functions()
+    assert len(names) >= 12
+    lib = ctypes.CDLL(nociwick.LIB_PATH)
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(names) == set(L.EXPORTED)
+
+
+def test_struct_layouts_match_bindings(tmp_path):
+    probe = tmp_path / "probe.c"
+    probe.write_text(r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "nociwick.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(nw_det), offsetof(nw_det, rank_a), offsetof(nw_det, idx_a),
+         offsetof(nw_det, rank_b), offsetof(nw_det, idx_b), offsetof(nw_det, phase), sizeof(nw_system));
+  printf("%zu %zu %zu %zu %zu\n", sizeof(nw_refs), sizeof(nw_opts), sizeof(nw_info),
+         offsetof(nw_system, s), offsetof(nw_refs, c_alpha));
+  return 0;
+}
+''')
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(probe), "-o",
+                    str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    v = [int(x) for x in out]
+    f = NW_DET_DTYPE.fields
+    assert v[:6] == [NW_DET_DTYPE.itemsize, f["rank_a"][1], f["idx_a"][1], f["rank_b"][1], f["idx_b"][1],
+                     f["phase"][1]]
+    assert v[6] == ctypes.sizeof(L.NwSystem)
+    assert v[7:10] == [ctypes.sizeof(L.NwRefs), ctypes.sizeof(L.NwOpts), ctypes.sizeof(L.NwInfo)]
+    assert v[10] == L.NwSystem.s.offset and v[11] == L.NwRefs.c_alpha.offset
+
+
+def test_header_compiles_as_cxx(tmp_path):
+    src = tmp_path / "probe.cpp"
+    src.write_text('#include "nociwick.h"\nint main() { return nw_status_string(NW_OK) ? 0 : 1; }\n')
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
+                    str(src)], check=True)
+
+
+def test_status_strings_and_argument_errors():
+    lib = L.load()
+    assert lib.nw_status_string(0) == b"ok"
+    assert lib.nw_status_string(6) == b"no CUDA device"
+    out = ctypes.c_void_p()
+    assert lib.nw_ctx_create(None, None, None, ctypes.byref(out)) == 1
+    assert lib.nw_ctx_destroy(None) == 0
+    assert lib.nw_build_intermediates(None) == 1
+    assert lib.nw_eval_hs_pairs(None, None, 0, None, None) == 1
+
+
+def test_invalid_system_rejected_before_device_use():
+    from nociwick import synthetic as sy
+    s = sy.make_system(6, 2, 2, 2, 10, seed=1)
+    h = s.h.copy()
+    h[0, 0] = np.nan
+    with pytest.raises(L.NwError) as e:
+        nociwick.WicksShared(s.s, h, s.eri, s.enuc, s.refs)
+    assert e.value.status == 1
+
+
+def test_no_device_reported_without_gpu():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from nociwick import synthetic as sy
+    s = sy.make_system(6, 2, 2, 2, 10, seed=1)
+    with pytest.raises(L.NwError) as e:
+        nociwick.WicksShared(s.s, s.h, s.eri, s.enuc, s.refs)
+    assert e.value.status == 6
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    with pytest.raises(RuntimeError):
+        L.load(str(tmp_path / "absent.so"))

@@ -1,0 +1,165 @@
+"""GPU parity: the sm_100a engine against the FP64 oracle, through the C ABI.
+
+Tolerances (FP64 end to end; the target bound on matrix elements is 1e-9 Eh):
+* ATOL = 1e-10 for the well-conditioned workloads (smallest occupied-overlap singular value of
+  any reference pair above ~0.3);
+* ATOL_STRESS = 1e-9 for the stress systems whose forced zero-overlap references leave other
+  reference pairs nearly singular (singular values down to ~0.01): there the two-body terms
+  scale as 1/s^2, and a 1e-14 relative perturbation of the input orbitals already moves the
+  oracle's own elements by ~4e-10, so the GPU and oracle builds (different but equally exact
+  FP64 operation orders) agree only to that level.
+"""
+import numpy as np
+import pytest
+
+import nociwick
+from nociwick import synthetic as sy
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+ATOL = 1e-10
+ATOL_STRESS = 1e-9
+
+
+def _engine(system, tol=1e-8, convention="reference"):
+    return nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=tol,
+                                convention=convention).build()
+
+
+def _compare(system, basis, pairs, convention="reference", tol=1e-8, orc=None):
+    orc = orc or Oracle.from_system(system, tol=tol)
+    ob = orc.oracle_basis(basis)
+    with _engine(system, tol, convention) as w:
+        w.set_basis(basis)
+        hs = w.eval_pairs(pairs)
+        m = w.zero_counts()
+    h_ref, s_ref = orc.eval_pairs(ob, pairs, exact=(convention == "exact"))
+    m_ref = np.array([[b.aa.m, b.bb.m] for b in orc.builds]).reshape(m.shape)
+    assert np.array_equal(m, m_ref)
+    dh = np.abs(hs[:, 0] - h_ref)
+    ds = np.abs(hs[:, 1] - s_ref)
+    return dh, ds, hs, h_ref, s_ref
+
+
+@pytest.mark.parametrize("zero_pairs", [[], [(0, 1, 1, 0)], [(0, 1, 0, 2)], [(1, 2, 1, 1)], [(0, 2, 2, 1)]])
+@pytest.mark.parametrize("convention", ["reference", "exact"])
+def test_small_all_ranks(zero_pairs, convention):
+    """n = 8, 3 + 3 electrons, 3 references, excitations up to quadruples (L up to 8 per spin),
+    every m pattern, same-parent pairs included."""
+    system = sy.make_system(8, 3, 3, 3, 20, seed=1, k_scale=0.3, zero_pairs=zero_pairs, enuc=0.37)
+    basis = sy.sd_basis(8, 3, 3, 3, orders=(1, 2, 3, 4))
+    pairs = sy.sample_pairs(basis, 6000, seed=3, distinct_parents=False)
+    dh, ds, *_ = _compare(system, basis, pairs, convention)
+    assert dh.max() <= ATOL_STRESS and ds.max() <= ATOL, (dh.max(), ds.max())
+
+
+def test_config2_standin_sample():
+    """Linear-H6/cc-pVDZ stand-in (n = 30, 3 + 3 electrons, RHF + two UHF references, all
+    singles and doubles: 26490 determinants); 20000 uniform pairs from different parents."""
+    system = sy.config2_system()
+    basis = sy.sd_basis(30, 3, 3, 3)
+    assert basis.shape[0] == 26490
+    pairs = sy.sample_pairs(basis, 20000, seed=12345)
+    dh, ds, *_ = _compare(system, basis, pairs)
+    assert dh.max() <= ATOL and ds.max() <= ATOL, (dh.max(), ds.max())
+
+
+def test_overlap_only_matches():
+    import torch
+    system = sy.make_system(8, 3, 3, 3, 20, seed=2, k_scale=0.3, zero_pairs=[(0, 1, 1, 0), (1, 2, 0, 2)])
+    basis = sy.sd_basis(8, 3, 3, 3, orders=(1, 2, 3))
+    pairs = sy.sample_pairs(basis, 5000, seed=5, distinct_parents=False)
+    orc = Oracle.from_system(system)
+    _, s_ref = orc.eval_pairs(orc.oracle_basis(basis), pairs)
+    with _engine(system) as w:
+        w.set_basis(basis)
+        dp = torch.from_numpy(pairs.astype(np.uint32).view(np.int32)).cuda()
+        out = torch.empty(pairs.shape[0], dtype=torch.float64, device="cuda")
+        w.eval_overlap_device(dp.data_ptr(), pairs.shape[0], out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        w.sync(torch.cuda.current_stream().cuda_stream)
+        s = out.cpu().numpy()
+    assert np.max(np.abs(s - s_ref)) <= ATOL_STRESS
+
+
+def test_device_entry_matches_host_entry_and_is_deterministic():
+    import torch
+    system = sy.config2_system()
+    basis = sy.sd_basis(30, 3, 3, 3)
+    pairs = sy.sample_pairs(basis, 200000, seed=9)
+    with _engine(system) as w:
+        w.set_basis(basis)
+        host = w.eval_pairs(pairs)
+        stream = torch.cuda.current_stream().cuda_stream
+        dp = torch.from_numpy(pairs.astype(np.uint32).view(np.int32)).cuda()
+        out = torch.empty((pairs.shape[0], 2), dtype=torch.float64, device="cuda")
+        w.eval_pairs_device(dp.data_ptr(), pairs.shape[0], out.data_ptr(), stream)
+        w.sync(stream)
+        dev1 = out.cpu().numpy().copy()
+        w.eval_pairs_device(dp.data_ptr(), pairs.shape[0], out.data_ptr(), stream)
+        w.sync(stream)
+        dev2 = out.cpu().numpy()
+    assert np.array_equal(host, dev1)
+    assert np.array_equal(dev1, dev2)
+
+
+def test_hermiticity_at_scale():
+    """Size-independent property at bench scale: H and S are symmetric, so (a, b) and (b, a)
+    agree; 2 x 10^6 pairs."""
+    system = sy.config2_system()
+    basis = sy.sd_basis(30, 3, 3, 3)
+    pairs = sy.sample_pairs(basis, 2_000_000, seed=21, canonical=False)
+    with _engine(system) as w:
+        w.set_basis(basis)
+        fwd = w.eval_pairs(pairs)
+        rev = w.eval_pairs(np.ascontiguousarray(pairs[:, ::-1]))
+    scale = np.maximum(1.0, np.abs(fwd))
+    assert np.max(np.abs(fwd - rev) / scale) <= 1e-11
+
+
+def test_edge_cases():
+    system = sy.make_system(8, 3, 3, 2, 20, seed=4)
+    basis = sy.sd_basis(8, 3, 3, 2, orders=(1, 2, 3))
+    with _engine(system) as w:
+        w.set_basis(basis)
+        # empty request
+        assert w.eval_pairs(np.zeros((0, 2), np.uint32)).shape == (0, 2)
+        # same parent, more than a double excitation apart: exact zeros
+        ranks = basis["rank_a"].astype(int) + basis["rank_b"].astype(int)
+        a = int(np.nonzero((basis["parent"] == 0) & (ranks == 3))[0][0])
+        b = int(np.nonzero((basis["parent"] == 0) & (ranks == 3))[0][-1])
+        out = w.eval_pairs(np.array([[a, b]], np.uint32))
+        orc = Oracle.from_system(system)
+        ref = orc.eval_pairs(orc.oracle_basis(basis), np.array([[a, b]]))
+        assert np.allclose(out[0], [ref[0][0], ref[1][0]], atol=ATOL)
+        # out-of-range index is an error, not a fault
+        with pytest.raises(nociwick.NwError):
+            w.eval_pairs(np.array([[0, basis.shape[0]]], np.uint32))
+        # the context stays usable afterwards
+        again = w.eval_pairs(np.array([[a, b]], np.uint32))
+        assert np.array_equal(again, out)
+
+
+def test_invalid_basis_rejected():
+    system = sy.make_system(8, 3, 3, 2, 20, seed=4)
+    basis = sy.sd_basis(8, 3, 3, 2)
+    bad = basis.copy()
+    bad["idx_a"][5, 4] = 1          # particle index inside the occupied block
+    with _engine(system) as w:
+        with pytest.raises(nociwick.NwError):
+            w.set_basis(bad)
+        bad2 = basis.copy()
+        bad2["parent"][3] = 7
+        with pytest.raises(nociwick.NwError):
+            w.set_basis(bad2)
+
+
+def test_config3_full_orbital_count():
+    """n = 64, 6 + 6 electrons, naux = 256 Cholesky ERIs, zero-overlap pairs with m = 1 and
+    m = 2 (three references to keep the oracle build short)."""
+    system = sy.make_system(64, 6, 6, 3, 256, seed=3, k_scale=0.3, zero_pairs=[(0, 1, 1, 0), (1, 2, 0, 2)])
+    basis = sy.sd_basis(64, 6, 6, 3)
+    pairs = sy.sample_pairs_by_rank(basis, 30000, seed=4)
+    orc = Oracle.from_system(system, tol=1e-8, with_mo_cache=False)
+    for convention in ("reference", "exact"):
+        dh, ds, *_ = _compare(system, basis, pairs, convention, orc=orc)
+        assert dh.max() <= ATOL_STRESS and ds.max() <= ATOL_STRESS, (convention, dh.max(), ds.max())
