@@ -61,18 +61,37 @@ def workload(name: str, npairs: int, rank: int):
     if name == "config2":
         system = sy.config2_system()
         basis = sy.sd_basis(30, 3, 3, 3)
-        pairs = sy.sample_pairs(basis, npairs, seed=12345 + rank)
+        pairs = sy.sample_pairs(basis, npairs, seed=rank_seed(12345, rank))
         cfg = {"workload": "H6/cc-pVDZ NOCISD(3) stand-in: n=30, 3a+3b electrons, RHF+2 UHF refs, "
                            "26490 SD determinants, uniform pairs across parents",
                "nmo": 30, "nocc": [3, 3], "nref": 3, "ndet": int(basis.shape[0]), "npairs_per_gpu": npairs}
     else:
         system = sy.config3_system()
         basis = sy.sd_basis(64, 6, 6, 8)
-        pairs = sy.sample_pairs_by_rank(basis, npairs, seed=3 + rank)
+        pairs = sy.sample_pairs_by_rank(basis, npairs, seed=rank_seed(3, rank))
         cfg = {"workload": "synthetic stress: n=64, 6a+6b electrons, naux=256, 8 refs, 6/64 ordered ref "
                            "pairs with zero-overlap orbitals, contraction rank 0-4 uniform",
                "nmo": 64, "nocc": [6, 6], "nref": 8, "ndet": int(basis.shape[0]), "npairs_per_gpu": npairs}
     return system, basis, pairs.astype(np.uint32), cfg
+
+
+def rank_seed(base: int, rank: int) -> int:
+    """Each rank evaluates its own batch: the seed of rank r's pair sample."""
+    return base + rank
+
+
+def reduce_max(values, dist, device):
+    """Max over ranks of per-rank device times (any torch.distributed backend)."""
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def aggregate_rate(npairs_per_rank: int, world: int, steps: int, t_ms: float) -> float:
+    """Whole-job pairs per second: every rank's pairs over the slowest rank's time."""
+    return npairs_per_rank * world * steps / (t_ms / 1e3)
 
 
 def algorithmic_bytes(basis, pairs) -> float:
@@ -86,7 +105,9 @@ def algorithmic_bytes(basis, pairs) -> float:
 
 
 class ClockSampler:
-    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+    """nvidia-smi samples (every 50 ms) of SM clock and throttle reasons.  The sampler runs over a
+    0.5 s pre-roll of back-to-back steps and then the timed region, which is shorter than the
+    sampling period at small step counts; the pre-roll keeps the GPU at the same load."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -101,7 +122,7 @@ class ClockSampler:
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.device)], stdout=self.file,
+                                          "-lms", "50", "-i", str(self.device)], stdout=self.file,
                                          stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -252,6 +273,11 @@ def run_ours(args, rank, world, local_rank):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     with ClockSampler(local_rank) as clk:
+        t_roll = time.perf_counter()
+        while time.perf_counter() - t_roll < 0.5:
+            for _ in range(10):
+                step_device()
+            torch.cuda.synchronize()
         ev0.record(stream)
         for _ in range(args.steps):
             step_device()
@@ -280,15 +306,11 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     barrier()
     t_e2e = ev2.elapsed_time(ev3)
-    if dist is not None:
-        t = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_dev, t_e2e = float(t[0]), float(t[1])
+    t_dev, t_e2e = reduce_max([t_dev, t_e2e], dist, f"cuda:{local_rank}")
     if rank != 0:
         return
-    total_pairs = npairs * world
-    value = total_pairs * args.steps / (t_dev / 1e3)
-    e2e = total_pairs * args.steps / (t_e2e / 1e3)
+    value = aggregate_rate(npairs, world, args.steps, t_dev)
+    e2e = aggregate_rate(npairs, world, args.steps, t_e2e)
     ev_ms = statistics.median([p["eval_m0"] + p["eval_gen"] for p in phases])
     phase_ms = {k: statistics.median([p[k] for p in phases]) for k in phases[0]}
     alg_bytes = algorithmic_bytes(basis, pairs)

@@ -266,6 +266,7 @@ nw_status nw_ctx_destroy(nw_ctx* ctx) {
   if (ctx->d_dets) cudaFree(ctx->d_dets);
   free_buf(ctx->keys);
   free_buf(ctx->perm);
+  free_buf(ctx->spairs);
   free_buf(ctx->counts);
   free_buf(ctx->offsets);
   free_buf(ctx->flag);

@@ -34,6 +34,14 @@ __device__ __forceinline__ void store_hs(double* out, uint64_t i, double h, doub
   reinterpret_cast<double2*>(out)[i] = make_double2(h, s);
 }
 
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Keys of every pair, and per-key counts.  Lanes of a warp holding the same key add their count
+// with one atomic (warp-aggregated through __match_any_sync).
 template <bool kShared>
 __global__ void __launch_bounds__(256) classify_kernel(EvalParams P, const uint32_t* __restrict__ pairs,
                                                        uint64_t npairs, uint32_t* __restrict__ keys,
@@ -45,6 +53,7 @@ __global__ void __launch_bounds__(256) classify_kernel(EvalParams P, const uint3
     for (int k = threadIdx.x; k < nkeys; k += blockDim.x) hist[k] = 0;
     __syncthreads();
   }
+  const int lane = threadIdx.x & 31;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < npairs; i += stride) {
     const uint2 ab = __ldg(reinterpret_cast<const uint2*>(pairs) + i);
@@ -70,13 +79,16 @@ __global__ void __launch_bounds__(256) classify_kernel(EvalParams P, const uint3
         const int cls = rank_class(x.ra + w.ra, x.rb + w.rb);
         // fast pairs: class-major keys [0, kClasses * nfast); m > 0 pairs after them
         key = (uint32_t)(ord < P.nfast ? cls * P.nfast + ord : kClasses * P.nfast + (ord - P.nfast) * kClasses + cls);
-        if (kShared)
-          atomicAdd(&hist[key], 1u);
-        else
-          atomicAdd(&counts[key], 1u);
       }
     }
     keys[i] = key;
+    const unsigned grp = __match_any_sync(__activemask(), key);
+    if (key != kSkipKey && lane == __ffs(grp) - 1) {
+      if (kShared)
+        atomicAdd(&hist[key], (uint32_t)__popc(grp));
+      else
+        atomicAdd(&counts[key], (uint32_t)__popc(grp));
+    }
   }
   if (kShared) {
     __syncthreads();
@@ -114,53 +126,64 @@ __global__ void scan_kernel(const uint32_t* __restrict__ counts, int nkeys, uint
   }
 }
 
+// Scatter each pair (and its position in the request) into key order.  A block owns a
+// contiguous chunk: it counts its keys, reserves one run per key with a single global atomic,
+// then places each pair at run base + rank (warp-aggregated ranks).
 template <bool kShared>
-__global__ void __launch_bounds__(256) scatter_kernel(const uint32_t* __restrict__ keys, uint64_t npairs,
+__global__ void __launch_bounds__(256) scatter_kernel(const uint32_t* __restrict__ keys,
+                                                      const uint32_t* __restrict__ pairs, uint64_t npairs,
                                                       uint32_t* __restrict__ cursor, int nkeys, uint64_t chunk,
-                                                      uint32_t* __restrict__ perm) {
+                                                      uint2* __restrict__ spairs, uint32_t* __restrict__ sidx) {
   extern __shared__ uint32_t base[];
   const uint64_t c0 = blockIdx.x * chunk;
   const uint64_t c1 = min(npairs, c0 + chunk);
   if (c0 >= npairs) return;
-  if (!kShared) {
+  const int lane = threadIdx.x & 31;
+  uint32_t* slot = kShared ? base : cursor;
+  if (kShared) {
+    for (int k = threadIdx.x; k < nkeys; k += blockDim.x) base[k] = 0;
+    __syncthreads();
     for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
       const uint32_t k = keys[i];
-      if (k != kSkipKey) perm[atomicAdd(&cursor[k], 1u)] = (uint32_t)i;
+      const unsigned grp = __match_any_sync(__activemask(), k);
+      if (k != kSkipKey && lane == __ffs(grp) - 1) atomicAdd(&base[k], (uint32_t)__popc(grp));
     }
-    return;
+    __syncthreads();
+    for (int k = threadIdx.x; k < nkeys; k += blockDim.x) {
+      const uint32_t c = base[k];
+      base[k] = c ? atomicAdd(&cursor[k], c) : 0u;
+    }
+    __syncthreads();
   }
-  for (int k = threadIdx.x; k < nkeys; k += blockDim.x) base[k] = 0;
-  __syncthreads();
   for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
     const uint32_t k = keys[i];
-    if (k != kSkipKey) atomicAdd(&base[k], 1u);
-  }
-  __syncthreads();
-  for (int k = threadIdx.x; k < nkeys; k += blockDim.x) {
-    const uint32_t c = base[k];
-    base[k] = c ? atomicAdd(&cursor[k], c) : 0u;
-  }
-  __syncthreads();
-  for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-    const uint32_t k = keys[i];
-    if (k != kSkipKey) perm[atomicAdd(&base[k], 1u)] = (uint32_t)i;
+    const unsigned act = __activemask();
+    const unsigned grp = __match_any_sync(act, k);
+    const int leader = __ffs(grp) - 1;
+    uint32_t b = 0;
+    if (k != kSkipKey && lane == leader) b = atomicAdd(&slot[k], (uint32_t)__popc(grp));
+    b = __shfl_sync(grp, b, leader);
+    if (k != kSkipKey) {
+      const uint32_t pos = b + (uint32_t)__popc(grp & lanemask_lt());
+      spairs[pos] = __ldg(reinterpret_cast<const uint2*>(pairs) + i);
+      sidx[pos] = (uint32_t)i;
+    }
   }
 }
 
-// One kernel per contraction-rank class (L_alpha, L_beta): the sorted range of class c over
-// all fast reference pairs is [offsets[c * nfast], offsets[(c + 1) * nfast]).
+// One contraction-rank class (L_alpha, L_beta) over its sorted range
+// [offsets[c * nfast], offsets[(c + 1) * nfast]) of all fast reference pairs.
 template <int LA, int LB>
-__global__ void __launch_bounds__(256) eval_class_kernel(EvalParams P, const uint32_t* __restrict__ pairs,
-                                                         const uint32_t* __restrict__ perm,
-                                                         const uint32_t* __restrict__ offsets,
-                                                         double* __restrict__ out) {
+__device__ __forceinline__ void run_class(const EvalParams& P, const uint2* __restrict__ spairs,
+                                          const uint32_t* __restrict__ sidx, const uint32_t* __restrict__ offsets,
+                                          double* __restrict__ out) {
   constexpr int c = LA * 5 + LB;
   const uint32_t begin = offsets[c * P.nfast];
   const uint32_t end = offsets[(c + 1) * P.nfast];
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t t = begin + blockIdx.x * blockDim.x + threadIdx.x; t < end; t += stride) {
-    const uint32_t i = perm[t];
-    const uint2 ab = __ldg(reinterpret_cast<const uint2*>(pairs) + i);
+    const uint2 ab = spairs[t];
+    const uint32_t i = sidx[t];
     const DetRec x = load_det(P.dets, ab.x);
     const DetRec w = load_det(P.dets, ab.y);
     const FastPair fp = P.fast[(int)x.parent * P.nref + (int)w.parent];
@@ -170,17 +193,63 @@ __global__ void __launch_bounds__(256) eval_class_kernel(EvalParams P, const uin
   }
 }
 
+// The 25 fixed-rank classes in three kernels grouped by register demand, so the dominant
+// small-rank classes keep a small register footprint (high occupancy) and the rare
+// quadruple-rank classes do not force it up.
+__global__ void __launch_bounds__(256) eval_light_kernel(EvalParams P, const uint2* __restrict__ spairs,
+                                                         const uint32_t* __restrict__ sidx,
+                                                         const uint32_t* __restrict__ offsets,
+                                                         double* __restrict__ out) {
+  run_class<2, 2>(P, spairs, sidx, offsets, out);
+  run_class<2, 1>(P, spairs, sidx, offsets, out);
+  run_class<1, 2>(P, spairs, sidx, offsets, out);
+  run_class<2, 0>(P, spairs, sidx, offsets, out);
+  run_class<0, 2>(P, spairs, sidx, offsets, out);
+  run_class<1, 1>(P, spairs, sidx, offsets, out);
+  run_class<1, 0>(P, spairs, sidx, offsets, out);
+  run_class<0, 1>(P, spairs, sidx, offsets, out);
+  run_class<0, 0>(P, spairs, sidx, offsets, out);
+}
+
+__global__ void __launch_bounds__(256) eval_medium_kernel(EvalParams P, const uint2* __restrict__ spairs,
+                                                          const uint32_t* __restrict__ sidx,
+                                                          const uint32_t* __restrict__ offsets,
+                                                          double* __restrict__ out) {
+  run_class<3, 1>(P, spairs, sidx, offsets, out);
+  run_class<1, 3>(P, spairs, sidx, offsets, out);
+  run_class<3, 0>(P, spairs, sidx, offsets, out);
+  run_class<0, 3>(P, spairs, sidx, offsets, out);
+  run_class<3, 2>(P, spairs, sidx, offsets, out);
+  run_class<2, 3>(P, spairs, sidx, offsets, out);
+  run_class<3, 3>(P, spairs, sidx, offsets, out);
+}
+
+__global__ void __launch_bounds__(256) eval_heavy_kernel(EvalParams P, const uint2* __restrict__ spairs,
+                                                         const uint32_t* __restrict__ sidx,
+                                                         const uint32_t* __restrict__ offsets,
+                                                         double* __restrict__ out) {
+  run_class<4, 0>(P, spairs, sidx, offsets, out);
+  run_class<0, 4>(P, spairs, sidx, offsets, out);
+  run_class<4, 1>(P, spairs, sidx, offsets, out);
+  run_class<1, 4>(P, spairs, sidx, offsets, out);
+  run_class<4, 2>(P, spairs, sidx, offsets, out);
+  run_class<2, 4>(P, spairs, sidx, offsets, out);
+  run_class<4, 3>(P, spairs, sidx, offsets, out);
+  run_class<3, 4>(P, spairs, sidx, offsets, out);
+  run_class<4, 4>(P, spairs, sidx, offsets, out);
+}
+
 // Contraction ranks above 4 in either spin (class 25), runtime-size arithmetic.
-__global__ void __launch_bounds__(128) eval_rt_kernel(EvalParams P, const uint32_t* __restrict__ pairs,
-                                                      const uint32_t* __restrict__ perm,
+__global__ void __launch_bounds__(128) eval_rt_kernel(EvalParams P, const uint2* __restrict__ spairs,
+                                                      const uint32_t* __restrict__ sidx,
                                                       const uint32_t* __restrict__ offsets,
                                                       double* __restrict__ out) {
   const uint32_t begin = offsets[25 * P.nfast];
   const uint32_t end = offsets[26 * P.nfast];
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t t = begin + blockIdx.x * blockDim.x + threadIdx.x; t < end; t += stride) {
-    const uint32_t i = perm[t];
-    const uint2 ab = __ldg(reinterpret_cast<const uint2*>(pairs) + i);
+    const uint2 ab = spairs[t];
+    const uint32_t i = sidx[t];
     const DetRec x = load_det(P.dets, ab.x);
     const DetRec w = load_det(P.dets, ab.y);
     const FastPair fp = P.fast[(int)x.parent * P.nref + (int)w.parent];
@@ -190,15 +259,6 @@ __global__ void __launch_bounds__(128) eval_rt_kernel(EvalParams P, const uint32
   }
 }
 
-using ClassKernel = void (*)(EvalParams, const uint32_t*, const uint32_t*, const uint32_t*, double*);
-
-#define NW_K(A, B) &eval_class_kernel<A, B>
-const ClassKernel kClassKernels[25] = {
-    NW_K(0, 0), NW_K(0, 1), NW_K(0, 2), NW_K(0, 3), NW_K(0, 4), NW_K(1, 0), NW_K(1, 1), NW_K(1, 2), NW_K(1, 3),
-    NW_K(1, 4), NW_K(2, 0), NW_K(2, 1), NW_K(2, 2), NW_K(2, 3), NW_K(2, 4), NW_K(3, 0), NW_K(3, 1), NW_K(3, 2),
-    NW_K(3, 3), NW_K(3, 4), NW_K(4, 0), NW_K(4, 1), NW_K(4, 2), NW_K(4, 3), NW_K(4, 4)};
-#undef NW_K
-
 // ---------------------------------------------------------------------------------------
 // m > 0 reference pairs.
 // ---------------------------------------------------------------------------------------
@@ -207,16 +267,16 @@ __device__ __noinline__ void eval_gen_one(const GenPair& g, const DetRec& x, con
   eval_gen_pair(g, x, w, P.n, P.nocc_a, P.nocc_b, P.enuc, P.tol, P.exact != 0, H, S);
 }
 
-__global__ void __launch_bounds__(128) eval_gen_kernel(EvalParams P, const uint32_t* __restrict__ pairs,
-                                                       const uint32_t* __restrict__ perm,
+__global__ void __launch_bounds__(128) eval_gen_kernel(EvalParams P, const uint2* __restrict__ spairs,
+                                                       const uint32_t* __restrict__ sidx,
                                                        const uint32_t* __restrict__ offsets, int nkeys,
                                                        double* __restrict__ out) {
   const uint32_t begin = offsets[kClasses * P.nfast];
   const uint32_t end = offsets[nkeys];
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t t = begin + blockIdx.x * blockDim.x + threadIdx.x; t < end; t += stride) {
-    const uint32_t i = perm[t];
-    const uint2 ab = __ldg(reinterpret_cast<const uint2*>(pairs) + i);
+    const uint2 ab = spairs[t];
+    const uint32_t i = sidx[t];
     const DetRec x = load_det(P.dets, ab.x);
     const DetRec w = load_det(P.dets, ab.y);
     const GenPair& g = P.gen[(int)x.parent * P.nref + (int)w.parent];
@@ -300,10 +360,12 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
   const int nkeys = ctx->nref * ctx->nref * kClasses;
   if ((st = ensure(ctx, ctx->keys, npairs * sizeof(uint32_t))) != NW_OK) return st;
   if ((st = ensure(ctx, ctx->perm, npairs * sizeof(uint32_t))) != NW_OK) return st;
+  if ((st = ensure(ctx, ctx->spairs, npairs * sizeof(uint2))) != NW_OK) return st;
   if ((st = ensure(ctx, ctx->counts, (size_t)(nkeys + 1) * sizeof(uint32_t) * 2)) != NW_OK) return st;
   if ((st = ensure(ctx, ctx->offsets, (size_t)(nkeys + 1) * sizeof(uint32_t))) != NW_OK) return st;
   uint32_t* keys = static_cast<uint32_t*>(ctx->keys.p);
-  uint32_t* perm = static_cast<uint32_t*>(ctx->perm.p);
+  uint32_t* sidx = static_cast<uint32_t*>(ctx->perm.p);
+  uint2* spairs = static_cast<uint2*>(ctx->spairs.p);
   uint32_t* counts = static_cast<uint32_t*>(ctx->counts.p);
   uint32_t* cursor = counts + (nkeys + 1);
   uint32_t* offsets = static_cast<uint32_t*>(ctx->offsets.p);
@@ -326,23 +388,22 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
   const uint64_t chunk = std::max<uint64_t>(4096, (npairs + 148 * 8 - 1) / (148 * 8));
   const int sblocks = (int)((npairs + chunk - 1) / chunk);
   if (shared_hist)
-    scatter_kernel<true><<<sblocks, 256, hist_bytes, stream>>>(keys, npairs, cursor, nkeys, chunk, perm);
+    scatter_kernel<true><<<sblocks, 256, hist_bytes, stream>>>(keys, pairs, npairs, cursor, nkeys, chunk, spairs, sidx);
   else
-    scatter_kernel<false><<<sblocks, 256, 0, stream>>>(keys, npairs, cursor, nkeys, chunk, perm);
+    scatter_kernel<false><<<sblocks, 256, 0, stream>>>(keys, pairs, npairs, cursor, nkeys, chunk, spairs, sidx);
   NW_CUDA(ctx, cudaGetLastError());
   if (tm) NW_CUDA(ctx, cudaEventRecord(ctx->ev[3], stream));
   if (ctx->nfast > 0) {
-    // Class kernels in order of decreasing expected work would not change the total; the grid
-    // is sized for the whole batch and threads beyond a class's range exit at once.
-    const int cgrid = grid_stride_blocks(npairs, 256, 8);
-    for (int c = 0; c < 25; ++c) kClassKernels[c]<<<cgrid, 256, 0, stream>>>(P, pairs, perm, offsets, out);
-    NW_CUDA(ctx, cudaGetLastError());
-    eval_rt_kernel<<<148 * 2, 128, 0, stream>>>(P, pairs, perm, offsets, out);
+    const int g = grid_stride_blocks(npairs, 256, 8);
+    eval_light_kernel<<<g, 256, 0, stream>>>(P, spairs, sidx, offsets, out);
+    eval_medium_kernel<<<148 * 2, 256, 0, stream>>>(P, spairs, sidx, offsets, out);
+    eval_heavy_kernel<<<148, 256, 0, stream>>>(P, spairs, sidx, offsets, out);
+    eval_rt_kernel<<<148 * 2, 128, 0, stream>>>(P, spairs, sidx, offsets, out);
     NW_CUDA(ctx, cudaGetLastError());
   }
   if (tm) NW_CUDA(ctx, cudaEventRecord(ctx->ev[4], stream));
   if (ctx->nfast < ctx->nref * ctx->nref) {
-    eval_gen_kernel<<<148 * 4, 128, 0, stream>>>(P, pairs, perm, offsets, nkeys, out);
+    eval_gen_kernel<<<148 * 4, 128, 0, stream>>>(P, spairs, sidx, offsets, nkeys, out);
     NW_CUDA(ctx, cudaGetLastError());
   }
   if (tm) {

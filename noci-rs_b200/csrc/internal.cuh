@@ -69,7 +69,7 @@ struct nw_ctx {
   uint64_t ndet = 0;
 
   // evaluation scratch (grown on demand)
-  nw::DevBuf keys, perm, counts, offsets, flag;
+  nw::DevBuf keys, perm, spairs, counts, offsets, flag;
   uint32_t* h_flag = nullptr;      // pinned mirror of the device error flag
   nw::DevBuf io_pairs, io_hs;      // staging for the host-buffer entry point
 

@@ -62,6 +62,9 @@ def lib():
         L.orc_eval_overlap.argtypes = [dp, i64p, dp, i32p, ctypes.c_int, ctypes.c_void_p,
                                        ctypes.c_int64, ctypes.c_int64, dp]
         L.orc_eval_overlap.restype = ctypes.c_int
+        L.orc_eval_m_pairs.argtypes = [dp, i64p, dp, i32p, ctypes.c_int, ctypes.c_void_p, i64p, ctypes.c_int64,
+                                       dp, i64p, dp, ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp, dp]
+        L.orc_eval_m_pairs.restype = ctypes.c_int
         assert L.orc_layout(3) == ORACLE_DET_DTYPE.itemsize, "oracle Det layout mismatch"
         _lib = L
     return _lib
@@ -280,6 +283,49 @@ class Oracle:
                            self.nref, obasis.ctypes.data_as(ctypes.c_void_p), a, b,
                            ctypes.byref(s))
         return s.value
+
+    def set_fock(self, fa: np.ndarray, fb: np.ndarray):
+        """update_wicks_fock (src/noci/wicks.rs:290-330): Fock intermediates of every pair."""
+        w = _SlabWriter()
+        npair = len(self.builds)
+        foffs = np.zeros((npair, 2, 4), np.int64)
+        fvals = np.zeros((npair, 2, 2))
+        for p in range(npair):
+            x, wref = divmod(p, self.nref)
+            rx, rw = self.refs[x], self.refs[wref]
+            for sp, fock in enumerate((fa, fb)):
+                cx, ox = (rx[0], rx[1]) if sp == 0 else (rx[2], rx[3])
+                cw, ow = (rw[0], rw[1]) if sp == 0 else (rw[2], rw[3])
+                f0, ff = _wb.construct_f(self.s, fock, cx, ox, cw, ow, self.tol)
+                fvals[p, sp] = f0
+                for k in range(4):
+                    foffs[p, sp, k] = w.put(ff[k >> 1][k & 1].T)
+        self.fslab, self.foffs, self.fvals = w.finish(), foffs, fvals
+        return self
+
+    def eval_m_pairs(self, obasis: np.ndarray, pairs: np.ndarray, e0: float, exact: bool = False):
+        """(M, F, S) per pair with M = F - E0 S (calculate_m_pair_wicks, src/noci/m.rs:160-197)."""
+        L = lib()
+        pairs = np.ascontiguousarray(pairs, dtype=np.int64)
+        n = pairs.shape[0]
+        m, f, s = np.empty(n), np.empty(n), np.empty(n)
+        L.orc_eval_m_pairs(_ptr(self.slab, ctypes.c_double), _ptr(self.offs, ctypes.c_int64),
+                           _ptr(self.vals, ctypes.c_double), _ptr(self.ints, ctypes.c_int32), self.nref,
+                           obasis.ctypes.data_as(ctypes.c_void_p), _ptr(pairs, ctypes.c_int64), n,
+                           _ptr(self.fslab, ctypes.c_double), _ptr(self.foffs, ctypes.c_int64),
+                           _ptr(self.fvals, ctypes.c_double), e0, self.tol, 1 if exact else 0,
+                           _ptr(m, ctypes.c_double), _ptr(f, ctypes.c_double), _ptr(s, ctypes.c_double))
+        return m, f, s
+
+    def naive_m(self, obasis: np.ndarray, a: int, b: int, fa, fb, e0: float):
+        """calculate_m_pair_naive (src/noci/m.rs:106-130) between canonical determinants."""
+        ca_x, oa_x, cb_x, ob_x = self.det_orbitals(obasis, a)
+        ca_w, oa_w, cb_w, ob_w = self.det_orbitals(obasis, b)
+        pa = _naive.build_s_pair(_wb.occ_coeffs(ca_x, oa_x), _wb.occ_coeffs(ca_w, oa_w), self.s, self.tol)
+        pb = _naive.build_s_pair(_wb.occ_coeffs(cb_x, ob_x), _wb.occ_coeffs(cb_w, ob_w), self.s, self.tol)
+        s = pa.s * pb.s
+        f = pb.s * _naive.one_electron(fa, pa) + pa.s * _naive.one_electron(fb, pb)
+        return f - e0 * s, f, s
 
     def det_orbitals(self, obasis: np.ndarray, i: int):
         """Orbital coefficients and integer occupation masks of determinant i (naive path)."""

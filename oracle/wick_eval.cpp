@@ -730,6 +730,62 @@ void eval_one(const Ctx& c, int64_t a, int64_t b, double* h, double* s) {
     hs_gen(pv, pa, pb, exc, c.enuc, c.tol, c.exact, h, s);
 }
 
+// ---------------------------------------------------------------------------------------
+// Fock one-body element and the SNOCI operator M = F - E0 S (onebody.rs:40-520, m.rs:160-197).
+// Per pair and spin: F0f[2] (scalar) and ff_t[2][2] (transposed [c][r]) from
+// construct_f_scalar (build.rs:564-617).
+// ---------------------------------------------------------------------------------------
+struct FockSpin {
+  double f0f[2];
+  const double* ff_t[2][2];
+};
+
+// xw_f for one spin: phase * tsp * sum over distributions of the one-body operator
+// (m = 0: one distribution, no threshold; m > 0: get_det_adjt_same with pbits = 1).
+double xw_f_spin(const SpinView& w, const FockSpin& f, const SpinPrep& p, double tol, bool exact) {
+  const int l = p.l, n = w.nmo;
+  double acc = 0.0;
+  double dm[kMaxL * kMaxL], cof[kMaxL * kMaxL];
+  if (w.m == 0) {
+    double det = 1.0;
+    if (l > 0) det = cofactors(cof, p.d0, l);
+    double contrib = det * f.f0f[0];
+    for (int b = 0; b < l; ++b) {
+      const double* fsl = f.ff_t[0][0];
+      const int64_t base = (int64_t)p.cols[b] * n;
+      double corr = 0.0;
+      for (int r = 0; r < l; ++r) corr += (fsl[base + p.rows[r]] - p.d0[r * l + b]) * cof[r * l + b];
+      contrib -= det + corr;
+    }
+    acc = contrib;
+  } else {
+    for_each_m_combination(l + 1, w.m, [&](uint64_t bits) {
+      const int mi = bit(bits, 0);
+      const uint64_t cb = bits >> 1;
+      mix(dm, p, cb);
+      double det = 1.0;
+      bool ok = true;
+      if (l > 0) {
+        if (exact)
+          det = cofactors(cof, dm, l);
+        else
+          ok = cofactors_tol(cof, dm, l, tol, &det);
+      }
+      if (!ok) return;
+      double contrib = det * f.f0f[mi];
+      for (int b = 0; b < l; ++b) {
+        const double* fsl = f.ff_t[mi][bit(cb, b)];
+        const int64_t base = (int64_t)p.cols[b] * n;
+        double corr = 0.0;
+        for (int r = 0; r < l; ++r) corr += (fsl[base + p.rows[r]] - dm[r * l + b]) * cof[r * l + b];
+        contrib -= det + corr;
+      }
+      acc += contrib;
+    });
+  }
+  return w.phase * w.tsp * acc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -833,6 +889,43 @@ int orc_eval_overlap(const double* slab, const int64_t* offs, const double* vals
   prepare_same(pv.bb, x.holes_b, x.parts_b, x.rank_b, w.holes_b, w.parts_b, w.rank_b, pb);
   const double exc = (x.pha * w.pha) * (x.phb * w.phb);
   *s = exc * overlap_spin(pv.aa, pa) * overlap_spin(pv.bb, pb);
+  return 0;
+}
+
+// M = F - E0 S for npairs pairs via the Wick path (calculate_m_pair_wicks, m.rs:160-197).
+// focks: per ordered pair, per spin, offsets of ff_t[2][2] into fslab and f0f[2] values.
+int orc_eval_m_pairs(const double* slab, const int64_t* offs, const double* vals, const int32_t* ints, int nref,
+                     const void* basis, const int64_t* pairs, int64_t npairs, const double* fslab,
+                     const int64_t* foffs, const double* fvals, double e0, double tol, int flags, double* m_out,
+                     double* f_out, double* s_out) {
+  const Det* bs = reinterpret_cast<const Det*>(basis);
+  const bool exact = (flags & 1) != 0;
+  for (int64_t i = 0; i < npairs; ++i) {
+    const Det& x = bs[pairs[2 * i]];
+    const Det& w = bs[pairs[2 * i + 1]];
+    const int64_t pidx = (int64_t)x.parent * nref + w.parent;
+    const PairView pv = make_view(slab, offs + pidx * kNoff, vals + pidx * kNval, ints + pidx * kNint);
+    SpinPrep pa, pb;
+    prepare_same(pv.aa, x.holes_a, x.parts_a, x.rank_a, w.holes_a, w.parts_a, w.rank_a, pa);
+    prepare_same(pv.bb, x.holes_b, x.parts_b, x.rank_b, w.holes_b, w.parts_b, w.rank_b, pb);
+    FockSpin fs[2];
+    for (int sp = 0; sp < 2; ++sp) {
+      const int64_t* fo = foffs + (pidx * 2 + sp) * 4;
+      for (int k = 0; k < 4; ++k) fs[sp].ff_t[k >> 1][k & 1] = fslab + fo[k];
+      fs[sp].f0f[0] = fvals[(pidx * 2 + sp) * 2];
+      fs[sp].f0f[1] = fvals[(pidx * 2 + sp) * 2 + 1];
+    }
+    const double ph = (x.pha * w.pha) * (x.phb * w.phb);
+    const double oa = overlap_spin(pv.aa, pa), ob = overlap_spin(pv.bb, pb);
+    double f = 0.0;
+    if (ob != 0.0) f += xw_f_spin(pv.aa, fs[0], pa, tol, exact) * ob;
+    if (oa != 0.0) f += xw_f_spin(pv.bb, fs[1], pb, tol, exact) * oa;
+    f *= ph;
+    const double s = ph * oa * ob;
+    f_out[i] = f;
+    s_out[i] = s;
+    m_out[i] = f - e0 * s;
+  }
   return 0;
 }
 

@@ -98,3 +98,28 @@ def test_no_device_reported_without_gpu():
 def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(RuntimeError):
         L.load(str(tmp_path / "absent.so"))
+
+
+def test_cxx_host_interface_compiles_and_links(tmp_path):
+    """The header-only C++ mirror of the reference interface builds against the library."""
+    src = tmp_path / "use.cpp"
+    src.write_text(r'''
+#include "wicks.hpp"
+int main() {
+  nociwick::AoData ao;
+  nociwick::References refs;
+  try {
+    auto w = nociwick::build_wicks_shared(ao, refs, 1e-8);
+    (void)w;
+  } catch (const nociwick::Error& e) {
+    return e.status == NW_ERR_INVALID ? 0 : 1;
+  }
+  return 2;
+}
+''')
+    exe = tmp_path / "use"
+    libdir = os.path.dirname(nociwick.LIB_PATH)
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I", os.path.join(ROOT, "noci-rs_b200", "host"),
+                    str(src), "-L", libdir, "-lnociwick", "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
+    # empty inputs are rejected with NW_ERR_INVALID before any device use
+    assert subprocess.run([str(exe)]).returncode == 0

@@ -143,7 +143,8 @@ def test_invalid_basis_rejected():
     system = sy.make_system(8, 3, 3, 2, 20, seed=4)
     basis = sy.sd_basis(8, 3, 3, 2)
     bad = basis.copy()
-    bad["idx_a"][5, 4] = 1          # particle index inside the occupied block
+    k = int(np.nonzero(basis["rank_a"] == 1)[0][0])
+    bad["idx_a"][k, 4] = 1          # particle index inside the occupied block
     with _engine(system) as w:
         with pytest.raises(nociwick.NwError):
             w.set_basis(bad)
@@ -163,3 +164,26 @@ def test_config3_full_orbital_count():
     for convention in ("reference", "exact"):
         dh, ds, *_ = _compare(system, basis, pairs, convention, orc=orc)
         assert dh.max() <= ATOL_STRESS and ds.max() <= ATOL_STRESS, (convention, dh.max(), ds.max())
+
+
+def test_golden_fixtures():
+    """GPU against the committed fixtures (oracle values and brute-force Fock-space values)."""
+    import os
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    g = np.load(os.path.join(gold, "tiny_zero_overlap.npz"))
+    refs = [(g["ca"][i], 3, g["cb"][i], 3) for i in range(g["ca"].shape[0])]
+    for convention, hk, sk in (("reference", "h_ref", "s_ref"), ("exact", "h_exact", "s_exact")):
+        with nociwick.WicksShared(g["s"], g["h"], g["eri"], float(g["enuc"]), refs, tol=float(g["tol"]),
+                                  convention=convention) as w:
+            w.build().set_basis(g["basis"])
+            hs = w.eval_pairs(g["pairs"])
+        assert np.max(np.abs(hs[:, 0] - g[hk])) <= ATOL and np.max(np.abs(hs[:, 1] - g[sk])) <= ATOL
+        if convention == "exact":
+            n = g["fock_hs"].shape[0]
+            assert np.max(np.abs(hs[:n] - g["fock_hs"])) <= ATOL
+    c2 = np.load(os.path.join(gold, "config2_sample.npz"))
+    system = sy.config2_system()
+    with _engine(system) as w:
+        w.set_basis(sy.sd_basis(30, 3, 3, 3))
+        hs = w.eval_pairs(c2["pairs"])
+    assert np.max(np.abs(hs[:, 0] - c2["h"])) <= ATOL and np.max(np.abs(hs[:, 1] - c2["s"])) <= ATOL

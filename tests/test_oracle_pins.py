@@ -180,3 +180,27 @@ def test_reference_and_exact_agree_without_zero_overlap(small_m0):
     system, basis, orc, ob, fs = small_m0
     for a, b in _sample(basis, 100, 8):
         assert orc.eval_wick(ob, int(a), int(b)) == orc.eval_wick(ob, int(a), int(b), exact=True)
+
+
+@pytest.mark.parametrize("zp", [[], [(0, 1, 1, 0)], [(0, 1, 0, 2)]])
+def test_fock_m_operator_matches_naive(zp):
+    """SNOCI operator M = F - E0 S (calculate_m_pair_wicks, src/noci/m.rs:160-197) from the Fock
+    intermediates of update_wicks_fock equals the generalised Slater-Condon M
+    (calculate_m_pair_naive) for m = 0 and, in the exact convention, for m > 0."""
+    system = sy.make_system(8, 3, 3, 3, 20, seed=1, k_scale=0.3, zero_pairs=zp)
+    orc = Oracle.from_system(system, tol=1e-8)
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal((8, 8))
+    b = rng.standard_normal((8, 8))
+    fa, fb = a + a.T, b + b.T
+    orc.set_fock(fa, fb)
+    basis = sy.sd_basis(8, 3, 3, 3)
+    ob = orc.oracle_basis(basis)
+    pairs = sy.sample_pairs(basis, 300, seed=2, distinct_parents=False)
+    m, f, s = orc.eval_m_pairs(ob, pairs, -1.7, exact=True)
+    for k, (x, w) in enumerate(pairs):
+        mn, fn, sn = orc.naive_m(ob, int(x), int(w), fa, fb, -1.7)
+        assert abs(m[k] - mn) < 1e-12 and abs(s[k] - sn) < 1e-12
+    if not zp:
+        mr, _, _ = orc.eval_m_pairs(ob, pairs, -1.7, exact=False)
+        assert np.array_equal(mr, m)
