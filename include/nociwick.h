@@ -136,6 +136,20 @@ NW_API nw_status nw_eval_hs_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev,
 NW_API nw_status nw_eval_hs_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* hs_host,
                            void* stream);
 
+/* (H, S) exactly as nw_eval_hs_pairs_device, but without allocating device memory: for callers
+ * that cannot call cudaMalloc while they evaluate pairs (a host whose memory pool already owns
+ * nearly all of HBM, or a latency-critical loop that cannot take cudaMalloc's implicit
+ * synchronisation or its failure path).  No counterpart in the reference.
+ * Limits: at most 1,048,576 pairs per call and at most 64 references (larger requests return
+ * NW_ERR_UNSUPPORTED).  The per-call scratch lives in one fixed device array of about 18 MB that
+ * every GPU loading this library holds until the process exits; its device address is looked
+ * up on the first call on each device, so make that first call before any stream capture.
+ * All calls share the array: calls whose work overlaps on the GPU race and must be serialised.
+ * Pair indices out of range of the basis give NaN results (this variant does not report them
+ * through nw_sync). */
+NW_API nw_status nw_eval_hs_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs,
+                                          double* hs_dev, void* stream);
+
 /* Overlap only, S for each pair (hs_dev[i]), device buffers.
  * Replaces xw_overlap (src/nonorthogonalwicks/eval/overlap.rs:42-65) times the phases. */
 NW_API nw_status nw_eval_s_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* s_dev,

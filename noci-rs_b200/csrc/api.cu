@@ -186,6 +186,12 @@ nw_status nw_eval_hs_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64
   return nw::eval_pairs(ctx, pairs_dev, npairs, hs_dev, false, static_cast<cudaStream_t>(stream));
 }
 
+nw_status nw_eval_hs_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* hs_dev,
+                                   void* stream) {
+  if (!ctx || (npairs && (!pairs_dev || !hs_dev))) return NW_ERR_INVALID;
+  return nw::eval_pairs_noalloc(ctx, pairs_dev, npairs, hs_dev, static_cast<cudaStream_t>(stream));
+}
+
 nw_status nw_eval_s_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* s_dev,
                                  void* stream) {
   if (!ctx || (npairs && (!pairs_dev || !s_dev))) return NW_ERR_INVALID;

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 
 #include "internal.cuh"
@@ -409,6 +410,133 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
   if (tm) {
     NW_CUDA(ctx, cudaEventRecord(ctx->ev[5], stream));
     ctx->timed_valid = true;
+  }
+  return NW_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free variant of the pair evaluation (nw_eval_hs_pairs_noalloc).
+//
+// Some callers cannot allocate device memory when they evaluate pairs: a host that hands
+// nearly all of HBM to its own memory pool (a framework's caching allocator, a solver's
+// preallocated workspace), or a latency-critical loop that cannot afford cudaMalloc's implicit
+// synchronisation or its failure path.  For them the per-call scratch of the evaluation (keys,
+// key-sorted pair payload, request indices, per-key counts and offsets, error flag) lives in
+// the fixed device array below instead of buffers grown with cudaMalloc.
+//
+// The array is a file-scope __device__ variable, so every GPU that loads this library holds
+// it (18,055,680 bytes, 17.2 MiB) until the process exits.  Host code cannot use its name as a device
+// address: the address is looked up with cudaGetSymbolAddress once per device, with that
+// device current, on the first call of the entry point on that device (that first call
+// should therefore come before any stream capture).  Every call shares the array and it keeps
+// the last call's contents: the counts and the error flag are cleared at the start of each
+// call, and calls whose work overlaps on the GPU (different streams, concurrent host threads)
+// race on it and must be serialised by the caller.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+constexpr uint64_t kNoallocMaxPairs = 1ull << 20;                       // 1,048,576 pairs per call
+constexpr int kNoallocMaxRefs = 64;                                      // reference determinants
+constexpr uint64_t kNoallocMaxKeys = (uint64_t)kNoallocMaxRefs * kNoallocMaxRefs * kClasses;
+constexpr uint64_t kNoallocOffKeys = 0;
+constexpr uint64_t kNoallocOffPairs = kNoallocOffKeys + 4 * kNoallocMaxPairs;
+constexpr uint64_t kNoallocOffIdx = kNoallocOffPairs + 8 * kNoallocMaxPairs;
+constexpr uint64_t kNoallocOffCounts = kNoallocOffIdx + 4 * kNoallocMaxPairs;
+constexpr uint64_t kNoallocOffOffsets = kNoallocOffCounts + 8 * (kNoallocMaxKeys + 1);
+constexpr uint64_t kNoallocOffFlag = ((kNoallocOffOffsets + 4 * (kNoallocMaxKeys + 1) + 255) / 256) * 256;
+constexpr uint64_t kNoallocBytes = kNoallocOffFlag + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device (looked up once per device).
+nw_status noalloc_scratch(nw_ctx* ctx, unsigned char** out) {
+  if (ctx->device < 0 || ctx->device >= kNoallocMaxDevices)
+    return fail(ctx, NW_ERR_UNSUPPORTED, "device ordinal too large for the allocation-free entry point");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[ctx->device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return cuda_fail(ctx, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    g_noalloc_ptr[ctx->device] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_ptr[ctx->device]);
+  return NW_OK;
+}
+
+}  // namespace
+
+nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, cudaStream_t stream) {
+  if (!ctx->built) return fail(ctx, NW_ERR_STATE, "intermediates not built");
+  if (!ctx->d_dets) return fail(ctx, NW_ERR_STATE, "no determinant basis set");
+  if (npairs > kNoallocMaxPairs)
+    return fail(ctx, NW_ERR_UNSUPPORTED, "allocation-free evaluation takes at most " +
+                                              std::to_string(kNoallocMaxPairs) + " pairs per call");
+  if (ctx->nref > kNoallocMaxRefs)
+    return fail(ctx, NW_ERR_UNSUPPORTED, "allocation-free evaluation supports at most " +
+                                              std::to_string(kNoallocMaxRefs) + " references");
+  if ((reinterpret_cast<uintptr_t>(pairs) & 7) != 0) return fail(ctx, NW_ERR_INVALID, "pairs must be 8-byte aligned");
+  if ((reinterpret_cast<uintptr_t>(out) & 15) != 0) return fail(ctx, NW_ERR_INVALID, "output must be 16-byte aligned");
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  unsigned char* base = nullptr;
+  nw_status st = noalloc_scratch(ctx, &base);
+  if (st != NW_OK) return st;
+  if (npairs == 0) return NW_OK;
+  EvalParams P;
+  P.dets = ctx->d_dets;
+  P.ndet = ctx->ndet;
+  P.fast = ctx->d_fast;
+  P.gen = ctx->d_gen;
+  P.order = ctx->d_order;
+  P.nref = ctx->nref;
+  P.n = ctx->nmo;
+  P.nocc_a = ctx->nocc_a;
+  P.nocc_b = ctx->nocc_b;
+  P.nfast = ctx->nfast;
+  P.exact = ctx->convention == NW_CONVENTION_EXACT ? 1 : 0;
+  P.enuc = ctx->enuc;
+  P.tol = ctx->tol;
+  const int nkeys = ctx->nref * ctx->nref * kClasses;
+  uint32_t* keys = reinterpret_cast<uint32_t*>(base + kNoallocOffKeys);
+  uint2* spairs = reinterpret_cast<uint2*>(base + kNoallocOffPairs);
+  uint32_t* sidx = reinterpret_cast<uint32_t*>(base + kNoallocOffIdx);
+  uint32_t* counts = reinterpret_cast<uint32_t*>(base + kNoallocOffCounts);
+  uint32_t* cursor = counts + (nkeys + 1);
+  uint32_t* offsets = reinterpret_cast<uint32_t*>(base + kNoallocOffOffsets);
+  uint32_t* flag = reinterpret_cast<uint32_t*>(base + kNoallocOffFlag);
+  NW_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(uint32_t), stream));
+  NW_CUDA(ctx, cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (nkeys + 1), stream));
+  const size_t hist_bytes = (size_t)nkeys * sizeof(uint32_t);
+  const bool shared_hist = hist_bytes <= 48 * 1024;
+  const int cblocks = grid_stride_blocks(npairs, 256, 8);
+  if (shared_hist)
+    classify_kernel<true><<<cblocks, 256, hist_bytes, stream>>>(P, pairs, npairs, keys, counts, nkeys, out, 2, flag);
+  else
+    classify_kernel<false><<<cblocks, 256, 0, stream>>>(P, pairs, npairs, keys, counts, nkeys, out, 2, flag);
+  NW_CUDA(ctx, cudaGetLastError());
+  scan_kernel<<<1, 1024, 0, stream>>>(counts, nkeys, offsets, cursor);
+  NW_CUDA(ctx, cudaGetLastError());
+  const uint64_t chunk = std::max<uint64_t>(4096, (npairs + 148 * 8 - 1) / (148 * 8));
+  const int sblocks = (int)((npairs + chunk - 1) / chunk);
+  if (shared_hist)
+    scatter_kernel<true><<<sblocks, 256, hist_bytes, stream>>>(keys, pairs, npairs, cursor, nkeys, chunk, spairs, sidx);
+  else
+    scatter_kernel<false><<<sblocks, 256, 0, stream>>>(keys, pairs, npairs, cursor, nkeys, chunk, spairs, sidx);
+  NW_CUDA(ctx, cudaGetLastError());
+  if (ctx->nfast > 0) {
+    const int g = grid_stride_blocks(npairs, 256, 8);
+    eval_light_kernel<<<g, 256, 0, stream>>>(P, spairs, sidx, offsets, out);
+    eval_medium_kernel<<<148 * 2, 256, 0, stream>>>(P, spairs, sidx, offsets, out);
+    eval_heavy_kernel<<<148, 256, 0, stream>>>(P, spairs, sidx, offsets, out);
+    eval_rt_kernel<<<148 * 2, 128, 0, stream>>>(P, spairs, sidx, offsets, out);
+    NW_CUDA(ctx, cudaGetLastError());
+  }
+  if (ctx->nfast < ctx->nref * ctx->nref) {
+    eval_gen_kernel<<<148 * 4, 128, 0, stream>>>(P, spairs, sidx, offsets, nkeys, out);
+    NW_CUDA(ctx, cudaGetLastError());
   }
   return NW_OK;
 }

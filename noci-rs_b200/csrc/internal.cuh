@@ -95,6 +95,8 @@ nw_status build_all(nw_ctx* ctx);
 // Evaluation (eval.cu).
 nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, bool overlap_only,
                      cudaStream_t stream);
+// Same evaluation with its scratch in a fixed device array (no device allocation).
+nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, cudaStream_t stream);
 
 }  // namespace nw
 

@@ -28,6 +28,7 @@ NW_OK = 0
 _STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "allocation failed", 4: "unsupported input",
            5: "call out of order", 6: "no CUDA device"}
 CONVENTIONS = {"reference": 0, "exact": 1}
+NOALLOC_MAX_PAIRS = 1 << 20
 
 
 class NwError(RuntimeError):
@@ -57,7 +58,8 @@ class NwInfo(ctypes.Structure):
 
 
 EXPORTED = ("nw_ctx_create", "nw_build_intermediates", "nw_pair_zero_counts", "nw_set_basis",
-            "nw_eval_hs_pairs_device", "nw_eval_hs_pairs", "nw_eval_s_pairs_device", "nw_sync",
+            "nw_eval_hs_pairs_device", "nw_eval_hs_pairs", "nw_eval_hs_pairs_noalloc",
+            "nw_eval_s_pairs_device", "nw_sync",
             "nw_set_timing", "nw_last_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
             "nw_last_error")
 
@@ -80,6 +82,7 @@ def load(path: Optional[str] = None):
     L.nw_set_basis.argtypes = [vp, vp, ctypes.c_uint64]
     L.nw_eval_hs_pairs_device.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_eval_hs_pairs.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
+    L.nw_eval_hs_pairs_noalloc.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_eval_s_pairs_device.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_sync.argtypes = [vp, vp]
     L.nw_set_timing.argtypes = [vp, ctypes.c_int]
@@ -195,6 +198,13 @@ class WicksShared:
         self._check(self._lib.nw_eval_hs_pairs_device(self._ctx, ctypes.c_void_p(pairs_ptr), npairs,
                                                       ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream)),
                     "nw_eval_hs_pairs_device")
+
+    def eval_pairs_noalloc(self, pairs_ptr: int, npairs: int, out_ptr: int, stream: int = 0):
+        """(H, S) into device memory without any device allocation (fixed scratch array; at most
+        NOALLOC_MAX_PAIRS pairs per call; calls sharing the GPU must not overlap)."""
+        self._check(self._lib.nw_eval_hs_pairs_noalloc(self._ctx, ctypes.c_void_p(pairs_ptr), npairs,
+                                                       ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream)),
+                    "nw_eval_hs_pairs_noalloc")
 
     def eval_overlap_device(self, pairs_ptr: int, npairs: int, out_ptr: int, stream: int = 0):
         self._check(self._lib.nw_eval_s_pairs_device(self._ctx, ctypes.c_void_p(pairs_ptr), npairs,
