@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cublas_v2.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -58,6 +59,93 @@ bool finite_all(const double* p, size_t n) {
   for (size_t i = 0; i < n; ++i)
     if (!std::isfinite(p[i])) return false;
   return true;
+}
+
+// Page-locked host memory (cudaHostAlloc / cudaHostRegister): only such buffers let the copy
+// engines run asynchronously, so only they take the pipelined path.
+bool is_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+nw_status pipe_setup(nw_ctx* ctx) {
+  if (ctx->s_in) return NW_OK;
+  NW_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_in, cudaStreamNonBlocking));
+  NW_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_comp, cudaStreamNonBlocking));
+  NW_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking));
+  NW_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_start, cudaEventDisableTiming));
+  for (int i = 0; i < 2; ++i) {
+    NW_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_in[i], cudaEventDisableTiming));
+    NW_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_comp[i], cudaEventDisableTiming));
+  }
+  return NW_OK;
+}
+
+// Waits for everything the pipeline queued (the caller's host buffers must not be touched by
+// copies after the call returns, also on error paths).
+cudaError_t pipe_drain(nw_ctx* ctx) {
+  cudaError_t first = cudaSuccess;
+  for (cudaStream_t q : {ctx->s_in, ctx->s_comp, ctx->s_out}) {
+    if (!q) continue;
+    const cudaError_t e = cudaStreamSynchronize(q);
+    if (first == cudaSuccess) first = e;
+  }
+  return first;
+}
+
+// Host-buffer evaluation as a three-stage pipeline over chunks of the request: chunk k+1 is
+// copied in (copy engine, host -> device) while chunk k is evaluated and chunk k-1 is copied
+// out (second copy engine, device -> host), so PCIe transfer in both directions overlaps the
+// kernels.  Starts after the work already queued on `caller` and returns when the results
+// are in hs_host.
+nw_status eval_hs_pipelined(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* hs_host, uint32_t* dp,
+                            double* dh, cudaStream_t caller) {
+  nw_status st = pipe_setup(ctx);
+  if (st != NW_OK) return st;
+  if ((st = nw::ensure(ctx, ctx->flag, 256)) != NW_OK) return st;
+  uint32_t* flag = static_cast<uint32_t*>(ctx->flag.p);
+  NW_CUDA(ctx, cudaEventRecord(ctx->ev_start, caller));
+  for (cudaStream_t q : {ctx->s_in, ctx->s_comp, ctx->s_out}) NW_CUDA(ctx, cudaStreamWaitEvent(q, ctx->ev_start, 0));
+  NW_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(uint32_t), ctx->s_comp));
+  uint64_t chunk = (npairs + nw::kPipeChunks - 1) / nw::kPipeChunks;
+  chunk = std::max<uint64_t>(nw::kPipeMinChunk, (chunk + 255) / 256 * 256);
+  uint64_t k = 0;
+  for (uint64_t o = 0; o < npairs; o += chunk, ++k) {
+    const uint64_t nk = std::min(chunk, npairs - o);
+    const int slot = (int)(k & 1);
+    cudaError_t e = cudaMemcpyAsync(dp + 2 * o, pairs_host + 2 * o, nk * 2 * sizeof(uint32_t),
+                                    cudaMemcpyHostToDevice, ctx->s_in);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_in[slot], ctx->s_in);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->s_comp, ctx->ev_in[slot], 0);
+    if (e != cudaSuccess) {
+      pipe_drain(ctx);
+      return nw::cuda_fail(ctx, e, "pipelined copy-in");
+    }
+    st = nw::eval_pairs(ctx, dp + 2 * o, nk, dh + 2 * o, false, ctx->s_comp, false);
+    if (st != NW_OK) {
+      pipe_drain(ctx);
+      return st;
+    }
+    e = cudaEventRecord(ctx->ev_comp[slot], ctx->s_comp);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->s_out, ctx->ev_comp[slot], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(hs_host + 2 * o, dh + 2 * o, nk * 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->s_out);
+    if (e != cudaSuccess) {
+      pipe_drain(ctx);
+      return nw::cuda_fail(ctx, e, "pipelined copy-out");
+    }
+  }
+  cudaError_t e = cudaMemcpyAsync(ctx->h_flag, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->s_comp);
+  const cudaError_t ed = pipe_drain(ctx);
+  if (e != cudaSuccess) return nw::cuda_fail(ctx, e, "pipelined flag read");
+  if (ed != cudaSuccess) return nw::cuda_fail(ctx, ed, "pipelined evaluation");
+  NW_CUDA(ctx, cudaGetLastError());
+  if (*ctx->h_flag) return nw::fail(ctx, NW_ERR_INVALID, "pair index out of range of the determinant basis");
+  return NW_OK;
 }
 
 }  // namespace
@@ -170,12 +258,18 @@ nw_status nw_set_basis(nw_ctx* ctx, const nw_det* basis, uint64_t ndet) {
   }
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
   if (ctx->d_dets) cudaFree(ctx->d_dets);
+  if (ctx->d_desc) cudaFree(ctx->d_desc);
   ctx->d_dets = nullptr;
+  ctx->d_desc = nullptr;
   ctx->ndet = 0;
   if (ndet == 0) return NW_OK;
-  if (cudaMalloc(&ctx->d_dets, ndet * sizeof(nw_det)) != cudaSuccess)
+  std::vector<uint16_t> desc(ndet);
+  for (uint64_t i = 0; i < ndet; ++i) desc[i] = (uint16_t)nw::det_desc(basis[i].parent, basis[i].rank_a, basis[i].rank_b);
+  if (cudaMalloc(&ctx->d_dets, ndet * sizeof(nw_det)) != cudaSuccess ||
+      cudaMalloc(&ctx->d_desc, ndet * sizeof(uint16_t)) != cudaSuccess)
     return nw::fail(ctx, NW_ERR_ALLOC, "basis allocation failed");
   NW_CUDA(ctx, cudaMemcpy(ctx->d_dets, basis, ndet * sizeof(nw_det), cudaMemcpyHostToDevice));
+  NW_CUDA(ctx, cudaMemcpy(ctx->d_desc, desc.data(), ndet * sizeof(uint16_t), cudaMemcpyHostToDevice));
   ctx->ndet = ndet;
   return NW_OK;
 }
@@ -208,6 +302,8 @@ nw_status nw_eval_hs_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npa
   if ((st = nw::ensure(ctx, ctx->io_hs, npairs * 2 * sizeof(double))) != NW_OK) return st;
   uint32_t* dp = static_cast<uint32_t*>(ctx->io_pairs.p);
   double* dh = static_cast<double*>(ctx->io_hs.p);
+  if (npairs >= 2 * nw::kPipeMinChunk && is_pinned(pairs_host) && is_pinned(hs_host))
+    return eval_hs_pipelined(ctx, pairs_host, npairs, hs_host, dp, dh, s);
   NW_CUDA(ctx, cudaMemcpyAsync(dp, pairs_host, npairs * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
   if ((st = nw::eval_pairs(ctx, dp, npairs, dh, false, s)) != NW_OK) return st;
   NW_CUDA(ctx, cudaMemcpyAsync(hs_host, dh, npairs * 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -270,9 +366,11 @@ nw_status nw_ctx_destroy(nw_ctx* ctx) {
   if (ctx->d_gen) cudaFree(ctx->d_gen);
   if (ctx->d_order) cudaFree(ctx->d_order);
   if (ctx->d_dets) cudaFree(ctx->d_dets);
+  if (ctx->d_desc) cudaFree(ctx->d_desc);
   free_buf(ctx->keys);
+  free_buf(ctx->ranks);
+  free_buf(ctx->tsum);
   free_buf(ctx->perm);
-  free_buf(ctx->spairs);
   free_buf(ctx->counts);
   free_buf(ctx->offsets);
   free_buf(ctx->flag);
@@ -281,6 +379,10 @@ nw_status nw_ctx_destroy(nw_ctx* ctx) {
   if (ctx->h_flag) cudaFreeHost(ctx->h_flag);
   for (int i = 0; i < 6; ++i)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+  for (cudaStream_t q : {ctx->s_in, ctx->s_comp, ctx->s_out})
+    if (q) cudaStreamDestroy(q);
+  for (cudaEvent_t e : {ctx->ev_start, ctx->ev_in[0], ctx->ev_in[1], ctx->ev_comp[0], ctx->ev_comp[1]})
+    if (e) cudaEventDestroy(e);
   if (ctx->blas) cublasDestroy(ctx->blas);
   delete ctx;
   return NW_OK;

@@ -1,17 +1,18 @@
 // Batched (H, S) evaluation of determinant pairs on the B200.
 //
 // Pipeline for one request batch (all on one stream, no host synchronisation):
-//   1. classify: read each pair's two 32-byte determinant records, give exact zeros to
-//      same-parent pairs more than a double excitation apart (noci-rs hs.rs:96-101), and key
-//      every other pair by (ordered reference pair, contraction ranks) in a block-local
-//      shared-memory histogram;
-//   2. scan the per-key counts (one block);
-//   3. scatter pair indices into key order, reserving each block's run with one global atomic
-//      per key;
-//   4. evaluate: one thread per pair; a warp sees one (reference pair, L_alpha, L_beta) bin,
-//      so the fused m = 0 evaluator runs divergence-free with its contraction determinant,
-//      cofactors and gathered intermediates in registers.  Reference pairs with zero-overlap
-//      orbitals (m > 0) are evaluated by a separate kernel over the tail of the sorted order.
+//   1. classify: read each pair's two 16-bit determinant descriptors (the full 32-byte records
+//      only for same-parent pairs, which get exact zeros when more than a double excitation
+//      apart, noci-rs hs.rs:96-101), key every other pair by (contraction-rank class, bra
+//      determinant, ket reference) -- pair_sort_key -- and take its rank within the key from a
+//      global per-key counter;
+//   2. scan the per-key counts (three passes over tiles);
+//   3. scatter each pair and its request index to offsets[key] + rank;
+//   4. evaluate: one thread per pair; a warp sees one (L_alpha, L_beta) class, mostly one bra
+//      determinant, so the fused m = 0 evaluator runs divergence-free with its contraction
+//      determinant, cofactors and gathered intermediates in registers, and the lanes share the
+//      bra's rows of the gathered tables.  Reference pairs with zero-overlap orbitals (m > 0)
+//      are evaluated by a separate kernel over the tail of the sorted order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,26 +36,15 @@ __device__ __forceinline__ void store_hs(double* out, uint64_t i, double h, doub
   reinterpret_cast<double2*>(out)[i] = make_double2(h, s);
 }
 
-__device__ __forceinline__ unsigned lanemask_lt() {
-  unsigned m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
-
-// Keys of every pair, and per-key counts.  Lanes of a warp holding the same key add their count
-// with one atomic (warp-aggregated through __match_any_sync).
-template <bool kShared>
+// Sort key of every pair (pair_sort_key) and its rank among the pairs with the same key, taken
+// from the per-key counter with one global atomic per pair.  The class comes from the 16-bit
+// determinant descriptors; the full records are read only for same-parent pairs, which need
+// the excitation-distance rule.
 __global__ void __launch_bounds__(256) classify_kernel(EvalParams P, const uint32_t* __restrict__ pairs,
                                                        uint64_t npairs, uint32_t* __restrict__ keys,
-                                                       uint32_t* __restrict__ counts, int nkeys,
+                                                       uint32_t* __restrict__ ranks, uint32_t* __restrict__ counts,
                                                        double* __restrict__ out, int out_stride,
                                                        uint32_t* __restrict__ flag) {
-  extern __shared__ uint32_t hist[];
-  if (kShared) {
-    for (int k = threadIdx.x; k < nkeys; k += blockDim.x) hist[k] = 0;
-    __syncthreads();
-  }
-  const int lane = threadIdx.x & 31;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < npairs; i += stride) {
     const uint2 ab = __ldg(reinterpret_cast<const uint2*>(pairs) + i);
@@ -67,124 +57,136 @@ __global__ void __launch_bounds__(256) classify_kernel(EvalParams P, const uint3
       else
         out[i] = nan;
     } else {
-      const DetRec x = load_det(P.dets, ab.x);
-      const DetRec w = load_det(P.dets, ab.y);
-      if (far_same_parent(x, w)) {
+      const uint32_t dx = __ldg(P.desc + ab.x), dw = __ldg(P.desc + ab.y);
+      const int px = (int)(dx & 0xFF), pw = (int)(dw & 0xFF);
+      bool far = false;
+      if (px == pw) far = far_same_parent(load_det(P.dets, ab.x), load_det(P.dets, ab.y));
+      if (far) {
         if (out_stride == 2)
           store_hs(out, i, 0.0, 0.0);
         else
           out[i] = 0.0;
       } else {
-        const int p = (int)x.parent * P.nref + (int)w.parent;
-        const int ord = __ldg(P.order + p);
-        const int cls = rank_class(x.ra + w.ra, x.rb + w.rb);
-        // fast pairs: class-major keys [0, kClasses * nfast); m > 0 pairs after them
-        key = (uint32_t)(ord < P.nfast ? cls * P.nfast + ord : kClasses * P.nfast + (ord - P.nfast) * kClasses + cls);
+        const int cls = rank_class((int)((dx >> 8) & 15) + (int)((dw >> 8) & 15), (int)(dx >> 12) + (int)(dw >> 12));
+        const int ord = __ldg(P.order + px * P.nref + pw);
+        key = pair_sort_key(cls, ab.x, pw, ord, P.nfast, P.nref, P.nbucket, P.shift);
       }
     }
     keys[i] = key;
-    const unsigned grp = __match_any_sync(__activemask(), key);
-    if (key != kSkipKey && lane == __ffs(grp) - 1) {
-      if (kShared)
-        atomicAdd(&hist[key], (uint32_t)__popc(grp));
-      else
-        atomicAdd(&counts[key], (uint32_t)__popc(grp));
-    }
-  }
-  if (kShared) {
-    __syncthreads();
-    for (int k = threadIdx.x; k < nkeys; k += blockDim.x)
-      if (hist[k]) atomicAdd(&counts[k], hist[k]);
+    if (key != kSkipKey) ranks[i] = atomicAdd(&counts[key], 1u);
   }
 }
 
-// Exclusive scan of counts into offsets[0..nkeys]; cursor gets a copy for the scatter.
-__global__ void scan_kernel(const uint32_t* __restrict__ counts, int nkeys, uint32_t* __restrict__ offsets,
-                            uint32_t* __restrict__ cursor) {
-  __shared__ uint32_t part[1024];
-  const int t = threadIdx.x, nt = blockDim.x;
-  const int per = (nkeys + nt - 1) / nt;
-  const int k0 = t * per, k1 = min(nkeys, k0 + per);
+// Exclusive scan of counts[0..n) into offsets[0..n] (offsets[n] = total), in three passes over
+// tiles of kScanTile counters: tile sums, a one-block scan of the tile sums, then each tile's
+// scan from its base.  Tiles are walked in rounds of one counter per thread (coalesced).
+constexpr int kScanThreads = 256;
+constexpr int kScanTile = kScanThreads * 16;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_tot, uint32_t* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+    if (lane >= d) x += y;
+  }
+  if (lane == 31) warp_tot[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t t = lane < kScanThreads / 32 ? warp_tot[lane] : 0u;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, t, d);
+      if (lane >= d) t += y;
+    }
+    if (lane < kScanThreads / 32) warp_tot[lane] = t;
+    if (lane == kScanThreads / 32 - 1) *total = t;
+  }
+  __syncthreads();
+  const uint32_t excl = x - v + (wid > 0 ? warp_tot[wid - 1] : 0u);
+  __syncthreads();
+  return excl;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_tiles_kernel(const uint32_t* __restrict__ counts, uint32_t n,
+                                                                   uint32_t* __restrict__ tsum) {
+  __shared__ uint32_t red[kScanThreads / 32];
+  const uint32_t base = blockIdx.x * (uint32_t)kScanTile;
   uint32_t s = 0;
-  for (int k = k0; k < k1; ++k) s += counts[k];
-  part[t] = s;
-  __syncthreads();
-  if (t == 0) {
-    uint32_t run = 0;
-    for (int i = 0; i < nt; ++i) {
-      const uint32_t v = part[i];
-      part[i] = run;
-      run += v;
-    }
-    offsets[nkeys] = run;
+  for (int r = 0; r < kScanTile / kScanThreads; ++r) {
+    const uint32_t k = base + r * kScanThreads + threadIdx.x;
+    if (k < n) s += counts[k];
   }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, d);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
   __syncthreads();
-  uint32_t run = part[t];
-  for (int k = k0; k < k1; ++k) {
-    offsets[k] = run;
-    cursor[k] = run;
-    run += counts[k];
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < kScanThreads / 32; ++w) t += red[w];
+    tsum[blockIdx.x] = t;
   }
 }
 
-// Scatter each pair (and its position in the request) into key order.  A block owns a
-// contiguous chunk: it counts its keys, reserves one run per key with a single global atomic,
-// then places each pair at run base + rank (warp-aggregated ranks).
-template <bool kShared>
-__global__ void __launch_bounds__(256) scatter_kernel(const uint32_t* __restrict__ keys,
-                                                      const uint32_t* __restrict__ pairs, uint64_t npairs,
-                                                      uint32_t* __restrict__ cursor, int nkeys, uint64_t chunk,
-                                                      uint2* __restrict__ spairs, uint32_t* __restrict__ sidx) {
-  extern __shared__ uint32_t base[];
-  const uint64_t c0 = blockIdx.x * chunk;
-  const uint64_t c1 = min(npairs, c0 + chunk);
-  if (c0 >= npairs) return;
-  const int lane = threadIdx.x & 31;
-  uint32_t* slot = kShared ? base : cursor;
-  if (kShared) {
-    for (int k = threadIdx.x; k < nkeys; k += blockDim.x) base[k] = 0;
-    __syncthreads();
-    for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-      const uint32_t k = keys[i];
-      const unsigned grp = __match_any_sync(__activemask(), k);
-      if (k != kSkipKey && lane == __ffs(grp) - 1) atomicAdd(&base[k], (uint32_t)__popc(grp));
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < nkeys; k += blockDim.x) {
-      const uint32_t c = base[k];
-      base[k] = c ? atomicAdd(&cursor[k], c) : 0u;
-    }
+__global__ void __launch_bounds__(kScanThreads) scan_top_kernel(uint32_t* __restrict__ tsum, int ntiles) {
+  __shared__ uint32_t warp_tot[kScanThreads / 32];
+  __shared__ uint32_t total;
+  uint32_t carry = 0;
+  for (int b = 0; b < ntiles; b += kScanThreads) {
+    const int k = b + threadIdx.x;
+    const uint32_t v = k < ntiles ? tsum[k] : 0u;
+    const uint32_t e = block_exclusive_scan(v, warp_tot, &total);
+    if (k < ntiles) tsum[k] = carry + e;
+    carry += total;
     __syncthreads();
   }
-  for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_down_kernel(const uint32_t* __restrict__ counts, uint32_t n,
+                                                                  const uint32_t* __restrict__ tsum,
+                                                                  uint32_t* __restrict__ offsets) {
+  __shared__ uint32_t warp_tot[kScanThreads / 32];
+  __shared__ uint32_t total;
+  const uint32_t base = blockIdx.x * (uint32_t)kScanTile;
+  uint32_t carry = tsum[blockIdx.x];
+  for (int r = 0; r < kScanTile / kScanThreads; ++r) {
+    const uint32_t k = base + r * kScanThreads + threadIdx.x;
+    const uint32_t v = k < n ? counts[k] : 0u;
+    const uint32_t e = block_exclusive_scan(v, warp_tot, &total);
+    if (k <= n) offsets[k] = carry + e;  // offsets[n] = total of all counters
+    carry += total;
+    if (base + (r + 1) * kScanThreads > n) break;
+  }
+}
+
+// Scatter each pair's position in the request to offsets[key] + rank (the evaluators read the
+// pair itself through that index: one random 4-byte write here instead of 12).
+__global__ void __launch_bounds__(256) scatter_kernel(const uint32_t* __restrict__ keys,
+                                                      const uint32_t* __restrict__ ranks, uint64_t npairs,
+                                                      const uint32_t* __restrict__ offsets,
+                                                      uint32_t* __restrict__ sidx) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < npairs; i += stride) {
     const uint32_t k = keys[i];
-    const unsigned act = __activemask();
-    const unsigned grp = __match_any_sync(act, k);
-    const int leader = __ffs(grp) - 1;
-    uint32_t b = 0;
-    if (k != kSkipKey && lane == leader) b = atomicAdd(&slot[k], (uint32_t)__popc(grp));
-    b = __shfl_sync(grp, b, leader);
-    if (k != kSkipKey) {
-      const uint32_t pos = b + (uint32_t)__popc(grp & lanemask_lt());
-      spairs[pos] = __ldg(reinterpret_cast<const uint2*>(pairs) + i);
-      sidx[pos] = (uint32_t)i;
-    }
+    if (k == kSkipKey) continue;
+    sidx[__ldg(offsets + k) + ranks[i]] = (uint32_t)i;
   }
 }
 
 // One contraction-rank class (L_alpha, L_beta) over its sorted range
-// [offsets[c * nfast], offsets[(c + 1) * nfast]) of all fast reference pairs.
+// [offsets[c * nbucket], offsets[(c + 1) * nbucket]) of all fast reference pairs.
 template <int LA, int LB>
-__device__ __forceinline__ void run_class(const EvalParams& P, const uint2* __restrict__ spairs,
+__device__ __forceinline__ void run_class(const EvalParams& P, const uint2* __restrict__ pairs,
                                           const uint32_t* __restrict__ sidx, const uint32_t* __restrict__ offsets,
                                           double* __restrict__ out) {
   constexpr int c = LA * 5 + LB;
-  const uint32_t begin = offsets[c * P.nfast];
-  const uint32_t end = offsets[(c + 1) * P.nfast];
+  const uint32_t begin = offsets[c * P.nbucket];
+  const uint32_t end = offsets[(c + 1) * P.nbucket];
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t t = begin + blockIdx.x * blockDim.x + threadIdx.x; t < end; t += stride) {
-    const uint2 ab = spairs[t];
     const uint32_t i = sidx[t];
+    const uint2 ab = __ldg(pairs + i);
     const DetRec x = load_det(P.dets, ab.x);
     const DetRec w = load_det(P.dets, ab.y);
     const FastPair fp = P.fast[(int)x.parent * P.nref + (int)w.parent];
@@ -197,60 +199,60 @@ __device__ __forceinline__ void run_class(const EvalParams& P, const uint2* __re
 // The 25 fixed-rank classes in three kernels grouped by register demand, so the dominant
 // small-rank classes keep a small register footprint (high occupancy) and the rare
 // quadruple-rank classes do not force it up.
-__global__ void __launch_bounds__(256) eval_light_kernel(EvalParams P, const uint2* __restrict__ spairs,
+__global__ void __launch_bounds__(256) eval_light_kernel(EvalParams P, const uint2* __restrict__ pairs,
                                                          const uint32_t* __restrict__ sidx,
                                                          const uint32_t* __restrict__ offsets,
                                                          double* __restrict__ out) {
-  run_class<2, 2>(P, spairs, sidx, offsets, out);
-  run_class<2, 1>(P, spairs, sidx, offsets, out);
-  run_class<1, 2>(P, spairs, sidx, offsets, out);
-  run_class<2, 0>(P, spairs, sidx, offsets, out);
-  run_class<0, 2>(P, spairs, sidx, offsets, out);
-  run_class<1, 1>(P, spairs, sidx, offsets, out);
-  run_class<1, 0>(P, spairs, sidx, offsets, out);
-  run_class<0, 1>(P, spairs, sidx, offsets, out);
-  run_class<0, 0>(P, spairs, sidx, offsets, out);
+  run_class<2, 2>(P, pairs, sidx, offsets, out);
+  run_class<2, 1>(P, pairs, sidx, offsets, out);
+  run_class<1, 2>(P, pairs, sidx, offsets, out);
+  run_class<2, 0>(P, pairs, sidx, offsets, out);
+  run_class<0, 2>(P, pairs, sidx, offsets, out);
+  run_class<1, 1>(P, pairs, sidx, offsets, out);
+  run_class<1, 0>(P, pairs, sidx, offsets, out);
+  run_class<0, 1>(P, pairs, sidx, offsets, out);
+  run_class<0, 0>(P, pairs, sidx, offsets, out);
 }
 
-__global__ void __launch_bounds__(256) eval_medium_kernel(EvalParams P, const uint2* __restrict__ spairs,
+__global__ void __launch_bounds__(256) eval_medium_kernel(EvalParams P, const uint2* __restrict__ pairs,
                                                           const uint32_t* __restrict__ sidx,
                                                           const uint32_t* __restrict__ offsets,
                                                           double* __restrict__ out) {
-  run_class<3, 1>(P, spairs, sidx, offsets, out);
-  run_class<1, 3>(P, spairs, sidx, offsets, out);
-  run_class<3, 0>(P, spairs, sidx, offsets, out);
-  run_class<0, 3>(P, spairs, sidx, offsets, out);
-  run_class<3, 2>(P, spairs, sidx, offsets, out);
-  run_class<2, 3>(P, spairs, sidx, offsets, out);
-  run_class<3, 3>(P, spairs, sidx, offsets, out);
+  run_class<3, 1>(P, pairs, sidx, offsets, out);
+  run_class<1, 3>(P, pairs, sidx, offsets, out);
+  run_class<3, 0>(P, pairs, sidx, offsets, out);
+  run_class<0, 3>(P, pairs, sidx, offsets, out);
+  run_class<3, 2>(P, pairs, sidx, offsets, out);
+  run_class<2, 3>(P, pairs, sidx, offsets, out);
+  run_class<3, 3>(P, pairs, sidx, offsets, out);
 }
 
-__global__ void __launch_bounds__(256) eval_heavy_kernel(EvalParams P, const uint2* __restrict__ spairs,
+__global__ void __launch_bounds__(256) eval_heavy_kernel(EvalParams P, const uint2* __restrict__ pairs,
                                                          const uint32_t* __restrict__ sidx,
                                                          const uint32_t* __restrict__ offsets,
                                                          double* __restrict__ out) {
-  run_class<4, 0>(P, spairs, sidx, offsets, out);
-  run_class<0, 4>(P, spairs, sidx, offsets, out);
-  run_class<4, 1>(P, spairs, sidx, offsets, out);
-  run_class<1, 4>(P, spairs, sidx, offsets, out);
-  run_class<4, 2>(P, spairs, sidx, offsets, out);
-  run_class<2, 4>(P, spairs, sidx, offsets, out);
-  run_class<4, 3>(P, spairs, sidx, offsets, out);
-  run_class<3, 4>(P, spairs, sidx, offsets, out);
-  run_class<4, 4>(P, spairs, sidx, offsets, out);
+  run_class<4, 0>(P, pairs, sidx, offsets, out);
+  run_class<0, 4>(P, pairs, sidx, offsets, out);
+  run_class<4, 1>(P, pairs, sidx, offsets, out);
+  run_class<1, 4>(P, pairs, sidx, offsets, out);
+  run_class<4, 2>(P, pairs, sidx, offsets, out);
+  run_class<2, 4>(P, pairs, sidx, offsets, out);
+  run_class<4, 3>(P, pairs, sidx, offsets, out);
+  run_class<3, 4>(P, pairs, sidx, offsets, out);
+  run_class<4, 4>(P, pairs, sidx, offsets, out);
 }
 
 // Contraction ranks above 4 in either spin (class 25), runtime-size arithmetic.
-__global__ void __launch_bounds__(128) eval_rt_kernel(EvalParams P, const uint2* __restrict__ spairs,
+__global__ void __launch_bounds__(128) eval_rt_kernel(EvalParams P, const uint2* __restrict__ pairs,
                                                       const uint32_t* __restrict__ sidx,
                                                       const uint32_t* __restrict__ offsets,
                                                       double* __restrict__ out) {
-  const uint32_t begin = offsets[25 * P.nfast];
-  const uint32_t end = offsets[26 * P.nfast];
+  const uint32_t begin = offsets[25 * P.nbucket];
+  const uint32_t end = offsets[26 * P.nbucket];
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t t = begin + blockIdx.x * blockDim.x + threadIdx.x; t < end; t += stride) {
-    const uint2 ab = spairs[t];
     const uint32_t i = sidx[t];
+    const uint2 ab = __ldg(pairs + i);
     const DetRec x = load_det(P.dets, ab.x);
     const DetRec w = load_det(P.dets, ab.y);
     const FastPair fp = P.fast[(int)x.parent * P.nref + (int)w.parent];
@@ -268,16 +270,16 @@ __device__ __noinline__ void eval_gen_one(const GenPair& g, const DetRec& x, con
   eval_gen_pair(g, x, w, P.n, P.nocc_a, P.nocc_b, P.enuc, P.tol, P.exact != 0, H, S);
 }
 
-__global__ void __launch_bounds__(128) eval_gen_kernel(EvalParams P, const uint2* __restrict__ spairs,
+__global__ void __launch_bounds__(128) eval_gen_kernel(EvalParams P, const uint2* __restrict__ pairs,
                                                        const uint32_t* __restrict__ sidx,
                                                        const uint32_t* __restrict__ offsets, int nkeys,
                                                        double* __restrict__ out) {
-  const uint32_t begin = offsets[kClasses * P.nfast];
+  const uint32_t begin = offsets[kClasses * P.nbucket];
   const uint32_t end = offsets[nkeys];
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t t = begin + blockIdx.x * blockDim.x + threadIdx.x; t < end; t += stride) {
-    const uint2 ab = spairs[t];
     const uint32_t i = sidx[t];
+    const uint2 ab = __ldg(pairs + i);
     const DetRec x = load_det(P.dets, ab.x);
     const DetRec w = load_det(P.dets, ab.y);
     const GenPair& g = P.gen[(int)x.parent * P.nref + (int)w.parent];
@@ -321,17 +323,7 @@ inline int grid_stride_blocks(uint64_t work, int block, int per_sm) {
   return (int)g;
 }
 
-}  // namespace
-
-nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, bool overlap_only,
-                     cudaStream_t stream) {
-  if (!ctx->built) return fail(ctx, NW_ERR_STATE, "intermediates not built");
-  if (!ctx->d_dets) return fail(ctx, NW_ERR_STATE, "no determinant basis set");
-  if (npairs == 0) return NW_OK;
-  if (npairs >= 0xFFFFFFFFull) return fail(ctx, NW_ERR_UNSUPPORTED, "at most 2^32 - 2 pairs per call");
-  if ((reinterpret_cast<uintptr_t>(pairs) & 7) != 0) return fail(ctx, NW_ERR_INVALID, "pairs must be 8-byte aligned");
-  if ((reinterpret_cast<uintptr_t>(out) & (overlap_only ? 7 : 15)) != 0)
-    return fail(ctx, NW_ERR_INVALID, "output must be 16-byte aligned (8 for overlap only)");
+EvalParams make_params(const nw_ctx* ctx) {
   EvalParams P;
   P.dets = ctx->d_dets;
   P.ndet = ctx->ndet;
@@ -346,11 +338,91 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
   P.exact = ctx->convention == NW_CONVENTION_EXACT ? 1 : 0;
   P.enuc = ctx->enuc;
   P.tol = ctx->tol;
+  P.desc = ctx->d_desc;
+  P.nbucket = 1;
+  P.shift = 0;
+  return P;
+}
+
+// Device scratch of one sorted evaluation.
+struct SortScratch {
+  uint32_t* keys;     // npairs
+  uint32_t* ranks;    // npairs
+  uint32_t* sidx;     // npairs
+  uint32_t* counts;   // nkeys
+  uint32_t* offsets;  // nkeys + 1
+  uint32_t* tsum;     // nkeys / kScanTile + 1
+  uint32_t* flag;
+};
+
+// Fine-key budget: at most kFineMax counters, and at most about one per pair of the request so
+// the counter memset and scan stay small next to the evaluation.
+constexpr uint64_t kFineMax = 1ull << 23;
+constexpr uint64_t kFineMin = 1ull << 14;
+
+// Number of sort keys for this request with at most `cap` counters for the fast classes;
+// fills P.nbucket / P.shift.
+uint64_t plan_keys(const nw_ctx* ctx, EvalParams& P, uint64_t cap) {
+  uint32_t nb = 1;
+  P.shift = sort_key_shift(ctx->ndet, ctx->nref, cap, &nb);
+  P.nbucket = nb;
+  const uint64_t ngen = (uint64_t)ctx->nref * ctx->nref - (uint64_t)ctx->nfast;
+  return (uint64_t)kClasses * nb + (uint64_t)kClasses * ngen;
+}
+
+// classify -> scan -> scatter -> evaluate, all on `stream`.  The flag must already be cleared
+// (or hold earlier calls' reports); ev (six events or null) brackets the phases.
+nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const uint32_t* pairs, uint64_t npairs,
+                        double* out, const SortScratch& S, cudaStream_t stream, cudaEvent_t* ev) {
+  if (ev) NW_CUDA(ctx, cudaEventRecord(ev[0], stream));
+  NW_CUDA(ctx, cudaMemsetAsync(S.counts, 0, sizeof(uint32_t) * nkeys, stream));
+  classify_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(P, pairs, npairs, S.keys, S.ranks,
+                                                                          S.counts, out, 2, S.flag);
+  NW_CUDA(ctx, cudaGetLastError());
+  if (ev) NW_CUDA(ctx, cudaEventRecord(ev[1], stream));
+  const int ntiles = (int)(nkeys / kScanTile + 1);
+  scan_tiles_kernel<<<ntiles, kScanThreads, 0, stream>>>(S.counts, (uint32_t)nkeys, S.tsum);
+  scan_top_kernel<<<1, kScanThreads, 0, stream>>>(S.tsum, ntiles);
+  scan_down_kernel<<<ntiles, kScanThreads, 0, stream>>>(S.counts, (uint32_t)nkeys, S.tsum, S.offsets);
+  NW_CUDA(ctx, cudaGetLastError());
+  if (ev) NW_CUDA(ctx, cudaEventRecord(ev[2], stream));
+  scatter_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(S.keys, S.ranks, npairs, S.offsets, S.sidx);
+  NW_CUDA(ctx, cudaGetLastError());
+  if (ev) NW_CUDA(ctx, cudaEventRecord(ev[3], stream));
+  const uint2* pp = reinterpret_cast<const uint2*>(pairs);
+  if (ctx->nfast > 0) {
+    eval_light_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
+    eval_medium_kernel<<<148 * 2, 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
+    eval_heavy_kernel<<<148, 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
+    eval_rt_kernel<<<148 * 2, 128, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
+    NW_CUDA(ctx, cudaGetLastError());
+  }
+  if (ev) NW_CUDA(ctx, cudaEventRecord(ev[4], stream));
+  if (ctx->nfast < ctx->nref * ctx->nref) {
+    eval_gen_kernel<<<148 * 4, 128, 0, stream>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out);
+    NW_CUDA(ctx, cudaGetLastError());
+  }
+  if (ev) NW_CUDA(ctx, cudaEventRecord(ev[5], stream));
+  return NW_OK;
+}
+
+}  // namespace
+
+nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, bool overlap_only,
+                     cudaStream_t stream, bool clear_flag) {
+  if (!ctx->built) return fail(ctx, NW_ERR_STATE, "intermediates not built");
+  if (!ctx->d_dets) return fail(ctx, NW_ERR_STATE, "no determinant basis set");
+  if (npairs == 0) return NW_OK;
+  if (npairs >= 0xFFFFFFFFull) return fail(ctx, NW_ERR_UNSUPPORTED, "at most 2^32 - 2 pairs per call");
+  if ((reinterpret_cast<uintptr_t>(pairs) & 7) != 0) return fail(ctx, NW_ERR_INVALID, "pairs must be 8-byte aligned");
+  if ((reinterpret_cast<uintptr_t>(out) & (overlap_only ? 7 : 15)) != 0)
+    return fail(ctx, NW_ERR_INVALID, "output must be 16-byte aligned (8 for overlap only)");
+  EvalParams P = make_params(ctx);
 
   nw_status st = ensure(ctx, ctx->flag, 256);
   if (st != NW_OK) return st;
   uint32_t* flag = static_cast<uint32_t*>(ctx->flag.p);
-  NW_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(uint32_t), stream));
+  if (clear_flag) NW_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(uint32_t), stream));
 
   if (overlap_only) {
     eval_s_kernel<<<grid_stride_blocks(npairs, 128, 16), 128, 0, stream>>>(P, pairs, npairs, out, flag);
@@ -358,60 +430,24 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
     return NW_OK;
   }
 
-  const int nkeys = ctx->nref * ctx->nref * kClasses;
+  const uint64_t nkeys = plan_keys(ctx, P, std::min(kFineMax, std::max(kFineMin, npairs)));
   if ((st = ensure(ctx, ctx->keys, npairs * sizeof(uint32_t))) != NW_OK) return st;
+  if ((st = ensure(ctx, ctx->ranks, npairs * sizeof(uint32_t))) != NW_OK) return st;
   if ((st = ensure(ctx, ctx->perm, npairs * sizeof(uint32_t))) != NW_OK) return st;
-  if ((st = ensure(ctx, ctx->spairs, npairs * sizeof(uint2))) != NW_OK) return st;
-  if ((st = ensure(ctx, ctx->counts, (size_t)(nkeys + 1) * sizeof(uint32_t) * 2)) != NW_OK) return st;
-  if ((st = ensure(ctx, ctx->offsets, (size_t)(nkeys + 1) * sizeof(uint32_t))) != NW_OK) return st;
-  uint32_t* keys = static_cast<uint32_t*>(ctx->keys.p);
-  uint32_t* sidx = static_cast<uint32_t*>(ctx->perm.p);
-  uint2* spairs = static_cast<uint2*>(ctx->spairs.p);
-  uint32_t* counts = static_cast<uint32_t*>(ctx->counts.p);
-  uint32_t* cursor = counts + (nkeys + 1);
-  uint32_t* offsets = static_cast<uint32_t*>(ctx->offsets.p);
-  NW_CUDA(ctx, cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (nkeys + 1), stream));
-
-  const bool tm = ctx->timing;
-  if (tm) NW_CUDA(ctx, cudaEventRecord(ctx->ev[0], stream));
-  const size_t hist_bytes = (size_t)nkeys * sizeof(uint32_t);
-  const bool shared_hist = hist_bytes <= 48 * 1024;
-  const int cblocks = grid_stride_blocks(npairs, 256, 8);
-  if (shared_hist)
-    classify_kernel<true><<<cblocks, 256, hist_bytes, stream>>>(P, pairs, npairs, keys, counts, nkeys, out, 2, flag);
-  else
-    classify_kernel<false><<<cblocks, 256, 0, stream>>>(P, pairs, npairs, keys, counts, nkeys, out, 2, flag);
-  NW_CUDA(ctx, cudaGetLastError());
-  if (tm) NW_CUDA(ctx, cudaEventRecord(ctx->ev[1], stream));
-  scan_kernel<<<1, 1024, 0, stream>>>(counts, nkeys, offsets, cursor);
-  NW_CUDA(ctx, cudaGetLastError());
-  if (tm) NW_CUDA(ctx, cudaEventRecord(ctx->ev[2], stream));
-  const uint64_t chunk = std::max<uint64_t>(4096, (npairs + 148 * 8 - 1) / (148 * 8));
-  const int sblocks = (int)((npairs + chunk - 1) / chunk);
-  if (shared_hist)
-    scatter_kernel<true><<<sblocks, 256, hist_bytes, stream>>>(keys, pairs, npairs, cursor, nkeys, chunk, spairs, sidx);
-  else
-    scatter_kernel<false><<<sblocks, 256, 0, stream>>>(keys, pairs, npairs, cursor, nkeys, chunk, spairs, sidx);
-  NW_CUDA(ctx, cudaGetLastError());
-  if (tm) NW_CUDA(ctx, cudaEventRecord(ctx->ev[3], stream));
-  if (ctx->nfast > 0) {
-    const int g = grid_stride_blocks(npairs, 256, 8);
-    eval_light_kernel<<<g, 256, 0, stream>>>(P, spairs, sidx, offsets, out);
-    eval_medium_kernel<<<148 * 2, 256, 0, stream>>>(P, spairs, sidx, offsets, out);
-    eval_heavy_kernel<<<148, 256, 0, stream>>>(P, spairs, sidx, offsets, out);
-    eval_rt_kernel<<<148 * 2, 128, 0, stream>>>(P, spairs, sidx, offsets, out);
-    NW_CUDA(ctx, cudaGetLastError());
-  }
-  if (tm) NW_CUDA(ctx, cudaEventRecord(ctx->ev[4], stream));
-  if (ctx->nfast < ctx->nref * ctx->nref) {
-    eval_gen_kernel<<<148 * 4, 128, 0, stream>>>(P, spairs, sidx, offsets, nkeys, out);
-    NW_CUDA(ctx, cudaGetLastError());
-  }
-  if (tm) {
-    NW_CUDA(ctx, cudaEventRecord(ctx->ev[5], stream));
-    ctx->timed_valid = true;
-  }
-  return NW_OK;
+  if ((st = ensure(ctx, ctx->counts, nkeys * sizeof(uint32_t))) != NW_OK) return st;
+  if ((st = ensure(ctx, ctx->offsets, (nkeys + 1) * sizeof(uint32_t))) != NW_OK) return st;
+  if ((st = ensure(ctx, ctx->tsum, (nkeys / kScanTile + 1) * sizeof(uint32_t))) != NW_OK) return st;
+  SortScratch S;
+  S.keys = static_cast<uint32_t*>(ctx->keys.p);
+  S.ranks = static_cast<uint32_t*>(ctx->ranks.p);
+  S.sidx = static_cast<uint32_t*>(ctx->perm.p);
+  S.counts = static_cast<uint32_t*>(ctx->counts.p);
+  S.offsets = static_cast<uint32_t*>(ctx->offsets.p);
+  S.tsum = static_cast<uint32_t*>(ctx->tsum.p);
+  S.flag = flag;
+  st = launch_sorted(ctx, P, nkeys, pairs, npairs, out, S, stream, ctx->timing ? ctx->ev : nullptr);
+  if (st == NW_OK && ctx->timing) ctx->timed_valid = true;
+  return st;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -421,13 +457,13 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
 // nearly all of HBM to its own memory pool (a framework's caching allocator, a solver's
 // preallocated workspace), or a latency-critical loop that cannot afford cudaMalloc's implicit
 // synchronisation or its failure path.  For them the per-call scratch of the evaluation (keys,
-// key-sorted pair payload, request indices, per-key counts and offsets, error flag) lives in
-// the fixed device array below instead of buffers grown with cudaMalloc.
+// ranks, key-sorted request indices, per-key counts and offsets, error flag)
+// lives in the fixed device array below instead of buffers grown with cudaMalloc.
 //
 // The array is a file-scope __device__ variable, so every GPU that loads this library holds
-// it (18,055,680 bytes, 17.2 MiB) until the process exits.  Host code cannot use its name as a device
-// address: the address is looked up with cudaGetSymbolAddress once per device, with that
-// device current, on the first call of the entry point on that device (that first call
+// it (14,287,360 bytes, 13.6 MiB) until the process exits.  Host code cannot use its name as a
+// device address: the address is looked up with cudaGetSymbolAddress once per device, with
+// that device current, on the first call of the entry point on that device (that first call
 // should therefore come before any stream capture).  Every call shares the array and it keeps
 // the last call's contents: the counts and the error flag are cleared at the start of each
 // call, and calls whose work overlaps on the GPU (different streams, concurrent host threads)
@@ -437,13 +473,17 @@ namespace {
 
 constexpr uint64_t kNoallocMaxPairs = 1ull << 20;                       // 1,048,576 pairs per call
 constexpr int kNoallocMaxRefs = 64;                                      // reference determinants
-constexpr uint64_t kNoallocMaxKeys = (uint64_t)kNoallocMaxRefs * kNoallocMaxRefs * kClasses;
+// keys: the fast classes get at least kClasses * 64 * 64 counters, the zero-overlap reference
+// pairs up to kClasses * 64 * 64 more
+constexpr uint64_t kNoallocMaxKeys = 2ull * kNoallocMaxRefs * kNoallocMaxRefs * kClasses;
+constexpr uint64_t kNoallocTiles = kNoallocMaxKeys / kScanTile + 1;
 constexpr uint64_t kNoallocOffKeys = 0;
-constexpr uint64_t kNoallocOffPairs = kNoallocOffKeys + 4 * kNoallocMaxPairs;
-constexpr uint64_t kNoallocOffIdx = kNoallocOffPairs + 8 * kNoallocMaxPairs;
+constexpr uint64_t kNoallocOffRanks = kNoallocOffKeys + 4 * kNoallocMaxPairs;
+constexpr uint64_t kNoallocOffIdx = kNoallocOffRanks + 4 * kNoallocMaxPairs;
 constexpr uint64_t kNoallocOffCounts = kNoallocOffIdx + 4 * kNoallocMaxPairs;
-constexpr uint64_t kNoallocOffOffsets = kNoallocOffCounts + 8 * (kNoallocMaxKeys + 1);
-constexpr uint64_t kNoallocOffFlag = ((kNoallocOffOffsets + 4 * (kNoallocMaxKeys + 1) + 255) / 256) * 256;
+constexpr uint64_t kNoallocOffOffsets = kNoallocOffCounts + 4 * kNoallocMaxKeys;
+constexpr uint64_t kNoallocOffTsum = kNoallocOffOffsets + 4 * (kNoallocMaxKeys + 1);
+constexpr uint64_t kNoallocOffFlag = ((kNoallocOffTsum + 4 * kNoallocTiles + 255) / 256) * 256;
 constexpr uint64_t kNoallocBytes = kNoallocOffFlag + 256;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
@@ -485,60 +525,21 @@ nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs
   nw_status st = noalloc_scratch(ctx, &base);
   if (st != NW_OK) return st;
   if (npairs == 0) return NW_OK;
-  EvalParams P;
-  P.dets = ctx->d_dets;
-  P.ndet = ctx->ndet;
-  P.fast = ctx->d_fast;
-  P.gen = ctx->d_gen;
-  P.order = ctx->d_order;
-  P.nref = ctx->nref;
-  P.n = ctx->nmo;
-  P.nocc_a = ctx->nocc_a;
-  P.nocc_b = ctx->nocc_b;
-  P.nfast = ctx->nfast;
-  P.exact = ctx->convention == NW_CONVENTION_EXACT ? 1 : 0;
-  P.enuc = ctx->enuc;
-  P.tol = ctx->tol;
-  const int nkeys = ctx->nref * ctx->nref * kClasses;
-  uint32_t* keys = reinterpret_cast<uint32_t*>(base + kNoallocOffKeys);
-  uint2* spairs = reinterpret_cast<uint2*>(base + kNoallocOffPairs);
-  uint32_t* sidx = reinterpret_cast<uint32_t*>(base + kNoallocOffIdx);
-  uint32_t* counts = reinterpret_cast<uint32_t*>(base + kNoallocOffCounts);
-  uint32_t* cursor = counts + (nkeys + 1);
-  uint32_t* offsets = reinterpret_cast<uint32_t*>(base + kNoallocOffOffsets);
-  uint32_t* flag = reinterpret_cast<uint32_t*>(base + kNoallocOffFlag);
-  NW_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(uint32_t), stream));
-  NW_CUDA(ctx, cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (nkeys + 1), stream));
-  const size_t hist_bytes = (size_t)nkeys * sizeof(uint32_t);
-  const bool shared_hist = hist_bytes <= 48 * 1024;
-  const int cblocks = grid_stride_blocks(npairs, 256, 8);
-  if (shared_hist)
-    classify_kernel<true><<<cblocks, 256, hist_bytes, stream>>>(P, pairs, npairs, keys, counts, nkeys, out, 2, flag);
-  else
-    classify_kernel<false><<<cblocks, 256, 0, stream>>>(P, pairs, npairs, keys, counts, nkeys, out, 2, flag);
-  NW_CUDA(ctx, cudaGetLastError());
-  scan_kernel<<<1, 1024, 0, stream>>>(counts, nkeys, offsets, cursor);
-  NW_CUDA(ctx, cudaGetLastError());
-  const uint64_t chunk = std::max<uint64_t>(4096, (npairs + 148 * 8 - 1) / (148 * 8));
-  const int sblocks = (int)((npairs + chunk - 1) / chunk);
-  if (shared_hist)
-    scatter_kernel<true><<<sblocks, 256, hist_bytes, stream>>>(keys, pairs, npairs, cursor, nkeys, chunk, spairs, sidx);
-  else
-    scatter_kernel<false><<<sblocks, 256, 0, stream>>>(keys, pairs, npairs, cursor, nkeys, chunk, spairs, sidx);
-  NW_CUDA(ctx, cudaGetLastError());
-  if (ctx->nfast > 0) {
-    const int g = grid_stride_blocks(npairs, 256, 8);
-    eval_light_kernel<<<g, 256, 0, stream>>>(P, spairs, sidx, offsets, out);
-    eval_medium_kernel<<<148 * 2, 256, 0, stream>>>(P, spairs, sidx, offsets, out);
-    eval_heavy_kernel<<<148, 256, 0, stream>>>(P, spairs, sidx, offsets, out);
-    eval_rt_kernel<<<148 * 2, 128, 0, stream>>>(P, spairs, sidx, offsets, out);
-    NW_CUDA(ctx, cudaGetLastError());
-  }
-  if (ctx->nfast < ctx->nref * ctx->nref) {
-    eval_gen_kernel<<<148 * 4, 128, 0, stream>>>(P, spairs, sidx, offsets, nkeys, out);
-    NW_CUDA(ctx, cudaGetLastError());
-  }
-  return NW_OK;
+  EvalParams P = make_params(ctx);
+  const uint64_t ngen = (uint64_t)ctx->nref * ctx->nref - (uint64_t)ctx->nfast;
+  const uint64_t fast_cap = std::min(kNoallocMaxKeys - (uint64_t)kClasses * ngen, std::max(kFineMin, npairs));
+  const uint64_t nkeys = plan_keys(ctx, P, fast_cap);
+  if (nkeys > kNoallocMaxKeys) return fail(ctx, NW_ERR_UNSUPPORTED, "sort keys exceed the allocation-free scratch");
+  SortScratch S;
+  S.keys = reinterpret_cast<uint32_t*>(base + kNoallocOffKeys);
+  S.ranks = reinterpret_cast<uint32_t*>(base + kNoallocOffRanks);
+  S.sidx = reinterpret_cast<uint32_t*>(base + kNoallocOffIdx);
+  S.counts = reinterpret_cast<uint32_t*>(base + kNoallocOffCounts);
+  S.offsets = reinterpret_cast<uint32_t*>(base + kNoallocOffOffsets);
+  S.tsum = reinterpret_cast<uint32_t*>(base + kNoallocOffTsum);
+  S.flag = reinterpret_cast<uint32_t*>(base + kNoallocOffFlag);
+  NW_CUDA(ctx, cudaMemsetAsync(S.flag, 0, sizeof(uint32_t), stream));
+  return launch_sorted(ctx, P, nkeys, pairs, npairs, out, S, stream, nullptr);
 }
 
 }  // namespace nw

@@ -15,7 +15,7 @@
 namespace nw {
 
 constexpr int kMaxL = 8;          // largest contraction-determinant dimension per spin
-constexpr int kClasses = 26;      // (L_alpha, L_beta) in 0..4 x 0..4, plus one "other" class
+constexpr int kClasses = kRankClasses;  // (L_alpha, L_beta) in 0..4 x 0..4, plus one "other" class
 constexpr uint32_t kSkipKey = 0xFFFFFFFFu;
 
 struct EvalParams {
@@ -27,6 +27,9 @@ struct EvalParams {
   int32_t nref, n, nocc_a, nocc_b;
   int32_t nfast;           // number of fast ordered pairs (sort positions 0..nfast-1)
   int32_t exact;
+  const uint16_t* desc;    // per-determinant class descriptor (det_desc)
+  uint32_t nbucket;        // sort keys per rank class for fast pairs (pair_sort_key)
+  int32_t shift;
   double enuc, tol;
 };
 
@@ -66,12 +69,17 @@ struct nw_ctx {
 
   // resident basis
   nw_det* d_dets = nullptr;
+  uint16_t* d_desc = nullptr;      // det_desc of every record
   uint64_t ndet = 0;
 
   // evaluation scratch (grown on demand)
-  nw::DevBuf keys, perm, spairs, counts, offsets, flag;
+  nw::DevBuf keys, perm, counts, offsets, flag, ranks, tsum;
   uint32_t* h_flag = nullptr;      // pinned mirror of the device error flag
   nw::DevBuf io_pairs, io_hs;      // staging for the host-buffer entry point
+  // copy-in / evaluate / copy-out streams and chunk events of the pipelined host-buffer path
+  cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
+  cudaEvent_t ev_start = nullptr;
+  cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr};
 
   cublasHandle_t blas = nullptr;
   std::string last_error;
@@ -84,6 +92,10 @@ struct nw_ctx {
 
 namespace nw {
 
+// Pipelined host-buffer path: about kPipeChunks chunks of at least kPipeMinChunk pairs.
+constexpr uint64_t kPipeChunks = 16;
+constexpr uint64_t kPipeMinChunk = 1ull << 18;
+
 // Records an error on the context and returns the status.
 nw_status fail(nw_ctx* ctx, nw_status st, const std::string& msg);
 nw_status cuda_fail(nw_ctx* ctx, cudaError_t e, const char* what);
@@ -93,8 +105,9 @@ nw_status ensure(nw_ctx* ctx, DevBuf& b, size_t bytes);
 nw_status build_all(nw_ctx* ctx);
 
 // Evaluation (eval.cu).
+// clear_flag = false keeps the out-of-range flag of earlier calls (chunked host path).
 nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, bool overlap_only,
-                     cudaStream_t stream);
+                     cudaStream_t stream, bool clear_flag = true);
 // Same evaluation with its scratch in a fixed device array (no device allocation).
 nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, cudaStream_t stream);
 

@@ -890,6 +890,34 @@ NW_HD bool far_same_parent(const DetRec& x, const DetRec& w) {
 
 NW_HD int rank_class(int la, int lb) { return (la <= 4 && lb <= 4) ? la * 5 + lb : 25; }
 
+// ---------------------------------------------------------------------------------------
+// Sort keys of the evaluation pipeline.  A pair of a fast reference pair (no zero-overlap
+// orbitals) gets  cls * nbucket + ((bra * nref + ket_parent) >> shift):  class-major, so each
+// evaluator kernel walks one contiguous range per class, and inside a class the pairs of one
+// bra determinant (and ket reference) lie together, so the lanes of a warp share the bra's
+// rows of the intermediates.  Pairs of reference pairs with zero-overlap orbitals follow,
+// keyed by (sort position - nfast, class).  Keys are < kRankClasses * (nbucket + nref^2).
+// ---------------------------------------------------------------------------------------
+constexpr int kRankClasses = 26;
+
+NW_HD uint32_t pair_sort_key(int cls, uint32_t bra, int ket_parent, int ord, int nfast, int nref, uint32_t nbucket,
+                             int shift) {
+  if (ord < nfast) return (uint32_t)cls * nbucket + (uint32_t)((((uint64_t)bra * (uint64_t)nref) + ket_parent) >> shift);
+  return (uint32_t)kRankClasses * nbucket + (uint32_t)((ord - nfast) * kRankClasses + cls);
+}
+
+// Smallest shift for which the fast-pair keys, kRankClasses * nbucket, fit in cap (cap >= 26).
+NW_HD int sort_key_shift(uint64_t ndet, int nref, uint64_t cap, uint32_t* nbucket) {
+  const uint64_t span = ndet * (uint64_t)nref;
+  int s = 0;
+  while (s < 63 && (uint64_t)kRankClasses * (((span - 1) >> s) + 1) > cap) ++s;
+  *nbucket = (uint32_t)(((span - 1) >> s) + 1);
+  return s;
+}
+
+// 16-bit class descriptor of a determinant record: parent (8 bits), rank_a, rank_b (4 bits each).
+NW_HD uint32_t det_desc(uint32_t parent, int ra, int rb) { return parent | ((uint32_t)ra << 8) | ((uint32_t)rb << 12); }
+
 NW_HD void labels_rt(const DetRec& x, const DetRec& w, int spin, int nocc, int n, int* rows, int* cols) {
   uint8_t bx[8], bw[8];
   const uint64_t ix = spin ? x.ib : x.ia, iw = spin ? w.ib : w.ia;

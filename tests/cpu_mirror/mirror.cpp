@@ -95,6 +95,30 @@ int mir_far_same_parent(const void* dets, uint32_t a, uint32_t b) {
   return far_same_parent(rec_at(dets, a), rec_at(dets, b)) ? 1 : 0;
 }
 
+// The sort keys of the evaluation pipeline (classify_kernel) for a request, with the key plan
+// (sort_key_shift) of a counter budget `cap`: keys[i] (0xFFFFFFFF for same-parent pairs that
+// are more than a double excitation apart), returns the number of keys, nbucket/shift out.
+uint64_t mir_sort_keys(const void* dets, uint64_t ndet, int nref, const int32_t* order, int nfast,
+                       const uint32_t* pairs, uint64_t npairs, uint64_t cap, uint32_t* keys, uint32_t* nbucket,
+                       int32_t* shift) {
+  uint32_t nb = 1;
+  const int s = sort_key_shift(ndet, nref, cap, &nb);
+  *nbucket = nb;
+  *shift = s;
+  for (uint64_t i = 0; i < npairs; ++i) {
+    const DetRec x = rec_at(dets, pairs[2 * i]), w = rec_at(dets, pairs[2 * i + 1]);
+    const uint32_t dx = det_desc(x.parent, x.ra, x.rb), dw = det_desc(w.parent, w.ra, w.rb);
+    const int px = (int)(dx & 0xFF), pw = (int)(dw & 0xFF);
+    if (px == pw && far_same_parent(x, w)) {
+      keys[i] = 0xFFFFFFFFu;
+      continue;
+    }
+    const int cls = rank_class((int)((dx >> 8) & 15) + (int)((dw >> 8) & 15), (int)(dx >> 12) + (int)(dw >> 12));
+    keys[i] = pair_sort_key(cls, pairs[2 * i], pw, order[px * nref + pw], nfast, nref, nb, s);
+  }
+  return (uint64_t)kRankClasses * nb + (uint64_t)kRankClasses * ((uint64_t)nref * nref - nfast);
+}
+
 // Labels through the register (compile-time L) path and the runtime path.
 int mir_labels(const void* dets, uint32_t a, uint32_t b, int spin, int nocc, int n, int32_t* rows_ct, int32_t* cols_ct,
                int32_t* rows_rt, int32_t* cols_rt) {

@@ -26,6 +26,9 @@ def lib():
         L = ctypes.CDLL(_PATH)
         L.mir_unpack.argtypes = [VP, ctypes.c_int64, I32, I32, I32, U64, U64, D]
         L.mir_far_same_parent.argtypes = [VP, ctypes.c_uint32, ctypes.c_uint32]
+        L.mir_sort_keys.argtypes = [VP, ctypes.c_uint64, ctypes.c_int, I32, ctypes.c_int, U32, ctypes.c_uint64,
+                                    ctypes.c_uint64, U32, U32, I32]
+        L.mir_sort_keys.restype = ctypes.c_uint64
         L.mir_labels.argtypes = [VP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                  I32, I32, I32, I32]
         L.mir_svd.argtypes = [ctypes.c_int, D, ctypes.c_double, D, D, D, D]

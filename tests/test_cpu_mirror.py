@@ -133,3 +133,49 @@ def test_jacobi_svd_and_canonical_gauge(nzero):
     if nzero >= 1:
         z = slice(o - nzero, o)
         assert np.max(np.abs(u[:, z] - un[:, z])) < 1e-12 and np.max(np.abs(v[:, z] - vn[:, z])) < 1e-12
+
+
+@pytest.mark.parametrize("cap", [1 << 23, 5000, 26])
+def test_sort_keys_group_classes_and_bras(setup, cap):
+    """pair_sort_key / sort_key_shift as classify_kernel uses them: fast-pair keys lie in their
+    class's range [cls * nbucket, (cls + 1) * nbucket), keys of zero-overlap reference pairs
+    after all of them, every key below the planned count, the fast-class counters within the
+    budget, and with shift 0 one key holds one (bra, ket reference) combination."""
+    import ctypes
+    n, o, system, orc, basis, ob = setup
+    nref = 3
+    # the two forced zero-overlap reference pairs of the fixture, both orders
+    gen = {(0, 1), (1, 0), (1, 2), (2, 1)}
+    fast = [(x, w) for x in range(nref) for w in range(nref) if (x, w) not in gen]
+    slow = [(x, w) for x in range(nref) for w in range(nref) if (x, w) in gen]
+    order = np.zeros(nref * nref, np.int32)
+    for k, (x, w) in enumerate(fast + slow):
+        order[x * nref + w] = k
+    nfast = len(fast)
+    pairs = sy.sample_pairs(basis, 20000, seed=5, distinct_parents=False).astype(np.uint32)
+    keys = np.zeros(pairs.shape[0], np.uint32)
+    nb, sh = np.zeros(1, np.uint32), np.zeros(1, np.int32)
+    nkeys = MR.lib().mir_sort_keys(basis.ctypes.data_as(ctypes.c_void_p), basis.shape[0], nref, MR.p(order, ctypes.c_int32),
+                                   nfast, MR.p(pairs, ctypes.c_uint32), pairs.shape[0], cap, MR.p(keys, ctypes.c_uint32),
+                                   MR.p(nb, ctypes.c_uint32), MR.p(sh, ctypes.c_int32))
+    nb, sh = int(nb[0]), int(sh[0])
+    assert 26 * nb <= max(cap, 26) and nkeys == 26 * nb + 26 * len(slow)
+    ra, rb = basis["rank_a"].astype(int), basis["rank_b"].astype(int)
+    par = basis["parent"].astype(int)
+    live = keys != 0xFFFFFFFF
+    a, b = pairs[live, 0].astype(int), pairs[live, 1].astype(int)
+    k = keys[live].astype(np.int64)
+    assert np.all(k < nkeys)
+    la, lb = ra[a] + ra[b], rb[a] + rb[b]
+    cls = np.where((la <= 4) & (lb <= 4), la * 5 + lb, 25)
+    isfast = order[par[a] * nref + par[b]] < nfast
+    assert np.all(k[isfast] // nb == cls[isfast])
+    assert np.all(k[~isfast] >= 26 * nb)
+    assert np.all((k[~isfast] - 26 * nb) % 26 == cls[~isfast])
+    if sh == 0:
+        combo = a.astype(np.int64) * nref + par[b]
+        for key in np.unique(k[isfast])[:500]:
+            assert len(np.unique(combo[isfast][k[isfast] == key])) == 1
+    # far same-parent pairs are exactly the skipped ones
+    same = par[pairs[:, 0]] == par[pairs[:, 1]]
+    assert np.all(same[~live])

@@ -102,6 +102,40 @@ def test_device_entry_matches_host_entry_and_is_deterministic():
     assert np.array_equal(dev1, dev2)
 
 
+def test_pinned_host_entry_pipeline():
+    """Page-locked host buffers take the chunked copy-in / evaluate / copy-out pipeline of
+    nw_eval_hs_pairs; its results equal the device entry point's bit for bit, and an
+    out-of-range index in a late chunk is still reported."""
+    import torch
+    system = sy.config2_system()
+    basis = sy.sd_basis(30, 3, 3, 3)
+    pairs = sy.sample_pairs(basis, 1_500_001, seed=31).astype(np.uint32)
+    n = pairs.shape[0]
+    with _engine(system) as w:
+        w.set_basis(basis)
+        stream = torch.cuda.current_stream().cuda_stream
+        dp = torch.from_numpy(pairs.view(np.int32)).cuda()
+        dev = torch.empty((n, 2), dtype=torch.float64, device="cuda")
+        w.eval_pairs_device(dp.data_ptr(), n, dev.data_ptr(), stream)
+        w.sync(stream)
+        expected = dev.cpu().numpy()
+        hp = torch.from_numpy(pairs.view(np.int32).copy()).pin_memory()
+        ho = torch.full((n, 2), float("nan"), dtype=torch.float64).pin_memory()
+        st = w._lib.nw_eval_hs_pairs(w._ctx, hp.data_ptr(), n, ho.data_ptr(), None)
+        assert st == 0, w._lib.nw_last_error(w._ctx)
+        assert np.array_equal(ho.numpy(), expected)
+        # pageable buffers (single-shot path) agree too
+        assert np.array_equal(w.eval_pairs(pairs), expected)
+        hp.numpy().reshape(n, 2)[n - 3, 1] = basis.shape[0]
+        st = w._lib.nw_eval_hs_pairs(w._ctx, hp.data_ptr(), n, ho.data_ptr(), None)
+        assert st == 1
+        got = ho.numpy()
+        assert np.isnan(got[n - 3]).all()
+        mask = np.ones(n, bool)
+        mask[n - 3] = False
+        assert np.array_equal(got[mask], expected[mask])
+
+
 def test_hermiticity_at_scale():
     """Size-independent property at bench scale: H and S are symmetric, so (a, b) and (b, a)
     agree; 2 x 10^6 pairs."""
