@@ -155,6 +155,27 @@ NW_API nw_status nw_eval_hs_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs_dev
 NW_API nw_status nw_eval_s_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* s_dev,
                                  void* stream);
 
+/* Fock tables for the (F, S) path from the AO Fock matrices of each spin (row-major nao x nao,
+ * host memory): F^(mi,mj) = cx^(mi)^T F xc^(mj) and F_0^(m) = tr(M^(m) F) for every ordered
+ * reference pair, from the pairing kept by nw_build_intermediates.  Call again whenever the
+ * Fock matrices change (each SNOCI iteration).
+ * Replaces update_wicks_fock (src/noci/wicks.rs:290-330) and
+ * SameSpinBuild::construct_f_scalar (src/nonorthogonalwicks/build.rs:564-617). */
+NW_API nw_status nw_update_fock(nw_ctx* ctx, const double* fock_a, const double* fock_b);
+
+/* (F, S) per pair into fs_dev[2i], fs_dev[2i+1]: the Fock one-body element <x|F|w> and the
+ * overlap, device buffers, asynchronous on `stream`.  The SNOCI operator element is
+ * M = F - E0 S.  Same-parent pairs more than a double excitation apart give (0, 0).
+ * Replaces xw_f_overlap_prepared (src/nonorthogonalwicks/eval/prepareonebodyoverlap.rs:57-100),
+ * xw_f (eval/onebody.rs:40) and calculate_m_pair_wicks (src/noci/m.rs:160-197) before its
+ * E0 shift. */
+NW_API nw_status nw_eval_fs_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs,
+                                         double* fs_dev, void* stream);
+
+/* The same with host buffers (copies in, evaluates, copies out, returns when done). */
+NW_API nw_status nw_eval_fs_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* fs_host,
+                                  void* stream);
+
 /* Wait for the work queued on `stream` and report pair indices that were out of range in an
  * earlier device-buffer call (those outputs are NaN). */
 NW_API nw_status nw_sync(nw_ctx* ctx, void* stream);

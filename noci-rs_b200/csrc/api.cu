@@ -102,8 +102,8 @@ cudaError_t pipe_drain(nw_ctx* ctx) {
 // out (second copy engine, device -> host), so PCIe transfer in both directions overlaps the
 // kernels.  Starts after the work already queued on `caller` and returns when the results
 // are in hs_host.
-nw_status eval_hs_pipelined(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* hs_host, uint32_t* dp,
-                            double* dh, cudaStream_t caller) {
+nw_status eval_hs_pipelined(nw_ctx* ctx, nw::EvalMode mode, const uint32_t* pairs_host, uint64_t npairs,
+                            double* hs_host, uint32_t* dp, double* dh, cudaStream_t caller) {
   nw_status st = pipe_setup(ctx);
   if (st != NW_OK) return st;
   if ((st = nw::ensure(ctx, ctx->flag, 256)) != NW_OK) return st;
@@ -125,7 +125,7 @@ nw_status eval_hs_pipelined(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t np
       pipe_drain(ctx);
       return nw::cuda_fail(ctx, e, "pipelined copy-in");
     }
-    st = nw::eval_pairs(ctx, dp + 2 * o, nk, dh + 2 * o, false, ctx->s_comp, false);
+    st = nw::eval_pairs(ctx, dp + 2 * o, nk, dh + 2 * o, mode, ctx->s_comp, false);
     if (st != NW_OK) {
       pipe_drain(ctx);
       return st;
@@ -144,6 +144,29 @@ nw_status eval_hs_pipelined(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t np
   if (e != cudaSuccess) return nw::cuda_fail(ctx, e, "pipelined flag read");
   if (ed != cudaSuccess) return nw::cuda_fail(ctx, ed, "pipelined evaluation");
   NW_CUDA(ctx, cudaGetLastError());
+  if (*ctx->h_flag) return nw::fail(ctx, NW_ERR_INVALID, "pair index out of range of the determinant basis");
+  return NW_OK;
+}
+
+// Host-buffer evaluation (H, S) or (F, S): copy in, evaluate, copy out, synchronise.
+nw_status eval_host(nw_ctx* ctx, nw::EvalMode mode, const uint32_t* pairs_host, uint64_t npairs, double* out_host,
+                    void* stream) {
+  if (!ctx || (npairs && (!pairs_host || !out_host))) return NW_ERR_INVALID;
+  if (npairs == 0) return NW_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  nw_status st = nw::ensure(ctx, ctx->io_pairs, npairs * 2 * sizeof(uint32_t));
+  if (st != NW_OK) return st;
+  if ((st = nw::ensure(ctx, ctx->io_hs, npairs * 2 * sizeof(double))) != NW_OK) return st;
+  uint32_t* dp = static_cast<uint32_t*>(ctx->io_pairs.p);
+  double* dh = static_cast<double*>(ctx->io_hs.p);
+  if (npairs >= 2 * nw::kPipeMinChunk && is_pinned(pairs_host) && is_pinned(out_host))
+    return eval_hs_pipelined(ctx, mode, pairs_host, npairs, out_host, dp, dh, s);
+  NW_CUDA(ctx, cudaMemcpyAsync(dp, pairs_host, npairs * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  if ((st = nw::eval_pairs(ctx, dp, npairs, dh, mode, s)) != NW_OK) return st;
+  NW_CUDA(ctx, cudaMemcpyAsync(out_host, dh, npairs * 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  NW_CUDA(ctx, cudaMemcpyAsync(ctx->h_flag, ctx->flag.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  NW_CUDA(ctx, cudaStreamSynchronize(s));
   if (*ctx->h_flag) return nw::fail(ctx, NW_ERR_INVALID, "pair index out of range of the determinant basis");
   return NW_OK;
 }
@@ -277,7 +300,7 @@ nw_status nw_set_basis(nw_ctx* ctx, const nw_det* basis, uint64_t ndet) {
 nw_status nw_eval_hs_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* hs_dev,
                                   void* stream) {
   if (!ctx || (npairs && (!pairs_dev || !hs_dev))) return NW_ERR_INVALID;
-  return nw::eval_pairs(ctx, pairs_dev, npairs, hs_dev, false, static_cast<cudaStream_t>(stream));
+  return nw::eval_pairs(ctx, pairs_dev, npairs, hs_dev, nw::EvalMode::kHS, static_cast<cudaStream_t>(stream));
 }
 
 nw_status nw_eval_hs_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* hs_dev,
@@ -289,28 +312,29 @@ nw_status nw_eval_hs_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs_dev, uint6
 nw_status nw_eval_s_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* s_dev,
                                  void* stream) {
   if (!ctx || (npairs && (!pairs_dev || !s_dev))) return NW_ERR_INVALID;
-  return nw::eval_pairs(ctx, pairs_dev, npairs, s_dev, true, static_cast<cudaStream_t>(stream));
+  return nw::eval_pairs(ctx, pairs_dev, npairs, s_dev, nw::EvalMode::kS, static_cast<cudaStream_t>(stream));
 }
 
 nw_status nw_eval_hs_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* hs_host, void* stream) {
-  if (!ctx || (npairs && (!pairs_host || !hs_host))) return NW_ERR_INVALID;
-  if (npairs == 0) return NW_OK;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return eval_host(ctx, nw::EvalMode::kHS, pairs_host, npairs, hs_host, stream);
+}
+
+nw_status nw_update_fock(nw_ctx* ctx, const double* fock_a, const double* fock_b) {
+  if (!ctx || !fock_a || !fock_b) return NW_ERR_INVALID;
+  const size_t n2 = (size_t)ctx->nao * ctx->nao;
+  if (!finite_all(fock_a, n2) || !finite_all(fock_b, n2)) return nw::fail(ctx, NW_ERR_INVALID, "non-finite Fock matrix");
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
-  nw_status st = nw::ensure(ctx, ctx->io_pairs, npairs * 2 * sizeof(uint32_t));
-  if (st != NW_OK) return st;
-  if ((st = nw::ensure(ctx, ctx->io_hs, npairs * 2 * sizeof(double))) != NW_OK) return st;
-  uint32_t* dp = static_cast<uint32_t*>(ctx->io_pairs.p);
-  double* dh = static_cast<double*>(ctx->io_hs.p);
-  if (npairs >= 2 * nw::kPipeMinChunk && is_pinned(pairs_host) && is_pinned(hs_host))
-    return eval_hs_pipelined(ctx, pairs_host, npairs, hs_host, dp, dh, s);
-  NW_CUDA(ctx, cudaMemcpyAsync(dp, pairs_host, npairs * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-  if ((st = nw::eval_pairs(ctx, dp, npairs, dh, false, s)) != NW_OK) return st;
-  NW_CUDA(ctx, cudaMemcpyAsync(hs_host, dh, npairs * 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
-  NW_CUDA(ctx, cudaMemcpyAsync(ctx->h_flag, ctx->flag.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  NW_CUDA(ctx, cudaStreamSynchronize(s));
-  if (*ctx->h_flag) return nw::fail(ctx, NW_ERR_INVALID, "pair index out of range of the determinant basis");
-  return NW_OK;
+  return nw::update_fock(ctx, fock_a, fock_b);
+}
+
+nw_status nw_eval_fs_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* fs_dev,
+                                  void* stream) {
+  if (!ctx || (npairs && (!pairs_dev || !fs_dev))) return NW_ERR_INVALID;
+  return nw::eval_pairs(ctx, pairs_dev, npairs, fs_dev, nw::EvalMode::kFS, static_cast<cudaStream_t>(stream));
+}
+
+nw_status nw_eval_fs_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* fs_host, void* stream) {
+  return eval_host(ctx, nw::EvalMode::kFS, pairs_host, npairs, fs_host, stream);
 }
 
 nw_status nw_sync(nw_ctx* ctx, void* stream) {
@@ -367,6 +391,9 @@ nw_status nw_ctx_destroy(nw_ctx* ctx) {
   if (ctx->d_order) cudaFree(ctx->d_order);
   if (ctx->d_dets) cudaFree(ctx->d_dets);
   if (ctx->d_desc) cudaFree(ctx->d_desc);
+  for (double* b : {ctx->d_fbase, ctx->d_fock, ctx->d_fslab})
+    if (b) cudaFree(b);
+  if (ctx->d_fockp) cudaFree(ctx->d_fockp);
   free_buf(ctx->keys);
   free_buf(ctx->ranks);
   free_buf(ctx->tsum);

@@ -245,6 +245,17 @@ __global__ void trace_kernel(const double* const* __restrict__ as, const double*
   if (threadIdx.x == 0) out[blockIdx.x] = red[0];
 }
 
+// Fock records: frecx = {X0, F^(00)}, frecy = {Y0, F^(00)} from the Hamiltonian records.
+__global__ void fock_records_kernel(const double2* __restrict__ recx, const double2* __restrict__ recy,
+                                    const double* __restrict__ ff00, int n, double2* __restrict__ frecx,
+                                    double2* __restrict__ frecy) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n; idx += gridDim.x * blockDim.x) {
+    const double f = ff00[idx];
+    frecx[idx] = make_double2(recx[idx].x, f);
+    frecy[idx] = make_double2(recy[idx].x, f);
+  }
+}
+
 // dst[c][r] = src[r][c] (n x n)
 __global__ void transpose_kernel(const double* __restrict__ src, int n, double* __restrict__ dst) {
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n; idx += gridDim.x * blockDim.x) {
@@ -729,8 +740,132 @@ nw_status build_all(nw_ctx* ctx) {
   NW_CUDA(ctx, cudaMemcpy(ctx->d_fast, hfast.data(), sizeof(FastPair) * npair, cudaMemcpyHostToDevice));
   NW_CUDA(ctx, cudaMemcpy(ctx->d_gen, hgen.data(), sizeof(GenPair) * npair, cudaMemcpyHostToDevice));
   NW_CUDA(ctx, cudaMemcpy(ctx->d_order, ctx->order_host.data(), sizeof(int32_t) * npair, cudaMemcpyHostToDevice));
+
+  // ---------------- kept for the Fock path ----------------
+  // per (pair, spin): [M^(0), M^(1), cx^(0), cx^(1), xc^(0), xc^(1)]
+  ctx->fock_ready = false;
+  if (ctx->d_fbase) {
+    cudaFree(ctx->d_fbase);
+    ctx->d_fbase = nullptr;
+  }
+  if (cudaMalloc(&ctx->d_fbase, sizeof(double) * nps * 6 * n2) != cudaSuccess)
+    return fail(ctx, NW_ERR_ALLOC, "Fock basis allocation failed");
+  const double* kept[3] = {M, cx, xc};
+  for (int k = 0; k < 3; ++k)
+    NW_CUDA(ctx, cudaMemcpy2D(ctx->d_fbase + 2 * k * n2, 6 * n2 * sizeof(double), kept[k], 2 * n2 * sizeof(double),
+                              2 * n2 * sizeof(double), nps, cudaMemcpyDeviceToDevice));
+  ctx->fast_host = hfast;
+  ctx->gen_host = hgen;
+  ctx->generic_host = generic;
   NW_CUDA(ctx, cudaDeviceSynchronize());
   ctx->built = true;
+  return NW_OK;
+}
+
+// Fock tables for the F + S path (update_wicks_fock, src/noci/wicks.rs:290-330, with
+// construct_f_scalar, build.rs:564-617): per (pair, spin) F^(mi,mj) = cx^(mi)^T F xc^(mj) and
+// F_0^(m) = tr(M^(m) F) from the M, cx, xc kept by the build (the same Loewdin pairing and
+// null gauge as the Hamiltonian intermediates).
+nw_status update_fock(nw_ctx* ctx, const double* fa, const double* fb) {
+  if (!ctx->built || !ctx->d_fbase) return fail(ctx, NW_ERR_STATE, "intermediates not built");
+  const int n = ctx->nmo, nref = ctx->nref, npair = nref * nref, nps = 2 * npair;
+  const size_t n2 = (size_t)n * n;
+  cublasHandle_t h = ctx->blas;
+  ctx->fock_ready = false;
+  if (!ctx->d_fock && cudaMalloc(&ctx->d_fock, sizeof(double) * 2 * n2) != cudaSuccess)
+    return fail(ctx, NW_ERR_ALLOC, "Fock matrix allocation failed");
+  NW_CUDA(ctx, cudaMemcpy(ctx->d_fock, fa, sizeof(double) * n2, cudaMemcpyHostToDevice));
+  NW_CUDA(ctx, cudaMemcpy(ctx->d_fock + n2, fb, sizeof(double) * n2, cudaMemcpyHostToDevice));
+  double* work = nullptr;
+  if (cudaMalloc(&work, sizeof(double) * nps * 6 * n2) != cudaSuccess)
+    return fail(ctx, NW_ERR_ALLOC, "Fock workspace allocation failed");
+  struct Free {
+    void* p;
+    ~Free() { cudaFree(p); }
+  } free_work{work};
+  double* Fxc = work;                 // [ps][mj]
+  double* ff = work + nps * 2 * n2;   // [ps][mi][mj]
+  const double* fbase = ctx->d_fbase;
+  // Fxc[2p+s][mj] = F_s xc[2p+s][mj]
+  for (int s = 0; s < 2; ++s)
+    for (int mj = 0; mj < 2; ++mj)
+      NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, ctx->d_fock + s * n2, n, 0, fbase + s * 6 * n2 + (4 + mj) * n2,
+                          n, 12 * n2, 0.0, Fxc + (size_t)(s * 2 + mj) * n2, n, 4 * n2, npair));
+  // ff[ps][mi][mj] = cx[ps][mi]^T Fxc[ps][mj]
+  for (int mi = 0; mi < 2; ++mi)
+    for (int mj = 0; mj < 2; ++mj)
+      NW_BLAS(ctx, gemm_b(h, true, false, n, n, n, 1.0, fbase + (2 + mi) * n2, n, 6 * n2, Fxc + mj * n2, n, 2 * n2, 0.0,
+                          ff + (size_t)(mi * 2 + mj) * n2, n, 4 * n2, nps));
+  // f0f[ps][m] = tr(M[ps][m] F_s)
+  const int ntr = 2 * nps;
+  std::vector<const double*> ha(ntr), hb(ntr);
+  for (int ps = 0; ps < nps; ++ps)
+    for (int m = 0; m < 2; ++m) {
+      ha[ps * 2 + m] = fbase + (size_t)ps * 6 * n2 + m * n2;
+      hb[ps * 2 + m] = ctx->d_fock + (ps & 1) * n2;
+    }
+  std::vector<double> f0f(ntr);
+  {
+    const double** dptr = nullptr;
+    double* dtr = nullptr;
+    NW_CUDA(ctx, cudaMalloc(&dptr, sizeof(double*) * 2 * ntr));
+    NW_CUDA(ctx, cudaMalloc(&dtr, sizeof(double) * ntr));
+    cudaError_t e = cudaMemcpy(dptr, ha.data(), sizeof(double*) * ntr, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dptr + ntr, hb.data(), sizeof(double*) * ntr, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      trace_kernel<<<ntr, 256>>>(dptr, dptr + ntr, n, dtr);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(f0f.data(), dtr, sizeof(double) * ntr, cudaMemcpyDeviceToHost);
+    cudaFree(dptr);
+    cudaFree(dtr);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "Fock trace kernel");
+  }
+  // slab: fast pairs {X0|Y0, F^(00)} records per spin, other pairs F^(mi,mj) transposed
+  size_t slab = 0;
+  std::vector<size_t> off(npair);
+  for (int p = 0; p < npair; ++p) {
+    off[p] = slab;
+    slab += 8 * n2;  // per spin: two records of 2 n^2 doubles (fast) or four n^2 matrices (other)
+  }
+  if (ctx->d_fslab) {
+    cudaFree(ctx->d_fslab);
+    ctx->d_fslab = nullptr;
+  }
+  if (cudaMalloc(&ctx->d_fslab, sizeof(double) * std::max<size_t>(slab, 32)) != cudaSuccess)
+    return fail(ctx, NW_ERR_ALLOC, "Fock table allocation failed");
+  std::vector<FockPair> hfock(npair);
+  std::memset(hfock.data(), 0, sizeof(FockPair) * npair);
+  const int g2 = grid_for(n2);
+  for (int p = 0; p < npair; ++p) {
+    for (int s = 0; s < 2; ++s) {
+      const int ps = 2 * p + s;
+      FockSpinTab& t = s ? hfock[p].b : hfock[p].a;
+      double* base = ctx->d_fslab + off[p] + (size_t)s * 4 * n2;
+      const double* ffps = ff + (size_t)ps * 4 * n2;
+      if (!ctx->generic_host[p]) {
+        const FastSpin& fs = s ? ctx->fast_host[p].b : ctx->fast_host[p].a;
+        double2* frecx = reinterpret_cast<double2*>(base);
+        double2* frecy = reinterpret_cast<double2*>(base + 2 * n2);
+        fock_records_kernel<<<g2, 256>>>(fs.recx, fs.recy, ffps, n, frecx, frecy);
+        t.recx = frecx;
+        t.recy = frecy;
+      } else {
+        for (int k = 0; k < 4; ++k) {
+          transpose_kernel<<<g2, 256>>>(ffps + k * n2, n, base + k * n2);
+          t.ff_t[k >> 1][k & 1] = base + k * n2;
+        }
+      }
+      NW_CUDA(ctx, cudaGetLastError());
+      t.f0f[0] = f0f[ps * 2];
+      t.f0f[1] = f0f[ps * 2 + 1];
+    }
+  }
+  if (!ctx->d_fockp && cudaMalloc(&ctx->d_fockp, sizeof(FockPair) * npair) != cudaSuccess)
+    return fail(ctx, NW_ERR_ALLOC, "Fock table allocation failed");
+  NW_CUDA(ctx, cudaMemcpy(ctx->d_fockp, hfock.data(), sizeof(FockPair) * npair, cudaMemcpyHostToDevice));
+  NW_CUDA(ctx, cudaDeviceSynchronize());
+  ctx->fock_ready = true;
   return NW_OK;
 }
 

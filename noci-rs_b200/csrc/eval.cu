@@ -40,40 +40,64 @@ __device__ __forceinline__ void store_hs(double* out, uint64_t i, double h, doub
 // from the per-key counter with one global atomic per pair.  The class comes from the 16-bit
 // determinant descriptors; the full records are read only for same-parent pairs, which need
 // the excitation-distance rule.
+__device__ __forceinline__ uint32_t classify_one(const EvalParams& P, uint2 ab, uint64_t i, double* __restrict__ out,
+                                                 int out_stride, uint32_t* __restrict__ flag) {
+  if (ab.x >= P.ndet || ab.y >= P.ndet) {
+    atomicOr(flag, 1u);
+    const double nan = __longlong_as_double(0x7FF8000000000000ll);
+    if (out_stride == 2)
+      store_hs(out, i, nan, nan);
+    else
+      out[i] = nan;
+    return kSkipKey;
+  }
+  const uint32_t dx = __ldg(P.desc + ab.x), dw = __ldg(P.desc + ab.y);
+  const int px = (int)(dx & 0xFF), pw = (int)(dw & 0xFF);
+  if (px == pw && far_same_parent(load_det(P.dets, ab.x), load_det(P.dets, ab.y))) {
+    if (out_stride == 2)
+      store_hs(out, i, 0.0, 0.0);
+    else
+      out[i] = 0.0;
+    return kSkipKey;
+  }
+  const int cls = rank_class((int)((dx >> 8) & 15) + (int)((dw >> 8) & 15), (int)(dx >> 12) + (int)(dw >> 12));
+  const int ord = __ldg(P.order + px * P.nref + pw);
+  return pair_sort_key(cls, ab.x, pw, ord, P.nfast, P.nref, P.nbucket, P.shift);
+}
+
+// Items per thread and loop trip in the sort kernels: independent loads and atomics of
+// kSortUnroll pairs are in flight together (the chains are latency-bound otherwise).
+constexpr int kSortUnroll = 4;
+
 __global__ void __launch_bounds__(256) classify_kernel(EvalParams P, const uint32_t* __restrict__ pairs,
                                                        uint64_t npairs, uint32_t* __restrict__ keys,
                                                        uint32_t* __restrict__ ranks, uint32_t* __restrict__ counts,
                                                        double* __restrict__ out, int out_stride,
                                                        uint32_t* __restrict__ flag) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < npairs; i += stride) {
-    const uint2 ab = __ldg(reinterpret_cast<const uint2*>(pairs) + i);
-    uint32_t key = kSkipKey;
-    if (ab.x >= P.ndet || ab.y >= P.ndet) {
-      atomicOr(flag, 1u);
-      const double nan = __longlong_as_double(0x7FF8000000000000ll);
-      if (out_stride == 2)
-        store_hs(out, i, nan, nan);
-      else
-        out[i] = nan;
-    } else {
-      const uint32_t dx = __ldg(P.desc + ab.x), dw = __ldg(P.desc + ab.y);
-      const int px = (int)(dx & 0xFF), pw = (int)(dw & 0xFF);
-      bool far = false;
-      if (px == pw) far = far_same_parent(load_det(P.dets, ab.x), load_det(P.dets, ab.y));
-      if (far) {
-        if (out_stride == 2)
-          store_hs(out, i, 0.0, 0.0);
-        else
-          out[i] = 0.0;
-      } else {
-        const int cls = rank_class((int)((dx >> 8) & 15) + (int)((dw >> 8) & 15), (int)(dx >> 12) + (int)(dw >> 12));
-        const int ord = __ldg(P.order + px * P.nref + pw);
-        key = pair_sort_key(cls, ab.x, pw, ord, P.nfast, P.nref, P.nbucket, P.shift);
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i0 < npairs; i0 += kSortUnroll * nthreads) {
+    uint2 ab[kSortUnroll];
+    uint32_t key[kSortUnroll], rk[kSortUnroll];
+#pragma unroll
+    for (int u = 0; u < kSortUnroll; ++u) {
+      const uint64_t i = i0 + u * nthreads;
+      ab[u] = i < npairs ? __ldg(reinterpret_cast<const uint2*>(pairs) + i) : make_uint2(0u, 0u);
+    }
+#pragma unroll
+    for (int u = 0; u < kSortUnroll; ++u) {
+      const uint64_t i = i0 + u * nthreads;
+      key[u] = i < npairs ? classify_one(P, ab[u], i, out, out_stride, flag) : kSkipKey;
+    }
+#pragma unroll
+    for (int u = 0; u < kSortUnroll; ++u) rk[u] = key[u] != kSkipKey ? atomicAdd(&counts[key[u]], 1u) : 0u;
+#pragma unroll
+    for (int u = 0; u < kSortUnroll; ++u) {
+      const uint64_t i = i0 + u * nthreads;
+      if (i < npairs) {
+        keys[i] = key[u];
+        ranks[i] = rk[u];
       }
     }
-    keys[i] = key;
-    if (key != kSkipKey) ranks[i] = atomicAdd(&counts[key], 1u);
   }
 }
 
@@ -166,11 +190,20 @@ __global__ void __launch_bounds__(256) scatter_kernel(const uint32_t* __restrict
                                                       const uint32_t* __restrict__ ranks, uint64_t npairs,
                                                       const uint32_t* __restrict__ offsets,
                                                       uint32_t* __restrict__ sidx) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < npairs; i += stride) {
-    const uint32_t k = keys[i];
-    if (k == kSkipKey) continue;
-    sidx[__ldg(offsets + k) + ranks[i]] = (uint32_t)i;
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i0 < npairs; i0 += kSortUnroll * nthreads) {
+    uint32_t k[kSortUnroll], r[kSortUnroll], o[kSortUnroll];
+#pragma unroll
+    for (int u = 0; u < kSortUnroll; ++u) {
+      const uint64_t i = i0 + u * nthreads;
+      k[u] = i < npairs ? keys[i] : kSkipKey;
+      r[u] = i < npairs ? ranks[i] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < kSortUnroll; ++u) o[u] = k[u] != kSkipKey ? __ldg(offsets + k[u]) : 0u;
+#pragma unroll
+    for (int u = 0; u < kSortUnroll; ++u)
+      if (k[u] != kSkipKey) sidx[o[u] + r[u]] = (uint32_t)(i0 + u * nthreads);
   }
 }
 
@@ -290,6 +323,94 @@ __global__ void __launch_bounds__(128) eval_gen_kernel(EvalParams P, const uint2
 }
 
 // ---------------------------------------------------------------------------------------
+// Fock one-body element with the overlap, (F, S) per pair, over the same sorted order.
+// ---------------------------------------------------------------------------------------
+template <int LA, int LB>
+__device__ __forceinline__ void run_fs_class(const EvalParams& P, const uint2* __restrict__ pairs,
+                                             const uint32_t* __restrict__ sidx, const uint32_t* __restrict__ offsets,
+                                             double* __restrict__ out) {
+  constexpr int c = LA * 5 + LB;
+  const uint32_t begin = offsets[c * P.nbucket];
+  const uint32_t end = offsets[(c + 1) * P.nbucket];
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t t = begin + blockIdx.x * blockDim.x + threadIdx.x; t < end; t += stride) {
+    const uint32_t i = sidx[t];
+    const uint2 ab = __ldg(pairs + i);
+    const DetRec x = load_det(P.dets, ab.x);
+    const DetRec w = load_det(P.dets, ab.y);
+    const int p = (int)x.parent * P.nref + (int)w.parent;
+    double f, s;
+    if constexpr (c == 25)
+      eval_fs_m0_rt(P.fast[p], P.fock[p], x, w, P.n, P.nocc_a, P.nocc_b, &f, &s);
+    else
+      eval_fs_m0_ct<LA, LB>(P.fast[p], P.fock[p], x, w, P.n, P.nocc_a, P.nocc_b, &f, &s);
+    store_hs(out, i, f, s);
+  }
+}
+
+__global__ void __launch_bounds__(256) eval_fs_light_kernel(EvalParams P, const uint2* __restrict__ pairs,
+                                                            const uint32_t* __restrict__ sidx,
+                                                            const uint32_t* __restrict__ offsets,
+                                                            double* __restrict__ out) {
+  run_fs_class<2, 2>(P, pairs, sidx, offsets, out);
+  run_fs_class<2, 1>(P, pairs, sidx, offsets, out);
+  run_fs_class<1, 2>(P, pairs, sidx, offsets, out);
+  run_fs_class<2, 0>(P, pairs, sidx, offsets, out);
+  run_fs_class<0, 2>(P, pairs, sidx, offsets, out);
+  run_fs_class<1, 1>(P, pairs, sidx, offsets, out);
+  run_fs_class<1, 0>(P, pairs, sidx, offsets, out);
+  run_fs_class<0, 1>(P, pairs, sidx, offsets, out);
+  run_fs_class<0, 0>(P, pairs, sidx, offsets, out);
+}
+
+__global__ void __launch_bounds__(256) eval_fs_heavy_kernel(EvalParams P, const uint2* __restrict__ pairs,
+                                                            const uint32_t* __restrict__ sidx,
+                                                            const uint32_t* __restrict__ offsets,
+                                                            double* __restrict__ out) {
+  run_fs_class<3, 1>(P, pairs, sidx, offsets, out);
+  run_fs_class<1, 3>(P, pairs, sidx, offsets, out);
+  run_fs_class<3, 0>(P, pairs, sidx, offsets, out);
+  run_fs_class<0, 3>(P, pairs, sidx, offsets, out);
+  run_fs_class<3, 2>(P, pairs, sidx, offsets, out);
+  run_fs_class<2, 3>(P, pairs, sidx, offsets, out);
+  run_fs_class<3, 3>(P, pairs, sidx, offsets, out);
+  run_fs_class<4, 0>(P, pairs, sidx, offsets, out);
+  run_fs_class<0, 4>(P, pairs, sidx, offsets, out);
+  run_fs_class<4, 1>(P, pairs, sidx, offsets, out);
+  run_fs_class<1, 4>(P, pairs, sidx, offsets, out);
+  run_fs_class<4, 2>(P, pairs, sidx, offsets, out);
+  run_fs_class<2, 4>(P, pairs, sidx, offsets, out);
+  run_fs_class<4, 3>(P, pairs, sidx, offsets, out);
+  run_fs_class<3, 4>(P, pairs, sidx, offsets, out);
+  run_fs_class<4, 4>(P, pairs, sidx, offsets, out);
+  run_fs_class<5, 0>(P, pairs, sidx, offsets, out);  // class 25: runtime ranks
+}
+
+__device__ __noinline__ void eval_fs_gen_one(const GenPair& g, const FockPair& fk, const DetRec& x, const DetRec& w,
+                                             const EvalParams& P, double* F, double* S) {
+  eval_fs_gen_pair(g, fk, x, w, P.n, P.nocc_a, P.nocc_b, P.tol, P.exact != 0, F, S);
+}
+
+__global__ void __launch_bounds__(128) eval_fs_gen_kernel(EvalParams P, const uint2* __restrict__ pairs,
+                                                          const uint32_t* __restrict__ sidx,
+                                                          const uint32_t* __restrict__ offsets, int nkeys,
+                                                          double* __restrict__ out) {
+  const uint32_t begin = offsets[kClasses * P.nbucket];
+  const uint32_t end = offsets[nkeys];
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t t = begin + blockIdx.x * blockDim.x + threadIdx.x; t < end; t += stride) {
+    const uint32_t i = sidx[t];
+    const uint2 ab = __ldg(pairs + i);
+    const DetRec x = load_det(P.dets, ab.x);
+    const DetRec w = load_det(P.dets, ab.y);
+    const int p = (int)x.parent * P.nref + (int)w.parent;
+    double f, s;
+    eval_fs_gen_one(P.gen[p], P.fock[p], x, w, P, &f, &s);
+    store_hs(out, i, f, s);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // Overlap only (no sorting: one cheap determinant per spin).
 // ---------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(128) eval_s_kernel(EvalParams P, const uint32_t* __restrict__ pairs,
@@ -339,6 +460,7 @@ EvalParams make_params(const nw_ctx* ctx) {
   P.enuc = ctx->enuc;
   P.tol = ctx->tol;
   P.desc = ctx->d_desc;
+  P.fock = ctx->d_fockp;
   P.nbucket = 1;
   P.shift = 0;
   return P;
@@ -373,7 +495,8 @@ uint64_t plan_keys(const nw_ctx* ctx, EvalParams& P, uint64_t cap) {
 // classify -> scan -> scatter -> evaluate, all on `stream`.  The flag must already be cleared
 // (or hold earlier calls' reports); ev (six events or null) brackets the phases.
 nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const uint32_t* pairs, uint64_t npairs,
-                        double* out, const SortScratch& S, cudaStream_t stream, cudaEvent_t* ev) {
+                        double* out, const SortScratch& S, cudaStream_t stream, cudaEvent_t* ev,
+                        EvalMode mode = EvalMode::kHS) {
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[0], stream));
   NW_CUDA(ctx, cudaMemsetAsync(S.counts, 0, sizeof(uint32_t) * nkeys, stream));
   classify_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(P, pairs, npairs, S.keys, S.ranks,
@@ -391,15 +514,23 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[3], stream));
   const uint2* pp = reinterpret_cast<const uint2*>(pairs);
   if (ctx->nfast > 0) {
-    eval_light_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
-    eval_medium_kernel<<<148 * 2, 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
-    eval_heavy_kernel<<<148, 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
-    eval_rt_kernel<<<148 * 2, 128, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
+    if (mode == EvalMode::kFS) {
+      eval_fs_light_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
+      eval_fs_heavy_kernel<<<148 * 2, 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
+    } else {
+      eval_light_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
+      eval_medium_kernel<<<148 * 2, 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
+      eval_heavy_kernel<<<148, 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
+      eval_rt_kernel<<<148 * 2, 128, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
+    }
     NW_CUDA(ctx, cudaGetLastError());
   }
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[4], stream));
   if (ctx->nfast < ctx->nref * ctx->nref) {
-    eval_gen_kernel<<<148 * 4, 128, 0, stream>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out);
+    if (mode == EvalMode::kFS)
+      eval_fs_gen_kernel<<<148 * 4, 128, 0, stream>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out);
+    else
+      eval_gen_kernel<<<148 * 4, 128, 0, stream>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out);
     NW_CUDA(ctx, cudaGetLastError());
   }
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[5], stream));
@@ -408,10 +539,12 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
 
 }  // namespace
 
-nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, bool overlap_only,
+nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, EvalMode mode,
                      cudaStream_t stream, bool clear_flag) {
   if (!ctx->built) return fail(ctx, NW_ERR_STATE, "intermediates not built");
   if (!ctx->d_dets) return fail(ctx, NW_ERR_STATE, "no determinant basis set");
+  if (mode == EvalMode::kFS && !ctx->fock_ready) return fail(ctx, NW_ERR_STATE, "Fock tables not set (nw_update_fock)");
+  const bool overlap_only = mode == EvalMode::kS;
   if (npairs == 0) return NW_OK;
   if (npairs >= 0xFFFFFFFFull) return fail(ctx, NW_ERR_UNSUPPORTED, "at most 2^32 - 2 pairs per call");
   if ((reinterpret_cast<uintptr_t>(pairs) & 7) != 0) return fail(ctx, NW_ERR_INVALID, "pairs must be 8-byte aligned");
@@ -445,7 +578,7 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
   S.offsets = static_cast<uint32_t*>(ctx->offsets.p);
   S.tsum = static_cast<uint32_t*>(ctx->tsum.p);
   S.flag = flag;
-  st = launch_sorted(ctx, P, nkeys, pairs, npairs, out, S, stream, ctx->timing ? ctx->ev : nullptr);
+  st = launch_sorted(ctx, P, nkeys, pairs, npairs, out, S, stream, ctx->timing ? ctx->ev : nullptr, mode);
   if (st == NW_OK && ctx->timing) ctx->timed_valid = true;
   return st;
 }

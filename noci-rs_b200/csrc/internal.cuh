@@ -28,6 +28,7 @@ struct EvalParams {
   int32_t nfast;           // number of fast ordered pairs (sort positions 0..nfast-1)
   int32_t exact;
   const uint16_t* desc;    // per-determinant class descriptor (det_desc)
+  const FockPair* fock;    // Fock tables (after nw_update_fock), indexed like fast/gen
   uint32_t nbucket;        // sort keys per rank class for fast pairs (pair_sort_key)
   int32_t shift;
   double enuc, tol;
@@ -81,6 +82,17 @@ struct nw_ctx {
   cudaEvent_t ev_start = nullptr;
   cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr};
 
+  // Fock (F + S) path: per (pair, spin) [M^(0), M^(1), cx^(0), cx^(1), xc^(0), xc^(1)] kept
+  // from the build, the AO Fock matrices, their per-pair tables and records
+  double* d_fbase = nullptr;        // 2 nref^2 x 6 x n^2
+  double* d_fock = nullptr;         // F_alpha, F_beta (nao x nao each)
+  double* d_fslab = nullptr;
+  nw::FockPair* d_fockp = nullptr;  // nref^2
+  bool fock_ready = false;
+  std::vector<nw::FastPair> fast_host;
+  std::vector<nw::GenPair> gen_host;
+  std::vector<char> generic_host;  // per ordered pair: m_alpha + m_beta > 0
+
   cublasHandle_t blas = nullptr;
   std::string last_error;
 
@@ -103,10 +115,15 @@ nw_status ensure(nw_ctx* ctx, DevBuf& b, size_t bytes);
 
 // Build (build.cu).
 nw_status build_all(nw_ctx* ctx);
+// Fock tables from AO Fock matrices (build.cu).
+nw_status update_fock(nw_ctx* ctx, const double* fa, const double* fb);
+
+// What a pair evaluation produces.
+enum class EvalMode { kHS, kS, kFS };
 
 // Evaluation (eval.cu).
 // clear_flag = false keeps the out-of-range flag of earlier calls (chunked host path).
-nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, bool overlap_only,
+nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, EvalMode mode,
                      cudaStream_t stream, bool clear_flag = true);
 // Same evaluation with its scratch in a fixed device array (no device allocation).
 nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, cudaStream_t stream);

@@ -77,6 +77,21 @@ struct GenPair {
   double vba0[2][2];
 };
 
+// Fock-operator tables of one ordered reference pair (update_wicks_fock, src/noci/wicks.rs:290-330;
+// construct_f_scalar, src/nonorthogonalwicks/build.rs:564-617).  Pairs without zero-overlap
+// orbitals read records {X^(0)|Y^(0), F^(00)} gathered like the Hamiltonian records; the
+// others read F^(mi,mj) transposed ([c][r]) next to their reference-ordered X/Y.
+struct FockSpinTab {
+  const double2* recx;       // n*n {X^(0)[r][c], F^(00)[r][c]}
+  const double2* recy;       // n*n {Y^(0)[r][c], F^(00)[r][c]}
+  const double* ff_t[2][2];  // F^(mi,mj)[c][r]
+  double f0f[2];             // F_0^(m) = tr(M^(m) F)
+};
+
+struct FockPair {
+  FockSpinTab a, b;
+};
+
 
 // ---------------------------------------------------------------------------------------
 // Small determinants.
@@ -1102,6 +1117,178 @@ NW_HD double eval_s_pair(const FastPair* fp, const GenPair* g, const DetRec& x, 
     pref = g->a.pref * g->b.pref;
   }
   return x.phase * w.phase * pref * sa * sb;
+}
+
+// ---------------------------------------------------------------------------------------
+// Fock one-body element with the overlap (xw_f_overlap_prepared,
+// src/nonorthogonalwicks/eval/prepareonebodyoverlap.rs:57-100; xw_f, eval/onebody.rs:40;
+// combined per spin as calculate_m_pair_wicks, src/noci/m.rs:160-197).
+// Per spin:  F_sigma = F_0 det D - sum_{r,c} cof[r][c] F[row_r][col_c]  (m = 0), and the
+// distribution sum over (m_1; m_col...) for m > 0.  With the spin overlaps S_sigma:
+//   F = ph (F_alpha S_beta + F_beta S_alpha),  S = ph S_alpha S_beta,
+// where a term is skipped when the other spin's overlap is exactly zero (m.rs:187-193).
+// ---------------------------------------------------------------------------------------
+template <int L>
+NW_HD void spin_f_ct(const double2* rec_lo, const double2* rec_up, double f0, int n, const int* rows,
+                     const int* cols, double* det_out, double* f_out) {
+  if (L == 0) {
+    *det_out = 1.0;
+    *f_out = f0;
+    return;
+  }
+  double d[L > 0 ? L * L : 1], fc[L > 0 ? L * L : 1], cof[L > 0 ? L * L : 1];
+#pragma unroll
+  for (int i = 0; i < L; ++i)
+#pragma unroll
+    for (int j = 0; j < L; ++j) {
+      const int64_t e = (int64_t)rows[i] * n + cols[j];
+#ifdef __CUDA_ARCH__
+      const double2 v = __ldg(i >= j ? rec_lo + e : rec_up + e);
+#else
+      const double2 v = i >= j ? rec_lo[e] : rec_up[e];
+#endif
+      d[i * L + j] = v.x;
+      fc[i * L + j] = v.y;
+    }
+  const double det = cofactors_ct<L>(cof, d);
+  double f = f0 * det;
+#pragma unroll
+  for (int i = 0; i < L * L; ++i) f -= cof[i] * fc[i];
+  *det_out = det;
+  *f_out = f;
+}
+
+NW_HD void spin_f_rt(int L, const double2* rec_lo, const double2* rec_up, double f0, int n, const int* rows,
+                     const int* cols, double* det_out, double* f_out) {
+  if (L == 0) {
+    *det_out = 1.0;
+    *f_out = f0;
+    return;
+  }
+  double d[kML * kML], fc[kML * kML], cof[kML * kML];
+  for (int i = 0; i < L; ++i)
+    for (int j = 0; j < L; ++j) {
+      const int64_t e = (int64_t)rows[i] * n + cols[j];
+      const double2 v = i >= j ? rec_lo[e] : rec_up[e];
+      d[i * L + j] = v.x;
+      fc[i * L + j] = v.y;
+    }
+  const double det = cofactors_rt(cof, d, L);
+  double f = f0 * det;
+  for (int i = 0; i < L * L; ++i) f -= cof[i] * fc[i];
+  *det_out = det;
+  *f_out = f;
+}
+
+// m > 0: sum over the distributions (m_1; m_col_1..L) with sum m (onebody.rs, helpers.rs:682-712);
+// the column-replacement correction is formed as in the reference, sum_r (F - D) cof, so that
+// det + correction replaces column c by the Fock column.
+NW_HD double spin_f_gen_hd(int m, const double* const (*ff_t)[2], const double* f0f, int n, int l, const int* rows,
+                           const int* cols, const double* d0, const double* d1, double tol, bool exact) {
+  double acc = 0.0;
+  double dm[kML * kML], cof[kML * kML];
+  uint64_t bits;
+  bool more = first_combination(l + 1, m, &bits);
+  while (more) {
+    const int mi = bitk(bits, 0);
+    const uint64_t cb = bits >> 1;
+    mix_rt(dm, d0, d1, l, cb);
+    double det = 1.0;
+    bool ok = true;
+    if (l > 0) {
+      if (exact)
+        det = cofactors_rt(cof, dm, l);
+      else
+        ok = cofactors_tol_rt(cof, dm, l, tol, &det);
+    }
+    if (ok) {
+      double contrib = det * f0f[mi];
+      for (int b = 0; b < l; ++b) {
+        const double* fsl = ff_t[mi][bitk(cb, b)];
+        const int64_t base = (int64_t)cols[b] * n;
+        double corr = 0.0;
+        for (int r = 0; r < l; ++r) corr += (fsl[base + rows[r]] - dm[r * l + b]) * cof[r * l + b];
+        contrib -= det + corr;
+      }
+      acc += contrib;
+    }
+    more = advance_combination(l + 1, m, &bits);
+  }
+  return acc;
+}
+
+NW_HD void combine_fs(double ph, double pa, double deta, double fa, double pb, double detb, double fb, double* F,
+                      double* S) {
+  const double sa = pa * deta, sb = pb * detb;
+  double f = 0.0;
+  if (sb != 0.0) f += pa * fa * sb;
+  if (sa != 0.0) f += pb * fb * sa;
+  *F = ph * f;
+  *S = ph * sa * sb;
+}
+
+template <int LA, int LB>
+NW_HD void eval_fs_m0_ct(const FastPair& fp, const FockPair& fk, const DetRec& x, const DetRec& w, int n, int oa,
+                         int ob, double* F, double* S) {
+  int ra[LA > 0 ? LA : 1], ca[LA > 0 ? LA : 1], rb[LB > 0 ? LB : 1], cb[LB > 0 ? LB : 1];
+  det_labels_ct<LA>(x.ra, x.ia, w.ia, oa, n, ra, ca);
+  det_labels_ct<LB>(x.rb, x.ib, w.ib, ob, n, rb, cb);
+  double deta, fa, detb, fb;
+  spin_f_ct<LA>(fk.a.recx, fk.a.recy, fk.a.f0f[0], n, ra, ca, &deta, &fa);
+  spin_f_ct<LB>(fk.b.recx, fk.b.recy, fk.b.f0f[0], n, rb, cb, &detb, &fb);
+  combine_fs(x.phase * w.phase, fp.a.pref, deta, fa, fp.b.pref, detb, fb, F, S);
+}
+
+NW_HD void eval_fs_m0_rt(const FastPair& fp, const FockPair& fk, const DetRec& x, const DetRec& w, int n, int oa,
+                         int ob, double* F, double* S) {
+  int ra[kML], ca[kML], rb[kML], cb[kML];
+  labels_rt(x, w, 0, oa, n, ra, ca);
+  labels_rt(x, w, 1, ob, n, rb, cb);
+  double deta, fa, detb, fb;
+  spin_f_rt(x.ra + w.ra, fk.a.recx, fk.a.recy, fk.a.f0f[0], n, ra, ca, &deta, &fa);
+  spin_f_rt(x.rb + w.rb, fk.b.recx, fk.b.recy, fk.b.f0f[0], n, rb, cb, &detb, &fb);
+  combine_fs(x.phase * w.phase, fp.a.pref, deta, fa, fp.b.pref, detb, fb, F, S);
+}
+
+#define NW_FS_CASE(A, B)                                       \
+  case (A) * 5 + (B):                                          \
+    eval_fs_m0_ct<A, B>(fp, fk, x, w, n, oa, ob, F, S);        \
+    return;
+
+// Rank dispatch of the m = 0 (F, S) evaluator for one pair (the kernels dispatch per class).
+NW_HD void eval_fs_m0_pair(const FastPair& fp, const FockPair& fk, const DetRec& x, const DetRec& w, int n, int oa,
+                           int ob, double* F, double* S) {
+  const int la = x.ra + w.ra, lb = x.rb + w.rb;
+  if (la <= 4 && lb <= 4) {
+    switch (la * 5 + lb) {
+      NW_FS_CASE(0, 0) NW_FS_CASE(0, 1) NW_FS_CASE(0, 2) NW_FS_CASE(0, 3) NW_FS_CASE(0, 4)
+      NW_FS_CASE(1, 0) NW_FS_CASE(1, 1) NW_FS_CASE(1, 2) NW_FS_CASE(1, 3) NW_FS_CASE(1, 4)
+      NW_FS_CASE(2, 0) NW_FS_CASE(2, 1) NW_FS_CASE(2, 2) NW_FS_CASE(2, 3) NW_FS_CASE(2, 4)
+      NW_FS_CASE(3, 0) NW_FS_CASE(3, 1) NW_FS_CASE(3, 2) NW_FS_CASE(3, 3) NW_FS_CASE(3, 4)
+      NW_FS_CASE(4, 0) NW_FS_CASE(4, 1) NW_FS_CASE(4, 2) NW_FS_CASE(4, 3) NW_FS_CASE(4, 4)
+      default: break;
+    }
+  }
+  eval_fs_m0_rt(fp, fk, x, w, n, oa, ob, F, S);
+}
+#undef NW_FS_CASE
+
+NW_HD void eval_fs_gen_pair(const GenPair& g, const FockPair& fk, const DetRec& x, const DetRec& w, int n, int oa,
+                            int ob, double tol, bool exact, double* F, double* S) {
+  const int la = x.ra + w.ra, lb = x.rb + w.rb;
+  int ra[kML], ca[kML], rb[kML], cb[kML];
+  labels_rt(x, w, 0, oa, n, ra, ca);
+  labels_rt(x, w, 1, ob, n, rb, cb);
+  double d0[kML * kML], d1[kML * kML];
+  build_d_rt(d0, g.a.x[0], g.a.y[0], n, la, ra, ca);
+  build_d_rt(d1, g.a.x[1], g.a.y[1], n, la, ra, ca);
+  const double deta = overlap_spin_hd(g.a.m, la, d0, d1);
+  const double fa = spin_f_gen_hd(g.a.m, fk.a.ff_t, fk.a.f0f, n, la, ra, ca, d0, d1, tol, exact);
+  build_d_rt(d0, g.b.x[0], g.b.y[0], n, lb, rb, cb);
+  build_d_rt(d1, g.b.x[1], g.b.y[1], n, lb, rb, cb);
+  const double detb = overlap_spin_hd(g.b.m, lb, d0, d1);
+  const double fb = spin_f_gen_hd(g.b.m, fk.b.ff_t, fk.b.f0f, n, lb, rb, cb, d0, d1, tol, exact);
+  combine_fs(x.phase * w.phase, g.a.pref, deta, fa, g.b.pref, detb, fb, F, S);
 }
 
 // ---------------------------------------------------------------------------------------

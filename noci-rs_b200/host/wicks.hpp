@@ -72,6 +72,19 @@ class WicksShared {
     check(nw_eval_hs_pairs_device(ctx_, pairs_dev, npairs, hs_dev, stream), "nw_eval_hs_pairs_device");
   }
 
+  // Fock tables from AO Fock matrices (update_wicks_fock, src/noci/wicks.rs:290-330).
+  void update_fock(const std::vector<double>& fock_a, const std::vector<double>& fock_b) {
+    check(nw_update_fock(ctx_, fock_a.data(), fock_b.data()), "nw_update_fock");
+  }
+
+  // (F, S) per pair; the SNOCI element is M = F - E0 S (calculate_m_pair_wicks, src/noci/m.rs:160-197).
+  std::vector<std::pair<double, double>> fs_pairs(const std::vector<uint32_t>& pairs, void* stream = nullptr) {
+    std::vector<std::pair<double, double>> out(pairs.size() / 2);
+    check(nw_eval_fs_pairs(ctx_, pairs.data(), pairs.size() / 2, reinterpret_cast<double*>(out.data()), stream),
+          "nw_eval_fs_pairs");
+    return out;
+  }
+
   std::vector<int32_t> zero_counts(int nref) const {
     std::vector<int32_t> m(2 * (size_t)nref * nref);
     check(nw_pair_zero_counts(ctx_, m.data()), "nw_pair_zero_counts");

@@ -59,7 +59,7 @@ class NwInfo(ctypes.Structure):
 
 EXPORTED = ("nw_ctx_create", "nw_build_intermediates", "nw_pair_zero_counts", "nw_set_basis",
             "nw_eval_hs_pairs_device", "nw_eval_hs_pairs", "nw_eval_hs_pairs_noalloc",
-            "nw_eval_s_pairs_device", "nw_sync",
+            "nw_eval_s_pairs_device", "nw_update_fock", "nw_eval_fs_pairs_device", "nw_eval_fs_pairs", "nw_sync",
             "nw_set_timing", "nw_last_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
             "nw_last_error")
 
@@ -84,6 +84,9 @@ def load(path: Optional[str] = None):
     L.nw_eval_hs_pairs.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_eval_hs_pairs_noalloc.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_eval_s_pairs_device.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
+    L.nw_update_fock.argtypes = [vp, vp, vp]
+    L.nw_eval_fs_pairs_device.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
+    L.nw_eval_fs_pairs.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_sync.argtypes = [vp, vp]
     L.nw_set_timing.argtypes = [vp, ctypes.c_int]
     L.nw_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
@@ -210,6 +213,29 @@ class WicksShared:
         self._check(self._lib.nw_eval_s_pairs_device(self._ctx, ctypes.c_void_p(pairs_ptr), npairs,
                                                      ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream)),
                     "nw_eval_s_pairs_device")
+
+    # -- Fock (F, S) path ---------------------------------------------------------------------
+    def update_fock(self, fock_a: np.ndarray, fock_b: np.ndarray):
+        """update_wicks_fock (src/noci/wicks.rs:290-330): Fock tables from AO Fock matrices."""
+        fa = np.ascontiguousarray(fock_a, dtype=np.float64)
+        fb = np.ascontiguousarray(fock_b, dtype=np.float64)
+        self._check(self._lib.nw_update_fock(self._ctx, fa.ctypes.data, fb.ctypes.data), "nw_update_fock")
+        return self
+
+    def eval_fs_pairs(self, pairs: np.ndarray, out: Optional[np.ndarray] = None, stream: int = 0):
+        """(F, S) for host pairs (n, 2) -> host array (n, 2); M = F - E0 S is the SNOCI element."""
+        pairs = np.ascontiguousarray(pairs, dtype=np.uint32)
+        n = pairs.shape[0]
+        if out is None:
+            out = np.empty((n, 2), np.float64)
+        self._check(self._lib.nw_eval_fs_pairs(self._ctx, pairs.ctypes.data, n, out.ctypes.data,
+                                               ctypes.c_void_p(stream)), "nw_eval_fs_pairs")
+        return out
+
+    def eval_fs_pairs_device(self, pairs_ptr: int, npairs: int, out_ptr: int, stream: int = 0):
+        self._check(self._lib.nw_eval_fs_pairs_device(self._ctx, ctypes.c_void_p(pairs_ptr), npairs,
+                                                      ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream)),
+                    "nw_eval_fs_pairs_device")
 
     def set_timing(self, enable: bool = True):
         self._check(self._lib.nw_set_timing(self._ctx, 1 if enable else 0), "nw_set_timing")

@@ -204,6 +204,47 @@ void mir_eval_s_gen(const double* slab, const int64_t* offs, const double* vals,
   }
 }
 
+// (F, S) on the fast layout: Fock records {X0|Y0, F^(00)} interleaved, F_0^(0) and pref per spin.
+void mir_eval_fs_fast(const double* frecx_a, const double* frecy_a, double f0_a, double pref_a, const double* frecx_b,
+                      const double* frecy_b, double f0_b, double pref_b, int n, int oa, int ob, const void* dets,
+                      const uint32_t* pairs, int64_t npairs, double* fs) {
+  FastPair fp;
+  std::memset(&fp, 0, sizeof(fp));
+  fp.a.pref = pref_a;
+  fp.b.pref = pref_b;
+  FockPair fk;
+  std::memset(&fk, 0, sizeof(fk));
+  fk.a.recx = reinterpret_cast<const double2*>(frecx_a);
+  fk.a.recy = reinterpret_cast<const double2*>(frecy_a);
+  fk.a.f0f[0] = f0_a;
+  fk.b.recx = reinterpret_cast<const double2*>(frecx_b);
+  fk.b.recy = reinterpret_cast<const double2*>(frecy_b);
+  fk.b.f0f[0] = f0_b;
+  for (int64_t i = 0; i < npairs; ++i) {
+    const DetRec x = rec_at(dets, pairs[2 * i]), w = rec_at(dets, pairs[2 * i + 1]);
+    eval_fs_m0_pair(fp, fk, x, w, n, oa, ob, &fs[2 * i], &fs[2 * i + 1]);
+  }
+}
+
+// (F, S) on the reference-ordered layout: ff_t[spin][mi*2+mj] transposed Fock columns.
+void mir_eval_fs_gen(const double* slab, const int64_t* offs, const double* vals, const int32_t* ints,
+                     const double* fslab, const int64_t* foffs, const double* fvals, int n, int oa, int ob, double tol,
+                     int exact, const void* dets, const uint32_t* pairs, int64_t npairs, double* fs) {
+  const GenPair g = gen_from_oracle(slab, offs, vals, ints);
+  FockPair fk;
+  std::memset(&fk, 0, sizeof(fk));
+  FockSpinTab* t[2] = {&fk.a, &fk.b};
+  for (int sp = 0; sp < 2; ++sp) {
+    for (int k = 0; k < 4; ++k) t[sp]->ff_t[k >> 1][k & 1] = fslab + foffs[sp * 4 + k];
+    t[sp]->f0f[0] = fvals[sp * 2];
+    t[sp]->f0f[1] = fvals[sp * 2 + 1];
+  }
+  for (int64_t i = 0; i < npairs; ++i) {
+    const DetRec x = rec_at(dets, pairs[2 * i]), w = rec_at(dets, pairs[2 * i + 1]);
+    eval_fs_gen_pair(g, fk, x, w, n, oa, ob, tol, exact != 0, &fs[2 * i], &fs[2 * i + 1]);
+  }
+}
+
 void mir_layout(int which, const double* td, const double* te, int64_t n, double* out) {
   const int64_t n4 = n * n * n * n;
   for (int64_t idx = 0; idx < n4; ++idx) {

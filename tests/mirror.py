@@ -39,6 +39,10 @@ def lib():
                                    ctypes.c_double, ctypes.c_int, VP, U32, ctypes.c_int64, D]
         L.mir_eval_s_gen.argtypes = [D, I64, D, I32, ctypes.c_int, ctypes.c_int, ctypes.c_int, VP, U32,
                                      ctypes.c_int64, D]
+        L.mir_eval_fs_fast.argtypes = [D, D, ctypes.c_double, ctypes.c_double, D, D, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, VP, U32, ctypes.c_int64, D]
+        L.mir_eval_fs_gen.argtypes = [D, I64, D, I32, D, I64, D, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_double, ctypes.c_int, VP, U32, ctypes.c_int64, D]
         L.mir_layout.argtypes = [ctypes.c_int, D, D, ctypes.c_int64, D]
         _lib = L
     return _lib
@@ -119,3 +123,37 @@ def layout(which, td, te=None):
     out = np.empty(n ** 4)
     lib().mir_layout(which, p(td, ctypes.c_double), p(te, ctypes.c_double), n, p(out, ctypes.c_double))
     return out.reshape(n, n, n, n)
+
+
+def eval_fs_fast(orc, build, pidx, n, oa, ob, dets, pairs):
+    """(F, S) of one fast ordered pair through the device code, from the oracle's Fock tables."""
+    pairs = np.ascontiguousarray(pairs, dtype=np.uint32)
+    fs = np.empty(2 * pairs.shape[0])
+    recs = []
+    for sp, ss in enumerate((build.aa, build.bb)):
+        ff00 = orc.fslab[orc.foffs[pidx, sp, 0]:orc.foffs[pidx, sp, 0] + n * n].reshape(n, n).T
+        rx = np.ascontiguousarray(np.stack([ss.x[0], ff00], axis=-1))
+        ry = np.ascontiguousarray(np.stack([ss.y[0], ff00], axis=-1))
+        recs.append((rx, ry, float(orc.fvals[pidx, sp, 0]), ss.phase * ss.tilde_s_prod))
+    (rxa, rya, fa, pa), (rxb, ryb, fb, pb) = recs
+    lib().mir_eval_fs_fast(p(rxa, ctypes.c_double), p(rya, ctypes.c_double), fa, pa, p(rxb, ctypes.c_double),
+                           p(ryb, ctypes.c_double), fb, pb, n, oa, ob, dets.ctypes.data_as(VP),
+                           p(pairs, ctypes.c_uint32), pairs.shape[0], p(fs, ctypes.c_double))
+    return fs[0::2], fs[1::2]
+
+
+def eval_fs_gen(orc, pidx, n, oa, ob, dets, pairs, exact=False):
+    """(F, S) of one ordered pair with zero-overlap orbitals through the device code."""
+    pairs = np.ascontiguousarray(pairs, dtype=np.uint32)
+    fs = np.empty(2 * pairs.shape[0])
+    offs = np.ascontiguousarray(orc.offs[pidx])
+    vals = np.ascontiguousarray(orc.vals[pidx])
+    ints = np.ascontiguousarray(orc.ints[pidx])
+    foffs = np.ascontiguousarray(orc.foffs[pidx].reshape(-1))
+    fvals = np.ascontiguousarray(orc.fvals[pidx].reshape(-1))
+    lib().mir_eval_fs_gen(p(orc.slab, ctypes.c_double), p(offs, ctypes.c_int64), p(vals, ctypes.c_double),
+                          p(ints, ctypes.c_int32), p(orc.fslab, ctypes.c_double), p(foffs, ctypes.c_int64),
+                          p(fvals, ctypes.c_double), n, oa, ob, orc.tol, 1 if exact else 0,
+                          dets.ctypes.data_as(VP), p(pairs, ctypes.c_uint32), pairs.shape[0],
+                          p(fs, ctypes.c_double))
+    return fs[0::2], fs[1::2]

@@ -179,3 +179,32 @@ def test_sort_keys_group_classes_and_bras(setup, cap):
     # far same-parent pairs are exactly the skipped ones
     same = par[pairs[:, 0]] == par[pairs[:, 1]]
     assert np.all(same[~live])
+
+
+def test_fock_evaluators_match_oracle(setup):
+    """(F, S) device code (fast records and the m > 0 distribution sum) against the oracle's
+    calculate_m_pair_wicks restatement, all contraction ranks up to 4 + 4."""
+    n, o, system, orc, basis, ob = setup
+    rng = np.random.default_rng(7)
+    a = rng.normal(0.0, 0.3, (n, n))
+    fa = 0.5 * (a + a.T) + system.h
+    b = rng.normal(0.0, 0.3, (n, n))
+    fb = 0.5 * (b + b.T) + system.h
+    orc.set_fock(fa, fb)
+    par = basis["parent"].astype(int)
+    for x in range(3):
+        for w in range(3):
+            pid = x * 3 + w
+            bld = orc.builds[pid]
+            ia = np.nonzero(par == x)[0]
+            iw = np.nonzero(par == w)[0]
+            pairs = np.stack([rng.choice(ia, 300), rng.choice(iw, 300)], 1)
+            if bld.aa.m == 0 and bld.bb.m == 0:
+                _, f_ref, s_ref = orc.eval_m_pairs(ob, pairs, 0.0)
+                f, s = MR.eval_fs_fast(orc, bld, pid, n, o, o, basis, pairs)
+                assert np.max(np.abs(f - f_ref)) < TIGHT and np.max(np.abs(s - s_ref)) < TIGHT
+            else:
+                for exact in (False, True):
+                    _, f_ref, s_ref = orc.eval_m_pairs(ob, pairs, 0.0, exact=exact)
+                    f, s = MR.eval_fs_gen(orc, pid, n, o, o, basis, pairs, exact=exact)
+                    assert np.max(np.abs(f - f_ref)) < TIGHT and np.max(np.abs(s - s_ref)) < TIGHT
