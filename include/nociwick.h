@@ -176,6 +176,27 @@ NW_API nw_status nw_eval_fs_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev,
 NW_API nw_status nw_eval_fs_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* fs_host,
                                   void* stream);
 
+/* Dense (H, S) matrices of a block of the resident basis: h_out[i*nr + j] = H(left[i], right[j]),
+ * likewise s_out (host, row-major nl x nr).  With symmetric != 0 (nl == nr) only j >= i is
+ * evaluated and mirrored.  Pairs are generated and evaluated on the device in row blocks.
+ * Replaces build_noci_hs with calculate_matrix_elements / scatter_matrix_elements
+ * (src/noci/matrix.rs:39-110). */
+NW_API nw_status nw_build_hs_matrix(nw_ctx* ctx, const uint32_t* left, uint64_t nl, const uint32_t* right,
+                                    uint64_t nr, int symmetric, double* h_out, double* s_out);
+
+/* The same for (F, S) after nw_update_fock.  Replaces build_noci_fock (src/noci/matrix.rs:124-175). */
+NW_API nw_status nw_build_fs_matrix(nw_ctx* ctx, const uint32_t* left, uint64_t nl, const uint32_t* right,
+                                    uint64_t nr, int symmetric, double* f_out, double* s_out);
+
+/* Generalised eigenproblem H C = S C e in FP64 on the GPU (host row-major n x n inputs; only
+ * the lower triangles enter the eigensolves, the full H enters X^T H X).  With project != 0 the
+ * orthogonaliser is X = U_+ diag(lambda_+^-1/2) over the overlap eigenvalues > tol, else
+ * X = U diag(lambda^-1/2) U^T.  Writes nkept = k eigenvalues (ascending) to evals and the
+ * row-major n x k eigenvectors C = X U to c (room for n*n doubles).
+ * Replaces general_evp / loewdin_x / positive_subspace (src/maths/linalg.rs:180-256). */
+NW_API nw_status nw_general_evp(nw_ctx* ctx, int32_t n, const double* h, const double* s, int project, double tol,
+                                double* evals, double* c, int32_t* nkept);
+
 /* Wait for the work queued on `stream` and report pair indices that were out of range in an
  * earlier device-buffer call (those outputs are NaN). */
 NW_API nw_status nw_sync(nw_ctx* ctx, void* stream);

@@ -337,6 +337,31 @@ nw_status nw_eval_fs_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npa
   return eval_host(ctx, nw::EvalMode::kFS, pairs_host, npairs, fs_host, stream);
 }
 
+nw_status nw_build_hs_matrix(nw_ctx* ctx, const uint32_t* left, uint64_t nl, const uint32_t* right, uint64_t nr,
+                             int symmetric, double* h_out, double* s_out) {
+  if (!ctx || (nl && !left) || (nr && !right) || (nl && nr && (!h_out || !s_out))) return NW_ERR_INVALID;
+  return nw::build_matrix(ctx, nw::EvalMode::kHS, left, nl, right, nr, symmetric != 0, h_out, s_out);
+}
+
+nw_status nw_build_fs_matrix(nw_ctx* ctx, const uint32_t* left, uint64_t nl, const uint32_t* right, uint64_t nr,
+                             int symmetric, double* f_out, double* s_out) {
+  if (!ctx || (nl && !left) || (nr && !right) || (nl && nr && (!f_out || !s_out))) return NW_ERR_INVALID;
+  if (!ctx->fock_ready) return nw::fail(ctx, NW_ERR_STATE, "Fock tables not set (nw_update_fock)");
+  return nw::build_matrix(ctx, nw::EvalMode::kFS, left, nl, right, nr, symmetric != 0, f_out, s_out);
+}
+
+nw_status nw_general_evp(nw_ctx* ctx, int32_t n, const double* h, const double* s, int project, double tol,
+                         double* evals, double* c, int32_t* nkept) {
+  if (!ctx || n <= 0 || !h || !s || !evals || !c || !nkept) return NW_ERR_INVALID;
+  if (!(tol >= 0.0) || !std::isfinite(tol)) return NW_ERR_INVALID;
+  const size_t n2 = (size_t)n * n;
+  if (!finite_all(h, n2) || !finite_all(s, n2)) return nw::fail(ctx, NW_ERR_INVALID, "non-finite matrix entry");
+  int k = 0;
+  const nw_status st = nw::general_evp(ctx, n, h, s, project != 0, tol, evals, c, &k);
+  *nkept = k;
+  return st;
+}
+
 nw_status nw_sync(nw_ctx* ctx, void* stream) {
   if (!ctx) return NW_ERR_INVALID;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -411,6 +436,7 @@ nw_status nw_ctx_destroy(nw_ctx* ctx) {
   for (cudaEvent_t e : {ctx->ev_start, ctx->ev_in[0], ctx->ev_in[1], ctx->ev_comp[0], ctx->ev_comp[1]})
     if (e) cudaEventDestroy(e);
   if (ctx->blas) cublasDestroy(ctx->blas);
+  if (ctx->solver) cusolverDnDestroy(ctx->solver);
   delete ctx;
   return NW_OK;
 }

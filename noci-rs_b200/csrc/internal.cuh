@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 #include <cublas_v2.h>
+#include <cusolverDn.h>
 #include <stdint.h>
 
 #include <string>
@@ -94,6 +95,7 @@ struct nw_ctx {
   std::vector<char> generic_host;  // per ordered pair: m_alpha + m_beta > 0
 
   cublasHandle_t blas = nullptr;
+  cusolverDnHandle_t solver = nullptr;  // created by the first generalised eigensolve
   std::string last_error;
 
   // optional per-phase timing of the evaluation pipeline
@@ -125,6 +127,12 @@ enum class EvalMode { kHS, kS, kFS };
 // clear_flag = false keeps the out-of-range flag of earlier calls (chunked host path).
 nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, EvalMode mode,
                      cudaStream_t stream, bool clear_flag = true);
+// Dense matrices over left x right determinant blocks and the generalised eigenproblem (matrix.cu).
+nw_status build_matrix(nw_ctx* ctx, EvalMode mode, const uint32_t* left, uint64_t nl, const uint32_t* right,
+                       uint64_t nr, bool symmetric, double* a_host, double* s_host);
+nw_status general_evp(nw_ctx* ctx, int n, const double* h, const double* s, bool project, double tol, double* evals,
+                      double* c, int* nkept);
+
 // Same evaluation with its scratch in a fixed device array (no device allocation).
 nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, cudaStream_t stream);
 

@@ -59,7 +59,8 @@ class NwInfo(ctypes.Structure):
 
 EXPORTED = ("nw_ctx_create", "nw_build_intermediates", "nw_pair_zero_counts", "nw_set_basis",
             "nw_eval_hs_pairs_device", "nw_eval_hs_pairs", "nw_eval_hs_pairs_noalloc",
-            "nw_eval_s_pairs_device", "nw_update_fock", "nw_eval_fs_pairs_device", "nw_eval_fs_pairs", "nw_sync",
+            "nw_eval_s_pairs_device", "nw_update_fock", "nw_eval_fs_pairs_device", "nw_eval_fs_pairs",
+            "nw_build_hs_matrix", "nw_build_fs_matrix", "nw_general_evp", "nw_sync",
             "nw_set_timing", "nw_last_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
             "nw_last_error")
 
@@ -87,6 +88,10 @@ def load(path: Optional[str] = None):
     L.nw_update_fock.argtypes = [vp, vp, vp]
     L.nw_eval_fs_pairs_device.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_eval_fs_pairs.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
+    L.nw_build_hs_matrix.argtypes = [vp, vp, ctypes.c_uint64, vp, ctypes.c_uint64, ctypes.c_int, vp, vp]
+    L.nw_build_fs_matrix.argtypes = [vp, vp, ctypes.c_uint64, vp, ctypes.c_uint64, ctypes.c_int, vp, vp]
+    L.nw_general_evp.argtypes = [vp, ctypes.c_int32, vp, vp, ctypes.c_int, ctypes.c_double, vp, vp,
+                                 ctypes.POINTER(ctypes.c_int32)]
     L.nw_sync.argtypes = [vp, vp]
     L.nw_set_timing.argtypes = [vp, ctypes.c_int]
     L.nw_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
@@ -236,6 +241,39 @@ class WicksShared:
         self._check(self._lib.nw_eval_fs_pairs_device(self._ctx, ctypes.c_void_p(pairs_ptr), npairs,
                                                       ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream)),
                     "nw_eval_fs_pairs_device")
+
+    # -- dense matrices and the generalised eigenproblem ------------------------------------
+    def _matrix(self, fn, where, left, right, symmetric):
+        nd = self.info()["ndet"]
+        left = np.arange(nd, dtype=np.uint32) if left is None else np.ascontiguousarray(left, dtype=np.uint32)
+        right = left if right is None else np.ascontiguousarray(right, dtype=np.uint32)
+        a = np.empty((left.shape[0], right.shape[0]))
+        s = np.empty_like(a)
+        self._check(fn(self._ctx, left.ctypes.data, left.shape[0], right.ctypes.data, right.shape[0],
+                       1 if symmetric else 0, a.ctypes.data, s.ctypes.data), where)
+        return a, s
+
+    def build_hs_matrix(self, left=None, right=None, symmetric: bool = True):
+        """build_noci_hs (src/noci/matrix.rs): dense H and S over a block of the resident basis
+        (default: the whole basis, symmetric)."""
+        return self._matrix(self._lib.nw_build_hs_matrix, "nw_build_hs_matrix", left, right, symmetric)
+
+    def build_fs_matrix(self, left=None, right=None, symmetric: bool = True):
+        """build_noci_fock (src/noci/matrix.rs): dense F and S after update_fock."""
+        return self._matrix(self._lib.nw_build_fs_matrix, "nw_build_fs_matrix", left, right, symmetric)
+
+    def general_evp(self, h: np.ndarray, s: np.ndarray, project: bool = True, tol: float = 1e-8):
+        """general_evp (src/maths/linalg.rs:230-256) on the GPU: (eigenvalues, eigenvectors C)."""
+        h = np.ascontiguousarray(h, dtype=np.float64)
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        n = h.shape[0]
+        evals = np.empty(n)
+        c = np.empty(n * n)
+        k = ctypes.c_int32()
+        self._check(self._lib.nw_general_evp(self._ctx, n, h.ctypes.data, s.ctypes.data, 1 if project else 0, tol,
+                                             evals.ctypes.data, c.ctypes.data, ctypes.byref(k)), "nw_general_evp")
+        k = k.value
+        return evals[:k].copy(), c[:n * k].reshape(n, k).copy()
 
     def set_timing(self, enable: bool = True):
         self._check(self._lib.nw_set_timing(self._ctx, 1 if enable else 0), "nw_set_timing")

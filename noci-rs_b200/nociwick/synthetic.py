@@ -285,6 +285,12 @@ def sample_pairs_by_rank(basis: np.ndarray, npairs: int, seed: int,
     return out
 
 
+def config1_system(seed: int = 1) -> System:
+    """Linear-H2/cc-pVDZ stand-in (n = 10, 1 + 1 electrons, RHF-like + two spin-polarised
+    references, E_nuc of H2 at 1.5 Angstrom); the basis is the three references."""
+    return make_system(10, 1, 1, 3, 40, seed, k_scale=0.75, uhf_like=True, enuc=0.35275)
+
+
 def config2_system(seed: int = 2) -> System:
     """Stand-in for linear H6/cc-pVDZ: n = 30, 3 alpha + 3 beta electrons, RHF + 2 UHF refs."""
     return make_system(30, 3, 3, 3, 120, seed, k_scale=0.08, uhf_like=True, enuc=0.0)
