@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--npairs", type=int, default=10_000_000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-qmc", action="store_true", help="skip the NOCI-QMC steps/s leg")
+    ap.add_argument("--qmc-reports", type=int, default=30, help="timed QMC report blocks (10 steps each)")
     return ap.parse_args()
 
 
@@ -229,6 +231,81 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def qmc_leg(args, rank, world, local_rank, dist):
+    """QMC steps/s on the H8/cc-pVDZ NOCISD(3)-QMC stand-in (n = 40, 4 + 4 electrons, three
+    references, 85755 determinants): 10^6 walkers, dt = 1e-3, uniform generator, 10 steps per
+    report block, the whole block on the device (one CUDA graph).  A step is one cycle: sample,
+    spawn, (H, S) of every attempt, rounding, accumulation."""
+    import torch
+    import nociwick
+    from nociwick import synthetic as sy
+    system = sy.config4_system()
+    basis = sy.sd_basis(40, 4, 4, 3)
+    nd = basis.shape[0]
+    w = nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8,
+                             device=local_rank).build()
+    w.set_basis(basis)
+    refs = np.nonzero((basis["rank_a"] == 0) & (basis["rank_b"] == 0))[0].astype(np.uint32)
+    hr, sr = w.build_hs_matrix(refs, refs)
+    er, cr = w.general_evp(hr, sr, project=True, tol=1e-8)
+    c0 = np.zeros(nd)
+    c0[refs] = cr[:, 0]
+    walkers = 1e6
+    # population control from the first block (initial = target population), started at the
+    # reference-space NOCI energy; strong damping holds the 1-norm near 10^6 walkers
+    q = nociwick.Qmc(w, c0, refs, dt=1e-3, initial_population=walkers, target_population=walkers,
+                     shift_damping=0.5, initial_shift=float(er[0]), ncycles=10, propagator="unshifted",
+                     seed=rank_seed(4242, rank), max_attempts=48_000_000)
+    # equilibration: 40 report blocks (400 steps) bring the walkers from the three references
+    # to a steady 1-norm near 10^6 over the whole space before the timed blocks
+    q.run(40)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    rep = q.run(args.qmc_reports)
+    ms = q.last_run_ms()
+    (ms,) = reduce_max([ms], dist, f"cuda:{local_rank}")
+    steps = args.qmc_reports * 10
+    out = {"metric": "QMC steps/s", "value": steps / (ms / 1e3),
+           "unit": "steps/s", "ms_per_step": ms / steps, "n_gpus": world,
+           "scaling": "replicas" if world > 1 else None,
+           "config": {"workload": "H8/cc-pVDZ NOCISD(3)-QMC stand-in: n=40, 4a+4b electrons, RHF+2 UHF refs, "
+                                  "85755 SD determinants", "walkers": walkers, "dt": 1e-3, "ncycles": 10,
+                      "generator": "uniform", "propagator": "unshifted", "shift_damping": 0.5, "ndet": int(nd)},
+           "walkers_mean": float(rep["nw"].mean()),
+           "attempts_per_step": float(rep["nattempts"].mean() / 10),
+           "eproj_last": float(rep["eproj_num"][-1] / rep["eproj_den"][-1]), "shift_last": float(rep["shift"][-1]),
+           "timing": "CUDA events around the graph launches of the timed report blocks (max over ranks)"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = qmc_cpu_baseline(system, basis, c0, refs, q, float(rep["shift"][-1]))
+    q.close()
+    w.close()
+    return out
+
+
+def qmc_cpu_baseline(system, basis, c0, refs, q, shift):
+    """The CPU restatement of the same propagation (oracle/qmc.py: numpy plus the oracle's C++
+    pair evaluator on all host cores), timed over two cycles started from the GPU run's
+    populations and shift."""
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import Oracle
+    from oracle.qmc import OracleQmc
+    cores = os.cpu_count() or 1
+    orc = Oracle.from_system(system, tol=1e-8, with_mo_cache=False)
+    ob = orc.oracle_basis(basis)
+    cq = OracleQmc(orc, ob, c0, refs, dt=1e-3, initial_population=1e6, target_population=1e6, shift_damping=0.05,
+                   initial_shift=shift, ncycles=10, propagator="unshifted", seed=9, nthreads=cores)
+    cq.pop = q.populations()
+    ncyc = 2
+    t0 = time.perf_counter()
+    for _ in range(ncyc):
+        cq.cycle_delta()
+    dt = time.perf_counter() - t0
+    return {"value": ncyc / dt, "unit": "steps/s", "cores": cores, "kind": "port",
+            "sample": f"{ncyc} cycles from the GPU run's populations ({cq.attempts / ncyc:.0f} attempts per step), "
+                      f"numpy restatement of walkers.rs with the C++ FP64 pair evaluator, {cores} threads"}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import nociwick
@@ -307,6 +384,10 @@ def run_ours(args, rank, world, local_rank):
     barrier()
     t_e2e = ev2.elapsed_time(ev3)
     t_dev, t_e2e = reduce_max([t_dev, t_e2e], dist, f"cuda:{local_rank}")
+    hs_host = dout.cpu().numpy() if rank == 0 and world == 1 and not args.no_cpu_baseline else None
+    eng.close()
+    # every rank runs the QMC leg (it has collectives); rank 0 reports
+    qmc = None if args.no_qmc else qmc_leg(args, rank, world, local_rank, dist)
     if rank != 0:
         return
     value = aggregate_rate(npairs, world, args.steps, t_dev)
@@ -336,10 +417,11 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks,
         "gpu_launches": kernels_per_step * args.steps,
     }
-    if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(system, basis, pairs, args.cpu_seconds, gpu_hs=dout.cpu().numpy())
+    if qmc is not None:
+        line["qmc"] = qmc
+    if hs_host is not None:
+        line["cpu_baseline"] = cpu_baseline(system, basis, pairs, args.cpu_seconds, gpu_hs=hs_host)
     print(json.dumps(line), flush=True)
-    eng.close()
 
 
 def main():

@@ -197,6 +197,77 @@ NW_API nw_status nw_build_fs_matrix(nw_ctx* ctx, const uint32_t* left, uint64_t 
 NW_API nw_status nw_general_evp(nw_ctx* ctx, int32_t n, const double* h, const double* s, int project, double tol,
                                 double* evals, double* c, int32_t* nkept);
 
+/* ---------------------------------------------------------------------------------------
+ * NOCI-QMC on the GPU: signed real walkers over the resident basis, uniform excitation
+ * generator, FRI sampling and spawn rounding, shift control.  The whole report block (ncycles
+ * cycles of sample -> spawn -> (H, S) of every attempt -> rounding -> accumulation, then the
+ * population update, statistics and shift update) runs on the device and is replayed as one
+ * CUDA graph, with no host synchronisation inside a run.
+ * Replaces qmc_step for the signed-walker propagators (src/stochastic/walkers.rs:101-441) with
+ * propagate_iteration (src/stochastic/metric.rs:378-473), spawning / resolve_batched_spawning
+ * with the uniform generator (src/stochastic/state.rs:537-726), sample_populations / fri
+ * (metric.rs:579-699) and update_shift (metric.rs:729-751).  Random numbers come from a
+ * counter-based Philox4x32-10 stream per (seed, cycle, index), so runs are reproducible for a
+ * given seed but are not the reference's SmallRng sequence.
+ * --------------------------------------------------------------------------------------- */
+typedef enum nw_propagator {
+    NW_PROP_UNSHIFTED = 0,       /* U = 1 - dt (H - E_s S)                      */
+    NW_PROP_SHIFTED = 1,         /* U = (1 + dt E_s) - dt (H - E_s S)           */
+    NW_PROP_DOUBLY_SHIFTED = 2,  /* as SHIFTED with E_s = E_s^S (the default)   */
+    NW_PROP_DDS_U1 = 3,          /* difference doubly shifted, variant 1        */
+    NW_PROP_DDS_U2 = 4           /* difference doubly shifted, variant 2        */
+} nw_propagator;
+
+typedef struct nw_qmc_opts {
+    double dt;                  /* imaginary time step                                       */
+    double initial_population;  /* 1-norm of the initial populations (scaled c0)             */
+    double target_population;   /* 1-norm from which on the shift is updated                 */
+    double sampling_cutoff;     /* FRI cutoff of the sampled populations (0: exact sampling) */
+    double spawn_cutoff;        /* FRI cutoff of spawned amplitudes (0: none)                 */
+    double shift_damping;       /* shift damping factor                                       */
+    double initial_shift;       /* E_s at the start (noci-rs uses the first reference energy) */
+    int32_t ncycles;            /* cycles per report block                                    */
+    int32_t propagator;         /* nw_propagator                                              */
+    uint64_t seed;
+    uint64_t max_attempts;      /* spawning attempts one cycle can hold (0: 16 x the larger of
+                                   the target and initial populations + 2 ndet + 2^20)        */
+} nw_qmc_opts;
+
+typedef struct nw_qmc_report {
+    double shift;               /* E_s after the block's update                               */
+    double eproj_num;           /* projected energy = eproj_num / eproj_den                   */
+    double eproj_den;
+    double nw;                  /* 1-norm of the populations after the block                  */
+    double nref;                /* 1-norm on the reference determinants                       */
+    double sampled_norm;        /* 1-norm of the last cycle's sampled populations             */
+    uint64_t nocc;              /* determinants with a non-zero sampled population            */
+    uint64_t nattempts;         /* spawning attempts in the block                             */
+} nw_qmc_report;
+
+typedef struct nw_qmc nw_qmc;
+
+/* Set up a run over the resident basis: diagonal (H, S), the projected-energy couplings
+ * sum_i c0_i (H_iw, S_iw) over the reference determinants ref_idx, and the initial populations
+ * initial_population * c0 / |c0|_1 (c0 has one entry per determinant).
+ * Replaces the setup of qmc_step (walkers.rs:101-330) and initialise_populations (walkers.rs:27-48). */
+NW_API nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, const uint32_t* ref_idx,
+                               uint64_t nref_idx, nw_qmc** out);
+/* Run nreports report blocks; reports[k] receives block k's statistics (host array).
+ * NW_ERR_UNSUPPORTED if a cycle needed more spawning attempts than max_attempts. */
+NW_API nw_status nw_qmc_run(nw_qmc* q, int32_t nreports, nw_qmc_report* reports);
+/* Replace the current shift E_s (restart, or an equilibration estimate). */
+NW_API nw_status nw_qmc_set_shift(nw_qmc* q, double shift);
+/* Device time of the report blocks of the last nw_qmc_run (CUDA events around the graph
+ * launches on the run's stream), in milliseconds. */
+NW_API nw_status nw_qmc_last_run_ms(const nw_qmc* q, float* ms);
+/* Current populations (one per determinant), and replacing them (restart). */
+NW_API nw_status nw_qmc_populations(nw_qmc* q, double* populations);
+NW_API nw_status nw_qmc_set_populations(nw_qmc* q, const double* populations);
+/* One cycle's population change from the current populations without applying it (for checks
+ * of the estimator): delta = -dt (H - E^S S - E^I) sampled populations, stochastically. */
+NW_API nw_status nw_qmc_cycle_delta(nw_qmc* q, uint64_t cycle, double* delta);
+NW_API nw_status nw_qmc_destroy(nw_qmc* q);
+
 /* Wait for the work queued on `stream` and report pair indices that were out of range in an
  * earlier device-buffer call (those outputs are NaN). */
 NW_API nw_status nw_sync(nw_ctx* ctx, void* stream);

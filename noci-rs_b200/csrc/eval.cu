@@ -70,10 +70,11 @@ __device__ __forceinline__ uint32_t classify_one(const EvalParams& P, uint2 ab, 
 constexpr int kSortUnroll = 4;
 
 __global__ void __launch_bounds__(256) classify_kernel(EvalParams P, const uint32_t* __restrict__ pairs,
-                                                       uint64_t npairs, uint32_t* __restrict__ keys,
-                                                       uint32_t* __restrict__ ranks, uint32_t* __restrict__ counts,
-                                                       double* __restrict__ out, int out_stride,
-                                                       uint32_t* __restrict__ flag) {
+                                                       uint64_t npairs, const uint32_t* __restrict__ npairs_dev,
+                                                       uint32_t* __restrict__ keys, uint32_t* __restrict__ ranks,
+                                                       uint32_t* __restrict__ counts, double* __restrict__ out,
+                                                       int out_stride, uint32_t* __restrict__ flag) {
+  if (npairs_dev) npairs = min(npairs, (uint64_t)*npairs_dev);
   const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i0 < npairs; i0 += kSortUnroll * nthreads) {
     uint2 ab[kSortUnroll];
@@ -188,8 +189,10 @@ __global__ void __launch_bounds__(kScanThreads) scan_down_kernel(const uint32_t*
 // pair itself through that index: one random 4-byte write here instead of 12).
 __global__ void __launch_bounds__(256) scatter_kernel(const uint32_t* __restrict__ keys,
                                                       const uint32_t* __restrict__ ranks, uint64_t npairs,
+                                                      const uint32_t* __restrict__ npairs_dev,
                                                       const uint32_t* __restrict__ offsets,
                                                       uint32_t* __restrict__ sidx) {
+  if (npairs_dev) npairs = min(npairs, (uint64_t)*npairs_dev);
   const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i0 < npairs; i0 += kSortUnroll * nthreads) {
     uint32_t k[kSortUnroll], r[kSortUnroll], o[kSortUnroll];
@@ -444,6 +447,8 @@ inline int grid_stride_blocks(uint64_t work, int block, int per_sm) {
   return (int)g;
 }
 
+}  // namespace
+
 EvalParams make_params(const nw_ctx* ctx) {
   EvalParams P;
   P.dets = ctx->d_dets;
@@ -466,21 +471,9 @@ EvalParams make_params(const nw_ctx* ctx) {
   return P;
 }
 
-// Device scratch of one sorted evaluation.
-struct SortScratch {
-  uint32_t* keys;     // npairs
-  uint32_t* ranks;    // npairs
-  uint32_t* sidx;     // npairs
-  uint32_t* counts;   // nkeys
-  uint32_t* offsets;  // nkeys + 1
-  uint32_t* tsum;     // nkeys / kScanTile + 1
-  uint32_t* flag;
-};
 
 // Fine-key budget: at most kFineMax counters, and at most about one per pair of the request so
 // the counter memset and scan stay small next to the evaluation.
-constexpr uint64_t kFineMax = 1ull << 23;
-constexpr uint64_t kFineMin = 1ull << 14;
 
 // Number of sort keys for this request with at most `cap` counters for the fast classes;
 // fills P.nbucket / P.shift.
@@ -492,14 +485,24 @@ uint64_t plan_keys(const nw_ctx* ctx, EvalParams& P, uint64_t cap) {
   return (uint64_t)kClasses * nb + (uint64_t)kClasses * ngen;
 }
 
+nw_status scan_exclusive(nw_ctx* ctx, const uint32_t* counts, uint64_t n, uint32_t* offsets, uint32_t* tsum,
+                         cudaStream_t stream) {
+  const int ntiles = (int)(n / kScanTile + 1);
+  scan_tiles_kernel<<<ntiles, kScanThreads, 0, stream>>>(counts, (uint32_t)n, tsum);
+  scan_top_kernel<<<1, kScanThreads, 0, stream>>>(tsum, ntiles);
+  scan_down_kernel<<<ntiles, kScanThreads, 0, stream>>>(counts, (uint32_t)n, tsum, offsets);
+  NW_CUDA(ctx, cudaGetLastError());
+  return NW_OK;
+}
+
 // classify -> scan -> scatter -> evaluate, all on `stream`.  The flag must already be cleared
 // (or hold earlier calls' reports); ev (six events or null) brackets the phases.
 nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const uint32_t* pairs, uint64_t npairs,
-                        double* out, const SortScratch& S, cudaStream_t stream, cudaEvent_t* ev,
-                        EvalMode mode = EvalMode::kHS) {
+                        double* out, const SortScratch& S, cudaStream_t stream, cudaEvent_t* ev, EvalMode mode,
+                        const uint32_t* npairs_dev) {
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[0], stream));
   NW_CUDA(ctx, cudaMemsetAsync(S.counts, 0, sizeof(uint32_t) * nkeys, stream));
-  classify_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(P, pairs, npairs, S.keys, S.ranks,
+  classify_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(P, pairs, npairs, npairs_dev, S.keys, S.ranks,
                                                                           S.counts, out, 2, S.flag);
   NW_CUDA(ctx, cudaGetLastError());
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[1], stream));
@@ -509,7 +512,8 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
   scan_down_kernel<<<ntiles, kScanThreads, 0, stream>>>(S.counts, (uint32_t)nkeys, S.tsum, S.offsets);
   NW_CUDA(ctx, cudaGetLastError());
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[2], stream));
-  scatter_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(S.keys, S.ranks, npairs, S.offsets, S.sidx);
+  scatter_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(S.keys, S.ranks, npairs, npairs_dev,
+                                                                         S.offsets, S.sidx);
   NW_CUDA(ctx, cudaGetLastError());
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[3], stream));
   const uint2* pp = reinterpret_cast<const uint2*>(pairs);
@@ -537,7 +541,6 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
   return NW_OK;
 }
 
-}  // namespace
 
 nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, EvalMode mode,
                      cudaStream_t stream, bool clear_flag) {

@@ -133,6 +133,36 @@ nw_status build_matrix(nw_ctx* ctx, EvalMode mode, const uint32_t* left, uint64_
 nw_status general_evp(nw_ctx* ctx, int n, const double* h, const double* s, bool project, double tol, double* evals,
                       double* c, int* nkept);
 
+// Device scratch of one sorted evaluation (classify -> scan -> scatter -> evaluate).
+struct SortScratch {
+  uint32_t* keys;     // npairs
+  uint32_t* ranks;    // npairs
+  uint32_t* sidx;     // npairs
+  uint32_t* counts;   // nkeys
+  uint32_t* offsets;  // nkeys + 1
+  uint32_t* tsum;     // nkeys / 4096 + 1
+  uint32_t* flag;
+};
+
+// Fine-key budget of the sort (pair_sort_key): at most kFineMax counters, and at most about one
+// per pair of the request so the counter memset and scan stay small next to the evaluation.
+constexpr uint64_t kFineMax = 1ull << 23;
+constexpr uint64_t kFineMin = 1ull << 14;
+
+EvalParams make_params(const nw_ctx* ctx);
+// Number of sort keys with at most `cap` counters for the fast classes; fills P.nbucket/P.shift.
+uint64_t plan_keys(const nw_ctx* ctx, EvalParams& P, uint64_t cap);
+// classify -> scan -> scatter -> evaluate on `stream` (no allocation, no host synchronisation).
+// With npairs_dev the number of pairs is read on the device (at most npairs, the capacity the
+// launch is sized for); ev (six events or null) brackets the phases.
+nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const uint32_t* pairs, uint64_t npairs,
+                        double* out, const SortScratch& S, cudaStream_t stream, cudaEvent_t* ev,
+                        EvalMode mode = EvalMode::kHS, const uint32_t* npairs_dev = nullptr);
+
+// Exclusive scan of n counters into offsets[0..n] (offsets[n] = total); tsum holds n / 4096 + 1.
+nw_status scan_exclusive(nw_ctx* ctx, const uint32_t* counts, uint64_t n, uint32_t* offsets, uint32_t* tsum,
+                         cudaStream_t stream);
+
 // Same evaluation with its scratch in a fixed device array (no device allocation).
 nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, cudaStream_t stream);
 

@@ -1,0 +1,572 @@
+// NOCI-QMC with signed real walkers on the GPU (nw_qmc_*).
+//
+// One cycle (propagate_iteration, src/stochastic/metric.rs:378-473, for the uniform generator):
+//   1. qmc_sample_kernel   per determinant: sampled population n~ = Phi_c1(N) (FRI), the
+//                          diagonal change -dt (H_gg - E^S S_gg - E^I) n~ into delta, and the
+//                          number of spawning attempts max(1, ceil|n~|);
+//   2. scan of the attempts -> the attempt slots of every determinant;
+//   3. qmc_spawn_kernel    per attempt: its parent (binary search over the slots), a uniform
+//                          child != parent, the canonical pair (min, max);
+//   4. (H, S) of all attempts through the engine's sorted pair pipeline, with the number of
+//      attempts read on the device;
+//   5. qmc_apply_kernel    per attempt: -dt (H - E^S S) (n~ / attempts) (N - 1), FRI-rounded
+//                          with the spawn cutoff, added to delta[child] (FP64 atomics).
+// After ncycles: qmc_block_kernel adds delta to the populations (annihilation happens in the
+// dense accumulation) and reduces the statistics per block; qmc_finalize_kernel sums them in a
+// fixed order, updates the shift (update_shift, metric.rs:729-751) and writes the report.
+// Every per-run quantity (shift, cycle counter, attempt count) lives in device memory, so a
+// report block is captured once as a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "internal.cuh"
+#include "qmc_math.cuh"
+
+namespace {
+
+constexpr int kReportRing = 4096;   // device report slots between host copies
+constexpr int kBlockThreads = 256;
+constexpr int kStatBlocks = 296;     // 2 x 148 SMs
+constexpr int kStats = 6;            // nw, nref, num, den, sampled norm, nocc
+
+struct QmcState {
+  double shift;
+  double nw_prev;
+  uint64_t cycle;
+  uint64_t report;
+  uint64_t attempts;   // attempts of the current block
+  uint32_t npairs;     // attempts of the current cycle held in the buffers
+  uint32_t overflow;   // a cycle needed more attempts than the buffers hold
+  int32_t reached;
+  int32_t pad;
+};
+
+struct QmcParams {
+  uint64_t ndet;
+  uint64_t cap;
+  uint64_t seed;
+  double dt, target, c_sample, c_spawn, damping;
+  int32_t ncycles, prop;
+};
+
+template <class T>
+T* dalloc(size_t count, bool* ok) {
+  void* p = nullptr;
+  if (cudaMalloc(&p, std::max<size_t>(count * sizeof(T), 256)) != cudaSuccess) {
+    *ok = false;
+    return nullptr;
+  }
+  return static_cast<T*>(p);
+}
+
+__global__ void qmc_sample_kernel(QmcParams q, const QmcState* __restrict__ st, const double* __restrict__ pop,
+                                  const double2* __restrict__ diag, double* __restrict__ sampled,
+                                  uint32_t* __restrict__ na, double* __restrict__ delta) {
+  const uint64_t cycle = st->cycle;
+  const double es = st->shift;
+  for (uint64_t d = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; d < q.ndet; d += (uint64_t)gridDim.x * blockDim.x) {
+    const double p = pop[d];
+    double n = 0.0;
+    if (p != 0.0) n = nwq::fri(p, q.c_sample, nwq::uniform1(q.seed, cycle, d, nwq::kDrawSample));
+    sampled[d] = n;
+    const uint64_t a = nwq::attempts(n);
+    na[d] = a > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)a;
+    if (n != 0.0) {
+      const double2 hs = diag[d];
+      delta[d] += nwq::diagonal_change(q.prop, q.dt, es, hs.x, hs.y, n);
+    }
+  }
+}
+
+__global__ void qmc_count_kernel(QmcParams q, QmcState* __restrict__ st, const uint32_t* __restrict__ off) {
+  const uint64_t total = off[q.ndet];
+  const uint64_t held = total < q.cap ? total : q.cap;
+  if (total > q.cap) st->overflow = 1;
+  st->npairs = (uint32_t)held;
+  st->attempts += total;
+}
+
+// Largest g with off[g] <= t (off non-decreasing, off[0] = 0, t < off[ndet]).
+__device__ __forceinline__ uint64_t owner_of(const uint32_t* __restrict__ off, uint64_t ndet, uint32_t t) {
+  uint64_t lo = 0, hi = ndet;  // invariant: off[lo] <= t < off[hi]
+  while (hi - lo > 1) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (off[mid] <= t)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__global__ void qmc_spawn_kernel(QmcParams q, const QmcState* __restrict__ st, const uint32_t* __restrict__ off,
+                                 const double* __restrict__ sampled, const uint32_t* __restrict__ na,
+                                 uint2* __restrict__ pairs, uint32_t* __restrict__ child, double* __restrict__ amp) {
+  const uint32_t n = st->npairs;
+  const uint64_t cycle = st->cycle;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const uint64_t g = owner_of(off, q.ndet, t);
+    const uint64_t lam = nwq::uniform_child(g, q.ndet, nwq::uniform1(q.seed, cycle, t, nwq::kDrawChild));
+    pairs[t] = lam <= g ? make_uint2((uint32_t)lam, (uint32_t)g) : make_uint2((uint32_t)g, (uint32_t)lam);
+    child[t] = (uint32_t)lam;
+    amp[t] = sampled[g] / (double)na[g];
+  }
+}
+
+__global__ void qmc_apply_kernel(QmcParams q, const QmcState* __restrict__ st, const double2* __restrict__ hs,
+                                 const uint32_t* __restrict__ child, const double* __restrict__ amp,
+                                 double* __restrict__ delta) {
+  const uint32_t n = st->npairs;
+  const uint64_t cycle = st->cycle;
+  const double es = st->shift;
+  const double pgen = 1.0 / (double)(q.ndet - 1);
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const double2 v = hs[t];
+    const double raw = nwq::spawn_amplitude(q.prop, q.dt, es, v.x, v.y, amp[t], pgen);
+    const double dn = nwq::fri(raw, q.c_spawn, nwq::uniform1(q.seed, cycle, t, nwq::kDrawSpawn));
+    if (dn != 0.0) atomicAdd(delta + child[t], dn);
+  }
+}
+
+__global__ void qmc_next_cycle_kernel(QmcState* __restrict__ st) { st->cycle += 1; }
+
+// N += delta, delta = 0; per-block partial statistics in a fixed order.
+__global__ void __launch_bounds__(kBlockThreads) qmc_block_kernel(QmcParams q, double* __restrict__ pop,
+                                                                  double* __restrict__ delta,
+                                                                  const double* __restrict__ sampled,
+                                                                  const double2* __restrict__ refhs,
+                                                                  const uint8_t* __restrict__ isref, int apply,
+                                                                  double* __restrict__ partial) {
+  double acc[kStats] = {0, 0, 0, 0, 0, 0};
+  for (uint64_t d = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; d < q.ndet; d += (uint64_t)gridDim.x * blockDim.x) {
+    double p = pop[d];
+    if (apply) {
+      p += delta[d];
+      pop[d] = p;
+      delta[d] = 0.0;
+    }
+    const double a = fabs(p);
+    const double2 r = refhs[d];
+    const double sn = sampled[d];
+    acc[0] += a;
+    acc[1] += isref[d] ? a : 0.0;
+    acc[2] += p * r.x;
+    acc[3] += p * r.y;
+    acc[4] += fabs(sn);
+    acc[5] += sn != 0.0 ? 1.0 : 0.0;
+  }
+  __shared__ double red[kStats][kBlockThreads];
+#pragma unroll
+  for (int k = 0; k < kStats; ++k) red[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int w = kBlockThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int k = 0; k < kStats; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < kStats) partial[blockIdx.x * kStats + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// Sum the partials (fixed order), update the shift and write the report of this block.
+__global__ void qmc_finalize_kernel(QmcParams q, QmcState* __restrict__ st, const double* __restrict__ partial,
+                                    int nblocks, nw_qmc_report* __restrict__ ring, int write_report) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double tot[kStats] = {0, 0, 0, 0, 0, 0};
+  for (int b = 0; b < nblocks; ++b)
+    for (int k = 0; k < kStats; ++k) tot[k] += partial[b * kStats + k];
+  if (!write_report) {
+    st->nw_prev = tot[0];
+    return;
+  }
+  const double nw = tot[0];
+  if (!st->reached && nw >= q.target) st->reached = 1;
+  if (st->reached) st->shift = nwq::updated_shift(st->shift, q.damping, q.dt * (double)q.ncycles, nw, st->nw_prev);
+  st->nw_prev = nw;
+  nw_qmc_report& r = ring[st->report % kReportRing];
+  r.shift = st->shift;
+  r.eproj_num = tot[2];
+  r.eproj_den = tot[3];
+  r.nw = nw;
+  r.nref = tot[1];
+  r.sampled_norm = tot[4];
+  r.nocc = (uint64_t)tot[5];
+  r.nattempts = st->attempts;
+  st->attempts = 0;
+  st->report += 1;
+}
+
+__global__ void qmc_axpy2_kernel(uint64_t n, double c, const double2* __restrict__ x, double2* __restrict__ y) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const double2 v = x[i];
+    y[i].x += c * v.x;
+    y[i].y += c * v.y;
+  }
+}
+
+__global__ void qmc_pairs_kernel(uint64_t n, uint32_t bra, uint2* __restrict__ pairs, int diagonal) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    pairs[i] = diagonal ? make_uint2((uint32_t)i, (uint32_t)i) : make_uint2(bra, (uint32_t)i);
+}
+
+inline int grid_for(uint64_t work, int per_sm = 8) {
+  uint64_t g = (work + kBlockThreads - 1) / kBlockThreads;
+  g = std::min<uint64_t>(g, 148ull * per_sm);
+  return (int)std::max<uint64_t>(g, 1);
+}
+
+}  // namespace
+
+struct nw_qmc {
+  nw_ctx* ctx = nullptr;
+  nw_qmc_opts opts{};
+  QmcParams q{};
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // bracket the graph launches of the last run
+  float last_ms = 0.0f;
+  // device state
+  QmcState* st = nullptr;
+  double* pop = nullptr;
+  double* sampled = nullptr;
+  double* delta = nullptr;
+  uint32_t* na = nullptr;
+  uint32_t* off = nullptr;
+  uint32_t* tsum = nullptr;
+  double2* diag = nullptr;
+  double2* refhs = nullptr;
+  uint8_t* isref = nullptr;
+  uint2* pairs = nullptr;
+  uint32_t* child = nullptr;
+  double* amp = nullptr;
+  double2* hs = nullptr;
+  double* partial = nullptr;
+  nw_qmc_report* ring = nullptr;
+  // sort scratch for the attempts
+  nw::EvalParams P{};
+  uint64_t nkeys = 0;
+  nw::SortScratch S{};
+  std::vector<void*> owned;
+};
+
+namespace {
+
+nw_status qmc_fail(nw_qmc* q, nw_status s, const std::string& m) { return nw::fail(q->ctx, s, m); }
+
+// One cycle's launches (steps 1-5 of the file comment), then the cycle counter.
+nw_status enqueue_cycle(nw_qmc* q) {
+  nw_ctx* ctx = q->ctx;
+  const cudaStream_t s = q->stream;
+  const uint64_t nd = q->q.ndet;
+  qmc_sample_kernel<<<grid_for(nd), kBlockThreads, 0, s>>>(q->q, q->st, q->pop, q->diag, q->sampled, q->na, q->delta);
+  NW_CUDA(ctx, cudaGetLastError());
+  nw_status st = nw::scan_exclusive(ctx, q->na, nd, q->off, q->tsum, s);
+  if (st != NW_OK) return st;
+  qmc_count_kernel<<<1, 1, 0, s>>>(q->q, q->st, q->off);
+  qmc_spawn_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(q->q, q->st, q->off, q->sampled, q->na, q->pairs,
+                                                                q->child, q->amp);
+  NW_CUDA(ctx, cudaGetLastError());
+  st = nw::launch_sorted(ctx, q->P, q->nkeys, reinterpret_cast<const uint32_t*>(q->pairs), q->q.cap,
+                         reinterpret_cast<double*>(q->hs), q->S, s, nullptr, nw::EvalMode::kHS, &q->st->npairs);
+  if (st != NW_OK) return st;
+  qmc_apply_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(q->q, q->st, q->hs, q->child, q->amp, q->delta);
+  qmc_next_cycle_kernel<<<1, 1, 0, s>>>(q->st);
+  NW_CUDA(ctx, cudaGetLastError());
+  return NW_OK;
+}
+
+nw_status enqueue_block(nw_qmc* q) {
+  for (int c = 0; c < q->q.ncycles; ++c) {
+    const nw_status st = enqueue_cycle(q);
+    if (st != NW_OK) return st;
+  }
+  qmc_block_kernel<<<kStatBlocks, kBlockThreads, 0, q->stream>>>(q->q, q->pop, q->delta, q->sampled, q->refhs, q->isref,
+                                                                 1, q->partial);
+  qmc_finalize_kernel<<<1, 32, 0, q->stream>>>(q->q, q->st, q->partial, kStatBlocks, q->ring, 1);
+  NW_CUDA(q->ctx, cudaGetLastError());
+  return NW_OK;
+}
+
+// Statistics of the current populations as the previous-block reference (no report written).
+nw_status reset_reference_stats(nw_qmc* q) {
+  NW_CUDA(q->ctx, cudaMemsetAsync(q->sampled, 0, sizeof(double) * q->q.ndet, q->stream));
+  qmc_block_kernel<<<kStatBlocks, kBlockThreads, 0, q->stream>>>(q->q, q->pop, q->delta, q->sampled, q->refhs, q->isref,
+                                                                 0, q->partial);
+  qmc_finalize_kernel<<<1, 32, 0, q->stream>>>(q->q, q->st, q->partial, kStatBlocks, q->ring, 0);
+  NW_CUDA(q->ctx, cudaGetLastError());
+  NW_CUDA(q->ctx, cudaStreamSynchronize(q->stream));
+  return NW_OK;
+}
+
+void release(nw_qmc* q) {
+  if (q->graph) cudaGraphExecDestroy(q->graph);
+  if (q->ev0) cudaEventDestroy(q->ev0);
+  if (q->ev1) cudaEventDestroy(q->ev1);
+  for (void* p : q->owned)
+    if (p) cudaFree(p);
+  if (q->stream) cudaStreamDestroy(q->stream);
+  delete q;
+}
+
+}  // namespace
+
+extern "C" {
+
+nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, const uint32_t* ref_idx,
+                        uint64_t nref_idx, nw_qmc** out) {
+  if (!out) return NW_ERR_INVALID;
+  *out = nullptr;
+  if (!ctx || !opts || !c0 || (nref_idx && !ref_idx)) return NW_ERR_INVALID;
+  if (!ctx->built) return nw::fail(ctx, NW_ERR_STATE, "intermediates not built");
+  if (!ctx->d_dets || ctx->ndet < 2) return nw::fail(ctx, NW_ERR_STATE, "QMC needs a resident basis of >= 2 determinants");
+  if (!(opts->dt > 0.0) || opts->ncycles < 1 || opts->propagator < 0 || opts->propagator > 4 ||
+      !(opts->initial_population > 0.0) || !(opts->sampling_cutoff >= 0.0) || !(opts->spawn_cutoff >= 0.0) ||
+      !std::isfinite(opts->initial_shift) || !std::isfinite(opts->shift_damping))
+    return nw::fail(ctx, NW_ERR_INVALID, "invalid QMC options");
+  const uint64_t nd = ctx->ndet;
+  double norm = 0.0;
+  for (uint64_t i = 0; i < nd; ++i) {
+    if (!std::isfinite(c0[i])) return nw::fail(ctx, NW_ERR_INVALID, "non-finite initial coefficient");
+    norm += std::fabs(c0[i]);
+  }
+  if (norm == 0.0) return nw::fail(ctx, NW_ERR_INVALID, "initial coefficients are all zero");
+  for (uint64_t k = 0; k < nref_idx; ++k)
+    if (ref_idx[k] >= nd) return nw::fail(ctx, NW_ERR_INVALID, "reference index out of range");
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+
+  nw_qmc* q = new (std::nothrow) nw_qmc;
+  if (!q) return NW_ERR_ALLOC;
+  q->ctx = ctx;
+  q->opts = *opts;
+  uint64_t cap = opts->max_attempts;
+  // automatic: the 1-norm can overshoot the target many times before the shift holds it
+  // (below the annihilation plateau it grows at the sign-incoherent rate)
+  if (cap == 0) cap = (uint64_t)(16.0 * std::max(opts->target_population, opts->initial_population)) + 2 * nd + (1u << 20);
+  cap = std::min<uint64_t>(cap, 0xFFFFFFF0ull);
+  q->q = QmcParams{nd,
+                   cap,
+                   opts->seed,
+                   opts->dt,
+                   opts->target_population,
+                   opts->sampling_cutoff,
+                   opts->spawn_cutoff,
+                   opts->shift_damping,
+                   opts->ncycles,
+                   opts->propagator};
+  bool ok = true;
+  auto take = [&](auto*& p, size_t count) {
+    using T = std::remove_reference_t<decltype(*p)>;
+    p = dalloc<T>(count, &ok);
+    q->owned.push_back(p);
+  };
+  take(q->st, 1);
+  take(q->pop, nd);
+  take(q->sampled, nd);
+  take(q->delta, nd);
+  take(q->na, nd);
+  take(q->off, nd + 1);
+  take(q->tsum, nd / 4096 + 1);
+  take(q->diag, nd);
+  take(q->refhs, nd);
+  take(q->isref, nd);
+  take(q->pairs, std::max<uint64_t>(cap, nd));
+  take(q->child, cap);
+  take(q->amp, cap);
+  take(q->hs, std::max<uint64_t>(cap, nd));
+  take(q->partial, (size_t)kStatBlocks * kStats);
+  take(q->ring, kReportRing);
+  q->P = nw::make_params(ctx);
+  q->nkeys = nw::plan_keys(ctx, q->P, std::min(nw::kFineMax, std::max(nw::kFineMin, cap)));
+  take(q->S.keys, cap);
+  take(q->S.ranks, cap);
+  take(q->S.sidx, cap);
+  take(q->S.counts, q->nkeys);
+  take(q->S.offsets, q->nkeys + 1);
+  take(q->S.tsum, q->nkeys / 4096 + 1);
+  take(q->S.flag, 64);
+  if (!ok) {
+    release(q);
+    return nw::fail(ctx, NW_ERR_ALLOC, "QMC buffer allocation failed");
+  }
+  if (cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&q->ev0) != cudaSuccess || cudaEventCreate(&q->ev1) != cudaSuccess) {
+    release(q);
+    return nw::fail(ctx, NW_ERR_CUDA, "QMC stream creation failed");
+  }
+  nw_status st = NW_OK;
+  do {
+    // diagonal (H_gg, S_gg) and projected-energy couplings sum_i c0_i (H_ig, S_ig)
+    qmc_pairs_kernel<<<grid_for(nd), kBlockThreads, 0, q->stream>>>(nd, 0, q->pairs, 1);
+    if ((st = nw::eval_pairs(ctx, reinterpret_cast<uint32_t*>(q->pairs), nd, reinterpret_cast<double*>(q->diag),
+                             nw::EvalMode::kHS, q->stream)) != NW_OK)
+      break;
+    if (cudaMemsetAsync(q->refhs, 0, sizeof(double2) * nd, q->stream) != cudaSuccess) {
+      st = nw::fail(ctx, NW_ERR_CUDA, "memset");
+      break;
+    }
+    std::vector<uint8_t> isref(nd, 0);
+    for (uint64_t k = 0; k < nref_idx && st == NW_OK; ++k) {
+      const uint32_t i = ref_idx[k];
+      isref[i] = 1;
+      if (c0[i] == 0.0) continue;
+      qmc_pairs_kernel<<<grid_for(nd), kBlockThreads, 0, q->stream>>>(nd, i, q->pairs, 0);
+      if ((st = nw::eval_pairs(ctx, reinterpret_cast<uint32_t*>(q->pairs), nd, reinterpret_cast<double*>(q->hs),
+                               nw::EvalMode::kHS, q->stream)) != NW_OK)
+        break;
+      qmc_axpy2_kernel<<<grid_for(nd), kBlockThreads, 0, q->stream>>>(nd, c0[i], q->hs, q->refhs);
+    }
+    if (st != NW_OK) break;
+    std::vector<double> pop(nd);
+    const double scale = opts->initial_population / norm;
+    for (uint64_t i = 0; i < nd; ++i) pop[i] = scale * c0[i];
+    QmcState hst{};
+    hst.shift = opts->initial_shift;
+    if (cudaMemcpyAsync(q->isref, isref.data(), nd, cudaMemcpyHostToDevice, q->stream) != cudaSuccess ||
+        cudaMemcpyAsync(q->pop, pop.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, q->stream) != cudaSuccess ||
+        cudaMemcpyAsync(q->st, &hst, sizeof(hst), cudaMemcpyHostToDevice, q->stream) != cudaSuccess ||
+        cudaMemsetAsync(q->delta, 0, sizeof(double) * nd, q->stream) != cudaSuccess ||
+        cudaMemsetAsync(q->S.flag, 0, 64, q->stream) != cudaSuccess ||
+        cudaStreamSynchronize(q->stream) != cudaSuccess) {
+      st = nw::fail(ctx, NW_ERR_CUDA, "QMC initialisation copies failed");
+      break;
+    }
+    st = reset_reference_stats(q);
+  } while (false);
+  if (st != NW_OK) {
+    release(q);
+    return st;
+  }
+  *out = q;
+  return NW_OK;
+}
+
+nw_status nw_qmc_run(nw_qmc* q, int32_t nreports, nw_qmc_report* reports) {
+  if (!q || nreports < 0 || (nreports && !reports)) return NW_ERR_INVALID;
+  nw_ctx* ctx = q->ctx;
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (!q->graph) {
+    // capture one report block
+    cudaGraph_t g = nullptr;
+    NW_CUDA(ctx, cudaStreamBeginCapture(q->stream, cudaStreamCaptureModeThreadLocal));
+    const nw_status st = enqueue_block(q);
+    const cudaError_t e = cudaStreamEndCapture(q->stream, &g);
+    if (st != NW_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e != cudaSuccess) return nw::cuda_fail(ctx, e, "QMC graph capture");
+    const cudaError_t ei = cudaGraphInstantiate(&q->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      q->graph = nullptr;
+      return nw::cuda_fail(ctx, ei, "QMC graph instantiation");
+    }
+  }
+  QmcState hst{};
+  NW_CUDA(ctx, cudaMemcpyAsync(&hst, q->st, sizeof(hst), cudaMemcpyDeviceToHost, q->stream));
+  NW_CUDA(ctx, cudaStreamSynchronize(q->stream));
+  uint64_t first = hst.report;
+  int done = 0;
+  q->last_ms = 0.0f;
+  while (done < nreports) {
+    const int chunk = std::min(nreports - done, kReportRing);
+    NW_CUDA(ctx, cudaEventRecord(q->ev0, q->stream));
+    for (int r = 0; r < chunk; ++r) NW_CUDA(ctx, cudaGraphLaunch(q->graph, q->stream));
+    NW_CUDA(ctx, cudaEventRecord(q->ev1, q->stream));
+    for (int r = 0; r < chunk; ++r) {
+      const uint64_t slot = (first + (uint64_t)r) % kReportRing;
+      NW_CUDA(ctx, cudaMemcpyAsync(&reports[done + r], q->ring + slot, sizeof(nw_qmc_report), cudaMemcpyDeviceToHost,
+                                   q->stream));
+    }
+    NW_CUDA(ctx, cudaMemcpyAsync(&hst, q->st, sizeof(hst), cudaMemcpyDeviceToHost, q->stream));
+    NW_CUDA(ctx, cudaStreamSynchronize(q->stream));
+    float ms = 0.0f;
+    NW_CUDA(ctx, cudaEventElapsedTime(&ms, q->ev0, q->ev1));
+    q->last_ms += ms;
+    first += chunk;
+    done += chunk;
+    if (hst.overflow)
+      return qmc_fail(q, NW_ERR_UNSUPPORTED, "a QMC cycle needed more spawning attempts than max_attempts (" +
+                                                 std::to_string(q->q.cap) + ")");
+  }
+  return NW_OK;
+}
+
+nw_status nw_qmc_set_shift(nw_qmc* q, double shift) {
+  if (!q || !std::isfinite(shift)) return NW_ERR_INVALID;
+  nw_ctx* ctx = q->ctx;
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  QmcState hst{};
+  NW_CUDA(ctx, cudaMemcpyAsync(&hst, q->st, sizeof(hst), cudaMemcpyDeviceToHost, q->stream));
+  NW_CUDA(ctx, cudaStreamSynchronize(q->stream));
+  hst.shift = shift;
+  NW_CUDA(ctx, cudaMemcpyAsync(q->st, &hst, sizeof(hst), cudaMemcpyHostToDevice, q->stream));
+  NW_CUDA(ctx, cudaStreamSynchronize(q->stream));
+  return NW_OK;
+}
+
+nw_status nw_qmc_last_run_ms(const nw_qmc* q, float* ms) {
+  if (!q || !ms) return NW_ERR_INVALID;
+  *ms = q->last_ms;
+  return NW_OK;
+}
+
+nw_status nw_qmc_populations(nw_qmc* q, double* populations) {
+  if (!q || !populations) return NW_ERR_INVALID;
+  NW_CUDA(q->ctx, cudaSetDevice(q->ctx->device));
+  NW_CUDA(q->ctx, cudaMemcpyAsync(populations, q->pop, sizeof(double) * q->q.ndet, cudaMemcpyDeviceToHost, q->stream));
+  NW_CUDA(q->ctx, cudaStreamSynchronize(q->stream));
+  return NW_OK;
+}
+
+nw_status nw_qmc_set_populations(nw_qmc* q, const double* populations) {
+  if (!q || !populations) return NW_ERR_INVALID;
+  for (uint64_t i = 0; i < q->q.ndet; ++i)
+    if (!std::isfinite(populations[i])) return qmc_fail(q, NW_ERR_INVALID, "non-finite population");
+  NW_CUDA(q->ctx, cudaSetDevice(q->ctx->device));
+  NW_CUDA(q->ctx, cudaMemcpyAsync(q->pop, populations, sizeof(double) * q->q.ndet, cudaMemcpyHostToDevice, q->stream));
+  return reset_reference_stats(q);
+}
+
+nw_status nw_qmc_cycle_delta(nw_qmc* q, uint64_t cycle, double* delta) {
+  if (!q || !delta) return NW_ERR_INVALID;
+  nw_ctx* ctx = q->ctx;
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  QmcState hst{};
+  NW_CUDA(ctx, cudaMemcpyAsync(&hst, q->st, sizeof(hst), cudaMemcpyDeviceToHost, q->stream));
+  NW_CUDA(ctx, cudaStreamSynchronize(q->stream));
+  const uint64_t saved_cycle = hst.cycle, saved_attempts = hst.attempts;
+  hst.cycle = cycle;
+  NW_CUDA(ctx, cudaMemcpyAsync(q->st, &hst, sizeof(hst), cudaMemcpyHostToDevice, q->stream));
+  NW_CUDA(ctx, cudaMemsetAsync(q->delta, 0, sizeof(double) * q->q.ndet, q->stream));
+  nw_status st = enqueue_cycle(q);
+  if (st != NW_OK) return st;
+  NW_CUDA(ctx, cudaMemcpyAsync(delta, q->delta, sizeof(double) * q->q.ndet, cudaMemcpyDeviceToHost, q->stream));
+  NW_CUDA(ctx, cudaMemsetAsync(q->delta, 0, sizeof(double) * q->q.ndet, q->stream));
+  NW_CUDA(ctx, cudaMemcpyAsync(&hst, q->st, sizeof(hst), cudaMemcpyDeviceToHost, q->stream));
+  NW_CUDA(ctx, cudaStreamSynchronize(q->stream));
+  const bool overflow = hst.overflow != 0;
+  hst.cycle = saved_cycle;
+  hst.attempts = saved_attempts;
+  hst.overflow = 0;
+  NW_CUDA(ctx, cudaMemcpyAsync(q->st, &hst, sizeof(hst), cudaMemcpyHostToDevice, q->stream));
+  NW_CUDA(ctx, cudaStreamSynchronize(q->stream));
+  if (overflow) return qmc_fail(q, NW_ERR_UNSUPPORTED, "spawning attempts exceeded max_attempts");
+  return NW_OK;
+}
+
+nw_status nw_qmc_destroy(nw_qmc* q) {
+  if (!q) return NW_OK;
+  cudaSetDevice(q->ctx->device);
+  if (q->stream) cudaStreamSynchronize(q->stream);
+  release(q);
+  return NW_OK;
+}
+
+}  // extern "C"

@@ -52,6 +52,24 @@ class NwOpts(ctypes.Structure):
     _fields_ = [("tol", ctypes.c_double), ("convention", ctypes.c_int32), ("device", ctypes.c_int32)]
 
 
+class NwQmcOpts(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("initial_population", ctypes.c_double),
+                ("target_population", ctypes.c_double), ("sampling_cutoff", ctypes.c_double),
+                ("spawn_cutoff", ctypes.c_double), ("shift_damping", ctypes.c_double),
+                ("initial_shift", ctypes.c_double), ("ncycles", ctypes.c_int32), ("propagator", ctypes.c_int32),
+                ("seed", ctypes.c_uint64), ("max_attempts", ctypes.c_uint64)]
+
+
+class NwQmcReport(ctypes.Structure):
+    _fields_ = [("shift", ctypes.c_double), ("eproj_num", ctypes.c_double), ("eproj_den", ctypes.c_double),
+                ("nw", ctypes.c_double), ("nref", ctypes.c_double), ("sampled_norm", ctypes.c_double),
+                ("nocc", ctypes.c_uint64), ("nattempts", ctypes.c_uint64)]
+
+
+PROPAGATORS = {"unshifted": 0, "shifted": 1, "doubly-shifted": 2, "difference-doubly-shifted-u1": 3,
+               "difference-doubly-shifted-u2": 4}
+
+
 class NwInfo(ctypes.Structure):
     _fields_ = [("nref", ctypes.c_int32), ("nmo", ctypes.c_int32), ("ngeneric", ctypes.c_int32),
                 ("pad", ctypes.c_int32), ("slab_bytes", ctypes.c_uint64), ("ndet", ctypes.c_uint64)]
@@ -60,7 +78,9 @@ class NwInfo(ctypes.Structure):
 EXPORTED = ("nw_ctx_create", "nw_build_intermediates", "nw_pair_zero_counts", "nw_set_basis",
             "nw_eval_hs_pairs_device", "nw_eval_hs_pairs", "nw_eval_hs_pairs_noalloc",
             "nw_eval_s_pairs_device", "nw_update_fock", "nw_eval_fs_pairs_device", "nw_eval_fs_pairs",
-            "nw_build_hs_matrix", "nw_build_fs_matrix", "nw_general_evp", "nw_sync",
+            "nw_build_hs_matrix", "nw_build_fs_matrix", "nw_general_evp",
+            "nw_qmc_create", "nw_qmc_run", "nw_qmc_set_shift", "nw_qmc_last_run_ms", "nw_qmc_populations", "nw_qmc_set_populations", "nw_qmc_cycle_delta",
+            "nw_qmc_destroy", "nw_sync",
             "nw_set_timing", "nw_last_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
             "nw_last_error")
 
@@ -92,6 +112,14 @@ def load(path: Optional[str] = None):
     L.nw_build_fs_matrix.argtypes = [vp, vp, ctypes.c_uint64, vp, ctypes.c_uint64, ctypes.c_int, vp, vp]
     L.nw_general_evp.argtypes = [vp, ctypes.c_int32, vp, vp, ctypes.c_int, ctypes.c_double, vp, vp,
                                  ctypes.POINTER(ctypes.c_int32)]
+    L.nw_qmc_create.argtypes = [vp, ctypes.POINTER(NwQmcOpts), vp, vp, ctypes.c_uint64, ctypes.POINTER(vp)]
+    L.nw_qmc_run.argtypes = [vp, ctypes.c_int32, vp]
+    L.nw_qmc_last_run_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    L.nw_qmc_set_shift.argtypes = [vp, ctypes.c_double]
+    L.nw_qmc_populations.argtypes = [vp, vp]
+    L.nw_qmc_set_populations.argtypes = [vp, vp]
+    L.nw_qmc_cycle_delta.argtypes = [vp, ctypes.c_uint64, vp]
+    L.nw_qmc_destroy.argtypes = [vp]
     L.nw_sync.argtypes = [vp, vp]
     L.nw_set_timing.argtypes = [vp, ctypes.c_int]
     L.nw_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
@@ -286,6 +314,78 @@ class WicksShared:
 
     def sync(self, stream: int = 0):
         self._check(self._lib.nw_sync(self._ctx, ctypes.c_void_p(stream)), "nw_sync")
+
+
+class Qmc:
+    """NOCI-QMC with signed real walkers on the GPU (qmc_step of src/stochastic/walkers.rs with
+    the uniform generator).  ``c0`` has one coefficient per determinant of the resident basis;
+    ``ref_idx`` are the reference determinants used for the projected energy."""
+
+    REPORT_FIELDS = ("shift", "eproj_num", "eproj_den", "nw", "nref", "sampled_norm", "nocc", "nattempts")
+
+    def __init__(self, wicks: "WicksShared", c0, ref_idx, dt: float, initial_population: float = 100.0,
+                 target_population: float = 1e5, sampling_cutoff: float = 0.0, spawn_cutoff: float = 0.0,
+                 shift_damping: float = 5e-4, initial_shift: float = 0.0, ncycles: int = 10,
+                 propagator: str = "unshifted", seed: int = 1, max_attempts: int = 0):
+        self._w = wicks
+        self._lib = wicks._lib
+        c0 = np.ascontiguousarray(c0, dtype=np.float64)
+        ref = np.ascontiguousarray(ref_idx, dtype=np.uint32)
+        o = NwQmcOpts(dt, initial_population, target_population, sampling_cutoff, spawn_cutoff, shift_damping,
+                      initial_shift, ncycles, PROPAGATORS[propagator] if isinstance(propagator, str) else propagator,
+                      seed, max_attempts)
+        self._q = ctypes.c_void_p()
+        self.ndet = c0.shape[0]
+        wicks._check(self._lib.nw_qmc_create(wicks._ctx, ctypes.byref(o), c0.ctypes.data, ref.ctypes.data,
+                                             ref.shape[0], ctypes.byref(self._q)), "nw_qmc_create")
+
+    def run(self, nreports: int) -> np.ndarray:
+        """Run report blocks; returns a structured array of per-block statistics."""
+        reps = (NwQmcReport * max(nreports, 1))()
+        self._w._check(self._lib.nw_qmc_run(self._q, nreports, reps), "nw_qmc_run")
+        dt = np.dtype([(f, np.float64) for f in self.REPORT_FIELDS[:6]] + [("nocc", np.uint64), ("nattempts", np.uint64)])
+        out = np.frombuffer(bytes(reps), dtype=dt)[:nreports].copy()
+        return out
+
+    def set_shift(self, shift: float):
+        self._w._check(self._lib.nw_qmc_set_shift(self._q, shift), "nw_qmc_set_shift")
+
+    def last_run_ms(self) -> float:
+        """Device ms of the report blocks of the last run (CUDA events on the run's stream)."""
+        ms = ctypes.c_float()
+        self._w._check(self._lib.nw_qmc_last_run_ms(self._q, ctypes.byref(ms)), "nw_qmc_last_run_ms")
+        return float(ms.value)
+
+    def populations(self) -> np.ndarray:
+        out = np.empty(self.ndet)
+        self._w._check(self._lib.nw_qmc_populations(self._q, out.ctypes.data), "nw_qmc_populations")
+        return out
+
+    def set_populations(self, pop):
+        pop = np.ascontiguousarray(pop, dtype=np.float64)
+        self._w._check(self._lib.nw_qmc_set_populations(self._q, pop.ctypes.data), "nw_qmc_set_populations")
+
+    def cycle_delta(self, cycle: int) -> np.ndarray:
+        out = np.empty(self.ndet)
+        self._w._check(self._lib.nw_qmc_cycle_delta(self._q, cycle, out.ctypes.data), "nw_qmc_cycle_delta")
+        return out
+
+    def close(self):
+        if getattr(self, "_q", None) and self._q.value:
+            self._lib.nw_qmc_destroy(self._q)
+            self._q = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def build_wicks_shared(ao, refs, tol: float = 1e-8, convention: str = "reference", device: int = 0) -> WicksShared:

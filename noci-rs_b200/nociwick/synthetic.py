@@ -99,14 +99,16 @@ def _force_zero_overlap(rng, cx: np.ndarray, cw: np.ndarray, nocc: int, k: int) 
 def make_system(nmo: int, nocc_a: int, nocc_b: int, nref: int, naux: int, seed: int,
                 sigma_h: float = 0.5, sigma_l: float = 0.1, k_scale: float = 0.3,
                 zero_pairs: Sequence[Tuple[int, int, int, int]] = (), enuc: float = 0.0,
-                uhf_like: bool = False) -> System:
+                uhf_like: bool = False, orbital_energies: Optional[np.ndarray] = None) -> System:
     """Build a seeded synthetic system.
 
     ``zero_pairs`` lists (x, w, k_alpha, k_beta): reference w is modified so that the ordered
     pairs (x, w) and (w, x) have k_alpha / k_beta zero-overlap orbital pairs.  With
     ``uhf_like`` the references are an RHF-like set (C_a = C_b = Q) followed by alternating
     spin-polarised sets (C_a = Q exp(K), C_b = Q exp(-K), then alpha and beta swapped), as in
-    the RHF + UHF(+,-) + UHF(-,+) reference spaces of noci-rs inputs.
+    the RHF + UHF(+,-) + UHF(-,+) reference spaces of noci-rs inputs.  ``orbital_energies``
+    adds Q diag(eps) Q^T to h, so the base orbitals carry molecule-like orbital energies
+    (occupied first) and the excited determinants lie above the references.
     """
     rng = np.random.default_rng(seed)
     n = nmo
@@ -117,6 +119,8 @@ def make_system(nmo: int, nocc_a: int, nocc_b: int, nref: int, naux: int, seed: 
     eri = np.tensordot(chol, chol, axes=(0, 0))       # (mu nu|lam sig)
     s = np.eye(n)
     q = _random_orthonormal(rng, n)
+    if orbital_energies is not None:
+        h = h + q @ np.diag(np.asarray(orbital_energies, float)) @ q.T
     refs = []
     if uhf_like:
         refs.append((q.copy(), (1 << nocc_a) - 1, q.copy(), (1 << nocc_b) - 1))
@@ -294,6 +298,17 @@ def config1_system(seed: int = 1) -> System:
 def config2_system(seed: int = 2) -> System:
     """Stand-in for linear H6/cc-pVDZ: n = 30, 3 alpha + 3 beta electrons, RHF + 2 UHF refs."""
     return make_system(30, 3, 3, 3, 120, seed, k_scale=0.08, uhf_like=True, enuc=0.0)
+
+
+def config4_system(seed: int = 4) -> System:
+    """Linear-H8/cc-pVDZ NOCISD(3)-QMC stand-in dimensions: n = 40, 4 + 4 electrons, an RHF-like
+    and two spin-polarised references (all singles and doubles: 85755 determinants).  Unlike the
+    unstructured stand-ins it carries orbital energies (occupied -1.0..-0.5, virtual 0.2..2.5 Eh)
+    and weak random couplings, so excited determinants lie above the references and the
+    off-diagonal row sums of H and S stay molecule-like (sum_w |S_xw| < 1)."""
+    eps = np.concatenate([np.linspace(-1.0, -0.5, 4), np.linspace(0.2, 2.5, 36)])
+    return make_system(40, 4, 4, 3, 160, seed, sigma_h=0.02, sigma_l=0.02, k_scale=0.3, uhf_like=True,
+                       enuc=0.0, orbital_energies=eps)
 
 
 def config3_system(seed: int = 3, nmo: int = 64, nref: int = 8) -> System:

@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cstring>
 
+#include "../../noci-rs_b200/csrc/qmc_math.cuh"
 #include "../../noci-rs_b200/csrc/wick_math.cuh"
 
 using namespace nw;
@@ -75,6 +76,24 @@ DetRec rec_at(const void* dets, uint32_t i) {
 }  // namespace
 
 extern "C" {
+
+// NOCI-QMC arithmetic (qmc_math.cuh).
+void mir_philox(const uint32_t* ctr, uint32_t k0, uint32_t k1, uint32_t* out) {
+  const nwq::U4 r = nwq::philox4x32_10(nwq::U4{ctr[0], ctr[1], ctr[2], ctr[3]}, k0, k1);
+  out[0] = r.x;
+  out[1] = r.y;
+  out[2] = r.z;
+  out[3] = r.w;
+}
+void mir_uniform2(uint64_t seed, uint64_t cycle, uint64_t index, uint32_t purpose, double* out) {
+  nwq::uniform2(seed, cycle, index, purpose, &out[0], &out[1]);
+}
+double mir_fri(double x, double c, double u) { return nwq::fri(x, c, u); }
+uint64_t mir_uniform_child(uint64_t g, uint64_t n, double u) { return nwq::uniform_child(g, n, u); }
+uint64_t mir_attempts(double n) { return nwq::attempts(n); }
+double mir_diagonal_change(int prop, double dt, double es, double h, double s, double n) {
+  return nwq::diagonal_change(prop, dt, es, h, s, n);
+}
 
 int mir_layout_sizes(int which) { return which == 0 ? kNoff : which == 1 ? kNval : kNint; }
 

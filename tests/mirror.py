@@ -43,6 +43,17 @@ def lib():
                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, VP, U32, ctypes.c_int64, D]
         L.mir_eval_fs_gen.argtypes = [D, I64, D, I32, D, I64, D, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_double, ctypes.c_int, VP, U32, ctypes.c_int64, D]
+        L.mir_philox.argtypes = [U32, ctypes.c_uint32, ctypes.c_uint32, U32]
+        L.mir_uniform2.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, D]
+        L.mir_fri.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.mir_fri.restype = ctypes.c_double
+        L.mir_uniform_child.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_double]
+        L.mir_uniform_child.restype = ctypes.c_uint64
+        L.mir_attempts.argtypes = [ctypes.c_double]
+        L.mir_attempts.restype = ctypes.c_uint64
+        L.mir_diagonal_change.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_double]
+        L.mir_diagonal_change.restype = ctypes.c_double
         L.mir_layout.argtypes = [ctypes.c_int, D, D, ctypes.c_int64, D]
         _lib = L
     return _lib

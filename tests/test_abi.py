@@ -40,6 +40,8 @@ int main(void) {
          offsetof(nw_det, rank_b), offsetof(nw_det, idx_b), offsetof(nw_det, phase), sizeof(nw_system));
   printf("%zu %zu %zu %zu %zu\n", sizeof(nw_refs), sizeof(nw_opts), sizeof(nw_info),
          offsetof(nw_system, s), offsetof(nw_refs, c_alpha));
+  printf("%zu %zu %zu %zu %zu\n", sizeof(nw_qmc_opts), offsetof(nw_qmc_opts, ncycles), offsetof(nw_qmc_opts, seed),
+         sizeof(nw_qmc_report), offsetof(nw_qmc_report, nocc));
   return 0;
 }
 ''')
@@ -54,6 +56,8 @@ int main(void) {
     assert v[6] == ctypes.sizeof(L.NwSystem)
     assert v[7:10] == [ctypes.sizeof(L.NwRefs), ctypes.sizeof(L.NwOpts), ctypes.sizeof(L.NwInfo)]
     assert v[10] == L.NwSystem.s.offset and v[11] == L.NwRefs.c_alpha.offset
+    assert v[12:17] == [ctypes.sizeof(L.NwQmcOpts), L.NwQmcOpts.ncycles.offset, L.NwQmcOpts.seed.offset,
+                        ctypes.sizeof(L.NwQmcReport), L.NwQmcReport.nocc.offset]
 
 
 def test_header_compiles_as_cxx(tmp_path):
