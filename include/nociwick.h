@@ -268,6 +268,53 @@ NW_API nw_status nw_qmc_set_populations(nw_qmc* q, const double* populations);
 NW_API nw_status nw_qmc_cycle_delta(nw_qmc* q, uint64_t cycle, double* delta);
 NW_API nw_status nw_qmc_destroy(nw_qmc* q);
 
+/* ---------------------------------------------------------------------------------------
+ * NOCI-PT2 / SNOCI linear solve: the candidate-candidate shifted Fock matrix M = F - E0 S
+ * stored on the device (packed upper triangle, n (n + 1) / 2 doubles), its mat-vec, and
+ * restarted right-preconditioned GMRES on the projected operator
+ *   M^Omega x = M x - f_a0 (s_0a . x) - s_a0 (f_0a . x) + 2 E0 s_a0 (s_0a . x),
+ * all in FP64.  Replaces build_candidate_m / fill_candidate_m and apply_candidate_m /
+ * apply_omega_m (src/snoci/operators.rs:205-296, 375-488, 696-955), Preconditioner
+ * (src/snoci/types.rs:138-288) and gmres (src/snoci/gmres.rs:406-544) for real states with no
+ * imaginary shift.
+ * --------------------------------------------------------------------------------------- */
+typedef enum { NW_PRECOND_DIAG = 0, NW_PRECOND_WOODBURY = 1 } nw_preconditioner;
+
+typedef struct nw_pt2_projection {
+    double e0;                  /* zeroth-order energy E0                                    */
+    const double* s_a0;         /* <Phi_a|Psi_0> per candidate (host, n)                     */
+    const double* s_0a;         /* <Psi_0|Phi_a>                                             */
+    const double* f_a0;         /* <Phi_a|F|Psi_0>                                           */
+    const double* f_0a;         /* <Psi_0|F|Phi_a>                                           */
+} nw_pt2_projection;
+
+typedef struct nw_gmres_opts {
+    int32_t max_iter;           /* total Arnoldi steps (noci-rs default 100)                  */
+    int32_t restart;            /* Krylov dimension per cycle (default 200)                   */
+    double res_tol;             /* |b - A x| / sqrt(n) at convergence (default 1e-8)          */
+    int32_t preconditioner;     /* nw_preconditioner (noci-rs default Woodbury)               */
+    int32_t pad;
+} nw_gmres_opts;
+
+typedef struct nw_gmres_info {
+    double residual_rms;        /* true residual |b - A x| / sqrt(n)                          */
+    int32_t iterations;
+    int32_t converged;
+} nw_gmres_info;
+
+typedef struct nw_pt2 nw_pt2;
+
+/* Build M = F - E0 S over candidates cand[0..n) of the resident basis (after nw_update_fock). */
+NW_API nw_status nw_pt2_create(nw_ctx* ctx, const uint32_t* cand, uint64_t n, double e0, nw_pt2** out);
+/* y = M x (host vectors of n), the unprojected candidate mat-vec (apply_candidate_m). */
+NW_API nw_status nw_pt2_apply_m(nw_pt2* p, const double* x, double* y);
+/* Device time of the last nw_pt2_apply_m product (CUDA events), in milliseconds. */
+NW_API nw_status nw_pt2_last_apply_ms(const nw_pt2* p, float* ms);
+/* Solve M^Omega x = rhs by GMRES from x = 0 (host vectors). */
+NW_API nw_status nw_pt2_solve(nw_pt2* p, const nw_pt2_projection* proj, const double* rhs, const nw_gmres_opts* opts,
+                              double* x, nw_gmres_info* info);
+NW_API nw_status nw_pt2_destroy(nw_pt2* p);
+
 /* Wait for the work queued on `stream` and report pair indices that were out of range in an
  * earlier device-buffer call (those outputs are NaN). */
 NW_API nw_status nw_sync(nw_ctx* ctx, void* stream);

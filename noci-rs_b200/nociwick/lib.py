@@ -70,6 +70,20 @@ PROPAGATORS = {"unshifted": 0, "shifted": 1, "doubly-shifted": 2, "difference-do
                "difference-doubly-shifted-u2": 4}
 
 
+class NwPt2Projection(ctypes.Structure):
+    _fields_ = [("e0", ctypes.c_double), ("s_a0", ctypes.c_void_p), ("s_0a", ctypes.c_void_p),
+                ("f_a0", ctypes.c_void_p), ("f_0a", ctypes.c_void_p)]
+
+
+class NwGmresOpts(ctypes.Structure):
+    _fields_ = [("max_iter", ctypes.c_int32), ("restart", ctypes.c_int32), ("res_tol", ctypes.c_double),
+                ("preconditioner", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+class NwGmresInfo(ctypes.Structure):
+    _fields_ = [("residual_rms", ctypes.c_double), ("iterations", ctypes.c_int32), ("converged", ctypes.c_int32)]
+
+
 class NwInfo(ctypes.Structure):
     _fields_ = [("nref", ctypes.c_int32), ("nmo", ctypes.c_int32), ("ngeneric", ctypes.c_int32),
                 ("pad", ctypes.c_int32), ("slab_bytes", ctypes.c_uint64), ("ndet", ctypes.c_uint64)]
@@ -80,7 +94,8 @@ EXPORTED = ("nw_ctx_create", "nw_build_intermediates", "nw_pair_zero_counts", "n
             "nw_eval_s_pairs_device", "nw_update_fock", "nw_eval_fs_pairs_device", "nw_eval_fs_pairs",
             "nw_build_hs_matrix", "nw_build_fs_matrix", "nw_general_evp",
             "nw_qmc_create", "nw_qmc_run", "nw_qmc_set_shift", "nw_qmc_last_run_ms", "nw_qmc_populations", "nw_qmc_set_populations", "nw_qmc_cycle_delta",
-            "nw_qmc_destroy", "nw_sync",
+            "nw_qmc_destroy", "nw_pt2_create", "nw_pt2_apply_m", "nw_pt2_last_apply_ms", "nw_pt2_solve",
+            "nw_pt2_destroy", "nw_sync",
             "nw_set_timing", "nw_last_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
             "nw_last_error")
 
@@ -120,6 +135,12 @@ def load(path: Optional[str] = None):
     L.nw_qmc_set_populations.argtypes = [vp, vp]
     L.nw_qmc_cycle_delta.argtypes = [vp, ctypes.c_uint64, vp]
     L.nw_qmc_destroy.argtypes = [vp]
+    L.nw_pt2_create.argtypes = [vp, vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(vp)]
+    L.nw_pt2_apply_m.argtypes = [vp, vp, vp]
+    L.nw_pt2_last_apply_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    L.nw_pt2_solve.argtypes = [vp, ctypes.POINTER(NwPt2Projection), vp, ctypes.POINTER(NwGmresOpts), vp,
+                               ctypes.POINTER(NwGmresInfo)]
+    L.nw_pt2_destroy.argtypes = [vp]
     L.nw_sync.argtypes = [vp, vp]
     L.nw_set_timing.argtypes = [vp, ctypes.c_int]
     L.nw_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
@@ -374,6 +395,62 @@ class Qmc:
         if getattr(self, "_q", None) and self._q.value:
             self._lib.nw_qmc_destroy(self._q)
             self._q = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Pt2:
+    """NOCI-PT2 / SNOCI linear solve on the GPU: M = F - E0 S over candidate determinants of the
+    resident basis (packed on the device), its mat-vec and GMRES on the projected operator
+    (build_candidate_m, apply_candidate_m, apply_omega_m and gmres of src/snoci)."""
+
+    def __init__(self, wicks: "WicksShared", candidates, e0: float):
+        self._w = wicks
+        self._lib = wicks._lib
+        cand = np.ascontiguousarray(candidates, dtype=np.uint32)
+        self.n = cand.shape[0]
+        self._p = ctypes.c_void_p()
+        wicks._check(self._lib.nw_pt2_create(wicks._ctx, cand.ctypes.data, self.n, e0, ctypes.byref(self._p)),
+                     "nw_pt2_create")
+
+    def apply_m(self, x) -> np.ndarray:
+        """y = M x (apply_candidate_m)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.n)
+        self._w._check(self._lib.nw_pt2_apply_m(self._p, x.ctypes.data, y.ctypes.data), "nw_pt2_apply_m")
+        return y
+
+    def last_apply_ms(self) -> float:
+        ms = ctypes.c_float()
+        self._w._check(self._lib.nw_pt2_last_apply_ms(self._p, ctypes.byref(ms)), "nw_pt2_last_apply_ms")
+        return float(ms.value)
+
+    def solve(self, e0, s_a0, s_0a, f_a0, f_0a, rhs, max_iter: int = 100, restart: int = 200,
+              res_tol: float = 1e-8, preconditioner: str = "woodbury"):
+        """GMRES on M^Omega x = rhs; returns (x, info)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (s_a0, s_0a, f_a0, f_0a, rhs)]
+        proj = NwPt2Projection(e0, *(a.ctypes.data for a in arrs[:4]))
+        opts = NwGmresOpts(max_iter, restart, res_tol, 1 if preconditioner == "woodbury" else 0, 0)
+        x = np.empty(self.n)
+        info = NwGmresInfo()
+        self._w._check(self._lib.nw_pt2_solve(self._p, ctypes.byref(proj), arrs[4].ctypes.data, ctypes.byref(opts),
+                                              x.ctypes.data, ctypes.byref(info)), "nw_pt2_solve")
+        return x, {"residual_rms": info.residual_rms, "iterations": info.iterations, "converged": bool(info.converged)}
+
+    def close(self):
+        if getattr(self, "_p", None) and self._p.value:
+            self._lib.nw_pt2_destroy(self._p)
+            self._p = ctypes.c_void_p()
 
     def __del__(self):
         try:

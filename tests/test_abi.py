@@ -42,6 +42,8 @@ int main(void) {
          offsetof(nw_system, s), offsetof(nw_refs, c_alpha));
   printf("%zu %zu %zu %zu %zu\n", sizeof(nw_qmc_opts), offsetof(nw_qmc_opts, ncycles), offsetof(nw_qmc_opts, seed),
          sizeof(nw_qmc_report), offsetof(nw_qmc_report, nocc));
+  printf("%zu %zu %zu %zu %zu\n", sizeof(nw_pt2_projection), sizeof(nw_gmres_opts), offsetof(nw_gmres_opts, res_tol),
+         offsetof(nw_gmres_opts, preconditioner), sizeof(nw_gmres_info));
   return 0;
 }
 ''')
@@ -58,6 +60,8 @@ int main(void) {
     assert v[10] == L.NwSystem.s.offset and v[11] == L.NwRefs.c_alpha.offset
     assert v[12:17] == [ctypes.sizeof(L.NwQmcOpts), L.NwQmcOpts.ncycles.offset, L.NwQmcOpts.seed.offset,
                         ctypes.sizeof(L.NwQmcReport), L.NwQmcReport.nocc.offset]
+    assert v[17:22] == [ctypes.sizeof(L.NwPt2Projection), ctypes.sizeof(L.NwGmresOpts), L.NwGmresOpts.res_tol.offset,
+                        L.NwGmresOpts.preconditioner.offset, ctypes.sizeof(L.NwGmresInfo)]
 
 
 def test_header_compiles_as_cxx(tmp_path):

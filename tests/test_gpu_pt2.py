@@ -1,0 +1,91 @@
+"""GPU NOCI-PT2 solve (nw_pt2_*) against the CPU restatement (oracle/pt2.py) on dense matrices
+built by the oracle: the stored M = F - E0 S and its mat-vec, GMRES on the projected operator
+with both preconditioners, and E_PT2 = a.M^Omega.a + 2 a.v."""
+import numpy as np
+import pytest
+
+import nociwick
+from nociwick import synthetic as sy
+from oracle import linalg as LA
+from oracle import pt2 as PT
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def snoci_system():
+    eps = np.concatenate([np.linspace(-1.0, -0.5, 2), np.linspace(0.2, 2.5, 6)])
+    system = sy.make_system(8, 2, 2, 2, 20, seed=3, sigma_h=0.05, sigma_l=0.05, k_scale=0.3, uhf_like=True,
+                            orbital_energies=eps)
+    basis = sy.sd_basis(8, 2, 2, 2)
+    orc = Oracle.from_system(system, tol=1e-8)
+    ob = orc.oracle_basis(basis)
+    nd = basis.shape[0]
+    pairs = np.array([(a, b) for a in range(nd) for b in range(nd)])
+    h, s = orc.eval_pairs(ob, pairs)
+    h, s = h.reshape(nd, nd), s.reshape(nd, nd)
+    orc.set_fock(system.h, system.h)
+    _, f, _ = orc.eval_m_pairs(ob, pairs, 0.0)
+    f = f.reshape(nd, nd)
+    refs = np.nonzero((basis["rank_a"] == 0) & (basis["rank_b"] == 0))[0]
+    ec, cc = LA.general_evp(h[np.ix_(refs, refs)], s[np.ix_(refs, refs)], True, 1e-8)
+    c = cc[:, 0]
+    e0 = float(c @ f[np.ix_(refs, refs)] @ c)
+    return system, basis, h, s, f, refs, c, float(ec[0]), e0
+
+
+def _pieces(h, s, f, refs, c, ecur, e0, cand):
+    m = f[np.ix_(cand, cand)] - e0 * s[np.ix_(cand, cand)]
+    p = {"e0": e0, "s_a0": s[np.ix_(cand, refs)] @ c, "s_0a": s[np.ix_(refs, cand)].T @ c,
+         "f_a0": f[np.ix_(cand, refs)] @ c, "f_0a": f[np.ix_(refs, cand)].T @ c}
+    v = h[np.ix_(cand, refs)] @ c - ecur * p["s_a0"]
+    return m, p, v
+
+
+@pytest.mark.parametrize("kind", ["woodbury", "diag"])
+def test_pt2_single_parent_candidates(snoci_system, kind):
+    """Candidates of one parent (orthonormal among themselves): a unique solution, reached in
+    a few iterations by both the GPU and the CPU GMRES."""
+    system, basis, h, s, f, refs, c, ecur, e0 = snoci_system
+    cand = np.nonzero((basis["parent"] == 0) & ((basis["rank_a"] + basis["rank_b"]) > 0))[0].astype(np.uint32)
+    m, p, v = _pieces(h, s, f, refs, c, ecur, e0, cand)
+    pre = PT.preconditioner(np.diag(m), p, kind)
+    x_ref, res_ref, it_ref, _ = PT.gmres(lambda z: PT.apply_omega(m, p, z), pre, -v, max_iter=100, restart=30,
+                                         res_tol=1e-10)
+    with nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8).build() as w:
+        w.set_basis(basis)
+        w.update_fock(system.h, system.h)
+        with nociwick.Pt2(w, cand, e0) as pt:
+            xv = np.random.default_rng(1).normal(size=cand.shape[0])
+            assert np.max(np.abs(pt.apply_m(xv) - m @ xv)) <= 1e-10
+            x, info = pt.solve(e0, p["s_a0"], p["s_0a"], p["f_a0"], p["f_0a"], -v, max_iter=100, restart=30,
+                               res_tol=1e-10, preconditioner=kind)
+    assert info["converged"] and info["residual_rms"] <= 1e-10
+    assert abs(info["iterations"] - it_ref) <= 1
+    assert np.max(np.abs(x - x_ref)) <= 1e-8
+
+
+def test_pt2_full_candidate_pool(snoci_system):
+    """All non-reference determinants as candidates: the pool is linearly dependent (singular
+    projected operator), so GMRES stops on its iteration limit; the GPU mat-vec matches the
+    dense product and E_PT2 agrees with the CPU restatement."""
+    system, basis, h, s, f, refs, c, ecur, e0 = snoci_system
+    cand = np.setdiff1d(np.arange(basis.shape[0]), refs).astype(np.uint32)
+    m, p, v = _pieces(h, s, f, refs, c, ecur, e0, cand)
+    a = np.array([PT.apply_omega(m, p, e) for e in np.eye(cand.shape[0])]).T
+    pre = PT.preconditioner(np.diag(m), p, "woodbury")
+    x_ref, _, _, _ = PT.gmres(lambda z: PT.apply_omega(m, p, z), pre, -v, max_iter=120, restart=40, res_tol=1e-10)
+    with nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8).build() as w:
+        w.set_basis(basis)
+        w.update_fock(system.h, system.h)
+        with nociwick.Pt2(w, cand, e0) as pt:
+            xv = np.random.default_rng(2).normal(size=cand.shape[0])
+            y = pt.apply_m(xv)
+            x, info = pt.solve(e0, p["s_a0"], p["s_0a"], p["f_a0"], p["f_0a"], -v, max_iter=120, restart=40,
+                               res_tol=1e-10)
+    assert np.max(np.abs(y - m @ xv)) <= 1e-9 * max(1.0, np.abs(m @ xv).max())
+    ept2 = x @ a @ x + 2 * x @ v
+    ept2_ref = x_ref @ a @ x_ref + 2 * x_ref @ v
+    assert abs(ept2 - ept2_ref) <= 1e-7
+    assert np.linalg.norm(a @ x + v) / np.sqrt(cand.shape[0]) <= 1e-5
