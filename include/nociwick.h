@@ -268,6 +268,50 @@ NW_API nw_status nw_qmc_set_populations(nw_qmc* q, const double* populations);
 NW_API nw_status nw_qmc_cycle_delta(nw_qmc* q, uint64_t cycle, double* delta);
 NW_API nw_status nw_qmc_destroy(nw_qmc* q);
 
+/* Learned spawning proposal (no counterpart in the reference, which offers uniform,
+ * heat-bath and overlap-weighted generators, src/input/qmc.rs:10).  Children are grouped into
+ * bins (child reference x (rank_a, rank_b) class); a small MLP (descriptor of the parent:
+ * one-hot reference, one-hot ranks, changed orbitals -> 128 -> 128 -> bins, ReLU, BF16 weights,
+ * FP32 accumulation) gives p(bin | parent); a child is drawn from the mixture
+ *   pgen = mix / (N - 1) + (1 - mix) p(bin | parent) / |bin without the parent|,
+ * so every attempt still carries its exact generation probability and the spawn stays
+ * unbiased.  The network is trained on the GPU (own forward, backward and Adam kernels) by the
+ * weighted cross entropy -sum w log p(bin | parent) over harvested attempts with
+ * w = |H - E^S S| / ((N - 1) pgen), whose minimiser puts each bin's probability in proportion
+ * to its coupling mass.  Needs at most 8 references. */
+typedef struct nw_mlp_opts {
+    int32_t epochs;             /* passes over the harvested attempts                         */
+    int32_t batch;              /* rows per Adam step (<= 4096)                               */
+    double lr;                  /* Adam learning rate                                         */
+    uint64_t seed;              /* minibatch draws                                            */
+} nw_mlp_opts;
+
+typedef struct nw_mlp_report {
+    double loss_first;          /* loss of the first and last minibatch                        */
+    double loss_last;
+    uint64_t samples;           /* harvested attempts used                                     */
+    int32_t steps;
+    int32_t pad;
+} nw_mlp_report;
+
+/* Record (parent, child bin, weight) of every attempt of the following runs (enable = 1 clears
+ * the buffer of 4,194,304 attempts; later attempts beyond it are not recorded). */
+NW_API nw_status nw_qmc_harvest(nw_qmc* q, int32_t enable);
+/* Train the proposal network on the harvested attempts and rebuild p(bin | parent) for every
+ * determinant. */
+NW_API nw_status nw_qmc_train_proposal(nw_qmc* q, const nw_mlp_opts* opts, nw_mlp_report* rep);
+/* Uniform generator (learned = 0) or the learned mixture with uniform weight mix in (0, 1]. */
+NW_API nw_status nw_qmc_set_generator(nw_qmc* q, int32_t learned, double mix);
+/* Network shape, parameters (layout W1[128][din], b1, W2[128][128], b2, W3[nbin][128], b3),
+ * and the loss and parameter gradients of a given batch (for checks of the kernels). */
+NW_API nw_status nw_qmc_proposal_dims(nw_qmc* q, int32_t* din, int32_t* nbin, uint64_t* nparams);
+NW_API nw_status nw_qmc_mlp_params(nw_qmc* q, float* params);
+NW_API nw_status nw_qmc_set_mlp_params(nw_qmc* q, const float* params);
+NW_API nw_status nw_qmc_mlp_loss_grad(nw_qmc* q, const uint32_t* parents, const uint32_t* bins, const float* w,
+                                      int32_t n, double* loss, float* grads);
+/* p(bin | det) of the current network (nbin values; bins without a child of det are 0). */
+NW_API nw_status nw_qmc_proposal_probs(nw_qmc* q, uint32_t det, double* probs);
+
 /* ---------------------------------------------------------------------------------------
  * NOCI-PT2 / SNOCI linear solve: the candidate-candidate shifted Fock matrix M = F - E0 S
  * stored on the device (packed upper triangle, n (n + 1) / 2 doubles), its mat-vec, and

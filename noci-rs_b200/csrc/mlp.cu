@@ -1,0 +1,215 @@
+// Small MLP of the learned QMC proposal: forward, backward and Adam kernels (FP32 compute,
+// BF16 weight copies in the products, FP32 accumulation).  The network is tiny (din x 128,
+// 128 x 128, 128 x nout) and runs once per training step and once per determinant when the
+// proposal table is rebuilt, so one tiled product kernel serves every layer and pass.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "internal.cuh"
+#include "mlp.cuh"
+#include "qmc_math.cuh"
+
+namespace nw {
+namespace {
+
+constexpr int kT = 64;   // output tile
+constexpr int kL = 16;   // reduction chunk
+
+__device__ __forceinline__ float to_f(float v) { return v; }
+__device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+enum Epi { kPlain = 0, kBiasRelu = 1, kBias = 2, kReluMask = 3 };
+
+// C[M x N] = epi(A[M x L] B[L x N]); A[i][l] = A[i * asr + l * asc], B[l][j] = B[l * bsr + j * bsc].
+template <typename TB>
+__global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int L, const float* __restrict__ A, long asr, long asc,
+                                                   const TB* __restrict__ B, long bsr, long bsc, float* __restrict__ C,
+                                                   int ldc, int epi, const float* __restrict__ bias,
+                                                   const float* __restrict__ mask) {
+  __shared__ float As[kL][kT + 1];
+  __shared__ float Bs[kL][kT + 1];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int row0 = blockIdx.y * kT, col0 = blockIdx.x * kT;
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+  for (int l0 = 0; l0 < L; l0 += kL) {
+    for (int e = threadIdx.x; e < kT * kL; e += 256) {
+      const int r = e / kL, c = e % kL, gr = row0 + r, gc = l0 + c;
+      As[c][r] = (gr < M && gc < L) ? A[gr * asr + gc * asc] : 0.0f;
+    }
+    for (int e = threadIdx.x; e < kT * kL; e += 256) {
+      const int r = e / kT, c = e % kT, gr = l0 + r, gc = col0 + c;
+      Bs[r][c] = (gr < L && gc < N) ? to_f(B[gr * bsr + gc * bsc]) : 0.0f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kL; ++k) {
+      float a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[k][ty * 4 + i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[k][tx * 4 + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = row0 + ty * 4 + i, c = col0 + tx * 4 + j;
+      if (r >= M || c >= N) continue;
+      float v = acc[i][j];
+      if (epi == kBiasRelu) v = fmaxf(v + bias[c], 0.0f);
+      if (epi == kBias) v += bias[c];
+      if (epi == kReluMask) v = mask[(size_t)r * ldc + c] > 0.0f ? v : 0.0f;
+      C[(size_t)r * ldc + c] = v;
+    }
+}
+
+// out[j] = sum_r X[r][j] (column sums of a B x N matrix).
+__global__ void colsum_kernel(const float* __restrict__ x, int B, int N, float* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  float s = 0.0f;
+  for (int r = 0; r < B; ++r) s += x[(size_t)r * N + j];
+  out[j] = s;
+}
+
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, size_t n, float lr, float c1, float c2) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = 0.9f * m[i] + 0.1f * gi;
+    const float vi = 0.999f * v[i] + 0.001f * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + 1e-8f);
+  }
+}
+
+__global__ void to_bf16_kernel(const float* __restrict__ p, size_t n, __nv_bfloat16* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = __float2bfloat16_rn(p[i]);
+}
+
+template <typename TB>
+nw_status gemm(nw_ctx* ctx, int M, int N, int L, const float* A, long asr, long asc, const TB* B, long bsr, long bsc,
+               float* C, int ldc, int epi, const float* bias, const float* mask, cudaStream_t s) {
+  const dim3 grid((N + kT - 1) / kT, (M + kT - 1) / kT);
+  gemm_kernel<TB><<<grid, 256, 0, s>>>(M, N, L, A, asr, asc, B, bsr, bsc, C, ldc, epi, bias, mask);
+  NW_CUDA(ctx, cudaGetLastError());
+  return NW_OK;
+}
+
+}  // namespace
+
+size_t mlp_param_count(int din, int nout) {
+  return (size_t)kMlpWidth * din + kMlpWidth + (size_t)kMlpWidth * kMlpWidth + kMlpWidth + (size_t)nout * kMlpWidth +
+         nout;
+}
+
+nw_status mlp_create(nw_ctx* ctx, Mlp* m, int din, int nout, int bcap, uint64_t seed) {
+  m->din = din;
+  m->nout = nout;
+  m->bcap = bcap;
+  m->nparams = mlp_param_count(din, nout);
+  const size_t np = m->nparams;
+  float** bufs[] = {&m->params, &m->grads, &m->adam_m, &m->adam_v};
+  for (float** b : bufs)
+    if (cudaMalloc(b, sizeof(float) * np) != cudaSuccess) return fail(ctx, NW_ERR_ALLOC, "MLP parameters");
+  if (cudaMalloc(&m->wbf, sizeof(__nv_bfloat16) * np) != cudaSuccess) return fail(ctx, NW_ERR_ALLOC, "MLP weights");
+  struct Act {
+    float** p;
+    size_t n;
+  } acts[] = {{&m->x, (size_t)bcap * din},   {&m->h1, (size_t)bcap * kMlpWidth}, {&m->h2, (size_t)bcap * kMlpWidth},
+              {&m->z, (size_t)bcap * nout}, {&m->d2, (size_t)bcap * kMlpWidth}, {&m->d1, (size_t)bcap * kMlpWidth}};
+  for (const Act& a : acts)
+    if (cudaMalloc(a.p, sizeof(float) * std::max<size_t>(a.n, 1)) != cudaSuccess)
+      return fail(ctx, NW_ERR_ALLOC, "MLP activations");
+  // uniform +-sqrt(6 / fan_in) weights, zero biases
+  std::vector<float> h(np, 0.0f);
+  struct Blk {
+    size_t off, n;
+    int fan_in;
+  } w[] = {{m->off_w1(), (size_t)kMlpWidth * din, din},
+           {m->off_w2(), (size_t)kMlpWidth * kMlpWidth, kMlpWidth},
+           {m->off_w3(), (size_t)nout * kMlpWidth, kMlpWidth}};
+  for (const Blk& b : w) {
+    const double a = std::sqrt(6.0 / b.fan_in);
+    for (size_t i = 0; i < b.n; ++i) h[b.off + i] = (float)((2.0 * nwq::uniform1(seed, 0, b.off + i, 7) - 1.0) * a);
+  }
+  NW_CUDA(ctx, cudaMemcpy(m->params, h.data(), sizeof(float) * np, cudaMemcpyHostToDevice));
+  NW_CUDA(ctx, cudaMemset(m->adam_m, 0, sizeof(float) * np));
+  NW_CUDA(ctx, cudaMemset(m->adam_v, 0, sizeof(float) * np));
+  NW_CUDA(ctx, cudaMemset(m->grads, 0, sizeof(float) * np));
+  m->adam_t = 0;
+  return mlp_sync_bf16(ctx, m, nullptr);
+}
+
+void mlp_destroy(Mlp* m) {
+  void* bufs[] = {m->params, m->grads, m->adam_m, m->adam_v, m->wbf, m->x, m->h1, m->h2, m->z, m->d2, m->d1};
+  for (void* p : bufs)
+    if (p) cudaFree(p);
+  *m = Mlp{};
+}
+
+nw_status mlp_sync_bf16(nw_ctx* ctx, Mlp* m, cudaStream_t s) {
+  to_bf16_kernel<<<256, 256, 0, s>>>(m->params, m->nparams, m->wbf);
+  NW_CUDA(ctx, cudaGetLastError());
+  return NW_OK;
+}
+
+nw_status mlp_forward(nw_ctx* ctx, Mlp* m, int B, cudaStream_t s) {
+  const int W = kMlpWidth;
+  const float* P = m->params;
+  nw_status st = gemm(ctx, B, W, m->din, m->x, m->din, 1, m->wbf + m->off_w1(), 1, m->din, m->h1, W, kBiasRelu,
+                      P + m->off_b1(), nullptr, s);
+  if (st == NW_OK)
+    st = gemm(ctx, B, W, W, m->h1, W, 1, m->wbf + m->off_w2(), 1, W, m->h2, W, kBiasRelu, P + m->off_b2(), nullptr, s);
+  if (st == NW_OK)
+    st = gemm(ctx, B, m->nout, W, m->h2, W, 1, m->wbf + m->off_w3(), 1, W, m->z, m->nout, kBias, P + m->off_b3(),
+              nullptr, s);
+  return st;
+}
+
+nw_status mlp_backward(nw_ctx* ctx, Mlp* m, int B, cudaStream_t s) {
+  const int W = kMlpWidth, K = m->nout, D = m->din;
+  float* G = m->grads;
+  // layer 3: dW3 = dZ^T H2, db3 = colsum dZ, d2 = (dZ W3) o [H2 > 0]
+  nw_status st = gemm(ctx, K, W, B, m->z, 1, K, m->h2, W, 1, G + m->off_w3(), W, kPlain, nullptr, nullptr, s);
+  colsum_kernel<<<(K + 127) / 128, 128, 0, s>>>(m->z, B, K, G + m->off_b3());
+  if (st == NW_OK)
+    st = gemm(ctx, B, W, K, m->z, K, 1, m->wbf + m->off_w3(), W, 1, m->d2, W, kReluMask, nullptr, m->h2, s);
+  // layer 2
+  if (st == NW_OK) st = gemm(ctx, W, W, B, m->d2, 1, W, m->h1, W, 1, G + m->off_w2(), W, kPlain, nullptr, nullptr, s);
+  colsum_kernel<<<1, 128, 0, s>>>(m->d2, B, W, G + m->off_b2());
+  if (st == NW_OK)
+    st = gemm(ctx, B, W, W, m->d2, W, 1, m->wbf + m->off_w2(), W, 1, m->d1, W, kReluMask, nullptr, m->h1, s);
+  // layer 1
+  if (st == NW_OK) st = gemm(ctx, W, D, B, m->d1, 1, W, m->x, D, 1, G + m->off_w1(), D, kPlain, nullptr, nullptr, s);
+  colsum_kernel<<<1, 128, 0, s>>>(m->d1, B, W, G + m->off_b1());
+  if (st == NW_OK) NW_CUDA(ctx, cudaGetLastError());
+  return st;
+}
+
+nw_status mlp_adam(nw_ctx* ctx, Mlp* m, float lr, cudaStream_t s) {
+  m->adam_t += 1;
+  const float c1 = (float)(1.0 / (1.0 - std::pow(0.9, m->adam_t)));
+  const float c2 = (float)(1.0 / (1.0 - std::pow(0.999, m->adam_t)));
+  adam_kernel<<<256, 256, 0, s>>>(m->params, m->grads, m->adam_m, m->adam_v, m->nparams, lr, c1, c2);
+  NW_CUDA(ctx, cudaGetLastError());
+  return mlp_sync_bf16(ctx, m, s);
+}
+
+}  // namespace nw

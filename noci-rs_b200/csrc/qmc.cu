@@ -20,12 +20,14 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <new>
 #include <string>
 #include <type_traits>
 #include <vector>
 
 #include "internal.cuh"
+#include "mlp.cuh"
 #include "qmc_math.cuh"
 
 namespace {
@@ -34,6 +36,10 @@ constexpr int kReportRing = 4096;   // device report slots between host copies
 constexpr int kBlockThreads = 256;
 constexpr int kStatBlocks = 296;     // 2 x 148 SMs
 constexpr int kStats = 6;            // nw, nref, num, den, sampled norm, nocc
+constexpr uint32_t kRankBins = 25;   // (rank_a, rank_b) classes per child reference
+constexpr int kLearnMaxRefs = 8;     // learned proposal: at most 8 x 25 bins
+constexpr uint64_t kHarvestCap = 1ull << 22;
+constexpr int kTrainBatchCap = 4096;
 
 struct QmcState {
   double shift;
@@ -53,7 +59,46 @@ struct QmcParams {
   uint64_t seed;
   double dt, target, c_sample, c_spawn, damping;
   int32_t ncycles, prop;
+  int32_t gen;      // 0: uniform generator, 1: learned proposal mixed with the uniform one
+  int32_t harvest;  // record the attempts for training the proposal
+  double mix;       // weight of the uniform generator in the learned mixture
+  uint32_t nbin;    // proposal bins (child reference x rank class)
+  uint32_t pad;
+  uint64_t hcap;    // harvest buffer capacity
 };
+
+// One harvested attempt: parent, the child's bin and the weight |H - E^S S| / ((N - 1) pgen),
+// an unbiased sample of the per-bin coupling mass sum_{child in bin} |H - E^S S|.
+struct HarvestSample {
+  uint32_t parent;
+  uint32_t bin;
+  float w;
+  uint32_t pad;
+};
+
+// Learned proposal: bins and the cumulative bin probabilities of every parent.
+struct Proposal {
+  const float* cdf;          // [ndet][nbin] cumulative p(bin | parent)
+  const uint32_t* det_bin;   // [ndet] bin of each determinant
+  const uint32_t* bin_off;   // [nbin + 1] offsets into bin_mem
+  const uint32_t* bin_mem;   // [ndet] determinants grouped by bin
+  const uint32_t* pos;       // [ndet] position of a determinant inside its bin
+  HarvestSample* samples;    // [hcap]
+  unsigned long long* nsamples;
+};
+
+// Determinants of bin b other than the parent g.
+__host__ __device__ __forceinline__ uint32_t bin_size_without(const Proposal& pr, uint32_t b, uint32_t g) {
+  return pr.bin_off[b + 1] - pr.bin_off[b] - (pr.det_bin[g] == b ? 1u : 0u);
+}
+
+// pgen(child | parent) of the learned mixture.
+__device__ __forceinline__ double learned_pgen(const QmcParams& q, const Proposal& pr, uint32_t g, uint32_t lam) {
+  const uint32_t b = pr.det_bin[lam];
+  const float* c = pr.cdf + (uint64_t)g * q.nbin;
+  const double pb = (double)c[b] - (b > 0 ? (double)c[b - 1] : 0.0);
+  return q.mix / (double)(q.ndet - 1) + (1.0 - q.mix) * pb / (double)bin_size_without(pr, b, g);
+}
 
 template <class T>
 T* dalloc(size_t count, bool* ok) {
@@ -105,32 +150,69 @@ __device__ __forceinline__ uint64_t owner_of(const uint32_t* __restrict__ off, u
   return lo;
 }
 
-__global__ void qmc_spawn_kernel(QmcParams q, const QmcState* __restrict__ st, const uint32_t* __restrict__ off,
-                                 const double* __restrict__ sampled, const uint32_t* __restrict__ na,
-                                 uint2* __restrict__ pairs, uint32_t* __restrict__ child, double* __restrict__ amp) {
+__global__ void qmc_spawn_kernel(QmcParams q, Proposal pr, const QmcState* __restrict__ st,
+                                 const uint32_t* __restrict__ off, const double* __restrict__ sampled,
+                                 const uint32_t* __restrict__ na, uint2* __restrict__ pairs, uint32_t* __restrict__ child,
+                                 uint32_t* __restrict__ parent, double* __restrict__ amp, double* __restrict__ pg) {
   const uint32_t n = st->npairs;
   const uint64_t cycle = st->cycle;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const uint64_t g = owner_of(off, q.ndet, t);
-    const uint64_t lam = nwq::uniform_child(g, q.ndet, nwq::uniform1(q.seed, cycle, t, nwq::kDrawChild));
+    double u0, u1;
+    nwq::uniform2(q.seed, cycle, t, nwq::kDrawChild, &u0, &u1);
+    uint64_t lam;
+    if (q.gen == 0) {
+      lam = nwq::uniform_child(g, q.ndet, u0);
+    } else {
+      double u2, u3;
+      nwq::uniform2(q.seed, cycle, t, nwq::kDrawChildBin, &u2, &u3);
+      if (u1 < q.mix) {
+        lam = nwq::uniform_child(g, q.ndet, u2);
+      } else {
+        // bin from the parent's cumulative probabilities, then uniformly inside the bin
+        const float* c = pr.cdf + g * q.nbin;
+        uint32_t b = 0;
+        while (b + 1 < q.nbin && !(u2 < (double)c[b])) ++b;
+        const uint32_t size = bin_size_without(pr, b, (uint32_t)g);
+        uint32_t idx = (uint32_t)(u3 * (double)size);
+        if (idx >= size) idx = size - 1;
+        if (pr.det_bin[g] == b && idx >= pr.pos[g]) ++idx;
+        lam = pr.bin_mem[pr.bin_off[b] + idx];
+      }
+      pg[t] = learned_pgen(q, pr, (uint32_t)g, (uint32_t)lam);
+    }
     pairs[t] = lam <= g ? make_uint2((uint32_t)lam, (uint32_t)g) : make_uint2((uint32_t)g, (uint32_t)lam);
     child[t] = (uint32_t)lam;
+    parent[t] = (uint32_t)g;
     amp[t] = sampled[g] / (double)na[g];
   }
 }
 
-__global__ void qmc_apply_kernel(QmcParams q, const QmcState* __restrict__ st, const double2* __restrict__ hs,
-                                 const uint32_t* __restrict__ child, const double* __restrict__ amp,
-                                 double* __restrict__ delta) {
+__global__ void qmc_apply_kernel(QmcParams q, Proposal pr, const QmcState* __restrict__ st,
+                                 const double2* __restrict__ hs, const uint32_t* __restrict__ child,
+                                 const uint32_t* __restrict__ parent, const double* __restrict__ amp,
+                                 const double* __restrict__ pg, double* __restrict__ delta) {
   const uint32_t n = st->npairs;
   const uint64_t cycle = st->cycle;
   const double es = st->shift;
-  const double pgen = 1.0 / (double)(q.ndet - 1);
+  const double pu = 1.0 / (double)(q.ndet - 1);
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const double2 v = hs[t];
+    const double pgen = q.gen == 0 ? pu : pg[t];
     const double raw = nwq::spawn_amplitude(q.prop, q.dt, es, v.x, v.y, amp[t], pgen);
     const double dn = nwq::fri(raw, q.c_spawn, nwq::uniform1(q.seed, cycle, t, nwq::kDrawSpawn));
     if (dn != 0.0) atomicAdd(delta + child[t], dn);
+    if (q.harvest) {
+      const unsigned long long k = atomicAdd(pr.nsamples, 1ull);
+      if (k < q.hcap) {
+        HarvestSample hsmp;
+        hsmp.parent = parent[t];
+        hsmp.bin = pr.det_bin[child[t]];
+        hsmp.w = (float)(fabs(v.x - nwq::overlap_shift(q.prop, es) * v.y) * pu / pgen);
+        hsmp.pad = 0;
+        pr.samples[k] = hsmp;
+      }
+    }
   }
 }
 
@@ -215,6 +297,113 @@ __global__ void qmc_pairs_kernel(uint64_t n, uint32_t bra, uint2* __restrict__ p
     pairs[i] = diagonal ? make_uint2((uint32_t)i, (uint32_t)i) : make_uint2(bra, (uint32_t)i);
 }
 
+// ---------------------------------------------------------------------------------------
+// Learned proposal: descriptors, training batches, weighted cross entropy, proposal table.
+// Descriptor of a determinant (din floats, zero-padded): one-hot parent reference, one-hot
+// alpha and beta excitation ranks (0..4), and per spin the indicator of the orbitals whose
+// occupation the excitation changes (its holes and particles).
+// ---------------------------------------------------------------------------------------
+__global__ void feature_kernel(const nw_det* __restrict__ dets, const uint32_t* __restrict__ rows, uint32_t row0,
+                               int B, int din, int nref, int nmo, float* __restrict__ x) {
+  const int r = blockIdx.x;
+  if (r >= B) return;
+  float* xr = x + (size_t)r * din;
+  for (int j = threadIdx.x; j < din; j += blockDim.x) xr[j] = 0.0f;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const uint32_t g = rows ? rows[r] : row0 + (uint32_t)r;
+  const nw_det d = dets[g];
+  xr[d.parent] = 1.0f;
+  xr[nref + d.rank_a] = 1.0f;
+  xr[nref + 5 + d.rank_b] = 1.0f;
+  const int base_a = nref + 10, base_b = nref + 10 + nmo;
+  for (int k = 0; k < d.rank_a; ++k) {
+    xr[base_a + d.idx_a[k]] = 1.0f;
+    xr[base_a + d.idx_a[4 + k]] = 1.0f;
+  }
+  for (int k = 0; k < d.rank_b; ++k) {
+    xr[base_b + d.idx_b[k]] = 1.0f;
+    xr[base_b + d.idx_b[4 + k]] = 1.0f;
+  }
+}
+
+// Random minibatch of harvested samples (with replacement).
+__global__ void gather_batch_kernel(const HarvestSample* __restrict__ samples, uint64_t ns, uint64_t seed,
+                                    uint64_t step, int B, uint32_t* __restrict__ rows, uint32_t* __restrict__ tbin,
+                                    float* __restrict__ w) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= B) return;
+  uint64_t k = (uint64_t)(nwq::uniform1(seed, step, (uint64_t)r, nwq::kDrawTrain) * (double)ns);
+  if (k >= ns) k = ns - 1;
+  const HarvestSample h = samples[k];
+  rows[r] = h.parent;
+  tbin[r] = h.bin;
+  w[r] = h.w;
+}
+
+__global__ void sum_kernel(const float* __restrict__ w, int B, float* __restrict__ out) {
+  __shared__ float red[256];
+  float a = 0.0f;
+  for (int r = threadIdx.x; r < B; r += blockDim.x) a += w[r];
+  red[threadIdx.x] = a;
+  __syncthreads();
+  for (int k = 128; k > 0; k >>= 1) {
+    if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
+}
+
+// Softmax over the bins that hold a child of the row's parent; in place, z becomes
+// dL/dz of L = -sum_r w_r log p(bin_r | parent_r) / sum_r w_r.
+__global__ void ce_kernel(float* __restrict__ z, int B, int K, const uint32_t* __restrict__ rows,
+                          const uint32_t* __restrict__ tbin, const float* __restrict__ w,
+                          const float* __restrict__ wsum, Proposal pr, double* __restrict__ loss) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= B) return;
+  float* zr = z + (size_t)r * K;
+  const uint32_t g = rows[r];
+  float mx = -INFINITY;
+  for (int k = 0; k < K; ++k)
+    if (bin_size_without(pr, (uint32_t)k, g) > 0) mx = fmaxf(mx, zr[k]);
+  float se = 0.0f;
+  for (int k = 0; k < K; ++k)
+    if (bin_size_without(pr, (uint32_t)k, g) > 0) se += __expf(zr[k] - mx);
+  const float scale = w[r] / *wsum;
+  const uint32_t t = tbin[r];
+  atomicAdd(loss, -(double)scale * (double)(zr[t] - mx - __logf(se)));
+  for (int k = 0; k < K; ++k) {
+    const bool valid = bin_size_without(pr, (uint32_t)k, g) > 0;
+    const float p = valid ? __expf(zr[k] - mx) / se : 0.0f;
+    zr[k] = valid ? scale * (p - (k == (int)t ? 1.0f : 0.0f)) : 0.0f;
+  }
+}
+
+// Cumulative bin probabilities of determinants row0 .. row0 + B - 1 from their logits.
+__global__ void table_kernel(const float* __restrict__ z, int B, int K, uint32_t row0, Proposal pr,
+                             float* __restrict__ cdf) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= B) return;
+  const float* zr = z + (size_t)r * K;
+  const uint32_t g = row0 + (uint32_t)r;
+  float mx = -INFINITY;
+  int last = -1;
+  for (int k = 0; k < K; ++k)
+    if (bin_size_without(pr, (uint32_t)k, g) > 0) {
+      mx = fmaxf(mx, zr[k]);
+      last = k;
+    }
+  double se = 0.0;
+  for (int k = 0; k < K; ++k)
+    if (bin_size_without(pr, (uint32_t)k, g) > 0) se += exp((double)(zr[k] - mx));
+  float* c = cdf + (uint64_t)g * K;
+  double acc = 0.0;
+  for (int k = 0; k < K; ++k) {
+    if (bin_size_without(pr, (uint32_t)k, g) > 0) acc += exp((double)(zr[k] - mx)) / se;
+    c[k] = k >= last ? 1.0f : (float)acc;
+  }
+}
+
 inline int grid_for(uint64_t work, int per_sm = 8) {
   uint64_t g = (work + kBlockThreads - 1) / kBlockThreads;
   g = std::min<uint64_t>(g, 148ull * per_sm);
@@ -245,6 +434,8 @@ struct nw_qmc {
   uint2* pairs = nullptr;
   uint32_t* child = nullptr;
   double* amp = nullptr;
+  uint32_t* parent = nullptr;
+  double* pg = nullptr;
   double2* hs = nullptr;
   double* partial = nullptr;
   nw_qmc_report* ring = nullptr;
@@ -253,6 +444,18 @@ struct nw_qmc {
   uint64_t nkeys = 0;
   nw::SortScratch S{};
   std::vector<void*> owned;
+  // learned proposal
+  Proposal pr{};
+  float* cdf = nullptr;
+  bool learnable = false;    // nref small enough for the bin output layer
+  bool table_ready = false;  // cdf built by a training run
+  std::vector<uint32_t> h_det_bin, h_bin_off;  // host copies of the bins (argument checks)
+  nw::Mlp mlp{};
+  uint32_t* trows = nullptr;  // training batch: parents, target bins, weights, weight sum
+  uint32_t* tbin = nullptr;
+  float* tw = nullptr;
+  float* twsum = nullptr;
+  double* tloss = nullptr;
 };
 
 namespace {
@@ -269,13 +472,14 @@ nw_status enqueue_cycle(nw_qmc* q) {
   nw_status st = nw::scan_exclusive(ctx, q->na, nd, q->off, q->tsum, s);
   if (st != NW_OK) return st;
   qmc_count_kernel<<<1, 1, 0, s>>>(q->q, q->st, q->off);
-  qmc_spawn_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(q->q, q->st, q->off, q->sampled, q->na, q->pairs,
-                                                                q->child, q->amp);
+  qmc_spawn_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(q->q, q->pr, q->st, q->off, q->sampled, q->na,
+                                                                q->pairs, q->child, q->parent, q->amp, q->pg);
   NW_CUDA(ctx, cudaGetLastError());
   st = nw::launch_sorted(ctx, q->P, q->nkeys, reinterpret_cast<const uint32_t*>(q->pairs), q->q.cap,
                          reinterpret_cast<double*>(q->hs), q->S, s, nullptr, nw::EvalMode::kHS, &q->st->npairs);
   if (st != NW_OK) return st;
-  qmc_apply_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(q->q, q->st, q->hs, q->child, q->amp, q->delta);
+  qmc_apply_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(q->q, q->pr, q->st, q->hs, q->child, q->parent,
+                                                                q->amp, q->pg, q->delta);
   qmc_next_cycle_kernel<<<1, 1, 0, s>>>(q->st);
   NW_CUDA(ctx, cudaGetLastError());
   return NW_OK;
@@ -305,6 +509,7 @@ nw_status reset_reference_stats(nw_qmc* q) {
 }
 
 void release(nw_qmc* q) {
+  nw::mlp_destroy(&q->mlp);
   if (q->graph) cudaGraphExecDestroy(q->graph);
   if (q->ev0) cudaEventDestroy(q->ev0);
   if (q->ev1) cudaEventDestroy(q->ev1);
@@ -314,9 +519,172 @@ void release(nw_qmc* q) {
   delete q;
 }
 
+// Loss and parameter gradients of the weighted cross entropy for the batch held in
+// trows / tbin / tw (B rows); the loss goes to *loss_out when it is not null.
+nw_status batch_loss_grad(nw_qmc* q, int B, double* loss_out) {
+  nw_ctx* ctx = q->ctx;
+  const cudaStream_t s = q->stream;
+  nw::Mlp& m = q->mlp;
+  feature_kernel<<<B, 128, 0, s>>>(ctx->d_dets, q->trows, 0, B, m.din, ctx->nref, ctx->nmo, m.x);
+  NW_CUDA(ctx, cudaGetLastError());
+  nw_status st = nw::mlp_forward(ctx, &m, B, s);
+  if (st != NW_OK) return st;
+  sum_kernel<<<1, 256, 0, s>>>(q->tw, B, q->twsum);
+  NW_CUDA(ctx, cudaMemsetAsync(q->tloss, 0, sizeof(double), s));
+  ce_kernel<<<(B + 127) / 128, 128, 0, s>>>(m.z, B, m.nout, q->trows, q->tbin, q->tw, q->twsum, q->pr, q->tloss);
+  NW_CUDA(ctx, cudaGetLastError());
+  if ((st = nw::mlp_backward(ctx, &m, B, s)) != NW_OK) return st;
+  if (loss_out) {
+    NW_CUDA(ctx, cudaMemcpyAsync(loss_out, q->tloss, sizeof(double), cudaMemcpyDeviceToHost, s));
+    NW_CUDA(ctx, cudaStreamSynchronize(s));
+  }
+  return NW_OK;
+}
+
+// Cumulative bin probabilities of every determinant from the current network.
+nw_status build_table(nw_qmc* q) {
+  nw_ctx* ctx = q->ctx;
+  const cudaStream_t s = q->stream;
+  nw::Mlp& m = q->mlp;
+  for (uint64_t r0 = 0; r0 < q->q.ndet; r0 += (uint64_t)m.bcap) {
+    const int B = (int)std::min<uint64_t>((uint64_t)m.bcap, q->q.ndet - r0);
+    feature_kernel<<<B, 128, 0, s>>>(ctx->d_dets, nullptr, (uint32_t)r0, B, m.din, ctx->nref, ctx->nmo, m.x);
+    NW_CUDA(ctx, cudaGetLastError());
+    const nw_status st = nw::mlp_forward(ctx, &m, B, s);
+    if (st != NW_OK) return st;
+    table_kernel<<<(B + 127) / 128, 128, 0, s>>>(m.z, B, m.nout, (uint32_t)r0, q->pr, q->cdf);
+    NW_CUDA(ctx, cudaGetLastError());
+  }
+  NW_CUDA(ctx, cudaStreamSynchronize(s));
+  q->table_ready = true;
+  return NW_OK;
+}
+
+void invalidate_graph(nw_qmc* q) {
+  if (q->graph) cudaGraphExecDestroy(q->graph);
+  q->graph = nullptr;
+}
+
 }  // namespace
 
 extern "C" {
+
+nw_status nw_qmc_harvest(nw_qmc* q, int32_t enable) {
+  if (!q) return NW_ERR_INVALID;
+  if (!q->learnable) return qmc_fail(q, NW_ERR_UNSUPPORTED, "learned proposal needs at most 8 references");
+  NW_CUDA(q->ctx, cudaSetDevice(q->ctx->device));
+  if (enable) NW_CUDA(q->ctx, cudaMemsetAsync(q->pr.nsamples, 0, sizeof(unsigned long long), q->stream));
+  NW_CUDA(q->ctx, cudaStreamSynchronize(q->stream));
+  q->q.harvest = enable ? 1 : 0;
+  invalidate_graph(q);
+  return NW_OK;
+}
+
+nw_status nw_qmc_train_proposal(nw_qmc* q, const nw_mlp_opts* opts, nw_mlp_report* rep) {
+  if (!q || !opts || !rep) return NW_ERR_INVALID;
+  if (!q->learnable) return qmc_fail(q, NW_ERR_UNSUPPORTED, "learned proposal needs at most 8 references");
+  if (opts->epochs < 0 || opts->batch < 1 || opts->batch > kTrainBatchCap || !(opts->lr > 0.0))
+    return qmc_fail(q, NW_ERR_INVALID, "invalid training options (batch <= 4096)");
+  nw_ctx* ctx = q->ctx;
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  unsigned long long count = 0;
+  NW_CUDA(ctx, cudaMemcpy(&count, q->pr.nsamples, sizeof(count), cudaMemcpyDeviceToHost));
+  const uint64_t ns = std::min<uint64_t>(count, kHarvestCap);
+  std::memset(rep, 0, sizeof(*rep));
+  rep->samples = ns;
+  if (ns == 0) return qmc_fail(q, NW_ERR_STATE, "no harvested attempts to train on (nw_qmc_harvest)");
+  const int B = opts->batch;
+  const uint64_t per_epoch = (ns + (uint64_t)B - 1) / (uint64_t)B;
+  const uint64_t steps = (uint64_t)opts->epochs * per_epoch;
+  for (uint64_t step = 0; step < steps; ++step) {
+    gather_batch_kernel<<<(B + 127) / 128, 128, 0, q->stream>>>(q->pr.samples, ns, opts->seed, step, B, q->trows,
+                                                                q->tbin, q->tw);
+    NW_CUDA(ctx, cudaGetLastError());
+    const bool report = step == 0 || step + 1 == steps;
+    double loss = 0.0;
+    nw_status st = batch_loss_grad(q, B, report ? &loss : nullptr);
+    if (st != NW_OK) return st;
+    if (step == 0) rep->loss_first = loss;
+    if (step + 1 == steps) rep->loss_last = loss;
+    if ((st = nw::mlp_adam(ctx, &q->mlp, (float)opts->lr, q->stream)) != NW_OK) return st;
+  }
+  rep->steps = (int32_t)steps;
+  return build_table(q);
+}
+
+nw_status nw_qmc_set_generator(nw_qmc* q, int32_t learned, double mix) {
+  if (!q || !(mix > 0.0) || !(mix <= 1.0)) return NW_ERR_INVALID;
+  if (learned && !q->table_ready) return qmc_fail(q, NW_ERR_STATE, "no trained proposal (nw_qmc_train_proposal)");
+  q->q.gen = learned ? 1 : 0;
+  q->q.mix = mix;
+  invalidate_graph(q);
+  return NW_OK;
+}
+
+nw_status nw_qmc_proposal_dims(nw_qmc* q, int32_t* din, int32_t* nbin, uint64_t* nparams) {
+  if (!q || !din || !nbin || !nparams) return NW_ERR_INVALID;
+  if (!q->learnable) return qmc_fail(q, NW_ERR_UNSUPPORTED, "learned proposal needs at most 8 references");
+  *din = q->mlp.din;
+  *nbin = q->mlp.nout;
+  *nparams = q->mlp.nparams;
+  return NW_OK;
+}
+
+nw_status nw_qmc_mlp_params(nw_qmc* q, float* params) {
+  if (!q || !params) return NW_ERR_INVALID;
+  if (!q->learnable) return qmc_fail(q, NW_ERR_UNSUPPORTED, "learned proposal needs at most 8 references");
+  NW_CUDA(q->ctx, cudaSetDevice(q->ctx->device));
+  NW_CUDA(q->ctx, cudaMemcpy(params, q->mlp.params, sizeof(float) * q->mlp.nparams, cudaMemcpyDeviceToHost));
+  return NW_OK;
+}
+
+nw_status nw_qmc_set_mlp_params(nw_qmc* q, const float* params) {
+  if (!q || !params) return NW_ERR_INVALID;
+  if (!q->learnable) return qmc_fail(q, NW_ERR_UNSUPPORTED, "learned proposal needs at most 8 references");
+  for (size_t i = 0; i < q->mlp.nparams; ++i)
+    if (!std::isfinite(params[i])) return qmc_fail(q, NW_ERR_INVALID, "non-finite parameter");
+  NW_CUDA(q->ctx, cudaSetDevice(q->ctx->device));
+  NW_CUDA(q->ctx, cudaMemcpy(q->mlp.params, params, sizeof(float) * q->mlp.nparams, cudaMemcpyHostToDevice));
+  nw_status st = nw::mlp_sync_bf16(q->ctx, &q->mlp, nullptr);
+  if (st != NW_OK) return st;
+  NW_CUDA(q->ctx, cudaDeviceSynchronize());
+  return build_table(q);
+}
+
+nw_status nw_qmc_mlp_loss_grad(nw_qmc* q, const uint32_t* parents, const uint32_t* bins, const float* w, int32_t n,
+                               double* loss, float* grads) {
+  if (!q || !parents || !bins || !w || !loss || !grads || n < 1) return NW_ERR_INVALID;
+  if (!q->learnable) return qmc_fail(q, NW_ERR_UNSUPPORTED, "learned proposal needs at most 8 references");
+  if (n > kTrainBatchCap) return qmc_fail(q, NW_ERR_UNSUPPORTED, "at most 4096 rows");
+  for (int32_t r = 0; r < n; ++r) {
+    if (parents[r] >= q->q.ndet || bins[r] >= q->q.nbin || !std::isfinite(w[r]) || w[r] < 0.0f)
+      return qmc_fail(q, NW_ERR_INVALID, "invalid training row");
+    const uint32_t b = bins[r];
+    if (q->h_bin_off[b + 1] - q->h_bin_off[b] - (q->h_det_bin[parents[r]] == b ? 1u : 0u) == 0)
+      return qmc_fail(q, NW_ERR_INVALID, "training row targets a bin without a child of its parent");
+  }
+  nw_ctx* ctx = q->ctx;
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  NW_CUDA(ctx, cudaMemcpy(q->trows, parents, sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+  NW_CUDA(ctx, cudaMemcpy(q->tbin, bins, sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+  NW_CUDA(ctx, cudaMemcpy(q->tw, w, sizeof(float) * n, cudaMemcpyHostToDevice));
+  nw_status st = batch_loss_grad(q, n, loss);
+  if (st != NW_OK) return st;
+  NW_CUDA(ctx, cudaMemcpy(grads, q->mlp.grads, sizeof(float) * q->mlp.nparams, cudaMemcpyDeviceToHost));
+  return NW_OK;
+}
+
+nw_status nw_qmc_proposal_probs(nw_qmc* q, uint32_t det, double* probs) {
+  if (!q || !probs) return NW_ERR_INVALID;
+  if (!q->table_ready) return qmc_fail(q, NW_ERR_STATE, "no trained proposal");
+  if (det >= q->q.ndet) return qmc_fail(q, NW_ERR_INVALID, "determinant index out of range");
+  std::vector<float> c(q->q.nbin);
+  NW_CUDA(q->ctx, cudaSetDevice(q->ctx->device));
+  NW_CUDA(q->ctx, cudaMemcpy(c.data(), q->cdf + (uint64_t)det * q->q.nbin, sizeof(float) * q->q.nbin,
+                             cudaMemcpyDeviceToHost));
+  for (uint32_t b = 0; b < q->q.nbin; ++b) probs[b] = (double)c[b] - (b > 0 ? (double)c[b - 1] : 0.0);
+  return NW_OK;
+}
 
 nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, const uint32_t* ref_idx,
                         uint64_t nref_idx, nw_qmc** out) {
@@ -358,7 +726,13 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
                    opts->spawn_cutoff,
                    opts->shift_damping,
                    opts->ncycles,
-                   opts->propagator};
+                   opts->propagator,
+                   0,
+                   0,
+                   0.1,
+                   (uint32_t)ctx->nref * kRankBins,
+                   0,
+                   kHarvestCap};
   bool ok = true;
   auto take = [&](auto*& p, size_t count) {
     using T = std::remove_reference_t<decltype(*p)>;
@@ -378,6 +752,8 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
   take(q->pairs, std::max<uint64_t>(cap, nd));
   take(q->child, cap);
   take(q->amp, cap);
+  take(q->parent, cap);
+  take(q->pg, cap);
   take(q->hs, std::max<uint64_t>(cap, nd));
   take(q->partial, (size_t)kStatBlocks * kStats);
   take(q->ring, kReportRing);
@@ -390,6 +766,53 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
   take(q->S.offsets, q->nkeys + 1);
   take(q->S.tsum, q->nkeys / 4096 + 1);
   take(q->S.flag, 64);
+  // learned-proposal bins: child reference x (rank_a, rank_b) class
+  q->learnable = ctx->nref <= kLearnMaxRefs;
+  std::vector<uint32_t> det_bin(nd), bin_off(q->q.nbin + 1, 0), bin_mem(nd), pos(nd);
+  if (q->learnable && ok) {
+    std::vector<uint16_t> desc(nd);
+    if (cudaMemcpy(desc.data(), ctx->d_desc, sizeof(uint16_t) * nd, cudaMemcpyDeviceToHost) != cudaSuccess) ok = false;
+    for (uint64_t g = 0; g < nd; ++g) {
+      const uint32_t par = desc[g] & 0xFF, ra = (desc[g] >> 8) & 15, rb = desc[g] >> 12;
+      det_bin[g] = par * kRankBins + ra * 5 + rb;
+      ++bin_off[det_bin[g] + 1];
+    }
+    for (uint32_t b = 0; b < q->q.nbin; ++b) bin_off[b + 1] += bin_off[b];
+    std::vector<uint32_t> fill(bin_off.begin(), bin_off.end() - 1);
+    for (uint64_t g = 0; g < nd; ++g) {
+      pos[g] = fill[det_bin[g]] - bin_off[det_bin[g]];
+      bin_mem[fill[det_bin[g]]++] = (uint32_t)g;
+    }
+    uint32_t *d_bin = nullptr, *d_off = nullptr, *d_mem = nullptr, *d_pos = nullptr;
+    take(d_bin, nd);
+    take(d_off, q->q.nbin + 1);
+    take(d_mem, nd);
+    take(d_pos, nd);
+    take(q->cdf, nd * q->q.nbin);
+    HarvestSample* samples = nullptr;
+    unsigned long long* nsamples = nullptr;
+    take(samples, kHarvestCap);
+    take(nsamples, 1);
+    take(q->trows, kTrainBatchCap);
+    take(q->tbin, kTrainBatchCap);
+    take(q->tw, kTrainBatchCap);
+    take(q->twsum, 1);
+    take(q->tloss, 1);
+    if (ok) {
+      ok = cudaMemcpy(d_bin, det_bin.data(), sizeof(uint32_t) * nd, cudaMemcpyHostToDevice) == cudaSuccess &&
+           cudaMemcpy(d_off, bin_off.data(), sizeof(uint32_t) * (q->q.nbin + 1), cudaMemcpyHostToDevice) == cudaSuccess &&
+           cudaMemcpy(d_mem, bin_mem.data(), sizeof(uint32_t) * nd, cudaMemcpyHostToDevice) == cudaSuccess &&
+           cudaMemcpy(d_pos, pos.data(), sizeof(uint32_t) * nd, cudaMemcpyHostToDevice) == cudaSuccess &&
+           cudaMemset(nsamples, 0, sizeof(unsigned long long)) == cudaSuccess;
+    }
+    q->pr = Proposal{q->cdf, d_bin, d_off, d_mem, d_pos, samples, nsamples};
+    q->h_det_bin = det_bin;
+    q->h_bin_off = bin_off;
+    if (ok) {
+      const int din = ((ctx->nref + 10 + 2 * ctx->nmo) + 31) / 32 * 32;
+      ok = nw::mlp_create(ctx, &q->mlp, din, (int)q->q.nbin, kTrainBatchCap, opts->seed ^ 0x5EEDull) == NW_OK;
+    }
+  }
   if (!ok) {
     release(q);
     return nw::fail(ctx, NW_ERR_ALLOC, "QMC buffer allocation failed");

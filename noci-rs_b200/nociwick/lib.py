@@ -70,6 +70,16 @@ PROPAGATORS = {"unshifted": 0, "shifted": 1, "doubly-shifted": 2, "difference-do
                "difference-doubly-shifted-u2": 4}
 
 
+class NwMlpOpts(ctypes.Structure):
+    _fields_ = [("epochs", ctypes.c_int32), ("batch", ctypes.c_int32), ("lr", ctypes.c_double),
+                ("seed", ctypes.c_uint64)]
+
+
+class NwMlpReport(ctypes.Structure):
+    _fields_ = [("loss_first", ctypes.c_double), ("loss_last", ctypes.c_double), ("samples", ctypes.c_uint64),
+                ("steps", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
 class NwPt2Projection(ctypes.Structure):
     _fields_ = [("e0", ctypes.c_double), ("s_a0", ctypes.c_void_p), ("s_0a", ctypes.c_void_p),
                 ("f_a0", ctypes.c_void_p), ("f_0a", ctypes.c_void_p)]
@@ -94,7 +104,9 @@ EXPORTED = ("nw_ctx_create", "nw_build_intermediates", "nw_pair_zero_counts", "n
             "nw_eval_s_pairs_device", "nw_update_fock", "nw_eval_fs_pairs_device", "nw_eval_fs_pairs",
             "nw_build_hs_matrix", "nw_build_fs_matrix", "nw_general_evp",
             "nw_qmc_create", "nw_qmc_run", "nw_qmc_set_shift", "nw_qmc_last_run_ms", "nw_qmc_populations", "nw_qmc_set_populations", "nw_qmc_cycle_delta",
-            "nw_qmc_destroy", "nw_pt2_create", "nw_pt2_apply_m", "nw_pt2_last_apply_ms", "nw_pt2_solve",
+            "nw_qmc_destroy", "nw_qmc_harvest", "nw_qmc_train_proposal", "nw_qmc_set_generator",
+            "nw_qmc_proposal_dims", "nw_qmc_mlp_params", "nw_qmc_set_mlp_params", "nw_qmc_mlp_loss_grad",
+            "nw_qmc_proposal_probs", "nw_pt2_create", "nw_pt2_apply_m", "nw_pt2_last_apply_ms", "nw_pt2_solve",
             "nw_pt2_destroy", "nw_sync",
             "nw_set_timing", "nw_last_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
             "nw_last_error")
@@ -135,6 +147,15 @@ def load(path: Optional[str] = None):
     L.nw_qmc_set_populations.argtypes = [vp, vp]
     L.nw_qmc_cycle_delta.argtypes = [vp, ctypes.c_uint64, vp]
     L.nw_qmc_destroy.argtypes = [vp]
+    L.nw_qmc_harvest.argtypes = [vp, ctypes.c_int32]
+    L.nw_qmc_train_proposal.argtypes = [vp, ctypes.POINTER(NwMlpOpts), ctypes.POINTER(NwMlpReport)]
+    L.nw_qmc_set_generator.argtypes = [vp, ctypes.c_int32, ctypes.c_double]
+    L.nw_qmc_proposal_dims.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                       ctypes.POINTER(ctypes.c_uint64)]
+    L.nw_qmc_mlp_params.argtypes = [vp, vp]
+    L.nw_qmc_set_mlp_params.argtypes = [vp, vp]
+    L.nw_qmc_mlp_loss_grad.argtypes = [vp, vp, vp, vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_double), vp]
+    L.nw_qmc_proposal_probs.argtypes = [vp, ctypes.c_uint32, vp]
     L.nw_pt2_create.argtypes = [vp, vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(vp)]
     L.nw_pt2_apply_m.argtypes = [vp, vp, vp]
     L.nw_pt2_last_apply_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
@@ -389,6 +410,51 @@ class Qmc:
     def cycle_delta(self, cycle: int) -> np.ndarray:
         out = np.empty(self.ndet)
         self._w._check(self._lib.nw_qmc_cycle_delta(self._q, cycle, out.ctypes.data), "nw_qmc_cycle_delta")
+        return out
+
+    # -- learned proposal -------------------------------------------------------------------
+    def harvest(self, enable: bool = True):
+        """Record the attempts of the following runs for training the proposal."""
+        self._w._check(self._lib.nw_qmc_harvest(self._q, 1 if enable else 0), "nw_qmc_harvest")
+
+    def train_proposal(self, epochs: int = 2, batch: int = 4096, lr: float = 1e-3, seed: int = 7) -> dict:
+        rep = NwMlpReport()
+        self._w._check(self._lib.nw_qmc_train_proposal(self._q, ctypes.byref(NwMlpOpts(epochs, batch, lr, seed)),
+                                                       ctypes.byref(rep)), "nw_qmc_train_proposal")
+        return {"loss_first": rep.loss_first, "loss_last": rep.loss_last, "samples": rep.samples, "steps": rep.steps}
+
+    def set_generator(self, learned: bool, mix: float = 0.1):
+        self._w._check(self._lib.nw_qmc_set_generator(self._q, 1 if learned else 0, mix), "nw_qmc_set_generator")
+
+    def proposal_dims(self):
+        din, nbin, npar = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_uint64()
+        self._w._check(self._lib.nw_qmc_proposal_dims(self._q, ctypes.byref(din), ctypes.byref(nbin),
+                                                      ctypes.byref(npar)), "nw_qmc_proposal_dims")
+        return din.value, nbin.value, npar.value
+
+    def mlp_params(self) -> np.ndarray:
+        out = np.empty(self.proposal_dims()[2], np.float32)
+        self._w._check(self._lib.nw_qmc_mlp_params(self._q, out.ctypes.data), "nw_qmc_mlp_params")
+        return out
+
+    def set_mlp_params(self, params):
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        self._w._check(self._lib.nw_qmc_set_mlp_params(self._q, params.ctypes.data), "nw_qmc_set_mlp_params")
+
+    def mlp_loss_grad(self, parents, bins, w):
+        parents = np.ascontiguousarray(parents, dtype=np.uint32)
+        bins = np.ascontiguousarray(bins, dtype=np.uint32)
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        loss = ctypes.c_double()
+        grads = np.empty(self.proposal_dims()[2], np.float32)
+        self._w._check(self._lib.nw_qmc_mlp_loss_grad(self._q, parents.ctypes.data, bins.ctypes.data, w.ctypes.data,
+                                                      parents.shape[0], ctypes.byref(loss), grads.ctypes.data),
+                       "nw_qmc_mlp_loss_grad")
+        return loss.value, grads
+
+    def proposal_probs(self, det: int) -> np.ndarray:
+        out = np.empty(self.proposal_dims()[1])
+        self._w._check(self._lib.nw_qmc_proposal_probs(self._q, det, out.ctypes.data), "nw_qmc_proposal_probs")
         return out
 
     def close(self):

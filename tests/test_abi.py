@@ -44,6 +44,8 @@ int main(void) {
          sizeof(nw_qmc_report), offsetof(nw_qmc_report, nocc));
   printf("%zu %zu %zu %zu %zu\n", sizeof(nw_pt2_projection), sizeof(nw_gmres_opts), offsetof(nw_gmres_opts, res_tol),
          offsetof(nw_gmres_opts, preconditioner), sizeof(nw_gmres_info));
+  printf("%zu %zu %zu %zu\n", sizeof(nw_mlp_opts), offsetof(nw_mlp_opts, seed), sizeof(nw_mlp_report),
+         offsetof(nw_mlp_report, steps));
   return 0;
 }
 ''')
@@ -62,6 +64,8 @@ int main(void) {
                         ctypes.sizeof(L.NwQmcReport), L.NwQmcReport.nocc.offset]
     assert v[17:22] == [ctypes.sizeof(L.NwPt2Projection), ctypes.sizeof(L.NwGmresOpts), L.NwGmresOpts.res_tol.offset,
                         L.NwGmresOpts.preconditioner.offset, ctypes.sizeof(L.NwGmresInfo)]
+    assert v[22:26] == [ctypes.sizeof(L.NwMlpOpts), L.NwMlpOpts.seed.offset, ctypes.sizeof(L.NwMlpReport),
+                        L.NwMlpReport.steps.offset]
 
 
 def test_header_compiles_as_cxx(tmp_path):
