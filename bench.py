@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-qmc", action="store_true", help="skip the NOCI-QMC steps/s leg")
     ap.add_argument("--qmc-reports", type=int, default=30, help="timed QMC report blocks (10 steps each)")
+    ap.add_argument("--qmc-compare-reports", type=int, default=400,
+                    help="report blocks per generator in the uniform vs learned comparison (0: skip it)")
     return ap.parse_args()
 
 
@@ -278,8 +280,60 @@ def qmc_leg(args, rank, world, local_rank, dist):
            "timing": "CUDA events around the graph launches of the timed report blocks (max over ranks)"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = qmc_cpu_baseline(system, basis, c0, refs, q, float(rep["shift"][-1]))
+    if args.qmc_compare_reports > 0:
+        out["generators"] = compare_generators(q, args.qmc_compare_reports)
     q.close()
     w.close()
+    return out
+
+
+def blocking_error(x):
+    """Standard error of the mean of a correlated series: the largest of the naive errors
+    over successive pairwise blockings (Flyvbjerg-Petersen) with at least 16 blocks left."""
+    x = np.asarray(x, np.float64)
+    best = 0.0
+    while x.shape[0] >= 16:
+        best = max(best, float(x.std(ddof=1) / np.sqrt(x.shape[0])))
+        n = x.shape[0] // 2 * 2
+        x = 0.5 * (x[0:n:2] + x[1:n:2])
+    return best
+
+
+def compare_generators(q, nreports, target=1e-4):
+    """Wall time to a 0.1 mEh projected-energy error bar, uniform generator vs the learned
+    proposal, from the equilibrated state of the steps/s run: the uniform generator runs
+    `nreports` blocks; then the attempts of two blocks are harvested, the proposal is trained
+    on the GPU (harvest + training time counted against the learned generator) and the
+    learned mixture runs `nreports` blocks.  Each run's error bar comes from a blocking
+    analysis of the per-block projected energies; the time to `target` scales the run's
+    device time by (error / target)^2."""
+    def measure(tag):
+        rep = q.run(nreports)
+        ms = q.last_run_ms()
+        e = rep["eproj_num"] / rep["eproj_den"]
+        err = blocking_error(e)
+        return {"reports": int(nreports), "steps": int(nreports * 10), "device_ms": ms,
+                "eproj": float(rep["eproj_num"].sum() / rep["eproj_den"].sum()), "error_bar": err,
+                "attempts_per_step": float(rep["nattempts"].mean() / 10), "walkers_mean": float(rep["nw"].mean()),
+                "shift_mean": float(rep["shift"].mean()),
+                "seconds_to_0.1mEh": ms / 1e3 * (err / target) ** 2}
+    out = {"uniform": measure("uniform")}
+    t0 = time.perf_counter()
+    q.harvest(True)
+    q.run(2)
+    q.harvest(False)
+    tr = q.train_proposal(epochs=2, batch=4096, lr=1e-3, seed=5)
+    train_s = time.perf_counter() - t0
+    q.set_generator(True, 0.1)
+    lr_ = measure("learned")
+    q.set_generator(False, 0.1)
+    lr_["harvest_train_s"] = train_s
+    lr_["training"] = {k: (float(v) if isinstance(v, float) else int(v)) for k, v in tr.items()}
+    lr_["seconds_to_0.1mEh_incl_training"] = lr_["seconds_to_0.1mEh"] + train_s
+    lr_["mix"] = 0.1
+    out["learned"] = lr_
+    out["note"] = ("same walker state; each generator's time to a 0.1 mEh error bar = its run's device time x "
+                   "(blocking error / 1e-4)^2")
     return out
 
 

@@ -150,3 +150,34 @@ def test_invalid_training_rows_are_rejected():
             q.mlp_loss_grad([0], [det_bin[1]], [float("nan")])
         with pytest.raises(nociwick.NwError):
             q.train_proposal()                            # nothing harvested
+
+
+def test_learned_run_converges_to_noci_ground_state():
+    """A full run with shift control under the learned mixture estimates the same energy as the
+    uniform generator: the lowest eigenvalue of H c = E S c, within its blocked error bar."""
+    w, basis, h, s, refs = _setup()
+    nd = basis.shape[0]
+    with w:
+        e0 = w.general_evp(h, s, project=True, tol=1e-8)[0][0]
+        er, cr = w.general_evp(h[np.ix_(refs, refs)], s[np.ix_(refs, refs)], project=True, tol=1e-8)
+        c0 = np.zeros(nd)
+        c0[refs] = cr[:, 0]
+        e_ref0 = h[refs[0], refs[0]] / s[refs[0], refs[0]]
+        with nociwick.Qmc(w, c0, refs, dt=0.004, initial_population=500.0, target_population=3e5,
+                          shift_damping=0.05, initial_shift=e_ref0, ncycles=10, propagator="unshifted",
+                          seed=77, max_attempts=20_000_000) as q:
+            q.run(200)
+            q.harvest(True)
+            q.run(2)
+            q.harvest(False)
+            q.train_proposal(epochs=4, batch=4096, lr=1e-3, seed=3)
+            q.set_generator(True, 0.1)
+            rep = q.run(600)
+    tail = rep[100:]
+    eproj = tail["eproj_num"] / tail["eproj_den"]
+    blocks = eproj[: (len(eproj) // 25) * 25].reshape(-1, 25).mean(axis=1)
+    mean = tail["eproj_num"].sum() / tail["eproj_den"].sum()
+    err = blocks.std(ddof=1) / np.sqrt(len(blocks))
+    print("learned run: E_proj", mean, "+-", err, "E0", e0)
+    assert abs(mean - e0) < 5 * err + 5e-4, (mean, e0, err)
+    assert abs(tail["shift"].mean() - e0) < 0.05
