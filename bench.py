@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-qmc", action="store_true", help="skip the NOCI-QMC steps/s leg")
     ap.add_argument("--qmc-reports", type=int, default=30, help="timed QMC report blocks (10 steps each)")
+    ap.add_argument("--no-pt2", action="store_true", help="skip the NOCI-PT2 mat-vec / GMRES leg")
+    ap.add_argument("--pt2-ncand", type=int, default=0, help="PT2 candidates (0: all 125685 of the stand-in)")
+    ap.add_argument("--pt2-products", type=int, default=10, help="timed candidate mat-vec products")
     ap.add_argument("--qmc-compare-reports", type=int, default=400,
                     help="report blocks per generator in the uniform vs learned comparison (0: skip it)")
     return ap.parse_args()
@@ -287,6 +290,76 @@ def qmc_leg(args, rank, world, local_rank, dist):
     return out
 
 
+def pt2_leg(args, rank, world, local_rank, dist):
+    """NOCI-PT2 on the F2/cc-pVDZ stand-in (n = 28, 9 + 9 electrons, three references, 125685
+    candidates): the packed candidate matrix M = F - E0 S (7.9e9 entries, 63 GB of HBM) built by
+    the F+S pair path, its symmetric mat-vec (the GMRES H.v of SNOCI/PT2; HBM-bound, the whole
+    triangle streamed once per product) and the restarted GMRES solve at tolerance 1e-8.
+    The Fock matrices are those of the first reference's determinant."""
+    import torch
+    import nociwick
+    from nociwick import synthetic as sy
+    system = sy.config5_system()
+    basis = sy.sd_basis(28, 9, 9, 3)
+    nd = basis.shape[0]
+    w = nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8,
+                             device=local_rank).build()
+    w.set_basis(basis)
+    refs = np.nonzero((basis["rank_a"] == 0) & (basis["rank_b"] == 0))[0].astype(np.uint32)
+    cand = np.setdiff1d(np.arange(nd), refs).astype(np.uint32)
+    if args.pt2_ncand > 0:
+        cand = cand[: args.pt2_ncand]
+    n = int(cand.shape[0])
+    hr, sr = w.build_hs_matrix(refs, refs)
+    er, cr = w.general_evp(hr, sr, project=True, tol=1e-8)
+    c = cr[:, 0]
+    w.update_fock(*sy.reference_fock(system, 0))
+    fr, _ = w.build_fs_matrix(refs, refs)
+    e0 = float(c @ fr @ c)
+    h_ar, s_ar = w.build_hs_matrix(cand, refs, symmetric=False)
+    f_ar, _ = w.build_fs_matrix(cand, refs, symmetric=False)
+    f_ra, s_ra = w.build_fs_matrix(refs, cand, symmetric=False)
+    s_a0, f_a0, s_0a, f_0a = s_ar @ c, f_ar @ c, s_ra.T @ c, f_ra.T @ c
+    rhs = -(h_ar @ c - float(er[0]) * s_a0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pt = nociwick.Pt2(w, cand, e0)
+    build_s = time.perf_counter() - t0
+    x = np.random.default_rng(rank_seed(55, rank)).normal(size=n)
+    for _ in range(3):
+        pt.apply_m(x)
+    ms = []
+    for _ in range(args.pt2_products):
+        pt.apply_m(x)
+        ms.append(pt.last_apply_ms())
+    ms_mean = float(np.mean(ms))
+    (ms_max,) = reduce_max([ms_mean], dist, f"cuda:{local_rank}")
+    t0 = time.perf_counter()
+    amp, info = pt.solve(e0, s_a0, s_0a, f_a0, f_0a, rhs, max_iter=60, restart=30, res_tol=1e-8,
+                         preconditioner="woodbury")
+    solve_s = time.perf_counter() - t0
+    sx, fx = float(s_0a @ amp), float(f_0a @ amp)
+    m_omega_a = pt.apply_m(amp) - f_a0 * sx - s_a0 * fx + 2.0 * e0 * s_a0 * sx
+    e_pt2 = float(amp @ m_omega_a + 2.0 * (amp @ -rhs))
+    pt.close()
+    w.close()
+    entries = n * (n + 1) // 2
+    bytes_per_product = 8 * entries
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_per_product / (ms_max / 1e3) / 1e9
+    return {"metric": "candidate M.v products/s", "value": 1e3 / ms_max, "unit": "products/s",
+            "ms_per_product": ms_max, "n_gpus": world,
+            "config": {"workload": "F2/cc-pVDZ selected-NOCI + NOCI-PT2(3) stand-in: n=28, 9a+9b electrons, RHF+2 UHF "
+                                   "refs, all SD candidates", "ncand": n, "packed_entries": entries,
+                       "gmres": {"restart": 30, "max_iter": 60, "res_tol": 1e-8, "preconditioner": "woodbury"}},
+            "roofline": {"bound": "hbm", "kernel": "packed_symv_kernel", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "algorithmic_bytes_per_product": bytes_per_product, "peak_kind": f"{peak_kind} hbm_gbs"},
+            "build_seconds": build_s, "solve_seconds": solve_s, "gmres": info, "e0": e0, "e_pt2": e_pt2,
+            "timing": "CUDA events around the mat-vec kernel (mean of the timed products, max over ranks); "
+                      "build and solve by host clock"}
+
+
 def blocking_error(x):
     """Standard error of the mean of a correlated series: the largest of the naive errors
     over successive pairwise blockings (Flyvbjerg-Petersen) with at least 16 blocks left."""
@@ -442,6 +515,7 @@ def run_ours(args, rank, world, local_rank):
     eng.close()
     # every rank runs the QMC leg (it has collectives); rank 0 reports
     qmc = None if args.no_qmc else qmc_leg(args, rank, world, local_rank, dist)
+    pt2 = None if args.no_pt2 else pt2_leg(args, rank, world, local_rank, dist)
     if rank != 0:
         return
     value = aggregate_rate(npairs, world, args.steps, t_dev)
@@ -473,6 +547,8 @@ def run_ours(args, rank, world, local_rank):
     }
     if qmc is not None:
         line["qmc"] = qmc
+    if pt2 is not None:
+        line["pt2"] = pt2
     if hs_host is not None:
         line["cpu_baseline"] = cpu_baseline(system, basis, pairs, args.cpu_seconds, gpu_hs=hs_host)
     print(json.dumps(line), flush=True)

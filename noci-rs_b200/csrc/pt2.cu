@@ -53,14 +53,23 @@ __device__ inline void tile_of(uint64_t t, uint64_t nb, uint64_t* I, uint64_t* J
   *J = i + (t - start(i));
 }
 
-__global__ void __launch_bounds__(kTile) packed_symv_kernel(const double* __restrict__ m, uint64_t n, uint64_t nb,
-                                                            const double* __restrict__ x, double* __restrict__ y) {
+// One 256 x 256 tile per block, 8 warps x 32 rows; a lane holds 8 columns (stride 32, so each
+// load instruction of a warp reads 256 contiguous bytes of one packed row).  A warp issues the
+// loads of kSymvRows rows before it reduces any of them, so 8 x kSymvRows x 256 bytes per warp
+// are in flight; the row sums go to y[rows] and, off the diagonal, the per-lane column sums
+// to y[cols].
+constexpr int kSymvRows = 2;
+
+__global__ void __launch_bounds__(kTile, 2) packed_symv_kernel(const double* __restrict__ m, uint64_t n, uint64_t nb,
+                                                               const double* __restrict__ x, double* __restrict__ y) {
+  __shared__ double xrow[kTile];
   __shared__ double rowsum[kTile];
   __shared__ double colsum[kTileWarps][kTile];
   uint64_t I, J;
   tile_of(blockIdx.x, nb, &I, &J);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint64_t r0 = I * kTile, c0 = J * kTile;
+  xrow[threadIdx.x] = r0 + threadIdx.x < n ? x[r0 + threadIdx.x] : 0.0;
   double xc[kColsPerLane], cacc[kColsPerLane];
 #pragma unroll
   for (int k = 0; k < kColsPerLane; ++k) {
@@ -68,26 +77,34 @@ __global__ void __launch_bounds__(kTile) packed_symv_kernel(const double* __rest
     xc[k] = b < n ? x[b] : 0.0;
     cacc[k] = 0.0;
   }
-  for (int rr = 0; rr < kRowsPerWarp; ++rr) {
-    const int rl = warp * kRowsPerWarp + rr;
-    const uint64_t a = r0 + rl;
-    double rs = 0.0;
-    if (a < n) {
-      const double xa = x[a];
-      const double* row = m + row_start(a, n) - a;  // row[b] = M[a][b] for b >= a
+  __syncthreads();
+  for (int rr = 0; rr < kRowsPerWarp; rr += kSymvRows) {
+    double v[kSymvRows][kColsPerLane];
+#pragma unroll
+    for (int g = 0; g < kSymvRows; ++g) {
+      const uint64_t a = r0 + warp * kRowsPerWarp + rr + g;
+      const double* row = m + (a < n ? row_start(a, n) - a : 0);  // row[b] = M[a][b] for b >= a
 #pragma unroll
       for (int k = 0; k < kColsPerLane; ++k) {
         const uint64_t b = c0 + lane + 32 * k;
-        if (b < n && b >= a) {
-          const double v = __ldcs(row + b);
-          rs += v * xc[k];
-          if (b != a) cacc[k] += v * xa;
-        }
+        v[g][k] = (a < n && b < n && b >= a) ? __ldcs(row + b) : 0.0;
       }
     }
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) rs += __shfl_xor_sync(0xFFFFFFFFu, rs, off);
-    if (lane == 0) rowsum[rl] = rs;
+    for (int g = 0; g < kSymvRows; ++g) {
+      const int rl = warp * kRowsPerWarp + rr + g;
+      const uint64_t a = r0 + rl;
+      const double xa = xrow[rl];
+      double rs = 0.0;
+#pragma unroll
+      for (int k = 0; k < kColsPerLane; ++k) {
+        rs = fma(v[g][k], xc[k], rs);
+        if (c0 + lane + 32 * k != a) cacc[k] = fma(v[g][k], xa, cacc[k]);
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) rs += __shfl_xor_sync(0xFFFFFFFFu, rs, off);
+      if (lane == 0) rowsum[rl] = rs;
+    }
   }
 #pragma unroll
   for (int k = 0; k < kColsPerLane; ++k) colsum[warp][lane + 32 * k] = cacc[k];
@@ -97,7 +114,7 @@ __global__ void __launch_bounds__(kTile) packed_symv_kernel(const double* __rest
   double cs = 0.0;
 #pragma unroll
   for (int w = 0; w < kTileWarps; ++w) cs += colsum[w][t];
-  // column sums of the strictly upper part (b > a was enforced above)
+  // column sums of the strictly upper part (entries with b < a were loaded as zero)
   if (c0 + t < n && cs != 0.0) atomicAdd(y + c0 + t, cs);
 }
 

@@ -311,6 +311,28 @@ def config4_system(seed: int = 4) -> System:
                        enuc=0.0, orbital_energies=eps)
 
 
+def config5_system(seed: int = 5) -> System:
+    """F2/cc-pVDZ selected-NOCI + NOCI-PT2 stand-in dimensions: n = 28, 9 + 9 electrons, an
+    RHF-like and two spin-polarised references; all singles and doubles of the three
+    references give 125688 determinants (125685 PT2 candidates).  Orbital energies as in the
+    QMC stand-in (occupied -1.5..-0.5, virtual 0.2..2.5 Eh) with weak random couplings."""
+    eps = np.concatenate([np.linspace(-1.5, -0.5, 9), np.linspace(0.2, 2.5, 19)])
+    return make_system(28, 9, 9, 3, 112, seed, sigma_h=0.02, sigma_l=0.02, k_scale=0.3, uhf_like=True,
+                       enuc=0.0, orbital_energies=eps)
+
+
+def reference_fock(system: System, r: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+    """AO Fock matrices of reference r's determinant: F_s = h + J[D_a + D_b] - K[D_s] with
+    D_s = C_s[:, :nocc_s] C_s[:, :nocc_s]^T (orthonormal AO basis)."""
+    ca, _, cb, _ = system.refs[r]
+    da = ca[:, :system.nocc_a] @ ca[:, :system.nocc_a].T
+    db = cb[:, :system.nocc_b] @ cb[:, :system.nocc_b].T
+    j = np.einsum("pqrs,rs->pq", system.eri, da + db)
+    ka = np.einsum("prqs,rs->pq", system.eri, da)
+    kb = np.einsum("prqs,rs->pq", system.eri, db)
+    return system.h + j - ka, system.h + j - kb
+
+
 def config3_system(seed: int = 3, nmo: int = 64, nref: int = 8) -> System:
     """Synthetic stress system: n = 64, 6 + 6 electrons, naux = 256, 8 references, zero-overlap
     pairs forced in 3 unordered reference pairs (6 of 64 ordered pairs)."""
