@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-pt2", action="store_true", help="skip the NOCI-PT2 mat-vec / GMRES leg")
     ap.add_argument("--pt2-ncand", type=int, default=0, help="PT2 candidates (0: all 125685 of the stand-in)")
     ap.add_argument("--pt2-products", type=int, default=10, help="timed candidate mat-vec products")
+    ap.add_argument("--qmc-equil", type=int, default=40, help="QMC equilibration report blocks")
+    ap.add_argument("--qmc-train-epochs", type=int, default=2, help="epochs of proposal training")
     ap.add_argument("--qmc-compare-reports", type=int, default=400,
                     help="report blocks per generator in the uniform vs learned comparison (0: skip it)")
     return ap.parse_args()
@@ -261,9 +263,9 @@ def qmc_leg(args, rank, world, local_rank, dist):
     q = nociwick.Qmc(w, c0, refs, dt=1e-3, initial_population=walkers, target_population=walkers,
                      shift_damping=0.5, initial_shift=float(er[0]), ncycles=10, propagator="unshifted",
                      seed=rank_seed(4242, rank), max_attempts=48_000_000)
-    # equilibration: 40 report blocks (400 steps) bring the walkers from the three references
+    # equilibration: 40 report blocks (400 steps, --qmc-equil) bring the walkers from the three references
     # to a steady 1-norm near 10^6 over the whole space before the timed blocks
-    q.run(40)
+    q.run(args.qmc_equil)
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
@@ -284,7 +286,7 @@ def qmc_leg(args, rank, world, local_rank, dist):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = qmc_cpu_baseline(system, basis, c0, refs, q, float(rep["shift"][-1]))
     if args.qmc_compare_reports > 0:
-        out["generators"] = compare_generators(q, args.qmc_compare_reports)
+        out["generators"] = compare_generators(q, args.qmc_compare_reports, epochs=args.qmc_train_epochs)
     q.close()
     w.close()
     return out
@@ -372,7 +374,7 @@ def blocking_error(x):
     return best
 
 
-def compare_generators(q, nreports, target=1e-4):
+def compare_generators(q, nreports, target=1e-4, epochs=2):
     """Wall time to a 0.1 mEh projected-energy error bar, uniform generator vs the learned
     proposal, from the equilibrated state of the steps/s run: the uniform generator runs
     `nreports` blocks; then the attempts of two blocks are harvested, the proposal is trained
@@ -395,7 +397,7 @@ def compare_generators(q, nreports, target=1e-4):
     q.harvest(True)
     q.run(2)
     q.harvest(False)
-    tr = q.train_proposal(epochs=2, batch=4096, lr=1e-3, seed=5)
+    tr = q.train_proposal(epochs=epochs, batch=4096, lr=1e-3, seed=5)
     train_s = time.perf_counter() - t0
     q.set_generator(True, 0.1)
     lr_ = measure("learned")

@@ -76,7 +76,13 @@ __global__ void __launch_bounds__(256) classify_kernel(EvalParams P, const uint3
                                                        int out_stride, uint32_t* __restrict__ flag) {
   if (npairs_dev) npairs = min(npairs, (uint64_t)*npairs_dev);
   const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i0 < npairs; i0 += kSortUnroll * nthreads) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t lanes_below = (1u << lane) - 1u;
+  // The trip count depends only on the warp's first index, so every lane of a warp runs every
+  // iteration and the full-mask warp intrinsics below are well defined.
+  const uint64_t warp0 = blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x & ~31u);
+  for (uint64_t w0 = warp0; w0 < npairs; w0 += kSortUnroll * nthreads) {
+    const uint64_t i0 = w0 + lane;
     uint2 ab[kSortUnroll];
     uint32_t key[kSortUnroll], rk[kSortUnroll];
 #pragma unroll
@@ -89,8 +95,18 @@ __global__ void __launch_bounds__(256) classify_kernel(EvalParams P, const uint3
       const uint64_t i = i0 + u * nthreads;
       key[u] = i < npairs ? classify_one(P, ab[u], i, out, out_stride, flag) : kSkipKey;
     }
+    // Ranks inside each key's bucket: lanes holding the same key take consecutive ranks from
+    // one atomic of their leader (attempts of one QMC parent share keys, so per-lane atomics
+    // would serialise on a single counter).
 #pragma unroll
-    for (int u = 0; u < kSortUnroll; ++u) rk[u] = key[u] != kSkipKey ? atomicAdd(&counts[key[u]], 1u) : 0u;
+    for (int u = 0; u < kSortUnroll; ++u) {
+      const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key[u]);
+      const int leader = __ffs(peers) - 1;
+      uint32_t base = 0u;
+      if (lane == leader && key[u] != kSkipKey) base = atomicAdd(&counts[key[u]], (uint32_t)__popc(peers));
+      base = __shfl_sync(0xFFFFFFFFu, base, leader);
+      rk[u] = key[u] != kSkipKey ? base + (uint32_t)__popc(peers & lanes_below) : 0u;
+    }
 #pragma unroll
     for (int u = 0; u < kSortUnroll; ++u) {
       const uint64_t i = i0 + u * nthreads;

@@ -18,6 +18,7 @@ namespace {
 
 constexpr int kT = 64;   // output tile
 constexpr int kL = 16;   // reduction chunk
+constexpr int kSplitMax = 32;  // k-split blocks of a weight-gradient product
 
 __device__ __forceinline__ float to_f(float v) { return v; }
 __device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
@@ -25,28 +26,32 @@ __device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float
 enum Epi { kPlain = 0, kBiasRelu = 1, kBias = 2, kReluMask = 3 };
 
 // C[M x N] = epi(A[M x L] B[L x N]); A[i][l] = A[i * asr + l * asc], B[l][j] = B[l * bsr + j * bsc].
+// With gridDim.z > 1 the reduction range is split: block z covers [z * lsplit, (z + 1) * lsplit)
+// and writes its plain partial product to C + z * M * ldc (summed by splitk_sum_kernel).
 template <typename TB>
 __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int L, const float* __restrict__ A, long asr, long asc,
                                                    const TB* __restrict__ B, long bsr, long bsc, float* __restrict__ C,
                                                    int ldc, int epi, const float* __restrict__ bias,
-                                                   const float* __restrict__ mask) {
+                                                   const float* __restrict__ mask, int lsplit) {
   __shared__ float As[kL][kT + 1];
   __shared__ float Bs[kL][kT + 1];
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
   const int row0 = blockIdx.y * kT, col0 = blockIdx.x * kT;
+  const int lbeg = blockIdx.z * lsplit, lend = min(L, lbeg + lsplit);
+  C += (size_t)blockIdx.z * M * ldc;
   float acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
-  for (int l0 = 0; l0 < L; l0 += kL) {
+  for (int l0 = lbeg; l0 < lend; l0 += kL) {
     for (int e = threadIdx.x; e < kT * kL; e += 256) {
       const int r = e / kL, c = e % kL, gr = row0 + r, gc = l0 + c;
-      As[c][r] = (gr < M && gc < L) ? A[gr * asr + gc * asc] : 0.0f;
+      As[c][r] = (gr < M && gc < lend) ? A[gr * asr + gc * asc] : 0.0f;
     }
     for (int e = threadIdx.x; e < kT * kL; e += 256) {
       const int r = e / kT, c = e % kT, gr = l0 + r, gc = col0 + c;
-      Bs[r][c] = (gr < L && gc < N) ? to_f(B[gr * bsr + gc * bsc]) : 0.0f;
+      Bs[r][c] = (gr < lend && gc < N) ? to_f(B[gr * bsr + gc * bsc]) : 0.0f;
     }
     __syncthreads();
 #pragma unroll
@@ -77,13 +82,32 @@ __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int L, const fl
     }
 }
 
-// out[j] = sum_r X[r][j] (column sums of a B x N matrix).
-__global__ void colsum_kernel(const float* __restrict__ x, int B, int N, float* __restrict__ out) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= N) return;
+// C[i] = sum_z P[z][i] over the k-split partial products (fixed order).
+__global__ void splitk_sum_kernel(const float* __restrict__ part, int splits, size_t count, float* __restrict__ c) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+    float s = 0.0f;
+    for (int z = 0; z < splits; ++z) s += part[(size_t)z * count + i];
+    c[i] = s;
+  }
+}
+
+// out[j] = sum_r X[r][j] (column sums of a B x N matrix): 32 columns x 8 row groups per block,
+// coalesced across the columns, then a fixed-order sum over the row groups.
+__global__ void __launch_bounds__(256) colsum_kernel(const float* __restrict__ x, int B, int N, float* __restrict__ out) {
+  __shared__ float part[8][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int j = blockIdx.x * 32 + tx;
   float s = 0.0f;
-  for (int r = 0; r < B; ++r) s += x[(size_t)r * N + j];
-  out[j] = s;
+  if (j < N)
+    for (int r = ty; r < B; r += 8) s += x[(size_t)r * N + j];
+  part[ty][tx] = s;
+  __syncthreads();
+  if (ty == 0 && j < N) {
+    float t = 0.0f;
+#pragma unroll
+    for (int g = 0; g < 8; ++g) t += part[g][tx];
+    out[j] = t;
+  }
 }
 
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
@@ -107,7 +131,21 @@ template <typename TB>
 nw_status gemm(nw_ctx* ctx, int M, int N, int L, const float* A, long asr, long asc, const TB* B, long bsr, long bsc,
                float* C, int ldc, int epi, const float* bias, const float* mask, cudaStream_t s) {
   const dim3 grid((N + kT - 1) / kT, (M + kT - 1) / kT);
-  gemm_kernel<TB><<<grid, 256, 0, s>>>(M, N, L, A, asr, asc, B, bsr, bsc, C, ldc, epi, bias, mask);
+  gemm_kernel<TB><<<grid, 256, 0, s>>>(M, N, L, A, asr, asc, B, bsr, bsc, C, ldc, epi, bias, mask, L);
+  NW_CUDA(ctx, cudaGetLastError());
+  return NW_OK;
+}
+
+// Weight gradients (few output tiles, long reduction over the batch): the reduction is split
+// over kSplitMax blocks along z into m->part, then summed in a fixed order.
+nw_status gemm_splitk(nw_ctx* ctx, Mlp* m, int M, int N, int L, const float* A, long asr, long asc, const float* B,
+                      long bsr, long bsc, float* C, cudaStream_t s) {
+  const int lsplit = std::max(kL, (L + kSplitMax - 1) / kSplitMax + kL - 1) / kL * kL;
+  const int splits = (L + lsplit - 1) / lsplit;
+  const dim3 grid((N + kT - 1) / kT, (M + kT - 1) / kT, splits);
+  gemm_kernel<float><<<grid, 256, 0, s>>>(M, N, L, A, asr, asc, B, bsr, bsc, m->part, N, kPlain, nullptr, nullptr, lsplit);
+  const size_t count = (size_t)M * N;
+  splitk_sum_kernel<<<(int)std::min<size_t>((count + 255) / 256, 1184), 256, 0, s>>>(m->part, splits, count, C);
   NW_CUDA(ctx, cudaGetLastError());
   return NW_OK;
 }
@@ -129,6 +167,8 @@ nw_status mlp_create(nw_ctx* ctx, Mlp* m, int din, int nout, int bcap, uint64_t 
   for (float** b : bufs)
     if (cudaMalloc(b, sizeof(float) * np) != cudaSuccess) return fail(ctx, NW_ERR_ALLOC, "MLP parameters");
   if (cudaMalloc(&m->wbf, sizeof(__nv_bfloat16) * np) != cudaSuccess) return fail(ctx, NW_ERR_ALLOC, "MLP weights");
+  const size_t part = (size_t)kSplitMax * kMlpWidth * std::max(std::max(din, nout), kMlpWidth);
+  if (cudaMalloc(&m->part, sizeof(float) * part) != cudaSuccess) return fail(ctx, NW_ERR_ALLOC, "MLP split-k partials");
   struct Act {
     float** p;
     size_t n;
@@ -158,7 +198,7 @@ nw_status mlp_create(nw_ctx* ctx, Mlp* m, int din, int nout, int bcap, uint64_t 
 }
 
 void mlp_destroy(Mlp* m) {
-  void* bufs[] = {m->params, m->grads, m->adam_m, m->adam_v, m->wbf, m->x, m->h1, m->h2, m->z, m->d2, m->d1};
+  void* bufs[] = {m->params, m->grads, m->adam_m, m->adam_v, m->wbf, m->x, m->h1, m->h2, m->z, m->d2, m->d1, m->part};
   for (void* p : bufs)
     if (p) cudaFree(p);
   *m = Mlp{};
@@ -187,18 +227,18 @@ nw_status mlp_backward(nw_ctx* ctx, Mlp* m, int B, cudaStream_t s) {
   const int W = kMlpWidth, K = m->nout, D = m->din;
   float* G = m->grads;
   // layer 3: dW3 = dZ^T H2, db3 = colsum dZ, d2 = (dZ W3) o [H2 > 0]
-  nw_status st = gemm(ctx, K, W, B, m->z, 1, K, m->h2, W, 1, G + m->off_w3(), W, kPlain, nullptr, nullptr, s);
-  colsum_kernel<<<(K + 127) / 128, 128, 0, s>>>(m->z, B, K, G + m->off_b3());
+  nw_status st = gemm_splitk(ctx, m, K, W, B, m->z, 1, K, m->h2, W, 1, G + m->off_w3(), s);
+  colsum_kernel<<<(K + 31) / 32, 256, 0, s>>>(m->z, B, K, G + m->off_b3());
   if (st == NW_OK)
     st = gemm(ctx, B, W, K, m->z, K, 1, m->wbf + m->off_w3(), W, 1, m->d2, W, kReluMask, nullptr, m->h2, s);
   // layer 2
-  if (st == NW_OK) st = gemm(ctx, W, W, B, m->d2, 1, W, m->h1, W, 1, G + m->off_w2(), W, kPlain, nullptr, nullptr, s);
-  colsum_kernel<<<1, 128, 0, s>>>(m->d2, B, W, G + m->off_b2());
+  if (st == NW_OK) st = gemm_splitk(ctx, m, W, W, B, m->d2, 1, W, m->h1, W, 1, G + m->off_w2(), s);
+  colsum_kernel<<<(W + 31) / 32, 256, 0, s>>>(m->d2, B, W, G + m->off_b2());
   if (st == NW_OK)
     st = gemm(ctx, B, W, W, m->d2, W, 1, m->wbf + m->off_w2(), W, 1, m->d1, W, kReluMask, nullptr, m->h1, s);
   // layer 1
-  if (st == NW_OK) st = gemm(ctx, W, D, B, m->d1, 1, W, m->x, D, 1, G + m->off_w1(), D, kPlain, nullptr, nullptr, s);
-  colsum_kernel<<<1, 128, 0, s>>>(m->d1, B, W, G + m->off_b1());
+  if (st == NW_OK) st = gemm_splitk(ctx, m, W, D, B, m->d1, 1, W, m->x, D, 1, G + m->off_w1(), s);
+  colsum_kernel<<<(W + 31) / 32, 256, 0, s>>>(m->d1, B, W, G + m->off_b1());
   if (st == NW_OK) NW_CUDA(ctx, cudaGetLastError());
   return st;
 }

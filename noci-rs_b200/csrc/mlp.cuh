@@ -30,6 +30,7 @@ struct Mlp {
   float* z = nullptr;            // [bcap][nout] logits, then dZ
   float* d2 = nullptr;           // [bcap][128]
   float* d1 = nullptr;           // [bcap][128]
+  float* part = nullptr;         // k-split partial products of the weight gradients
   int adam_t = 0;
   size_t off_w1() const { return 0; }
   size_t off_b1() const { return (size_t)kMlpWidth * din; }

@@ -170,9 +170,16 @@ __global__ void qmc_spawn_kernel(QmcParams q, Proposal pr, const QmcState* __res
         lam = nwq::uniform_child(g, q.ndet, u2);
       } else {
         // bin from the parent's cumulative probabilities, then uniformly inside the bin
+        // first bin with u2 < cdf (the last valid bin and those after it hold 1.0 > u2)
         const float* c = pr.cdf + g * q.nbin;
-        uint32_t b = 0;
-        while (b + 1 < q.nbin && !(u2 < (double)c[b])) ++b;
+        uint32_t b = 0, hi = q.nbin - 1;
+        while (b < hi) {
+          const uint32_t mid = (b + hi) >> 1;
+          if (u2 < (double)c[mid])
+            hi = mid;
+          else
+            b = mid + 1;
+        }
         const uint32_t size = bin_size_without(pr, b, (uint32_t)g);
         uint32_t idx = (uint32_t)(u3 * (double)size);
         if (idx >= size) idx = size - 1;
@@ -758,7 +765,10 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
   take(q->partial, (size_t)kStatBlocks * kStats);
   take(q->ring, kReportRing);
   q->P = nw::make_params(ctx);
-  q->nkeys = nw::plan_keys(ctx, q->P, std::min(nw::kFineMax, std::max(nw::kFineMin, cap)));
+  // fine sort keys sized for the attempts of a typical cycle (about the walker 1-norm), not
+  // for the capacity: every cycle clears and scans all keys
+  const uint64_t typical = (uint64_t)(2.0 * std::max(opts->target_population, opts->initial_population)) + nd;
+  q->nkeys = nw::plan_keys(ctx, q->P, std::min<uint64_t>(nw::kFineMax, std::max<uint64_t>(nw::kFineMin, std::min(typical, cap))));
   take(q->S.keys, cap);
   take(q->S.ranks, cap);
   take(q->S.sidx, cap);
