@@ -91,22 +91,25 @@ __global__ void splitk_sum_kernel(const float* __restrict__ part, int splits, si
   }
 }
 
-// out[j] = sum_r X[r][j] (column sums of a B x N matrix): 32 columns x 8 row groups per block,
-// coalesced across the columns, then a fixed-order sum over the row groups.
-__global__ void __launch_bounds__(256) colsum_kernel(const float* __restrict__ x, int B, int N, float* __restrict__ out) {
+// Partial column sums of a B x N matrix: block (x, y) sums rows [y * rows, (y + 1) * rows) of
+// columns 32x .. 32x + 31 (32 columns x 8 row groups, coalesced across the columns) into
+// out[y * N + j]; splitk_sum_kernel adds the row splits in a fixed order.
+__global__ void __launch_bounds__(256) colsum_kernel(const float* __restrict__ x, int B, int N, int rows,
+                                                     float* __restrict__ out) {
   __shared__ float part[8][33];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int j = blockIdx.x * 32 + tx;
+  const int r0 = blockIdx.y * rows, r1 = min(B, r0 + rows);
   float s = 0.0f;
   if (j < N)
-    for (int r = ty; r < B; r += 8) s += x[(size_t)r * N + j];
+    for (int r = r0 + ty; r < r1; r += 8) s += x[(size_t)r * N + j];
   part[ty][tx] = s;
   __syncthreads();
   if (ty == 0 && j < N) {
     float t = 0.0f;
 #pragma unroll
     for (int g = 0; g < 8; ++g) t += part[g][tx];
-    out[j] = t;
+    out[(size_t)blockIdx.y * N + j] = t;
   }
 }
 
@@ -146,6 +149,16 @@ nw_status gemm_splitk(nw_ctx* ctx, Mlp* m, int M, int N, int L, const float* A, 
   gemm_kernel<float><<<grid, 256, 0, s>>>(M, N, L, A, asr, asc, B, bsr, bsc, m->part, N, kPlain, nullptr, nullptr, lsplit);
   const size_t count = (size_t)M * N;
   splitk_sum_kernel<<<(int)std::min<size_t>((count + 255) / 256, 1184), 256, 0, s>>>(m->part, splits, count, C);
+  NW_CUDA(ctx, cudaGetLastError());
+  return NW_OK;
+}
+
+// out[j] = sum_r X[r][j] through the split buffer m->part.
+nw_status colsum(nw_ctx* ctx, Mlp* m, const float* x, int B, int N, float* out, cudaStream_t s) {
+  const int rows = std::max(8, (B + kSplitMax - 1) / kSplitMax);
+  const int splits = (B + rows - 1) / rows;
+  colsum_kernel<<<dim3((N + 31) / 32, splits), 256, 0, s>>>(x, B, N, rows, m->part);
+  splitk_sum_kernel<<<(N + 255) / 256, 256, 0, s>>>(m->part, splits, (size_t)N, out);
   NW_CUDA(ctx, cudaGetLastError());
   return NW_OK;
 }
@@ -228,17 +241,17 @@ nw_status mlp_backward(nw_ctx* ctx, Mlp* m, int B, cudaStream_t s) {
   float* G = m->grads;
   // layer 3: dW3 = dZ^T H2, db3 = colsum dZ, d2 = (dZ W3) o [H2 > 0]
   nw_status st = gemm_splitk(ctx, m, K, W, B, m->z, 1, K, m->h2, W, 1, G + m->off_w3(), s);
-  colsum_kernel<<<(K + 31) / 32, 256, 0, s>>>(m->z, B, K, G + m->off_b3());
+  if (st == NW_OK) st = colsum(ctx, m, m->z, B, K, G + m->off_b3(), s);
   if (st == NW_OK)
     st = gemm(ctx, B, W, K, m->z, K, 1, m->wbf + m->off_w3(), W, 1, m->d2, W, kReluMask, nullptr, m->h2, s);
   // layer 2
   if (st == NW_OK) st = gemm_splitk(ctx, m, W, W, B, m->d2, 1, W, m->h1, W, 1, G + m->off_w2(), s);
-  colsum_kernel<<<(W + 31) / 32, 256, 0, s>>>(m->d2, B, W, G + m->off_b2());
+  if (st == NW_OK) st = colsum(ctx, m, m->d2, B, W, G + m->off_b2(), s);
   if (st == NW_OK)
     st = gemm(ctx, B, W, W, m->d2, W, 1, m->wbf + m->off_w2(), W, 1, m->d1, W, kReluMask, nullptr, m->h1, s);
   // layer 1
   if (st == NW_OK) st = gemm_splitk(ctx, m, W, D, B, m->d1, 1, W, m->x, D, 1, G + m->off_w1(), s);
-  colsum_kernel<<<(W + 31) / 32, 256, 0, s>>>(m->d1, B, W, G + m->off_b1());
+  if (st == NW_OK) st = colsum(ctx, m, m->d1, B, W, G + m->off_b1(), s);
   if (st == NW_OK) NW_CUDA(ctx, cudaGetLastError());
   return st;
 }

@@ -266,10 +266,17 @@ __global__ void __launch_bounds__(kBlockThreads) qmc_block_kernel(QmcParams q, d
 // Sum the partials (fixed order), update the shift and write the report of this block.
 __global__ void qmc_finalize_kernel(QmcParams q, QmcState* __restrict__ st, const double* __restrict__ partial,
                                     int nblocks, nw_qmc_report* __restrict__ ring, int write_report) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (blockIdx.x != 0) return;
+  // one warp: lane l sums blocks l, l + 32, ...; then a fixed butterfly over the lanes
   double tot[kStats] = {0, 0, 0, 0, 0, 0};
-  for (int b = 0; b < nblocks; ++b)
+  for (int b = threadIdx.x; b < nblocks; b += 32)
+#pragma unroll
     for (int k = 0; k < kStats; ++k) tot[k] += partial[b * kStats + k];
+#pragma unroll
+  for (int k = 0; k < kStats; ++k)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) tot[k] += __shfl_xor_sync(0xFFFFFFFFu, tot[k], off);
+  if (threadIdx.x != 0) return;
   if (!write_report) {
     st->nw_prev = tot[0];
     return;
