@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--no-pt2", action="store_true", help="skip the NOCI-PT2 mat-vec / GMRES leg")
     ap.add_argument("--pt2-ncand", type=int, default=0, help="PT2 candidates (0: all 125685 of the stand-in)")
     ap.add_argument("--pt2-products", type=int, default=10, help="timed candidate mat-vec products")
+    ap.add_argument("--no-snoci", action="store_true", help="skip the selected-NOCI screening leg")
     ap.add_argument("--qmc-equil", type=int, default=40, help="QMC equilibration report blocks")
     ap.add_argument("--qmc-train-epochs", type=int, default=2, help="epochs of proposal training")
     ap.add_argument("--qmc-compare-reports", type=int, default=400,
@@ -362,6 +363,71 @@ def pt2_leg(args, rank, world, local_rank, dist):
                       "build and solve by host clock"}
 
 
+def snoci_leg(args, rank, world, local_rank, dist):
+    """Selected-NOCI candidate screening on the F2/cc-pVDZ stand-in (config 5 dimensions: the
+    three references' 125685 SD candidates).  The first SNOCI step scores every candidate
+    exhaustively (H_ai, S_ai, F_ai, the 63 GB packed M, GMRES); the learned screener is then
+    trained on the exact scores of a random 30 % of the pool, ranks the whole pool, and the
+    same step is repeated over the top 25 % only.  Reported: time of each step, E_PT2 of
+    each, the overlap of the selected sets (max_add = 20) and the recall of the exhaustive top
+    200 among the kept candidates."""
+    import torch
+    import nociwick
+    from nociwick import snoci as sn
+    from nociwick import synthetic as sy
+    system = sy.config5_system()
+    opts = sn.SnociOptions(max_add=20, sigma=1e-8, gmres_max_iter=60, gmres_restart=30, gmres_res_tol=1e-8)
+    w = nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8,
+                             device=local_rank).build()
+    sel, lab = sn.reference_states(system.nref, system.nocc_a, system.nocc_b)
+    t0 = time.perf_counter()
+    pool = sn.CandidatePool(sel, lab, system.nmo)
+    w.set_basis(sn.to_nw_dets(np.concatenate([sel, pool.states])))
+    m, npool = sel.shape[0], pool.states.shape[0]
+    ecur, c = sn.solve_current_space(w, m, opts.lin_tol)
+    w.update_fock(*sn.fock(system.h, system.eri, *sn.noci_density(system, sel, c, opts.lin_tol)))
+    prep_s = time.perf_counter() - t0
+    cand_all = np.arange(m, m + npool, dtype=np.uint32)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    full, ept2_full, e0, info_full = sn.pt2_scores(w, m, cand_all, c, ecur, opts)
+    full_s = time.perf_counter() - t0
+    rng = np.random.default_rng(rank_seed(8, rank))
+    train = rng.choice(npool, int(0.3 * npool), replace=False)
+    t0 = time.perf_counter()
+    scr = nociwick.Screen(w, seed=17)
+    rep = scr.train(cand_all[train], np.log10(np.maximum(full[train], 1e-14)), epochs=30, batch=1024, lr=2e-3)
+    train_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    pred = scr.predict(cand_all)
+    nkeep = int(np.ceil(0.25 * npool))
+    keep = np.sort(np.argsort(-pred, kind="stable")[:nkeep])
+    kept, ept2_kept, _, info_kept = sn.pt2_scores(w, m, cand_all[keep], c, ecur, opts)
+    screen_s = time.perf_counter() - t0
+    scr.close()
+    w.close()
+    sel_full = set(sn.select_candidates(full, opts.sigma, opts.max_add).tolist())
+    sc = np.zeros(npool)
+    sc[keep] = kept
+    sel_scr = set(sn.select_candidates(sc, opts.sigma, opts.max_add).tolist())
+    top = np.argsort(-full, kind="stable")[:200]
+    held_out = np.setdiff1d(top, train)
+    return {"metric": "SNOCI step time", "unit": "s", "ncand": int(npool), "nref": int(m),
+            "config": {"workload": "F2/cc-pVDZ selected-NOCI + NOCI-PT2(3) stand-in: n=28, 9a+9b electrons, "
+                                   "RHF+2 UHF refs, first SNOCI step over all SD candidates",
+                       "max_add": opts.max_add, "keep_fraction": 0.25, "train_fraction": 0.3,
+                       "gmres": {"restart": 30, "max_iter": 60, "res_tol": 1e-8}},
+            "prepare_seconds": prep_s,
+            "exhaustive": {"seconds": full_s, "scored": int(npool), "ept2": ept2_full, "gmres": info_full},
+            "learned": {"train_seconds": train_s, "seconds": screen_s, "scored": int(nkeep), "ept2": ept2_kept,
+                        "gmres": info_kept, "training": rep,
+                        "selected_overlap": len(sel_full & sel_scr) / max(1, len(sel_full)),
+                        "top200_recall": float(np.isin(top, keep).mean()),
+                        "top200_recall_held_out": float(np.isin(held_out, keep).mean()) if held_out.size else None},
+            "e_current": ecur, "e0": e0,
+            "timing": "host clock around each step (device work synchronised by its result copies)"}
+
+
 def blocking_error(x):
     """Standard error of the mean of a correlated series: the largest of the naive errors
     over successive pairwise blockings (Flyvbjerg-Petersen) with at least 16 blocks left."""
@@ -518,6 +584,7 @@ def run_ours(args, rank, world, local_rank):
     # every rank runs the QMC leg (it has collectives); rank 0 reports
     qmc = None if args.no_qmc else qmc_leg(args, rank, world, local_rank, dist)
     pt2 = None if args.no_pt2 else pt2_leg(args, rank, world, local_rank, dist)
+    snoci_out = None if args.no_snoci else snoci_leg(args, rank, world, local_rank, dist)
     if rank != 0:
         return
     value = aggregate_rate(npairs, world, args.steps, t_dev)
@@ -551,6 +618,8 @@ def run_ours(args, rank, world, local_rank):
         line["qmc"] = qmc
     if pt2 is not None:
         line["pt2"] = pt2
+    if snoci_out is not None:
+        line["snoci"] = snoci_out
     if hs_host is not None:
         line["cpu_baseline"] = cpu_baseline(system, basis, pairs, args.cpu_seconds, gpu_hs=hs_host)
     print(json.dumps(line), flush=True)

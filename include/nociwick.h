@@ -312,6 +312,25 @@ NW_API nw_status nw_qmc_mlp_loss_grad(nw_qmc* q, const uint32_t* parents, const 
 /* p(bin | det) of the current network (nbin values; bins without a child of det are 0). */
 NW_API nw_status nw_qmc_proposal_probs(nw_qmc* q, uint32_t det, double* probs);
 
+/* Learned SNOCI candidate screener (no counterpart in the reference, which scores every
+ * candidate of the pool by the exhaustive NOCI-PT2 solve, src/snoci/step.rs:330-460, and
+ * selects with select_candidates, src/snoci/operators.rs:1064).  An MLP over the same
+ * determinant descriptor as the learned proposal (din -> 128 -> 128 -> 1, ReLU, BF16 weight
+ * copies, FP32 accumulation, Adam) regresses a target per determinant -- the caller passes
+ * log10 of the selection score |a_a V_a| of candidates it scored exactly -- with a
+ * mean-squared-error loss, trained on the GPU by the engine's own kernels.  Its predictions
+ * rank a pool so that only its highest-ranked part enters the candidate matrix M and GMRES.
+ * Indices refer to the context's resident basis at the time of the call (nw_set_basis). */
+typedef struct nw_screen nw_screen;
+NW_API nw_status nw_screen_create(nw_ctx* ctx, uint64_t seed, nw_screen** out);
+/* Train (or, after the first call, fine-tune) on n rows; targets are standardised with the
+ * mean and spread of the first call's targets. */
+NW_API nw_status nw_screen_train(nw_screen* s, const uint32_t* idx, const double* target, uint64_t n,
+                                 const nw_mlp_opts* opts, nw_mlp_report* rep);
+/* Predicted targets of n resident determinants. */
+NW_API nw_status nw_screen_predict(nw_screen* s, const uint32_t* idx, uint64_t n, double* out);
+NW_API nw_status nw_screen_destroy(nw_screen* s);
+
 /* ---------------------------------------------------------------------------------------
  * NOCI-PT2 / SNOCI linear solve: the candidate-candidate shifted Fock matrix M = F - E0 S
  * stored on the device (packed upper triangle, n (n + 1) / 2 doubles), its mat-vec, and

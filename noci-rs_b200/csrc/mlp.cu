@@ -163,7 +163,45 @@ nw_status colsum(nw_ctx* ctx, Mlp* m, const float* x, int B, int N, float* out, 
   return NW_OK;
 }
 
+// Descriptor of a determinant (din floats, zero-padded): one-hot parent reference, one-hot
+// alpha and beta excitation ranks (0..4), and per spin the indicator of the orbitals whose
+// occupation the excitation changes (its holes and particles).
+__global__ void feature_kernel(const nw_det* __restrict__ dets, const uint32_t* __restrict__ rows, uint32_t row0,
+                               int B, int din, int nref, int nmo, float* __restrict__ x) {
+  const int r = blockIdx.x;
+  if (r >= B) return;
+  float* xr = x + (size_t)r * din;
+  for (int j = threadIdx.x; j < din; j += blockDim.x) xr[j] = 0.0f;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const uint32_t g = rows ? rows[r] : row0 + (uint32_t)r;
+  const nw_det d = dets[g];
+  xr[d.parent] = 1.0f;
+  xr[nref + d.rank_a] = 1.0f;
+  xr[nref + 5 + d.rank_b] = 1.0f;
+  const int base_a = nref + 10, base_b = nref + 10 + nmo;
+  for (int k = 0; k < d.rank_a; ++k) {
+    xr[base_a + d.idx_a[k]] = 1.0f;
+    xr[base_a + d.idx_a[4 + k]] = 1.0f;
+  }
+  for (int k = 0; k < d.rank_b; ++k) {
+    xr[base_b + d.idx_b[k]] = 1.0f;
+    xr[base_b + d.idx_b[4 + k]] = 1.0f;
+  }
+}
+
 }  // namespace
+
+int mlp_descriptor_width(int nref, int nmo) { return ((nref + 10 + 2 * nmo) + 31) / 32 * 32; }
+
+nw_status mlp_features(nw_ctx* ctx, Mlp* m, const nw_det* dets, const uint32_t* rows, uint32_t row0, int B,
+                       cudaStream_t s) {
+  if (B < 1 || B > m->bcap || m->din < mlp_descriptor_width(ctx->nref, ctx->nmo))
+    return fail(ctx, NW_ERR_INVALID, "descriptor batch does not fit the network");
+  feature_kernel<<<B, 128, 0, s>>>(dets, rows, row0, B, m->din, ctx->nref, ctx->nmo, m->x);
+  NW_CUDA(ctx, cudaGetLastError());
+  return NW_OK;
+}
 
 size_t mlp_param_count(int din, int nout) {
   return (size_t)kMlpWidth * din + kMlpWidth + (size_t)kMlpWidth * kMlpWidth + kMlpWidth + (size_t)nout * kMlpWidth +

@@ -41,6 +41,11 @@ struct Mlp {
 };
 
 size_t mlp_param_count(int din, int nout);
+// Width of the determinant descriptor (rounded up to 32): nref + 10 + 2 nmo.
+int mlp_descriptor_width(int nref, int nmo);
+// Descriptors of dets[rows[r]] (or dets[row0 + r] when rows is null), r < B <= bcap, into m->x.
+nw_status mlp_features(nw_ctx* ctx, Mlp* m, const nw_det* dets, const uint32_t* rows, uint32_t row0, int B,
+                       cudaStream_t s);
 // Allocates the MLP and initialises it (uniform +-sqrt(6 / fan_in) weights from a Philox stream
 // of `seed`, zero biases).
 nw_status mlp_create(nw_ctx* ctx, Mlp* m, int din, int nout, int bcap, uint64_t seed);

@@ -312,35 +312,9 @@ __global__ void qmc_pairs_kernel(uint64_t n, uint32_t bra, uint2* __restrict__ p
 }
 
 // ---------------------------------------------------------------------------------------
-// Learned proposal: descriptors, training batches, weighted cross entropy, proposal table.
-// Descriptor of a determinant (din floats, zero-padded): one-hot parent reference, one-hot
-// alpha and beta excitation ranks (0..4), and per spin the indicator of the orbitals whose
-// occupation the excitation changes (its holes and particles).
+// Learned proposal: training batches, weighted cross entropy, proposal table (the
+// determinant descriptors are nw::mlp_features).
 // ---------------------------------------------------------------------------------------
-__global__ void feature_kernel(const nw_det* __restrict__ dets, const uint32_t* __restrict__ rows, uint32_t row0,
-                               int B, int din, int nref, int nmo, float* __restrict__ x) {
-  const int r = blockIdx.x;
-  if (r >= B) return;
-  float* xr = x + (size_t)r * din;
-  for (int j = threadIdx.x; j < din; j += blockDim.x) xr[j] = 0.0f;
-  __syncthreads();
-  if (threadIdx.x != 0) return;
-  const uint32_t g = rows ? rows[r] : row0 + (uint32_t)r;
-  const nw_det d = dets[g];
-  xr[d.parent] = 1.0f;
-  xr[nref + d.rank_a] = 1.0f;
-  xr[nref + 5 + d.rank_b] = 1.0f;
-  const int base_a = nref + 10, base_b = nref + 10 + nmo;
-  for (int k = 0; k < d.rank_a; ++k) {
-    xr[base_a + d.idx_a[k]] = 1.0f;
-    xr[base_a + d.idx_a[4 + k]] = 1.0f;
-  }
-  for (int k = 0; k < d.rank_b; ++k) {
-    xr[base_b + d.idx_b[k]] = 1.0f;
-    xr[base_b + d.idx_b[4 + k]] = 1.0f;
-  }
-}
-
 // Random minibatch of harvested samples (with replacement).
 __global__ void gather_batch_kernel(const HarvestSample* __restrict__ samples, uint64_t ns, uint64_t seed,
                                     uint64_t step, int B, uint32_t* __restrict__ rows, uint32_t* __restrict__ tbin,
@@ -539,9 +513,9 @@ nw_status batch_loss_grad(nw_qmc* q, int B, double* loss_out) {
   nw_ctx* ctx = q->ctx;
   const cudaStream_t s = q->stream;
   nw::Mlp& m = q->mlp;
-  feature_kernel<<<B, 128, 0, s>>>(ctx->d_dets, q->trows, 0, B, m.din, ctx->nref, ctx->nmo, m.x);
-  NW_CUDA(ctx, cudaGetLastError());
-  nw_status st = nw::mlp_forward(ctx, &m, B, s);
+  nw_status st = nw::mlp_features(ctx, &m, ctx->d_dets, q->trows, 0, B, s);
+  if (st != NW_OK) return st;
+  st = nw::mlp_forward(ctx, &m, B, s);
   if (st != NW_OK) return st;
   sum_kernel<<<1, 256, 0, s>>>(q->tw, B, q->twsum);
   NW_CUDA(ctx, cudaMemsetAsync(q->tloss, 0, sizeof(double), s));
@@ -562,9 +536,8 @@ nw_status build_table(nw_qmc* q) {
   nw::Mlp& m = q->mlp;
   for (uint64_t r0 = 0; r0 < q->q.ndet; r0 += (uint64_t)m.bcap) {
     const int B = (int)std::min<uint64_t>((uint64_t)m.bcap, q->q.ndet - r0);
-    feature_kernel<<<B, 128, 0, s>>>(ctx->d_dets, nullptr, (uint32_t)r0, B, m.din, ctx->nref, ctx->nmo, m.x);
-    NW_CUDA(ctx, cudaGetLastError());
-    const nw_status st = nw::mlp_forward(ctx, &m, B, s);
+    nw_status st = nw::mlp_features(ctx, &m, ctx->d_dets, nullptr, (uint32_t)r0, B, s);
+    if (st == NW_OK) st = nw::mlp_forward(ctx, &m, B, s);
     if (st != NW_OK) return st;
     table_kernel<<<(B + 127) / 128, 128, 0, s>>>(m.z, B, m.nout, (uint32_t)r0, q->pr, q->cdf);
     NW_CUDA(ctx, cudaGetLastError());
@@ -826,7 +799,7 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
     q->h_det_bin = det_bin;
     q->h_bin_off = bin_off;
     if (ok) {
-      const int din = ((ctx->nref + 10 + 2 * ctx->nmo) + 31) / 32 * 32;
+      const int din = nw::mlp_descriptor_width(ctx->nref, ctx->nmo);
       ok = nw::mlp_create(ctx, &q->mlp, din, (int)q->q.nbin, kTrainBatchCap, opts->seed ^ 0x5EEDull) == NW_OK;
     }
   }

@@ -107,7 +107,8 @@ EXPORTED = ("nw_ctx_create", "nw_build_intermediates", "nw_pair_zero_counts", "n
             "nw_qmc_destroy", "nw_qmc_harvest", "nw_qmc_train_proposal", "nw_qmc_set_generator",
             "nw_qmc_proposal_dims", "nw_qmc_mlp_params", "nw_qmc_set_mlp_params", "nw_qmc_mlp_loss_grad",
             "nw_qmc_proposal_probs", "nw_pt2_create", "nw_pt2_apply_m", "nw_pt2_last_apply_ms", "nw_pt2_solve",
-            "nw_pt2_destroy", "nw_sync",
+            "nw_pt2_destroy", "nw_screen_create", "nw_screen_train", "nw_screen_predict", "nw_screen_destroy",
+            "nw_sync",
             "nw_set_timing", "nw_last_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
             "nw_last_error")
 
@@ -162,6 +163,10 @@ def load(path: Optional[str] = None):
     L.nw_pt2_solve.argtypes = [vp, ctypes.POINTER(NwPt2Projection), vp, ctypes.POINTER(NwGmresOpts), vp,
                                ctypes.POINTER(NwGmresInfo)]
     L.nw_pt2_destroy.argtypes = [vp]
+    L.nw_screen_create.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(vp)]
+    L.nw_screen_train.argtypes = [vp, vp, vp, ctypes.c_uint64, ctypes.POINTER(NwMlpOpts), ctypes.POINTER(NwMlpReport)]
+    L.nw_screen_predict.argtypes = [vp, vp, ctypes.c_uint64, vp]
+    L.nw_screen_destroy.argtypes = [vp]
     L.nw_sync.argtypes = [vp, vp]
     L.nw_set_timing.argtypes = [vp, ctypes.c_int]
     L.nw_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
@@ -517,6 +522,51 @@ class Pt2:
         if getattr(self, "_p", None) and self._p.value:
             self._lib.nw_pt2_destroy(self._p)
             self._p = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Screen:
+    """Learned SNOCI candidate screener on the GPU (nw_screen_*): an MLP over determinant
+    descriptors regressing a per-determinant target (log10 of the PT2 selection score).
+    Indices refer to the resident basis at the time of each call."""
+
+    def __init__(self, wicks: "WicksShared", seed: int = 17):
+        self._w = wicks
+        self._lib = wicks._lib
+        self._s = ctypes.c_void_p()
+        wicks._check(self._lib.nw_screen_create(wicks._ctx, seed, ctypes.byref(self._s)), "nw_screen_create")
+
+    def train(self, idx, target, epochs: int = 20, batch: int = 1024, lr: float = 1e-3, seed: int = 3) -> dict:
+        idx = np.ascontiguousarray(idx, dtype=np.uint32)
+        target = np.ascontiguousarray(target, dtype=np.float64)
+        rep = NwMlpReport()
+        self._w._check(self._lib.nw_screen_train(self._s, idx.ctypes.data, target.ctypes.data, idx.shape[0],
+                                                 ctypes.byref(NwMlpOpts(epochs, batch, lr, seed)), ctypes.byref(rep)),
+                       "nw_screen_train")
+        return {"loss_first": rep.loss_first, "loss_last": rep.loss_last, "samples": rep.samples, "steps": rep.steps}
+
+    def predict(self, idx) -> np.ndarray:
+        idx = np.ascontiguousarray(idx, dtype=np.uint32)
+        out = np.empty(idx.shape[0])
+        self._w._check(self._lib.nw_screen_predict(self._s, idx.ctypes.data, idx.shape[0], out.ctypes.data),
+                       "nw_screen_predict")
+        return out
+
+    def close(self):
+        if getattr(self, "_s", None) and self._s.value:
+            self._lib.nw_screen_destroy(self._s)
+            self._s = ctypes.c_void_p()
 
     def __del__(self):
         try:
