@@ -350,6 +350,10 @@ class WicksShared:
         k = k.value
         return evals[:k].copy(), c[:n * k].reshape(n, k).copy()
 
+    def pt2(self, candidates, e0: float) -> "Pt2":
+        """The packed candidate matrix M = F - E0 S over resident determinants (nw_pt2_create)."""
+        return Pt2(self, candidates, e0)
+
     def set_timing(self, enable: bool = True):
         self._check(self._lib.nw_set_timing(self._ctx, 1 if enable else 0), "nw_set_timing")
 

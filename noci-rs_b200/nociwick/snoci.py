@@ -278,6 +278,7 @@ class SnociOptions:
     density_phases: bool = True     # reference density convention (see noci_density)
     keep_fraction: float = 0.25     # learned screener: share of the pool kept for PT2
     min_keep: int = 64
+    audit: bool = False             # screened iterations also score the whole pool (the judge)
 
 
 @dataclass
@@ -293,6 +294,9 @@ class SnociIteration:
     selected: int
     seconds: float
     screened: bool
+    recall: Optional[float] = None        # audit: exhaustive top picks found among the kept
+    best_kept: Optional[bool] = None       # audit: the exhaustive best candidate was kept
+    same_selection: Optional[bool] = None  # audit: the screened step selected the same set
 
 
 @dataclass
@@ -304,6 +308,7 @@ class SnociResult:
     labels: list
     iterations: List[SnociIteration] = field(default_factory=list)
     stop: str = ""
+    added: list = field(default_factory=list)   # labels selected by the last iteration
 
 
 def solve_current_space(wicks, m: int, tol: float):
@@ -322,7 +327,6 @@ def pt2_scores(wicks, m: int, cand: np.ndarray, c: np.ndarray, ecurrent: float, 
     transposed contractions are equal), V^Omega = H_ai c - E_current s_a0, GMRES on
     M^Omega a = -V^Omega, E_PT2 = a.M^Omega a + 2 a.V^Omega and the scores |a_a V_a^Omega|
     (src/snoci/step.rs:265-441).  Returns (scores, E_PT2, E0, GMRES info)."""
-    from .lib import Pt2
     cur = np.arange(m, dtype=np.uint32)
     cand = np.ascontiguousarray(cand, dtype=np.uint32)
     h_ai, s_ai = wicks.build_hs_matrix(cand, cur, symmetric=False)
@@ -332,7 +336,7 @@ def pt2_scores(wicks, m: int, cand: np.ndarray, c: np.ndarray, ecurrent: float, 
     s_a0 = s_ai @ c
     f_a0 = f_ai @ c
     v_omega = h_ai @ c - ecurrent * s_a0
-    with Pt2(wicks, cand, e0) as pt:
+    with wicks.pt2(cand, e0) as pt:
         amp, info = pt.solve(e0, s_a0, s_a0, f_a0, f_a0, -v_omega, max_iter=opts.gmres_max_iter,
                              restart=opts.gmres_restart, res_tol=opts.gmres_res_tol,
                              preconditioner=opts.preconditioner)
@@ -368,7 +372,7 @@ def snoci(wicks, system, opts: SnociOptions, screener=None) -> SnociResult:
         cand_all = np.arange(m, m + npool, dtype=np.uint32)
         screened = screener is not None and screener.ready
         if screened:
-            keep = screener.keep(cand_all, opts)
+            keep = screener.keep(cand_all, opts, pool.states)
         else:
             keep = np.arange(npool)
         cand = cand_all[keep]
@@ -376,13 +380,22 @@ def snoci(wicks, system, opts: SnociOptions, screener=None) -> SnociResult:
         scores = np.zeros(npool)
         scores[keep] = kept_scores
         if screener is not None:
-            screener.learn(cand, kept_scores)
+            screener.learn(cand, kept_scores, pool.states[keep])
         remaining = max(opts.max_dim - m, 0)
         chosen = select_candidates(scores, opts.sigma, min(opts.max_add, remaining)) if remaining else np.zeros(0, int)
+        seconds = time.perf_counter() - t0
+        recall = best = same = None
+        if screened and opts.audit:
+            exact, _, _, _ = pt2_scores(wicks, m, cand_all, c, ecurrent, opts)
+            top = select_candidates(exact, opts.sigma, min(opts.max_add, remaining)) if remaining else chosen
+            recall = float(np.isin(top, keep).mean()) if top.size else 1.0
+            best = bool(np.isin(top[:1], keep).all())
+            same = set(top.tolist()) == set(chosen.tolist())
         rec = SnociIteration(it, m, npool, int(cand.shape[0]), ecurrent, e0, ept2, info, int(chosen.shape[0]),
-                             time.perf_counter() - t0, screened)
+                             seconds, screened, recall, best, same)
         result = SnociResult(ecurrent, ept2, c, sel, sel_labels,
-                             ([] if result is None else result.iterations) + [rec])
+                             ([] if result is None else result.iterations) + [rec],
+                             added=[pool.labels[i] for i in chosen])
         if remaining == 0:
             result.stop = "max_dim"
             return result
@@ -397,35 +410,61 @@ def snoci(wicks, system, opts: SnociOptions, screener=None) -> SnociResult:
         sel = np.concatenate([sel, new_states])
         sel_labels = sel_labels + new_labels
         pool.update(sel_labels, new_states, new_labels)
-    # maximum iteration reached: the energy of the final selected space
+    # maximum iteration reached: the state of the last iteration (its current-space energy,
+    # before that iteration's selections), as snoci_step returns final_state (step.rs:525-549)
+    if result is not None:
+        result.stop = "max_iter"
+        return result
     wicks.set_basis(to_nw_dets(sel))
     energy, c = solve_current_space(wicks, sel.shape[0], opts.lin_tol)
-    return SnociResult(energy, result.ept2 if result else 0.0, c, sel, sel_labels,
-                       result.iterations if result else [], "max_iter")
+    return SnociResult(energy, 0.0, c, sel, sel_labels, [], "max_iter")
+
+
+def _excitation_class(states: np.ndarray) -> np.ndarray:
+    """(parent, rank_a, rank_b) of each state as one integer."""
+    return (states["parent"].astype(np.int64) * 64 + _popcount(states["ha"]) * 8 + _popcount(states["hb"]))
 
 
 class LearnedScreen:
     """Learned screening policy for ``snoci``: the first iteration scores the whole pool
     (exhaustive) and trains the GPU screener (``lib.Screen``) on log10 of the scores; later
-    iterations keep the ``keep_fraction`` of the pool (at least ``min_keep``) that the screener
-    ranks highest, score only those exactly (M and GMRES over the kept candidates) and
-    fine-tune the screener on them.  Selection still uses the exact scores."""
+    iterations score exactly (M and GMRES) only
+      * every candidate of an excitation class (parent, rank_a, rank_b) with fewer than
+        ``min_class`` exactly scored examples so far (new classes appear as the selected space
+        grows: excitations of selected determinants reach triples and quadruples), and
+      * the candidates the screener ranks highest, up to ``keep_fraction`` of the pool (at
+        least ``min_keep``),
+    and fine-tune the screener on them.  Selection still uses the exact scores."""
 
     def __init__(self, wicks, epochs: int = 40, finetune_epochs: int = 10, batch: int = 1024, lr: float = 2e-3,
-                 floor: float = 1e-14, seed: int = 17):
+                 floor: float = 1e-14, seed: int = 17, min_class: int = 32):
         from .lib import Screen
         self.net = Screen(wicks, seed)
         self.epochs, self.finetune_epochs, self.batch, self.lr, self.floor = epochs, finetune_epochs, batch, lr, floor
+        self.min_class = min_class
+        self.clip: Optional[float] = None   # targets below the first set's median are clipped to it
+        self.seen: dict = {}
         self.ready = False
         self.reports: List[dict] = []
 
-    def keep(self, cand_all: np.ndarray, opts: SnociOptions) -> np.ndarray:
+    def keep(self, cand_all: np.ndarray, opts: SnociOptions, states: np.ndarray) -> np.ndarray:
+        cls = _excitation_class(states)
+        explore = np.array([self.seen.get(int(c), 0) < self.min_class for c in cls], bool)
         pred = self.net.predict(cand_all)
+        pred[explore] = np.inf
         nkeep = min(cand_all.shape[0], max(opts.min_keep, int(np.ceil(opts.keep_fraction * cand_all.shape[0]))))
+        nkeep = max(nkeep, int(explore.sum()))
         return np.sort(np.argsort(-pred, kind="stable")[:nkeep])
 
-    def learn(self, cand: np.ndarray, scores: np.ndarray):
+    def learn(self, cand: np.ndarray, scores: np.ndarray, states: np.ndarray):
+        for c, k in zip(*np.unique(_excitation_class(states), return_counts=True)):
+            self.seen[int(c)] = self.seen.get(int(c), 0) + int(k)
         target = np.log10(np.maximum(scores, self.floor))
+        if self.clip is None:
+            self.clip = float(np.median(target))
+        # only the ranking of the upper half matters for selection: the negligible tail is
+        # flattened so the fit spends its capacity there
+        target = np.maximum(target, self.clip)
         rep = self.net.train(cand, target, epochs=self.finetune_epochs if self.ready else self.epochs,
                              batch=min(self.batch, max(1, cand.shape[0])), lr=self.lr, seed=len(self.reports) + 1)
         self.reports.append(rep)
