@@ -85,6 +85,9 @@ def workload(name: str, npairs: int, rank: int):
     return system, basis, pairs.astype(np.uint32), cfg
 
 
+EVAL_TRAFFIC_CONFIG2_10M = 1_438_561_280  # bytes per step, see profiles/eval_traffic_config2_10Mpairs.md
+
+
 def rank_seed(base: int, rank: int) -> int:
     """Each rank evaluates its own batch: the seed of rank r's pair sample."""
     return base + rank
@@ -594,6 +597,13 @@ def run_ours(args, rank, world, local_rank):
     alg_bytes = algorithmic_bytes(basis, pairs)
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (ev_ms / 1e3) / 1e9
+    # DRAM bytes (read + write) of one step's evaluator launches, measured by ncu on this
+    # default workload (profiles/eval_traffic_config2_10Mpairs.md); other workloads: not captured
+    traffic, traffic_src = None, None
+    if args.workload == "config2" and npairs == 10_000_000:
+        traffic = EVAL_TRAFFIC_CONFIG2_10M
+        traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one step's evaluator launches, " \
+                      "profiles/eval_traffic_config2_10Mpairs.md"
     clocks = clk.summary()
     # classify, scan, scatter, then the light / medium / heavy / runtime-rank evaluator kernels
     # and, when some reference pair has zero-overlap orbital pairs, the generic evaluator
@@ -608,7 +618,8 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": npairs * 8, "d2h_bytes_per_step": npairs * 16,
                 "gpu_launches": kernels_per_step * args.steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "evaluator phase (eval_light/medium/heavy/rt kernels + eval_gen_kernel)",
+                     "traffic": traffic, "traffic_source": traffic_src,
+                     "kernel": "evaluator phase (eval_light/medium/heavy/rt kernels + eval_gen_kernel)",
                      "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_step": alg_bytes,
                      "eval_ms": ev_ms, "phase_ms": phase_ms},
         "clocks": clocks,
