@@ -61,8 +61,8 @@ def parse():
     ap.add_argument("--no-snoci", action="store_true", help="skip the selected-NOCI screening leg")
     ap.add_argument("--qmc-equil", type=int, default=40, help="QMC equilibration report blocks")
     ap.add_argument("--qmc-train-epochs", type=int, default=2, help="epochs of proposal training")
-    ap.add_argument("--qmc-compare-reports", type=int, default=400,
-                    help="report blocks per generator in the uniform vs learned comparison (0: skip it)")
+    ap.add_argument("--qmc-compare-reports", type=int, default=2000,
+                    help="report blocks (10 steps each) per generator in the uniform vs learned comparison (0: skip)")
     return ap.parse_args()
 
 
@@ -290,7 +290,9 @@ def qmc_leg(args, rank, world, local_rank, dist):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = qmc_cpu_baseline(system, basis, c0, refs, q, float(rep["shift"][-1]))
     if args.qmc_compare_reports > 0:
-        out["generators"] = compare_generators(q, args.qmc_compare_reports, epochs=args.qmc_train_epochs)
+        n = args.qmc_compare_reports
+        out["generators"] = compare_generators(q, n, epochs=args.qmc_train_epochs,
+                                               harvest_reports=max(1, min(200, n // 10)))
     q.close()
     w.close()
     return out
@@ -443,41 +445,48 @@ def blocking_error(x):
     return best
 
 
-def compare_generators(q, nreports, target=1e-4, epochs=2):
+def compare_generators(q, nreports, target=1e-4, epochs=2, harvest_reports=200):
     """Wall time to a 0.1 mEh projected-energy error bar, uniform generator vs the learned
-    proposal, from the equilibrated state of the steps/s run: the uniform generator runs
-    `nreports` blocks; then the attempts of two blocks are harvested, the proposal is trained
-    on the GPU (harvest + training time counted against the learned generator) and the
-    learned mixture runs `nreports` blocks.  Each run's error bar comes from a blocking
-    analysis of the per-block projected energies; the time to `target` scales the run's
-    device time by (error / target)^2."""
-    def measure(tag):
-        rep = q.run(nreports)
-        ms = q.last_run_ms()
+    proposal, each over `nreports` report blocks (2x10^4 steps by default) from the equilibrated
+    state of the steps/s run.  Uniform arm: all blocks with the uniform generator.  Learned arm:
+    the first `harvest_reports` blocks (2000 steps) run the uniform generator while attempts are
+    harvested (thinned at random to fit the 4.2M-sample buffer), the proposal is trained on the
+    GPU, and the remaining blocks use the learned mixture.  Each arm's error bar comes from a
+    blocking analysis of the per-block projected energies of its measured blocks (all blocks
+    for the uniform arm, the learned blocks for the learned arm); the time to `target` scales
+    the measured blocks' device time by (error / target)^2, plus, for the learned arm, the
+    harvest blocks and the training."""
+    def stats(rep, ms):
         e = rep["eproj_num"] / rep["eproj_den"]
         err = blocking_error(e)
-        return {"reports": int(nreports), "steps": int(nreports * 10), "device_ms": ms,
+        return {"reports": int(rep.shape[0]), "steps": int(rep.shape[0] * 10), "device_ms": ms,
                 "eproj": float(rep["eproj_num"].sum() / rep["eproj_den"].sum()), "error_bar": err,
                 "attempts_per_step": float(rep["nattempts"].mean() / 10), "walkers_mean": float(rep["nw"].mean()),
-                "shift_mean": float(rep["shift"].mean()),
-                "seconds_to_0.1mEh": ms / 1e3 * (err / target) ** 2}
-    out = {"uniform": measure("uniform")}
-    t0 = time.perf_counter()
-    q.harvest(True)
-    q.run(2)
+                "shift_mean": float(rep["shift"].mean()), "seconds_to_0.1mEh": ms / 1e3 * (err / target) ** 2}
+    rep = q.run(nreports)
+    out = {"uniform": stats(rep, q.last_run_ms())}
+    attempts_per_report = float(rep["nattempts"].mean())
+    keep = min(1.0, 4_194_304 / max(1.0, attempts_per_report * harvest_reports))
+    q.harvest(True, keep)
+    rep_h = q.run(harvest_reports)
+    harvest_ms = q.last_run_ms()
     q.harvest(False)
+    t0 = time.perf_counter()
     tr = q.train_proposal(epochs=epochs, batch=4096, lr=1e-3, seed=5)
     train_s = time.perf_counter() - t0
     q.set_generator(True, 0.1)
-    lr_ = measure("learned")
+    rep_l = q.run(nreports - harvest_reports)
+    lr_ = stats(rep_l, q.last_run_ms())
     q.set_generator(False, 0.1)
-    lr_["harvest_train_s"] = train_s
-    lr_["training"] = {k: (float(v) if isinstance(v, float) else int(v)) for k, v in tr.items()}
-    lr_["seconds_to_0.1mEh_incl_training"] = lr_["seconds_to_0.1mEh"] + train_s
-    lr_["mix"] = 0.1
+    lr_.update({"harvest_reports": int(harvest_reports), "harvest_keep_probability": keep,
+                "harvest_device_ms": harvest_ms, "train_seconds": train_s,
+                "training": {k: (float(v) if isinstance(v, float) else int(v)) for k, v in tr.items()},
+                "mix": 0.1})
+    lr_["seconds_to_0.1mEh_incl_harvest_training"] = lr_["seconds_to_0.1mEh"] + harvest_ms / 1e3 + train_s
     out["learned"] = lr_
-    out["note"] = ("same walker state; each generator's time to a 0.1 mEh error bar = its run's device time x "
-                   "(blocking error / 1e-4)^2")
+    out["speedup_to_0.1mEh"] = out["uniform"]["seconds_to_0.1mEh"] / lr_["seconds_to_0.1mEh_incl_harvest_training"]
+    out["note"] = ("same walker state at the start of each arm; time to a 0.1 mEh error bar = the measured blocks' "
+                   "device time x (blocking error / 1e-4)^2 (+ harvest blocks and training for the learned arm)")
     return out
 
 

@@ -294,9 +294,11 @@ typedef struct nw_mlp_report {
     int32_t pad;
 } nw_mlp_report;
 
-/* Record (parent, child bin, weight) of every attempt of the following runs (enable = 1 clears
- * the buffer of 4,194,304 attempts; later attempts beyond it are not recorded). */
-NW_API nw_status nw_qmc_harvest(nw_qmc* q, int32_t enable);
+/* Record (parent, child bin, weight) of the attempts of the following runs, each with
+ * probability keep_probability in (0, 1] (an unbiased thinning, so that a long stretch of steps
+ * fits the buffer); enable = 1 clears the buffer of 4,194,304 attempts, attempts beyond it are
+ * not recorded. */
+NW_API nw_status nw_qmc_harvest(nw_qmc* q, int32_t enable, double keep_probability);
 /* Train the proposal network on the harvested attempts and rebuild p(bin | parent) for every
  * determinant. */
 NW_API nw_status nw_qmc_train_proposal(nw_qmc* q, const nw_mlp_opts* opts, nw_mlp_report* rep);

@@ -65,6 +65,7 @@ struct QmcParams {
   uint32_t nbin;    // proposal bins (child reference x rank class)
   uint32_t pad;
   uint64_t hcap;    // harvest buffer capacity
+  double hkeep;     // probability of recording an attempt while harvesting
 };
 
 // One harvested attempt: parent, the child's bin and the weight |H - E^S S| / ((N - 1) pgen),
@@ -150,14 +151,38 @@ __device__ __forceinline__ uint64_t owner_of(const uint32_t* __restrict__ off, u
   return lo;
 }
 
+// Attempts are grouped in chunks of 2^kChunkShift; cown[c] = owner of the chunk's first attempt.
+constexpr int kChunkShift = 8;
+
+__global__ void qmc_chunk_kernel(QmcParams q, const QmcState* __restrict__ st, const uint32_t* __restrict__ off,
+                                 uint32_t* __restrict__ cown) {
+  const uint32_t n = st->npairs;
+  const uint32_t nchunk = (n + (1u << kChunkShift) - 1) >> kChunkShift;
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunk; c += gridDim.x * blockDim.x)
+    cown[c] = (uint32_t)owner_of(off, q.ndet, c << kChunkShift);
+}
+
 __global__ void qmc_spawn_kernel(QmcParams q, Proposal pr, const QmcState* __restrict__ st,
-                                 const uint32_t* __restrict__ off, const double* __restrict__ sampled,
+                                 const uint32_t* __restrict__ off, const uint32_t* __restrict__ cown,
+                                 const double* __restrict__ sampled,
                                  const uint32_t* __restrict__ na, uint2* __restrict__ pairs, uint32_t* __restrict__ child,
                                  uint32_t* __restrict__ parent, double* __restrict__ amp, double* __restrict__ pg) {
   const uint32_t n = st->npairs;
   const uint64_t cycle = st->cycle;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const uint64_t g = owner_of(off, q.ndet, t);
+    // owners of this chunk's first attempt and of the next chunk's bound the search
+    const uint32_t c = t >> kChunkShift;
+    const uint64_t lo = cown[c];
+    const uint64_t hi = ((uint64_t)(c + 1) << kChunkShift) < n ? cown[c + 1] : q.ndet - 1;
+    uint64_t a = lo, b = hi + 1;  // off[a] <= t < off[b]
+    while (b - a > 1) {
+      const uint64_t mid = (a + b) >> 1;
+      if (off[mid] <= t)
+        a = mid;
+      else
+        b = mid;
+    }
+    const uint64_t g = a;
     double u0, u1;
     nwq::uniform2(q.seed, cycle, t, nwq::kDrawChild, &u0, &u1);
     uint64_t lam;
@@ -209,7 +234,7 @@ __global__ void qmc_apply_kernel(QmcParams q, Proposal pr, const QmcState* __res
     const double raw = nwq::spawn_amplitude(q.prop, q.dt, es, v.x, v.y, amp[t], pgen);
     const double dn = nwq::fri(raw, q.c_spawn, nwq::uniform1(q.seed, cycle, t, nwq::kDrawSpawn));
     if (dn != 0.0) atomicAdd(delta + child[t], dn);
-    if (q.harvest) {
+    if (q.harvest && (q.hkeep >= 1.0 || nwq::uniform1(q.seed, cycle, t, nwq::kDrawHarvest) < q.hkeep)) {
       const unsigned long long k = atomicAdd(pr.nsamples, 1ull);
       if (k < q.hcap) {
         HarvestSample hsmp;
@@ -415,6 +440,7 @@ struct nw_qmc {
   double* delta = nullptr;
   uint32_t* na = nullptr;
   uint32_t* off = nullptr;
+  uint32_t* cown = nullptr;  // owner of the first attempt of each chunk
   uint32_t* tsum = nullptr;
   double2* diag = nullptr;
   double2* refhs = nullptr;
@@ -460,7 +486,8 @@ nw_status enqueue_cycle(nw_qmc* q) {
   nw_status st = nw::scan_exclusive(ctx, q->na, nd, q->off, q->tsum, s);
   if (st != NW_OK) return st;
   qmc_count_kernel<<<1, 1, 0, s>>>(q->q, q->st, q->off);
-  qmc_spawn_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(q->q, q->pr, q->st, q->off, q->sampled, q->na,
+  qmc_chunk_kernel<<<grid_for((q->q.cap >> kChunkShift) + 1), kBlockThreads, 0, s>>>(q->q, q->st, q->off, q->cown);
+  qmc_spawn_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(q->q, q->pr, q->st, q->off, q->cown, q->sampled, q->na,
                                                                 q->pairs, q->child, q->parent, q->amp, q->pg);
   NW_CUDA(ctx, cudaGetLastError());
   st = nw::launch_sorted(ctx, q->P, q->nkeys, reinterpret_cast<const uint32_t*>(q->pairs), q->q.cap,
@@ -556,13 +583,14 @@ void invalidate_graph(nw_qmc* q) {
 
 extern "C" {
 
-nw_status nw_qmc_harvest(nw_qmc* q, int32_t enable) {
-  if (!q) return NW_ERR_INVALID;
+nw_status nw_qmc_harvest(nw_qmc* q, int32_t enable, double keep_probability) {
+  if (!q || !(keep_probability > 0.0) || !(keep_probability <= 1.0)) return NW_ERR_INVALID;
   if (!q->learnable) return qmc_fail(q, NW_ERR_UNSUPPORTED, "learned proposal needs at most 8 references");
   NW_CUDA(q->ctx, cudaSetDevice(q->ctx->device));
   if (enable) NW_CUDA(q->ctx, cudaMemsetAsync(q->pr.nsamples, 0, sizeof(unsigned long long), q->stream));
   NW_CUDA(q->ctx, cudaStreamSynchronize(q->stream));
   q->q.harvest = enable ? 1 : 0;
+  q->q.hkeep = keep_probability;
   invalidate_graph(q);
   return NW_OK;
 }
@@ -719,7 +747,8 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
                    0.1,
                    (uint32_t)ctx->nref * kRankBins,
                    0,
-                   kHarvestCap};
+                   kHarvestCap,
+                   1.0};
   bool ok = true;
   auto take = [&](auto*& p, size_t count) {
     using T = std::remove_reference_t<decltype(*p)>;
@@ -732,6 +761,7 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
   take(q->delta, nd);
   take(q->na, nd);
   take(q->off, nd + 1);
+  take(q->cown, (cap >> kChunkShift) + 2);
   take(q->tsum, nd / 4096 + 1);
   take(q->diag, nd);
   take(q->refhs, nd);

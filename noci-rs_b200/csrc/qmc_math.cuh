@@ -56,6 +56,7 @@ constexpr uint32_t kDrawChild = 2;   // uniform child of a spawning attempt
 constexpr uint32_t kDrawSpawn = 3;   // FRI rounding of a spawned amplitude
 constexpr uint32_t kDrawChildBin = 4;  // bin and member of a learned-proposal attempt
 constexpr uint32_t kDrawTrain = 5;   // minibatch draws of the proposal training
+constexpr uint32_t kDrawHarvest = 6;  // thinning of the harvested attempts
 
 // Two uniform doubles in [0, 1) with 53 random bits each, for (seed, cycle, index, purpose).
 NWQ_HD void uniform2(uint64_t seed, uint64_t cycle, uint64_t index, uint32_t purpose, double* u0, double* u1) {

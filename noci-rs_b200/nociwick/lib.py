@@ -148,7 +148,7 @@ def load(path: Optional[str] = None):
     L.nw_qmc_set_populations.argtypes = [vp, vp]
     L.nw_qmc_cycle_delta.argtypes = [vp, ctypes.c_uint64, vp]
     L.nw_qmc_destroy.argtypes = [vp]
-    L.nw_qmc_harvest.argtypes = [vp, ctypes.c_int32]
+    L.nw_qmc_harvest.argtypes = [vp, ctypes.c_int32, ctypes.c_double]
     L.nw_qmc_train_proposal.argtypes = [vp, ctypes.POINTER(NwMlpOpts), ctypes.POINTER(NwMlpReport)]
     L.nw_qmc_set_generator.argtypes = [vp, ctypes.c_int32, ctypes.c_double]
     L.nw_qmc_proposal_dims.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
@@ -422,9 +422,10 @@ class Qmc:
         return out
 
     # -- learned proposal -------------------------------------------------------------------
-    def harvest(self, enable: bool = True):
-        """Record the attempts of the following runs for training the proposal."""
-        self._w._check(self._lib.nw_qmc_harvest(self._q, 1 if enable else 0), "nw_qmc_harvest")
+    def harvest(self, enable: bool = True, keep: float = 1.0):
+        """Record the attempts of the following runs (each with probability `keep`) for training
+        the proposal."""
+        self._w._check(self._lib.nw_qmc_harvest(self._q, 1 if enable else 0, keep), "nw_qmc_harvest")
 
     def train_proposal(self, epochs: int = 2, batch: int = 4096, lr: float = 1e-3, seed: int = 7) -> dict:
         rep = NwMlpReport()
