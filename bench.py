@@ -590,6 +590,20 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     barrier()
     t_e2e = ev2.elapsed_time(ev3)
+    # the host link alone: pinned copies of one step's pairs (H2D) and results (D2H) on the
+    # launching stream; the pipelined entry point overlaps both directions with the evaluation,
+    # so a step cannot take less than the slowest of the three
+    h2d_ms, d2h_ms = [], []
+    for dst, src, acc in ((dpairs, hpairs, h2d_ms), (hout, dout, d2h_ms)):
+        for _ in range(2):
+            dst.copy_(src, non_blocking=True)
+        e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e4.record(stream)
+        for _ in range(5):
+            dst.copy_(src, non_blocking=True)
+        e5.record(stream)
+        torch.cuda.synchronize()
+        acc.append(e4.elapsed_time(e5) / 5)
     t_dev, t_e2e = reduce_max([t_dev, t_e2e], dist, f"cuda:{local_rank}")
     hs_host = dout.cpu().numpy() if rank == 0 and world == 1 and not args.no_cpu_baseline else None
     eng.close()
@@ -625,7 +639,12 @@ def run_ours(args, rank, world, local_rank):
                        % (npairs * 8 >> 20, npairs * 16 >> 20, info["slab_bytes"] >> 20),
                        build_seconds=round(build_s, 3), parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": npairs * 8, "d2h_bytes_per_step": npairs * 16,
-                "gpu_launches": kernels_per_step * args.steps},
+                "gpu_launches": kernels_per_step * args.steps,
+                "link": {"h2d_gbs": npairs * 8 / h2d_ms[0] / 1e6, "d2h_gbs": npairs * 16 / d2h_ms[0] / 1e6,
+                         "bound_value": aggregate_rate(npairs, world, 1, max(h2d_ms[0], d2h_ms[0], t_dev / args.steps)),
+                         "frac": e2e / aggregate_rate(npairs, world, 1, max(h2d_ms[0], d2h_ms[0], t_dev / args.steps)),
+                         "note": "pinned copies of one step's buffers timed alone; bound = pairs / max(H2D, D2H, "
+                                 "device step)"}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "traffic_source": traffic_src,
                      "kernel": "evaluator phase (eval_light/medium/heavy/rt kernels + eval_gen_kernel)",
