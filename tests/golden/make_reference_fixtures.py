@@ -338,6 +338,8 @@ FIXTURES = {
     "REF_NOCI_H4_STO-3G_1_75": ("STO-3G", square(1.75), H4_SQUARE_STATES, None, None),
     "REF_NOCI_F2_STO-3G_1_75": ("STO-3G", chain(1.75, (-0.5, 0.5), ["F", "F"]), H2_STATES, None, None),
     "REF_NOCI_LiH_6-31G_2_8": ("6-31G", chain(2.8, (-0.5, 0.5), ["Li", "H"]), LIH_STATES, None, None),
+    "DET_H2_STO-3G_1_5": ("STO-3G", chain(1.5, (-0.5, 0.5)), H2_STATES, (1, 2), None),
+    "DET_F2_sto-3g_1_75": ("STO-3G", chain(1.75, (-0.5, 0.5), ["F", "F"]), H2_STATES, (1, 2), None),
     "PT2_H2_STO-3G_1_5": ("STO-3G", chain(1.5, (-0.5, 0.5)), H2_STATES, (1, 2), {"max_iter": 1, **GMRES_128}),
     "PT2_H2_3-21G_1_5": ("3-21G", chain(1.5, (-0.5, 0.5)), H2_STATES, (1, 2), {"max_iter": 1, **GMRES_128}),
     "SNOCI_H2_STO-3G_1_5": ("STO-3G", chain(1.5, (-0.5, 0.5)), H2_STATES, (1, 2),

@@ -10,6 +10,7 @@ import pytest
 import nociwick
 import reffix
 from nociwick import snoci as sn
+from nociwick import synthetic as sy
 
 pytestmark = pytest.mark.gpu
 
@@ -28,6 +29,18 @@ def test_reference_noci_energy(name):
         w.set_basis(sn.to_nw_dets(st))
         e, _ = sn.solve_current_space(w, st.shape[0], 1e-12)
     assert abs(e - meta["expected"]["reference_noci_energy"]) < 1e-8, (e, meta["expected"])
+
+
+@pytest.mark.parametrize("name", [n for n in NAMES if n.startswith("DET_")])
+def test_deterministic_noci_energy(name):
+    system, meta = reffix.load(name)
+    basis = sy.sd_basis(system.nmo, system.nocc_a, system.nocc_b, len(system.refs), orders=(1, 2),
+                        include_refs=True)
+    with _engine(system) as w:
+        w.set_basis(basis)
+        h, s = w.build_hs_matrix()
+        e, _ = w.general_evp(h, s, project=True, tol=1e-12)
+    assert abs(e[0] - meta["expected"]["deterministic_noci_energy"]) < 1e-8, (e[0], meta["expected"])
 
 
 @pytest.mark.parametrize("name", [n for n in NAMES if n.startswith(("PT2_", "SNOCI_"))])

@@ -8,6 +8,9 @@ ones to 2e-14 Eh); here the oracle's matrix elements give
   first order in the reference orbitals, which the reference's own SCF converges to
   e_tol = 1e-12 only, hence LiH's 2e-9); square H4 includes zero-overlap (m = 1 per spin)
   reference pairs, i.e. the distribution-sum evaluator;
+* the deterministic NOCI-QMC energy (tests/deterministic.rs: converged propagation in the
+  singles-and-doubles basis of the references) as the lowest GEVP root over that basis, to
+  1e-8 Eh (F2: 300 determinants, excited-excited pairs across references);
 * the NOCI-PT2 energy E_current + E_PT2 of one snoci_step (tests/pt2.rs:31-84) and the
   selected-NOCI energy after the fixture's SNOCI iterations (tests/snoci.rs:33-79), through
   the selected-NOCI driver nociwick.snoci run on the dense oracle engine (oracle/engine.py),
@@ -27,6 +30,7 @@ from oracle.engine import DenseEngine
 from oracle.oracle import Oracle
 
 REF_NOCI = [n for n in reffix.names()]
+DET = [n for n in reffix.names() if n.startswith("DET_")]
 PT2 = [n for n in reffix.names() if n.startswith("PT2_")]
 SNOCI = [n for n in reffix.names() if n.startswith("SNOCI_")]
 
@@ -49,6 +53,21 @@ def test_reference_noci_energy(name):
     assert np.allclose(sorted(meta["scf_energies"]), sorted(meta["expected"]["scf_energies"]), atol=1e-12)
     e = reference_noci(system)
     assert abs(e - meta["expected"]["reference_noci_energy"]) < 1e-8, (e, meta["expected"])
+
+
+@pytest.mark.parametrize("name", DET)
+def test_deterministic_noci_energy(name):
+    """The deterministic NOCI-QMC energy of tests/deterministic.rs: its propagation in the
+    singles-and-doubles basis of the references (references included) converges to the lowest
+    root of H c = E S c over that basis."""
+    system, meta = reffix.load(name)
+    basis = sy.sd_basis(system.nmo, system.nocc_a, system.nocc_b, len(system.refs), orders=(1, 2),
+                        include_refs=True)
+    with DenseEngine(system, tol=1e-12) as eng:
+        eng.set_basis(basis)
+        h, s = eng.build_hs_matrix()
+        e, _ = eng.general_evp(h, s, True, 1e-12)
+    assert abs(e[0] - meta["expected"]["deterministic_noci_energy"]) < 1e-8, (e[0], meta["expected"])
 
 
 @pytest.mark.parametrize("name", PT2)
