@@ -775,9 +775,10 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
   take(q->partial, (size_t)kStatBlocks * kStats);
   take(q->ring, kReportRing);
   q->P = nw::make_params(ctx);
-  // fine sort keys sized for the attempts of a typical cycle (about the walker 1-norm), not
-  // for the capacity: every cycle clears and scans all keys
-  const uint64_t typical = (uint64_t)(2.0 * std::max(opts->target_population, opts->initial_population)) + nd;
+  // fine sort keys sized from the walker 1-norm (a quarter of it: every cycle clears and
+  // scans all keys, and finer buckets gain the evaluators less than the scan costs), not from
+  // the attempt capacity
+  const uint64_t typical = (uint64_t)(0.25 * std::max(opts->target_population, opts->initial_population)) + nd;
   q->nkeys = nw::plan_keys(ctx, q->P, std::min<uint64_t>(nw::kFineMax, std::max<uint64_t>(nw::kFineMin, std::min(typical, cap))));
   take(q->S.keys, cap);
   take(q->S.ranks, cap);
