@@ -384,6 +384,21 @@ NW_API nw_status nw_pt2_destroy(nw_pt2* p);
  * earlier device-buffer call (those outputs are NaN). */
 NW_API nw_status nw_sync(nw_ctx* ctx, void* stream);
 
+/* Autotuner (no counterpart in the reference): times nw_eval_hs_pairs_device on the caller's
+ * device pairs (npairs of them, results into hs) for fine sort-key budgets 2^14 .. 2^23 and
+ * 4 / 8 / 16 blocks per SM of the grid-stride kernels, against the defaults, and keeps the
+ * fastest for the later calls on this context (budget 0 and blocks 0 in the report mean the
+ * defaults won).  Synchronises `stream`. */
+typedef struct nw_tune_report {
+    uint64_t key_budget;        /* chosen fine-key budget (0: default, min(2^23, max(2^14, npairs))) */
+    int32_t blocks_per_sm;      /* chosen blocks per SM (0: default 8)                           */
+    int32_t trials;             /* configurations timed                                         */
+    float best_ms;              /* per call, chosen configuration                               */
+    float default_ms;           /* per call, defaults                                           */
+} nw_tune_report;
+NW_API nw_status nw_autotune(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* hs, void* stream,
+                             nw_tune_report* rep);
+
 /* Per-phase device times of the most recent nw_eval_hs_pairs* call, measured with CUDA events
  * recorded on its stream while timing is enabled: ms[0] classify, ms[1] scan, ms[2] scatter,
  * ms[3] m = 0 evaluator, ms[4] m > 0 evaluator.  nw_last_timings waits for that call. */

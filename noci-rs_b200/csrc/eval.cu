@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 #include <string>
 
@@ -518,7 +519,8 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
                         const uint32_t* npairs_dev) {
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[0], stream));
   NW_CUDA(ctx, cudaMemsetAsync(S.counts, 0, sizeof(uint32_t) * nkeys, stream));
-  classify_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(P, pairs, npairs, npairs_dev, S.keys, S.ranks,
+  const int per_sm = ctx->tune_per_sm > 0 ? ctx->tune_per_sm : 8;
+  classify_kernel<<<grid_stride_blocks(npairs, 256, per_sm), 256, 0, stream>>>(P, pairs, npairs, npairs_dev, S.keys, S.ranks,
                                                                           S.counts, out, 2, S.flag);
   NW_CUDA(ctx, cudaGetLastError());
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[1], stream));
@@ -528,7 +530,7 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
   scan_down_kernel<<<ntiles, kScanThreads, 0, stream>>>(S.counts, (uint32_t)nkeys, S.tsum, S.offsets);
   NW_CUDA(ctx, cudaGetLastError());
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[2], stream));
-  scatter_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(S.keys, S.ranks, npairs, npairs_dev,
+  scatter_kernel<<<grid_stride_blocks(npairs, 256, per_sm), 256, 0, stream>>>(S.keys, S.ranks, npairs, npairs_dev,
                                                                          S.offsets, S.sidx);
   NW_CUDA(ctx, cudaGetLastError());
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[3], stream));
@@ -541,10 +543,10 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
     NW_CUDA(ctx, cudaEventRecord(ctx->ev_fork, stream));
     for (int i = 0; i < 2; ++i) NW_CUDA(ctx, cudaStreamWaitEvent(ctx->s_aux[i], ctx->ev_fork, 0));
     if (mode == EvalMode::kFS) {
-      eval_fs_light_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
+      eval_fs_light_kernel<<<grid_stride_blocks(npairs, 256, per_sm), 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
       eval_fs_heavy_kernel<<<148 * 2, 256, 0, ctx->s_aux[0]>>>(P, pp, S.sidx, S.offsets, out);
     } else {
-      eval_light_kernel<<<grid_stride_blocks(npairs, 256, 8), 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
+      eval_light_kernel<<<grid_stride_blocks(npairs, 256, per_sm), 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
       eval_medium_kernel<<<148 * 2, 256, 0, ctx->s_aux[0]>>>(P, pp, S.sidx, S.offsets, out);
       eval_heavy_kernel<<<148, 256, 0, ctx->s_aux[1]>>>(P, pp, S.sidx, S.offsets, out);
       eval_rt_kernel<<<148 * 2, 128, 0, ctx->s_aux[1]>>>(P, pp, S.sidx, S.offsets, out);
@@ -592,7 +594,8 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
     return NW_OK;
   }
 
-  const uint64_t nkeys = plan_keys(ctx, P, std::min(kFineMax, std::max(kFineMin, npairs)));
+  const uint64_t budget = ctx->tune_key_budget ? ctx->tune_key_budget : std::max(kFineMin, npairs);
+  const uint64_t nkeys = plan_keys(ctx, P, std::min(kFineMax, std::max(kFineMin, budget)));
   if ((st = ensure(ctx, ctx->keys, npairs * sizeof(uint32_t))) != NW_OK) return st;
   if ((st = ensure(ctx, ctx->ranks, npairs * sizeof(uint32_t))) != NW_OK) return st;
   if ((st = ensure(ctx, ctx->perm, npairs * sizeof(uint32_t))) != NW_OK) return st;
@@ -705,3 +708,70 @@ nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs
 }
 
 }  // namespace nw
+
+// ---------------------------------------------------------------------------------------
+// Autotuner: the fine sort-key budget (how finely pairs are bucketed by bra determinant
+// before evaluation: locality of the intermediates against the cost of clearing and scanning
+// the counters) and the blocks per SM of the grid-stride kernels, timed on the caller's pairs.
+// ---------------------------------------------------------------------------------------
+extern "C" nw_status nw_autotune(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* hs, void* stream,
+                                 nw_tune_report* rep) {
+  if (!ctx || !pairs || !hs || !rep || npairs == 0) return NW_ERR_INVALID;
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  static const uint64_t kBudgets[] = {1ull << 14, 1ull << 16, 1ull << 18, 1ull << 20, 1ull << 22, 1ull << 23};
+  static const int kPerSm[] = {4, 8, 16};
+  const uint64_t saved_budget = ctx->tune_key_budget;
+  const int saved_per_sm = ctx->tune_per_sm;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    return nw::fail(ctx, NW_ERR_CUDA, "autotune events");
+  }
+  std::memset(rep, 0, sizeof(*rep));
+  float best = 0.0f, dflt = 0.0f;
+  uint64_t best_budget = 0;
+  int best_per_sm = 0, trials = 0;
+  nw_status st = NW_OK;
+  // (0, 0) first: the untuned defaults
+  for (int b = -1; b < (int)(sizeof(kBudgets) / sizeof(kBudgets[0])) && st == NW_OK; ++b) {
+    for (int g = 0; g < (int)(sizeof(kPerSm) / sizeof(kPerSm[0])) && st == NW_OK; ++g) {
+      if (b < 0 && g > 0) break;
+      ctx->tune_key_budget = b < 0 ? 0 : kBudgets[b];
+      ctx->tune_per_sm = b < 0 ? 0 : kPerSm[g];
+      float ms = 0.0f;
+      for (int rep_i = 0; rep_i < 4 && st == NW_OK; ++rep_i) {
+        if (rep_i == 1 && cudaEventRecord(e0, s) != cudaSuccess) st = NW_ERR_CUDA;
+        if (st == NW_OK) st = nw::eval_pairs(ctx, pairs, npairs, hs, nw::EvalMode::kHS, s);
+      }
+      if (st == NW_OK && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+        st = nw::fail(ctx, NW_ERR_CUDA, "autotune timing");
+      if (st != NW_OK) break;
+      ms /= 3.0f;
+      ++trials;
+      if (b < 0) dflt = ms;
+      if (best_budget == 0 && best_per_sm == 0 && b < 0) best = ms;
+      if (b >= 0 && ms < best) {
+        best = ms;
+        best_budget = kBudgets[b];
+        best_per_sm = kPerSm[g];
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != NW_OK) {
+    ctx->tune_key_budget = saved_budget;
+    ctx->tune_per_sm = saved_per_sm;
+    return st;
+  }
+  ctx->tune_key_budget = best_budget;  // 0 / 0 keeps the defaults when they were fastest
+  ctx->tune_per_sm = best_per_sm;
+  rep->key_budget = best_budget;
+  rep->blocks_per_sm = best_per_sm;
+  rep->trials = trials;
+  rep->best_ms = best;
+  rep->default_ms = dflt;
+  return NW_OK;
+}

@@ -80,6 +80,11 @@ class NwMlpReport(ctypes.Structure):
                 ("steps", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
+class NwTuneReport(ctypes.Structure):
+    _fields_ = [("key_budget", ctypes.c_uint64), ("blocks_per_sm", ctypes.c_int32), ("trials", ctypes.c_int32),
+                ("best_ms", ctypes.c_float), ("default_ms", ctypes.c_float)]
+
+
 class NwPt2Projection(ctypes.Structure):
     _fields_ = [("e0", ctypes.c_double), ("s_a0", ctypes.c_void_p), ("s_0a", ctypes.c_void_p),
                 ("f_a0", ctypes.c_void_p), ("f_0a", ctypes.c_void_p)]
@@ -108,7 +113,7 @@ EXPORTED = ("nw_ctx_create", "nw_build_intermediates", "nw_pair_zero_counts", "n
             "nw_qmc_proposal_dims", "nw_qmc_mlp_params", "nw_qmc_set_mlp_params", "nw_qmc_mlp_loss_grad",
             "nw_qmc_proposal_probs", "nw_pt2_create", "nw_pt2_apply_m", "nw_pt2_last_apply_ms", "nw_pt2_solve",
             "nw_pt2_destroy", "nw_screen_create", "nw_screen_train", "nw_screen_predict", "nw_screen_destroy",
-            "nw_sync",
+            "nw_autotune", "nw_sync",
             "nw_set_timing", "nw_last_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
             "nw_last_error")
 
@@ -167,6 +172,7 @@ def load(path: Optional[str] = None):
     L.nw_screen_train.argtypes = [vp, vp, vp, ctypes.c_uint64, ctypes.POINTER(NwMlpOpts), ctypes.POINTER(NwMlpReport)]
     L.nw_screen_predict.argtypes = [vp, vp, ctypes.c_uint64, vp]
     L.nw_screen_destroy.argtypes = [vp]
+    L.nw_autotune.argtypes = [vp, vp, ctypes.c_uint64, vp, vp, ctypes.POINTER(NwTuneReport)]
     L.nw_sync.argtypes = [vp, vp]
     L.nw_set_timing.argtypes = [vp, ctypes.c_int]
     L.nw_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
@@ -349,6 +355,14 @@ class WicksShared:
                                              evals.ctypes.data, c.ctypes.data, ctypes.byref(k)), "nw_general_evp")
         k = k.value
         return evals[:k].copy(), c[:n * k].reshape(n, k).copy()
+
+    def autotune(self, pairs_ptr: int, npairs: int, out_ptr: int, stream: int = 0) -> dict:
+        """nw_autotune on device pairs: picks the fine-key budget and blocks per SM of later calls."""
+        rep = NwTuneReport()
+        self._check(self._lib.nw_autotune(self._ctx, ctypes.c_void_p(pairs_ptr), npairs, ctypes.c_void_p(out_ptr),
+                                          ctypes.c_void_p(stream), ctypes.byref(rep)), "nw_autotune")
+        return {"key_budget": rep.key_budget, "blocks_per_sm": rep.blocks_per_sm, "trials": rep.trials,
+                "best_ms": rep.best_ms, "default_ms": rep.default_ms}
 
     def pt2(self, candidates, e0: float) -> "Pt2":
         """The packed candidate matrix M = F - E0 S over resident determinants (nw_pt2_create)."""

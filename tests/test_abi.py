@@ -46,6 +46,7 @@ int main(void) {
          offsetof(nw_gmres_opts, preconditioner), sizeof(nw_gmres_info));
   printf("%zu %zu %zu %zu\n", sizeof(nw_mlp_opts), offsetof(nw_mlp_opts, seed), sizeof(nw_mlp_report),
          offsetof(nw_mlp_report, steps));
+  printf("%zu %zu %zu\n", sizeof(nw_tune_report), offsetof(nw_tune_report, trials), offsetof(nw_tune_report, default_ms));
   return 0;
 }
 ''')
@@ -66,6 +67,7 @@ int main(void) {
                         L.NwGmresOpts.preconditioner.offset, ctypes.sizeof(L.NwGmresInfo)]
     assert v[22:26] == [ctypes.sizeof(L.NwMlpOpts), L.NwMlpOpts.seed.offset, ctypes.sizeof(L.NwMlpReport),
                         L.NwMlpReport.steps.offset]
+    assert v[26:29] == [ctypes.sizeof(L.NwTuneReport), L.NwTuneReport.trials.offset, L.NwTuneReport.default_ms.offset]
 
 
 def test_header_compiles_as_cxx(tmp_path):

@@ -102,6 +102,26 @@ def test_device_entry_matches_host_entry_and_is_deterministic():
     assert np.array_equal(dev1, dev2)
 
 
+def test_autotune_keeps_every_result_bit():
+    """nw_autotune only changes the bucketing and the grid of later calls; every element is
+    computed by the same arithmetic, so results are bit-identical before and after."""
+    import torch
+    system = sy.config2_system()
+    basis = sy.sd_basis(30, 3, 3, 3)
+    pairs = sy.sample_pairs(basis, 300000, seed=13)
+    with _engine(system) as w:
+        w.set_basis(basis)
+        before = w.eval_pairs(pairs)
+        stream = torch.cuda.current_stream().cuda_stream
+        dp = torch.from_numpy(pairs.astype(np.uint32).view(np.int32)).cuda()
+        out = torch.empty((pairs.shape[0], 2), dtype=torch.float64, device="cuda")
+        rep = w.autotune(dp.data_ptr(), pairs.shape[0], out.data_ptr(), stream)
+        after = w.eval_pairs(pairs)
+    assert rep["trials"] == 19 and rep["best_ms"] <= rep["default_ms"] + 1e-6
+    assert rep["key_budget"] in (0, 1 << 14, 1 << 16, 1 << 18, 1 << 20, 1 << 22, 1 << 23)
+    assert np.array_equal(before, after)
+
+
 def test_pinned_host_entry_pipeline():
     """Page-locked host buffers take the chunked copy-in / evaluate / copy-out pipeline of
     nw_eval_hs_pairs; its results equal the device entry point's bit for bit, and an
