@@ -429,19 +429,22 @@ class LearnedScreen:
     """Learned screening policy for ``snoci``: the first iteration scores the whole pool
     (exhaustive) and trains the GPU screener (``lib.Screen``) on log10 of the scores; later
     iterations score exactly (M and GMRES) only
-      * every candidate of an excitation class (parent, rank_a, rank_b) with fewer than
-        ``min_class`` exactly scored examples so far (new classes appear as the selected space
-        grows: excitations of selected determinants reach triples and quadruples), and
+      * candidates of every excitation class (parent, rank_a, rank_b) with fewer than
+        ``min_class`` exactly scored examples so far -- all of them, or a seeded random
+        ``explore_per_class`` of a large class (new classes appear as the selected space grows:
+        excitations of selected determinants reach triples and quadruples), and
       * the candidates the screener ranks highest, up to ``keep_fraction`` of the pool (at
         least ``min_keep``),
     and fine-tune the screener on them.  Selection still uses the exact scores."""
 
     def __init__(self, wicks, epochs: int = 40, finetune_epochs: int = 10, batch: int = 1024, lr: float = 2e-3,
-                 floor: float = 1e-14, seed: int = 17, min_class: int = 32):
+                 floor: float = 1e-14, seed: int = 17, min_class: int = 32, explore_per_class: int = 256):
         from .lib import Screen
         self.net = Screen(wicks, seed)
         self.epochs, self.finetune_epochs, self.batch, self.lr, self.floor = epochs, finetune_epochs, batch, lr, floor
         self.min_class = min_class
+        self.explore_per_class = explore_per_class
+        self.rng = np.random.default_rng(seed)
         self.clip: Optional[float] = None   # targets below the first set's median are clipped to it
         self.seen: dict = {}
         self.ready = False
@@ -449,7 +452,14 @@ class LearnedScreen:
 
     def keep(self, cand_all: np.ndarray, opts: SnociOptions, states: np.ndarray) -> np.ndarray:
         cls = _excitation_class(states)
-        explore = np.array([self.seen.get(int(c), 0) < self.min_class for c in cls], bool)
+        explore = np.zeros(cls.shape[0], bool)
+        for c in np.unique(cls):
+            if self.seen.get(int(c), 0) >= self.min_class:
+                continue
+            members = np.nonzero(cls == c)[0]
+            if members.shape[0] > self.explore_per_class:
+                members = self.rng.choice(members, self.explore_per_class, replace=False)
+            explore[members] = True
         pred = self.net.predict(cand_all)
         pred[explore] = np.inf
         nkeep = min(cand_all.shape[0], max(opts.min_keep, int(np.ceil(opts.keep_fraction * cand_all.shape[0]))))
