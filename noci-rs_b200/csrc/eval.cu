@@ -21,50 +21,11 @@
 #include <string>
 
 #include "internal.cuh"
+#include "sort.cuh"
 #include "wick_math.cuh"
 
 namespace nw {
 namespace {
-
-__device__ __forceinline__ DetRec load_det(const nw_det* dets, uint32_t i) {
-  const ulonglong2* p = reinterpret_cast<const ulonglong2*>(dets + i);
-  const ulonglong2 lo = __ldg(p);
-  const ulonglong2 hi = __ldg(p + 1);
-  return unpack_det(lo.x, lo.y, hi.x, hi.y);
-}
-
-__device__ __forceinline__ void store_hs(double* out, uint64_t i, double h, double s) {
-  reinterpret_cast<double2*>(out)[i] = make_double2(h, s);
-}
-
-// Sort key of every pair (pair_sort_key) and its rank among the pairs with the same key, taken
-// from the per-key counter with one global atomic per pair.  The class comes from the 16-bit
-// determinant descriptors; the full records are read only for same-parent pairs, which need
-// the excitation-distance rule.
-__device__ __forceinline__ uint32_t classify_one(const EvalParams& P, uint2 ab, uint64_t i, double* __restrict__ out,
-                                                 int out_stride, uint32_t* __restrict__ flag) {
-  if (ab.x >= P.ndet || ab.y >= P.ndet) {
-    atomicOr(flag, 1u);
-    const double nan = __longlong_as_double(0x7FF8000000000000ll);
-    if (out_stride == 2)
-      store_hs(out, i, nan, nan);
-    else
-      out[i] = nan;
-    return kSkipKey;
-  }
-  const uint32_t dx = __ldg(P.desc + ab.x), dw = __ldg(P.desc + ab.y);
-  const int px = (int)(dx & 0xFF), pw = (int)(dw & 0xFF);
-  if (px == pw && far_same_parent(load_det(P.dets, ab.x), load_det(P.dets, ab.y))) {
-    if (out_stride == 2)
-      store_hs(out, i, 0.0, 0.0);
-    else
-      out[i] = 0.0;
-    return kSkipKey;
-  }
-  const int cls = rank_class((int)((dx >> 8) & 15) + (int)((dw >> 8) & 15), (int)(dx >> 12) + (int)(dw >> 12));
-  const int ord = __ldg(P.order + px * P.nref + pw);
-  return pair_sort_key(cls, ab.x, pw, ord, P.nfast, P.nref, P.nbucket, P.shift);
-}
 
 // Items per thread and loop trip in the sort kernels: independent loads and atomics of
 // kSortUnroll pairs are in flight together (the chains are latency-bound otherwise).
@@ -516,13 +477,15 @@ nw_status scan_exclusive(nw_ctx* ctx, const uint32_t* counts, uint64_t n, uint32
 // (or hold earlier calls' reports); ev (six events or null) brackets the phases.
 nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const uint32_t* pairs, uint64_t npairs,
                         double* out, const SortScratch& S, cudaStream_t stream, cudaEvent_t* ev, EvalMode mode,
-                        const uint32_t* npairs_dev) {
+                        const uint32_t* npairs_dev, bool classified) {
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[0], stream));
-  NW_CUDA(ctx, cudaMemsetAsync(S.counts, 0, sizeof(uint32_t) * nkeys, stream));
   const int per_sm = ctx->tune_per_sm > 0 ? ctx->tune_per_sm : 8;
-  classify_kernel<<<grid_stride_blocks(npairs, 256, per_sm), 256, 0, stream>>>(P, pairs, npairs, npairs_dev, S.keys, S.ranks,
-                                                                          S.counts, out, 2, S.flag);
-  NW_CUDA(ctx, cudaGetLastError());
+  if (!classified) {
+    NW_CUDA(ctx, cudaMemsetAsync(S.counts, 0, sizeof(uint32_t) * nkeys, stream));
+    classify_kernel<<<grid_stride_blocks(npairs, 256, per_sm), 256, 0, stream>>>(P, pairs, npairs, npairs_dev, S.keys,
+                                                                                 S.ranks, S.counts, out, 2, S.flag);
+    NW_CUDA(ctx, cudaGetLastError());
+  }
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[1], stream));
   const int ntiles = (int)(nkeys / kScanTile + 1);
   scan_tiles_kernel<<<ntiles, kScanThreads, 0, stream>>>(S.counts, (uint32_t)nkeys, S.tsum);

@@ -160,10 +160,13 @@ EvalParams make_params(const nw_ctx* ctx);
 uint64_t plan_keys(const nw_ctx* ctx, EvalParams& P, uint64_t cap);
 // classify -> scan -> scatter -> evaluate on `stream` (no allocation, no host synchronisation).
 // With npairs_dev the number of pairs is read on the device (at most npairs, the capacity the
-// launch is sized for); ev (six events or null) brackets the phases.
+// launch is sized for); ev (six events or null) brackets the phases.  With classified the
+// caller has already cleared S.counts and written S.keys / S.ranks (and the outputs of
+// skipped pairs), e.g. the fused QMC spawn kernel, and the pipeline starts at the scan.
 nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const uint32_t* pairs, uint64_t npairs,
                         double* out, const SortScratch& S, cudaStream_t stream, cudaEvent_t* ev,
-                        EvalMode mode = EvalMode::kHS, const uint32_t* npairs_dev = nullptr);
+                        EvalMode mode = EvalMode::kHS, const uint32_t* npairs_dev = nullptr,
+                        bool classified = false);
 
 // Exclusive scan of n counters into offsets[0..n] (offsets[n] = total); tsum holds n / 4096 + 1.
 nw_status scan_exclusive(nw_ctx* ctx, const uint32_t* counts, uint64_t n, uint32_t* offsets, uint32_t* tsum,

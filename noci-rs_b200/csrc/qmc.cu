@@ -29,6 +29,7 @@
 #include "internal.cuh"
 #include "mlp.cuh"
 #include "qmc_math.cuh"
+#include "sort.cuh"
 
 namespace {
 
@@ -162,61 +163,85 @@ __global__ void qmc_chunk_kernel(QmcParams q, const QmcState* __restrict__ st, c
     cown[c] = (uint32_t)owner_of(off, q.ndet, c << kChunkShift);
 }
 
-__global__ void qmc_spawn_kernel(QmcParams q, Proposal pr, const QmcState* __restrict__ st,
+// Spawn attempts and classify their pairs for the sorted evaluation in one pass: the child
+// of every attempt, its pair, amplitude and generation probability, then the pair's sort key
+// (nw::classify_one) and its rank within the key, taken warp-aggregated from the per-key
+// counters (attempts of one parent share keys).  The loop is warp-uniform (its trip count
+// depends on the warp's first attempt only), so every lane reaches the full-mask intrinsics.
+__global__ void qmc_spawn_kernel(QmcParams q, Proposal pr, nw::EvalParams P, const QmcState* __restrict__ st,
                                  const uint32_t* __restrict__ off, const uint32_t* __restrict__ cown,
                                  const double* __restrict__ sampled,
                                  const uint32_t* __restrict__ na, uint2* __restrict__ pairs, uint32_t* __restrict__ child,
-                                 uint32_t* __restrict__ parent, double* __restrict__ amp, double* __restrict__ pg) {
+                                 uint32_t* __restrict__ parent, double* __restrict__ amp, double* __restrict__ pg,
+                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ ranks,
+                                 uint32_t* __restrict__ counts, double* __restrict__ hs, uint32_t* __restrict__ flag) {
   const uint32_t n = st->npairs;
   const uint64_t cycle = st->cycle;
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    // owners of this chunk's first attempt and of the next chunk's bound the search
-    const uint32_t c = t >> kChunkShift;
-    const uint64_t lo = cown[c];
-    const uint64_t hi = ((uint64_t)(c + 1) << kChunkShift) < n ? cown[c + 1] : q.ndet - 1;
-    uint64_t a = lo, b = hi + 1;  // off[a] <= t < off[b]
-    while (b - a > 1) {
-      const uint64_t mid = (a + b) >> 1;
-      if (off[mid] <= t)
-        a = mid;
-      else
-        b = mid;
-    }
-    const uint64_t g = a;
-    double u0, u1;
-    nwq::uniform2(q.seed, cycle, t, nwq::kDrawChild, &u0, &u1);
-    uint64_t lam;
-    if (q.gen == 0) {
-      lam = nwq::uniform_child(g, q.ndet, u0);
-    } else {
-      double u2, u3;
-      nwq::uniform2(q.seed, cycle, t, nwq::kDrawChildBin, &u2, &u3);
-      if (u1 < q.mix) {
-        lam = nwq::uniform_child(g, q.ndet, u2);
-      } else {
-        // bin from the parent's cumulative probabilities, then uniformly inside the bin
-        // first bin with u2 < cdf (the last valid bin and those after it hold 1.0 > u2)
-        const float* c = pr.cdf + g * q.nbin;
-        uint32_t b = 0, hi = q.nbin - 1;
-        while (b < hi) {
-          const uint32_t mid = (b + hi) >> 1;
-          if (u2 < (double)c[mid])
-            hi = mid;
-          else
-            b = mid + 1;
-        }
-        const uint32_t size = bin_size_without(pr, b, (uint32_t)g);
-        uint32_t idx = (uint32_t)(u3 * (double)size);
-        if (idx >= size) idx = size - 1;
-        if (pr.det_bin[g] == b && idx >= pr.pos[g]) ++idx;
-        lam = pr.bin_mem[pr.bin_off[b] + idx];
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lanes_below = (1u << lane) - 1u;
+  for (uint32_t w0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); w0 < n; w0 += gridDim.x * blockDim.x) {
+    const uint32_t t = w0 + lane;
+    uint32_t key = nw::kSkipKey;
+    if (t < n) {
+      // owners of this chunk's first attempt and of the next chunk's bound the search
+      const uint32_t c = t >> kChunkShift;
+      const uint64_t lo = cown[c];
+      const uint64_t hi = ((uint64_t)(c + 1) << kChunkShift) < n ? cown[c + 1] : q.ndet - 1;
+      uint64_t a = lo, b = hi + 1;  // off[a] <= t < off[b]
+      while (b - a > 1) {
+        const uint64_t mid = (a + b) >> 1;
+        if (off[mid] <= t)
+          a = mid;
+        else
+          b = mid;
       }
-      pg[t] = learned_pgen(q, pr, (uint32_t)g, (uint32_t)lam);
+      const uint64_t g = a;
+      double u0, u1;
+      nwq::uniform2(q.seed, cycle, t, nwq::kDrawChild, &u0, &u1);
+      uint64_t lam;
+      if (q.gen == 0) {
+        lam = nwq::uniform_child(g, q.ndet, u0);
+      } else {
+        double u2, u3;
+        nwq::uniform2(q.seed, cycle, t, nwq::kDrawChildBin, &u2, &u3);
+        if (u1 < q.mix) {
+          lam = nwq::uniform_child(g, q.ndet, u2);
+        } else {
+          // bin from the parent's cumulative probabilities, then uniformly inside the bin
+          // first bin with u2 < cdf (the last valid bin and those after it hold 1.0 > u2)
+          const float* c = pr.cdf + g * q.nbin;
+          uint32_t b = 0, hi = q.nbin - 1;
+          while (b < hi) {
+            const uint32_t mid = (b + hi) >> 1;
+            if (u2 < (double)c[mid])
+              hi = mid;
+            else
+              b = mid + 1;
+          }
+          const uint32_t size = bin_size_without(pr, b, (uint32_t)g);
+          uint32_t idx = (uint32_t)(u3 * (double)size);
+          if (idx >= size) idx = size - 1;
+          if (pr.det_bin[g] == b && idx >= pr.pos[g]) ++idx;
+          lam = pr.bin_mem[pr.bin_off[b] + idx];
+        }
+        pg[t] = learned_pgen(q, pr, (uint32_t)g, (uint32_t)lam);
+      }
+      const uint2 ab = lam <= g ? make_uint2((uint32_t)lam, (uint32_t)g) : make_uint2((uint32_t)g, (uint32_t)lam);
+      pairs[t] = ab;
+      child[t] = (uint32_t)lam;
+      parent[t] = (uint32_t)g;
+      amp[t] = sampled[g] / (double)na[g];
+      key = nw::classify_one(P, ab, t, hs, 2, flag);
     }
-    pairs[t] = lam <= g ? make_uint2((uint32_t)lam, (uint32_t)g) : make_uint2((uint32_t)g, (uint32_t)lam);
-    child[t] = (uint32_t)lam;
-    parent[t] = (uint32_t)g;
-    amp[t] = sampled[g] / (double)na[g];
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0u;
+    if ((int)lane == leader && key != nw::kSkipKey) base = atomicAdd(&counts[key], (uint32_t)__popc(peers));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    if (t < n) {
+      keys[t] = key;
+      ranks[t] = key != nw::kSkipKey ? base + (uint32_t)__popc(peers & lanes_below) : 0u;
+    }
   }
 }
 
@@ -487,11 +512,13 @@ nw_status enqueue_cycle(nw_qmc* q) {
   if (st != NW_OK) return st;
   qmc_count_kernel<<<1, 1, 0, s>>>(q->q, q->st, q->off);
   qmc_chunk_kernel<<<grid_for((q->q.cap >> kChunkShift) + 1), kBlockThreads, 0, s>>>(q->q, q->st, q->off, q->cown);
-  qmc_spawn_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(q->q, q->pr, q->st, q->off, q->cown, q->sampled, q->na,
-                                                                q->pairs, q->child, q->parent, q->amp, q->pg);
+  NW_CUDA(ctx, cudaMemsetAsync(q->S.counts, 0, sizeof(uint32_t) * q->nkeys, s));
+  qmc_spawn_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(
+      q->q, q->pr, q->P, q->st, q->off, q->cown, q->sampled, q->na, q->pairs, q->child, q->parent, q->amp, q->pg,
+      q->S.keys, q->S.ranks, q->S.counts, reinterpret_cast<double*>(q->hs), q->S.flag);
   NW_CUDA(ctx, cudaGetLastError());
   st = nw::launch_sorted(ctx, q->P, q->nkeys, reinterpret_cast<const uint32_t*>(q->pairs), q->q.cap,
-                         reinterpret_cast<double*>(q->hs), q->S, s, nullptr, nw::EvalMode::kHS, &q->st->npairs);
+                         reinterpret_cast<double*>(q->hs), q->S, s, nullptr, nw::EvalMode::kHS, &q->st->npairs, true);
   if (st != NW_OK) return st;
   qmc_apply_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(q->q, q->pr, q->st, q->hs, q->child, q->parent,
                                                                 q->amp, q->pg, q->delta);
