@@ -387,8 +387,9 @@ NW_API nw_status nw_sync(nw_ctx* ctx, void* stream);
 /* Autotuner (no counterpart in the reference): times nw_eval_hs_pairs_device on the caller's
  * device pairs (npairs of them, results into hs) for fine sort-key budgets 2^14 .. 2^23 and
  * 4 / 8 / 16 blocks per SM of the grid-stride kernels, against the defaults, and keeps the
- * fastest for the later calls on this context (budget 0 and blocks 0 in the report mean the
- * defaults won).  Synchronises `stream`. */
+ * fastest for the later calls on this context, the budget as keys per pair so that calls of
+ * other sizes scale it (budget 0 and blocks 0 in the report mean the defaults won).
+ * Synchronises `stream`. */
 typedef struct nw_tune_report {
     uint64_t key_budget;        /* chosen fine-key budget (0: default, min(2^23, max(2^14, npairs))) */
     int32_t blocks_per_sm;      /* chosen blocks per SM (0: default 8)                           */

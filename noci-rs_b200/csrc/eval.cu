@@ -557,7 +557,8 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
     return NW_OK;
   }
 
-  const uint64_t budget = ctx->tune_key_budget ? ctx->tune_key_budget : std::max(kFineMin, npairs);
+  const uint64_t budget =
+      ctx->tune_keys_per_pair > 0.0 ? (uint64_t)(ctx->tune_keys_per_pair * (double)npairs) : std::max(kFineMin, npairs);
   const uint64_t nkeys = plan_keys(ctx, P, std::min(kFineMax, std::max(kFineMin, budget)));
   if ((st = ensure(ctx, ctx->keys, npairs * sizeof(uint32_t))) != NW_OK) return st;
   if ((st = ensure(ctx, ctx->ranks, npairs * sizeof(uint32_t))) != NW_OK) return st;
@@ -673,7 +674,8 @@ nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs
 }  // namespace nw
 
 // ---------------------------------------------------------------------------------------
-// Autotuner: the fine sort-key budget (how finely pairs are bucketed by bra determinant
+// Autotuner: the fine sort-key budget (how finely pairs are bucketed by bra determinant; kept
+// per pair so that it scales with the size of later calls
 // before evaluation: locality of the intermediates against the cost of clearing and scanning
 // the counters) and the blocks per SM of the grid-stride kernels, timed on the caller's pairs.
 // ---------------------------------------------------------------------------------------
@@ -684,7 +686,7 @@ extern "C" nw_status nw_autotune(nw_ctx* ctx, const uint32_t* pairs, uint64_t np
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
   static const uint64_t kBudgets[] = {1ull << 14, 1ull << 16, 1ull << 18, 1ull << 20, 1ull << 22, 1ull << 23};
   static const int kPerSm[] = {4, 8, 16};
-  const uint64_t saved_budget = ctx->tune_key_budget;
+  const double saved_ratio = ctx->tune_keys_per_pair;
   const int saved_per_sm = ctx->tune_per_sm;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
@@ -700,7 +702,7 @@ extern "C" nw_status nw_autotune(nw_ctx* ctx, const uint32_t* pairs, uint64_t np
   for (int b = -1; b < (int)(sizeof(kBudgets) / sizeof(kBudgets[0])) && st == NW_OK; ++b) {
     for (int g = 0; g < (int)(sizeof(kPerSm) / sizeof(kPerSm[0])) && st == NW_OK; ++g) {
       if (b < 0 && g > 0) break;
-      ctx->tune_key_budget = b < 0 ? 0 : kBudgets[b];
+      ctx->tune_keys_per_pair = b < 0 ? 0.0 : (double)kBudgets[b] / (double)npairs;
       ctx->tune_per_sm = b < 0 ? 0 : kPerSm[g];
       float ms = 0.0f;
       for (int rep_i = 0; rep_i < 4 && st == NW_OK; ++rep_i) {
@@ -725,11 +727,13 @@ extern "C" nw_status nw_autotune(nw_ctx* ctx, const uint32_t* pairs, uint64_t np
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (st != NW_OK) {
-    ctx->tune_key_budget = saved_budget;
+    ctx->tune_keys_per_pair = saved_ratio;
     ctx->tune_per_sm = saved_per_sm;
     return st;
   }
-  ctx->tune_key_budget = best_budget;  // 0 / 0 keeps the defaults when they were fastest
+  // kept as keys per pair, so later calls of other sizes (e.g. the chunks of the host-buffer
+  // pipeline) scale it; 0 / 0 keeps the defaults when they were fastest
+  ctx->tune_keys_per_pair = (double)best_budget / (double)npairs;
   ctx->tune_per_sm = best_per_sm;
   rep->key_budget = best_budget;
   rep->blocks_per_sm = best_per_sm;

@@ -104,7 +104,7 @@ struct nw_ctx {
   // optional per-phase timing of the evaluation pipeline
   bool timing = false;
   // launch configuration chosen by nw_autotune (0: defaults)
-  uint64_t tune_key_budget = 0;   // fine sort-key budget of nw_eval_hs_pairs*
+  double tune_keys_per_pair = 0.0;  // fine sort-key budget of nw_eval_hs_pairs* per pair
   int tune_per_sm = 0;            // blocks per SM of classify / scatter / light evaluator
   bool timed_valid = false;
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
