@@ -119,7 +119,9 @@ NW_API nw_status nw_build_intermediates(nw_ctx* ctx);
 NW_API nw_status nw_pair_zero_counts(const nw_ctx* ctx, int32_t* m);
 
 /* Upload the determinant basis once (host array of ndet records); it stays resident.
- * Replaces the reduced_basis argument of calculate_hs_pairs_wicks_batched (src/noci/hs.rs:72-78). */
+ * Replaces the reduced_basis argument of calculate_hs_pairs_wicks_batched (src/noci/hs.rs:72-78).
+ * Returns NW_ERR_STATE while a QMC object of the context exists (it evaluates against the
+ * resident basis every cycle). */
 NW_API nw_status nw_set_basis(nw_ctx* ctx, const nw_det* basis, uint64_t ndet);
 
 /* (H, S) for npairs requests (a_i, b_i) = pairs[2i], pairs[2i+1] into the resident basis,

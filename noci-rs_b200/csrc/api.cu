@@ -264,6 +264,8 @@ nw_status nw_pair_zero_counts(const nw_ctx* ctx, int32_t* m) {
 nw_status nw_set_basis(nw_ctx* ctx, const nw_det* basis, uint64_t ndet) {
   if (!ctx || (!basis && ndet)) return NW_ERR_INVALID;
   if (ndet >= 0xFFFFFFFFull) return nw::fail(ctx, NW_ERR_UNSUPPORTED, "at most 2^32 - 2 determinants");
+  if (ctx->live_qmc > 0)
+    return nw::fail(ctx, NW_ERR_STATE, "a QMC object uses the resident basis (nw_qmc_destroy it first)");
   // Validate every record: parent in range, ranks <= 4, holes ascending in the occupied
   // block, particles ascending in the virtual block.
   for (uint64_t i = 0; i < ndet; ++i) {

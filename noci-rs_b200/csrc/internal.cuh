@@ -105,6 +105,7 @@ struct nw_ctx {
   bool timing = false;
   // launch configuration chosen by nw_autotune (0: defaults)
   double tune_keys_per_pair = 0.0;  // fine sort-key budget of nw_eval_hs_pairs* per pair
+  int live_qmc = 0;                 // QMC objects evaluating against the resident basis
   int tune_per_sm = 0;            // blocks per SM of classify / scatter / light evaluator
   bool timed_valid = false;
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};

@@ -489,6 +489,7 @@ struct nw_qmc {
   bool learnable = false;    // nref small enough for the bin output layer
   bool table_ready = false;  // cdf built by a training run
   std::vector<uint32_t> h_det_bin, h_bin_off;  // host copies of the bins (argument checks)
+  bool counted = false;  // holds one of ctx->live_qmc
   nw::Mlp mlp{};
   uint32_t* trows = nullptr;  // training batch: parents, target bins, weights, weight sum
   uint32_t* tbin = nullptr;
@@ -551,6 +552,7 @@ nw_status reset_reference_stats(nw_qmc* q) {
 }
 
 void release(nw_qmc* q) {
+  if (q->counted) q->ctx->live_qmc -= 1;
   nw::mlp_destroy(&q->mlp);
   if (q->graph) cudaGraphExecDestroy(q->graph);
   if (q->ev0) cudaEventDestroy(q->ev0);
@@ -753,6 +755,8 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
   nw_qmc* q = new (std::nothrow) nw_qmc;
   if (!q) return NW_ERR_ALLOC;
   q->ctx = ctx;
+  q->counted = true;
+  ctx->live_qmc += 1;
   q->opts = *opts;
   uint64_t cap = opts->max_attempts;
   // automatic: the 1-norm can overshoot the target many times before the shift holds it

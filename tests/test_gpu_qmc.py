@@ -91,3 +91,17 @@ def test_capacity_overflow_is_reported():
         p = np.linspace(-1.0, 1.0, nd)
         q.set_populations(p)
         assert np.array_equal(q.populations(), p)
+
+
+def test_basis_is_locked_while_a_qmc_object_lives():
+    w, basis, h, s, refs = _setup()
+    nd = basis.shape[0]
+    c0 = np.zeros(nd)
+    c0[refs] = 1.0
+    with w:
+        q = nociwick.Qmc(w, c0, refs, dt=0.004, initial_population=100.0)
+        with pytest.raises(nociwick.NwError) as e:
+            w.set_basis(basis)
+        assert e.value.status == 5          # NW_ERR_STATE
+        q.close()
+        w.set_basis(basis)          # allowed again once the QMC object is gone
