@@ -203,8 +203,38 @@ def cpu_baseline(system, basis, pairs, seconds: float, gpu_hs=None):
            "sample": f"first {nsample} pairs of the same batch ({dt:.1f} s of CPU work, C++ FP64 restatement "
                      f"of the reference evaluator, {cores} threads)"}
     if gpu_hs is not None:
-        err = max(float(np.max(np.abs(gpu_hs[:nsample, 0] - h))), float(np.max(np.abs(gpu_hs[:nsample, 1] - s))))
-        out["max_abs_err_gpu_vs_cpu"] = err
+        dh = np.abs(gpu_hs[:nsample, 0] - h)
+        ds = np.abs(gpu_hs[:nsample, 1] - s)
+        out["max_abs_err_gpu_vs_cpu"] = max(float(dh.max()), float(ds.max()))
+        out["rms_abs_err_h"] = float(np.sqrt(np.mean(dh ** 2)))
+        # The elements of a reference pair whose smallest non-zero paired singular value s is
+        # small are ill-conditioned (two-body terms scale as 1/s^2): report the error by s.
+        smin = reference_pair_conditioning(system)
+        par = basis["parent"][sample[:, 0]].astype(np.int64) * len(system.refs) + basis["parent"][sample[:, 1]]
+        cond = smin[par]
+        buckets = {}
+        for name, sel in (("s_min>=1e-2", cond >= 1e-2), ("1e-3<=s_min<1e-2", (cond >= 1e-3) & (cond < 1e-2)),
+                          ("s_min<1e-3", cond < 1e-3)):
+            if sel.any():
+                buckets[name] = {"pairs": int(sel.sum()), "max_abs_err_h": float(dh[sel].max()),
+                                 "max_abs_err_s": float(ds[sel].max())}
+        out["err_by_reference_pair_conditioning"] = buckets
+    return out
+
+
+def reference_pair_conditioning(system) -> np.ndarray:
+    """Smallest non-zero (above the 1e-8 zero tolerance) paired singular value of the occupied
+    overlaps of every ordered reference pair, both spins."""
+    nref = len(system.refs)
+    out = np.ones(nref * nref)
+    for x, (cxa, oxa, cxb, oxb) in enumerate(system.refs):
+        for w, (cwa, owa, cwb, owb) in enumerate(system.refs):
+            sv = []
+            for cx, cw, no in ((cxa, cwa, bin(oxa).count("1")), (cxb, cwb, bin(oxb).count("1"))):
+                sv.append(np.linalg.svd(cx[:, :no].T @ system.s @ cw[:, :no], compute_uv=False))
+            v = np.concatenate(sv)
+            v = v[v > 1e-8]
+            out[x * nref + w] = v.min() if v.size else 1.0
     return out
 
 

@@ -235,7 +235,7 @@ nw_status nw_ctx_create(const nw_system* sys, const nw_refs* refs, const nw_opts
   if (st == NW_OK) st = upload(ctx, &ctx->d_ca, refs->c_alpha, (size_t)nref * nao * nmo);
   if (st == NW_OK) st = upload(ctx, &ctx->d_cb, refs->c_beta, (size_t)nref * nao * nmo);
   if (st == NW_OK && cudaMallocHost(&ctx->h_flag, sizeof(uint32_t)) != cudaSuccess) st = NW_ERR_ALLOC;
-  for (int i = 0; i < 2 && st == NW_OK; ++i)
+  for (int i = 0; i < 3 && st == NW_OK; ++i)
     if (cudaStreamCreateWithFlags(&ctx->s_aux[i], cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming) != cudaSuccess)
       st = NW_ERR_CUDA;
@@ -438,10 +438,10 @@ nw_status nw_ctx_destroy(nw_ctx* ctx) {
   if (ctx->h_flag) cudaFreeHost(ctx->h_flag);
   for (int i = 0; i < 6; ++i)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
-  for (cudaStream_t q : {ctx->s_in, ctx->s_comp, ctx->s_out, ctx->s_aux[0], ctx->s_aux[1]})
+  for (cudaStream_t q : {ctx->s_in, ctx->s_comp, ctx->s_out, ctx->s_aux[0], ctx->s_aux[1], ctx->s_aux[2]})
     if (q) cudaStreamDestroy(q);
   for (cudaEvent_t e : {ctx->ev_start, ctx->ev_in[0], ctx->ev_in[1], ctx->ev_comp[0], ctx->ev_comp[1], ctx->ev_fork,
-                        ctx->ev_join[0], ctx->ev_join[1]})
+                        ctx->ev_join[0], ctx->ev_join[1], ctx->ev_join[2]})
     if (e) cudaEventDestroy(e);
   if (ctx->blas) cublasDestroy(ctx->blas);
   if (ctx->solver) cusolverDnDestroy(ctx->solver);

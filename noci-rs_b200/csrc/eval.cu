@@ -498,13 +498,14 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
   NW_CUDA(ctx, cudaGetLastError());
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[3], stream));
   const uint2* pp = reinterpret_cast<const uint2*>(pairs);
-  if (ctx->nfast > 0) {
-    // The class kernels write disjoint outputs and each is limited by its own occupancy, so
-    // the medium and the heavy / runtime-rank classes run on forked streams beside the light
-    // ones and join before the generic evaluator (also inside a stream capture: the forked
-    // streams join the capture through the fork event).
-    NW_CUDA(ctx, cudaEventRecord(ctx->ev_fork, stream));
-    for (int i = 0; i < 2; ++i) NW_CUDA(ctx, cudaStreamWaitEvent(ctx->s_aux[i], ctx->ev_fork, 0));
+  // The class kernels write disjoint outputs and each is limited by its own occupancy, so the
+  // medium, the heavy / runtime-rank and the zero-overlap generic classes run on streams forked
+  // off the launching one, beside the light classes, and join before the call returns (also
+  // inside a stream capture: the forked streams join the capture through the fork event).
+  const bool fast = ctx->nfast > 0, gen = ctx->nfast < ctx->nref * ctx->nref;
+  NW_CUDA(ctx, cudaEventRecord(ctx->ev_fork, stream));
+  for (int i = 0; i < 3; ++i) NW_CUDA(ctx, cudaStreamWaitEvent(ctx->s_aux[i], ctx->ev_fork, 0));
+  if (fast) {
     if (mode == EvalMode::kFS) {
       eval_fs_light_kernel<<<grid_stride_blocks(npairs, 256, per_sm), 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
       eval_fs_heavy_kernel<<<148 * 2, 256, 0, ctx->s_aux[0]>>>(P, pp, S.sidx, S.offsets, out);
@@ -515,19 +516,19 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
       eval_rt_kernel<<<148 * 2, 128, 0, ctx->s_aux[1]>>>(P, pp, S.sidx, S.offsets, out);
     }
     NW_CUDA(ctx, cudaGetLastError());
-    for (int i = 0; i < 2; ++i) {
-      NW_CUDA(ctx, cudaEventRecord(ctx->ev_join[i], ctx->s_aux[i]));
-      NW_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->ev_join[i], 0));
-    }
   }
-  if (ev) NW_CUDA(ctx, cudaEventRecord(ev[4], stream));
-  if (ctx->nfast < ctx->nref * ctx->nref) {
+  if (gen) {
     if (mode == EvalMode::kFS)
-      eval_fs_gen_kernel<<<148 * 4, 128, 0, stream>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out);
+      eval_fs_gen_kernel<<<148 * 4, 128, 0, ctx->s_aux[2]>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out);
     else
-      eval_gen_kernel<<<148 * 4, 128, 0, stream>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out);
+      eval_gen_kernel<<<148 * 4, 128, 0, ctx->s_aux[2]>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out);
     NW_CUDA(ctx, cudaGetLastError());
   }
+  for (int i = 0; i < 3; ++i) {
+    NW_CUDA(ctx, cudaEventRecord(ctx->ev_join[i], ctx->s_aux[i]));
+    NW_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->ev_join[i], 0));
+  }
+  if (ev) NW_CUDA(ctx, cudaEventRecord(ev[4], stream));
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[5], stream));
   return NW_OK;
 }

@@ -80,9 +80,10 @@ struct nw_ctx {
   nw::DevBuf io_pairs, io_hs;      // staging for the host-buffer entry point
   // copy-in / evaluate / copy-out streams and chunk events of the pipelined host-buffer path
   cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
-  // class evaluators forked off the launching stream (medium ranks; heavy and runtime ranks)
-  cudaStream_t s_aux[2] = {nullptr, nullptr};
-  cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+  // class evaluators forked off the launching stream (medium ranks; heavy and runtime ranks;
+  // the zero-overlap generic evaluator)
+  cudaStream_t s_aux[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t ev_start = nullptr;
   cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr};
 
