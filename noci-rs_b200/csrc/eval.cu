@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(128) eval_rt_kernel(EvalParams P, const uint2*
 // ---------------------------------------------------------------------------------------
 __device__ __noinline__ void eval_gen_one(const GenPair& g, const DetRec& x, const DetRec& w, const EvalParams& P,
                                           double* H, double* S) {
-  eval_gen_pair(g, x, w, P.n, P.nocc_a, P.nocc_b, P.enuc, P.tol, P.exact != 0, H, S);
+  eval_gen_any(g, x, w, P.n, P.nocc_a, P.nocc_b, P.enuc, P.tol, P.exact != 0, H, S);
 }
 
 __global__ void __launch_bounds__(128) eval_gen_kernel(EvalParams P, const uint2* __restrict__ pairs,
@@ -460,7 +460,7 @@ uint64_t plan_keys(const nw_ctx* ctx, EvalParams& P, uint64_t cap) {
   P.shift = sort_key_shift(ctx->ndet, ctx->nref, cap, &nb);
   P.nbucket = nb;
   const uint64_t ngen = (uint64_t)ctx->nref * ctx->nref - (uint64_t)ctx->nfast;
-  return (uint64_t)kClasses * nb + (uint64_t)kClasses * ngen;
+  return (uint64_t)kClasses * nb + (uint64_t)kGenClasses * ngen;
 }
 
 nw_status scan_exclusive(nw_ctx* ctx, const uint32_t* counts, uint64_t n, uint32_t* offsets, uint32_t* tsum,
@@ -604,8 +604,8 @@ namespace {
 constexpr uint64_t kNoallocMaxPairs = 1ull << 20;                       // 1,048,576 pairs per call
 constexpr int kNoallocMaxRefs = 64;                                      // reference determinants
 // keys: the fast classes get at least kClasses * 64 * 64 counters, the zero-overlap reference
-// pairs up to kClasses * 64 * 64 more
-constexpr uint64_t kNoallocMaxKeys = 2ull * kNoallocMaxRefs * kNoallocMaxRefs * kClasses;
+// pairs up to kGenClasses * 64 * 64 more
+constexpr uint64_t kNoallocMaxKeys = (uint64_t)kNoallocMaxRefs * kNoallocMaxRefs * (kClasses + kGenClasses);
 constexpr uint64_t kNoallocTiles = kNoallocMaxKeys / kScanTile + 1;
 constexpr uint64_t kNoallocOffKeys = 0;
 constexpr uint64_t kNoallocOffRanks = kNoallocOffKeys + 4 * kNoallocMaxPairs;
@@ -657,7 +657,7 @@ nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs
   if (npairs == 0) return NW_OK;
   EvalParams P = make_params(ctx);
   const uint64_t ngen = (uint64_t)ctx->nref * ctx->nref - (uint64_t)ctx->nfast;
-  const uint64_t fast_cap = std::min(kNoallocMaxKeys - (uint64_t)kClasses * ngen, std::max(kFineMin, npairs));
+  const uint64_t fast_cap = std::min(kNoallocMaxKeys - (uint64_t)kGenClasses * ngen, std::max(kFineMin, npairs));
   const uint64_t nkeys = plan_keys(ctx, P, fast_cap);
   if (nkeys > kNoallocMaxKeys) return fail(ctx, NW_ERR_UNSUPPORTED, "sort keys exceed the allocation-free scratch");
   SortScratch S;

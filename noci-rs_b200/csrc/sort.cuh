@@ -45,9 +45,9 @@ __device__ __forceinline__ uint32_t classify_one(const EvalParams& P, uint2 ab, 
       out[i] = 0.0;
     return kSkipKey;
   }
-  const int cls = rank_class((int)((dx >> 8) & 15) + (int)((dw >> 8) & 15), (int)(dx >> 12) + (int)(dw >> 12));
+  const int la = (int)((dx >> 8) & 15) + (int)((dw >> 8) & 15), lb = (int)(dx >> 12) + (int)(dw >> 12);
   const int ord = __ldg(P.order + px * P.nref + pw);
-  return pair_sort_key(cls, ab.x, pw, ord, P.nfast, P.nref, P.nbucket, P.shift);
+  return pair_sort_key(la, lb, ab.x, pw, ord, P.nfast, P.nref, P.nbucket, P.shift);
 }
 
 

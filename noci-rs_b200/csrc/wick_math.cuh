@@ -17,8 +17,10 @@
 
 #ifdef __CUDACC__
 #define NW_HD __host__ __device__ __forceinline__
+#define NW_HD_CALL __host__ __device__ __noinline__  // a real call: its own register allocation
 #else
 #define NW_HD inline
+#define NW_HD_CALL inline
 #include <cmath>
 using std::fabs;
 using std::sqrt;
@@ -911,14 +913,20 @@ NW_HD int rank_class(int la, int lb) { return (la <= 4 && lb <= 4) ? la * 5 + lb
 // evaluator kernel walks one contiguous range per class, and inside a class the pairs of one
 // bra determinant (and ket reference) lie together, so the lanes of a warp share the bra's
 // rows of the intermediates.  Pairs of reference pairs with zero-overlap orbitals follow,
-// keyed by (sort position - nfast, class).  Keys are < kRankClasses * (nbucket + nref^2).
+// keyed by (sort position - nfast, L_alpha, L_beta) with the full ranks 0..kML: their
+// distribution sums cost about L^7 per spin, so a warp whose lanes mixed ranks would run every
+// lane at the pace of its largest L.  Keys are < kRankClasses * nbucket + kGenClasses *
+// (nref^2 - nfast).
 // ---------------------------------------------------------------------------------------
 constexpr int kRankClasses = 26;
+constexpr int kGenClasses = (kML + 1) * (kML + 1);
 
-NW_HD uint32_t pair_sort_key(int cls, uint32_t bra, int ket_parent, int ord, int nfast, int nref, uint32_t nbucket,
-                             int shift) {
-  if (ord < nfast) return (uint32_t)cls * nbucket + (uint32_t)((((uint64_t)bra * (uint64_t)nref) + ket_parent) >> shift);
-  return (uint32_t)kRankClasses * nbucket + (uint32_t)((ord - nfast) * kRankClasses + cls);
+NW_HD uint32_t pair_sort_key(int la, int lb, uint32_t bra, int ket_parent, int ord, int nfast, int nref,
+                             uint32_t nbucket, int shift) {
+  if (ord < nfast)
+    return (uint32_t)rank_class(la, lb) * nbucket +
+           (uint32_t)((((uint64_t)bra * (uint64_t)nref) + ket_parent) >> shift);
+  return (uint32_t)kRankClasses * nbucket + (uint32_t)((ord - nfast) * kGenClasses + la * (kML + 1) + lb);
 }
 
 // Smallest shift for which the fast-pair keys, kRankClasses * nbucket, fit in cap (cap >= 26).
@@ -1034,20 +1042,10 @@ NW_HD void eval_m0_pair(const FastPair& fp, const DetRec& x, const DetRec& w, in
 // ---------------------------------------------------------------------------------------
 // m > 0 fused (H, S) for one pair on the reference-ordered intermediates.
 // ---------------------------------------------------------------------------------------
-NW_HD void eval_gen_pair(const GenPair& g, const DetRec& x, const DetRec& w, int n, int oa, int ob, double enuc,
-                         double tol, bool exact, double* H, double* S) {
-  const int la = x.ra + w.ra, lb = x.rb + w.rb;
-  int ra[kML], ca[kML], rb[kML], cb[kML];
-  labels_rt(x, w, 0, oa, n, ra, ca);
-  labels_rt(x, w, 1, ob, n, rb, cb);
-  double da0[kML * kML], da1[kML * kML], db0[kML * kML], db1[kML * kML];
-  build_d_rt(da0, g.a.x[0], g.a.y[0], n, la, ra, ca);
-  build_d_rt(da1, g.a.x[1], g.a.y[1], n, la, ra, ca);
-  build_d_rt(db0, g.b.x[0], g.b.y[0], n, lb, rb, cb);
-  build_d_rt(db1, g.b.x[1], g.b.y[1], n, lb, rb, cb);
-  GenSpinIn wa, wb;
+// Per-spin and mixed-spin tables of one reference pair, as the distribution sums read them.
+NW_HD void gen_inputs(const GenPair& g, GenSpinIn* wa, GenSpinIn* wb, GenDiffIn* wd) {
   const GenSpin* src[2] = {&g.a, &g.b};
-  GenSpinIn* dst[2] = {&wa, &wb};
+  GenSpinIn* dst[2] = {wa, wb};
   for (int s = 0; s < 2; ++s) {
     for (int i = 0; i < 2; ++i) {
       dst[s]->x[i] = src[s]->x[i];
@@ -1062,19 +1060,34 @@ NW_HD void eval_gen_pair(const GenPair& g, const DetRec& x, const DetRec& w, int
     for (int k = 0; k < 10; ++k) dst[s]->j[k] = src[s]->j[k];
     dst[s]->m = src[s]->m;
   }
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b) {
+      wd->vab0[a][b] = g.vab0[a][b];
+      for (int c = 0; c < 2; ++c) {
+        wd->vab_t[a][b][c] = g.vab_t[a][b][c];
+        wd->vba_t[a][b][c] = g.vba_t[a][b][c];
+        for (int d = 0; d < 2; ++d) wd->ii[a][b][c][d] = g.ii[a][b][c][d];
+      }
+    }
+}
+
+NW_HD void eval_gen_pair(const GenPair& g, const DetRec& x, const DetRec& w, int n, int oa, int ob, double enuc,
+                         double tol, bool exact, double* H, double* S) {
+  const int la = x.ra + w.ra, lb = x.rb + w.rb;
+  int ra[kML], ca[kML], rb[kML], cb[kML];
+  labels_rt(x, w, 0, oa, n, ra, ca);
+  labels_rt(x, w, 1, ob, n, rb, cb);
+  double da0[kML * kML], da1[kML * kML], db0[kML * kML], db1[kML * kML];
+  build_d_rt(da0, g.a.x[0], g.a.y[0], n, la, ra, ca);
+  build_d_rt(da1, g.a.x[1], g.a.y[1], n, la, ra, ca);
+  build_d_rt(db0, g.b.x[0], g.b.y[0], n, lb, rb, cb);
+  build_d_rt(db1, g.b.x[1], g.b.y[1], n, lb, rb, cb);
+  GenSpinIn wa, wb;
+  GenDiffIn wd;
+  gen_inputs(g, &wa, &wb, &wd);
   double sa, h1a, h2aa, sb, h1b, h2bb;
   same_spin_gen_hd(wa, n, la, ra, ca, da0, da1, tol, exact, &sa, &h1a, &h2aa);
   same_spin_gen_hd(wb, n, lb, rb, cb, db0, db1, tol, exact, &sb, &h1b, &h2bb);
-  GenDiffIn wd;
-  for (int a = 0; a < 2; ++a)
-    for (int b = 0; b < 2; ++b) {
-      wd.vab0[a][b] = g.vab0[a][b];
-      for (int c = 0; c < 2; ++c) {
-        wd.vab_t[a][b][c] = g.vab_t[a][b][c];
-        wd.vba_t[a][b][c] = g.vba_t[a][b][c];
-        for (int d = 0; d < 2; ++d) wd.ii[a][b][c][d] = g.ii[a][b][c][d];
-      }
-    }
   const double h2ab = diff_spin_gen_hd(wd, n, g.a.m, g.b.m, la, ra, ca, da0, da1, lb, rb, cb, db0, db1, tol, exact);
   const double pref = x.phase * w.phase * g.a.pref * g.b.pref;
   const double s = pref * sa * sb;
@@ -1083,6 +1096,295 @@ NW_HD void eval_gen_pair(const GenPair& g, const DetRec& x, const DetRec& w, int
   *S = s;
   *H = h;
 }
+
+// ---------------------------------------------------------------------------------------
+// Compile-time-L (<= 4 per spin) twins of same_spin_gen_hd, diff_spin_gen_hd and
+// eval_gen_pair: the same terms in the same order, with the distribution matrices, their
+// cofactors and the minors of the J term in registers by full unrolling instead of in
+// per-thread local memory.
+// ---------------------------------------------------------------------------------------
+template <int L>
+struct Sq {
+  static constexpr int v = L * L > 0 ? L * L : 1;
+};
+
+template <int L>
+NW_HD void mix_ct(double (&out)[Sq<L>::v], const double (&d0)[Sq<L>::v], const double (&d1)[Sq<L>::v],
+                  uint64_t cbits) {
+#pragma unroll
+  for (int r = 0; r < L; ++r)
+#pragma unroll
+    for (int c = 0; c < L; ++c) out[r * L + c] = bitk(cbits, c) ? d1[r * L + c] : d0[r * L + c];
+}
+
+template <int L>
+NW_HD void build_d_ct(double (&d)[Sq<L>::v], const double* xm, const double* ym, int n, const int* rows,
+                      const int* cols) {
+#pragma unroll
+  for (int r = 0; r < L; ++r)
+#pragma unroll
+    for (int c = 0; c < L; ++c) {
+      const int64_t e = (int64_t)rows[r] * n + cols[c];
+      d[r * L + c] = ldg_d((r >= c ? xm : ym) + e);
+    }
+}
+
+// cofactors_tol_rt for compile-time L.
+template <int L>
+NW_HD bool cofactors_tol_ct(double (&cof)[Sq<L>::v], const double (&a)[Sq<L>::v], double tol, double* det_out) {
+  const double d = cofactors_ct<L>(cof, a);
+  if (!(fabs(d) <= 1.7976931348623157e308) || fabs(d) <= tol) return false;
+  *det_out = d;
+  return true;
+}
+
+template <int L>
+NW_HD void minor_ct(double (&out)[Sq<L - 1>::v], const double (&a)[Sq<L>::v], int rr, int cc) {
+  int k = 0;
+#pragma unroll
+  for (int r = 0; r < L; ++r) {
+    if (r == rr) continue;
+#pragma unroll
+    for (int c = 0; c < L; ++c) {
+      if (c == cc) continue;
+      out[k++] = a[r * L + c];
+    }
+  }
+}
+
+template <int L>
+NW_HD void same_spin_gen_ct(const GenSpinIn& w, int n, const int* rows, const int* cols, const double (&d0)[Sq<L>::v],
+                            const double (&d1)[Sq<L>::v], double tol, bool exact, double* s_out, double* h1_out,
+                            double* h2_out) {
+  const int64_t n2 = (int64_t)n * n, n3 = n2 * n;
+  double s = 0.0, h1 = 0.0, h2 = 0.0;
+  uint64_t bits;
+  bool more = first_combination(L + 2, w.m, &bits);
+  while (more) {
+    const int m1 = bitk(bits, 0), m2 = bitk(bits, 1);
+    const uint64_t cb = bits >> 2;
+    double dm[Sq<L>::v], cof[Sq<L>::v];
+    mix_ct<L>(dm, d0, d1, cb);
+    double det = 1.0;
+    bool ok = true;
+    if (L > 0) {
+      if (exact)
+        det = cofactors_ct<L>(cof, dm);
+      else
+        ok = cofactors_tol_ct<L>(cof, dm, tol, &det);
+    }
+    if (ok) {
+      if (m1 == 0 && m2 == 0) s += det;
+      if (m2 == 0) {
+        double contrib = det * w.f0h[m1];
+#pragma unroll
+        for (int k = 0; k < L; ++k) {
+          const double* fsl = w.fh_t[m1][bitk(cb, k)];
+          const int64_t base = (int64_t)cols[k] * n;
+          double corr = 0.0;
+#pragma unroll
+          for (int r = 0; r < L; ++r) corr += (ldg_d(fsl + base + rows[r]) - dm[r * L + k]) * cof[r * L + k];
+          contrib -= det + corr;
+        }
+        h1 += contrib;
+      }
+      double contrib = ((exact && m1 + m2 == 1) ? 0.5 : 1.0) * w.v0[m1 + m2] * det;
+#pragma unroll
+      for (int k = 0; k < L; ++k) {
+        const double* vsl = w.v_t[m1][m2][bitk(cb, k)];
+        const int64_t base = (int64_t)cols[k] * n;
+        double corr = 0.0;
+#pragma unroll
+        for (int r = 0; r < L; ++r) corr += (ldg_d(vsl + base + rows[r]) - dm[r * L + k]) * cof[r * L + k];
+        contrib -= 2.0 * (det + corr);
+      }
+      if constexpr (L >= 2) {
+        constexpr int LM1 = L - 1;
+#pragma unroll
+        for (int i = 0; i < L; ++i)
+#pragma unroll
+          for (int j = 0; j < L; ++j) {
+            const double ph = ((i + j) & 1) ? -1.0 : 1.0;
+            const int ri = rows[i], cj = cols[j];
+            const int mj = bitk(cb, j);
+            double mn[Sq<LM1>::v], cofm[Sq<LM1>::v];
+            minor_ct<L>(mn, dm, i, j);
+            if (exact) {
+              cofactors_ct<LM1>(cofm, mn);
+            } else {
+              double dmin;
+              if (!cofactors_tol_ct<LM1>(cofm, mn, tol, &dmin)) continue;
+            }
+#pragma unroll
+            for (int k2 = 0; k2 < LM1; ++k2) {
+              const int kf = k2 < j ? k2 : k2 + 1;
+              const int mk = bitk(cb, kf);
+              int slot;
+              bool swap;
+              jslot_hd(m1, m2, mk, mj, &slot, &swap);
+              const double* jsl = w.j[slot];
+              const int cc = cols[kf];
+              double det_repl = 0.0;
+#pragma unroll
+              for (int r = 0; r < LM1; ++r) {
+                const int rf = r < i ? r : r + 1;
+                const int rr = rows[rf];
+                const double nv = ldg_d(!swap ? jsl + (ri * n3 + cj * n2 + (int64_t)rr * n + cc)
+                                              : jsl + (rr * n3 + cc * n2 + (int64_t)ri * n + cj));
+                det_repl += nv * cofm[r * LM1 + k2];
+              }
+              contrib += ph * det_repl;
+            }
+          }
+      }
+      h2 += contrib;
+    } else if (m1 == 0 && m2 == 0) {
+      s += det_small(dm, L);
+    }
+    more = advance_combination(L + 2, w.m, &bits);
+  }
+  *s_out = s;
+  *h1_out = h1;
+  *h2_out = h2;
+}
+
+template <int LA, int LB>
+NW_HD double diff_spin_gen_ct(const GenDiffIn& w, int n, int ma, int mb, const int* rows_a, const int* cols_a,
+                              const double (&da0)[Sq<LA>::v], const double (&da1)[Sq<LA>::v], const int* rows_b,
+                              const int* cols_b, const double (&db0)[Sq<LB>::v], const double (&db1)[Sq<LB>::v],
+                              double tol, bool exact) {
+  const int64_t n2 = (int64_t)n * n, n3 = n2 * n;
+  double h2ab = 0.0;
+  uint64_t bits_a;
+  bool more_a = first_combination(LA + 1, ma, &bits_a);
+  while (more_a) {
+    const uint64_t cba = bits_a >> 1;
+    double dma[Sq<LA>::v], cofa[Sq<LA>::v];
+    mix_ct<LA>(dma, da0, da1, cba);
+    double deta = 1.0;
+    bool oka = true;
+    if (exact)
+      deta = cofactors_ct<LA>(cofa, dma);
+    else
+      oka = cofactors_tol_ct<LA>(cofa, dma, tol, &deta);
+    if (oka) {
+      uint64_t bits_b;
+      bool more_b = first_combination(LB + 1, mb, &bits_b);
+      while (more_b) {
+        const uint64_t cbb = bits_b >> 1;
+        double dmb[Sq<LB>::v], cofb[Sq<LB>::v];
+        mix_ct<LB>(dmb, db0, db1, cbb);
+        double detb = 1.0;
+        bool okb = true;
+        if (exact)
+          detb = cofactors_ct<LB>(cofb, dmb);
+        else
+          okb = cofactors_tol_ct<LB>(cofb, dmb, tol, &detb);
+        if (okb) {
+          const int ma0 = bitk(bits_a, 0), mb0 = bitk(bits_b, 0);
+          double contrib = w.vab0[ma0][mb0] * deta * detb;
+#pragma unroll
+          for (int k = 0; k < LA; ++k) {
+            const double* vsl = w.vab_t[ma0][mb0][bitk(cba, k)];
+            const int64_t base = (int64_t)cols_a[k] * n;
+            double rep = 0.0;
+#pragma unroll
+            for (int r = 0; r < LA; ++r) rep += ldg_d(vsl + base + rows_a[r]) * cofa[r * LA + k];
+            contrib -= rep * detb;
+          }
+#pragma unroll
+          for (int k = 0; k < LB; ++k) {
+            const double* vsl = w.vba_t[mb0][ma0][bitk(cbb, k)];
+            const int64_t base = (int64_t)cols_b[k] * n;
+            double rep = 0.0;
+#pragma unroll
+            for (int r = 0; r < LB; ++r) rep += ldg_d(vsl + base + rows_b[r]) * cofb[r * LB + k];
+            contrib -= rep * deta;
+          }
+#pragma unroll
+          for (int i = 0; i < LA; ++i) {
+            const int ra = rows_a[i];
+#pragma unroll
+            for (int j = 0; j < LA; ++j) {
+              const int ca = cols_a[j];
+              const double cij = cofa[i * LA + j];
+              const int ma1 = bitk(cba, j);
+#pragma unroll
+              for (int k = 0; k < LB; ++k) {
+                const double* iisl = w.ii[ma0][ma1][mb0][bitk(cbb, k)];
+                double rep = 0.0;
+#pragma unroll
+                for (int r = 0; r < LB; ++r)
+                  rep += ldg_d(iisl + (ra * n3 + ca * n2 + (int64_t)rows_b[r] * n + cols_b[k])) * cofb[r * LB + k];
+                contrib += cij * rep;
+              }
+            }
+          }
+          h2ab += contrib;
+        }
+        more_b = advance_combination(LB + 1, mb, &bits_b);
+      }
+    }
+    more_a = advance_combination(LA + 1, ma, &bits_a);
+  }
+  return h2ab;
+}
+
+template <int LA, int LB>
+NW_HD void eval_gen_ct(const GenPair& g, const DetRec& x, const DetRec& w, int n, int oa, int ob, double enuc,
+                       double tol, bool exact, double* H, double* S) {
+  int ra[LA > 0 ? LA : 1], ca[LA > 0 ? LA : 1], rb[LB > 0 ? LB : 1], cb[LB > 0 ? LB : 1];
+  det_labels_ct<LA>(x.ra, x.ia, w.ia, oa, n, ra, ca);
+  det_labels_ct<LB>(x.rb, x.ib, w.ib, ob, n, rb, cb);
+  double da0[Sq<LA>::v], da1[Sq<LA>::v], db0[Sq<LB>::v], db1[Sq<LB>::v];
+  build_d_ct<LA>(da0, g.a.x[0], g.a.y[0], n, ra, ca);
+  build_d_ct<LA>(da1, g.a.x[1], g.a.y[1], n, ra, ca);
+  build_d_ct<LB>(db0, g.b.x[0], g.b.y[0], n, rb, cb);
+  build_d_ct<LB>(db1, g.b.x[1], g.b.y[1], n, rb, cb);
+  GenSpinIn wa, wb;
+  GenDiffIn wd;
+  gen_inputs(g, &wa, &wb, &wd);
+  double sa, h1a, h2aa, sb, h1b, h2bb;
+  same_spin_gen_ct<LA>(wa, n, ra, ca, da0, da1, tol, exact, &sa, &h1a, &h2aa);
+  same_spin_gen_ct<LB>(wb, n, rb, cb, db0, db1, tol, exact, &sb, &h1b, &h2bb);
+  const double h2ab = diff_spin_gen_ct<LA, LB>(wd, n, g.a.m, g.b.m, ra, ca, da0, da1, rb, cb, db0, db1, tol, exact);
+  const double pref = x.phase * w.phase * g.a.pref * g.b.pref;
+  const double s = pref * sa * sb;
+  double h = pref * (h1a * sb + h1b * sa + 0.5 * h2aa * sb + 0.5 * h2bb * sa + h2ab);
+  if (exact) h += enuc * s;
+  *S = s;
+  *H = h;
+}
+
+template <int LA, int LB>
+NW_HD_CALL void eval_gen_case(const GenPair& g, const DetRec& x, const DetRec& w, int n, int oa, int ob, double enuc,
+                              double tol, bool exact, double* H, double* S) {
+  eval_gen_ct<LA, LB>(g, x, w, n, oa, ob, enuc, tol, exact, H, S);
+}
+
+#define NW_GEN_CASE(A, B)                                                 \
+  case (A) * 5 + (B):                                                     \
+    eval_gen_case<A, B>(g, x, w, n, oa, ob, enuc, tol, exact, H, S);      \
+    return;
+
+// m > 0 (H, S) of one pair: the register twin (one call per (L_alpha, L_beta) case) for
+// contraction ranks up to 4 per spin, the runtime-size path above that.
+NW_HD void eval_gen_any(const GenPair& g, const DetRec& x, const DetRec& w, int n, int oa, int ob, double enuc,
+                        double tol, bool exact, double* H, double* S) {
+  const int la = x.ra + w.ra, lb = x.rb + w.rb;
+  if (la <= 4 && lb <= 4) {
+    switch (la * 5 + lb) {
+      NW_GEN_CASE(0, 0) NW_GEN_CASE(0, 1) NW_GEN_CASE(0, 2) NW_GEN_CASE(0, 3) NW_GEN_CASE(0, 4)
+      NW_GEN_CASE(1, 0) NW_GEN_CASE(1, 1) NW_GEN_CASE(1, 2) NW_GEN_CASE(1, 3) NW_GEN_CASE(1, 4)
+      NW_GEN_CASE(2, 0) NW_GEN_CASE(2, 1) NW_GEN_CASE(2, 2) NW_GEN_CASE(2, 3) NW_GEN_CASE(2, 4)
+      NW_GEN_CASE(3, 0) NW_GEN_CASE(3, 1) NW_GEN_CASE(3, 2) NW_GEN_CASE(3, 3) NW_GEN_CASE(3, 4)
+      NW_GEN_CASE(4, 0) NW_GEN_CASE(4, 1) NW_GEN_CASE(4, 2) NW_GEN_CASE(4, 3) NW_GEN_CASE(4, 4)
+      default: break;
+    }
+  }
+  eval_gen_pair(g, x, w, n, oa, ob, enuc, tol, exact, H, S);
+}
+#undef NW_GEN_CASE
 
 // Overlap only for one pair (fast or generic layout).
 NW_HD double eval_s_pair(const FastPair* fp, const GenPair* g, const DetRec& x, const DetRec& w, int n, int oa,

@@ -132,10 +132,10 @@ uint64_t mir_sort_keys(const void* dets, uint64_t ndet, int nref, const int32_t*
       keys[i] = 0xFFFFFFFFu;
       continue;
     }
-    const int cls = rank_class((int)((dx >> 8) & 15) + (int)((dw >> 8) & 15), (int)(dx >> 12) + (int)(dw >> 12));
-    keys[i] = pair_sort_key(cls, pairs[2 * i], pw, order[px * nref + pw], nfast, nref, nb, s);
+    const int la = (int)((dx >> 8) & 15) + (int)((dw >> 8) & 15), lb = (int)(dx >> 12) + (int)(dw >> 12);
+    keys[i] = pair_sort_key(la, lb, pairs[2 * i], pw, order[px * nref + pw], nfast, nref, nb, s);
   }
-  return (uint64_t)kRankClasses * nb + (uint64_t)kRankClasses * ((uint64_t)nref * nref - nfast);
+  return (uint64_t)kRankClasses * nb + (uint64_t)kGenClasses * ((uint64_t)nref * nref - nfast);
 }
 
 // Labels through the register (compile-time L) path and the runtime path.
@@ -203,14 +203,19 @@ void mir_eval_fast(const double* recx_a, const double* recy_a, const double* jas
   }
 }
 
-// One ordered reference pair on the reference-ordered layout (m > 0 path).
+// One ordered reference pair on the reference-ordered layout (m > 0 path): the runtime-size
+// evaluator for every pair (dispatch 0), or the kernel's dispatch (dispatch 1: the register
+// twins up to rank 4 per spin).
 void mir_eval_gen(const double* slab, const int64_t* offs, const double* vals, const int32_t* ints, int n, int oa,
                   int ob, double enuc, double tol, int exact, const void* dets, const uint32_t* pairs, int64_t npairs,
-                  double* hs) {
+                  double* hs, int dispatch) {
   const GenPair g = gen_from_oracle(slab, offs, vals, ints);
   for (int64_t i = 0; i < npairs; ++i) {
     const DetRec x = rec_at(dets, pairs[2 * i]), w = rec_at(dets, pairs[2 * i + 1]);
-    eval_gen_pair(g, x, w, n, oa, ob, enuc, tol, exact != 0, &hs[2 * i], &hs[2 * i + 1]);
+    if (dispatch)
+      eval_gen_any(g, x, w, n, oa, ob, enuc, tol, exact != 0, &hs[2 * i], &hs[2 * i + 1]);
+    else
+      eval_gen_pair(g, x, w, n, oa, ob, enuc, tol, exact != 0, &hs[2 * i], &hs[2 * i + 1]);
   }
 }
 

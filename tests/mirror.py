@@ -36,7 +36,7 @@ def lib():
                                     ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_double, VP, U32, ctypes.c_int64, D]
         L.mir_eval_gen.argtypes = [D, I64, D, I32, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
-                                   ctypes.c_double, ctypes.c_int, VP, U32, ctypes.c_int64, D]
+                                   ctypes.c_double, ctypes.c_int, VP, U32, ctypes.c_int64, D, ctypes.c_int]
         L.mir_eval_s_gen.argtypes = [D, I64, D, I32, ctypes.c_int, ctypes.c_int, ctypes.c_int, VP, U32,
                                      ctypes.c_int64, D]
         L.mir_eval_fs_fast.argtypes = [D, D, ctypes.c_double, ctypes.c_double, D, D, ctypes.c_double, ctypes.c_double,
@@ -90,7 +90,7 @@ def eval_fast(build, n, oa, ob, enuc, dets, pairs):
     return hs[0::2], hs[1::2]
 
 
-def eval_gen(orc, pidx, n, oa, ob, dets, pairs, exact=False):
+def eval_gen(orc, pidx, n, oa, ob, dets, pairs, exact=False, dispatch=False):
     pairs = np.ascontiguousarray(pairs, dtype=np.uint32)
     hs = np.empty(2 * pairs.shape[0])
     offs = np.ascontiguousarray(orc.offs[pidx])
@@ -99,7 +99,7 @@ def eval_gen(orc, pidx, n, oa, ob, dets, pairs, exact=False):
     lib().mir_eval_gen(p(orc.slab, ctypes.c_double), p(offs, ctypes.c_int64), p(vals, ctypes.c_double),
                        p(ints, ctypes.c_int32), n, oa, ob, orc.enuc, orc.tol, 1 if exact else 0,
                        dets.ctypes.data_as(VP), p(pairs, ctypes.c_uint32), pairs.shape[0],
-                       p(hs, ctypes.c_double))
+                       p(hs, ctypes.c_double), 1 if dispatch else 0)
     return hs[0::2], hs[1::2]
 
 

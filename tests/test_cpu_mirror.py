@@ -91,8 +91,9 @@ def test_fast_and_generic_evaluators_match_oracle(setup):
             else:
                 for exact in (False, True):
                     ref = np.array([orc.eval_wick(ob, int(p), int(q), exact=exact) for p, q in pairs])
-                    h, s = MR.eval_gen(orc, pid, n, o, o, basis, pairs, exact=exact)
-                    assert np.max(np.abs(h - ref[:, 0])) < TIGHT and np.max(np.abs(s - ref[:, 1])) < TIGHT
+                    for dispatch in (False, True):   # runtime-size path; register twins up to rank 4
+                        h, s = MR.eval_gen(orc, pid, n, o, o, basis, pairs, exact=exact, dispatch=dispatch)
+                        assert np.max(np.abs(h - ref[:, 0])) < TIGHT and np.max(np.abs(s - ref[:, 1])) < TIGHT
                 so = MR.eval_s_gen(orc, pid, n, o, o, basis, pairs)
                 ref_s = np.array([orc.eval_overlap(ob, int(p), int(q)) for p, q in pairs])
                 assert np.max(np.abs(so - ref_s)) < TIGHT
@@ -139,7 +140,7 @@ def test_jacobi_svd_and_canonical_gauge(nzero):
 def test_sort_keys_group_classes_and_bras(setup, cap):
     """pair_sort_key / sort_key_shift as classify_kernel uses them: fast-pair keys lie in their
     class's range [cls * nbucket, (cls + 1) * nbucket), keys of zero-overlap reference pairs
-    after all of them, every key below the planned count, the fast-class counters within the
+    after all of them grouped by the full (L_alpha, L_beta), every key below the planned count, the fast-class counters within the
     budget, and with shift 0 one key holds one (bra, ket reference) combination."""
     import ctypes
     n, o, system, orc, basis, ob = setup
@@ -159,7 +160,7 @@ def test_sort_keys_group_classes_and_bras(setup, cap):
                                    nfast, MR.p(pairs, ctypes.c_uint32), pairs.shape[0], cap, MR.p(keys, ctypes.c_uint32),
                                    MR.p(nb, ctypes.c_uint32), MR.p(sh, ctypes.c_int32))
     nb, sh = int(nb[0]), int(sh[0])
-    assert 26 * nb <= max(cap, 26) and nkeys == 26 * nb + 26 * len(slow)
+    assert 26 * nb <= max(cap, 26) and nkeys == 26 * nb + 81 * len(slow)
     ra, rb = basis["rank_a"].astype(int), basis["rank_b"].astype(int)
     par = basis["parent"].astype(int)
     live = keys != 0xFFFFFFFF
@@ -171,7 +172,7 @@ def test_sort_keys_group_classes_and_bras(setup, cap):
     isfast = order[par[a] * nref + par[b]] < nfast
     assert np.all(k[isfast] // nb == cls[isfast])
     assert np.all(k[~isfast] >= 26 * nb)
-    assert np.all((k[~isfast] - 26 * nb) % 26 == cls[~isfast])
+    assert np.all((k[~isfast] - 26 * nb) % 81 == (la * 9 + lb)[~isfast])
     if sh == 0:
         combo = a.astype(np.int64) * nref + par[b]
         for key in np.unique(k[isfast])[:500]:
