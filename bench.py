@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["config2", "config3"], default="config2")
     ap.add_argument("--npairs", type=int, default=10_000_000)
+    ap.add_argument("--nmo", type=int, default=64,
+                    help="orbitals of the config3 stress system (64; smaller only for profiler captures)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-qmc", action="store_true", help="skip the NOCI-QMC steps/s leg")
@@ -66,7 +68,7 @@ def parse():
     return ap.parse_args()
 
 
-def workload(name: str, npairs: int, rank: int):
+def workload(name: str, npairs: int, rank: int, nmo: int = 64):
     from nociwick import synthetic as sy
     if name == "config2":
         system = sy.config2_system()
@@ -76,12 +78,12 @@ def workload(name: str, npairs: int, rank: int):
                            "26490 SD determinants, uniform pairs across parents",
                "nmo": 30, "nocc": [3, 3], "nref": 3, "ndet": int(basis.shape[0]), "npairs_per_gpu": npairs}
     else:
-        system = sy.config3_system()
-        basis = sy.sd_basis(64, 6, 6, 8)
+        system = sy.config3_system(nmo=nmo)
+        basis = sy.sd_basis(nmo, 6, 6, 8)
         pairs = sy.sample_pairs_by_rank(basis, npairs, seed=rank_seed(3, rank))
-        cfg = {"workload": "synthetic stress: n=64, 6a+6b electrons, naux=256, 8 refs, 6/64 ordered ref "
+        cfg = {"workload": f"synthetic stress: n={nmo}, 6a+6b electrons, naux=256, 8 refs, 6/64 ordered ref "
                            "pairs with zero-overlap orbitals, contraction rank 0-4 uniform",
-               "nmo": 64, "nocc": [6, 6], "nref": 8, "ndet": int(basis.shape[0]), "npairs_per_gpu": npairs}
+               "nmo": nmo, "nocc": [6, 6], "nref": 8, "ndet": int(basis.shape[0]), "npairs_per_gpu": npairs}
     return system, basis, pairs.astype(np.uint32), cfg
 
 
@@ -241,7 +243,7 @@ def reference_pair_conditioning(system) -> np.ndarray:
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    system, basis, pairs, cfg = workload(args.workload, args.npairs, 0)
+    system, basis, pairs, cfg = workload(args.workload, args.npairs, 0, args.nmo)
     sys.path.insert(0, ROOT)
     from oracle.oracle import Oracle
     orc = Oracle.from_system(system, tol=1e-8, with_mo_cache=False)
@@ -568,7 +570,7 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         import torch.distributed as dist  # noqa: F811
     torch.cuda.set_device(local_rank)
-    system, basis, pairs, cfg = workload(args.workload, args.npairs, rank)
+    system, basis, pairs, cfg = workload(args.workload, args.npairs, rank, args.nmo)
     npairs = pairs.shape[0]
     eng = nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8,
                                device=local_rank)

@@ -284,14 +284,30 @@ __device__ __noinline__ void eval_gen_one(const GenPair& g, const DetRec& x, con
   eval_gen_any(g, x, w, P.n, P.nocc_a, P.nocc_b, P.enuc, P.tol, P.exact != 0, H, S);
 }
 
+// Work distribution of the m > 0 evaluators: each warp takes the next 32 key-sorted pairs from a
+// counter (cleared before the launch).  The classes of one reference pair lie in one key range
+// in the same order for every reference pair, so with a static grid stride a thread would meet
+// the same (L_alpha, L_beta) class on every pass and the threads of the costly classes would
+// set the kernel's length while most SMs idle.  Needs every lane of the warp (blockDim % 32 == 0).
+template <typename F>
+__device__ __forceinline__ void for_each_gen_pair(uint32_t begin, uint32_t end, uint32_t* work, F&& f) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t nchunk = (end - begin + 31) / 32;
+  for (;;) {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(work, 1u);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if (c >= nchunk) break;
+    const uint32_t t = begin + c * 32 + lane;
+    if (t < end) f(t);
+  }
+}
+
 __global__ void __launch_bounds__(128) eval_gen_kernel(EvalParams P, const uint2* __restrict__ pairs,
                                                        const uint32_t* __restrict__ sidx,
                                                        const uint32_t* __restrict__ offsets, int nkeys,
-                                                       double* __restrict__ out) {
-  const uint32_t begin = offsets[kClasses * P.nbucket];
-  const uint32_t end = offsets[nkeys];
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t t = begin + blockIdx.x * blockDim.x + threadIdx.x; t < end; t += stride) {
+                                                       double* __restrict__ out, uint32_t* __restrict__ work) {
+  for_each_gen_pair(offsets[kClasses * P.nbucket], offsets[nkeys], work, [&](uint32_t t) {
     const uint32_t i = sidx[t];
     const uint2 ab = __ldg(pairs + i);
     const DetRec x = load_det(P.dets, ab.x);
@@ -300,7 +316,7 @@ __global__ void __launch_bounds__(128) eval_gen_kernel(EvalParams P, const uint2
     double h, s;
     eval_gen_one(g, x, w, P, &h, &s);
     store_hs(out, i, h, s);
-  }
+  });
 }
 
 // ---------------------------------------------------------------------------------------
@@ -375,11 +391,8 @@ __device__ __noinline__ void eval_fs_gen_one(const GenPair& g, const FockPair& f
 __global__ void __launch_bounds__(128) eval_fs_gen_kernel(EvalParams P, const uint2* __restrict__ pairs,
                                                           const uint32_t* __restrict__ sidx,
                                                           const uint32_t* __restrict__ offsets, int nkeys,
-                                                          double* __restrict__ out) {
-  const uint32_t begin = offsets[kClasses * P.nbucket];
-  const uint32_t end = offsets[nkeys];
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t t = begin + blockIdx.x * blockDim.x + threadIdx.x; t < end; t += stride) {
+                                                          double* __restrict__ out, uint32_t* __restrict__ work) {
+  for_each_gen_pair(offsets[kClasses * P.nbucket], offsets[nkeys], work, [&](uint32_t t) {
     const uint32_t i = sidx[t];
     const uint2 ab = __ldg(pairs + i);
     const DetRec x = load_det(P.dets, ab.x);
@@ -388,7 +401,7 @@ __global__ void __launch_bounds__(128) eval_fs_gen_kernel(EvalParams P, const ui
     double f, s;
     eval_fs_gen_one(P.gen[p], P.fock[p], x, w, P, &f, &s);
     store_hs(out, i, f, s);
-  }
+  });
 }
 
 // ---------------------------------------------------------------------------------------
@@ -518,10 +531,11 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
     NW_CUDA(ctx, cudaGetLastError());
   }
   if (gen) {
+    NW_CUDA(ctx, cudaMemsetAsync(S.work, 0, sizeof(uint32_t), ctx->s_aux[2]));
     if (mode == EvalMode::kFS)
-      eval_fs_gen_kernel<<<148 * 4, 128, 0, ctx->s_aux[2]>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out);
+      eval_fs_gen_kernel<<<148 * 4, 128, 0, ctx->s_aux[2]>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out, S.work);
     else
-      eval_gen_kernel<<<148 * 4, 128, 0, ctx->s_aux[2]>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out);
+      eval_gen_kernel<<<148 * 4, 128, 0, ctx->s_aux[2]>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out, S.work);
     NW_CUDA(ctx, cudaGetLastError());
   }
   for (int i = 0; i < 3; ++i) {
@@ -575,6 +589,7 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
   S.offsets = static_cast<uint32_t*>(ctx->offsets.p);
   S.tsum = static_cast<uint32_t*>(ctx->tsum.p);
   S.flag = flag;
+  S.work = flag + 8;
   st = launch_sorted(ctx, P, nkeys, pairs, npairs, out, S, stream, ctx->timing ? ctx->ev : nullptr, mode);
   if (st == NW_OK && ctx->timing) ctx->timed_valid = true;
   return st;
@@ -668,6 +683,7 @@ nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs
   S.offsets = reinterpret_cast<uint32_t*>(base + kNoallocOffOffsets);
   S.tsum = reinterpret_cast<uint32_t*>(base + kNoallocOffTsum);
   S.flag = reinterpret_cast<uint32_t*>(base + kNoallocOffFlag);
+  S.work = S.flag + 8;
   NW_CUDA(ctx, cudaMemsetAsync(S.flag, 0, sizeof(uint32_t), stream));
   return launch_sorted(ctx, P, nkeys, pairs, npairs, out, S, stream, nullptr);
 }

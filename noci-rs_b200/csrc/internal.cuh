@@ -150,6 +150,7 @@ struct SortScratch {
   uint32_t* offsets;  // nkeys + 1
   uint32_t* tsum;     // nkeys / 4096 + 1
   uint32_t* flag;
+  uint32_t* work;     // chunk counter of the m > 0 evaluators (a word of the flag buffer, >= 64 bytes)
 };
 
 // Fine-key budget of the sort (pair_sort_key): at most kFineMax counters, and at most about one

@@ -818,6 +818,7 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
   take(q->S.offsets, q->nkeys + 1);
   take(q->S.tsum, q->nkeys / 4096 + 1);
   take(q->S.flag, 64);
+  q->S.work = q->S.flag ? q->S.flag + 8 : nullptr;
   // learned-proposal bins: child reference x (rank_a, rank_b) class
   q->learnable = ctx->nref <= kLearnMaxRefs;
   std::vector<uint32_t> det_bin(nd), bin_off(q->q.nbin + 1, 0), bin_mem(nd), pos(nd);
