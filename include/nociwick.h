@@ -143,7 +143,7 @@ NW_API nw_status nw_eval_hs_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint6
  * nearly all of HBM, or a latency-critical loop that cannot take cudaMalloc's implicit
  * synchronisation or its failure path).  No counterpart in the reference.
  * Limits: at most 1,048,576 pairs per call and at most 64 references (larger requests return
- * NW_ERR_UNSUPPORTED).  The per-call scratch lives in one fixed device array of about 14 MB that
+ * NW_ERR_UNSUPPORTED).  The per-call scratch lives in one fixed device array of about 16 MB that
  * every GPU loading this library holds until the process exits; its device address is looked
  * up on the first call on each device, so make that first call before any stream capture.
  * All calls share the array: calls whose work overlaps on the GPU race and must be serialised.

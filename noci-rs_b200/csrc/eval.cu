@@ -146,20 +146,58 @@ __global__ void __launch_bounds__(kScanThreads) scan_top_kernel(uint32_t* __rest
   }
 }
 
+// Each thread owns kScanPer consecutive counters of the tile, so the tile takes one block-wide
+// scan (a round of block scans per kScanThreads counters left every launch as long as 16
+// dependent block barriers).  Full 16-counter runs of 16-byte-aligned buffers move as uint4.
+constexpr int kScanPer = kScanTile / kScanThreads;
+static_assert(kScanPer == 16, "four uint4 per thread");
+
 __global__ void __launch_bounds__(kScanThreads) scan_down_kernel(const uint32_t* __restrict__ counts, uint32_t n,
                                                                   const uint32_t* __restrict__ tsum,
                                                                   uint32_t* __restrict__ offsets) {
   __shared__ uint32_t warp_tot[kScanThreads / 32];
   __shared__ uint32_t total;
-  const uint32_t base = blockIdx.x * (uint32_t)kScanTile;
-  uint32_t carry = tsum[blockIdx.x];
-  for (int r = 0; r < kScanTile / kScanThreads; ++r) {
-    const uint32_t k = base + r * kScanThreads + threadIdx.x;
-    const uint32_t v = k < n ? counts[k] : 0u;
-    const uint32_t e = block_exclusive_scan(v, warp_tot, &total);
-    if (k <= n) offsets[k] = carry + e;  // offsets[n] = total of all counters
-    carry += total;
-    if (base + (r + 1) * kScanThreads > n) break;
+  const uint32_t k0 = blockIdx.x * (uint32_t)kScanTile + threadIdx.x * (uint32_t)kScanPer;
+  const bool vec = (uint64_t)k0 + kScanPer <= n &&
+                   ((reinterpret_cast<uintptr_t>(counts) | reinterpret_cast<uintptr_t>(offsets)) & 15) == 0;
+  uint32_t v[kScanPer];
+  if (vec) {
+#pragma unroll
+    for (int q = 0; q < kScanPer / 4; ++q) {
+      const uint4 c = __ldg(reinterpret_cast<const uint4*>(counts + k0) + q);
+      v[4 * q] = c.x;
+      v[4 * q + 1] = c.y;
+      v[4 * q + 2] = c.z;
+      v[4 * q + 3] = c.w;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < kScanPer; ++j) v[j] = (uint64_t)k0 + j < n ? counts[k0 + j] : 0u;
+  }
+  uint32_t sum = 0;
+#pragma unroll
+  for (int j = 0; j < kScanPer; ++j) sum += v[j];
+  uint32_t run = tsum[blockIdx.x] + block_exclusive_scan(sum, warp_tot, &total);
+  if (vec) {
+#pragma unroll
+    for (int q = 0; q < kScanPer / 4; ++q) {
+      uint4 o;
+      o.x = run;
+      run += v[4 * q];
+      o.y = run;
+      run += v[4 * q + 1];
+      o.z = run;
+      run += v[4 * q + 2];
+      o.w = run;
+      run += v[4 * q + 3];
+      reinterpret_cast<uint4*>(offsets + k0)[q] = o;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < kScanPer; ++j) {
+      if ((uint64_t)k0 + j <= n) offsets[k0 + j] = run;  // offsets[n] = total of all counters
+      run += v[j];
+    }
   }
 }
 
@@ -606,7 +644,7 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
 // lives in the fixed device array below instead of buffers grown with cudaMalloc.
 //
 // The array is a file-scope __device__ variable, so every GPU that loads this library holds
-// it (14,287,360 bytes, 13.6 MiB) until the process exits.  Host code cannot use its name as a
+// it (16,089,856 bytes, 15.3 MiB) until the process exits.  Host code cannot use its name as a
 // device address: the address is looked up with cudaGetSymbolAddress once per device, with
 // that device current, on the first call of the entry point on that device (that first call
 // should therefore come before any stream capture).  Every call shares the array and it keeps

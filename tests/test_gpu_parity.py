@@ -102,6 +102,26 @@ def test_device_entry_matches_host_entry_and_is_deterministic():
     assert np.array_equal(dev1, dev2)
 
 
+def test_zero_overlap_pairs_independent_of_position():
+    """The m > 0 evaluator hands 32-pair chunks to warps from a counter, so which warp computes a
+    pair changes from call to call; every pair is still computed by the same arithmetic, so its
+    (H, S) is bit-identical across calls, in a permuted request and inside a larger one, for
+    every contraction-rank case (up to quadruples: the register twins and the runtime path)."""
+    system = sy.make_system(8, 3, 3, 3, 20, seed=4, k_scale=0.3, zero_pairs=[(0, 1, 1, 0), (1, 2, 0, 2)])
+    basis = sy.sd_basis(8, 3, 3, 3, orders=(1, 2, 3, 4))
+    pairs = sy.sample_pairs(basis, 40000, seed=21)
+    perm = np.random.default_rng(5).permutation(pairs.shape[0])
+    with _engine(system) as w:
+        w.set_basis(basis)
+        first = w.eval_pairs(pairs)
+        again = w.eval_pairs(pairs)
+        permuted = w.eval_pairs(pairs[perm])
+        head = w.eval_pairs(pairs[:777])
+    assert np.array_equal(first, again)
+    assert np.array_equal(first[perm], permuted)
+    assert np.array_equal(first[:777], head)
+
+
 def test_autotune_keeps_every_result_bit():
     """nw_autotune only changes the bucketing and the grid of later calls; every element is
     computed by the same arithmetic, so results are bit-identical before and after."""
