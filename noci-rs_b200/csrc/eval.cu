@@ -80,9 +80,9 @@ __global__ void __launch_bounds__(256) classify_kernel(EvalParams P, const uint3
   }
 }
 
-// Exclusive scan of counts[0..n) into offsets[0..n] (offsets[n] = total), in three passes over
-// tiles of kScanTile counters: tile sums, a one-block scan of the tile sums, then each tile's
-// scan from its base.  Tiles are walked in rounds of one counter per thread (coalesced).
+// Exclusive scan of counts[0..n) into offsets[0..n] (offsets[n] = total), in two passes over
+// tiles of kScanTile counters: tile sums, then each tile's scan from its base, the sum of the
+// earlier tiles' sums that the tile's block adds up itself (at most a few thousand tiles).
 constexpr int kScanThreads = 256;
 constexpr int kScanTile = kScanThreads * 16;
 
@@ -132,20 +132,6 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles_kernel(const uint32_t
   }
 }
 
-__global__ void __launch_bounds__(kScanThreads) scan_top_kernel(uint32_t* __restrict__ tsum, int ntiles) {
-  __shared__ uint32_t warp_tot[kScanThreads / 32];
-  __shared__ uint32_t total;
-  uint32_t carry = 0;
-  for (int b = 0; b < ntiles; b += kScanThreads) {
-    const int k = b + threadIdx.x;
-    const uint32_t v = k < ntiles ? tsum[k] : 0u;
-    const uint32_t e = block_exclusive_scan(v, warp_tot, &total);
-    if (k < ntiles) tsum[k] = carry + e;
-    carry += total;
-    __syncthreads();
-  }
-}
-
 // Each thread owns kScanPer consecutive counters of the tile, so the tile takes one block-wide
 // scan (a round of block scans per kScanThreads counters left every launch as long as 16
 // dependent block barriers).  Full 16-counter runs of 16-byte-aligned buffers move as uint4.
@@ -177,7 +163,12 @@ __global__ void __launch_bounds__(kScanThreads) scan_down_kernel(const uint32_t*
   uint32_t sum = 0;
 #pragma unroll
   for (int j = 0; j < kScanPer; ++j) sum += v[j];
-  uint32_t run = tsum[blockIdx.x] + block_exclusive_scan(sum, warp_tot, &total);
+  // base of the tile: the sums of tiles 0 .. blockIdx.x - 1
+  uint32_t part = 0;
+  for (uint32_t t = threadIdx.x; t < blockIdx.x; t += kScanThreads) part += tsum[t];
+  block_exclusive_scan(part, warp_tot, &total);
+  const uint32_t base = total;  // read before the next scan rewrites it (behind its first barrier)
+  uint32_t run = base + block_exclusive_scan(sum, warp_tot, &total);
   if (vec) {
 #pragma unroll
     for (int q = 0; q < kScanPer / 4; ++q) {
@@ -518,7 +509,6 @@ nw_status scan_exclusive(nw_ctx* ctx, const uint32_t* counts, uint64_t n, uint32
                          cudaStream_t stream) {
   const int ntiles = (int)(n / kScanTile + 1);
   scan_tiles_kernel<<<ntiles, kScanThreads, 0, stream>>>(counts, (uint32_t)n, tsum);
-  scan_top_kernel<<<1, kScanThreads, 0, stream>>>(tsum, ntiles);
   scan_down_kernel<<<ntiles, kScanThreads, 0, stream>>>(counts, (uint32_t)n, tsum, offsets);
   NW_CUDA(ctx, cudaGetLastError());
   return NW_OK;
@@ -540,7 +530,6 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[1], stream));
   const int ntiles = (int)(nkeys / kScanTile + 1);
   scan_tiles_kernel<<<ntiles, kScanThreads, 0, stream>>>(S.counts, (uint32_t)nkeys, S.tsum);
-  scan_top_kernel<<<1, kScanThreads, 0, stream>>>(S.tsum, ntiles);
   scan_down_kernel<<<ntiles, kScanThreads, 0, stream>>>(S.counts, (uint32_t)nkeys, S.tsum, S.offsets);
   NW_CUDA(ctx, cudaGetLastError());
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[2], stream));
