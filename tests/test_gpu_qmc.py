@@ -92,6 +92,30 @@ def test_run_converges_to_noci_ground_state(zero_pairs):
     # above).
 
 
+def test_graph_block_matches_direct_cycle_zero_overlap():
+    """A report block of one cycle replayed from its CUDA graph changes the populations by the
+    delta of the same cycle run directly (same counter-based draws; the two differ only in the
+    order of the FP64 atomic accumulations), after several replays: every replay evaluates the
+    attempts on the zero-overlap reference pair (the m > 0 evaluator's work counter is cleared
+    inside the graph)."""
+    w, basis, h, s, refs = _setup(zero_pairs=((0, 1, 1, 0),))
+    nd = basis.shape[0]
+    c0 = np.zeros(nd)
+    c0[refs] = 1.0
+    with w, nociwick.Qmc(w, c0, refs, dt=0.004, initial_population=2000.0, target_population=1e5,
+                         sampling_cutoff=0.5, spawn_cutoff=0.05, initial_shift=-5.2, ncycles=1,
+                         propagator="unshifted", seed=7, max_attempts=1_000_000) as q:
+        q.run(4)                                   # capture, then replays; cycle counter = 4
+        for k in range(4, 7):
+            before = q.populations()
+            d = q.cycle_delta(k)
+            q.run(1)
+            after = q.populations()
+            scale = np.abs(before).max()
+            assert np.abs((after - before) - d).max() <= 1e-12 * scale, np.abs((after - before) - d).max()
+            assert np.abs(d).max() > 1e-6 * scale
+
+
 def test_capacity_overflow_is_reported():
     w, basis, h, s, refs = _setup()
     nd = basis.shape[0]
