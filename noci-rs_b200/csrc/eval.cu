@@ -6,13 +6,14 @@
 //      apart, noci-rs hs.rs:96-101), key every other pair by (contraction-rank class, bra
 //      determinant, ket reference) -- pair_sort_key -- and take its rank within the key from a
 //      global per-key counter;
-//   2. scan the per-key counts (three passes over tiles);
-//   3. scatter each pair and its request index to offsets[key] + rank;
+//   2. scan the per-key counts (two passes over tiles);
+//   3. scatter each pair's request index to offsets[key] + rank;
 //   4. evaluate: one thread per pair; a warp sees one (L_alpha, L_beta) class, mostly one bra
 //      determinant, so the fused m = 0 evaluator runs divergence-free with its contraction
 //      determinant, cofactors and gathered intermediates in registers, and the lanes share the
 //      bra's rows of the gathered tables.  Reference pairs with zero-overlap orbitals (m > 0)
-//      are evaluated by a separate kernel over the tail of the sorted order.
+//      are evaluated by a separate kernel over the tail of the sorted order, keyed by
+//      (reference pair, L_alpha, L_beta), whose warps take 32-pair chunks from a counter.
 #include <cuda_runtime.h>
 
 #include <algorithm>
