@@ -20,7 +20,7 @@ equal exactly when the reference's label strings ``"{generating label} {excitati
 
 The optional learned screener (``LearnedScreen``, passed to ``snoci``) keeps only the
 candidates an MLP ranks highest before M is built; the exhaustive screen stays the default and
-the judge of its error.
+the referee of its error.
 """
 from __future__ import annotations
 
@@ -278,7 +278,7 @@ class SnociOptions:
     density_phases: bool = True     # reference density convention (see noci_density)
     keep_fraction: float = 0.25     # learned screener: share of the pool kept for PT2
     min_keep: int = 64
-    audit: bool = False             # screened iterations also score the whole pool (the judge)
+    audit: bool = False             # screened iterations also score the whole pool (the referee)
 
 
 @dataclass

@@ -75,7 +75,7 @@ def test_first_step_matches_dense_restatement():
 
 
 def test_learned_screener_keeps_the_exhaustive_picks():
-    """Audited run (the exhaustive screen as the judge): at every screened iteration the
+    """Audited run (the exhaustive screen as the referee): at every screened iteration the
     candidates the exhaustive screen would select are among the kept ones, and the screened
     iterations score far fewer candidates than the exhaustive run."""
     system = _system(nmo=10, nocc=2, nref=3, seed=5)
