@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(256) eval_fs_heavy_kernel(EvalParams P, const 
 
 __device__ __noinline__ void eval_fs_gen_one(const GenPair& g, const FockPair& fk, const DetRec& x, const DetRec& w,
                                              const EvalParams& P, double* F, double* S) {
-  eval_fs_gen_pair(g, fk, x, w, P.n, P.nocc_a, P.nocc_b, P.tol, P.exact != 0, F, S);
+  eval_fs_gen_any(g, fk, x, w, P.n, P.nocc_a, P.nocc_b, P.tol, P.exact != 0, F, S);
 }
 
 __global__ void __launch_bounds__(128) eval_fs_gen_kernel(EvalParams P, const uint2* __restrict__ pairs,

@@ -1593,6 +1593,112 @@ NW_HD void eval_fs_gen_pair(const GenPair& g, const FockPair& fk, const DetRec& 
   combine_fs(x.phase * w.phase, g.a.pref, deta, fa, g.b.pref, detb, fb, F, S);
 }
 
+// Compile-time-L (<= 4 per spin) twins of overlap_spin_hd, spin_f_gen_hd and eval_fs_gen_pair:
+// the same terms in the same order, with the distribution matrices and cofactors in registers.
+template <int L>
+NW_HD double overlap_spin_ct(int m, const double (&d0)[Sq<L>::v], const double (&d1)[Sq<L>::v]) {
+  if (m > L) return 0.0;
+  if (m == 0) return det_small(d0, L);
+  if (m == L) return det_small(d1, L);
+  double acc = 0.0;
+  uint64_t bits;
+  bool more = first_combination(L, m, &bits);
+  while (more) {
+    double dm[Sq<L>::v];
+    mix_ct<L>(dm, d0, d1, bits);
+    acc += det_small(dm, L);
+    more = advance_combination(L, m, &bits);
+  }
+  return acc;
+}
+
+template <int L>
+NW_HD double spin_f_gen_ct(int m, const double* const (*ff_t)[2], const double* f0f, int n, const int* rows,
+                           const int* cols, const double (&d0)[Sq<L>::v], const double (&d1)[Sq<L>::v], double tol,
+                           bool exact) {
+  double acc = 0.0;
+  uint64_t bits;
+  bool more = first_combination(L + 1, m, &bits);
+  while (more) {
+    const int mi = bitk(bits, 0);
+    const uint64_t cb = bits >> 1;
+    double dm[Sq<L>::v], cof[Sq<L>::v];
+    mix_ct<L>(dm, d0, d1, cb);
+    double det = 1.0;
+    bool ok = true;
+    if (L > 0) {
+      if (exact)
+        det = cofactors_ct<L>(cof, dm);
+      else
+        ok = cofactors_tol_ct<L>(cof, dm, tol, &det);
+    }
+    if (ok) {
+      double contrib = det * f0f[mi];
+#pragma unroll
+      for (int b = 0; b < L; ++b) {
+        const double* fsl = ff_t[mi][bitk(cb, b)];
+        const int64_t base = (int64_t)cols[b] * n;
+        double corr = 0.0;
+#pragma unroll
+        for (int r = 0; r < L; ++r) corr += (ldg_d(fsl + base + rows[r]) - dm[r * L + b]) * cof[r * L + b];
+        contrib -= det + corr;
+      }
+      acc += contrib;
+    }
+    more = advance_combination(L + 1, m, &bits);
+  }
+  return acc;
+}
+
+template <int LA, int LB>
+NW_HD void eval_fs_gen_ct(const GenPair& g, const FockPair& fk, const DetRec& x, const DetRec& w, int n, int oa,
+                          int ob, double tol, bool exact, double* F, double* S) {
+  int ra[LA > 0 ? LA : 1], ca[LA > 0 ? LA : 1], rb[LB > 0 ? LB : 1], cb[LB > 0 ? LB : 1];
+  det_labels_ct<LA>(x.ra, x.ia, w.ia, oa, n, ra, ca);
+  det_labels_ct<LB>(x.rb, x.ib, w.ib, ob, n, rb, cb);
+  double d0[Sq<LA>::v], d1[Sq<LA>::v];
+  build_d_ct<LA>(d0, g.a.x[0], g.a.y[0], n, ra, ca);
+  build_d_ct<LA>(d1, g.a.x[1], g.a.y[1], n, ra, ca);
+  const double deta = overlap_spin_ct<LA>(g.a.m, d0, d1);
+  const double fa = spin_f_gen_ct<LA>(g.a.m, fk.a.ff_t, fk.a.f0f, n, ra, ca, d0, d1, tol, exact);
+  double e0[Sq<LB>::v], e1[Sq<LB>::v];
+  build_d_ct<LB>(e0, g.b.x[0], g.b.y[0], n, rb, cb);
+  build_d_ct<LB>(e1, g.b.x[1], g.b.y[1], n, rb, cb);
+  const double detb = overlap_spin_ct<LB>(g.b.m, e0, e1);
+  const double fb = spin_f_gen_ct<LB>(g.b.m, fk.b.ff_t, fk.b.f0f, n, rb, cb, e0, e1, tol, exact);
+  combine_fs(x.phase * w.phase, g.a.pref, deta, fa, g.b.pref, detb, fb, F, S);
+}
+
+template <int LA, int LB>
+NW_HD_CALL void eval_fs_gen_case(const GenPair& g, const FockPair& fk, const DetRec& x, const DetRec& w, int n,
+                                 int oa, int ob, double tol, bool exact, double* F, double* S) {
+  eval_fs_gen_ct<LA, LB>(g, fk, x, w, n, oa, ob, tol, exact, F, S);
+}
+
+#define NW_FS_GEN_CASE(A, B)                                                   \
+  case (A) * 5 + (B):                                                          \
+    eval_fs_gen_case<A, B>(g, fk, x, w, n, oa, ob, tol, exact, F, S);          \
+    return;
+
+// m > 0 (F, S) of one pair: the register twin (one call per (L_alpha, L_beta) case) for
+// contraction ranks up to 4 per spin, the runtime-size path above that.
+NW_HD void eval_fs_gen_any(const GenPair& g, const FockPair& fk, const DetRec& x, const DetRec& w, int n, int oa,
+                           int ob, double tol, bool exact, double* F, double* S) {
+  const int la = x.ra + w.ra, lb = x.rb + w.rb;
+  if (la <= 4 && lb <= 4) {
+    switch (la * 5 + lb) {
+      NW_FS_GEN_CASE(0, 0) NW_FS_GEN_CASE(0, 1) NW_FS_GEN_CASE(0, 2) NW_FS_GEN_CASE(0, 3) NW_FS_GEN_CASE(0, 4)
+      NW_FS_GEN_CASE(1, 0) NW_FS_GEN_CASE(1, 1) NW_FS_GEN_CASE(1, 2) NW_FS_GEN_CASE(1, 3) NW_FS_GEN_CASE(1, 4)
+      NW_FS_GEN_CASE(2, 0) NW_FS_GEN_CASE(2, 1) NW_FS_GEN_CASE(2, 2) NW_FS_GEN_CASE(2, 3) NW_FS_GEN_CASE(2, 4)
+      NW_FS_GEN_CASE(3, 0) NW_FS_GEN_CASE(3, 1) NW_FS_GEN_CASE(3, 2) NW_FS_GEN_CASE(3, 3) NW_FS_GEN_CASE(3, 4)
+      NW_FS_GEN_CASE(4, 0) NW_FS_GEN_CASE(4, 1) NW_FS_GEN_CASE(4, 2) NW_FS_GEN_CASE(4, 3) NW_FS_GEN_CASE(4, 4)
+      default: break;
+    }
+  }
+  eval_fs_gen_pair(g, fk, x, w, n, oa, ob, tol, exact, F, S);
+}
+#undef NW_FS_GEN_CASE
+
 // ---------------------------------------------------------------------------------------
 // Layout formulas of the build.  T4 buffers hold T(A,B,C,D)[p,q,r,s] at [p][r][q][s].
 // ---------------------------------------------------------------------------------------

@@ -253,7 +253,7 @@ void mir_eval_fs_fast(const double* frecx_a, const double* frecy_a, double f0_a,
 // (F, S) on the reference-ordered layout: ff_t[spin][mi*2+mj] transposed Fock columns.
 void mir_eval_fs_gen(const double* slab, const int64_t* offs, const double* vals, const int32_t* ints,
                      const double* fslab, const int64_t* foffs, const double* fvals, int n, int oa, int ob, double tol,
-                     int exact, const void* dets, const uint32_t* pairs, int64_t npairs, double* fs) {
+                     int exact, const void* dets, const uint32_t* pairs, int64_t npairs, double* fs, int dispatch) {
   const GenPair g = gen_from_oracle(slab, offs, vals, ints);
   FockPair fk;
   std::memset(&fk, 0, sizeof(fk));
@@ -265,7 +265,10 @@ void mir_eval_fs_gen(const double* slab, const int64_t* offs, const double* vals
   }
   for (int64_t i = 0; i < npairs; ++i) {
     const DetRec x = rec_at(dets, pairs[2 * i]), w = rec_at(dets, pairs[2 * i + 1]);
-    eval_fs_gen_pair(g, fk, x, w, n, oa, ob, tol, exact != 0, &fs[2 * i], &fs[2 * i + 1]);
+    if (dispatch)  // the kernel's dispatch: register twins up to rank 4 per spin
+      eval_fs_gen_any(g, fk, x, w, n, oa, ob, tol, exact != 0, &fs[2 * i], &fs[2 * i + 1]);
+    else
+      eval_fs_gen_pair(g, fk, x, w, n, oa, ob, tol, exact != 0, &fs[2 * i], &fs[2 * i + 1]);
   }
 }
 

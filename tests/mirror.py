@@ -42,7 +42,7 @@ def lib():
         L.mir_eval_fs_fast.argtypes = [D, D, ctypes.c_double, ctypes.c_double, D, D, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, VP, U32, ctypes.c_int64, D]
         L.mir_eval_fs_gen.argtypes = [D, I64, D, I32, D, I64, D, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                                      ctypes.c_double, ctypes.c_int, VP, U32, ctypes.c_int64, D]
+                                      ctypes.c_double, ctypes.c_int, VP, U32, ctypes.c_int64, D, ctypes.c_int]
         L.mir_philox.argtypes = [U32, ctypes.c_uint32, ctypes.c_uint32, U32]
         L.mir_uniform2.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, D]
         L.mir_fri.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
@@ -153,8 +153,9 @@ def eval_fs_fast(orc, build, pidx, n, oa, ob, dets, pairs):
     return fs[0::2], fs[1::2]
 
 
-def eval_fs_gen(orc, pidx, n, oa, ob, dets, pairs, exact=False):
-    """(F, S) of one ordered pair with zero-overlap orbitals through the device code."""
+def eval_fs_gen(orc, pidx, n, oa, ob, dets, pairs, exact=False, dispatch=False):
+    """(F, S) of one ordered pair with zero-overlap orbitals through the device code: the
+    runtime-size evaluator, or with dispatch the kernel's (register twins up to rank 4)."""
     pairs = np.ascontiguousarray(pairs, dtype=np.uint32)
     fs = np.empty(2 * pairs.shape[0])
     offs = np.ascontiguousarray(orc.offs[pidx])
@@ -166,5 +167,5 @@ def eval_fs_gen(orc, pidx, n, oa, ob, dets, pairs, exact=False):
                           p(ints, ctypes.c_int32), p(orc.fslab, ctypes.c_double), p(foffs, ctypes.c_int64),
                           p(fvals, ctypes.c_double), n, oa, ob, orc.tol, 1 if exact else 0,
                           dets.ctypes.data_as(VP), p(pairs, ctypes.c_uint32), pairs.shape[0],
-                          p(fs, ctypes.c_double))
+                          p(fs, ctypes.c_double), 1 if dispatch else 0)
     return fs[0::2], fs[1::2]

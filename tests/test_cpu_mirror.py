@@ -207,5 +207,6 @@ def test_fock_evaluators_match_oracle(setup):
             else:
                 for exact in (False, True):
                     _, f_ref, s_ref = orc.eval_m_pairs(ob, pairs, 0.0, exact=exact)
-                    f, s = MR.eval_fs_gen(orc, pid, n, o, o, basis, pairs, exact=exact)
-                    assert np.max(np.abs(f - f_ref)) < TIGHT and np.max(np.abs(s - s_ref)) < TIGHT
+                    for dispatch in (False, True):   # runtime-size path; register twins up to rank 4
+                        f, s = MR.eval_fs_gen(orc, pid, n, o, o, basis, pairs, exact=exact, dispatch=dispatch)
+                        assert np.max(np.abs(f - f_ref)) < TIGHT and np.max(np.abs(s - s_ref)) < TIGHT
