@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-qmc", action="store_true", help="skip the NOCI-QMC steps/s leg")
+    ap.add_argument("--no-config3", action="store_true", help="skip the config-3 H/S leg")
+    ap.add_argument("--config3-npairs", type=int, default=100_000_000, help="pairs of the config-3 H/S leg")
     ap.add_argument("--qmc-reports", type=int, default=30, help="timed QMC report blocks (10 steps each)")
     ap.add_argument("--no-pt2", action="store_true", help="skip the NOCI-PT2 mat-vec / GMRES leg")
     ap.add_argument("--pt2-ncand", type=int, default=0, help="PT2 candidates (0: all 125685 of the stand-in)")
@@ -63,8 +65,10 @@ def parse():
     ap.add_argument("--no-snoci", action="store_true", help="skip the selected-NOCI screening leg")
     ap.add_argument("--qmc-equil", type=int, default=40, help="QMC equilibration report blocks")
     ap.add_argument("--qmc-train-epochs", type=int, default=2, help="epochs of proposal training")
-    ap.add_argument("--qmc-compare-reports", type=int, default=2000,
-                    help="report blocks (10 steps each) per generator in the uniform vs learned comparison (0: skip)")
+    ap.add_argument("--qmc-seeds", type=int, default=3,
+                    help="independent runs per generator in the uniform vs learned comparison (0: skip)")
+    ap.add_argument("--qmc-max-seconds", type=float, default=30.0,
+                    help="device-time cap of each run of the generator comparison")
     return ap.parse_args()
 
 
@@ -88,7 +92,11 @@ def workload(name: str, npairs: int, rank: int, nmo: int = 64):
 
 
 PIPE_CHUNKS, PIPE_MIN_CHUNK = 16, 1 << 18  # chunking of the pinned-host entry (csrc/internal.cuh)
-EVAL_TRAFFIC_CONFIG2_10M = 1_438_561_280  # bytes per step, see profiles/eval_traffic_config2_10Mpairs.md
+# DRAM bytes (read + write) of one step's evaluator launches, from ncu captures of these workloads
+# (dram__bytes_read.sum + dram__bytes_write.sum; the summaries under profiles/ give the commands)
+EVAL_TRAFFIC = {
+    ("config2", 10_000_000): (1_438_561_280, "profiles/eval_traffic_config2_10Mpairs.md"),
+}
 
 
 def rank_seed(base: int, rank: int) -> int:
@@ -145,23 +153,29 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
+        self.rows = []
         if self.proc is not None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        if self.file is not None:
+            # read the samples and remove the temporary file here, so no exit path leaves it behind
+            try:
+                self.file.flush()
+                with open(self.file.name) as f:
+                    self.rows = [r.strip().split(",") for r in f if r.strip()]
+            finally:
+                self.file.close()
+                os.unlink(self.file.name)
 
     def summary(self):
         if self.proc is None or self.file is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.file.flush()
-        with open(self.file.name) as f:
-            rows = [r.strip().split(",") for r in f if r.strip()]
-        os.unlink(self.file.name)
         sm, smax, reasons = [], [], set()
         names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
+        for r in self.rows:
             r = [x.strip() for x in r]
             if len(r) < 9:
                 continue
@@ -322,11 +336,11 @@ def qmc_leg(args, rank, world, local_rank, dist):
            "timing": "CUDA events around the graph launches of the timed report blocks (max over ranks)"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = qmc_cpu_baseline(system, basis, c0, refs, q, float(rep["shift"][-1]))
-    if args.qmc_compare_reports > 0:
-        n = args.qmc_compare_reports
-        out["generators"] = compare_generators(q, n, epochs=args.qmc_train_epochs,
-                                               harvest_reports=max(1, min(200, n // 10)))
     q.close()
+    if args.qmc_seeds > 0:
+        out["generators"] = compare_generators(w, c0, refs, float(er[0]), walkers, args.qmc_seeds, rank,
+                                               epochs=args.qmc_train_epochs, max_seconds=args.qmc_max_seconds,
+                                               equil=args.qmc_equil)
     w.close()
     return out
 
@@ -484,61 +498,102 @@ def snoci_leg(args, rank, world, local_rank, dist):
             "timing": "host clock around each step (device work synchronised by its result copies)"}
 
 
-def blocking_error(x):
-    """Standard error of the mean of a correlated series: the largest of the naive errors
-    over successive pairwise blockings (Flyvbjerg-Petersen) with at least 16 blocks left."""
+def blocking_levels(x):
+    """Flyvbjerg-Petersen blocking of a correlated series: (blocks, standard error of the mean)
+    at each pairwise blocking level with at least 16 blocks left."""
     x = np.asarray(x, np.float64)
-    best = 0.0
+    out = []
     while x.shape[0] >= 16:
-        best = max(best, float(x.std(ddof=1) / np.sqrt(x.shape[0])))
+        out.append((int(x.shape[0]), float(x.std(ddof=1) / np.sqrt(x.shape[0]))))
         n = x.shape[0] // 2 * 2
         x = 0.5 * (x[0:n:2] + x[1:n:2])
-    return best
-
-
-def compare_generators(q, nreports, target=1e-4, epochs=2, harvest_reports=200):
-    """Wall time to a 0.1 mEh projected-energy error bar, uniform generator vs the learned
-    proposal, each over `nreports` report blocks (2x10^4 steps by default) from the equilibrated
-    state of the steps/s run.  Uniform arm: all blocks with the uniform generator.  Learned arm:
-    the first `harvest_reports` blocks (2000 steps) run the uniform generator while attempts are
-    harvested (thinned at random to fit the 4.2M-sample buffer), the proposal is trained on the
-    GPU, and the remaining blocks use the learned mixture.  Each arm's error bar comes from a
-    blocking analysis of the per-block projected energies of its measured blocks (all blocks
-    for the uniform arm, the learned blocks for the learned arm); the time to `target` scales
-    the measured blocks' device time by (error / target)^2, plus, for the learned arm, the
-    harvest blocks and the training."""
-    def stats(rep, ms):
-        e = rep["eproj_num"] / rep["eproj_den"]
-        err = blocking_error(e)
-        return {"reports": int(rep.shape[0]), "steps": int(rep.shape[0] * 10), "device_ms": ms,
-                "eproj": float(rep["eproj_num"].sum() / rep["eproj_den"].sum()), "error_bar": err,
-                "attempts_per_step": float(rep["nattempts"].mean() / 10), "walkers_mean": float(rep["nw"].mean()),
-                "shift_mean": float(rep["shift"].mean()), "seconds_to_0.1mEh": ms / 1e3 * (err / target) ** 2}
-    rep = q.run(nreports)
-    out = {"uniform": stats(rep, q.last_run_ms())}
-    attempts_per_report = float(rep["nattempts"].mean())
-    keep = min(1.0, 4_194_304 / max(1.0, attempts_per_report * harvest_reports))
-    q.harvest(True, keep)
-    rep_h = q.run(harvest_reports)
-    harvest_ms = q.last_run_ms()
-    q.harvest(False)
-    t0 = time.perf_counter()
-    tr = q.train_proposal(epochs=epochs, batch=4096, lr=1e-3, seed=5)
-    train_s = time.perf_counter() - t0
-    q.set_generator(True, 0.1)
-    rep_l = q.run(nreports - harvest_reports)
-    lr_ = stats(rep_l, q.last_run_ms())
-    q.set_generator(False, 0.1)
-    lr_.update({"harvest_reports": int(harvest_reports), "harvest_keep_probability": keep,
-                "harvest_device_ms": harvest_ms, "train_seconds": train_s,
-                "training": {k: (float(v) if isinstance(v, float) else int(v)) for k, v in tr.items()},
-                "mix": 0.1})
-    lr_["seconds_to_0.1mEh_incl_harvest_training"] = lr_["seconds_to_0.1mEh"] + harvest_ms / 1e3 + train_s
-    out["learned"] = lr_
-    out["speedup_to_0.1mEh"] = out["uniform"]["seconds_to_0.1mEh"] / lr_["seconds_to_0.1mEh_incl_harvest_training"]
-    out["note"] = ("same walker state at the start of each arm; time to a 0.1 mEh error bar = the measured blocks' "
-                   "device time x (blocking error / 1e-4)^2 (+ harvest blocks and training for the learned arm)")
     return out
+
+
+def blocking_error(x):
+    """Error bar of the mean: the largest blocked standard error, and whether the estimate has
+    reached a plateau (the deepest level agrees with the largest within the statistical
+    uncertainty of a blocked error, err / sqrt(2 (blocks - 1)), twice over)."""
+    lv = blocking_levels(x)
+    if not lv:
+        return float("inf"), False
+    best = max(e for _, e in lv)
+    nb, last = lv[-1]
+    plateau = len(lv) >= 3 and best - last <= 2.0 * last / np.sqrt(2.0 * (nb - 1))
+    return best, bool(plateau)
+
+
+def run_to_target(q, target, chunk_reports=100, min_reports=200, max_seconds=30.0):
+    """Run report blocks (10 steps each) until the blocking error of the projected energy over
+    the measured blocks is at most `target` at a plateau, or the device time reaches
+    max_seconds.  Returns the measured statistics; time is measured, not extrapolated."""
+    import time as _t
+    reps, dev_ms, wall = [], 0.0, 0.0
+    while True:
+        t0 = _t.perf_counter()
+        reps.append(q.run(chunk_reports))
+        wall += _t.perf_counter() - t0
+        dev_ms += q.last_run_ms()
+        rep = np.concatenate(reps)
+        e = rep["eproj_num"] / rep["eproj_den"]
+        err, plateau = blocking_error(e)
+        reached = rep.shape[0] >= min_reports and err <= target and plateau
+        if reached or dev_ms / 1e3 >= max_seconds:
+            return {"reached": bool(reached), "reports": int(rep.shape[0]), "steps": int(rep.shape[0] * 10),
+                    "device_s": dev_ms / 1e3, "wall_s": wall, "error_bar": err, "plateau": plateau,
+                    "eproj": float(rep["eproj_num"].sum() / rep["eproj_den"].sum()),
+                    "walkers_mean": float(rep["nw"].mean()), "attempts_per_step": float(rep["nattempts"].mean() / 10),
+                    "shift_mean": float(rep["shift"].mean())}
+
+
+def compare_generators(w, c0, refs, e_ref, walkers, seeds, rank, target=1e-4, epochs=2, harvest_reports=200,
+                       max_seconds=30.0, equil=40):
+    """Wall time to a 0.1 mEh projected-energy error bar, uniform generator vs the learned
+    proposal, measured for `seeds` independent runs of each arm (no extrapolation).  Each run
+    starts from the references, equilibrates `equil` report blocks with the uniform generator,
+    and then (learned arm) harvests attempts over `harvest_reports` blocks (2000 steps) with
+    the uniform generator, trains the proposal on the GPU and switches to the learned mixture
+    (uniform weight 0.1); both arms then run 100-block chunks until the blocking error of the
+    measured blocks is at most `target` at a plateau (at least 200 blocks), or until
+    `max_seconds` of device time.  The learned arm's time includes harvest and training."""
+    import nociwick
+    arms = {"uniform": [], "learned": []}
+    for k in range(seeds):
+        for arm in ("uniform", "learned"):
+            q = nociwick.Qmc(w, c0, refs, dt=1e-3, initial_population=walkers, target_population=walkers,
+                             shift_damping=0.5, initial_shift=e_ref, ncycles=10, propagator="unshifted",
+                             seed=rank_seed(9000 + 17 * k, rank), max_attempts=48_000_000)
+            q.run(equil)
+            extra = 0.0
+            info = {"seed": 9000 + 17 * k}
+            if arm == "learned":
+                t0 = time.perf_counter()
+                probe = q.run(20)
+                keep = min(1.0, 4_194_304 / max(1.0, float(probe["nattempts"].mean()) * harvest_reports))
+                q.harvest(True, keep)
+                q.run(harvest_reports)
+                q.harvest(False)
+                tr = q.train_proposal(epochs=epochs, batch=4096, lr=1e-3, seed=5 + k)
+                q.set_generator(True, 0.1)
+                extra = time.perf_counter() - t0
+                info.update({"harvest_and_training_s": extra, "harvest_keep_probability": keep,
+                             "training_loss": [float(tr["loss_first"]), float(tr["loss_last"])]})
+            r = run_to_target(q, target, max_seconds=max_seconds)
+            r.update(info)
+            r["seconds_to_0.1mEh"] = r["wall_s"] + extra
+            arms[arm].append(r)
+            q.close()
+    summary = {}
+    for arm, runs in arms.items():
+        t = np.array([r["seconds_to_0.1mEh"] for r in runs])
+        summary[arm] = {"mean_s": float(t.mean()), "min_s": float(t.min()), "max_s": float(t.max()),
+                        "reached": int(sum(r["reached"] for r in runs)), "runs": len(runs),
+                        "walkers": float(np.mean([r["walkers_mean"] for r in runs]))}
+    summary["speedup_mean"] = summary["uniform"]["mean_s"] / max(summary["learned"]["mean_s"], 1e-9)
+    return {"target_eh": target, "seeds": seeds, "runs": arms, "summary": summary,
+            "note": "measured wall time (host clock around the graph launches, plus harvest and training for the "
+                    "learned arm) until the blocking error of the measured blocks is at most 1e-4 Eh at a plateau; "
+                    "a run that hits the device-time cap reports reached = false and its time at the cap"}
 
 
 def qmc_cpu_baseline(system, basis, c0, refs, q, shift):
@@ -564,17 +619,18 @@ def qmc_cpu_baseline(system, basis, c0, refs, q, shift):
                       f"numpy restatement of walkers.rs with the C++ FP64 pair evaluator, {cores} threads"}
 
 
-def run_ours(args, rank, world, local_rank):
+def hs_leg(args, name, npairs, rank, world, local_rank, dist):
+    """One H/S workload: build, autotune, device-resident throughput (CUDA events on the
+    launching stream, max over ranks), evaluator-phase timing for the roofline, and the
+    end-to-end rate through the host-buffer C ABI call with pinned buffers."""
     import torch
     import nociwick
-    dist = None
-    if world > 1:
-        import torch.distributed as dist  # noqa: F811
     torch.cuda.set_device(local_rank)
-    system, basis, pairs, cfg = workload(args.workload, args.npairs, rank, args.nmo)
+    system, basis, pairs, cfg = workload(name, npairs, rank, args.nmo)
     npairs = pairs.shape[0]
     eng = nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8,
                                device=local_rank)
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     eng.build()
     build_s = time.perf_counter() - t0
@@ -620,11 +676,12 @@ def run_ours(args, rank, world, local_rank):
             step_device()
         ev1.record(stream)
         torch.cuda.synchronize()
+    clocks = clk.summary()
     barrier()
     t_dev = ev0.elapsed_time(ev1)
     eng.sync(sh)
     # evaluator-phase timing for the roofline (CUDA events recorded inside the library on the
-    # launching stream)
+    # launching stream, and on the forked stream of the m > 0 evaluator)
     eng.set_timing(True)
     phases = []
     for _ in range(min(args.steps, 10)):
@@ -660,64 +717,172 @@ def run_ours(args, rank, world, local_rank):
     t_dev, t_e2e = reduce_max([t_dev, t_e2e], dist, f"cuda:{local_rank}")
     hs_host = dout.cpu().numpy() if rank == 0 and world == 1 and not args.no_cpu_baseline else None
     eng.close()
-    # every rank runs the QMC leg (it has collectives); rank 0 reports
-    qmc = None if args.no_qmc else qmc_leg(args, rank, world, local_rank, dist)
-    pt2 = None if args.no_pt2 else pt2_leg(args, rank, world, local_rank, dist)
-    snoci_out = None if args.no_snoci else snoci_leg(args, rank, world, local_rank, dist)
-    if rank != 0:
-        return
+    del dpairs, dout, hpairs, hout
+    torch.cuda.empty_cache()
+
     value = aggregate_rate(npairs, world, args.steps, t_dev)
     e2e = aggregate_rate(npairs, world, args.steps, t_e2e)
-    ev_ms = statistics.median([p["eval_m0"] + p["eval_gen"] for p in phases])
+    ev_ms = statistics.median([p["eval_m0"] for p in phases])
+    gen_ms = statistics.median([p["eval_gen"] for p in phases])
     phase_ms = {k: statistics.median([p[k] for p in phases]) for k in phases[0]}
     alg_bytes = algorithmic_bytes(basis, pairs)
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (ev_ms / 1e3) / 1e9
-    # DRAM bytes (read + write) of one step's evaluator launches, measured by ncu on this
-    # default workload (profiles/eval_traffic_config2_10Mpairs.md); other workloads: not captured
-    traffic, traffic_src = None, None
-    if args.workload == "config2" and npairs == 10_000_000:
-        traffic = EVAL_TRAFFIC_CONFIG2_10M
-        traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one step's evaluator launches, " \
-                      "profiles/eval_traffic_config2_10Mpairs.md"
-    clocks = clk.summary()
+    traffic, traffic_src = EVAL_TRAFFIC.get((name, npairs), (None, None))
     # classify, the two scan kernels (tile sums, tile scans), scatter, then the light / medium /
     # heavy / runtime-rank evaluator kernels and, when some reference pair has zero-overlap
     # orbital pairs, the generic evaluator; the end-to-end call runs them once per pipeline chunk
     kernels_per_step = 4 + (4 if info["ngeneric"] < info["nref"] ** 2 else 0) + (1 if info["ngeneric"] > 0 else 0)
     chunk = max(PIPE_MIN_CHUNK, ((npairs + PIPE_CHUNKS - 1) // PIPE_CHUNKS + 255) // 256 * 256)
     e2e_chunks = (npairs + chunk - 1) // chunk
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": max(3, args.warmup), "ms_per_step": t_dev / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+    bound = aggregate_rate(npairs, world, 1, max(h2d_ms[0], d2h_ms[0], t_dev / args.steps))
+    out = {
+        "value": value, "ms_per_step": t_dev / args.steps,
         "config": dict(cfg, l2="inputs larger than L2: pairs %d MB + results %d MB + intermediates %d MB per step"
                        % (npairs * 8 >> 20, npairs * 16 >> 20, info["slab_bytes"] >> 20),
                        build_seconds=round(build_s, 3), parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": npairs * 8, "d2h_bytes_per_step": npairs * 16,
                 "gpu_launches": kernels_per_step * e2e_chunks * args.steps,
                 "link": {"h2d_gbs": npairs * 8 / h2d_ms[0] / 1e6, "d2h_gbs": npairs * 16 / d2h_ms[0] / 1e6,
-                         "bound_value": aggregate_rate(npairs, world, 1, max(h2d_ms[0], d2h_ms[0], t_dev / args.steps)),
-                         "frac": e2e / aggregate_rate(npairs, world, 1, max(h2d_ms[0], d2h_ms[0], t_dev / args.steps)),
+                         "bound_value": bound, "frac": e2e / bound,
                          "note": "pinned copies of one step's buffers timed alone; bound = pairs / max(H2D, D2H, "
                                  "device step)"}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "traffic_source": traffic_src,
                      "kernel": "evaluator phase (eval_light/medium/heavy/rt kernels + eval_gen_kernel)",
                      "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_step": alg_bytes,
-                     "eval_ms": ev_ms, "phase_ms": phase_ms},
+                     "bytes_formula": "B(La,Lb) = 8[2(La^2+Lb^2) + 2C(La,2)^2 + 2C(Lb,2)^2 + La^2 Lb^2] + 60 per pair "
+                                      "(m > 0 pairs counted with the m = 0 bytes of their ranks: a lower bound)",
+                     "eval_ms": ev_ms, "eval_gen_ms": gen_ms, "phase_ms": phase_ms},
         "clocks": clocks,
         "gpu_launches": kernels_per_step * args.steps,
         "autotune": tune,
     }
-    if qmc is not None:
-        line["qmc"] = qmc
+    return out, (system, basis, pairs, hs_host, info)
+
+
+def config3_check(system, basis, pairs, gpu_hs, seconds: float, ngroups: int = 12, min_pairs: int = 1_000_000):
+    """Element error of the config-3 GPU results against the FP64 oracle and the CPU rate, on a
+    bounded sample: every reference-pair group with zero-overlap orbitals plus seeded m = 0
+    groups (ngroups in all), at least min_pairs pairs.  The oracle's intermediates of all 64
+    reference pairs (n = 64) would need tens of GB of host memory, so it builds one group at a
+    time."""
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import Oracle
+    nref = len(system.refs)
+    par = basis["parent"].astype(np.int64)
+    grp = par[pairs[:, 0]] * nref + par[pairs[:, 1]]
+    smin = reference_pair_conditioning(system)
+    gen = [g for g in range(nref * nref) if g in set(x * nref + w for (x, w, _, _) in system.zero_pairs) |
+           set(w * nref + x for (x, w, _, _) in system.zero_pairs)]
+    rng = np.random.default_rng(31)
+    others = [g for g in rng.permutation(nref * nref).tolist() if g not in gen and g // nref != g % nref]
+    groups = (gen + others)[:ngroups]
+    per_group = max(1, min_pairs // len(groups) + 1)
+    cores = os.cpu_count() or 1
+    dh_all, ds_all, cond_all = [], [], []
+    cpu_pairs, cpu_s, build_s = 0, 0.0, 0.0
+    for g in groups:
+        sel = np.nonzero(grp == g)[0][:per_group]
+        if sel.size == 0:
+            continue
+        t0 = time.perf_counter()
+        orc = Oracle.from_system(system, tol=1e-8, with_mo_cache=False, only_pairs={g})
+        ob = orc.oracle_basis(basis)
+        build_s += time.perf_counter() - t0
+        t0 = time.perf_counter()
+        h, s = orc.eval_pairs(ob, pairs[sel].astype(np.int64), nthreads=cores)
+        cpu_s += time.perf_counter() - t0
+        cpu_pairs += sel.size
+        dh_all.append(np.abs(gpu_hs[sel, 0] - h))
+        ds_all.append(np.abs(gpu_hs[sel, 1] - s))
+        cond_all.append(np.full(sel.size, smin[g]))
+        del orc, ob
+    dh, ds, cond = np.concatenate(dh_all), np.concatenate(ds_all), np.concatenate(cond_all)
+    buckets = {}
+    for nm, sel in (("s_min>=1e-2", cond >= 1e-2), ("1e-3<=s_min<1e-2", (cond >= 1e-3) & (cond < 1e-2)),
+                    ("s_min<1e-3", cond < 1e-3)):
+        if sel.any():
+            buckets[nm] = {"pairs": int(sel.sum()), "max_abs_err_h": float(dh[sel].max()),
+                           "rms_abs_err_h": float(np.sqrt(np.mean(dh[sel] ** 2))),
+                           "max_abs_err_s": float(ds[sel].max())}
+    return {"checked_pairs": int(dh.size), "groups": [[int(g // nref), int(g % nref)] for g in groups],
+            "max_abs_err_h": float(dh.max()), "rms_abs_err_h": float(np.sqrt(np.mean(dh ** 2))),
+            "max_abs_err_s": float(ds.max()), "err_by_reference_pair_conditioning": buckets,
+            "oracle_build_seconds": build_s,
+            "cpu_baseline": {"value": cpu_pairs / max(cpu_s, 1e-9), "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{cpu_pairs} pairs of {len(groups)} of the {nref * nref} reference-pair groups "
+                                       f"({cpu_s:.1f} s of CPU work, C++ FP64 restatement, {cores} threads)"}}
+
+
+def tail_summary(line):
+    """The figures a reader of the end of the output needs, in a few hundred bytes."""
+    out = {"hs_config2": {"value": line["value"], "e2e": line["e2e"]["value"], "frac": line["roofline"]["frac"]}}
+    c3 = line.get("config3")
+    if c3:
+        out["hs_config3"] = {"value": c3["value"], "e2e": c3["e2e"]["value"], "frac": c3["roofline"]["frac"],
+                             "eval_gen_ms": c3["roofline"]["eval_gen_ms"], "eval_ms": c3["roofline"]["eval_ms"]}
+        chk = c3.get("oracle_check")
+        if chk:
+            out["hs_config3"].update({"checked": chk["checked_pairs"], "max_err_h": chk["max_abs_err_h"],
+                                      "rms_err_h": chk["rms_abs_err_h"], "cpu": chk["cpu_baseline"]["value"]})
+    q = line.get("qmc")
+    if q:
+        out["qmc"] = {"steps_per_s": q["value"], "walkers": q["walkers_mean"]}
+        if "cpu_baseline" in q:
+            out["qmc"]["cpu_steps_per_s"] = q["cpu_baseline"]["value"]
+        g = q.get("generators")
+        if g:
+            sm = g["summary"]
+            out["qmc"]["to_0.1mEh_s"] = {"uniform": sm["uniform"]["mean_s"], "learned": sm["learned"]["mean_s"],
+                                         "reached": [sm["uniform"]["reached"], sm["learned"]["reached"]],
+                                         "seeds": g["seeds"]}
+    return out
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+    torch.cuda.set_device(local_rank)
+    main, (system, basis, pairs, hs_host, _) = hs_leg(args, args.workload, args.npairs, rank, world, local_rank,
+                                                      dist)
+    cpu = None
+    if hs_host is not None:
+        cpu = cpu_baseline(system, basis, pairs, args.cpu_seconds, gpu_hs=hs_host)
+    del system, basis, pairs, hs_host
+    # every rank runs the other legs (they have collectives); rank 0 reports
+    pt2 = None if args.no_pt2 else pt2_leg(args, rank, world, local_rank, dist)
+    snoci_out = None if args.no_snoci else snoci_leg(args, rank, world, local_rank, dist)
+    c3 = None
+    if not args.no_config3 and args.workload != "config3":
+        c3, (system, basis, pairs, hs_host, _) = hs_leg(args, "config3", args.config3_npairs, rank, world,
+                                                        local_rank, dist)
+        if hs_host is not None:
+            c3["oracle_check"] = config3_check(system, basis, pairs, hs_host, args.cpu_seconds)
+        del system, basis, pairs, hs_host
+    qmc = None if args.no_qmc else qmc_leg(args, rank, world, local_rank, dist)
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": main["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": main["config"], "e2e": main["e2e"], "roofline": main["roofline"], "clocks": main["clocks"],
+        "gpu_launches": main["gpu_launches"], "autotune": main["autotune"],
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
     if pt2 is not None:
         line["pt2"] = pt2
     if snoci_out is not None:
         line["snoci"] = snoci_out
-    if hs_host is not None:
-        line["cpu_baseline"] = cpu_baseline(system, basis, pairs, args.cpu_seconds, gpu_hs=hs_host)
+    if c3 is not None:
+        line["config3"] = dict(c3, metric=METRIC, unit=UNIT, dtype="f64")
+    if qmc is not None:
+        line["qmc"] = qmc
+    line["tail_summary"] = tail_summary(line)
     print(json.dumps(line), flush=True)
 
 

@@ -405,7 +405,8 @@ NW_API nw_status nw_autotune(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs
 /* Per-phase device times of the most recent nw_eval_hs_pairs* call, measured with CUDA events
  * recorded on its stream while timing is enabled: ms[0] classify, ms[1] scan, ms[2] scatter,
  * ms[3] the evaluators (the m = 0 classes and the m > 0 generic evaluator run concurrently on
- * forked streams, so they are timed together), ms[4] 0.  nw_last_timings waits for that call. */
+ * forked streams, so they are timed together), ms[4] the m > 0 generic evaluator alone (events
+ * on its forked stream; 0 when the call had no such pair).  nw_last_timings waits for that call. */
 NW_API nw_status nw_set_timing(nw_ctx* ctx, int enable);
 NW_API nw_status nw_last_timings(nw_ctx* ctx, float* ms);
 

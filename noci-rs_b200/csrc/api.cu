@@ -385,7 +385,7 @@ nw_status nw_set_timing(nw_ctx* ctx, int enable) {
   if (!ctx) return NW_ERR_INVALID;
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
   if (enable && !ctx->ev[0]) {
-    for (int i = 0; i < 6; ++i) NW_CUDA(ctx, cudaEventCreate(&ctx->ev[i]));
+    for (int i = 0; i < 8; ++i) NW_CUDA(ctx, cudaEventCreate(&ctx->ev[i]));
   }
   ctx->timing = enable != 0;
   ctx->timed_valid = false;
@@ -396,7 +396,9 @@ nw_status nw_last_timings(nw_ctx* ctx, float* ms) {
   if (!ctx || !ms) return NW_ERR_INVALID;
   if (!ctx->timed_valid) return nw::fail(ctx, NW_ERR_STATE, "no timed evaluation recorded");
   NW_CUDA(ctx, cudaEventSynchronize(ctx->ev[5]));
-  for (int i = 0; i < 5; ++i) NW_CUDA(ctx, cudaEventElapsedTime(&ms[i], ctx->ev[i], ctx->ev[i + 1]));
+  for (int i = 0; i < 4; ++i) NW_CUDA(ctx, cudaEventElapsedTime(&ms[i], ctx->ev[i], ctx->ev[i + 1]));
+  ms[4] = 0.0f;
+  if (ctx->timed_gen) NW_CUDA(ctx, cudaEventElapsedTime(&ms[4], ctx->ev[6], ctx->ev[7]));
   return NW_OK;
 }
 
@@ -436,7 +438,7 @@ nw_status nw_ctx_destroy(nw_ctx* ctx) {
   free_buf(ctx->io_pairs);
   free_buf(ctx->io_hs);
   if (ctx->h_flag) cudaFreeHost(ctx->h_flag);
-  for (int i = 0; i < 6; ++i)
+  for (int i = 0; i < 8; ++i)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
   for (cudaStream_t q : {ctx->s_in, ctx->s_comp, ctx->s_out, ctx->s_aux[0], ctx->s_aux[1], ctx->s_aux[2]})
     if (q) cudaStreamDestroy(q);

@@ -516,7 +516,8 @@ nw_status scan_exclusive(nw_ctx* ctx, const uint32_t* counts, uint64_t n, uint32
 }
 
 // classify -> scan -> scatter -> evaluate, all on `stream`.  The flag must already be cleared
-// (or hold earlier calls' reports); ev (six events or null) brackets the phases.
+// (or hold earlier calls' reports); ev (eight events or null) brackets the phases: ev[0..5] on
+// `stream`, ev[6] / ev[7] around the m > 0 evaluator on its forked stream.
 nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const uint32_t* pairs, uint64_t npairs,
                         double* out, const SortScratch& S, cudaStream_t stream, cudaEvent_t* ev, EvalMode mode,
                         const uint32_t* npairs_dev, bool classified) {
@@ -560,12 +561,15 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
   }
   if (gen) {
     NW_CUDA(ctx, cudaMemsetAsync(S.work, 0, sizeof(uint32_t), ctx->s_aux[2]));
+    if (ev) NW_CUDA(ctx, cudaEventRecord(ev[6], ctx->s_aux[2]));
     if (mode == EvalMode::kFS)
       eval_fs_gen_kernel<<<148 * 4, 128, 0, ctx->s_aux[2]>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out, S.work);
     else
       eval_gen_kernel<<<148 * 4, 128, 0, ctx->s_aux[2]>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out, S.work);
     NW_CUDA(ctx, cudaGetLastError());
+    if (ev) NW_CUDA(ctx, cudaEventRecord(ev[7], ctx->s_aux[2]));
   }
+  if (ev) ctx->timed_gen = gen;
   for (int i = 0; i < 3; ++i) {
     NW_CUDA(ctx, cudaEventRecord(ctx->ev_join[i], ctx->s_aux[i]));
     NW_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->ev_join[i], 0));
@@ -700,7 +704,12 @@ nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs
   if (npairs == 0) return NW_OK;
   EvalParams P = make_params(ctx);
   const uint64_t ngen = (uint64_t)ctx->nref * ctx->nref - (uint64_t)ctx->nfast;
-  const uint64_t fast_cap = std::min(kNoallocMaxKeys - (uint64_t)kGenClasses * ngen, std::max(kFineMin, npairs));
+  // the same fine-key budget as the allocating path (nw_autotune's choice when there is one),
+  // clamped to the keys the fixed array holds
+  const uint64_t budget =
+      ctx->tune_keys_per_pair > 0.0 ? (uint64_t)(ctx->tune_keys_per_pair * (double)npairs) : std::max(kFineMin, npairs);
+  const uint64_t fast_cap = std::min(kNoallocMaxKeys - (uint64_t)kGenClasses * ngen,
+                                     std::min(kFineMax, std::max(kFineMin, budget)));
   const uint64_t nkeys = plan_keys(ctx, P, fast_cap);
   if (nkeys > kNoallocMaxKeys) return fail(ctx, NW_ERR_UNSUPPORTED, "sort keys exceed the allocation-free scratch");
   SortScratch S;

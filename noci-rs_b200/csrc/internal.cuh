@@ -109,7 +109,10 @@ struct nw_ctx {
   int live_qmc = 0;                 // QMC objects evaluating against the resident basis
   int tune_per_sm = 0;            // blocks per SM of classify / scatter / light evaluator
   bool timed_valid = false;
-  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool timed_gen = false;           // the last timed call ran the m > 0 evaluator (ev[6], ev[7])
+  // phase events: ev[0..5] on the launching stream, ev[6] / ev[7] around the m > 0 evaluator on
+  // its forked stream
+  cudaEvent_t ev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace nw {
@@ -163,7 +166,7 @@ EvalParams make_params(const nw_ctx* ctx);
 uint64_t plan_keys(const nw_ctx* ctx, EvalParams& P, uint64_t cap);
 // classify -> scan -> scatter -> evaluate on `stream` (no allocation, no host synchronisation).
 // With npairs_dev the number of pairs is read on the device (at most npairs, the capacity the
-// launch is sized for); ev (six events or null) brackets the phases.  With classified the
+// launch is sized for); ev (eight events or null) brackets the phases.  With classified the
 // caller has already cleared S.counts and written S.keys / S.ranks (and the outputs of
 // skipped pairs), e.g. the fused QMC spawn kernel, and the pipeline starts at the scan.
 nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const uint32_t* pairs, uint64_t npairs,

@@ -52,6 +52,10 @@ struct QmcState {
   uint32_t overflow;   // a cycle needed more attempts than the buffers hold
   int32_t reached;
   int32_t pad;
+  // 64-bit sum of the current cycle's attempts, added up by the sample kernel (the 32-bit
+  // per-determinant counts and their scan would wrap beyond 2^32 - 1), read and cleared by the
+  // count kernel
+  unsigned long long cycle_total;
 };
 
 struct QmcParams {
@@ -112,11 +116,12 @@ T* dalloc(size_t count, bool* ok) {
   return static_cast<T*>(p);
 }
 
-__global__ void qmc_sample_kernel(QmcParams q, const QmcState* __restrict__ st, const double* __restrict__ pop,
+__global__ void qmc_sample_kernel(QmcParams q, QmcState* __restrict__ st, const double* __restrict__ pop,
                                   const double2* __restrict__ diag, double* __restrict__ sampled,
                                   uint32_t* __restrict__ na, double* __restrict__ delta) {
   const uint64_t cycle = st->cycle;
   const double es = st->shift;
+  unsigned long long sum = 0ull;
   for (uint64_t d = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; d < q.ndet; d += (uint64_t)gridDim.x * blockDim.x) {
     const double p = pop[d];
     double n = 0.0;
@@ -124,17 +129,25 @@ __global__ void qmc_sample_kernel(QmcParams q, const QmcState* __restrict__ st, 
     sampled[d] = n;
     const uint64_t a = nwq::attempts(n);
     na[d] = a > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)a;
+    sum += a;
     if (n != 0.0) {
       const double2 hs = diag[d];
       delta[d] += nwq::diagonal_change(q.prop, q.dt, es, hs.x, hs.y, n);
     }
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xFFFFFFFFu, sum, o);
+  if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&st->cycle_total, sum);
 }
 
+// The 32-bit attempt offsets are valid only while the cycle's 64-bit total fits the buffers
+// (cap < 2^32); otherwise the cycle is flagged and the run fails on the host.
 __global__ void qmc_count_kernel(QmcParams q, QmcState* __restrict__ st, const uint32_t* __restrict__ off) {
-  const uint64_t total = off[q.ndet];
+  const unsigned long long total64 = st->cycle_total;
+  st->cycle_total = 0ull;
+  const uint64_t total = total64 <= q.cap ? (uint64_t)off[q.ndet] : (uint64_t)total64;
   const uint64_t held = total < q.cap ? total : q.cap;
-  if (total > q.cap) st->overflow = 1;
+  if (total64 > q.cap) st->overflow = 1;
   st->npairs = (uint32_t)held;
   st->attempts += total;
 }

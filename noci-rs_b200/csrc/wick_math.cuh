@@ -422,8 +422,6 @@ NW_HD bool advance_combination(int l, int m, uint64_t* x) {
 NW_HD void jslot_hd(int mi, int mj, int mk, int ml, int* slot, bool* swap) {
   const int key = (mi << 3) | (mj << 2) | (mk << 1) | ml;
   // (slot, swap) for the 16 binary assignments, SAME_SPIN_J_BRANCHES order (helpers.rs:165-191)
-  const int slots = 0;
-  (void)slots;
   int s = 0;
   bool w = false;
   switch (key) {

@@ -11,10 +11,12 @@ Reference files restated here (paths inside dy-cl/noci-rs):
   * src/lib.rs:114-167                ``ExcitationSpin::cache`` / ``ExcitationSpinCache``
   * src/lib.rs:230-266                ``ReducedTwoSpinDetState`` (phase = pha * phb)
 
-Parity status: the reference is Rust and cannot be compiled in this image, and its only
-golden data for this path are whole-pipeline energies that need PySCF integrals, so parity
-of this oracle against reference-produced numbers is unpinned; it is cross-checked against
-an independent generalised Slater-Condon path and a brute-force Fock-space evaluation.
+Parity status: pinned against reference-produced numbers.  The reference's own energy
+fixtures (tests/fixtures/*/expected.json of noci-rs: reference-space NOCI, deterministic
+SD-space, NOCI-PT2 and selected-NOCI energies of H2, H4, LiH and F2) are reproduced from
+integrals and SCF states rebuilt by tests/golden/make_reference_fixtures.py
+(tests/test_reference_fixtures.py); the oracle is also cross-checked against an independent
+generalised Slater-Condon path and a brute-force Fock-space evaluation.
 """
 from __future__ import annotations
 

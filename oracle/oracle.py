@@ -5,7 +5,12 @@ src/nonorthogonalwicks/layout.rs and calls the C++ evaluators of ``wick_eval.cpp
 ctypes.  Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of bench.py may
 use this module; the product library under noci-rs_b200/ never imports or links it.
 
-Parity status: unpinned against reference-produced numbers (see wick_build.py).
+Parity status: pinned against reference-produced numbers.  The reference's own energy
+fixtures (tests/fixtures/*/expected.json of noci-rs: reference-space NOCI, deterministic
+SD-space, NOCI-PT2 and selected-NOCI energies of H2, H4, LiH and F2) are reproduced from
+integrals and SCF states rebuilt by tests/golden/make_reference_fixtures.py
+(tests/test_reference_fixtures.py); the oracle is also cross-checked against an independent
+generalised Slater-Condon path and a brute-force Fock-space evaluation.
 """
 from __future__ import annotations
 
@@ -104,6 +109,9 @@ def pack_pairs(builds: Sequence[_wb.PairBuild], nmo: int, writer: Optional[_Slab
     vals = np.zeros((npair, nval))
     ints = np.zeros((npair, nint), np.int32)
     for p, b in enumerate(builds):
+        ints[p, 4] = nmo
+        if b is None:  # not built (Oracle.create with only_pairs): offsets stay -1
+            continue
         k = 0
         for s, (ss, hcol0) in enumerate(((b.aa, b.hcol0_a), (b.bb, b.hcol0_b))):
             for i in range(2):
@@ -143,7 +151,6 @@ def pack_pairs(builds: Sequence[_wb.PairBuild], nmo: int, writer: Optional[_Slab
                         offs[p, k] = w.put(b.ab.ii.get((a, bb, c, d))); k += 1
         vals[p, 14:18] = np.array(b.ab.vab0).ravel()
         vals[p, 18:22] = np.array(b.ab.vba0).ravel()
-        ints[p, 4] = nmo
     return w, offs, vals, ints
 
 
@@ -212,13 +219,17 @@ class Oracle:
     nmo: int
 
     @classmethod
-    def from_system(cls, sysm, tol: float = 1e-8, with_mo_cache: bool = True, null_gauge=None):
+    def from_system(cls, sysm, tol: float = 1e-8, with_mo_cache: bool = True, null_gauge=None,
+                    only_pairs=None):
         return cls.create(sysm.s, sysm.h, sysm.eri, sysm.enuc, sysm.refs, tol, with_mo_cache,
-                          null_gauge)
+                          null_gauge, only_pairs)
 
     @classmethod
-    def create(cls, s, h, eri, enuc, refs, tol=1e-8, with_mo_cache=True, null_gauge=None):
-        builds = _wb.build_all(s, h, eri, refs, tol, null_gauge)
+    def create(cls, s, h, eri, enuc, refs, tol=1e-8, with_mo_cache=True, null_gauge=None,
+               only_pairs=None):
+        """With ``only_pairs`` (ordered-pair indices x * nref + w) only those reference pairs
+        are built; requests may then only name determinants of those parent pairs."""
+        builds = _wb.build_all(s, h, eri, refs, tol, null_gauge, only=only_pairs)
         nmo = refs[0][0].shape[1]
         w, offs, vals, ints = pack_pairs(builds, nmo)
         mo_offs = mo_orth = None

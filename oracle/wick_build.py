@@ -23,8 +23,11 @@ Conventions: AO integrals in chemists' order eri[mu,nu,lam,sig] = (mu nu|lam sig
 (scripts/generate.py:14, PySCF int2e s1).  The ordered pair (x, w) is (bra, ket): the
 reference calls SameSpinBuild::new(ao, g = ref[w], l = ref[x]).
 
-Parity status: unpinned against reference-produced numbers (the Rust reference cannot be
-built here and its fixtures need PySCF); cross-checked by tests against the independent
+Parity status: pinned against reference-produced numbers.  The reference's own energy
+fixtures (tests/fixtures/*/expected.json of noci-rs: reference-space NOCI, deterministic
+SD-space, NOCI-PT2 and selected-NOCI energies of H2, H4, LiH and F2) are reproduced from
+integrals and SCF states rebuilt by tests/golden/make_reference_fixtures.py
+(tests/test_reference_fixtures.py); the oracle is also cross-checked against an independent
 generalised Slater-Condon path and a brute-force Fock-space evaluation.
 """
 from __future__ import annotations
@@ -341,10 +344,16 @@ def zero_count(s_ao, cx, occx, cw, occw, tol) -> int:
     return int(np.sum(np.abs(sv) <= tol))
 
 
-def build_all(s_ao, h, eri, refs, tol: float, null_gauge=None) -> List[PairBuild]:
-    """All nref^2 ordered pairs, index = x * nref + w (src/noci/wicks.rs:159-190)."""
+def build_all(s_ao, h, eri, refs, tol: float, null_gauge=None, only=None) -> List[Optional[PairBuild]]:
+    """All nref^2 ordered pairs, index = x * nref + w (src/noci/wicks.rs:159-190).  With
+    ``only`` (a set of ordered-pair indices) the other entries are None: a checker that
+    evaluates a few reference-pair groups of a large system builds just those."""
     out = []
-    for x in refs:
-        for w in refs:
+    nref = len(refs)
+    for ix, x in enumerate(refs):
+        for iw, w in enumerate(refs):
+            if only is not None and ix * nref + iw not in only:
+                out.append(None)
+                continue
             out.append(build_pair(s_ao, h, eri, x, w, tol, null_gauge))
     return out

@@ -22,9 +22,12 @@
 // The fixed-rank SIMD kernels of the reference are specialisations of the generic evaluators
 // restated here and give the same values up to rounding.
 //
-// Parity status: unpinned against reference-produced numbers (no Rust toolchain or PySCF in
-// this image); cross-checked in tests against generalised Slater-Condon and a brute-force
-// Fock-space evaluation.
+// Parity status: pinned against reference-produced numbers.  The reference's own energy
+// fixtures (tests/fixtures/*/expected.json of noci-rs: reference-space NOCI, deterministic
+// SD-space, NOCI-PT2 and selected-NOCI energies of H2, H4, LiH and F2) are reproduced from
+// integrals and SCF states rebuilt by tests/golden/make_reference_fixtures.py
+// (tests/test_reference_fixtures.py); the oracle is also cross-checked against an independent
+// generalised Slater-Condon path and a brute-force Fock-space evaluation.
 
 #include <algorithm>
 #include <cmath>

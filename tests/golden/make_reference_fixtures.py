@@ -21,8 +21,8 @@ fixture and, where the reference has one, of its ``_WICKS`` twin, which runs the
 through the Wick path) and the options of the fixture's input (excitation orders, snoci
 block).  Tests read only the archive.
 
-Run from the repository root with the reference checked out at /root/reference:
-    python tests/golden/make_reference_fixtures.py
+Run from the repository root, naming the reference checkout's fixture directory:
+    python tests/golden/make_reference_fixtures.py <noci-rs checkout>/tests/fixtures
 """
 import json
 import os
@@ -31,7 +31,6 @@ from math import exp, pi, sqrt
 import numpy as np
 from scipy.special import gamma, gammainc
 
-REF = "/root/reference/tests/fixtures"
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_fixtures.npz")
 BOHR = 0.52917721092
 
@@ -351,12 +350,12 @@ FIXTURES = {
 }
 
 
-def main():
+def main(ref_dir: str):
     arrays, meta = {}, {}
     for name, (basis, geom, recipes, orders, snoci) in FIXTURES.items():
-        with open(os.path.join(REF, name, "expected.json")) as f:
+        with open(os.path.join(ref_dir, name, "expected.json")) as f:
             expected = json.load(f)
-        wicks_path = os.path.join(REF, name + "_WICKS", "expected.json")
+        wicks_path = os.path.join(ref_dir, name + "_WICKS", "expected.json")
         expected_wicks = None
         if os.path.exists(wicks_path):
             with open(wicks_path) as f:
@@ -387,4 +386,7 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    import argparse
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("fixtures", help="tests/fixtures directory of a noci-rs checkout")
+    main(ap.parse_args().fixtures)
