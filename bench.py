@@ -17,7 +17,14 @@ among pairs whose parents differ (seed 12345).  A step evaluates (H, S) for the 
               bounded sample of the same pairs.
 
 ``--impl reference`` times that CPU restatement alone (the reference is Rust and cannot be
-built here; the restatement is the only runnable form of its algorithm).
+built here; the restatement is the only runnable form of its algorithm): the lane-batched
+fixed-rank path of calculate_hs_pairs_wicks_batched, 8 lanes with AVX-512, 4 with AVX2.
+
+Also on the line: ``config3`` (the synthetic n = 64 stress system, 8 references, zero-overlap
+reference pairs, 10^8 pairs: throughput, end to end, roofline, the m > 0 evaluator's time and
+the element error against the FP64 oracle on >= 10^6 pairs), ``pt2``, ``snoci``, ``qmc``
+(NOCI-QMC steps/s and the measured uniform-vs-learned generator comparison) and, last,
+``tail_summary`` with the headline figures of each.
 
 Multi-GPU: one process per GPU under torchrun; each rank evaluates its own 10^7-pair batch
 (no data-path collective, weak scaling); the time is the max over ranks.
@@ -200,26 +207,35 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+CPU_KIND = ("C++ FP64 restatement of the reference's CPU path (calculate_hs_pairs_wicks_batched with the 28 "
+            "(L_alpha, L_beta) bins flushed through lane-batched fixed-rank kernels, {lanes} lanes, generic "
+            "evaluator for the rest; the Rust reference cannot be built here)")
+
+
 def cpu_baseline(system, basis, pairs, seconds: float, gpu_hs=None):
-    """The FP64 CPU restatement of the reference path on every host core, on a bounded sample."""
+    """The reference's CPU path (the lane-batched restatement) on every host core, on a bounded
+    sample; the GPU results are checked against the scalar FP64 oracle on the same sample."""
     sys.path.insert(0, ROOT)
     from oracle.oracle import Oracle
     orc = Oracle.from_system(system, tol=1e-8, with_mo_cache=False)
     ob = orc.oracle_basis(basis)
     cores = os.cpu_count() or 1
-    cal = pairs[:min(pairs.shape[0], 100_000)].astype(np.int64)
+    cal = pairs[:min(pairs.shape[0], 200_000)].astype(np.int64)
+    orc.eval_pairs_binned(ob, cal, nthreads=cores)
     t0 = time.perf_counter()
-    orc.eval_pairs(ob, cal, nthreads=cores)
+    orc.eval_pairs_binned(ob, cal, nthreads=cores)
     rate = cal.shape[0] / max(time.perf_counter() - t0, 1e-6)
     nsample = int(min(pairs.shape[0], max(cal.shape[0], rate * seconds)))
     sample = pairs[:nsample].astype(np.int64)
     t0 = time.perf_counter()
-    h, s = orc.eval_pairs(ob, sample, nthreads=cores)
+    hb, sb, lanes = orc.eval_pairs_binned(ob, sample, nthreads=cores)
     dt = time.perf_counter() - t0
     out = {"value": nsample / dt, "unit": UNIT, "cores": cores, "kind": "port",
-           "sample": f"first {nsample} pairs of the same batch ({dt:.1f} s of CPU work, C++ FP64 restatement "
-                     f"of the reference evaluator, {cores} threads)"}
+           "sample": f"first {nsample} pairs of the same batch ({dt:.1f} s of CPU work, "
+                     + CPU_KIND.format(lanes=lanes) + f", {cores} threads)"}
     if gpu_hs is not None:
+        h, s = orc.eval_pairs(ob, sample, nthreads=cores)
+        out["binned_vs_scalar_oracle_max_abs"] = max(float(np.max(np.abs(hb - h))), float(np.max(np.abs(sb - s))))
         dh = np.abs(gpu_hs[:nsample, 0] - h)
         ds = np.abs(gpu_hs[:nsample, 1] - s)
         out["max_abs_err_gpu_vs_cpu"] = max(float(dh.max()), float(ds.max()))
@@ -256,6 +272,9 @@ def reference_pair_conditioning(system) -> np.ndarray:
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's CPU path for this workload (the lane-batched C++
+    restatement of calculate_hs_pairs_wicks_batched; the Rust reference cannot be built here) on
+    all host threads, rank 0 only, each step a bounded sample of the same pair batch."""
     if rank != 0:
         return
     system, basis, pairs, cfg = workload(args.workload, args.npairs, 0, args.nmo)
@@ -264,18 +283,19 @@ def run_reference(args, rank, world):
     orc = Oracle.from_system(system, tol=1e-8, with_mo_cache=False)
     ob = orc.oracle_basis(basis)
     cores = os.cpu_count() or 1
-    cal = pairs[:100_000].astype(np.int64)
+    cal = pairs[:200_000].astype(np.int64)
+    orc.eval_pairs_binned(ob, cal, nthreads=cores)
     t0 = time.perf_counter()
-    orc.eval_pairs(ob, cal, nthreads=cores)
+    orc.eval_pairs_binned(ob, cal, nthreads=cores)
     rate = cal.shape[0] / max(time.perf_counter() - t0, 1e-6)
     # each step is a bounded sample sized so warmup + steps take about two minutes
     per_step = int(max(10_000, min(pairs.shape[0], rate * 120.0 / max(1, args.steps + args.warmup))))
     sample = pairs[:per_step].astype(np.int64)
     for _ in range(args.warmup):
-        orc.eval_pairs(ob, sample, nthreads=cores)
+        orc.eval_pairs_binned(ob, sample, nthreads=cores)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        orc.eval_pairs(ob, sample, nthreads=cores)
+        _, _, lanes = orc.eval_pairs_binned(ob, sample, nthreads=cores)
     dt = time.perf_counter() - t0
     value = per_step * args.steps / dt
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
@@ -283,8 +303,8 @@ def run_reference(args, rank, world):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": dict(cfg, sample_pairs_per_step=per_step),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{per_step} pairs per step, C++ FP64 restatement of the reference "
-                                       f"evaluator (the Rust reference cannot be built here), {cores} threads"},
+                             "sample": f"{per_step} pairs per step, " + CPU_KIND.format(lanes=lanes)
+                                       + f", {cores} threads"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -781,7 +801,7 @@ def config3_check(system, basis, pairs, gpu_hs, seconds: float, ngroups: int = 1
     per_group = max(1, min_pairs // len(groups) + 1)
     cores = os.cpu_count() or 1
     dh_all, ds_all, cond_all = [], [], []
-    cpu_pairs, cpu_s, build_s = 0, 0.0, 0.0
+    cpu_pairs, cpu_s, build_s, lanes = 0, 0.0, 0.0, 0
     for g in groups:
         sel = np.nonzero(grp == g)[0][:per_group]
         if sel.size == 0:
@@ -790,10 +810,13 @@ def config3_check(system, basis, pairs, gpu_hs, seconds: float, ngroups: int = 1
         orc = Oracle.from_system(system, tol=1e-8, with_mo_cache=False, only_pairs={g})
         ob = orc.oracle_basis(basis)
         build_s += time.perf_counter() - t0
+        sp = pairs[sel].astype(np.int64)
+        orc.eval_pairs_binned(ob, sp[:4096], nthreads=cores)
         t0 = time.perf_counter()
-        h, s = orc.eval_pairs(ob, pairs[sel].astype(np.int64), nthreads=cores)
+        _, _, lanes = orc.eval_pairs_binned(ob, sp, nthreads=cores)
         cpu_s += time.perf_counter() - t0
         cpu_pairs += sel.size
+        h, s = orc.eval_pairs(ob, sp, nthreads=cores)
         dh_all.append(np.abs(gpu_hs[sel, 0] - h))
         ds_all.append(np.abs(gpu_hs[sel, 1] - s))
         cond_all.append(np.full(sel.size, smin[g]))
@@ -812,7 +835,8 @@ def config3_check(system, basis, pairs, gpu_hs, seconds: float, ngroups: int = 1
             "oracle_build_seconds": build_s,
             "cpu_baseline": {"value": cpu_pairs / max(cpu_s, 1e-9), "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{cpu_pairs} pairs of {len(groups)} of the {nref * nref} reference-pair groups "
-                                       f"({cpu_s:.1f} s of CPU work, C++ FP64 restatement, {cores} threads)"}}
+                                       f"({cpu_s:.1f} s of CPU work, " + CPU_KIND.format(lanes=lanes)
+                                       + f", {cores} threads)"}}
 
 
 def tail_summary(line):

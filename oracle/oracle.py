@@ -60,6 +60,10 @@ def lib():
                                      ctypes.c_int64, ctypes.c_double, ctypes.c_double, i64p, i32p,
                                      ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp]
         L.orc_eval_pairs.restype = ctypes.c_int
+        L.orc_eval_pairs_binned.argtypes = [dp, i64p, dp, i32p, ctypes.c_int, ctypes.c_void_p, i64p,
+                                            ctypes.c_int64, ctypes.c_double, ctypes.c_double, i64p, i32p,
+                                            ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp]
+        L.orc_eval_pairs_binned.restype = ctypes.c_int
         L.orc_eval_wick.argtypes = [dp, i64p, dp, i32p, ctypes.c_int, ctypes.c_void_p,
                                     ctypes.c_int64, ctypes.c_int64, ctypes.c_double,
                                     ctypes.c_double, ctypes.c_int, dp, dp]
@@ -275,6 +279,30 @@ class Oracle:
                          self.nmo, nthreads, 1 if exact else 0, _ptr(h, ctypes.c_double),
                          _ptr(s, ctypes.c_double))
         return h, s
+
+    def eval_pairs_binned(self, obasis: np.ndarray, pairs: np.ndarray, nthreads: int = 0, lanes: int = 0,
+                          exact: bool = False):
+        """(H, S) for pairs by the reference's own CPU path: dynamic chunks of requests over the
+        threads, each through calculate_hs_pairs_wicks_batched with the 28 (L_alpha, L_beta)
+        bins flushed through lane-batched fixed-rank kernels (8 lanes AVX-512, 4 lanes AVX2;
+        lanes = 0 picks the widest the host has).  Returns (h, s, lanes used)."""
+        L = lib()
+        pairs = np.ascontiguousarray(pairs, dtype=np.int64)
+        n = pairs.shape[0]
+        h = np.empty(n)
+        s = np.empty(n)
+        mo_offs = self.mo_offs if self.mo_offs is not None else np.zeros(1, np.int64)
+        mo_orth = self.mo_orth if self.mo_orth is not None else np.zeros(1, np.int32)
+        used = L.orc_eval_pairs_binned(
+            _ptr(self.slab, ctypes.c_double), _ptr(self.offs, ctypes.c_int64), _ptr(self.vals, ctypes.c_double),
+            _ptr(self.ints, ctypes.c_int32), self.nref, obasis.ctypes.data_as(ctypes.c_void_p),
+            _ptr(pairs, ctypes.c_int64), n, self.enuc, self.tol,
+            _ptr(mo_offs, ctypes.c_int64) if self.mo_offs is not None else None,
+            _ptr(mo_orth, ctypes.c_int32) if self.mo_orth is not None else None,
+            self.nmo, nthreads, 1 if exact else 0, lanes, _ptr(h, ctypes.c_double), _ptr(s, ctypes.c_double))
+        if used < 0:
+            raise RuntimeError(f"lane-batched CPU path: {lanes} lanes not supported on this host")
+        return h, s, used
 
     def eval_wick(self, obasis: np.ndarray, a: int, b: int, exact: bool = False):
         L = lib()

@@ -37,98 +37,9 @@
 #include <thread>
 #include <vector>
 
-namespace {
+#include "wick_oracle.h"
 
-constexpr int kMaxL = 8;
-constexpr int kSpinOffs = 27;   // x[2] y[2] fh[2][2] v[2][2][2] hcol0 j[10]
-constexpr int kNoff = 2 * kSpinOffs + 32;
-constexpr int kSpinVals = 7;    // phase tsp f0h[2] v0[3]
-constexpr int kNval = 2 * kSpinVals + 8;
-constexpr int kNint = 5;        // m_a nocc_a m_b nocc_b nmo
-
-struct SpinView {
-  const double* x[2];
-  const double* y[2];
-  const double* fh_t[2][2];
-  const double* v_t[2][2][2];
-  const double* hcol0_t;
-  const double* j[10];
-  int m, nocc, nmo;
-  double phase, tsp, f0h[2], v0[3];
-};
-
-struct DiffView {
-  const double* vab_t[2][2][2];
-  const double* vba_t[2][2][2];
-  const double* ii[2][2][2][2];
-  double vab0[2][2], vba0[2][2];
-  int nmo;
-};
-
-struct PairView {
-  SpinView aa, bb;
-  DiffView ab;
-};
-
-// One determinant: parent, per-spin ranks and ascending hole/particle lists, occupation masks.
-struct Det {
-  int32_t parent;
-  int32_t rank_a, rank_b;
-  uint8_t holes_a[kMaxL], parts_a[kMaxL], holes_b[kMaxL], parts_b[kMaxL];
-  uint64_t occ_a[2], occ_b[2];
-  double pha, phb;
-};
-
-inline const double* at(const double* base, int64_t off) { return off < 0 ? nullptr : base + off; }
-
-PairView make_view(const double* slab, const int64_t* offs, const double* vals, const int32_t* ints) {
-  PairView p{};
-  SpinView* sv[2] = {&p.aa, &p.bb};
-  for (int s = 0; s < 2; ++s) {
-    const int64_t* o = offs + s * kSpinOffs;
-    SpinView& v = *sv[s];
-    int k = 0;
-    for (int i = 0; i < 2; ++i) v.x[i] = at(slab, o[k++]);
-    for (int i = 0; i < 2; ++i) v.y[i] = at(slab, o[k++]);
-    for (int i = 0; i < 2; ++i)
-      for (int j = 0; j < 2; ++j) v.fh_t[i][j] = at(slab, o[k++]);
-    for (int i = 0; i < 2; ++i)
-      for (int j = 0; j < 2; ++j)
-        for (int l = 0; l < 2; ++l) v.v_t[i][j][l] = at(slab, o[k++]);
-    v.hcol0_t = at(slab, o[k++]);
-    for (int i = 0; i < 10; ++i) v.j[i] = at(slab, o[k++]);
-    const double* vv = vals + s * kSpinVals;
-    v.phase = vv[0];
-    v.tsp = vv[1];
-    v.f0h[0] = vv[2];
-    v.f0h[1] = vv[3];
-    v.v0[0] = vv[4];
-    v.v0[1] = vv[5];
-    v.v0[2] = vv[6];
-    v.m = ints[2 * s];
-    v.nocc = ints[2 * s + 1];
-    v.nmo = ints[4];
-  }
-  const int64_t* o = offs + 2 * kSpinOffs;
-  int k = 0;
-  for (int a = 0; a < 2; ++a)
-    for (int b = 0; b < 2; ++b)
-      for (int c = 0; c < 2; ++c) p.ab.vab_t[a][b][c] = at(slab, o[k++]);
-  for (int a = 0; a < 2; ++a)
-    for (int b = 0; b < 2; ++b)
-      for (int c = 0; c < 2; ++c) p.ab.vba_t[a][b][c] = at(slab, o[k++]);
-  for (int a = 0; a < 2; ++a)
-    for (int b = 0; b < 2; ++b)
-      for (int c = 0; c < 2; ++c)
-        for (int d = 0; d < 2; ++d) p.ab.ii[a][b][c][d] = at(slab, o[k++]);
-  const double* dv = vals + 2 * kSpinVals;
-  for (int a = 0; a < 2; ++a)
-    for (int b = 0; b < 2; ++b) p.ab.vab0[a][b] = dv[a * 2 + b];
-  for (int a = 0; a < 2; ++a)
-    for (int b = 0; b < 2; ++b) p.ab.vba0[a][b] = dv[4 + a * 2 + b];
-  p.ab.nmo = ints[4];
-  return p;
-}
+namespace orc {
 
 // ---------------------------------------------------------------------------------------
 // Tiny dense linear algebra (src/maths/wick.rs): closed forms for n <= 4, partial-pivot LU
@@ -557,26 +468,6 @@ double overlap_spin(const SpinView& w, const SpinPrep& p) {
   return pref * acc;
 }
 
-inline int popcount128(const uint64_t* a, const uint64_t* b) {
-  return __builtin_popcountll(a[0] ^ b[0]) + __builtin_popcountll(a[1] ^ b[1]);
-}
-
-struct Ctx {
-  const double* slab;
-  const int64_t* offs;
-  const double* vals;
-  const int32_t* ints;
-  int nref;
-  const Det* basis;
-  double enuc, tol;
-  bool exact;
-  // Same-parent orthogonal Slater-Condon caches (optional): per parent offsets of
-  // ha, hb (n^2), eri_aa_asym, eri_bb_asym, eri_ab_coul (n^4) and the orthogonality flag.
-  const int64_t* mo_offs;
-  const int32_t* mo_orth;
-  int nmo;
-};
-
 inline bool occ_bit(const uint64_t* o, int i) { return (o[i >> 6] >> (i & 63)) & 1ull; }
 
 int list_from_mask(const uint64_t* m, int nmo, int* out) {
@@ -721,6 +612,10 @@ void eval_one(const Ctx& c, int64_t a, int64_t b, double* h, double* s) {
       return;
     }
   }
+  eval_wick_pair(c, x, w, h, s);
+}
+
+void eval_wick_pair(const Ctx& c, const Det& x, const Det& w, double* h, double* s) {
   const int64_t pidx = (int64_t)x.parent * c.nref + w.parent;
   const PairView pv = make_view(c.slab, c.offs + pidx * kNoff, c.vals + pidx * kNval, c.ints + pidx * kNint);
   SpinPrep pa, pb;
@@ -789,7 +684,9 @@ double xw_f_spin(const SpinView& w, const FockSpin& f, const SpinPrep& p, double
   return w.phase * w.tsp * acc;
 }
 
-}  // namespace
+}  // namespace orc
+
+using namespace orc;
 
 extern "C" {
 
@@ -930,6 +827,44 @@ int orc_eval_m_pairs(const double* slab, const int64_t* offs, const double* vals
     m_out[i] = f - e0 * s;
   }
   return 0;
+}
+
+// The reference's own CPU path for the same requests: Rayon-style dynamic chunks of requests over
+// nthreads threads, each chunk through calculate_hs_pairs_wicks_batched with the lane-batched
+// fixed-rank kernels (wick_binned.cpp).  lanes = 8 (AVX-512), 4 (AVX2 + FMA) or 0 for the widest
+// the host supports (is_x86_feature_detected in the reference); the lanes used are returned, or
+// -1 when the host has neither (the requested width is not supported).
+int orc_eval_pairs_binned(const double* slab, const int64_t* offs, const double* vals, const int32_t* ints, int nref,
+                          const void* basis, const int64_t* pairs, int64_t npairs, double enuc, double tol,
+                          const int64_t* mo_offs, const int32_t* mo_orth, int nmo, int nthreads, int flags, int lanes,
+                          double* h_out, double* s_out) {
+  __builtin_cpu_init();
+  const bool has8 = __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512dq");
+  const bool has4 = __builtin_cpu_supports("avx2") && __builtin_cpu_supports("fma");
+  if (lanes == 0) lanes = has8 ? 8 : (has4 ? 4 : -1);
+  if ((lanes == 8 && !has8) || (lanes == 4 && !has4) || (lanes != 8 && lanes != 4)) return -1;
+  Ctx c{slab, offs, vals, ints, nref, reinterpret_cast<const Det*>(basis), enuc, tol, (flags & 1) != 0,
+        mo_offs, mo_orth, nmo};
+  int nt = nthreads > 0 ? nthreads : (int)std::thread::hardware_concurrency();
+  if (nt < 1) nt = 1;
+  std::atomic<int64_t> next{0};
+  const int64_t chunk = 4096;
+  auto worker = [&]() {
+    for (;;) {
+      const int64_t t0 = next.fetch_add(chunk);
+      if (t0 >= npairs) break;
+      const int64_t t1 = std::min(npairs, t0 + chunk);
+      if (lanes == 8)
+        hs_pairs_batched8(c, pairs, t0, t1, h_out, s_out);
+      else
+        hs_pairs_batched4(c, pairs, t0, t1, h_out, s_out);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int k = 1; k < nt; ++k) pool.emplace_back(worker);
+  worker();
+  for (auto& th : pool) th.join();
+  return lanes;
 }
 
 }  // extern "C"
