@@ -68,6 +68,20 @@ typedef struct {
     double phase;        /* alpha phase * beta phase relative to the parent          */
 } nw_det;
 
+/* Excitation cache of one spin (noci-rs ExcitationSpinCache, src/lib.rs:151-167): rank and the
+ * first four holes [0..3] then particles [4..7], ascending. */
+typedef struct {
+    uint8_t rank;
+    uint8_t indices[8];
+} nw_exc_spin;
+
+/* Both spins of a determinant's excitation from its parent (noci-rs ExcitationCache,
+ * src/lib.rs:136-149), the per-request input of xw_hamiltonian_overlap_prepared_batched. */
+typedef struct {
+    nw_exc_spin alpha;
+    nw_exc_spin beta;
+} nw_exc_cache;
+
 /* AO data (noci-rs AoData, src/lib.rs:52-76): only the fields the Wick path reads. */
 typedef struct {
     int32_t nao;         /* AO basis size                                            */
@@ -77,6 +91,21 @@ typedef struct {
     const double* h;     /* nao x nao core Hamiltonian                               */
     const double* eri;   /* nao^4 Coulomb integrals (mu nu|lam sig)                  */
 } nw_system;
+
+/* AO data with the two-electron integrals in Cholesky-factored form:
+ * (mu nu|lam sig) = sum_P chol[P][mu][nu] chol[P][lam][sig], each chol[P] symmetric, naux of
+ * them.  The reference reads the full eri_coul tensor (AoData.eri_coul, src/read.rs:28-61);
+ * this is the factored input of the same integrals. */
+typedef struct {
+    int32_t nao;
+    int32_t nmo;
+    int32_t naux;        /* Cholesky vectors                                         */
+    int32_t pad;
+    double enuc;
+    const double* s;     /* nao x nao overlap                                        */
+    const double* h;     /* nao x nao core Hamiltonian                               */
+    const double* chol;  /* naux x nao x nao                                         */
+} nw_system_cd;
 
 /* Reference determinants (noci-rs DetState ca/cb/oa/ob, src/scalar.rs:30-61). */
 typedef struct {
@@ -107,6 +136,12 @@ typedef struct nw_ctx nw_ctx;
 /* Create a context: copies the AO data and reference orbitals to the device.
  * Replaces the inputs of noci-rs build_wicks_shared (src/noci/wicks.rs:133-139). */
 NW_API nw_status nw_ctx_create(const nw_system* sys, const nw_refs* refs, const nw_opts* opts, nw_ctx** out);
+
+/* The same from Cholesky-factored integrals: the factors are copied to the device and kept, and
+ * the Coulomb tensor is formed there as L^T L on the engine's FP64 GEMM (nw_dgemm).  Every
+ * other call works on such a context as on one made by nw_ctx_create. */
+NW_API nw_status nw_ctx_create_cholesky(const nw_system_cd* sys, const nw_refs* refs, const nw_opts* opts,
+                                        nw_ctx** out);
 
 /* Build every ordered reference-pair intermediate on the GPU (Loewdin pairing by an FP64
  * Jacobi SVD, M^(0)/M^(1), X/Y, F, V, J and II tensors).
@@ -156,6 +191,32 @@ NW_API nw_status nw_eval_hs_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs_dev
  * Replaces xw_overlap (src/nonorthogonalwicks/eval/overlap.rs:42-65) times the phases. */
 NW_API nw_status nw_eval_s_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* s_dev,
                                  void* stream);
+
+/* The same with host buffers (copies in, evaluates, copies S out, returns when done); pair
+ * indices out of range give NW_ERR_INVALID.  Replaces xw_overlap_same_f64_batched
+ * (src/nonorthogonalwicks/eval/overlap.rs:2572-2856) as called by calculate_s_pair /
+ * src/noci/overlap.rs:162-186. */
+NW_API nw_status nw_eval_s_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* s_host,
+                                 void* stream);
+
+/* (H, S) for npairs requests of one ordered reference pair (bra reference lp, ket reference gp)
+ * from caller-held excitation caches: request i is the bra x[i] (a determinant of reference lp)
+ * against the ket w[i] (of reference gp), with phase[i] the product of both determinants'
+ * excitation phases; hs[2i] = H, hs[2i + 1] = S.  Host buffers; returns when the results are in
+ * hs_out.  Caches are checked like a resident basis (ranks <= 4, holes ascending in the
+ * occupied block, particles ascending in the virtual block, finite phase); a request that fails
+ * gets NaN and the call returns NW_ERR_INVALID.  On a diagonal block (lp == gp) requests more
+ * than a double excitation apart give exactly (0, 0).  Replaces
+ * xw_hamiltonian_overlap_prepared_batched (src/nonorthogonalwicks/eval/preparehamiltonianoverlap.rs:121-129)
+ * with its requests' ExcitationCache pairs, and xw_hamiltonian_overlap_prepared (:53-61) for
+ * one request. */
+NW_API nw_status nw_eval_hs_batched(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x, const nw_exc_cache* w,
+                                    const double* phase, uint64_t npairs, double* hs_out, void* stream);
+/* The same with device buffers, asynchronous on `stream`; failed requests are reported by
+ * nw_sync. */
+NW_API nw_status nw_eval_hs_batched_device(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x_dev,
+                                           const nw_exc_cache* w_dev, const double* phase_dev, uint64_t npairs,
+                                           double* hs_dev, void* stream);
 
 /* Fock tables for the (F, S) path from the AO Fock matrices of each spin (row-major nao x nao,
  * host memory): F^(mi,mj) = cx^(mi)^T F xc^(mj) and F_0^(m) = tr(M^(m) F) for every ordered
@@ -381,6 +442,19 @@ NW_API nw_status nw_pt2_last_apply_ms(const nw_pt2* p, float* ms);
 NW_API nw_status nw_pt2_solve(nw_pt2* p, const nw_pt2_projection* proj, const double* rhs, const nw_gmres_opts* opts,
                               double* x, nw_gmres_info* info);
 NW_API nw_status nw_pt2_destroy(nw_pt2* p);
+
+/* The engine's FP64 GEMM on the B200's FP64 tensor cores (DMMA), the product behind every dense
+ * contraction of nw_build_intermediates: row-major, strided-batched, device buffers, asynchronous
+ * on `stream`:  C[b] (m x n) = alpha op(A[b]) op(B[b]) + beta C[b]  for b < batch, where
+ * op(A) = A^T when trans_a != 0 (A stored k x m, leading dimension lda) and likewise B (stored
+ * n x k when transposed); a stride of 0 shares that operand across the batch.  Stands in for
+ * the dense products of src/nonorthogonalwicks/build.rs (construct_xy, build_cx_xc,
+ * build_j_coulomb / build_k_exchange, the F and V intermediates) and the four-index transform
+ * eri_ao2mo_into (src/maths/eri.rs:258).  NW_ERR_INVALID for null pointers, negative sizes,
+ * k == 0 with m, n > 0, more than 65535 batches or ceil(m / 64) > 65535. */
+NW_API nw_status nw_dgemm(int trans_a, int trans_b, int m, int n, int k, double alpha, const double* a, int lda,
+                          long long stride_a, const double* b, int ldb, long long stride_b, double beta, double* c,
+                          int ldc, long long stride_c, int batch, void* stream);
 
 /* Wait for the work queued on `stream` and report pair indices that were out of range in an
  * earlier device-buffer call (those outputs are NaN). */

@@ -197,20 +197,24 @@ const char* nw_status_string(nw_status st) {
 
 const char* nw_last_error(const nw_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
 
-nw_status nw_ctx_create(const nw_system* sys, const nw_refs* refs, const nw_opts* opts, nw_ctx** out) {
-  if (!out) return NW_ERR_INVALID;
-  *out = nullptr;
-  if (!sys || !refs || !opts || !sys->s || !sys->h || !sys->eri || !refs->c_alpha || !refs->c_beta)
-    return NW_ERR_INVALID;
-  const int nao = sys->nao, nmo = sys->nmo, nref = refs->nref;
+}  // extern "C"
+
+namespace {
+
+// Shared part of nw_ctx_create / nw_ctx_create_cholesky: validation of everything but the
+// two-electron integrals, the context, its streams and the uploads of S, h and the orbitals.
+nw_status create_base(int nao, int nmo, double enuc, const double* s, const double* h, const nw_refs* refs,
+                      const nw_opts* opts, nw_ctx** out) {
+  if (!s || !h || !refs || !opts || !refs->c_alpha || !refs->c_beta) return NW_ERR_INVALID;
+  const int nref = refs->nref;
   if (nao <= 0 || nmo <= 0 || nmo > 128 || nref <= 0 || nref > 256) return NW_ERR_UNSUPPORTED;
   if (refs->nocc_a < 0 || refs->nocc_b < 0 || refs->nocc_a > nmo || refs->nocc_b > nmo) return NW_ERR_INVALID;
   if (refs->nocc_a > 64 || refs->nocc_b > 64) return NW_ERR_UNSUPPORTED;
-  if (!(opts->tol >= 0.0) || !std::isfinite(opts->tol) || !std::isfinite(sys->enuc)) return NW_ERR_INVALID;
+  if (!(opts->tol >= 0.0) || !std::isfinite(opts->tol) || !std::isfinite(enuc)) return NW_ERR_INVALID;
   if (opts->convention != NW_CONVENTION_REFERENCE && opts->convention != NW_CONVENTION_EXACT) return NW_ERR_INVALID;
-  const size_t n2 = (size_t)nao * nao, n4 = n2 * n2;
-  if (!finite_all(sys->s, n2) || !finite_all(sys->h, n2) || !finite_all(sys->eri, n4) ||
-      !finite_all(refs->c_alpha, (size_t)nref * nao * nmo) || !finite_all(refs->c_beta, (size_t)nref * nao * nmo))
+  const size_t n2 = (size_t)nao * nao;
+  if (!finite_all(s, n2) || !finite_all(h, n2) || !finite_all(refs->c_alpha, (size_t)nref * nao * nmo) ||
+      !finite_all(refs->c_beta, (size_t)nref * nao * nmo))
     return NW_ERR_INVALID;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return NW_ERR_NO_DEVICE;
@@ -223,15 +227,14 @@ nw_status nw_ctx_create(const nw_system* sys, const nw_refs* refs, const nw_opts
   ctx->nref = nref;
   ctx->nocc_a = refs->nocc_a;
   ctx->nocc_b = refs->nocc_b;
-  ctx->enuc = sys->enuc;
+  ctx->enuc = enuc;
   ctx->tol = opts->tol;
   ctx->convention = opts->convention;
   nw_status st = NW_OK;
   if (cudaSetDevice(ctx->device) != cudaSuccess) st = NW_ERR_CUDA;
   if (st == NW_OK && cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) st = NW_ERR_CUDA;
-  if (st == NW_OK) st = upload(ctx, &ctx->d_s, sys->s, n2);
-  if (st == NW_OK) st = upload(ctx, &ctx->d_h, sys->h, n2);
-  if (st == NW_OK) st = upload(ctx, &ctx->d_eri, sys->eri, n4);
+  if (st == NW_OK) st = upload(ctx, &ctx->d_s, s, n2);
+  if (st == NW_OK) st = upload(ctx, &ctx->d_h, h, n2);
   if (st == NW_OK) st = upload(ctx, &ctx->d_ca, refs->c_alpha, (size_t)nref * nao * nmo);
   if (st == NW_OK) st = upload(ctx, &ctx->d_cb, refs->c_beta, (size_t)nref * nao * nmo);
   if (st == NW_OK && cudaMallocHost(&ctx->h_flag, sizeof(uint32_t)) != cudaSuccess) st = NW_ERR_ALLOC;
@@ -240,6 +243,56 @@ nw_status nw_ctx_create(const nw_system* sys, const nw_refs* refs, const nw_opts
         cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming) != cudaSuccess)
       st = NW_ERR_CUDA;
   if (st == NW_OK && cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess) st = NW_ERR_CUDA;
+  if (st != NW_OK) {
+    nw_ctx_destroy(ctx);
+    return st;
+  }
+  *out = ctx;
+  return NW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+nw_status nw_ctx_create(const nw_system* sys, const nw_refs* refs, const nw_opts* opts, nw_ctx** out) {
+  if (!out) return NW_ERR_INVALID;
+  *out = nullptr;
+  if (!sys || !sys->eri) return NW_ERR_INVALID;
+  const size_t n2 = (size_t)std::max(sys->nao, 0) * std::max(sys->nao, 0);
+  if (sys->nao > 0 && sys->nao <= 128 && !finite_all(sys->eri, n2 * n2)) return NW_ERR_INVALID;
+  nw_ctx* ctx = nullptr;
+  nw_status st = create_base(sys->nao, sys->nmo, sys->enuc, sys->s, sys->h, refs, opts, &ctx);
+  if (st != NW_OK) return st;
+  if ((st = upload(ctx, &ctx->d_eri, sys->eri, n2 * n2)) != NW_OK) {
+    nw_ctx_destroy(ctx);
+    return st;
+  }
+  *out = ctx;
+  return NW_OK;
+}
+
+nw_status nw_ctx_create_cholesky(const nw_system_cd* sys, const nw_refs* refs, const nw_opts* opts, nw_ctx** out) {
+  if (!out) return NW_ERR_INVALID;
+  *out = nullptr;
+  if (!sys || !sys->chol || sys->naux <= 0) return NW_ERR_INVALID;
+  if (sys->naux > 65536) return NW_ERR_UNSUPPORTED;
+  const int nao = sys->nao;
+  const size_t n2 = (size_t)std::max(nao, 0) * std::max(nao, 0);
+  if (nao > 0 && nao <= 128 && !finite_all(sys->chol, (size_t)sys->naux * n2)) return NW_ERR_INVALID;
+  nw_ctx* ctx = nullptr;
+  nw_status st = create_base(nao, sys->nmo, sys->enuc, sys->s, sys->h, refs, opts, &ctx);
+  if (st != NW_OK) return st;
+  // (mu nu|lam sig) = sum_P L[P][mu nu] L[P][lam sig]: E = L^T L with L as naux x n^2, on the
+  // engine's FP64 GEMM; the factors stay resident
+  ctx->naux = sys->naux;
+  st = upload(ctx, &ctx->d_chol, sys->chol, (size_t)sys->naux * n2);
+  if (st == NW_OK && cudaMalloc(&ctx->d_eri, n2 * n2 * sizeof(double)) != cudaSuccess) st = NW_ERR_ALLOC;
+  if (st == NW_OK) {
+    const cudaError_t e = nw::dgemm_strided(0, true, false, (int)n2, (int)n2, sys->naux, 1.0, ctx->d_chol, (int)n2, 0,
+                                            ctx->d_chol, (int)n2, 0, 0.0, ctx->d_eri, (int)n2, 0, 1);
+    if (e != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) st = nw::cuda_fail(ctx, e, "Cholesky integrals");
+  }
   if (st != NW_OK) {
     nw_ctx_destroy(ctx);
     return st;
@@ -417,7 +470,7 @@ nw_status nw_ctx_destroy(nw_ctx* ctx) {
   if (!ctx) return NW_OK;
   cudaSetDevice(ctx->device);
   cudaDeviceSynchronize();
-  double* bufs[] = {ctx->d_s, ctx->d_h, ctx->d_eri, ctx->d_ca, ctx->d_cb, ctx->d_slab};
+  double* bufs[] = {ctx->d_s, ctx->d_h, ctx->d_eri, ctx->d_chol, ctx->d_ca, ctx->d_cb, ctx->d_slab};
   for (double* b : bufs)
     if (b) cudaFree(b);
   if (ctx->d_fast) cudaFree(ctx->d_fast);
@@ -428,6 +481,10 @@ nw_status nw_ctx_destroy(nw_ctx* ctx) {
   for (double* b : {ctx->d_fbase, ctx->d_fock, ctx->d_fslab})
     if (b) cudaFree(b);
   if (ctx->d_fockp) cudaFree(ctx->d_fockp);
+  free_buf(ctx->bt_dets);
+  free_buf(ctx->bt_desc);
+  free_buf(ctx->bt_pairs);
+  free_buf(ctx->bt_in);
   free_buf(ctx->keys);
   free_buf(ctx->ranks);
   free_buf(ctx->tsum);

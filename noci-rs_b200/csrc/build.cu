@@ -10,10 +10,9 @@
 //   J^(m1..m4) and II^(ma0,maz,mb0,mby) four-index tensors         build.rs:261-313, :876-917
 // and packs them into the evaluator layout: pairs without zero-overlap orbitals get the
 // fast layout (records {X0|Y0, hcol0}, antisymmetrised J^(0000), II^(0000)); the others keep
-// the full reference-ordered set.  Dense products go through cuBLAS DGEMM (plain library
-// GEMMs); pairing, contractions and layout transforms are kernels in this file.
+// the full reference-ordered set.  Dense products run on the engine's FP64 tensor-core GEMM
+// (dgemm.cu); pairing, contractions and layout transforms are kernels in this file.
 #include <cuda_runtime.h>
-#include <cublas_v2.h>
 
 #include <algorithm>
 #include <cstring>
@@ -26,25 +25,32 @@
 namespace nw {
 namespace {
 
-#define NW_BLAS(ctx, call)                                                            \
-  do {                                                                                \
-    cublasStatus_t s_ = (call);                                                       \
-    if (s_ != CUBLAS_STATUS_SUCCESS)                                                  \
-      return nw::fail(ctx, NW_ERR_CUDA, std::string("cuBLAS failure ") + std::to_string((int)s_) + " in " #call); \
+#define NW_DG(ctx, call)                                                               \
+  do {                                                                                 \
+    const cudaError_t e_ = (call);                                                     \
+    if (e_ != cudaSuccess) return nw::cuda_fail(ctx, e_, #call);                       \
   } while (0)
 
-// Row-major C(MxN) = op(A)(MxK) op(B)(KxN) through column-major cuBLAS.
-inline cublasStatus_t gemm(cublasHandle_t h, bool ta, bool tb, int M, int N, int K, double alpha, const double* A,
-                           int lda, const double* B, int ldb, double beta, double* C, int ldc) {
-  return cublasDgemm(h, tb ? CUBLAS_OP_T : CUBLAS_OP_N, ta ? CUBLAS_OP_T : CUBLAS_OP_N, N, M, K, &alpha, B, ldb, A,
-                     lda, &beta, C, ldc);
+// Row-major C(MxN) = op(A)(MxK) op(B)(KxN) on the engine's FP64 tensor-core GEMM (dgemm.cu),
+// on the build's stream.
+inline cudaError_t gemm(cudaStream_t h, bool ta, bool tb, int M, int N, int K, double alpha, const double* A, int lda,
+                        const double* B, int ldb, double beta, double* C, int ldc) {
+  return dgemm_strided(h, ta, tb, M, N, K, alpha, A, lda, 0, B, ldb, 0, beta, C, ldc, 0, 1);
 }
 
-inline cublasStatus_t gemm_b(cublasHandle_t h, bool ta, bool tb, int M, int N, int K, double alpha, const double* A,
-                             int lda, long long sa, const double* B, int ldb, long long sb, double beta, double* C,
-                             int ldc, long long sc, int batch) {
-  return cublasDgemmStridedBatched(h, tb ? CUBLAS_OP_T : CUBLAS_OP_N, ta ? CUBLAS_OP_T : CUBLAS_OP_N, N, M, K,
-                                   &alpha, B, ldb, sb, A, lda, sa, &beta, C, ldc, sc, batch);
+inline cudaError_t gemm_b(cudaStream_t h, bool ta, bool tb, int M, int N, int K, double alpha, const double* A,
+                          int lda, long long sa, const double* B, int ldb, long long sb, double beta, double* C,
+                          int ldc, long long sc, int batch) {
+  return dgemm_strided(h, ta, tb, M, N, K, alpha, A, lda, sa, B, ldb, sb, beta, C, ldc, sc, batch);
+}
+
+// y[b][i] += alpha x[b][i] for a batch of vectors at strides sx, sy.
+__global__ void axpy_batched_kernel(double alpha, const double* __restrict__ x, long long sx, double* __restrict__ y,
+                                    long long sy, long long n) {
+  const double* xb = x + blockIdx.y * sx;
+  double* yb = y + blockIdx.y * sy;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    yb[i] += alpha * xb[i];
 }
 
 // Bump allocator over one device buffer, 256-byte aligned pieces.
@@ -310,16 +316,16 @@ __global__ void ii_kernel(const double* __restrict__ t4, int n, double* __restri
 // result in layout [p][r][q][s] in t4.  t1 is scratch of n^4 doubles (nao == nmo here).
 nw_status transform4(nw_ctx* ctx, const double* eri, int n, const double* A, const double* B, const double* C,
                      const double* D, double* t1, double* t4) {
-  cublasHandle_t h = ctx->blas;
+  const cudaStream_t h = 0;  // the build runs on the legacy default stream
   const long long n2 = (long long)n * n, n3 = n2 * n;
   // T1[p][nu lam sig] = A^T (n x n) * E (n x n^3)
-  NW_BLAS(ctx, gemm(h, true, false, n, (int)n3, n, 1.0, A, n, eri, (int)n3, 0.0, t1, (int)n3));
+  NW_DG(ctx, gemm(h, true, false, n, (int)n3, n, 1.0, A, n, eri, (int)n3, 0.0, t1, (int)n3));
   // T2[p][lam sig][q] = T1[p]^T (n^2 x n) * B (n x n)
-  NW_BLAS(ctx, gemm_b(h, true, false, (int)n2, n, n, 1.0, t1, (int)n2, n3, B, n, 0, 0.0, t4, n, n3, n));
+  NW_DG(ctx, gemm_b(h, true, false, (int)n2, n, n, 1.0, t1, (int)n2, n3, B, n, 0, 0.0, t4, n, n3, n));
   // T3[p][r][sig q] = C^T (n x n) * T2[p] (n x n^2)
-  NW_BLAS(ctx, gemm_b(h, true, false, n, (int)n2, n, 1.0, C, n, 0, t4, (int)n2, n3, 0.0, t1, (int)n2, n3, n));
+  NW_DG(ctx, gemm_b(h, true, false, n, (int)n2, n, 1.0, C, n, 0, t4, (int)n2, n3, 0.0, t1, (int)n2, n3, n));
   // T4[p r][q][s] = T3[pr]^T (n x n) * D (n x n)
-  NW_BLAS(ctx, gemm_b(h, true, false, n, n, n, 1.0, t1, n, n2, D, n, 0, 0.0, t4, n, n2, (int)n2));
+  NW_DG(ctx, gemm_b(h, true, false, n, n, n, 1.0, t1, n, n2, D, n, 0, 0.0, t4, n, n2, (int)n2));
   return NW_OK;
 }
 
@@ -338,7 +344,7 @@ nw_status build_all(nw_ctx* ctx) {
   const int oa = ctx->nocc_a, ob = ctx->nocc_b, omax = std::max(oa, ob);
   const size_t n2 = (size_t)n * n, n4 = n2 * n2;
   if (nao != n) return fail(ctx, NW_ERR_UNSUPPORTED, "this build requires nao == nmo");
-  cublasHandle_t h = ctx->blas;
+  const cudaStream_t h = 0;  // the build runs on the legacy default stream
 
   // ---------------- workspace ----------------
   const size_t per_ps = 2 * (size_t)nao * omax + omax + 2 * n2 /*M*/ + 4 * n2 /*rowc colc cxs cws*/ +
@@ -417,56 +423,54 @@ nw_status build_all(nw_ctx* ctx) {
   // ---------------- dense products ----------------
   const int B2 = nps * 2;  // (ps, m)
   // MtS = M^T S, MS = M S
-  NW_BLAS(ctx, gemm_b(h, true, false, n, n, n, 1.0, M, n, n2, ctx->d_s, n, 0, 0.0, MtS, n, n2, B2));
-  NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, M, n, n2, ctx->d_s, n, 0, 0.0, MS, n, n2, B2));
+  NW_DG(ctx, gemm_b(h, true, false, n, n, n, 1.0, M, n, n2, ctx->d_s, n, 0, 0.0, MtS, n, n2, B2));
+  NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, M, n, n2, ctx->d_s, n, 0, 0.0, MS, n, n2, B2));
   // products with the per-ps C copies, one call per m
   for (int m = 0; m < 2; ++m) {
     const size_t off = (size_t)m * n2;
-    NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, MtS + off, n, 2 * n2, cxs, n, n2, 0.0, mtsx + off, n, 2 * n2, nps));
-    NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, MtS + off, n, 2 * n2, cws, n, n2, 0.0, mtsw + off, n, 2 * n2, nps));
-    NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, MS + off, n, 2 * n2, cxs, n, n2, 0.0, msx + off, n, 2 * n2, nps));
-    NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, MS + off, n, 2 * n2, cws, n, n2, 0.0, msw + off, n, 2 * n2, nps));
+    NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, MtS + off, n, 2 * n2, cxs, n, n2, 0.0, mtsx + off, n, 2 * n2, nps));
+    NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, MtS + off, n, 2 * n2, cws, n, n2, 0.0, mtsw + off, n, 2 * n2, nps));
+    NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, MS + off, n, 2 * n2, cxs, n, n2, 0.0, msx + off, n, 2 * n2, nps));
+    NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, MS + off, n, 2 * n2, cws, n, n2, 0.0, msw + off, n, 2 * n2, nps));
   }
   cxxc_kernel<<<dim3(grid_for(n2) > 64 ? 64 : grid_for(n2), B2), 256>>>(mtsx, mtsw, msx, msw, cxs, cws, nao, n, oa, ob,
                                                                       cx, xc);
   NW_CUDA(ctx, cudaGetLastError());
   // X^(m) = rowc^T (S M S) colc: tmp = MS * S; X = rowc^T tmp colc
-  NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, ctx->d_s, n, 0, MS, n, n2, 0.0, tmp, n, n2, B2));  // S M S
+  NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, ctx->d_s, n, 0, MS, n, n2, 0.0, tmp, n, n2, B2));  // S M S
   for (int m = 0; m < 2; ++m) {
     const size_t off = (size_t)m * n2;
-    NW_BLAS(ctx, gemm_b(h, true, false, n, n, n, 1.0, rowc, n, n2, tmp + off, n, 2 * n2, 0.0, MS + off, n, 2 * n2, nps));
-    NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, MS + off, n, 2 * n2, colc, n, n2, 0.0, X + off, n, 2 * n2, nps));
+    NW_DG(ctx, gemm_b(h, true, false, n, n, n, 1.0, rowc, n, n2, tmp + off, n, 2 * n2, 0.0, MS + off, n, 2 * n2, nps));
+    NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, MS + off, n, 2 * n2, colc, n, n2, 0.0, X + off, n, 2 * n2, nps));
   }
   // Y^(0) = X^(0) - rowc^T S colc, Y^(1) = X^(1): tmp(ps,0) = rowc^T S, tmp(ps,1) = tmp(ps,0) colc
-  NW_BLAS(ctx, gemm_b(h, true, false, n, n, n, 1.0, rowc, n, n2, ctx->d_s, n, 0, 0.0, tmp, n, 2 * n2, nps));
-  NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, tmp, n, 2 * n2, colc, n, n2, 0.0, tmp + n2, n, 2 * n2, nps));
+  NW_DG(ctx, gemm_b(h, true, false, n, n, n, 1.0, rowc, n, n2, ctx->d_s, n, 0, 0.0, tmp, n, 2 * n2, nps));
+  NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, tmp, n, 2 * n2, colc, n, n2, 0.0, tmp + n2, n, 2 * n2, nps));
   NW_CUDA(ctx, cudaMemcpyAsync(Y, X, sizeof(double) * nps * 2 * n2, cudaMemcpyDeviceToDevice));
-  {
-    const double minus = -1.0;
-    // Y(ps,0) -= tmp(ps,1)
-    for (int ps = 0; ps < nps; ++ps)
-      NW_BLAS(ctx, cublasDaxpy(h, (int)n2, &minus, tmp + (size_t)ps * 2 * n2 + n2, 1, Y + (size_t)ps * 2 * n2, 1));
-  }
+  // Y(ps,0) -= tmp(ps,1)
+  axpy_batched_kernel<<<dim3(grid_for(n2) > 64 ? 64 : grid_for(n2), nps), 256>>>(-1.0, tmp + n2, 2 * (long long)n2, Y,
+                                                                              2 * (long long)n2, (long long)n2);
+  NW_CUDA(ctx, cudaGetLastError());
   // JK and Coulomb-only J for all (ps, m): rows of M are vec(M)
   g_kernel<<<grid_for(n4), 256>>>(ctx->d_eri, n, G);
   NW_CUDA(ctx, cudaGetLastError());
-  NW_BLAS(ctx, gemm(h, false, true, B2, (int)n2, (int)n2, 1.0, M, (int)n2, G, (int)n2, 0.0, JK, (int)n2));
-  NW_BLAS(ctx, gemm(h, false, true, B2, (int)n2, (int)n2, 1.0, M, (int)n2, ctx->d_eri, (int)n2, 0.0, Jc, (int)n2));
+  NW_DG(ctx, gemm(h, false, true, B2, (int)n2, (int)n2, 1.0, M, (int)n2, G, (int)n2, 0.0, JK, (int)n2));
+  NW_DG(ctx, gemm(h, false, true, B2, (int)n2, (int)n2, 1.0, M, (int)n2, ctx->d_eri, (int)n2, 0.0, Jc, (int)n2));
   // hxc[ps][mj] = h xc[mj]; Fh[ps][mi][mj] = cx[mi]^T hxc[mj]
-  NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, ctx->d_h, n, 0, xc, n, n2, 0.0, hxc, n, n2, B2));
+  NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, ctx->d_h, n, 0, xc, n, n2, 0.0, hxc, n, n2, B2));
   for (int mi = 0; mi < 2; ++mi)
     for (int mj = 0; mj < 2; ++mj)
-      NW_BLAS(ctx, gemm_b(h, true, false, n, n, n, 1.0, cx + mi * n2, n, 2 * n2, hxc + mj * n2, n, 2 * n2, 0.0,
+      NW_DG(ctx, gemm_b(h, true, false, n, n, n, 1.0, cx + mi * n2, n, 2 * n2, hxc + mj * n2, n, 2 * n2, 0.0,
                           Fh + (size_t)(mi * 2 + mj) * n2, n, 4 * n2, nps));
   // JKxc[ps][mk][mj] = JK[mk] xc[mj]; V[ps][mi][mj][mk] = cx[mi]^T JKxc[mk][mj]
   for (int mk = 0; mk < 2; ++mk)
     for (int mj = 0; mj < 2; ++mj)
-      NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, JK + mk * n2, n, 2 * n2, xc + mj * n2, n, 2 * n2, 0.0,
+      NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, JK + mk * n2, n, 2 * n2, xc + mj * n2, n, 2 * n2, 0.0,
                           JKxc + (size_t)(mk * 2 + mj) * n2, n, 4 * n2, nps));
   for (int mi = 0; mi < 2; ++mi)
     for (int mj = 0; mj < 2; ++mj)
       for (int mk = 0; mk < 2; ++mk)
-        NW_BLAS(ctx, gemm_b(h, true, false, n, n, n, 1.0, cx + mi * n2, n, 2 * n2, JKxc + (size_t)(mk * 2 + mj) * n2, n,
+        NW_DG(ctx, gemm_b(h, true, false, n, n, n, 1.0, cx + mi * n2, n, 2 * n2, JKxc + (size_t)(mk * 2 + mj) * n2, n,
                             4 * n2, 0.0, Vv + (size_t)((mi * 2 + mj) * 2 + mk) * n2, n, 8 * n2, nps));
   // Different-spin: for alpha (ps = 2p) vab[ma0][mb0][mak] = cx_a[ma0]^T Jc_b[mb0] xc_a[mak];
   // for beta (ps = 2p+1) vba[mb0][ma0][mbk] = cx_b[mb0]^T Jc_a[ma0] xc_b[mbk].
@@ -474,16 +478,16 @@ nw_status build_all(nw_ctx* ctx) {
   for (int mo = 0; mo < 2; ++mo)
     for (int mk = 0; mk < 2; ++mk) {
       // alpha rows: other = beta (ps+1)
-      NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, Jc + 2 * n2 + mo * n2, n, 4 * n2, xc + mk * n2, n, 4 * n2, 0.0,
+      NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, Jc + 2 * n2 + mo * n2, n, 4 * n2, xc + mk * n2, n, 4 * n2, 0.0,
                           JcXc + (size_t)(mo * 2 + mk) * n2, n, 8 * n2, npair));
       // beta rows: other = alpha (ps-1)
-      NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, Jc + mo * n2, n, 4 * n2, xc + 2 * n2 + mk * n2, n, 4 * n2, 0.0,
+      NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, Jc + mo * n2, n, 4 * n2, xc + 2 * n2 + mk * n2, n, 4 * n2, 0.0,
                           JcXc + 4 * n2 + (size_t)(mo * 2 + mk) * n2, n, 8 * n2, npair));
     }
   for (int mt = 0; mt < 2; ++mt)
     for (int mo = 0; mo < 2; ++mo)
       for (int mk = 0; mk < 2; ++mk)
-        NW_BLAS(ctx, gemm_b(h, true, false, n, n, n, 1.0, cx + mt * n2, n, 2 * n2, JcXc + (size_t)(mo * 2 + mk) * n2, n,
+        NW_DG(ctx, gemm_b(h, true, false, n, n, n, 1.0, cx + mt * n2, n, 2 * n2, JcXc + (size_t)(mo * 2 + mk) * n2, n,
                             4 * n2, 0.0, Vd + (size_t)((mt * 2 + mo) * 2 + mk) * n2, n, 8 * n2, nps));
 
   // ---------------- scalars ----------------
@@ -770,7 +774,7 @@ nw_status update_fock(nw_ctx* ctx, const double* fa, const double* fb) {
   if (!ctx->built || !ctx->d_fbase) return fail(ctx, NW_ERR_STATE, "intermediates not built");
   const int n = ctx->nmo, nref = ctx->nref, npair = nref * nref, nps = 2 * npair;
   const size_t n2 = (size_t)n * n;
-  cublasHandle_t h = ctx->blas;
+  const cudaStream_t h = 0;  // the build runs on the legacy default stream
   ctx->fock_ready = false;
   if (!ctx->d_fock && cudaMalloc(&ctx->d_fock, sizeof(double) * 2 * n2) != cudaSuccess)
     return fail(ctx, NW_ERR_ALLOC, "Fock matrix allocation failed");
@@ -789,12 +793,12 @@ nw_status update_fock(nw_ctx* ctx, const double* fa, const double* fb) {
   // Fxc[2p+s][mj] = F_s xc[2p+s][mj]
   for (int s = 0; s < 2; ++s)
     for (int mj = 0; mj < 2; ++mj)
-      NW_BLAS(ctx, gemm_b(h, false, false, n, n, n, 1.0, ctx->d_fock + s * n2, n, 0, fbase + s * 6 * n2 + (4 + mj) * n2,
+      NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, ctx->d_fock + s * n2, n, 0, fbase + s * 6 * n2 + (4 + mj) * n2,
                           n, 12 * n2, 0.0, Fxc + (size_t)(s * 2 + mj) * n2, n, 4 * n2, npair));
   // ff[ps][mi][mj] = cx[ps][mi]^T Fxc[ps][mj]
   for (int mi = 0; mi < 2; ++mi)
     for (int mj = 0; mj < 2; ++mj)
-      NW_BLAS(ctx, gemm_b(h, true, false, n, n, n, 1.0, fbase + (2 + mi) * n2, n, 6 * n2, Fxc + mj * n2, n, 2 * n2, 0.0,
+      NW_DG(ctx, gemm_b(h, true, false, n, n, n, 1.0, fbase + (2 + mi) * n2, n, 6 * n2, Fxc + mj * n2, n, 2 * n2, 0.0,
                           ff + (size_t)(mi * 2 + mj) * n2, n, 4 * n2, nps));
   // f0f[ps][m] = tr(M[ps][m] F_s)
   const int ntr = 2 * nps;

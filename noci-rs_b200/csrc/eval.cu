@@ -500,7 +500,7 @@ EvalParams make_params(const nw_ctx* ctx) {
 // fills P.nbucket / P.shift.
 uint64_t plan_keys(const nw_ctx* ctx, EvalParams& P, uint64_t cap) {
   uint32_t nb = 1;
-  P.shift = sort_key_shift(ctx->ndet, ctx->nref, cap, &nb);
+  P.shift = sort_key_shift(P.ndet, ctx->nref, cap, &nb);
   P.nbucket = nb;
   const uint64_t ngen = (uint64_t)ctx->nref * ctx->nref - (uint64_t)ctx->nfast;
   return (uint64_t)kClasses * nb + (uint64_t)kGenClasses * ngen;
@@ -584,6 +584,12 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
                      cudaStream_t stream, bool clear_flag) {
   if (!ctx->built) return fail(ctx, NW_ERR_STATE, "intermediates not built");
   if (!ctx->d_dets) return fail(ctx, NW_ERR_STATE, "no determinant basis set");
+  return eval_pairs_on(ctx, make_params(ctx), pairs, npairs, out, mode, stream, clear_flag);
+}
+
+nw_status eval_pairs_on(nw_ctx* ctx, EvalParams P, const uint32_t* pairs, uint64_t npairs, double* out, EvalMode mode,
+                        cudaStream_t stream, bool clear_flag) {
+  if (!ctx->built) return fail(ctx, NW_ERR_STATE, "intermediates not built");
   if (mode == EvalMode::kFS && !ctx->fock_ready) return fail(ctx, NW_ERR_STATE, "Fock tables not set (nw_update_fock)");
   const bool overlap_only = mode == EvalMode::kS;
   if (npairs == 0) return NW_OK;
@@ -591,7 +597,6 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
   if ((reinterpret_cast<uintptr_t>(pairs) & 7) != 0) return fail(ctx, NW_ERR_INVALID, "pairs must be 8-byte aligned");
   if ((reinterpret_cast<uintptr_t>(out) & (overlap_only ? 7 : 15)) != 0)
     return fail(ctx, NW_ERR_INVALID, "output must be 16-byte aligned (8 for overlap only)");
-  EvalParams P = make_params(ctx);
 
   nw_status st = ensure(ctx, ctx->flag, 256);
   if (st != NW_OK) return st;

@@ -56,6 +56,8 @@ struct nw_ctx {
   double* d_s = nullptr;
   double* d_h = nullptr;
   double* d_eri = nullptr;
+  double* d_chol = nullptr; // naux x nao x nao Cholesky vectors (nw_ctx_create_cholesky), else null
+  int naux = 0;
   double* d_ca = nullptr;   // nref x nao x nmo
   double* d_cb = nullptr;
 
@@ -78,6 +80,9 @@ struct nw_ctx {
   nw::DevBuf keys, perm, counts, offsets, flag, ranks, tsum;
   uint32_t* h_flag = nullptr;      // pinned mirror of the device error flag
   nw::DevBuf io_pairs, io_hs;      // staging for the host-buffer entry point
+  // determinant records, descriptors and pairs packed from caller excitation caches
+  // (nw_eval_hs_batched), and their device staging for host-buffer calls
+  nw::DevBuf bt_dets, bt_desc, bt_pairs, bt_in;
   // copy-in / evaluate / copy-out streams and chunk events of the pipelined host-buffer path
   cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
   // class evaluators forked off the launching stream (medium ranks; heavy and runtime ranks;
@@ -126,6 +131,13 @@ nw_status fail(nw_ctx* ctx, nw_status st, const std::string& msg);
 nw_status cuda_fail(nw_ctx* ctx, cudaError_t e, const char* what);
 nw_status ensure(nw_ctx* ctx, DevBuf& b, size_t bytes);
 
+// Row-major, strided-batched FP64 GEMM on the FP64 tensor cores (dgemm.cu):
+// C[b] (M x N) = alpha op(A[b]) op(B[b]) + beta C[b], op(X) = X^T when the flag is set
+// (A stored K x M, B stored N x K); a batch stride of 0 shares the operand.
+cudaError_t dgemm_strided(cudaStream_t stream, bool ta, bool tb, int M, int N, int K, double alpha, const double* A,
+                          int lda, long long sa, const double* B, int ldb, long long sb, double beta, double* C,
+                          int ldc, long long sc, int batch);
+
 // Build (build.cu).
 nw_status build_all(nw_ctx* ctx);
 // Fock tables from AO Fock matrices (build.cu).
@@ -138,6 +150,10 @@ enum class EvalMode { kHS, kS, kFS };
 // clear_flag = false keeps the out-of-range flag of earlier calls (chunked host path).
 nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, EvalMode mode,
                      cudaStream_t stream, bool clear_flag = true);
+// The same over a caller-supplied determinant table (P.dets / P.desc / P.ndet), e.g. the records
+// packed from excitation caches by nw_eval_hs_batched.
+nw_status eval_pairs_on(nw_ctx* ctx, EvalParams P, const uint32_t* pairs, uint64_t npairs, double* out, EvalMode mode,
+                        cudaStream_t stream, bool clear_flag = true);
 // Dense matrices over left x right determinant blocks and the generalised eigenproblem (matrix.cu).
 nw_status build_matrix(nw_ctx* ctx, EvalMode mode, const uint32_t* left, uint64_t nl, const uint32_t* right,
                        uint64_t nr, bool symmetric, double* a_host, double* s_host);

@@ -88,13 +88,6 @@ nw_status dev_alloc(nw_ctx* ctx, DevMem& m, size_t bytes, const char* what) {
       return fail(ctx, NW_ERR_CUDA, std::string(#call) + " failed: status " + std::to_string((int)s_)); \
   } while (0)
 
-#define NW_BLAS2(ctx, call)                                                                  \
-  do {                                                                                       \
-    const cublasStatus_t s_ = (call);                                                        \
-    if (s_ != CUBLAS_STATUS_SUCCESS)                                                         \
-      return fail(ctx, NW_ERR_CUDA, std::string(#call) + " failed: status " + std::to_string((int)s_)); \
-  } while (0)
-
 // Symmetric eigen-decomposition in place (column-major a, n x n, triangle `uplo`): eigenvalues
 // ascending into lam, eigenvectors as the columns of a.
 nw_status syevd(nw_ctx* ctx, cublasFillMode_t uplo, int n, double* a, double* lam) {
@@ -188,8 +181,7 @@ nw_status general_evp(nw_ctx* ctx, int n, const double* h, const double* s, bool
   if ((st = syevd(ctx, CUBLAS_FILL_MODE_UPPER, n, dS.as<double>(), dlam.as<double>())) != NW_OK) return st;
   std::vector<double> lam(n);
   NW_CUDA(ctx, cudaMemcpy(lam.data(), dlam.p, (size_t)n * 8, cudaMemcpyDeviceToHost));
-  cublasHandle_t bh = ctx->blas;
-  const double one = 1.0, zero = 0.0;
+  // the products below read the column-major (cuSOLVER) results as row-major transposes
   int k = n;
   double* X = nullptr;
   if (project) {
@@ -212,8 +204,8 @@ nw_status general_evp(nw_ctx* ctx, int n, const double* h, const double* s, bool
     NW_CUDA(ctx, cudaMemcpy(dT.p, dS.p, n2 * 8, cudaMemcpyDeviceToDevice));
     scale_columns_kernel<<<148 * 4, 256>>>(dT.as<double>(), dlam.as<double>(), n, n);
     NW_CUDA(ctx, cudaGetLastError());
-    NW_BLAS2(ctx, cublasDgemm(bh, CUBLAS_OP_N, CUBLAS_OP_T, n, n, n, &one, dT.as<double>(), n, dS.as<double>(), n, &zero,
-                              dX.as<double>(), n));
+    NW_CUDA(ctx, dgemm_strided(0, true, false, n, n, n, 1.0, dS.as<double>(), n, 0, dT.as<double>(), n, 0, 0.0,
+                               dX.as<double>(), n, 0, 1));
     X = dX.as<double>();
   }
   // Ht = X^T H X with the full H (the column-major view of the row-major H is H^T)
@@ -222,15 +214,15 @@ nw_status general_evp(nw_ctx* ctx, int n, const double* h, const double* s, bool
   if ((st = dev_alloc(ctx, dHt, (size_t)k * k * 8, "projected Hamiltonian")) != NW_OK) return st;
   if ((st = dev_alloc(ctx, deps, (size_t)k * 8, "eigenvalues")) != NW_OK) return st;
   if ((st = dev_alloc(ctx, dC, (size_t)n * k * 8, "eigenvectors")) != NW_OK) return st;
-  NW_BLAS2(ctx, cublasDgemm(bh, CUBLAS_OP_T, CUBLAS_OP_N, n, k, n, &one, dH.as<double>(), n, X, n, &zero,
-                            dHX.as<double>(), n));
-  NW_BLAS2(ctx, cublasDgemm(bh, CUBLAS_OP_T, CUBLAS_OP_N, k, k, n, &one, X, n, dHX.as<double>(), n, &zero,
-                            dHt.as<double>(), k));
+  NW_CUDA(ctx, dgemm_strided(0, false, true, k, n, n, 1.0, X, n, 0, dH.as<double>(), n, 0, 0.0, dHX.as<double>(), n,
+                             0, 1));
+  NW_CUDA(ctx, dgemm_strided(0, false, true, k, k, n, 1.0, dHX.as<double>(), n, 0, X, n, 0, 0.0, dHt.as<double>(), k,
+                             0, 1));
   // column-major Ht holds the matrix itself: its lower triangle is UPLO::Lower
   if ((st = syevd(ctx, CUBLAS_FILL_MODE_LOWER, k, dHt.as<double>(), deps.as<double>())) != NW_OK) return st;
   // C = X U2 (n x k); computed as C^T = U2^T X^T column-major (k x n) = row-major n x k
-  NW_BLAS2(ctx, cublasDgemm(bh, CUBLAS_OP_T, CUBLAS_OP_T, k, n, k, &one, dHt.as<double>(), k, X, n, &zero,
-                            dC.as<double>(), k));
+  NW_CUDA(ctx, dgemm_strided(0, true, true, n, k, k, 1.0, X, n, 0, dHt.as<double>(), k, 0, 0.0, dC.as<double>(), k,
+                             0, 1));
   NW_CUDA(ctx, cudaMemcpy(evals, deps.p, (size_t)k * 8, cudaMemcpyDeviceToHost));
   NW_CUDA(ctx, cudaMemcpy(c, dC.p, (size_t)n * k * 8, cudaMemcpyDeviceToHost));
   *nkept = k;

@@ -43,6 +43,25 @@ class NwSystem(ctypes.Structure):
                 ("eri", ctypes.POINTER(ctypes.c_double))]
 
 
+class NwSystemCd(ctypes.Structure):
+    _fields_ = [("nao", ctypes.c_int32), ("nmo", ctypes.c_int32), ("naux", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("enuc", ctypes.c_double), ("s", ctypes.POINTER(ctypes.c_double)),
+                ("h", ctypes.POINTER(ctypes.c_double)), ("chol", ctypes.POINTER(ctypes.c_double))]
+
+
+# ExcitationCache of noci-rs (src/lib.rs:136-167): per spin the rank and holes[0..3] then
+# particles[4..7]; 18 bytes, matching nw_exc_cache.
+NW_EXC_CACHE_DTYPE = np.dtype([("rank_a", "u1"), ("idx_a", "u1", (8,)), ("rank_b", "u1"), ("idx_b", "u1", (8,))])
+
+
+def exc_caches(dets: np.ndarray) -> np.ndarray:
+    """The excitation caches (NW_EXC_CACHE_DTYPE) of nw_det records."""
+    out = np.zeros(dets.shape[0], NW_EXC_CACHE_DTYPE)
+    for f in ("rank_a", "idx_a", "rank_b", "idx_b"):
+        out[f] = dets[f]
+    return out
+
+
 class NwRefs(ctypes.Structure):
     _fields_ = [("nref", ctypes.c_int32), ("nocc_a", ctypes.c_int32), ("nocc_b", ctypes.c_int32),
                 ("c_alpha", ctypes.POINTER(ctypes.c_double)), ("c_beta", ctypes.POINTER(ctypes.c_double))]
@@ -104,16 +123,16 @@ class NwInfo(ctypes.Structure):
                 ("pad", ctypes.c_int32), ("slab_bytes", ctypes.c_uint64), ("ndet", ctypes.c_uint64)]
 
 
-EXPORTED = ("nw_ctx_create", "nw_build_intermediates", "nw_pair_zero_counts", "nw_set_basis",
-            "nw_eval_hs_pairs_device", "nw_eval_hs_pairs", "nw_eval_hs_pairs_noalloc",
-            "nw_eval_s_pairs_device", "nw_update_fock", "nw_eval_fs_pairs_device", "nw_eval_fs_pairs",
+EXPORTED = ("nw_ctx_create", "nw_ctx_create_cholesky", "nw_build_intermediates", "nw_pair_zero_counts",
+            "nw_set_basis", "nw_eval_hs_pairs_device", "nw_eval_hs_pairs", "nw_eval_hs_pairs_noalloc",
+            "nw_eval_hs_batched", "nw_eval_hs_batched_device", "nw_eval_s_pairs_device", "nw_eval_s_pairs", "nw_update_fock", "nw_eval_fs_pairs_device", "nw_eval_fs_pairs",
             "nw_build_hs_matrix", "nw_build_fs_matrix", "nw_general_evp",
             "nw_qmc_create", "nw_qmc_run", "nw_qmc_set_shift", "nw_qmc_last_run_ms", "nw_qmc_populations", "nw_qmc_set_populations", "nw_qmc_cycle_delta",
             "nw_qmc_destroy", "nw_qmc_harvest", "nw_qmc_train_proposal", "nw_qmc_set_generator",
             "nw_qmc_proposal_dims", "nw_qmc_mlp_params", "nw_qmc_set_mlp_params", "nw_qmc_mlp_loss_grad",
             "nw_qmc_proposal_probs", "nw_pt2_create", "nw_pt2_apply_m", "nw_pt2_last_apply_ms", "nw_pt2_solve",
             "nw_pt2_destroy", "nw_screen_create", "nw_screen_train", "nw_screen_predict", "nw_screen_destroy",
-            "nw_autotune", "nw_sync",
+            "nw_autotune", "nw_dgemm", "nw_sync",
             "nw_set_timing", "nw_last_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
             "nw_last_error")
 
@@ -131,7 +150,12 @@ def load(path: Optional[str] = None):
     vp = ctypes.c_void_p
     L.nw_ctx_create.argtypes = [ctypes.POINTER(NwSystem), ctypes.POINTER(NwRefs), ctypes.POINTER(NwOpts),
                                 ctypes.POINTER(vp)]
+    L.nw_ctx_create_cholesky.argtypes = [ctypes.POINTER(NwSystemCd), ctypes.POINTER(NwRefs), ctypes.POINTER(NwOpts),
+                                         ctypes.POINTER(vp)]
     L.nw_build_intermediates.argtypes = [vp]
+    L.nw_eval_hs_batched.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_uint64, vp, vp]
+    L.nw_eval_hs_batched_device.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_uint64, vp, vp]
+    L.nw_eval_s_pairs.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_pair_zero_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
     L.nw_set_basis.argtypes = [vp, vp, ctypes.c_uint64]
     L.nw_eval_hs_pairs_device.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
@@ -174,6 +198,9 @@ def load(path: Optional[str] = None):
     L.nw_screen_destroy.argtypes = [vp]
     L.nw_autotune.argtypes = [vp, vp, ctypes.c_uint64, vp, vp, ctypes.POINTER(NwTuneReport)]
     L.nw_sync.argtypes = [vp, vp]
+    L.nw_dgemm.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                           vp, ctypes.c_int, ctypes.c_longlong, vp, ctypes.c_int, ctypes.c_longlong, ctypes.c_double,
+                           vp, ctypes.c_int, ctypes.c_longlong, ctypes.c_int, vp]
     L.nw_set_timing.argtypes = [vp, ctypes.c_int]
     L.nw_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     L.nw_ctx_info.argtypes = [vp, ctypes.POINTER(NwInfo)]
@@ -199,7 +226,9 @@ class WicksShared:
     determinant basis.  Mirrors noci-rs WicksShared/WicksView (storage.rs:35-150, view.rs:20-147)."""
 
     def __init__(self, s, h, eri, enuc: float, refs: Sequence[Tuple[np.ndarray, int, np.ndarray, int]],
-                 tol: float = 1e-8, convention: str = "reference", device: int = 0):
+                 tol: float = 1e-8, convention: str = "reference", device: int = 0, chol=None):
+        """With ``chol`` (naux x nao x nao Cholesky vectors) instead of ``eri`` (pass None) the
+        context is created from the factored integrals (nw_ctx_create_cholesky)."""
         self._lib = load()
         self._ctx = ctypes.c_void_p()
         nmo = refs[0][0].shape[1]
@@ -211,15 +240,25 @@ class WicksShared:
                 raise ValueError("reference occupations must be the first nocc orbitals (aufbau order)")
         self._s = np.ascontiguousarray(s, dtype=np.float64)
         self._h = np.ascontiguousarray(h, dtype=np.float64)
-        self._eri = np.ascontiguousarray(eri, dtype=np.float64)
         self._ca = np.ascontiguousarray(np.stack([r[0] for r in refs]), dtype=np.float64)
         self._cb = np.ascontiguousarray(np.stack([r[2] for r in refs]), dtype=np.float64)
-        sysd = NwSystem(nao, nmo, float(enuc), _dp(self._s), _dp(self._h), _dp(self._eri))
         rd = NwRefs(len(refs), nocc_a, nocc_b, _dp(self._ca), _dp(self._cb))
         od = NwOpts(float(tol), CONVENTIONS[convention], int(device))
-        st = self._lib.nw_ctx_create(ctypes.byref(sysd), ctypes.byref(rd), ctypes.byref(od), ctypes.byref(self._ctx))
+        if chol is not None:
+            self._chol = np.ascontiguousarray(chol, dtype=np.float64)
+            sysc = NwSystemCd(nao, nmo, self._chol.shape[0], 0, float(enuc), _dp(self._s), _dp(self._h),
+                              _dp(self._chol))
+            st = self._lib.nw_ctx_create_cholesky(ctypes.byref(sysc), ctypes.byref(rd), ctypes.byref(od),
+                                                  ctypes.byref(self._ctx))
+            where = "nw_ctx_create_cholesky"
+        else:
+            self._eri = np.ascontiguousarray(eri, dtype=np.float64)
+            sysd = NwSystem(nao, nmo, float(enuc), _dp(self._s), _dp(self._h), _dp(self._eri))
+            st = self._lib.nw_ctx_create(ctypes.byref(sysd), ctypes.byref(rd), ctypes.byref(od),
+                                         ctypes.byref(self._ctx))
+            where = "nw_ctx_create"
         if st != NW_OK:
-            raise NwError(st, "nw_ctx_create")
+            raise NwError(st, where)
         self.nref, self.nmo, self.nocc_a, self.nocc_b = len(refs), nmo, nocc_a, nocc_b
         self.tol, self.convention = tol, convention
         self._basis = None
@@ -281,6 +320,31 @@ class WicksShared:
             out = np.empty((n, 2), np.float64)
         self._check(self._lib.nw_eval_hs_pairs(self._ctx, pairs.ctypes.data, n, out.ctypes.data,
                                                ctypes.c_void_p(stream)), "nw_eval_hs_pairs")
+        return out
+
+    def eval_batched(self, lp: int, gp: int, x_caches: np.ndarray, w_caches: np.ndarray, phase: np.ndarray,
+                     stream: int = 0) -> np.ndarray:
+        """(H, S) of one ordered reference pair (lp, gp) from caller-held excitation caches
+        (xw_hamiltonian_overlap_prepared_batched): x_caches / w_caches of NW_EXC_CACHE_DTYPE,
+        phase the product of both excitation phases per request; returns (n, 2)."""
+        x = np.ascontiguousarray(x_caches, dtype=NW_EXC_CACHE_DTYPE)
+        w = np.ascontiguousarray(w_caches, dtype=NW_EXC_CACHE_DTYPE)
+        ph = np.ascontiguousarray(phase, dtype=np.float64)
+        n = x.shape[0]
+        if w.shape[0] != n or ph.shape[0] != n:
+            raise ValueError("x_caches, w_caches and phase must have one entry per request")
+        out = np.empty((n, 2), np.float64)
+        self._check(self._lib.nw_eval_hs_batched(self._ctx, int(lp), int(gp), x.ctypes.data, w.ctypes.data,
+                                                 ph.ctypes.data, n, out.ctypes.data, ctypes.c_void_p(stream)),
+                    "nw_eval_hs_batched")
+        return out
+
+    def eval_overlap(self, pairs: np.ndarray, stream: int = 0) -> np.ndarray:
+        """S for host pairs (n, 2) (nw_eval_s_pairs)."""
+        pairs = np.ascontiguousarray(pairs, dtype=np.uint32)
+        out = np.empty(pairs.shape[0], np.float64)
+        self._check(self._lib.nw_eval_s_pairs(self._ctx, pairs.ctypes.data, pairs.shape[0], out.ctypes.data,
+                                              ctypes.c_void_p(stream)), "nw_eval_s_pairs")
         return out
 
     def eval_pairs_device(self, pairs_ptr: int, npairs: int, out_ptr: int, stream: int = 0):

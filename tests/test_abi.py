@@ -47,6 +47,8 @@ int main(void) {
   printf("%zu %zu %zu %zu\n", sizeof(nw_mlp_opts), offsetof(nw_mlp_opts, seed), sizeof(nw_mlp_report),
          offsetof(nw_mlp_report, steps));
   printf("%zu %zu %zu\n", sizeof(nw_tune_report), offsetof(nw_tune_report, trials), offsetof(nw_tune_report, default_ms));
+  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(nw_system_cd), offsetof(nw_system_cd, naux), offsetof(nw_system_cd, enuc),
+         offsetof(nw_system_cd, chol), sizeof(nw_exc_cache), offsetof(nw_exc_cache, beta));
   return 0;
 }
 ''')
@@ -68,6 +70,9 @@ int main(void) {
     assert v[22:26] == [ctypes.sizeof(L.NwMlpOpts), L.NwMlpOpts.seed.offset, ctypes.sizeof(L.NwMlpReport),
                         L.NwMlpReport.steps.offset]
     assert v[26:29] == [ctypes.sizeof(L.NwTuneReport), L.NwTuneReport.trials.offset, L.NwTuneReport.default_ms.offset]
+    assert v[29:33] == [ctypes.sizeof(L.NwSystemCd), L.NwSystemCd.naux.offset, L.NwSystemCd.enuc.offset,
+                        L.NwSystemCd.chol.offset]
+    assert v[33:35] == [L.NW_EXC_CACHE_DTYPE.itemsize, L.NW_EXC_CACHE_DTYPE.fields["rank_b"][1]]
 
 
 def test_header_compiles_as_cxx(tmp_path):
