@@ -149,6 +149,29 @@ NW_API nw_status nw_ctx_create_cholesky(const nw_system_cd* sys, const nw_refs* 
  * SameSpinBuild::new / DiffSpinBuild::new (src/nonorthogonalwicks/build.rs:86-926). */
 NW_API nw_status nw_build_intermediates(nw_ctx* ctx);
 
+/* How nw_build_intermediates forms the four-index J and II tensors (build.rs:261-313, :876-917,
+ * eri_ao2mo_into, src/maths/eri.rs:258).  The Cholesky routes need a context made by
+ * nw_ctx_create_cholesky: T(A,B,C,D)[pq][rs] = sum_P (A^T L^P B)[pq] (C^T L^P D)[rs], one
+ * naux-deep product per tensor instead of four n^5 quarter transforms. */
+typedef enum {
+    NW_TRANSFORM_FP64 = 0,         /* four FP64 quarter transforms of the Coulomb tensor (default) */
+    NW_TRANSFORM_CHOL_FP64 = 1,    /* Cholesky route, FP64 product on the FP64 tensor cores      */
+    NW_TRANSFORM_CHOL_INT8 = 2,    /* Cholesky route on tcgen05: 8 signed int8 slices per factor
+                                      (Ozaki split, exact int32 sums), rebuilt in FP64             */
+    NW_TRANSFORM_CHOL_BF16X6 = 3   /* Cholesky route on tcgen05: 3 BF16 pieces per factor, the 6
+                                      leading products summed in FP32 (FP32-class accuracy)        */
+} nw_transform;
+
+/* Select the transform of the next nw_build_intermediates (NW_ERR_STATE for a Cholesky mode on
+ * a context without Cholesky factors). */
+NW_API nw_status nw_set_transform(nw_ctx* ctx, int32_t mode);
+
+/* The Cholesky-route product alone: t4[p][r][q][s] = sum_P u[P][p*n + q] v[P][r*n + s] for
+ * P < naux, p, q, r, s < n, with mode NW_TRANSFORM_CHOL_FP64, _INT8 or _BF16X6 (device buffers,
+ * synchronous).  No counterpart in the reference; exposed for checks of the split products. */
+NW_API nw_status nw_transform_product(int32_t mode, const double* u, const double* v, int32_t naux, int32_t n,
+                                      double* t4, void* stream);
+
 /* Zero-overlap counts (m_alpha, m_beta) of ordered pair x*nref + w, as planned by
  * plan_wicks_pairs (src/noci/wicks.rs:90-121).  m must hold 2*nref*nref ints. */
 NW_API nw_status nw_pair_zero_counts(const nw_ctx* ctx, int32_t* m);

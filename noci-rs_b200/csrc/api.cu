@@ -301,6 +301,45 @@ nw_status nw_ctx_create_cholesky(const nw_system_cd* sys, const nw_refs* refs, c
   return NW_OK;
 }
 
+nw_status nw_set_transform(nw_ctx* ctx, int32_t mode) {
+  if (!ctx) return NW_ERR_INVALID;
+  if (mode < NW_TRANSFORM_FP64 || mode > NW_TRANSFORM_CHOL_BF16X6) return nw::fail(ctx, NW_ERR_INVALID, "unknown transform");
+  if (mode != NW_TRANSFORM_FP64 && !ctx->d_chol)
+    return nw::fail(ctx, NW_ERR_STATE, "Cholesky transforms need a context from nw_ctx_create_cholesky");
+  ctx->transform = mode;
+  return NW_OK;
+}
+
+nw_status nw_transform_product(int32_t mode, const double* u, const double* v, int32_t naux, int32_t n, double* t4,
+                               void* stream) {
+  if (!u || !v || !t4 || naux <= 0 || n <= 0 || n > 128) return NW_ERR_INVALID;
+  if (mode != NW_TRANSFORM_CHOL_FP64 && mode != NW_TRANSFORM_CHOL_INT8 && mode != NW_TRANSFORM_CHOL_BF16X6)
+    return NW_ERR_INVALID;
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int n2 = n * n;
+  void* work = nullptr;
+  const size_t scratch = mode == NW_TRANSFORM_CHOL_FP64 ? (size_t)n2 * n2 * sizeof(double)
+                                                         : nw::split_product_scratch(mode, naux, n2, n2, nw::kOzakiSlices);
+  if (cudaMalloc(&work, scratch + 256) != cudaSuccess) return NW_ERR_ALLOC;
+  uint32_t* err = reinterpret_cast<uint32_t*>(static_cast<char*>(work) + scratch);
+  cudaError_t e = cudaMemsetAsync(err, 0, sizeof(uint32_t), s);
+  if (e == cudaSuccess) {
+    if (mode == NW_TRANSFORM_CHOL_FP64) {
+      e = nw::dgemm_strided(s, true, false, n2, n2, naux, 1.0, u, n2, 0, v, n2, 0, 0.0, static_cast<double*>(work), n2,
+                            0, 1);
+      if (e == cudaSuccess) e = nw::swap_qr(s, static_cast<const double*>(work), n, t4);
+    } else {
+      e = nw::split_product_pqrs(s, mode, nw::kOzakiSlices, u, v, naux, n, t4, work, scratch, err);
+    }
+  }
+  uint32_t herr = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(work);
+  if (e != cudaSuccess) return NW_ERR_CUDA;
+  return herr ? NW_ERR_CUDA : NW_OK;
+}
+
 nw_status nw_build_intermediates(nw_ctx* ctx) {
   if (!ctx) return NW_ERR_INVALID;
   NW_CUDA(ctx, cudaSetDevice(ctx->device));

@@ -312,10 +312,73 @@ __global__ void ii_kernel(const double* __restrict__ t4, int n, double* __restri
   }
 }
 
+// [p][q][r][s] -> [p][r][q][s]
+__global__ void swap_qr_kernel(const double* __restrict__ src, int n, double* __restrict__ dst) {
+  const size_t n2 = (size_t)n * n, n3 = n2 * n, n4 = n2 * n2;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n4; idx += (size_t)gridDim.x * blockDim.x) {
+    const size_t p = idx / n3, r = (idx / n2) % n, q = (idx / n) % n, s = idx % n;
+    dst[idx] = src[p * n3 + q * n2 + r * n + s];
+  }
+}
+
+// Cholesky-route workspace: W and the factors U, V (naux x n^2 each), the split pieces of the
+// tcgen05 product, and its error word.
+struct CholWork {
+  double *W, *U, *V;
+  void* split;
+  size_t split_bytes;
+  uint32_t* err;
+};
+
+nw_status chol_work(nw_ctx* ctx, int n, CholWork* w) {
+  const size_t fac = (size_t)ctx->naux * n * n;
+  const int mode = ctx->transform == NW_TRANSFORM_CHOL_FP64 ? NW_TRANSFORM_CHOL_INT8 : ctx->transform;
+  const size_t split = ctx->transform == NW_TRANSFORM_CHOL_FP64
+                           ? 0
+                           : split_product_scratch(mode, ctx->naux, n * n, n * n, kOzakiSlices);
+  const size_t bytes = 3 * fac * sizeof(double) + split + 1024;
+  nw_status st = ensure(ctx, ctx->chol_work, bytes);
+  if (st != NW_OK) return st;
+  char* base = static_cast<char*>(ctx->chol_work.p);
+  w->W = reinterpret_cast<double*>(base);
+  w->U = w->W + fac;
+  w->V = w->U + fac;
+  w->err = reinterpret_cast<uint32_t*>(w->V + fac);
+  w->split = reinterpret_cast<char*>(w->V + fac) + 256;
+  w->split_bytes = split;
+  NW_CUDA(ctx, cudaMemsetAsync(w->err, 0, sizeof(uint32_t)));
+  return NW_OK;
+}
+
+// The Cholesky route of T(A,B,C,D), result in [p][r][q][s] in t4 (t1 is n^4 scratch):
+// U[P] = A^T L^P B, V[P] = C^T L^P D (batched FP64 products), T[pq][rs] = sum_P U[P][pq] V[P][rs]
+// in FP64 (NW_TRANSFORM_CHOL_FP64) or as split products on tcgen05 (tc_gemm.cu).
+nw_status transform4_chol(nw_ctx* ctx, int n, const double* A, const double* B, const double* C, const double* D,
+                          double* t1, double* t4, const CholWork& w) {
+  const cudaStream_t h = 0;
+  const long long n2 = (long long)n * n;
+  const int naux = ctx->naux;
+  NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, ctx->d_chol, n, n2, B, n, 0, 0.0, w.W, n, n2, naux));
+  NW_DG(ctx, gemm_b(h, true, false, n, n, n, 1.0, A, n, 0, w.W, n, n2, 0.0, w.U, n, n2, naux));
+  NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, ctx->d_chol, n, n2, D, n, 0, 0.0, w.W, n, n2, naux));
+  NW_DG(ctx, gemm_b(h, true, false, n, n, n, 1.0, C, n, 0, w.W, n, n2, 0.0, w.V, n, n2, naux));
+  if (ctx->transform == NW_TRANSFORM_CHOL_FP64) {
+    NW_DG(ctx, gemm(h, true, false, (int)n2, (int)n2, naux, 1.0, w.U, (int)n2, w.V, (int)n2, 0.0, t1, (int)n2));
+    swap_qr_kernel<<<148 * 16, 256>>>(t1, n, t4);
+    NW_CUDA(ctx, cudaGetLastError());
+    return NW_OK;
+  }
+  NW_DG(ctx, split_product_pqrs(h, ctx->transform, kOzakiSlices, w.U, w.V, naux, n, t4, w.split, w.split_bytes,
+                                w.err));
+  return NW_OK;
+}
+
 // Four quarter transforms T(A,B,C,D)[p,q,r,s] = sum (mu nu|lam sig) A[mu,p] B[nu,q] C[lam,r] D[sig,s],
-// result in layout [p][r][q][s] in t4.  t1 is scratch of n^4 doubles (nao == nmo here).
+// result in layout [p][r][q][s] in t4.  t1 is scratch of n^4 doubles (nao == nmo here).  A
+// Cholesky transform mode takes the factored route instead.
 nw_status transform4(nw_ctx* ctx, const double* eri, int n, const double* A, const double* B, const double* C,
-                     const double* D, double* t1, double* t4) {
+                     const double* D, double* t1, double* t4, const CholWork* cw = nullptr) {
+  if (cw) return transform4_chol(ctx, n, A, B, C, D, t1, t4, *cw);
   const cudaStream_t h = 0;  // the build runs on the legacy default stream
   const long long n2 = (long long)n * n, n3 = n2 * n;
   // T1[p][nu lam sig] = A^T (n x n) * E (n x n^3)
@@ -337,6 +400,11 @@ inline int grid_for(size_t work, int block = 256) {
 }
 
 }  // namespace
+
+cudaError_t swap_qr(cudaStream_t st, const double* src, int n, double* dst) {
+  swap_qr_kernel<<<148 * 16, 256, 0, st>>>(src, n, dst);
+  return cudaGetLastError();
+}
 
 nw_status build_all(nw_ctx* ctx) {
   const int n = ctx->nmo, nao = ctx->nao, nref = ctx->nref;
@@ -401,6 +469,15 @@ nw_status build_all(nw_ctx* ctx) {
   double* tD = ar.take(n4);
   double* tE = ar.take(n4);
   if (!tE) return fail(ctx, NW_ERR_ALLOC, "build workspace too small");
+  // Cholesky route of the four-index tensors (nw_set_transform)
+  CholWork cw{};
+  const CholWork* cwp = nullptr;
+  if (ctx->transform != NW_TRANSFORM_FP64) {
+    if (!ctx->d_chol) return fail(ctx, NW_ERR_STATE, "Cholesky transform without Cholesky factors");
+    nw_status st = chol_work(ctx, n, &cw);
+    if (st != NW_OK) return st;
+    cwp = &cw;
+  }
 
   // ---------------- pairing ----------------
   {
@@ -633,9 +710,9 @@ nw_status build_all(nw_ctx* ctx) {
                                     Vv + (size_t)ps * 8 * n2, Vd + (size_t)ps * 8 * n2, n, recx, recy);
         NW_CUDA(ctx, cudaGetLastError());
         {
-          nw_status st = transform4(ctx, ctx->d_eri, n, CX(ps, 0), XC(ps, 0), CX(ps, 0), XC(ps, 0), tA, tD);
+          nw_status st = transform4(ctx, ctx->d_eri, n, CX(ps, 0), XC(ps, 0), CX(ps, 0), XC(ps, 0), tA, tD, cwp);
           if (st != NW_OK) return st;
-          st = transform4(ctx, ctx->d_eri, n, CX(ps, 0), CX(ps, 0), XC(ps, 0), XC(ps, 0), tA, tE);
+          st = transform4(ctx, ctx->d_eri, n, CX(ps, 0), CX(ps, 0), XC(ps, 0), XC(ps, 0), tA, tE, cwp);
           if (st != NW_OK) return st;
         }
         jas_kernel<<<g4, 256>>>(tD, tE, n, S0 + fo[p].jas[s]);
@@ -649,7 +726,7 @@ nw_status build_all(nw_ctx* ctx) {
         fs.g0 = tr[0] + 0.5 * tr[2];
       }
       {
-        nw_status st = transform4(ctx, ctx->d_eri, n, CX(psa, 0), XC(psa, 0), CX(psb, 0), XC(psb, 0), tA, tD);
+        nw_status st = transform4(ctx, ctx->d_eri, n, CX(psa, 0), XC(psa, 0), CX(psb, 0), XC(psb, 0), tA, tD, cwp);
         if (st != NW_OK) return st;
       }
       ii_kernel<<<g4, 256>>>(tD, n, S0 + fo[p].ii0);
@@ -686,9 +763,9 @@ nw_status build_all(nw_ctx* ctx) {
             continue;
           }
           const int a = br[sl][0], b = br[sl][1], c = br[sl][2], d = br[sl][3];
-          nw_status st = transform4(ctx, ctx->d_eri, n, CX(ps, a), XC(ps, b), CX(ps, c), XC(ps, d), tA, tD);
+          nw_status st = transform4(ctx, ctx->d_eri, n, CX(ps, a), XC(ps, b), CX(ps, c), XC(ps, d), tA, tD, cwp);
           if (st != NW_OK) return st;
-          st = transform4(ctx, ctx->d_eri, n, CX(ps, a), CX(ps, c), XC(ps, b), XC(ps, d), tA, tE);
+          st = transform4(ctx, ctx->d_eri, n, CX(ps, a), CX(ps, c), XC(ps, b), XC(ps, d), tA, tE, cwp);
           if (st != NW_OK) return st;
           jstored_kernel<<<g4, 256>>>(tD, tE, n, S0 + g.j[s][sl]);
           NW_CUDA(ctx, cudaGetLastError());
@@ -716,7 +793,7 @@ nw_status build_all(nw_ctx* ctx) {
           gp.ii[a0][az][b0][by] = nullptr;
           continue;
         }
-        nw_status st = transform4(ctx, ctx->d_eri, n, CX(psa, a0), XC(psa, az), CX(psb, b0), XC(psb, by), tA, tD);
+        nw_status st = transform4(ctx, ctx->d_eri, n, CX(psa, a0), XC(psa, az), CX(psb, b0), XC(psb, by), tA, tD, cwp);
         if (st != NW_OK) return st;
         ii_kernel<<<g4, 256>>>(tD, n, S0 + g.ii[k]);
         NW_CUDA(ctx, cudaGetLastError());
@@ -762,6 +839,11 @@ nw_status build_all(nw_ctx* ctx) {
   ctx->gen_host = hgen;
   ctx->generic_host = generic;
   NW_CUDA(ctx, cudaDeviceSynchronize());
+  if (cwp) {
+    uint32_t err = 0;
+    NW_CUDA(ctx, cudaMemcpy(&err, cw.err, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (err) return fail(ctx, NW_ERR_CUDA, "tcgen05 split product gave up waiting (flags " + std::to_string(err) + ")");
+  }
   ctx->built = true;
   return NW_OK;
 }

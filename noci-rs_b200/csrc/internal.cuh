@@ -58,6 +58,8 @@ struct nw_ctx {
   double* d_eri = nullptr;
   double* d_chol = nullptr; // naux x nao x nao Cholesky vectors (nw_ctx_create_cholesky), else null
   int naux = 0;
+  int transform = NW_TRANSFORM_FP64;  // four-index transform of the build (nw_set_transform)
+  nw::DevBuf chol_work;     // Cholesky-route factors, split pieces and error word of the build
   double* d_ca = nullptr;   // nref x nao x nmo
   double* d_cb = nullptr;
 
@@ -137,6 +139,15 @@ nw_status ensure(nw_ctx* ctx, DevBuf& b, size_t bytes);
 cudaError_t dgemm_strided(cudaStream_t stream, bool ta, bool tb, int M, int N, int K, double alpha, const double* A,
                           int lda, long long sa, const double* B, int ldb, long long sb, double beta, double* C,
                           int ldc, long long sc, int batch);
+
+// Cholesky-route product on tcgen05 (tc_gemm.cu): t4[p][r][q][s] = sum_k U[k][pq] V[k][rs] with
+// mode NW_TRANSFORM_CHOL_INT8 (slices int8 Ozaki slices, <= 8) or NW_TRANSFORM_CHOL_BF16X6.
+size_t split_product_scratch(int mode, int naux, int M, int N, int slices);
+cudaError_t split_product_pqrs(cudaStream_t st, int mode, int slices, const double* U, const double* V, int naux, int n,
+                               double* out, void* scratch, size_t scratch_bytes, uint32_t* err);
+constexpr int kOzakiSlices = 8;
+// [p][q][r][s] -> [p][r][q][s] of an n^4 tensor (build.cu).
+cudaError_t swap_qr(cudaStream_t st, const double* src, int n, double* dst);
 
 // Build (build.cu).
 nw_status build_all(nw_ctx* ctx);

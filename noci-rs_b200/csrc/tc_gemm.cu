@@ -1,0 +1,433 @@
+// Split-precision products on the 5th-generation tensor cores (tcgen05) for the Cholesky route
+// of the two-electron tensors.
+//
+// With Cholesky-factored integrals (mu nu|lam sig) = sum_P L^P[mu nu] L^P[lam sig], every
+// four-index transform of the build, T(A,B,C,D)[p,q,r,s] = sum (mu nu|lam sig) A[mu,p] B[nu,q]
+// C[lam,r] D[sig,s] (src/maths/eri.rs:258, the J and II tensors of
+// src/nonorthogonalwicks/build.rs:261-313,876-917), becomes one dense product
+//   T[pq][rs] = sum_P U[P][pq] V[P][rs],  U[P] = A^T L^P B,  V[P] = C^T L^P D,
+// an (n^2 x naux) x (naux x n^2) GEMM.  This file runs that product on tcgen05 from FP64 factors
+// in one of two split forms:
+//   * NW_TRANSFORM_CHOL_BF16X6: each factor entry is cut into three BF16 pieces (hi, mid, lo) and the six
+//     products of total order <= 2 are summed in FP32 in tensor memory (FP32-class result);
+//   * NW_TRANSFORM_CHOL_INT8: Ozaki-style integer slices.  Each row of U (and of V) is scaled by a power of
+//     two so its largest entry is at most 1/2, then cut into S signed 7-bit slices
+//     x = sum_i a_i 2^(-7 (i + 1)); the products of slices with i + j = s are summed exactly in
+//     INT32 in tensor memory (one accumulator per s), and the result is rebuilt in FP64 as
+//     sum_s 2^(e_row + e_col - 7 (s + 2)) C_s.  With S = 8 the result is FP64-faithful.
+//
+// Kernel shape: one CTA of 128 threads per 128 x 64 tile of T (cta_group::1, M = 128, N = 64).
+// Operands are pre-tiled in global memory by the split kernels in the tcgen05 no-swizzle K-major
+// layout (8-row x 16-byte core matrices), so each 128-byte-deep K tile of an operand is one
+// contiguous block moved by a single cp.async.bulk (no multicast) into a 6-stage ring of shared
+// memory, completion signalled on an mbarrier.  Thread 0 issues the copies, thread 32 the MMAs
+// (tcgen05.mma, one per 32-byte K step, then tcgen05.commit to free the stage); each product
+// (A piece, B piece) goes to its accumulator's 64 TMEM columns.  The epilogue loads the
+// accumulators with tcgen05.ld (warp w reads TMEM lanes 32w .. 32w + 31), rebuilds FP64 and
+// stores T in the [p][r][q][s] order of the build's T4 buffers.  Every mbarrier wait is bounded:
+// on a timeout the CTA records an error flag, stops issuing work, waits (bounded) for what it
+// issued, frees its tensor memory and returns.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "internal.cuh"
+
+namespace nw {
+namespace {
+
+constexpr int kTcThreads = 128;
+constexpr int kTileM = 128, kTileN = 64;
+constexpr int kKBytes = 128;                      // bytes of K per stage tile row
+constexpr int kStages = 6;                       // 144 KB of stages: one CTA per SM
+constexpr uint32_t kTileABytes = kTileM * kKBytes;  // 16 KB
+constexpr uint32_t kTileBBytes = kTileN * kKBytes;  // 8 KB
+constexpr int kMaxAcc = 8;                          // accumulators of 64 columns (512 TMEM columns)
+constexpr uint32_t kWaitLimit = 1u << 24;           // try_wait rounds before a wait gives up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// Waits for the phase of `parity` to complete; false after kWaitLimit unsuccessful rounds.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// Shared-memory matrix descriptor, no swizzle: start, leading-dimension byte offset (between
+// core matrices adjacent in K), stride byte offset (between 8-row groups), version 1.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor: D format (1 = F32, 2 = S32), A/B formats (kind::f16: 1 = BF16;
+// kind::i8: 1 = signed), both operands K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t idesc(uint32_t dfmt, uint32_t abfmt, uint32_t m, uint32_t n) {
+  return (dfmt << 4) | (abfmt << 7) | (abfmt << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
+}
+
+template <int kKind>  // 0: kind::f16 (BF16 in, F32 accumulate), 1: kind::i8 (S8 in, S32 accumulate)
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t accumulate) {
+  if constexpr (kKind == 0) {
+    constexpr uint32_t id = idesc(1, 1, kTileM, kTileN);
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            tmem),
+        "l"(ad), "l"(bd), "r"(id), "r"(accumulate));
+  } else {
+    constexpr uint32_t id = idesc(2, 1, kTileM, kTileN);
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            tmem),
+        "l"(ad), "l"(bd), "r"(id), "r"(accumulate));
+  }
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 8 consecutive 32-bit columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+struct TcArgs {
+  const uint8_t* a;        // pre-tiled A pieces: [piece][row tile][k tile][kTileABytes]
+  const uint8_t* b;        // pre-tiled B pieces: [piece][col tile][k tile][kTileBBytes]
+  long long a_piece, b_piece;  // bytes per piece
+  int nkt;                 // K tiles per piece
+  int mt, nt;              // row and column tiles
+  int nprod;               // products
+  int8_t pa[64], pb[64], pacc[64];  // per product: A piece, B piece, accumulator
+  int nacc;
+  double acc_scale[kMaxAcc];   // per accumulator: 2^(-7 (s + 2)) (int8) or 1 (bf16)
+  const int* erow;         // per row / column power-of-two exponents (int8), or null
+  const int* ecol;
+  int M, N;                // rows (pq) and columns (rs) of T
+  int n;                   // orbital count: T[pq][rs] is stored at [p][r][q][s]
+  double* out;
+  uint32_t* err;
+};
+
+template <int kKind>
+__global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_constant__ TcArgs g) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  // 1024-byte aligned stage ring: A tiles then B tiles; barriers after them
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* sa = smem;
+  uint8_t* sb = smem + kStages * kTileABytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sb + kStages * kTileBBytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* done = empty + kStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile uint32_t* abort_flag = tmem_slot + 1;
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tm = blockIdx.y, tn = blockIdx.x;
+  const uint32_t ncols = (uint32_t)g.nacc * kTileN <= 64 ? 64u
+                         : (uint32_t)g.nacc * kTileN <= 128 ? 128u
+                         : (uint32_t)g.nacc * kTileN <= 256 ? 256u : 512u;
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int nsteps = g.nprod * g.nkt;
+
+  if (tid == 0) {
+    // producer: one A tile and one B tile per step into the stage ring
+    int issued = 0;
+    for (int t = 0; t < nsteps; ++t) {
+      const int s = t % kStages, use = t / kStages;
+      if (use > 0 && !mbar_wait(&empty[s], (uint32_t)(use - 1) & 1u)) {
+        *abort_flag = 1;
+        atomicOr(g.err, 1u);
+        break;
+      }
+      if (*abort_flag) break;
+      const int p = t / g.nkt, kt = t % g.nkt;
+      const uint8_t* asrc = g.a + g.pa[p] * g.a_piece + ((long long)tm * g.nkt + kt) * kTileABytes;
+      const uint8_t* bsrc = g.b + g.pb[p] * g.b_piece + ((long long)tn * g.nkt + kt) * kTileBBytes;
+      mbar_expect_tx(&full[s], kTileABytes + kTileBBytes);
+      bulk_g2s(sa + s * kTileABytes, asrc, kTileABytes, &full[s]);
+      bulk_g2s(sb + s * kTileBBytes, bsrc, kTileBBytes, &full[s]);
+      ++issued;
+    }
+    // the copies of the last stages must have landed before the CTA may exit (on the normal
+    // path these phases completed long ago; after an abort they bound the wait for them)
+    for (int t = issued - kStages < 0 ? 0 : issued - kStages; t < issued; ++t)
+      if (!mbar_wait(&full[t % kStages], (uint32_t)(t / kStages) & 1u)) atomicOr(g.err, 8u);
+  } else if (tid == 32) {
+    // MMA issuer: four 32-byte K steps per stage into the product's accumulator
+    int issued = 0;
+    for (int t = 0; t < nsteps; ++t) {
+      const int s = t % kStages, use = t / kStages;
+      if (!mbar_wait(&full[s], (uint32_t)use & 1u)) {
+        *abort_flag = 1;
+        atomicOr(g.err, 2u);
+        break;
+      }
+      tc_fence_after();
+      const int p = t / g.nkt, kt = t % g.nkt;
+      const uint32_t dcol = tmem + (uint32_t)g.pacc[p] * kTileN;
+      // first K tile of the first product of each accumulator starts it
+      bool first = kt == 0;
+      for (int q = 0; q < p && first; ++q) first = g.pacc[q] != g.pacc[p];
+      const uint32_t a0 = smem_u32(sa + s * kTileABytes), b0 = smem_u32(sb + s * kTileBBytes);
+#pragma unroll
+      for (int k = 0; k < kKBytes / 32; ++k) {
+        const uint64_t ad = smem_desc(a0 + k * 256, 128, 1024);
+        const uint64_t bd = smem_desc(b0 + k * 256, 128, 1024);
+        mma<kKind>(dcol, ad, bd, (first && k == 0) ? 0u : 1u);
+      }
+      mma_commit(&empty[s]);
+      ++issued;
+    }
+    mma_commit(done);  // arrives once every MMA issued above has completed
+    (void)issued;
+  }
+  __syncwarp();
+  // epilogue: every thread owns row 32 warp + lane of the tile
+  const bool ok = mbar_wait(done, 0);
+  tc_fence_after();
+  if (!ok) atomicOr(g.err, 4u);
+  const int row = tm * kTileM + warp * 32 + (tid & 31);
+  // warp-uniform: tcgen05.ld is a whole-warp instruction
+  if (__all_sync(0xFFFFFFFFu, ok && !*abort_flag)) {
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    const int p = row / g.n, q = row % g.n;
+    const int er = g.erow && row < g.M ? g.erow[row] : 0;
+    for (int c8 = 0; c8 < kTileN; c8 += 8) {
+      double v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[j] = 0.0;
+      for (int a = 0; a < g.nacc; ++a) {
+        uint32_t r[8];
+        tmem_ld8(lane_base + (uint32_t)(a * kTileN + c8), r);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const double x = kKind == 0 ? (double)__uint_as_float(r[j]) : (double)(int32_t)r[j];
+          v[j] += g.acc_scale[a] * x;
+        }
+      }
+      if (row < g.M) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int col = tn * kTileN + c8 + j;
+          if (col >= g.N) break;
+          const int r = col / g.n, s = col % g.n;
+          const int ec = g.ecol ? g.ecol[col] : 0;
+          g.out[(((long long)p * g.n + r) * g.n + q) * g.n + s] = ldexp(v[j], er + ec);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+}
+
+// ---------------------------------------------------------------------------------------
+// Split kernels: FP64 factor F[k][row] (k < K, row < R; K-major rows of the product) into
+// pre-tiled pieces.  Tile (rt, kt) of piece c holds rows [rt * rows_t, +rows_t) and bytes
+// [kt * 128, +128) of K as core matrices [row group][16-byte K chunk][8 rows][16 bytes].
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ long long tiled_offset(int row, int kbyte, int rows_t, int nkt) {
+  const int rt = row / rows_t, rr = row % rows_t, kt = kbyte / kKBytes, kb = kbyte % kKBytes;
+  return ((long long)rt * nkt + kt) * (rows_t * kKBytes) + (long long)(rr / 8) * 8 * kKBytes +
+         (long long)(kb / 16) * 128 + (rr % 8) * 16 + (kb % 16);
+}
+
+// Per-row exponents e with max_k |F[k][row]| * 2^-e <= 1/2 (0 for an all-zero row).
+__global__ void row_exponent_kernel(const double* __restrict__ f, int K, int R, int* __restrict__ e) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < R; row += gridDim.x * blockDim.x) {
+    double mx = 0.0;
+    for (int k = 0; k < K; ++k) mx = fmax(mx, fabs(f[(long long)k * R + row]));
+    int ex = 0;
+    if (mx > 0.0) {
+      frexp(mx, &ex);   // mx = m 2^ex, m in [1/2, 1)
+      ex += 1;          // mx 2^-ex in [1/4, 1/2)
+    }
+    e[row] = ex;
+  }
+}
+
+// Ozaki slices: x = F / 2^e (|x| <= 1/2), a_0 = rint(x 2^7), then a_i = rint(r_i 2^7) of the
+// remainders; every slice fits a signed byte (|a_0| <= 64, later |a_i| <= 64).
+__global__ void int8_slices_kernel(const double* __restrict__ f, int K, int R, const int* __restrict__ e, int S,
+                                   int rows_t, int nkt, long long piece_bytes, int8_t* __restrict__ out) {
+  const long long total = (long long)K * R;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i / R), row = (int)(i % R);
+    double x = ldexp(f[i], -e[row]);
+    const long long off = tiled_offset(row, k, rows_t, nkt);
+    for (int c = 0; c < S; ++c) {
+      const double y = x * 128.0;
+      const double a = rint(y);
+      out[c * piece_bytes + off] = (int8_t)a;
+      x = y - a;
+    }
+  }
+}
+
+// BF16 pieces hi, mid, lo of each entry (round to nearest at each step).
+__global__ void bf16_pieces_kernel(const double* __restrict__ f, int K, int R, int rows_t, int nkt,
+                                   long long piece_bytes, uint8_t* __restrict__ out) {
+  const long long total = (long long)K * R;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i / R), row = (int)(i % R);
+    double x = f[i];
+    const long long off = tiled_offset(row, 2 * k, rows_t, nkt);
+    for (int c = 0; c < 3; ++c) {
+      const __nv_bfloat16 h = __double2bfloat16(x);
+      *reinterpret_cast<__nv_bfloat16*>(out + c * piece_bytes + off) = h;
+      x -= (double)__bfloat162float(h);
+    }
+  }
+}
+
+}  // namespace
+
+// Scratch of split_product_pqrs: pre-tiled pieces of both factors and the row exponents.
+size_t split_product_scratch(int mode, int naux, int M, int N, int slices) {
+  const int kbytes_per = mode == NW_TRANSFORM_CHOL_INT8 ? naux : 2 * naux;
+  const int nkt = (kbytes_per + kKBytes - 1) / kKBytes;
+  const int mt = (M + kTileM - 1) / kTileM, nt = (N + kTileN - 1) / kTileN;
+  const int pieces = mode == NW_TRANSFORM_CHOL_INT8 ? slices : 3;
+  const size_t a = (size_t)pieces * mt * nkt * kTileABytes, b = (size_t)pieces * nt * nkt * kTileBBytes;
+  return a + b + (size_t)(M + N) * sizeof(int) + 4096;
+}
+
+// T[p][r][q][s] = sum_k U[k][pq] V[k][rs] with the split products on tcgen05 (mode, slices).
+cudaError_t split_product_pqrs(cudaStream_t st, int mode, int slices, const double* U, const double* V, int naux, int n,
+                               double* out, void* scratch, size_t scratch_bytes, uint32_t* err) {
+  const int M = n * n, N = n * n;
+  if (mode != NW_TRANSFORM_CHOL_INT8 && mode != NW_TRANSFORM_CHOL_BF16X6) return cudaErrorInvalidValue;
+  if (mode == NW_TRANSFORM_CHOL_INT8 && (slices < 1 || slices > kMaxAcc)) return cudaErrorInvalidValue;
+  if (scratch_bytes < split_product_scratch(mode, naux, M, N, slices)) return cudaErrorInvalidValue;
+  const int kbytes_per = mode == NW_TRANSFORM_CHOL_INT8 ? naux : 2 * naux;
+  const int nkt = (kbytes_per + kKBytes - 1) / kKBytes;
+  const int mt = (M + kTileM - 1) / kTileM, nt = (N + kTileN - 1) / kTileN;
+  const int pieces = mode == NW_TRANSFORM_CHOL_INT8 ? slices : 3;
+  TcArgs g{};
+  g.a_piece = (long long)mt * nkt * kTileABytes;
+  g.b_piece = (long long)nt * nkt * kTileBBytes;
+  uint8_t* a = static_cast<uint8_t*>(scratch);
+  uint8_t* b = a + (size_t)pieces * g.a_piece;
+  int* erow = reinterpret_cast<int*>(b + (size_t)pieces * g.b_piece);
+  int* ecol = erow + M;
+  // zero padding (rows beyond M / N, K beyond naux)
+  cudaError_t e = cudaMemsetAsync(a, 0, (size_t)pieces * (g.a_piece + g.b_piece), st);
+  if (e != cudaSuccess) return e;
+  const int blocks = 148 * 8;
+  if (mode == NW_TRANSFORM_CHOL_INT8) {
+    row_exponent_kernel<<<(M + 255) / 256, 256, 0, st>>>(U, naux, M, erow);
+    row_exponent_kernel<<<(N + 255) / 256, 256, 0, st>>>(V, naux, N, ecol);
+    int8_slices_kernel<<<blocks, 256, 0, st>>>(U, naux, M, erow, slices, kTileM, nkt, g.a_piece,
+                                               reinterpret_cast<int8_t*>(a));
+    int8_slices_kernel<<<blocks, 256, 0, st>>>(V, naux, N, ecol, slices, kTileN, nkt, g.b_piece,
+                                               reinterpret_cast<int8_t*>(b));
+    // products of slices i + j = s into accumulator s, for s < slices
+    int np = 0;
+    for (int s = 0; s < slices; ++s)
+      for (int i = 0; i <= s; ++i) {
+        g.pa[np] = (int8_t)i;
+        g.pb[np] = (int8_t)(s - i);
+        g.pacc[np] = (int8_t)s;
+        ++np;
+      }
+    g.nprod = np;
+    g.nacc = slices;
+    for (int s = 0; s < slices; ++s) g.acc_scale[s] = ldexp(1.0, -7 * (s + 2));
+    g.erow = erow;
+    g.ecol = ecol;
+  } else {
+    bf16_pieces_kernel<<<blocks, 256, 0, st>>>(U, naux, M, kTileM, nkt, g.a_piece, a);
+    bf16_pieces_kernel<<<blocks, 256, 0, st>>>(V, naux, N, kTileN, nkt, g.b_piece, b);
+    // hi hi, hi mid, mid hi, hi lo, mid mid, lo hi: all into one FP32 accumulator
+    static const int8_t pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 0, 2, 1, 0};
+    for (int i = 0; i < 6; ++i) {
+      g.pa[i] = pa[i];
+      g.pb[i] = pb[i];
+      g.pacc[i] = 0;
+    }
+    g.nprod = 6;
+    g.nacc = 1;
+    g.acc_scale[0] = 1.0;
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  g.a = a;
+  g.b = b;
+  g.nkt = nkt;
+  g.mt = mt;
+  g.nt = nt;
+  g.M = M;
+  g.N = N;
+  g.n = n;
+  g.out = out;
+  g.err = err;
+  const size_t smem = kStages * (kTileABytes + kTileBBytes) + 1024 + 256;
+  const dim3 grid((unsigned)nt, (unsigned)mt);
+  if (mode == NW_TRANSFORM_CHOL_INT8) {
+    e = cudaFuncSetAttribute(tc_gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    tc_gemm_kernel<1><<<grid, kTcThreads, smem, st>>>(g);
+  } else {
+    e = cudaFuncSetAttribute(tc_gemm_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    tc_gemm_kernel<0><<<grid, kTcThreads, smem, st>>>(g);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace nw

@@ -29,6 +29,7 @@ _STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "allocation faile
            5: "call out of order", 6: "no CUDA device"}
 CONVENTIONS = {"reference": 0, "exact": 1}
 NOALLOC_MAX_PAIRS = 1 << 20
+TRANSFORMS = {"fp64": 0, "chol_fp64": 1, "chol_int8": 2, "chol_bf16x6": 3}
 
 
 class NwError(RuntimeError):
@@ -132,7 +133,7 @@ EXPORTED = ("nw_ctx_create", "nw_ctx_create_cholesky", "nw_build_intermediates",
             "nw_qmc_proposal_dims", "nw_qmc_mlp_params", "nw_qmc_set_mlp_params", "nw_qmc_mlp_loss_grad",
             "nw_qmc_proposal_probs", "nw_pt2_create", "nw_pt2_apply_m", "nw_pt2_last_apply_ms", "nw_pt2_solve",
             "nw_pt2_destroy", "nw_screen_create", "nw_screen_train", "nw_screen_predict", "nw_screen_destroy",
-            "nw_autotune", "nw_dgemm", "nw_sync",
+            "nw_autotune", "nw_dgemm", "nw_set_transform", "nw_transform_product", "nw_sync",
             "nw_set_timing", "nw_last_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
             "nw_last_error")
 
@@ -201,6 +202,8 @@ def load(path: Optional[str] = None):
     L.nw_dgemm.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                            vp, ctypes.c_int, ctypes.c_longlong, vp, ctypes.c_int, ctypes.c_longlong, ctypes.c_double,
                            vp, ctypes.c_int, ctypes.c_longlong, ctypes.c_int, vp]
+    L.nw_set_transform.argtypes = [vp, ctypes.c_int32]
+    L.nw_transform_product.argtypes = [ctypes.c_int32, vp, vp, ctypes.c_int32, ctypes.c_int32, vp, vp]
     L.nw_set_timing.argtypes = [vp, ctypes.c_int]
     L.nw_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     L.nw_ctx_info.argtypes = [vp, ctypes.POINTER(NwInfo)]
@@ -289,6 +292,13 @@ class WicksShared:
     # -- build / basis ---------------------------------------------------------------------
     def build(self):
         self._check(self._lib.nw_build_intermediates(self._ctx), "nw_build_intermediates")
+        return self
+
+    def set_transform(self, mode: str):
+        """Four-index transform of the next build: "fp64" (quarter transforms of the full
+        tensor), or on a Cholesky context "chol_fp64", "chol_int8" (tcgen05 Ozaki slices,
+        FP64-faithful) or "chol_bf16x6" (tcgen05 BF16 pieces, FP32 class)."""
+        self._check(self._lib.nw_set_transform(self._ctx, TRANSFORMS[mode]), "nw_set_transform")
         return self
 
     def zero_counts(self) -> np.ndarray:
