@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-qmc", action="store_true", help="skip the NOCI-QMC steps/s leg")
     ap.add_argument("--no-config3", action="store_true", help="skip the config-3 H/S leg")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision (Cholesky route) builds")
     ap.add_argument("--config3-npairs", type=int, default=100_000_000, help="pairs of the config-3 H/S leg")
     ap.add_argument("--qmc-reports", type=int, default=30, help="timed QMC report blocks (10 steps each)")
     ap.add_argument("--no-pt2", action="store_true", help="skip the NOCI-PT2 mat-vec / GMRES leg")
@@ -839,6 +840,65 @@ def config3_check(system, basis, pairs, gpu_hs, seconds: float, ngroups: int = 1
                                        + f", {cores} threads)"}}
 
 
+def mixed_leg(args, system, basis, pairs, hs_ref, fp64_build_s, fp64_eval_ms, local_rank):
+    """Mixed precision on the config-3 system (north_star's split products on tensor cores): the
+    Cholesky route of the J and II tensors, T[pq][rs] = sum_P U[P][pq] V[P][rs], built
+    (a) in FP64 on the FP64 tensor cores, (b) as int8 Ozaki slices on tcgen05 (exact int32 sums,
+    FP64-faithful), (c) as three BF16 pieces on tcgen05 (FP32 accumulation).  Per mode: build
+    time, the device pair rate, the one-shot rate (build + one evaluation of the batch), and
+    max / RMS |H - H_fp64| and max |S - S_fp64| over every pair of the batch against the FP64
+    build of the full Coulomb tensor, by reference-pair conditioning."""
+    import torch
+    import nociwick
+    npairs = pairs.shape[0]
+    dpairs = torch.from_numpy(pairs.view(np.int32)).to(f"cuda:{local_rank}")
+    dout = torch.empty((npairs, 2), dtype=torch.float64, device=f"cuda:{local_rank}")
+    stream = torch.cuda.current_stream()
+    smin = reference_pair_conditioning(system)
+    par = basis["parent"].astype(np.int64)
+    cond = smin[par[pairs[:, 0]] * len(system.refs) + par[pairs[:, 1]]]
+    out = {"fp64": {"build_seconds": fp64_build_s, "eval_ms": fp64_eval_ms,
+                    "one_shot_value": npairs / (fp64_build_s + fp64_eval_ms / 1e3),
+                    "note": "four FP64 quarter transforms of the full Coulomb tensor (the default build)"}}
+    for mode in ("chol_fp64", "chol_int8", "chol_bf16x6"):
+        eng = nociwick.WicksShared(system.s, system.h, None, system.enuc, system.refs, tol=1e-8, device=local_rank,
+                                   chol=system.chol)
+        eng.set_transform(mode)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.build()
+        build_s = time.perf_counter() - t0
+        eng.set_basis(basis)
+        for _ in range(2):
+            eng.eval_pairs_device(dpairs.data_ptr(), npairs, dout.data_ptr(), stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            eng.eval_pairs_device(dpairs.data_ptr(), npairs, dout.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        hs = dout.cpu().numpy()
+        eng.close()
+        dh = np.abs(hs[:, 0] - hs_ref[:, 0])
+        ds = np.abs(hs[:, 1] - hs_ref[:, 1])
+        buckets = {}
+        for nm, sel in (("s_min>=1e-2", cond >= 1e-2), ("1e-3<=s_min<1e-2", (cond >= 1e-3) & (cond < 1e-2)),
+                        ("s_min<1e-3", cond < 1e-3)):
+            if sel.any():
+                buckets[nm] = {"pairs": int(sel.sum()), "max_abs_err_h": float(dh[sel].max()),
+                               "rms_abs_err_h": float(np.sqrt(np.mean(dh[sel] ** 2)))}
+        out[mode] = {"build_seconds": build_s, "eval_ms": ms, "value": npairs / (ms / 1e3),
+                     "one_shot_value": npairs / (build_s + ms / 1e3),
+                     "max_abs_dh_vs_fp64": float(dh.max()), "rms_abs_dh_vs_fp64": float(np.sqrt(np.mean(dh ** 2))),
+                     "max_abs_ds_vs_fp64": float(ds.max()), "by_reference_pair_conditioning": buckets}
+    del dpairs, dout
+    torch.cuda.empty_cache()
+    out["note"] = ("the evaluator reads FP64 intermediates in every mode, so the device pair rate is the same; the "
+                   "split products change the build (the J / II tensors) and its accuracy")
+    return out
+
+
 def tail_summary(line):
     """The figures a reader of the end of the output needs, in a few hundred bytes."""
     out = {"hs_config2": {"value": line["value"], "e2e": line["e2e"]["value"], "frac": line["roofline"]["frac"]}}
@@ -850,6 +910,11 @@ def tail_summary(line):
         if chk:
             out["hs_config3"].update({"checked": chk["checked_pairs"], "max_err_h": chk["max_abs_err_h"],
                                       "rms_err_h": chk["rms_abs_err_h"], "cpu": chk["cpu_baseline"]["value"]})
+        mx = c3.get("mixed")
+        if mx:
+            out["mixed_config3"] = {m: {"build_s": v["build_seconds"], "one_shot": v["one_shot_value"],
+                                        "max_dh": v.get("max_abs_dh_vs_fp64")}
+                                    for m, v in mx.items() if isinstance(v, dict)}
     q = line.get("qmc")
     if q:
         out["qmc"] = {"steps_per_s": q["value"], "walkers": q["walkers_mean"]}
@@ -885,6 +950,9 @@ def run_ours(args, rank, world, local_rank):
                                                         local_rank, dist)
         if hs_host is not None:
             c3["oracle_check"] = config3_check(system, basis, pairs, hs_host, args.cpu_seconds)
+            if not args.no_mixed:
+                c3["mixed"] = mixed_leg(args, system, basis, pairs, hs_host, c3["config"]["build_seconds"],
+                                        c3["roofline"]["eval_ms"], local_rank)
         del system, basis, pairs, hs_host
     qmc = None if args.no_qmc else qmc_leg(args, rank, world, local_rank, dist)
     if rank != 0:

@@ -21,7 +21,7 @@ def _engine(system):
     return nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-12).build()
 
 
-@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("name", [n for n in NAMES if not n.startswith("QMC_")])
 def test_reference_noci_energy(name):
     system, meta = reffix.load(name)
     st, _ = sn.reference_states(len(system.refs), system.nocc_a, system.nocc_b)
@@ -55,3 +55,35 @@ def test_pt2_and_snoci_energies(name):
         assert abs(it.ecurrent + it.ept2 - expected["noci_pt2_energy"]) < 1e-8, (it.ecurrent + it.ept2, expected)
     else:
         assert abs(res.energy - expected["snoci_energy"]) < 1e-8, (res.energy, expected)
+
+
+@pytest.mark.parametrize("name", [n for n in NAMES if n.startswith("QMC_") and "TRAJECTORY_DDS2" in n])
+def test_qmc_trajectory_bounds(name):
+    """The reference's DDS-u2 trajectory fixtures (tests/qmc.rs:195-243, 499-545): a short
+    NOCI-QMC run with the fixture's qmc / prop blocks (uniform generator, 80 one-cycle reports
+    from 200 walkers towards 500) must give at least min_samples projected energies, all finite
+    and inside [min_energy, max_energy], spanning at least min_energy_span and ending at least
+    min_final_drop below the first.  The random stream is the engine's Philox, not the
+    reference's SmallRng, so the trajectory itself is not compared: only its bounds are."""
+    system, meta = reffix.load(name)
+    opt, exp = meta["qmc"], meta["expected"]
+    basis = sy.sd_basis(system.nmo, system.nocc_a, system.nocc_b, len(system.refs), orders=tuple(meta["orders"]),
+                        include_refs=True)
+    refs = np.nonzero((basis["rank_a"] == 0) & (basis["rank_b"] == 0))[0].astype(np.uint32)
+    with _engine(system) as w:
+        w.set_basis(basis)
+        hr, sr = w.build_hs_matrix(refs, refs)
+        er, cr = w.general_evp(hr, sr, project=True, tol=1e-12)
+        c0 = np.zeros(basis.shape[0])
+        c0[refs] = cr[:, 0]
+        with nociwick.Qmc(w, c0, refs, dt=opt["dt"], initial_population=opt["initial_population"],
+                          target_population=opt["target_population"], sampling_cutoff=opt["sampling_cutoff"],
+                          spawn_cutoff=opt["spawn_cutoff"], initial_shift=float(er[0]), ncycles=opt["ncycles"],
+                          propagator=opt["propagator"], seed=opt["seed"]) as q:
+            rep = q.run(opt["nreports"])
+    e = rep["eproj_num"] / rep["eproj_den"]
+    assert e.shape[0] >= exp["min_samples"]
+    assert np.all(np.isfinite(e))
+    assert np.all((e >= exp["min_energy"]) & (e <= exp["max_energy"])), (e.min(), e.max())
+    assert e.max() - e.min() >= exp["min_energy_span"], e
+    assert e[0] - e[-1] >= exp["min_final_drop"], (e[0], e[-1])

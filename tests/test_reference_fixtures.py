@@ -29,7 +29,7 @@ from oracle import linalg as LA
 from oracle.engine import DenseEngine
 from oracle.oracle import Oracle
 
-REF_NOCI = [n for n in reffix.names()]
+REF_NOCI = [n for n in reffix.names() if not n.startswith("QMC_")]
 DET = [n for n in reffix.names() if n.startswith("DET_")]
 PT2 = [n for n in reffix.names() if n.startswith("PT2_")]
 SNOCI = [n for n in reffix.names() if n.startswith("SNOCI_")]
