@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--no-qmc", action="store_true", help="skip the NOCI-QMC steps/s leg")
     ap.add_argument("--no-config3", action="store_true", help="skip the config-3 H/S leg")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision (Cholesky route) builds")
+    ap.add_argument("--no-autotune", action="store_true", help="default launch configuration (profiler captures)")
+    ap.add_argument("--snoci-exhaustive", action="store_true",
+                    help="also run the two SNOCI iterations exhaustively (matrix-free candidate M, minutes)")
     ap.add_argument("--config3-npairs", type=int, default=100_000_000, help="pairs of the config-3 H/S leg")
     ap.add_argument("--qmc-reports", type=int, default=30, help="timed QMC report blocks (10 steps each)")
     ap.add_argument("--no-pt2", action="store_true", help="skip the NOCI-PT2 mat-vec / GMRES leg")
@@ -487,6 +490,23 @@ def snoci_leg(args, rank, world, local_rank, dist):
     res = sn.snoci(w, system, it_opts, screener=ls)
     loop_s = time.perf_counter() - t0
     ls.close()
+    exhaustive_loop = None
+    if args.snoci_exhaustive:
+        # the same two iterations scored exhaustively: iteration 1's candidate M (3.7 TB packed)
+        # is applied matrix-free, every GMRES product evaluating its 4.6e11 pairs again
+        t0 = time.perf_counter()
+        res_x = sn.snoci(w, system, it_opts, screener=None)
+        exhaustive_loop = {"seconds": time.perf_counter() - t0, "energy": res_x.energy, "ept2": res_x.ept2,
+                           "energy_plus_ept2": res_x.energy + res_x.ept2,
+                           "learned_energy_plus_ept2": res.energy + res.ept2,
+                           "difference_mEh": 1e3 * ((res.energy + res.ept2) - (res_x.energy + res_x.ept2)),
+                           "e_current_difference_mEh": 1e3 * (res.energy - res_x.energy),
+                           "last_selection_overlap": len(set(res.added) & set(res_x.added)) / max(1, len(res_x.added)),
+                           "note": "the learned arm's E_PT2 sums only its kept candidates; the selections decide "
+                                   "the next variational energy",
+                           "iterations": [{"iteration": it.it, "pool": it.npool, "scored": it.nscored,
+                                           "seconds": it.seconds, "e_current": it.ecurrent, "ept2": it.ept2,
+                                           "gmres": it.gmres} for it in res_x.iterations]}
     w.close()
     iters = [{"iteration": it.it, "selected_space": it.nselected, "pool": it.npool, "scored": it.nscored,
               "screened": it.screened, "seconds": it.seconds, "e_current": it.ecurrent, "ept2": it.ept2,
@@ -512,7 +532,8 @@ def snoci_leg(args, rank, world, local_rank, dist):
                         "top200_recall": float(np.isin(top, keep).mean()),
                         "top200_recall_held_out": float(np.isin(held_out, keep).mean()) if held_out.size else None},
             "e_current": ecur, "e0": e0,
-            "two_iterations": {"seconds": loop_s, "iterations": iters,
+            "two_iterations_exhaustive": exhaustive_loop,
+            "two_iterations": {"seconds": loop_s, "energy": res.energy, "ept2": res.ept2, "iterations": iters,
                                "note": "snoci with the learned screener (keep 10 %): iteration 0 scores the "
                                        "whole pool and trains the screener, iteration 1 screens the grown "
                                        "pool, whose exhaustive M exceeds the 180 GB of HBM"},
@@ -679,7 +700,7 @@ def hs_leg(args, name, npairs, rank, world, local_rank, dist):
         torch.cuda.synchronize()
 
     # the engine's autotuner picks the fine-key budget and blocks per SM on this batch (untimed)
-    tune = eng.autotune(dpairs.data_ptr(), npairs, dout.data_ptr(), sh)
+    tune = None if args.no_autotune else eng.autotune(dpairs.data_ptr(), npairs, dout.data_ptr(), sh)
     for _ in range(max(3, args.warmup)):
         step_device()
     eng.sync(sh)

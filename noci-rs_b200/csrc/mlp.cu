@@ -1,7 +1,8 @@
 // Small MLP of the learned QMC proposal: forward, backward and Adam kernels (FP32 compute,
 // BF16 weight copies in the products, FP32 accumulation).  The network is tiny (din x 128,
 // 128 x 128, 128 x nout) and runs once per training step and once per determinant when the
-// proposal table is rebuilt, so one tiled product kernel serves every layer and pass.
+// proposal table is rebuilt, so one tiled product kernel serves every layer and pass; it runs
+// on the tensor cores as split-TF32 mma.sync products.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -25,25 +26,46 @@ __device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float
 
 enum Epi { kPlain = 0, kBiasRelu = 1, kBias = 2, kReluMask = 3 };
 
+// TF32 tensor-core product with a split of each operand into a TF32 head and a TF32 tail:
+// a b = a_h b_h + a_h b_t + a_t b_h + O(2^-22 |a b|), three m16n8k8 MMAs per step with FP32
+// accumulation, so the products keep FP32-class accuracy (the BF16 weight copies are exact
+// TF32 heads with a zero tail).
+__device__ __forceinline__ void split_tf32(float x, uint32_t& h, uint32_t& t) {
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+  const float r = x - __uint_as_float(h);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(r));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+               "{%0, %1, %2, %3};\n"
+               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
 // C[M x N] = epi(A[M x L] B[L x N]); A[i][l] = A[i * asr + l * asc], B[l][j] = B[l * bsr + j * bsc].
 // With gridDim.z > 1 the reduction range is split: block z covers [z * lsplit, (z + 1) * lsplit)
 // and writes its plain partial product to C + z * M * ldc (summed by splitk_sum_kernel).
+// A 64 x 64 tile per block of 8 warps (4 along M x 2 along N, each 16 x 32: four m16n8 tiles);
+// the panels are staged in shared memory k-major.
 template <typename TB>
 __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int L, const float* __restrict__ A, long asr, long asc,
                                                    const TB* __restrict__ B, long bsr, long bsc, float* __restrict__ C,
                                                    int ldc, int epi, const float* __restrict__ bias,
                                                    const float* __restrict__ mask, int lsplit) {
-  __shared__ float As[kL][kT + 1];
-  __shared__ float Bs[kL][kT + 1];
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  __shared__ float As[kL][kT + 8];  // row stride 72 floats: the fragment loads hit 32 distinct banks
+  __shared__ float Bs[kL][kT + 8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 3) * 16, wn = (warp >> 2) * 32;
   const int row0 = blockIdx.y * kT, col0 = blockIdx.x * kT;
   const int lbeg = blockIdx.z * lsplit, lend = min(L, lbeg + lsplit);
   C += (size_t)blockIdx.z * M * ldc;
   float acc[4][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int j = 0; j < 4; ++j)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+    for (int e = 0; e < 4; ++e) acc[j][e] = 0.0f;
   for (int l0 = lbeg; l0 < lend; l0 += kL) {
     for (int e = threadIdx.x; e < kT * kL; e += 256) {
       const int r = e / kL, c = e % kL, gr = row0 + r, gc = l0 + c;
@@ -55,26 +77,31 @@ __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int L, const fl
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < kL; ++k) {
-      float a[4], b[4];
+    for (int k0 = 0; k0 < kL; k0 += 8) {
+      uint32_t ah[4], at[4];
+      split_tf32(As[k0 + t][wm + g], ah[0], at[0]);
+      split_tf32(As[k0 + t][wm + g + 8], ah[1], at[1]);
+      split_tf32(As[k0 + t + 4][wm + g], ah[2], at[2]);
+      split_tf32(As[k0 + t + 4][wm + g + 8], ah[3], at[3]);
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[k][ty * 4 + i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[k][tx * 4 + j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+      for (int j = 0; j < 4; ++j) {
+        uint32_t bh[2], bt[2];
+        split_tf32(Bs[k0 + t][wn + j * 8 + g], bh[0], bt[0]);
+        split_tf32(Bs[k0 + t + 4][wn + j * 8 + g], bh[1], bt[1]);
+        mma_tf32(acc[j], at, bh);
+        mma_tf32(acc[j], ah, bt);
+        mma_tf32(acc[j], ah, bh);
+      }
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int j = 0; j < 4; ++j)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int r = row0 + ty * 4 + i, c = col0 + tx * 4 + j;
+    for (int e = 0; e < 4; ++e) {
+      const int r = row0 + wm + g + (e >> 1) * 8, c = col0 + wn + j * 8 + 2 * t + (e & 1);
       if (r >= M || c >= N) continue;
-      float v = acc[i][j];
+      float v = acc[j][e];
       if (epi == kBiasRelu) v = fmaxf(v + bias[c], 0.0f);
       if (epi == kBias) v += bias[c];
       if (epi == kReluMask) v = mask[(size_t)r * ldc + c] > 0.0f ? v : 0.0f;

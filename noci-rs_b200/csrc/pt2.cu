@@ -9,7 +9,10 @@
 //   mat-vec   : apply_candidate_m (operators.rs:375-488) with the stored matrix: one pass over
 //               the packed triangle in 256 x 256 tiles; a tile adds its row sums to y[rows] and,
 //               off the diagonal, its column sums to y[cols] (FP64 atomics, 512 per tile).  The
-//               triangle is streamed from HBM once per product.
+//               triangle is streamed from HBM once per product.  Without a stored matrix
+//               (nw_pt2_create_matrix_free, operators.rs:424-471) every product evaluates the
+//               upper-triangle (F, S) pairs again through the sorted pair pipeline, block by
+//               block, and accumulates them into y directly: no n^2 storage.
 //   projected : apply_omega_m / apply_projection_correction (operators.rs:696-955):
 //               y = M x - f_a0 (s_0a.x) - s_a0 (f_0a.x) + 2 E0 s_a0 (s_0a.x).
 //   GMRES     : gmres / run_arnoldi_cycle (src/snoci/gmres.rs:268-544): zero start, Arnoldi on
@@ -149,6 +152,61 @@ __global__ void upper_pairs_kernel(const uint32_t* __restrict__ cand, uint64_t n
   }
 }
 
+// Matrix-free product of one block of upper-triangle entries base .. base + count (rows from
+// r0): M_ab = F_ab - e0 S_ab, y[a] += M_ab x[b] and, off the diagonal, y[b] += M_ab x[a]
+// (apply_candidate_m without a cached matrix, src/snoci/operators.rs:424-471).  Each thread
+// takes kMfRun consecutive entries, which lie in one row except at row ends, and adds its row
+// sum with one atomic per row it touches; the column terms go out one atomic each.
+constexpr int kMfRun = 8;
+
+__global__ void mf_apply_kernel(const double2* __restrict__ fs, uint64_t n, uint64_t r0, uint64_t base,
+                                uint64_t count, double e0, const double* __restrict__ x, double* __restrict__ y) {
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) * kMfRun; k0 < count; k0 += nthreads * kMfRun) {
+    const uint64_t p0 = base + k0;
+    uint64_t lo = r0, hi = n;  // row of entry p0: largest a with row_start(a) <= p0
+    while (hi - lo > 1) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if (row_start(mid, n) <= p0)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    uint64_t a = lo, b = lo + (p0 - row_start(lo, n));
+    double xa = x[a], rowsum = 0.0;
+    const uint64_t kend = k0 + kMfRun < count ? k0 + kMfRun : count;
+    for (uint64_t k = k0; k < kend; ++k) {
+      if (b >= n) {  // next row
+        if (rowsum != 0.0) atomicAdd(y + a, rowsum);
+        ++a;
+        b = a;
+        xa = x[a];
+        rowsum = 0.0;
+      }
+      const double2 v = fs[k];
+      const double m = v.x - e0 * v.y;
+      rowsum = fma(m, x[b], rowsum);
+      if (b != a) {
+        const double cy = m * xa;
+        if (cy != 0.0) atomicAdd(y + b, cy);
+      }
+      ++b;
+    }
+    if (rowsum != 0.0) atomicAdd(y + a, rowsum);
+  }
+}
+
+// diagonal pairs (cand[a], cand[a])
+__global__ void diag_pairs_kernel(const uint32_t* __restrict__ cand, uint64_t n, uint2* __restrict__ pairs) {
+  for (uint64_t a = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; a < n; a += (uint64_t)gridDim.x * blockDim.x)
+    pairs[a] = make_uint2(cand[a], cand[a]);
+}
+
+__global__ void diag_fill_kernel(const double2* __restrict__ fs, uint64_t n, double e0, double* __restrict__ d) {
+  for (uint64_t a = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; a < n; a += (uint64_t)gridDim.x * blockDim.x)
+    d[a] = fs[a].x - e0 * fs[a].y;
+}
+
 __global__ void mul_kernel(const double* __restrict__ a, const double* __restrict__ b, uint64_t n,
                            double* __restrict__ out) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -163,9 +221,14 @@ struct nw_pt2 {
   nw_ctx* ctx = nullptr;
   uint64_t n = 0;
   double e0 = 0.0;
-  double* m = nullptr;      // packed upper triangle, n (n + 1) / 2
+  double* m = nullptr;      // packed upper triangle, n (n + 1) / 2 (null when matrix-free)
   double* mdiag = nullptr;  // diagonal of M
   float last_symv_ms = 0.0f;
+  // matrix-free mode: candidates, and one block of upper-triangle pairs and their (F, S)
+  uint32_t* dcand = nullptr;
+  uint2* pairs = nullptr;
+  double2* fs = nullptr;
+  uint64_t blk = 0;
 };
 
 namespace {
@@ -178,13 +241,41 @@ nw_status pfail(nw_pt2* p, nw_status s, const std::string& m) { return nw::fail(
     if (s_ != CUBLAS_STATUS_SUCCESS) return pfail(p, NW_ERR_CUDA, std::string(#call) + " failed"); \
   } while (0)
 
-// y = M x (device vectors, legacy stream).
+// First row of the packed entry `base`: largest r with row_start(r) <= base.
+uint64_t first_row(uint64_t base, uint64_t n) {
+  uint64_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (row_start(mid, n) <= base)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// y = M x (device vectors, legacy stream): one pass over the packed triangle, or, matrix-free,
+// every upper-triangle pair evaluated again through the (F, S) pipeline block by block.
 nw_status symv(nw_pt2* p, const double* x, double* y) {
   const uint64_t n = p->n, nb = (n + kTile - 1) / kTile;
-  const uint64_t ntiles = nb * (nb + 1) / 2;
   NW_CUDA(p->ctx, cudaMemsetAsync(y, 0, sizeof(double) * n, nullptr));
-  packed_symv_kernel<<<(unsigned)ntiles, kTile>>>(p->m, n, nb, x, y);
-  NW_CUDA(p->ctx, cudaGetLastError());
+  if (p->m) {
+    const uint64_t ntiles = nb * (nb + 1) / 2;
+    packed_symv_kernel<<<(unsigned)ntiles, kTile>>>(p->m, n, nb, x, y);
+    NW_CUDA(p->ctx, cudaGetLastError());
+    return NW_OK;
+  }
+  const uint64_t len = n * (n + 1) / 2;
+  for (uint64_t base = 0; base < len; base += p->blk) {
+    const uint64_t count = std::min(p->blk, len - base);
+    const uint64_t r0 = first_row(base, n);
+    upper_pairs_kernel<<<grid_n(count), 256>>>(p->dcand, n, r0, base, count, p->pairs);
+    nw_status st = nw::eval_pairs(p->ctx, reinterpret_cast<const uint32_t*>(p->pairs), count,
+                                  reinterpret_cast<double*>(p->fs), nw::EvalMode::kFS, nullptr);
+    if (st != NW_OK) return st;
+    mf_apply_kernel<<<grid_n((count + kMfRun - 1) / kMfRun), 256>>>(p->fs, n, r0, base, count, p->e0, x, y);
+    NW_CUDA(p->ctx, cudaGetLastError());
+  }
   return NW_OK;
 }
 
@@ -297,6 +388,44 @@ nw_status nw_pt2_create(nw_ctx* ctx, const uint32_t* cand, uint64_t n, double e0
   if (cudaDeviceSynchronize() != cudaSuccess) return cleanup(nw::fail(ctx, NW_ERR_CUDA, "candidate matrix build"));
   *out = p;
   return cleanup(NW_OK);
+}
+
+nw_status nw_pt2_create_matrix_free(nw_ctx* ctx, const uint32_t* cand, uint64_t n, double e0, nw_pt2** out) {
+  if (!out) return NW_ERR_INVALID;
+  *out = nullptr;
+  if (!ctx || !cand || n == 0 || !std::isfinite(e0)) return NW_ERR_INVALID;
+  if (!ctx->fock_ready) return nw::fail(ctx, NW_ERR_STATE, "Fock tables not set (nw_update_fock)");
+  if (!ctx->d_dets) return nw::fail(ctx, NW_ERR_STATE, "no determinant basis set");
+  if (n > 0x7FFFFFFFull) return nw::fail(ctx, NW_ERR_UNSUPPORTED, "too many candidates");
+  for (uint64_t i = 0; i < n; ++i)
+    if (cand[i] >= ctx->ndet) return nw::fail(ctx, NW_ERR_INVALID, "candidate index out of range");
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  nw_pt2* p = new (std::nothrow) nw_pt2;
+  if (!p) return NW_ERR_ALLOC;
+  p->ctx = ctx;
+  p->n = n;
+  p->e0 = e0;
+  constexpr uint64_t kBlock = 1ull << 24;  // pairs per evaluation block
+  p->blk = std::max(std::min(kBlock, n * (n + 1) / 2), n);  // a block also holds the n diagonal pairs
+  auto cleanup = [&](nw_status st) {
+    if (st != NW_OK) nw_pt2_destroy(p);
+    return st;
+  };
+  if (cudaMalloc(&p->dcand, sizeof(uint32_t) * n) != cudaSuccess || cudaMalloc(&p->mdiag, sizeof(double) * n) != cudaSuccess ||
+      cudaMalloc(&p->pairs, sizeof(uint2) * p->blk) != cudaSuccess ||
+      cudaMalloc(&p->fs, sizeof(double2) * p->blk) != cudaSuccess)
+    return cleanup(nw::fail(ctx, NW_ERR_ALLOC, "matrix-free candidate buffers"));
+  if (cudaMemcpy(p->dcand, cand, sizeof(uint32_t) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+    return cleanup(nw::fail(ctx, NW_ERR_CUDA, "candidate upload"));
+  // the diagonal for the preconditioners
+  diag_pairs_kernel<<<grid_n(n), 256>>>(p->dcand, n, p->pairs);
+  nw_status st = nw::eval_pairs(ctx, reinterpret_cast<const uint32_t*>(p->pairs), n, reinterpret_cast<double*>(p->fs),
+                                nw::EvalMode::kFS, nullptr);
+  if (st != NW_OK) return cleanup(st);
+  diag_fill_kernel<<<grid_n(n), 256>>>(p->fs, n, e0, p->mdiag);
+  if (cudaDeviceSynchronize() != cudaSuccess) return cleanup(nw::fail(ctx, NW_ERR_CUDA, "matrix-free set-up"));
+  *out = p;
+  return NW_OK;
 }
 
 nw_status nw_pt2_apply_m(nw_pt2* p, const double* x, double* y) {
@@ -508,8 +637,9 @@ nw_status nw_pt2_solve(nw_pt2* p, const nw_pt2_projection* proj, const double* r
 nw_status nw_pt2_destroy(nw_pt2* p) {
   if (!p) return NW_OK;
   cudaSetDevice(p->ctx->device);
-  if (p->m) cudaFree(p->m);
-  if (p->mdiag) cudaFree(p->mdiag);
+  cudaDeviceSynchronize();
+  for (void* q : {(void*)p->m, (void*)p->mdiag, (void*)p->dcand, (void*)p->pairs, (void*)p->fs})
+    if (q) cudaFree(q);
   delete p;
   return NW_OK;
 }

@@ -131,7 +131,7 @@ EXPORTED = ("nw_ctx_create", "nw_ctx_create_cholesky", "nw_build_intermediates",
             "nw_qmc_create", "nw_qmc_run", "nw_qmc_set_shift", "nw_qmc_last_run_ms", "nw_qmc_populations", "nw_qmc_set_populations", "nw_qmc_cycle_delta",
             "nw_qmc_destroy", "nw_qmc_harvest", "nw_qmc_train_proposal", "nw_qmc_set_generator",
             "nw_qmc_proposal_dims", "nw_qmc_mlp_params", "nw_qmc_set_mlp_params", "nw_qmc_mlp_loss_grad",
-            "nw_qmc_proposal_probs", "nw_pt2_create", "nw_pt2_apply_m", "nw_pt2_last_apply_ms", "nw_pt2_solve",
+            "nw_qmc_proposal_probs", "nw_pt2_create", "nw_pt2_create_matrix_free", "nw_pt2_apply_m", "nw_pt2_last_apply_ms", "nw_pt2_solve",
             "nw_pt2_destroy", "nw_screen_create", "nw_screen_train", "nw_screen_predict", "nw_screen_destroy",
             "nw_autotune", "nw_dgemm", "nw_set_transform", "nw_transform_product", "nw_sync",
             "nw_set_timing", "nw_last_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
@@ -188,6 +188,7 @@ def load(path: Optional[str] = None):
     L.nw_qmc_mlp_loss_grad.argtypes = [vp, vp, vp, vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_double), vp]
     L.nw_qmc_proposal_probs.argtypes = [vp, ctypes.c_uint32, vp]
     L.nw_pt2_create.argtypes = [vp, vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(vp)]
+    L.nw_pt2_create_matrix_free.argtypes = [vp, vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(vp)]
     L.nw_pt2_apply_m.argtypes = [vp, vp, vp]
     L.nw_pt2_last_apply_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     L.nw_pt2_solve.argtypes = [vp, ctypes.POINTER(NwPt2Projection), vp, ctypes.POINTER(NwGmresOpts), vp,
@@ -438,9 +439,10 @@ class WicksShared:
         return {"key_budget": rep.key_budget, "blocks_per_sm": rep.blocks_per_sm, "trials": rep.trials,
                 "best_ms": rep.best_ms, "default_ms": rep.default_ms}
 
-    def pt2(self, candidates, e0: float) -> "Pt2":
-        """The packed candidate matrix M = F - E0 S over resident determinants (nw_pt2_create)."""
-        return Pt2(self, candidates, e0)
+    def pt2(self, candidates, e0: float, matrix_free: bool = False) -> "Pt2":
+        """The candidate operator M = F - E0 S over resident determinants: packed on the device
+        (nw_pt2_create) or applied matrix-free (nw_pt2_create_matrix_free)."""
+        return Pt2(self, candidates, e0, matrix_free=matrix_free)
 
     def set_timing(self, enable: bool = True):
         self._check(self._lib.nw_set_timing(self._ctx, 1 if enable else 0), "nw_set_timing")
@@ -578,14 +580,17 @@ class Pt2:
     resident basis (packed on the device), its mat-vec and GMRES on the projected operator
     (build_candidate_m, apply_candidate_m, apply_omega_m and gmres of src/snoci)."""
 
-    def __init__(self, wicks: "WicksShared", candidates, e0: float):
+    def __init__(self, wicks: "WicksShared", candidates, e0: float, matrix_free: bool = False):
+        """With ``matrix_free`` M is not stored: every product evaluates its pairs again
+        (nw_pt2_create_matrix_free), O(n) device memory instead of n^2 / 2 doubles."""
         self._w = wicks
         self._lib = wicks._lib
         cand = np.ascontiguousarray(candidates, dtype=np.uint32)
         self.n = cand.shape[0]
         self._p = ctypes.c_void_p()
-        wicks._check(self._lib.nw_pt2_create(wicks._ctx, cand.ctypes.data, self.n, e0, ctypes.byref(self._p)),
-                     "nw_pt2_create")
+        fn = self._lib.nw_pt2_create_matrix_free if matrix_free else self._lib.nw_pt2_create
+        wicks._check(fn(wicks._ctx, cand.ctypes.data, self.n, e0, ctypes.byref(self._p)),
+                     "nw_pt2_create_matrix_free" if matrix_free else "nw_pt2_create")
 
     def apply_m(self, x) -> np.ndarray:
         """y = M x (apply_candidate_m)."""

@@ -279,6 +279,7 @@ class SnociOptions:
     keep_fraction: float = 0.25     # learned screener: share of the pool kept for PT2
     min_keep: int = 64
     audit: bool = False             # screened iterations also score the whole pool (the referee)
+    packed_m_max_bytes: float = 120e9   # above this the candidate M is applied matrix-free
 
 
 @dataclass
@@ -326,7 +327,9 @@ def pt2_scores(wicks, m: int, cand: np.ndarray, c: np.ndarray, ecurrent: float, 
     E0 = c^T F c, the projection contractions s_a0 = S_ai c, f_a0 = F_ai c (real states, so the
     transposed contractions are equal), V^Omega = H_ai c - E_current s_a0, GMRES on
     M^Omega a = -V^Omega, E_PT2 = a.M^Omega a + 2 a.V^Omega and the scores |a_a V_a^Omega|
-    (src/snoci/step.rs:265-441).  Returns (scores, E_PT2, E0, GMRES info)."""
+    (src/snoci/step.rs:265-441).  A candidate M larger than opts.packed_m_max_bytes is applied
+    matrix-free (apply_candidate_m without a cached matrix).  Returns (scores, E_PT2, E0, GMRES
+    info)."""
     cur = np.arange(m, dtype=np.uint32)
     cand = np.ascontiguousarray(cand, dtype=np.uint32)
     h_ai, s_ai = wicks.build_hs_matrix(cand, cur, symmetric=False)
@@ -336,7 +339,8 @@ def pt2_scores(wicks, m: int, cand: np.ndarray, c: np.ndarray, ecurrent: float, 
     s_a0 = s_ai @ c
     f_a0 = f_ai @ c
     v_omega = h_ai @ c - ecurrent * s_a0
-    with wicks.pt2(cand, e0) as pt:
+    matrix_free = 8.0 * cand.shape[0] * (cand.shape[0] + 1) / 2 > opts.packed_m_max_bytes
+    with wicks.pt2(cand, e0, matrix_free=matrix_free) as pt:
         amp, info = pt.solve(e0, s_a0, s_a0, f_a0, f_a0, -v_omega, max_iter=opts.gmres_max_iter,
                              restart=opts.gmres_restart, res_tol=opts.gmres_res_tol,
                              preconditioner=opts.preconditioner)

@@ -80,7 +80,8 @@ class DenseEngine:
         self.orc.set_fock(fa, fb)
         return self
 
-    def pt2(self, cand, e0: float) -> DensePt2:
+    def pt2(self, cand, e0: float, matrix_free: bool = False) -> DensePt2:
+        # the dense oracle forms M itself either way; matrix_free only selects the GPU storage mode
         return DensePt2(self, cand, e0)
 
     def close(self):

@@ -86,7 +86,7 @@ inline vd det_n(const vd* a) {
 template <int L, int K>
 inline vd minor_det(const vd* a, int r0, int r1, int c0, int c1) {
   if constexpr (K == 0) return splat(1.0);
-  vd mn[Sz<K * K>::v];
+  vd mn[Sz<K * K>::v] = {};
   int k = 0;
   for (int i = 0; i < L; ++i) {
     if (i == r0 || i == r1) continue;

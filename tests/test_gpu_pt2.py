@@ -89,3 +89,31 @@ def test_pt2_full_candidate_pool(snoci_system):
     ept2_ref = x_ref @ a @ x_ref + 2 * x_ref @ v
     assert abs(ept2 - ept2_ref) <= 1e-7
     assert np.linalg.norm(a @ x + v) / np.sqrt(cand.shape[0]) <= 1e-5
+
+
+def test_matrix_free_operator_matches_packed(snoci_system):
+    """nw_pt2_create_matrix_free (apply_candidate_m without a cached matrix,
+    src/snoci/operators.rs:424-471): M x re-evaluated pair by pair equals the packed product and
+    the dense oracle M x over candidates of every parent (most pairs nonorthogonal Wick pairs),
+    and GMRES through it reaches the packed solve's solution on the single-parent candidates."""
+    system, basis, h, s, f, refs, c, ecur, e0 = snoci_system
+    cand = np.nonzero((basis["rank_a"] + basis["rank_b"]) > 0)[0].astype(np.uint32)
+    one = np.nonzero((basis["parent"] == 0) & ((basis["rank_a"] + basis["rank_b"]) > 0))[0].astype(np.uint32)
+    m, _, _ = _pieces(h, s, f, refs, c, ecur, e0, cand)
+    _, p, v = _pieces(h, s, f, refs, c, ecur, e0, one)
+    xv = np.random.default_rng(2).normal(size=cand.shape[0])
+    with nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8).build() as w:
+        w.set_basis(basis)
+        w.update_fock(system.h, system.h)
+        with nociwick.Pt2(w, cand, e0) as pk, nociwick.Pt2(w, cand, e0, matrix_free=True) as mf:
+            y_pk, y_mf = pk.apply_m(xv), mf.apply_m(xv)
+        args = (e0, p["s_a0"], p["s_0a"], p["f_a0"], p["f_0a"], -v)
+        kw = dict(max_iter=100, restart=30, res_tol=1e-10, preconditioner="woodbury")
+        with nociwick.Pt2(w, one, e0) as pk, nociwick.Pt2(w, one, e0, matrix_free=True) as mf:
+            a_pk, info_pk = pk.solve(*args, **kw)
+            a_mf, info_mf = mf.solve(*args, **kw)
+    scale = np.abs(m) @ np.abs(xv)
+    assert np.all(np.abs(y_mf - m @ xv) <= 1e-12 * scale + 1e-14)
+    assert np.all(np.abs(y_mf - y_pk) <= 1e-12 * scale + 1e-14)
+    assert info_mf["converged"] and info_pk["converged"]
+    assert np.max(np.abs(a_mf - a_pk)) <= 1e-8 * max(1.0, np.max(np.abs(a_pk)))
