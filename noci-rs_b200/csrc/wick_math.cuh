@@ -1150,8 +1150,8 @@ NW_HD void minor_ct(double (&out)[Sq<L - 1>::v], const double (&a)[Sq<L>::v], in
   }
 }
 
-template <int L>
-NW_HD void same_spin_gen_ct(const GenSpinIn& w, int n, const int* rows, const int* cols, const double (&d0)[Sq<L>::v],
+template <int L, typename SpinTab>
+NW_HD void same_spin_gen_ct(const SpinTab& w, int n, const int* rows, const int* cols, const double (&d0)[Sq<L>::v],
                             const double (&d1)[Sq<L>::v], double tol, bool exact, double* s_out, double* h1_out,
                             double* h2_out) {
   const int64_t n2 = (int64_t)n * n, n3 = n2 * n;
@@ -1246,8 +1246,8 @@ NW_HD void same_spin_gen_ct(const GenSpinIn& w, int n, const int* rows, const in
   *h2_out = h2;
 }
 
-template <int LA, int LB>
-NW_HD double diff_spin_gen_ct(const GenDiffIn& w, int n, int ma, int mb, const int* rows_a, const int* cols_a,
+template <int LA, int LB, typename DiffTab>
+NW_HD double diff_spin_gen_ct(const DiffTab& w, int n, int ma, int mb, const int* rows_a, const int* cols_a,
                               const double (&da0)[Sq<LA>::v], const double (&da1)[Sq<LA>::v], const int* rows_b,
                               const int* cols_b, const double (&db0)[Sq<LB>::v], const double (&db1)[Sq<LB>::v],
                               double tol, bool exact) {
@@ -1339,13 +1339,13 @@ NW_HD void eval_gen_ct(const GenPair& g, const DetRec& x, const DetRec& w, int n
   build_d_ct<LA>(da1, g.a.x[1], g.a.y[1], n, ra, ca);
   build_d_ct<LB>(db0, g.b.x[0], g.b.y[0], n, rb, cb);
   build_d_ct<LB>(db1, g.b.x[1], g.b.y[1], n, rb, cb);
-  GenSpinIn wa, wb;
-  GenDiffIn wd;
-  gen_inputs(g, &wa, &wb, &wd);
+  // the tables are read where they lie (the reference pair's GenPair record, global memory on
+  // the device): copying their ~100 pointers into per-thread structs indexed at run time put
+  // them in local memory
   double sa, h1a, h2aa, sb, h1b, h2bb;
-  same_spin_gen_ct<LA>(wa, n, ra, ca, da0, da1, tol, exact, &sa, &h1a, &h2aa);
-  same_spin_gen_ct<LB>(wb, n, rb, cb, db0, db1, tol, exact, &sb, &h1b, &h2bb);
-  const double h2ab = diff_spin_gen_ct<LA, LB>(wd, n, g.a.m, g.b.m, ra, ca, da0, da1, rb, cb, db0, db1, tol, exact);
+  same_spin_gen_ct<LA>(g.a, n, ra, ca, da0, da1, tol, exact, &sa, &h1a, &h2aa);
+  same_spin_gen_ct<LB>(g.b, n, rb, cb, db0, db1, tol, exact, &sb, &h1b, &h2bb);
+  const double h2ab = diff_spin_gen_ct<LA, LB>(g, n, g.a.m, g.b.m, ra, ca, da0, da1, rb, cb, db0, db1, tol, exact);
   const double pref = x.phase * w.phase * g.a.pref * g.b.pref;
   const double s = pref * sa * sb;
   double h = pref * (h1a * sb + h1b * sa + 0.5 * h2aa * sb + 0.5 * h2bb * sa + h2ab);
