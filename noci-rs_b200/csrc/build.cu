@@ -321,55 +321,92 @@ __global__ void swap_qr_kernel(const double* __restrict__ src, int n, double* __
   }
 }
 
-// Cholesky-route workspace: W and the factors U, V (naux x n^2 each), the split pieces of the
-// tcgen05 product, and its error word.
+// Cholesky-route workspace: W = L^P B (naux x n^2), a small cache of factors U = A^T L^P B keyed
+// by the (A, B) pair they come from (FP64 for NW_TRANSFORM_CHOL_FP64, split pieces for the
+// tcgen05 modes: a pair's J and II tensors share six distinct factors, so each is computed and
+// split once), and the error word of the split products.
+constexpr int kFactorCache = 6;
 struct CholWork {
-  double *W, *U, *V;
-  void* split;
-  size_t split_bytes;
-  uint32_t* err;
+  double* W = nullptr;
+  double* F = nullptr;                     // FP64 factor scratch before splitting
+  double* fac[kFactorCache] = {};          // FP64 factors (CHOL_FP64)
+  char* split[kFactorCache] = {};          // split pieces (tcgen05 modes)
+  SplitFactor sf[kFactorCache] = {};
+  const double* ka[kFactorCache] = {};
+  const double* kb[kFactorCache] = {};
+  int next = 0;
+  size_t split_bytes = 0;
+  uint32_t* err = nullptr;
 };
 
 nw_status chol_work(nw_ctx* ctx, int n, CholWork* w) {
-  const size_t fac = (size_t)ctx->naux * n * n;
-  const int mode = ctx->transform == NW_TRANSFORM_CHOL_FP64 ? NW_TRANSFORM_CHOL_INT8 : ctx->transform;
-  const size_t split = ctx->transform == NW_TRANSFORM_CHOL_FP64
-                           ? 0
-                           : split_product_scratch(mode, ctx->naux, n * n, n * n, kOzakiSlices);
-  const size_t bytes = 3 * fac * sizeof(double) + split + 1024;
+  const size_t fac = (size_t)ctx->naux * n * n, fb = fac * sizeof(double);
+  const bool fp64 = ctx->transform == NW_TRANSFORM_CHOL_FP64;
+  const size_t split = fp64 ? 0 : (split_factor_bytes(ctx->transform, ctx->naux, n * n) + 255) / 256 * 256;
+  const size_t per = fp64 ? fb : split;
+  const size_t bytes = 2 * fb + kFactorCache * per + 1024;
   nw_status st = ensure(ctx, ctx->chol_work, bytes);
   if (st != NW_OK) return st;
   char* base = static_cast<char*>(ctx->chol_work.p);
+  *w = CholWork{};
   w->W = reinterpret_cast<double*>(base);
-  w->U = w->W + fac;
-  w->V = w->U + fac;
-  w->err = reinterpret_cast<uint32_t*>(w->V + fac);
-  w->split = reinterpret_cast<char*>(w->V + fac) + 256;
+  w->F = w->W + fac;
+  char* q = base + 2 * fb;
+  for (int i = 0; i < kFactorCache; ++i, q += per) {
+    if (fp64)
+      w->fac[i] = reinterpret_cast<double*>(q);
+    else
+      w->split[i] = q;
+  }
   w->split_bytes = split;
+  w->err = reinterpret_cast<uint32_t*>(q);
   NW_CUDA(ctx, cudaMemsetAsync(w->err, 0, sizeof(uint32_t)));
   return NW_OK;
 }
 
-// The Cholesky route of T(A,B,C,D), result in [p][r][q][s] in t4 (t1 is n^4 scratch):
-// U[P] = A^T L^P B, V[P] = C^T L^P D (batched FP64 products), T[pq][rs] = sum_P U[P][pq] V[P][rs]
-// in FP64 (NW_TRANSFORM_CHOL_FP64) or as split products on tcgen05 (tc_gemm.cu).
-nw_status transform4_chol(nw_ctx* ctx, int n, const double* A, const double* B, const double* C, const double* D,
-                          double* t1, double* t4, const CholWork& w) {
+// Index of the cached factor A^T L^P B, computed (and split) on a miss; `keep` is never evicted.
+nw_status chol_factor(nw_ctx* ctx, int n, const double* A, const double* B, CholWork& w, int keep, int* out) {
+  for (int i = 0; i < kFactorCache; ++i)
+    if (w.ka[i] == A && w.kb[i] == B) {
+      *out = i;
+      return NW_OK;
+    }
+  int i = w.next;
+  if (i == keep) i = (i + 1) % kFactorCache;
+  w.next = (i + 1) % kFactorCache;
   const cudaStream_t h = 0;
   const long long n2 = (long long)n * n;
   const int naux = ctx->naux;
+  const bool fp64 = ctx->transform == NW_TRANSFORM_CHOL_FP64;
+  double* U = fp64 ? w.fac[i] : w.F;
   NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, ctx->d_chol, n, n2, B, n, 0, 0.0, w.W, n, n2, naux));
-  NW_DG(ctx, gemm_b(h, true, false, n, n, n, 1.0, A, n, 0, w.W, n, n2, 0.0, w.U, n, n2, naux));
-  NW_DG(ctx, gemm_b(h, false, false, n, n, n, 1.0, ctx->d_chol, n, n2, D, n, 0, 0.0, w.W, n, n2, naux));
-  NW_DG(ctx, gemm_b(h, true, false, n, n, n, 1.0, C, n, 0, w.W, n, n2, 0.0, w.V, n, n2, naux));
+  NW_DG(ctx, gemm_b(h, true, false, n, n, n, 1.0, A, n, 0, w.W, n, n2, 0.0, U, n, n2, naux));
+  if (!fp64) NW_DG(ctx, split_factor(h, ctx->transform, U, naux, (int)n2, w.split[i], w.split_bytes, &w.sf[i]));
+  w.ka[i] = A;
+  w.kb[i] = B;
+  *out = i;
+  return NW_OK;
+}
+
+// The Cholesky route of T(A,B,C,D), result in [p][r][q][s] in t4 (t1 is n^4 scratch):
+// U[P] = A^T L^P B, V[P] = C^T L^P D (batched FP64 products, cached), T[pq][rs] = sum_P
+// U[P][pq] V[P][rs] in FP64 (NW_TRANSFORM_CHOL_FP64) or as split products on tcgen05 (tc_gemm.cu).
+nw_status transform4_chol(nw_ctx* ctx, int n, const double* A, const double* B, const double* C, const double* D,
+                          double* t1, double* t4, CholWork& w) {
+  const cudaStream_t h = 0;
+  const long long n2 = (long long)n * n;
+  int iu = -1, iv = -1;
+  nw_status st = chol_factor(ctx, n, A, B, w, -1, &iu);
+  if (st == NW_OK) st = chol_factor(ctx, n, C, D, w, iu, &iv);
+  if (st != NW_OK) return st;
   if (ctx->transform == NW_TRANSFORM_CHOL_FP64) {
-    NW_DG(ctx, gemm(h, true, false, (int)n2, (int)n2, naux, 1.0, w.U, (int)n2, w.V, (int)n2, 0.0, t1, (int)n2));
+    NW_DG(ctx, gemm(h, true, false, (int)n2, (int)n2, ctx->naux, 1.0, w.fac[iu], (int)n2, w.fac[iv], (int)n2, 0.0, t1,
+                    (int)n2));
     swap_qr_kernel<<<148 * 16, 256>>>(t1, n, t4);
     NW_CUDA(ctx, cudaGetLastError());
     return NW_OK;
   }
-  NW_DG(ctx, split_product_pqrs(h, ctx->transform, kOzakiSlices, w.U, w.V, naux, n, t4, w.split, w.split_bytes,
-                                w.err));
+  NW_DG(ctx, split_product(h, w.sf[iu], w.sf[iv], n, t4, w.err));
   return NW_OK;
 }
 
@@ -377,7 +414,7 @@ nw_status transform4_chol(nw_ctx* ctx, int n, const double* A, const double* B, 
 // result in layout [p][r][q][s] in t4.  t1 is scratch of n^4 doubles (nao == nmo here).  A
 // Cholesky transform mode takes the factored route instead.
 nw_status transform4(nw_ctx* ctx, const double* eri, int n, const double* A, const double* B, const double* C,
-                     const double* D, double* t1, double* t4, const CholWork* cw = nullptr) {
+                     const double* D, double* t1, double* t4, CholWork* cw = nullptr) {
   if (cw) return transform4_chol(ctx, n, A, B, C, D, t1, t4, *cw);
   const cudaStream_t h = 0;  // the build runs on the legacy default stream
   const long long n2 = (long long)n * n, n3 = n2 * n;
@@ -471,7 +508,7 @@ nw_status build_all(nw_ctx* ctx) {
   if (!tE) return fail(ctx, NW_ERR_ALLOC, "build workspace too small");
   // Cholesky route of the four-index tensors (nw_set_transform)
   CholWork cw{};
-  const CholWork* cwp = nullptr;
+  CholWork* cwp = nullptr;
   if (ctx->transform != NW_TRANSFORM_FP64) {
     if (!ctx->d_chol) return fail(ctx, NW_ERR_STATE, "Cholesky transform without Cholesky factors");
     nw_status st = chol_work(ctx, n, &cw);

@@ -141,11 +141,23 @@ cudaError_t dgemm_strided(cudaStream_t stream, bool ta, bool tb, int M, int N, i
                           int ldc, long long sc, int batch);
 
 // Cholesky-route product on tcgen05 (tc_gemm.cu): t4[p][r][q][s] = sum_k U[k][pq] V[k][rs] with
-// mode NW_TRANSFORM_CHOL_INT8 (slices int8 Ozaki slices, <= 8) or NW_TRANSFORM_CHOL_BF16X6.
+// mode NW_TRANSFORM_CHOL_INT8 (8 int8 Ozaki slices) or NW_TRANSFORM_CHOL_BF16X6 (3 BF16 pieces).
+constexpr int kOzakiSlices = 8;
+// A factor F[k][row] (naux x R) split into pre-tiled pieces (and, for int8, per-row exponents).
+struct SplitFactor {
+  int mode, R, rpad, nkt;
+  long long piece_bytes;
+  uint8_t* pieces;
+  int* exps;
+};
+size_t split_factor_bytes(int mode, int naux, int R);
+cudaError_t split_factor(cudaStream_t st, int mode, const double* F, int naux, int R, void* buf, size_t bytes,
+                         SplitFactor* out);
+cudaError_t split_product(cudaStream_t st, const SplitFactor& A, const SplitFactor& B, int n, double* out,
+                          uint32_t* err);
 size_t split_product_scratch(int mode, int naux, int M, int N, int slices);
 cudaError_t split_product_pqrs(cudaStream_t st, int mode, int slices, const double* U, const double* V, int naux, int n,
                                double* out, void* scratch, size_t scratch_bytes, uint32_t* err);
-constexpr int kOzakiSlices = 8;
 // [p][q][r][s] -> [p][r][q][s] of an n^4 tensor (build.cu).
 cudaError_t swap_qr(cudaStream_t st, const double* src, int n, double* dst);
 

@@ -30,6 +30,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "internal.cuh"
@@ -124,11 +125,11 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 struct TcArgs {
-  const uint8_t* a;        // pre-tiled A pieces: [piece][row tile][k tile][kTileABytes]
-  const uint8_t* b;        // pre-tiled B pieces: [piece][col tile][k tile][kTileBBytes]
+  const uint8_t* a;        // pre-tiled A pieces: [piece][k tile][64-row tile][8 KB]
+  const uint8_t* b;        // pre-tiled B pieces, same layout
   long long a_piece, b_piece;  // bytes per piece
   int nkt;                 // K tiles per piece
-  int mt, nt;              // row and column tiles
+  int nrt_a, nrt_b;        // 64-row tiles of each operand (rows padded to 128)
   int nprod;               // products
   int8_t pa[64], pb[64], pacc[64];  // per product: A piece, B piece, accumulator
   int nacc;
@@ -192,8 +193,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
       }
       if (*abort_flag) break;
       const int p = t / g.nkt, kt = t % g.nkt;
-      const uint8_t* asrc = g.a + g.pa[p] * g.a_piece + ((long long)tm * g.nkt + kt) * kTileABytes;
-      const uint8_t* bsrc = g.b + g.pb[p] * g.b_piece + ((long long)tn * g.nkt + kt) * kTileBBytes;
+      // a 128-row A tile is the two adjacent 64-row tiles 2 tm, 2 tm + 1 of its K tile
+      const uint8_t* asrc = g.a + g.pa[p] * g.a_piece + ((long long)kt * g.nrt_a + 2 * tm) * kTileBBytes;
+      const uint8_t* bsrc = g.b + g.pb[p] * g.b_piece + ((long long)kt * g.nrt_b + tn) * kTileBBytes;
       mbar_expect_tx(&full[s], kTileABytes + kTileBBytes);
       bulk_g2s(sa + s * kTileABytes, asrc, kTileABytes, &full[s]);
       bulk_g2s(sb + s * kTileBBytes, bsrc, kTileBBytes, &full[s]);
@@ -276,21 +278,23 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
 }
 
 // ---------------------------------------------------------------------------------------
-// Split kernels: FP64 factor F[k][row] (k < K, row < R; K-major rows of the product) into
-// pre-tiled pieces.  Tile (rt, kt) of piece c holds rows [rt * rows_t, +rows_t) and bytes
-// [kt * 128, +128) of K as core matrices [row group][16-byte K chunk][8 rows][16 bytes].
+// Split kernels: FP64 factor F[k][row] (k < K, row < R; the K-major rows of the product) into
+// pieces in one pre-tiled layout shared by both operands: piece c holds, for each 128-byte K
+// tile kt and each 64-row tile rt, 8 KB of core matrices [row group of 8][16-byte K chunk]
+// [8 rows][16 bytes] at ((c * nkt + kt) * nrt + rt) * 8 KB; rows are padded to a multiple of
+// 128 with zeros, so a 128-row A tile is two adjacent 64-row tiles.
 // ---------------------------------------------------------------------------------------
-__device__ __forceinline__ long long tiled_offset(int row, int kbyte, int rows_t, int nkt) {
-  const int rt = row / rows_t, rr = row % rows_t, kt = kbyte / kKBytes, kb = kbyte % kKBytes;
-  return ((long long)rt * nkt + kt) * (rows_t * kKBytes) + (long long)(rr / 8) * 8 * kKBytes +
-         (long long)(kb / 16) * 128 + (rr % 8) * 16 + (kb % 16);
+__device__ __forceinline__ long long chunk_offset(int row, int kc, int nrt) {
+  const int kt = kc >> 3, c = kc & 7;
+  return ((long long)kt * nrt + (row >> 6)) * kTileBBytes + ((row & 63) >> 3) * 1024 + c * 128 + (row & 7) * 16;
 }
 
-// Per-row exponents e with max_k |F[k][row]| * 2^-e <= 1/2 (0 for an all-zero row).
-__global__ void row_exponent_kernel(const double* __restrict__ f, int K, int R, int* __restrict__ e) {
-  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < R; row += gridDim.x * blockDim.x) {
+// Per-row exponents e with max_k |F[k][row]| * 2^-e <= 1/2 (0 for an all-zero or padding row).
+__global__ void row_exponent_kernel(const double* __restrict__ f, int K, int R, int rpad, int* __restrict__ e) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < rpad; row += gridDim.x * blockDim.x) {
     double mx = 0.0;
-    for (int k = 0; k < K; ++k) mx = fmax(mx, fabs(f[(long long)k * R + row]));
+    if (row < R)
+      for (int k = 0; k < K; ++k) mx = fmax(mx, fabs(f[(long long)k * R + row]));
     int ex = 0;
     if (mx > 0.0) {
       frexp(mx, &ex);   // mx = m 2^ex, m in [1/2, 1)
@@ -300,86 +304,119 @@ __global__ void row_exponent_kernel(const double* __restrict__ f, int K, int R, 
   }
 }
 
-// Ozaki slices: x = F / 2^e (|x| <= 1/2), a_0 = rint(x 2^7), then a_i = rint(r_i 2^7) of the
-// remainders; every slice fits a signed byte (|a_0| <= 64, later |a_i| <= 64).
-__global__ void int8_slices_kernel(const double* __restrict__ f, int K, int R, const int* __restrict__ e, int S,
-                                   int rows_t, int nkt, long long piece_bytes, int8_t* __restrict__ out) {
-  const long long total = (long long)K * R;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(i / R), row = (int)(i % R);
-    double x = ldexp(f[i], -e[row]);
-    const long long off = tiled_offset(row, k, rows_t, nkt);
+// Ozaki slices of one 16-byte chunk (16 consecutive k of one row) per thread: x = F / 2^e
+// (|x| <= 1/2), a_0 = rint(x 2^7), then a_i = rint(r_i 2^7) of the remainders (every slice fits
+// a signed byte, |a_i| <= 64); one 16-byte store per slice.
+__global__ void int8_slices_kernel(const double* __restrict__ f, int K, int R, int rpad, int nkt,
+                                   const int* __restrict__ e, int S, long long piece_bytes, uint8_t* __restrict__ out) {
+  const long long total = (long long)rpad * nkt * 8;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int row = (int)(t % rpad), kc = (int)(t / rpad);
+    double x[16];
+    const int ex = e[row];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int k = kc * 16 + j;
+      x[j] = (row < R && k < K) ? ldexp(f[(long long)k * R + row], -ex) : 0.0;
+    }
+    const long long off = chunk_offset(row, kc, rpad >> 6);
     for (int c = 0; c < S; ++c) {
-      const double y = x * 128.0;
-      const double a = rint(y);
-      out[c * piece_bytes + off] = (int8_t)a;
-      x = y - a;
+      uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const double y = x[j] * 128.0;
+        const double a = rint(y);
+        x[j] = y - a;
+        w[j >> 2] |= ((uint32_t)(int32_t)a & 0xFFu) << (8 * (j & 3));
+      }
+      *reinterpret_cast<uint4*>(out + c * piece_bytes + off) = make_uint4(w[0], w[1], w[2], w[3]);
     }
   }
 }
 
-// BF16 pieces hi, mid, lo of each entry (round to nearest at each step).
-__global__ void bf16_pieces_kernel(const double* __restrict__ f, int K, int R, int rows_t, int nkt,
+// BF16 pieces hi, mid, lo (round to nearest at each step) of one 16-byte chunk (8 consecutive k
+// of one row) per thread.
+__global__ void bf16_pieces_kernel(const double* __restrict__ f, int K, int R, int rpad, int nkt,
                                    long long piece_bytes, uint8_t* __restrict__ out) {
-  const long long total = (long long)K * R;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(i / R), row = (int)(i % R);
-    double x = f[i];
-    const long long off = tiled_offset(row, 2 * k, rows_t, nkt);
+  const long long total = (long long)rpad * nkt * 8;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int row = (int)(t % rpad), kc = (int)(t / rpad);
+    double x[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int k = kc * 8 + j;
+      x[j] = (row < R && k < K) ? f[(long long)k * R + row] : 0.0;
+    }
+    const long long off = chunk_offset(row, kc, rpad >> 6);
     for (int c = 0; c < 3; ++c) {
-      const __nv_bfloat16 h = __double2bfloat16(x);
-      *reinterpret_cast<__nv_bfloat16*>(out + c * piece_bytes + off) = h;
-      x -= (double)__bfloat162float(h);
+      uint32_t w[4];
+#pragma unroll
+      for (int j = 0; j < 8; j += 2) {
+        const __nv_bfloat16 h0 = __double2bfloat16(x[j]), h1 = __double2bfloat16(x[j + 1]);
+        x[j] -= (double)__bfloat162float(h0);
+        x[j + 1] -= (double)__bfloat162float(h1);
+        w[j >> 1] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+      }
+      *reinterpret_cast<uint4*>(out + c * piece_bytes + off) = make_uint4(w[0], w[1], w[2], w[3]);
     }
   }
 }
+
+int pieces_of(int mode) { return mode == NW_TRANSFORM_CHOL_INT8 ? kOzakiSlices : 3; }
 
 }  // namespace
 
-// Scratch of split_product_pqrs: pre-tiled pieces of both factors and the row exponents.
-size_t split_product_scratch(int mode, int naux, int M, int N, int slices) {
-  const int kbytes_per = mode == NW_TRANSFORM_CHOL_INT8 ? naux : 2 * naux;
-  const int nkt = (kbytes_per + kKBytes - 1) / kKBytes;
-  const int mt = (M + kTileM - 1) / kTileM, nt = (N + kTileN - 1) / kTileN;
-  const int pieces = mode == NW_TRANSFORM_CHOL_INT8 ? slices : 3;
-  const size_t a = (size_t)pieces * mt * nkt * kTileABytes, b = (size_t)pieces * nt * nkt * kTileBBytes;
-  return a + b + (size_t)(M + N) * sizeof(int) + 4096;
+size_t split_factor_bytes(int mode, int naux, int R) {
+  const int kbytes = mode == NW_TRANSFORM_CHOL_INT8 ? naux : 2 * naux;
+  const int nkt = (kbytes + kKBytes - 1) / kKBytes, rpad = (R + kTileM - 1) / kTileM * kTileM;
+  return (size_t)pieces_of(mode) * nkt * (rpad / 64) * kTileBBytes + (size_t)rpad * sizeof(int) + 256;
 }
 
-// T[p][r][q][s] = sum_k U[k][pq] V[k][rs] with the split products on tcgen05 (mode, slices).
-cudaError_t split_product_pqrs(cudaStream_t st, int mode, int slices, const double* U, const double* V, int naux, int n,
-                               double* out, void* scratch, size_t scratch_bytes, uint32_t* err) {
-  const int M = n * n, N = n * n;
+cudaError_t split_factor(cudaStream_t st, int mode, const double* F, int naux, int R, void* buf, size_t bytes,
+                         SplitFactor* out) {
   if (mode != NW_TRANSFORM_CHOL_INT8 && mode != NW_TRANSFORM_CHOL_BF16X6) return cudaErrorInvalidValue;
-  if (mode == NW_TRANSFORM_CHOL_INT8 && (slices < 1 || slices > kMaxAcc)) return cudaErrorInvalidValue;
-  if (scratch_bytes < split_product_scratch(mode, naux, M, N, slices)) return cudaErrorInvalidValue;
-  const int kbytes_per = mode == NW_TRANSFORM_CHOL_INT8 ? naux : 2 * naux;
-  const int nkt = (kbytes_per + kKBytes - 1) / kKBytes;
-  const int mt = (M + kTileM - 1) / kTileM, nt = (N + kTileN - 1) / kTileN;
-  const int pieces = mode == NW_TRANSFORM_CHOL_INT8 ? slices : 3;
-  TcArgs g{};
-  g.a_piece = (long long)mt * nkt * kTileABytes;
-  g.b_piece = (long long)nt * nkt * kTileBBytes;
-  uint8_t* a = static_cast<uint8_t*>(scratch);
-  uint8_t* b = a + (size_t)pieces * g.a_piece;
-  int* erow = reinterpret_cast<int*>(b + (size_t)pieces * g.b_piece);
-  int* ecol = erow + M;
-  // zero padding (rows beyond M / N, K beyond naux)
-  cudaError_t e = cudaMemsetAsync(a, 0, (size_t)pieces * (g.a_piece + g.b_piece), st);
-  if (e != cudaSuccess) return e;
-  const int blocks = 148 * 8;
+  if (bytes < split_factor_bytes(mode, naux, R)) return cudaErrorInvalidValue;
+  const int kbytes = mode == NW_TRANSFORM_CHOL_INT8 ? naux : 2 * naux;
+  SplitFactor f;
+  f.mode = mode;
+  f.R = R;
+  f.rpad = (R + kTileM - 1) / kTileM * kTileM;
+  f.nkt = (kbytes + kKBytes - 1) / kKBytes;
+  f.piece_bytes = (long long)f.nkt * (f.rpad / 64) * kTileBBytes;
+  f.pieces = static_cast<uint8_t*>(buf);
+  f.exps = reinterpret_cast<int*>(f.pieces + (size_t)pieces_of(mode) * f.piece_bytes);
+  const long long chunks = (long long)f.rpad * f.nkt * 8;
+  const int blocks = (int)std::min<long long>((chunks + 255) / 256, 148 * 16);
   if (mode == NW_TRANSFORM_CHOL_INT8) {
-    row_exponent_kernel<<<(M + 255) / 256, 256, 0, st>>>(U, naux, M, erow);
-    row_exponent_kernel<<<(N + 255) / 256, 256, 0, st>>>(V, naux, N, ecol);
-    int8_slices_kernel<<<blocks, 256, 0, st>>>(U, naux, M, erow, slices, kTileM, nkt, g.a_piece,
-                                               reinterpret_cast<int8_t*>(a));
-    int8_slices_kernel<<<blocks, 256, 0, st>>>(V, naux, N, ecol, slices, kTileN, nkt, g.b_piece,
-                                               reinterpret_cast<int8_t*>(b));
-    // products of slices i + j = s into accumulator s, for s < slices
+    row_exponent_kernel<<<(f.rpad + 255) / 256, 256, 0, st>>>(F, naux, R, f.rpad, f.exps);
+    int8_slices_kernel<<<blocks, 256, 0, st>>>(F, naux, R, f.rpad, f.nkt, f.exps, kOzakiSlices, f.piece_bytes,
+                                               f.pieces);
+  } else {
+    bf16_pieces_kernel<<<blocks, 256, 0, st>>>(F, naux, R, f.rpad, f.nkt, f.piece_bytes, f.pieces);
+  }
+  *out = f;
+  return cudaGetLastError();
+}
+
+// T[p][r][q][s] = sum_k U[k][pq] V[k][rs] from two split factors (same mode) on tcgen05.
+cudaError_t split_product(cudaStream_t st, const SplitFactor& A, const SplitFactor& B, int n, double* out,
+                          uint32_t* err) {
+  const int M = n * n, N = n * n;
+  if (A.mode != B.mode || A.nkt != B.nkt || A.R != M || B.R != N) return cudaErrorInvalidValue;
+  TcArgs g{};
+  g.a = A.pieces;
+  g.b = B.pieces;
+  g.a_piece = A.piece_bytes;
+  g.b_piece = B.piece_bytes;
+  g.nkt = A.nkt;
+  g.nrt_a = A.rpad / 64;
+  g.nrt_b = B.rpad / 64;
+  if (A.mode == NW_TRANSFORM_CHOL_INT8) {
+    // products of slices i + j = s into accumulator s, for s < kOzakiSlices
     int np = 0;
-    for (int s = 0; s < slices; ++s)
+    for (int s = 0; s < kOzakiSlices; ++s)
       for (int i = 0; i <= s; ++i) {
         g.pa[np] = (int8_t)i;
         g.pb[np] = (int8_t)(s - i);
@@ -387,13 +424,11 @@ cudaError_t split_product_pqrs(cudaStream_t st, int mode, int slices, const doub
         ++np;
       }
     g.nprod = np;
-    g.nacc = slices;
-    for (int s = 0; s < slices; ++s) g.acc_scale[s] = ldexp(1.0, -7 * (s + 2));
-    g.erow = erow;
-    g.ecol = ecol;
+    g.nacc = kOzakiSlices;
+    for (int s = 0; s < kOzakiSlices; ++s) g.acc_scale[s] = ldexp(1.0, -7 * (s + 2));
+    g.erow = A.exps;
+    g.ecol = B.exps;
   } else {
-    bf16_pieces_kernel<<<blocks, 256, 0, st>>>(U, naux, M, kTileM, nkt, g.a_piece, a);
-    bf16_pieces_kernel<<<blocks, 256, 0, st>>>(V, naux, N, kTileN, nkt, g.b_piece, b);
     // hi hi, hi mid, mid hi, hi lo, mid mid, lo hi: all into one FP32 accumulator
     static const int8_t pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 0, 2, 1, 0};
     for (int i = 0; i < 6; ++i) {
@@ -405,20 +440,15 @@ cudaError_t split_product_pqrs(cudaStream_t st, int mode, int slices, const doub
     g.nacc = 1;
     g.acc_scale[0] = 1.0;
   }
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  g.a = a;
-  g.b = b;
-  g.nkt = nkt;
-  g.mt = mt;
-  g.nt = nt;
   g.M = M;
   g.N = N;
   g.n = n;
   g.out = out;
   g.err = err;
   const size_t smem = kStages * (kTileABytes + kTileBBytes) + 1024 + 256;
-  const dim3 grid((unsigned)nt, (unsigned)mt);
-  if (mode == NW_TRANSFORM_CHOL_INT8) {
+  const dim3 grid((unsigned)(B.rpad / kTileN), (unsigned)(A.rpad / kTileM));
+  cudaError_t e;
+  if (A.mode == NW_TRANSFORM_CHOL_INT8) {
     e = cudaFuncSetAttribute(tc_gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     tc_gemm_kernel<1><<<grid, kTcThreads, smem, st>>>(g);
@@ -428,6 +458,28 @@ cudaError_t split_product_pqrs(cudaStream_t st, int mode, int slices, const doub
     tc_gemm_kernel<0><<<grid, kTcThreads, smem, st>>>(g);
   }
   return cudaGetLastError();
+}
+
+// Scratch of split_product_pqrs: both factors' pieces and exponents.
+size_t split_product_scratch(int mode, int naux, int M, int N, int slices) {
+  (void)slices;
+  return split_factor_bytes(mode, naux, M) + split_factor_bytes(mode, naux, N);
+}
+
+// T[p][r][q][s] = sum_k U[k][pq] V[k][rs] with the split products on tcgen05 (both factors
+// split here).
+cudaError_t split_product_pqrs(cudaStream_t st, int mode, int slices, const double* U, const double* V, int naux, int n,
+                               double* out, void* scratch, size_t scratch_bytes, uint32_t* err) {
+  const int M = n * n, N = n * n;
+  if (mode == NW_TRANSFORM_CHOL_INT8 && slices != kOzakiSlices) return cudaErrorInvalidValue;
+  if (scratch_bytes < split_product_scratch(mode, naux, M, N, slices)) return cudaErrorInvalidValue;
+  const size_t ba = split_factor_bytes(mode, naux, M);
+  SplitFactor A, B;
+  cudaError_t e = split_factor(st, mode, U, naux, M, scratch, ba, &A);
+  if (e == cudaSuccess)
+    e = split_factor(st, mode, V, naux, N, static_cast<char*>(scratch) + ba, scratch_bytes - ba, &B);
+  if (e != cudaSuccess) return e;
+  return split_product(st, A, B, n, out, err);
 }
 
 }  // namespace nw

@@ -63,27 +63,34 @@ def test_qmc_trajectory_bounds(name):
     NOCI-QMC run with the fixture's qmc / prop blocks (uniform generator, 80 one-cycle reports
     from 200 walkers towards 500) must give at least min_samples projected energies, all finite
     and inside [min_energy, max_energy], spanning at least min_energy_span and ending at least
-    min_final_drop below the first.  The random stream is the engine's Philox, not the
-    reference's SmallRng, so the trajectory itself is not compared: only its bounds are."""
+    min_final_drop below the first.  The engine's random stream is Philox, not the reference's
+    SmallRng, so its trajectory for seed 1 is a different sample of the same process; with a few
+    hundred walkers a single trajectory's end-to-end drop is of the order of its noise.  So every
+    one of 8 independent trajectories (seeds 1..8) must satisfy the window, and the span and the
+    final drop are required of their mean trajectory."""
     system, meta = reffix.load(name)
     opt, exp = meta["qmc"], meta["expected"]
     basis = sy.sd_basis(system.nmo, system.nocc_a, system.nocc_b, len(system.refs), orders=tuple(meta["orders"]),
                         include_refs=True)
     refs = np.nonzero((basis["rank_a"] == 0) & (basis["rank_b"] == 0))[0].astype(np.uint32)
+    runs = []
     with _engine(system) as w:
         w.set_basis(basis)
         hr, sr = w.build_hs_matrix(refs, refs)
         er, cr = w.general_evp(hr, sr, project=True, tol=1e-12)
         c0 = np.zeros(basis.shape[0])
         c0[refs] = cr[:, 0]
-        with nociwick.Qmc(w, c0, refs, dt=opt["dt"], initial_population=opt["initial_population"],
-                          target_population=opt["target_population"], sampling_cutoff=opt["sampling_cutoff"],
-                          spawn_cutoff=opt["spawn_cutoff"], initial_shift=float(er[0]), ncycles=opt["ncycles"],
-                          propagator=opt["propagator"], seed=opt["seed"]) as q:
-            rep = q.run(opt["nreports"])
-    e = rep["eproj_num"] / rep["eproj_den"]
-    assert e.shape[0] >= exp["min_samples"]
-    assert np.all(np.isfinite(e))
-    assert np.all((e >= exp["min_energy"]) & (e <= exp["max_energy"])), (e.min(), e.max())
-    assert e.max() - e.min() >= exp["min_energy_span"], e
-    assert e[0] - e[-1] >= exp["min_final_drop"], (e[0], e[-1])
+        for seed in range(opt["seed"], opt["seed"] + 8):
+            with nociwick.Qmc(w, c0, refs, dt=opt["dt"], initial_population=opt["initial_population"],
+                              target_population=opt["target_population"], sampling_cutoff=opt["sampling_cutoff"],
+                              spawn_cutoff=opt["spawn_cutoff"], initial_shift=float(er[0]), ncycles=opt["ncycles"],
+                              propagator=opt["propagator"], seed=seed) as q:
+                rep = q.run(opt["nreports"])
+            runs.append(rep["eproj_num"] / rep["eproj_den"])
+    for e in runs:
+        assert e.shape[0] >= exp["min_samples"]
+        assert np.all(np.isfinite(e))
+        assert np.all((e >= exp["min_energy"]) & (e <= exp["max_energy"])), (e.min(), e.max())
+    mean = np.mean(runs, axis=0)
+    assert mean.max() - mean.min() >= exp["min_energy_span"], mean
+    assert mean[0] - mean[-1] >= exp["min_final_drop"], (mean[0], mean[-1], [e[0] - e[-1] for e in runs])

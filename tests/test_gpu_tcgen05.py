@@ -3,8 +3,9 @@ the FP64 product: t4[p][r][q][s] = sum_P U[P][pq] V[P][rs].
 
 * NW_TRANSFORM_CHOL_INT8 (Ozaki slices on the int8 tensor cores, exact int32 sums): FP64-faithful,
   |T - T_fp64| <= 1e-13 * sum_P |U||V| (8 slices of 7 bits, rebuilt in FP64);
-* NW_TRANSFORM_CHOL_BF16X6 (three BF16 pieces, six products in FP32): FP32-class,
-  |T - T_fp64| <= 2e-6 * sum_P |U||V|;
+* NW_TRANSFORM_CHOL_BF16X6 (three BF16 pieces, six products in FP32): FP32-class, bounded by
+  the FP32 accumulation over the 6 naux products, |T - T_fp64| <= 1e-4 * sum_P |U||V|
+  (about 6 naux 2^-24 for naux = 256);
 * NW_TRANSFORM_CHOL_FP64 (the FP64 tensor-core GEMM plus the index swap): to rounding.
 Sizes cover partial tiles (n^2 not a multiple of the 128 x 64 tile, naux not a multiple of the
 128-byte K tile) and the config-3 shape (n = 64, naux = 256).  Then whole builds: a Cholesky
@@ -35,7 +36,7 @@ def _product(mode, u, v, naux, n):
 
 
 @pytest.mark.parametrize("n,naux", [(5, 7), (12, 40), (30, 130), (64, 256)])
-@pytest.mark.parametrize("mode,rel", [("chol_fp64", 1e-13), ("chol_int8", 1e-13), ("chol_bf16x6", 2e-6)])
+@pytest.mark.parametrize("mode,rel", [("chol_fp64", 1e-13), ("chol_int8", 1e-13), ("chol_bf16x6", 1e-4)])
 def test_split_product_matches_fp64(n, naux, mode, rel):
     rng = np.random.default_rng(n * 100 + naux)
     # rows of very different magnitude exercise the per-row scaling of the integer slices
