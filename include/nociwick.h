@@ -157,7 +157,8 @@ typedef enum {
     NW_TRANSFORM_FP64 = 0,         /* four FP64 quarter transforms of the Coulomb tensor (default) */
     NW_TRANSFORM_CHOL_FP64 = 1,    /* Cholesky route, FP64 product on the FP64 tensor cores      */
     NW_TRANSFORM_CHOL_INT8 = 2,    /* Cholesky route on tcgen05: 8 signed int8 slices per factor
-                                      (Ozaki split, exact int32 sums), rebuilt in FP64             */
+                                      (Ozaki split, exact int32 sums), rebuilt in FP64; at most
+                                      16384 Cholesky vectors                                       */
     NW_TRANSFORM_CHOL_BF16X6 = 3   /* Cholesky route on tcgen05: 3 BF16 pieces per factor, the 6
                                       leading products summed in FP32 (FP32-class accuracy)        */
 } nw_transform;

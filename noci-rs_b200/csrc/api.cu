@@ -306,6 +306,9 @@ nw_status nw_set_transform(nw_ctx* ctx, int32_t mode) {
   if (mode < NW_TRANSFORM_FP64 || mode > NW_TRANSFORM_CHOL_BF16X6) return nw::fail(ctx, NW_ERR_INVALID, "unknown transform");
   if (mode != NW_TRANSFORM_FP64 && !ctx->d_chol)
     return nw::fail(ctx, NW_ERR_STATE, "Cholesky transforms need a context from nw_ctx_create_cholesky");
+  // int8 slice sums stay exact in INT32 while (s + 1) naux 64^2 < 2^31
+  if (mode == NW_TRANSFORM_CHOL_INT8 && ctx->naux > 16384)
+    return nw::fail(ctx, NW_ERR_UNSUPPORTED, "int8 split products take at most 16384 Cholesky vectors");
   ctx->transform = mode;
   return NW_OK;
 }
@@ -315,6 +318,7 @@ nw_status nw_transform_product(int32_t mode, const double* u, const double* v, i
   if (!u || !v || !t4 || naux <= 0 || n <= 0 || n > 128) return NW_ERR_INVALID;
   if (mode != NW_TRANSFORM_CHOL_FP64 && mode != NW_TRANSFORM_CHOL_INT8 && mode != NW_TRANSFORM_CHOL_BF16X6)
     return NW_ERR_INVALID;
+  if (mode == NW_TRANSFORM_CHOL_INT8 && naux > 16384) return NW_ERR_UNSUPPORTED;
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int n2 = n * n;
   void* work = nullptr;
