@@ -107,6 +107,7 @@ PIPE_CHUNKS, PIPE_MIN_CHUNK = 16, 1 << 18  # chunking of the pinned-host entry (
 # (dram__bytes_read.sum + dram__bytes_write.sum; the summaries under profiles/ give the commands)
 EVAL_TRAFFIC = {
     ("config2", 10_000_000): (1_438_561_280, "profiles/eval_traffic_config2_10Mpairs.md"),
+    ("config3", 100_000_000): (63_536_004_352, "profiles/eval_traffic_config3_100Mpairs.md"),
 }
 
 
@@ -729,6 +730,13 @@ def hs_leg(args, name, npairs, rank, world, local_rank, dist):
     for _ in range(min(args.steps, 10)):
         step_device()
         phases.append(eng.last_timings())
+    # each class evaluator's own device time: the same steps with the class kernels serialised
+    # (a profiling mode; the concurrent steps above are the timed configuration)
+    eng.set_timing(True, serial_classes=True)
+    classes = []
+    for _ in range(min(args.steps, 5)):
+        step_device()
+        classes.append(eng.last_class_timings())
     eng.set_timing(False)
     # end to end through the host-buffer entry point
     for _ in range(2):
@@ -765,8 +773,8 @@ def hs_leg(args, name, npairs, rank, world, local_rank, dist):
     value = aggregate_rate(npairs, world, args.steps, t_dev)
     e2e = aggregate_rate(npairs, world, args.steps, t_e2e)
     ev_ms = statistics.median([p["eval_m0"] for p in phases])
-    gen_ms = statistics.median([p["eval_gen"] for p in phases])
     phase_ms = {k: statistics.median([p[k] for p in phases]) for k in phases[0]}
+    class_ms = {k: statistics.median([c[k] for c in classes]) for k in classes[0]}
     alg_bytes = algorithmic_bytes(basis, pairs)
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (ev_ms / 1e3) / 1e9
@@ -795,7 +803,13 @@ def hs_leg(args, name, npairs, rank, world, local_rank, dist):
                      "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_step": alg_bytes,
                      "bytes_formula": "B(La,Lb) = 8[2(La^2+Lb^2) + 2C(La,2)^2 + 2C(Lb,2)^2 + La^2 Lb^2] + 60 per pair "
                                       "(m > 0 pairs counted with the m = 0 bytes of their ranks: a lower bound)",
-                     "eval_ms": ev_ms, "eval_gen_ms": gen_ms, "phase_ms": phase_ms},
+                     "eval_ms": ev_ms, "eval_gen_ms": class_ms["gen"], "phase_ms": phase_ms,
+                     "class_ms_serial": class_ms,
+                     "dram_frac": (traffic / (ev_ms / 1e3) / 1e9 / peak) if traffic else None,
+                     "note": "eval_ms: the class evaluators overlapped on forked streams (the timed step); "
+                             "eval_gen_ms and class_ms_serial: each class kernel's own time with the classes "
+                             "run one after another; dram_frac: measured DRAM bytes per step (traffic) over "
+                             "eval_ms"},
         "clocks": clocks,
         "gpu_launches": kernels_per_step * args.steps,
         "autotune": tune,
@@ -878,13 +892,18 @@ def mixed_leg(args, system, basis, pairs, hs_ref, fp64_build_s, fp64_eval_ms, lo
     smin = reference_pair_conditioning(system)
     par = basis["parent"].astype(np.int64)
     cond = smin[par[pairs[:, 0]] * len(system.refs) + par[pairs[:, 1]]]
-    out = {"fp64": {"build_seconds": fp64_build_s, "eval_ms": fp64_eval_ms,
-                    "one_shot_value": npairs / (fp64_build_s + fp64_eval_ms / 1e3),
-                    "note": "four FP64 quarter transforms of the full Coulomb tensor (the default build)"}}
-    for mode in ("chol_fp64", "chol_int8", "chol_bf16x6"):
-        eng = nociwick.WicksShared(system.s, system.h, None, system.enuc, system.refs, tol=1e-8, device=local_rank,
-                                   chol=system.chol)
-        eng.set_transform(mode)
+    out = {"first_build": {"build_seconds": fp64_build_s, "eval_ms": fp64_eval_ms,
+                           "note": "the config-3 leg's own FP64 build: the first on this process, so it includes "
+                                   "the allocation of the slab and the build buffers; fp64 below is a rebuild"}}
+    for mode in ("fp64", "chol_fp64", "chol_int8", "chol_bf16x6"):
+        if mode == "fp64":
+            # four FP64 quarter transforms of the full Coulomb tensor (the default build)
+            eng = nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8,
+                                       device=local_rank)
+        else:
+            eng = nociwick.WicksShared(system.s, system.h, None, system.enuc, system.refs, tol=1e-8,
+                                       device=local_rank, chol=system.chol)
+            eng.set_transform(mode)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         eng.build()
@@ -916,13 +935,15 @@ def mixed_leg(args, system, basis, pairs, hs_ref, fp64_build_s, fp64_eval_ms, lo
     del dpairs, dout
     torch.cuda.empty_cache()
     out["note"] = ("the evaluator reads FP64 intermediates in every mode, so the device pair rate is the same; the "
-                   "split products change the build (the J / II tensors) and its accuracy")
+                   "split products change the build (the J / II tensors) and its accuracy; errors against the "
+                   "config-3 leg's FP64 results (fp64 here: a rebuild, zero when the build is deterministic)")
     return out
 
 
 def tail_summary(line):
     """The figures a reader of the end of the output needs, in a few hundred bytes."""
-    out = {"hs_config2": {"value": line["value"], "e2e": line["e2e"]["value"], "frac": line["roofline"]["frac"]}}
+    wl = "hs_config3" if line["config"]["workload"].startswith("synthetic stress") else "hs_config2"
+    out = {wl: {"value": line["value"], "e2e": line["e2e"]["value"], "frac": line["roofline"]["frac"]}}
     c3 = line.get("config3")
     if c3:
         out["hs_config3"] = {"value": c3["value"], "e2e": c3["e2e"]["value"], "frac": c3["roofline"]["frac"],
@@ -933,7 +954,7 @@ def tail_summary(line):
                                       "rms_err_h": chk["rms_abs_err_h"], "cpu": chk["cpu_baseline"]["value"]})
         mx = c3.get("mixed")
         if mx:
-            out["mixed_config3"] = {m: {"build_s": v["build_seconds"], "one_shot": v["one_shot_value"],
+            out["mixed_config3"] = {m: {"build_s": v["build_seconds"], "one_shot": v.get("one_shot_value"),
                                         "max_dh": v.get("max_abs_dh_vs_fp64")}
                                     for m, v in mx.items() if isinstance(v, dict)}
     q = line.get("qmc")

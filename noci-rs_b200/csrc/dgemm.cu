@@ -5,15 +5,17 @@
 // src/nonorthogonalwicks/build.rs:198-313,526-683,808-917 and src/maths/eri.rs:258) are FP64
 // GEMMs: row-major C (M x N) = alpha op(A) op(B) + beta C, strided-batched.  tcgen05.mma has
 // no FP64 kind, so on sm_100a the FP64 tensor path is the DMMA instruction
-// mma.sync.aligned.m8n8k4.row.col.f64, issued here per warp.
+// mma.sync.aligned.m16n8k16.row.col.f64, issued here per warp.
 //
-// Tiling: a 64 x 64 tile of C per block of 128 threads (2 x 2 warps of 32 x 32, i.e. 4 x 4
-// DMMA tiles of 8 x 8 per warp, 32 FP64 accumulators per thread), K in steps of 16 staged
-// through shared memory as [k][m] and [k][n] panels (both operands k-major, so each lane's
-// fragment element is one aligned 8-byte load), with the next panel's global loads in flight
-// in registers while the current panel feeds the tensor cores.  Operands may be transposed
-// (op = ^T) and either batch stride may be 0 (a shared operand); edges are zero-filled, so any
-// M, N, K is accepted.
+// Tiling: a 64 x 64 tile of C per block of 128 threads (2 x 2 warps of 32 x 32, i.e. 2 x 4
+// DMMA tiles of 16 x 8 per warp, 32 FP64 accumulators per thread), one m16n8k16 DMMA per tile
+// and 16-deep K panel.  Panels move global -> shared with 8-byte cp.async (zero-fill past the
+// matrix edges, so any M, N, K) through a three-stage ring, so two panels are in flight while
+// the third feeds the tensor cores.  Each operand's panel keeps the operand's own contiguous
+// direction (k-major rows of 16 + 4 doubles, or m/n-major rows of 64 + 4 doubles): the copies
+// are coalesced, and the padded strides make every fragment load of a warp conflict-free.
+// Operands may be transposed (op = ^T, a template parameter) and either batch stride may be 0
+// (a shared operand).
 #include <cuda_runtime.h>
 
 #include "internal.cuh"
@@ -23,16 +25,31 @@ namespace {
 
 constexpr int kBM = 64, kBN = 64, kBK = 16;
 constexpr int kThreads = 128;
-constexpr int kPad = 8;                  // panel row stride kBM + 8 doubles: fragment loads of a
-constexpr int kLdA = kBM + kPad;         // warp touch each bank pair at most twice
-constexpr int kLdB = kBN + kPad;
-constexpr int kPerThreadA = kBM * kBK / kThreads;  // 8
-constexpr int kPerThreadB = kBK * kBN / kThreads;  // 8
+constexpr int kStages = 3;
+constexpr int kLdK = kBK + 4;   // k-contiguous panel rows (16 + 4 doubles)
+constexpr int kLdMN = kBM + 4;  // m- or n-contiguous panel rows (64 + 4 doubles)
+constexpr int kPanel = kBM * kLdK > kBK * kLdMN ? kBM * kLdK : kBK * kLdMN;  // doubles per panel
+constexpr size_t kSmem = (size_t)kStages * 2 * kPanel * sizeof(double);
 
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
+__device__ __forceinline__ void dmma16816(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7, %8, %9, %10, %11}, "
+      "{%12, %13, %14, %15}, {%0, %1, %2, %3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]), "d"(b[1]),
+        "d"(b[2]), "d"(b[3]));
+}
+
+// 8-byte asynchronous copy global -> shared; src_bytes = 0 writes a zero.
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(valid ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 struct GemmArgs {
@@ -42,34 +59,45 @@ struct GemmArgs {
   long long sa, sb, sc;   // batch strides (elements)
   int M, N, K, lda, ldb, ldc;
   double alpha, beta;
-  int ta, tb;
 };
 
-// Element e of the A panel (kBM x kBK of op(A)) at k-tile k0: its (m, k) inside the tile.  The
-// mapping follows the operand's contiguous index so that a warp's loads are consecutive.
-__device__ __forceinline__ void a_coord(int e, int ta, int* m, int* k) {
-  if (ta) {  // A stored K x M: m contiguous
-    *k = e / kBM;
-    *m = e % kBM;
-  } else {   // A stored M x K: k contiguous
-    *m = e / kBK;
-    *k = e % kBK;
+// Panel element (i, k) of a kRows x kBK panel: row-major over k when the operand is k-contiguous
+// in memory (KC), else k-major over the rows.
+template <bool KC>
+__device__ __forceinline__ int panel_index(int i, int k) {
+  return KC ? i * kLdK + k : k * kLdMN + i;
+}
+
+// Issue the copies of K panel kt of op(A) (rows m0..) and op(B) (columns n0..) into stage st.
+// TA: A stored K x M (m contiguous); TB: B stored N x K (k contiguous).
+template <bool TA, bool TB>
+__device__ __forceinline__ void load_panels(const GemmArgs& g, const double* A, const double* B, int m0, int n0,
+                                            int kt, double* as, double* bs) {
+  const int tid = threadIdx.x, k0 = kt * kBK;
+#pragma unroll
+  for (int u = 0; u < kBM * kBK / kThreads; ++u) {
+    const int e = tid + u * kThreads;
+    // consecutive threads take consecutive addresses of the operand's contiguous index
+    const int m = TA ? e % kBM : e / kBK, k = TA ? e / kBM : e % kBK;
+    const int gm = m0 + m, gk = k0 + k;
+    const bool ok = gm < g.M && gk < g.K;
+    const double* src = ok ? A + (TA ? (long long)gk * g.lda + gm : (long long)gm * g.lda + gk) : A;
+    cp_async8(as + panel_index<!TA>(m, k), src, ok);
+  }
+#pragma unroll
+  for (int u = 0; u < kBN * kBK / kThreads; ++u) {
+    const int e = tid + u * kThreads;
+    const int n = TB ? e / kBK : e % kBN, k = TB ? e % kBK : e / kBN;
+    const int gn = n0 + n, gk = k0 + k;
+    const bool ok = gn < g.N && gk < g.K;
+    const double* src = ok ? B + (TB ? (long long)gn * g.ldb + gk : (long long)gk * g.ldb + gn) : B;
+    cp_async8(bs + panel_index<TB>(n, k), src, ok);
   }
 }
 
-__device__ __forceinline__ void b_coord(int e, int tb, int* k, int* n) {
-  if (tb) {  // B stored N x K: k contiguous
-    *n = e / kBK;
-    *k = e % kBK;
-  } else {   // B stored K x N: n contiguous
-    *k = e / kBN;
-    *n = e % kBN;
-  }
-}
-
+template <bool TA, bool TB>
 __global__ void __launch_bounds__(kThreads) dgemm_kernel(GemmArgs g) {
-  __shared__ double As[kBK][kLdA];
-  __shared__ double Bs[kBK][kLdB];
+  extern __shared__ __align__(16) double dsm[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
   const int grp = lane >> 2, tig = lane & 3;
@@ -78,80 +106,79 @@ __global__ void __launch_bounds__(kThreads) dgemm_kernel(GemmArgs g) {
   const double* __restrict__ A = g.A + bz * g.sa;
   const double* __restrict__ B = g.B + bz * g.sb;
   double* __restrict__ C = g.C + bz * g.sc;
+  const int nk = (g.K + kBK - 1) / kBK;
 
-  double acc[4][4][2];
+  double acc[2][4][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-  double ra[kPerThreadA], rb[kPerThreadB];
-  auto load = [&](int k0) {
-#pragma unroll
-    for (int u = 0; u < kPerThreadA; ++u) {
-      int m, k;
-      a_coord(tid + u * kThreads, g.ta, &m, &k);
-      const int gm = m0 + m, gk = k0 + k;
-      ra[u] = (gm < g.M && gk < g.K) ? __ldg(A + (g.ta ? (long long)gk * g.lda + gm : (long long)gm * g.lda + gk))
-                                     : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < kPerThreadB; ++u) {
-      int k, n;
-      b_coord(tid + u * kThreads, g.tb, &k, &n);
-      const int gn = n0 + n, gk = k0 + k;
-      rb[u] = (gn < g.N && gk < g.K) ? __ldg(B + (g.tb ? (long long)gn * g.ldb + gk : (long long)gk * g.ldb + gn))
-                                     : 0.0;
-    }
-  };
-  auto store = [&]() {
-#pragma unroll
-    for (int u = 0; u < kPerThreadA; ++u) {
-      int m, k;
-      a_coord(tid + u * kThreads, g.ta, &m, &k);
-      As[k][m] = ra[u];
-    }
-#pragma unroll
-    for (int u = 0; u < kPerThreadB; ++u) {
-      int k, n;
-      b_coord(tid + u * kThreads, g.tb, &k, &n);
-      Bs[k][n] = rb[u];
-    }
-  };
-
-  load(0);
-  for (int k0 = 0; k0 < g.K; k0 += kBK) {
-    store();
-    __syncthreads();
-    if (k0 + kBK < g.K) load(k0 + kBK);  // next panel's loads overlap this panel's DMMAs
-#pragma unroll
-    for (int kk = 0; kk < kBK; kk += 4) {
-      double af[4], bf[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) af[i] = As[kk + tig][wm + i * 8 + grp];   // A[row grp][col tig]
-#pragma unroll
-      for (int j = 0; j < 4; ++j) bf[j] = Bs[kk + tig][wn + j * 8 + grp];   // B[row tig][col grp]
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
-    }
-    __syncthreads();
-  }
-  // D fragment: row grp, columns 2 tig, 2 tig + 1 of each 8 x 8 tile
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int gm = m0 + wm + i * 8 + grp, gn = n0 + wn + j * 8 + 2 * tig + h;
+      for (int h = 0; h < 4; ++h) acc[i][j][h] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < kStages - 1; ++s) {
+    if (s < nk) load_panels<TA, TB>(g, A, B, m0, n0, s, dsm + (2 * s) * kPanel, dsm + (2 * s + 1) * kPanel);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<kStages - 2>();  // panel kt has landed (this thread's copies)
+    __syncthreads();               // ... and every thread's; stage (kt - 1) % kStages is free
+    {
+      const int nx = kt + kStages - 1, st = nx % kStages;
+      if (nx < nk) load_panels<TA, TB>(g, A, B, m0, n0, nx, dsm + (2 * st) * kPanel, dsm + (2 * st + 1) * kPanel);
+      cp_async_commit();
+    }
+    const int st = kt % kStages;
+    const double* as = dsm + (2 * st) * kPanel;
+    const double* bs = dsm + (2 * st + 1) * kPanel;
+    // fragments: A[row grp + 8 (i % 2)][col tig + 4 (i / 2)], B[row tig + 4 i][col grp]
+    double af[2][8], bf[4][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        af[mt][i] = as[panel_index<!TA>(wm + mt * 16 + grp + 8 * (i & 1), tig + 4 * (i >> 1))];
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) bf[nt][i] = bs[panel_index<TB>(wn + nt * 8 + grp, tig + 4 * i)];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) dmma16816(acc[mt][nt], af[mt], bf[nt]);
+  }
+  cp_async_wait<0>();
+  // D fragment: rows grp, grp + 8 and columns 2 tig, 2 tig + 1 of each 16 x 8 tile
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const int gm = m0 + wm + mt * 16 + grp + 8 * (h >> 1), gn = n0 + wn + nt * 8 + 2 * tig + (h & 1);
         if (gm < g.M && gn < g.N) {
           double* c = C + (long long)gm * g.ldc + gn;
-          const double v = g.alpha * acc[i][j][h];
+          const double v = g.alpha * acc[mt][nt][h];
           *c = g.beta == 0.0 ? v : v + g.beta * *c;
         }
       }
+}
+
+template <bool TA, bool TB>
+cudaError_t launch(cudaStream_t stream, const GemmArgs& g, dim3 grid) {
+  // the three-stage ring is above the 48 KB default; raised once per device
+  static bool raised[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64 || !raised[dev]) {
+    e = cudaFuncSetAttribute(dgemm_kernel<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64) raised[dev] = true;
+  }
+  dgemm_kernel<TA, TB><<<grid, kThreads, kSmem, stream>>>(g);
+  return cudaGetLastError();
 }
 
 }  // namespace
@@ -163,9 +190,10 @@ cudaError_t dgemm_strided(cudaStream_t stream, bool ta, bool tb, int M, int N, i
   if (K <= 0) return cudaErrorInvalidValue;
   const long long gx = (N + kBN - 1) / kBN, gy = (M + kBM - 1) / kBM;
   if (gy > 65535 || batch > 65535 || gx > 0x7FFFFFFFll) return cudaErrorInvalidValue;
-  GemmArgs g{A, B, C, sa, sb, sc, M, N, K, lda, ldb, ldc, alpha, beta, ta ? 1 : 0, tb ? 1 : 0};
-  dgemm_kernel<<<dim3((unsigned)gx, (unsigned)gy, (unsigned)batch), kThreads, 0, stream>>>(g);
-  return cudaGetLastError();
+  GemmArgs g{A, B, C, sa, sb, sc, M, N, K, lda, ldb, ldc, alpha, beta};
+  const dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)batch);
+  if (ta) return tb ? launch<true, true>(stream, g, grid) : launch<true, false>(stream, g, grid);
+  return tb ? launch<false, true>(stream, g, grid) : launch<false, false>(stream, g, grid);
 }
 
 }  // namespace nw

@@ -16,17 +16,22 @@
 //     INT32 in tensor memory (one accumulator per s), and the result is rebuilt in FP64 as
 //     sum_s 2^(e_row + e_col - 7 (s + 2)) C_s.  With S = 8 the result is FP64-faithful.
 //
-// Kernel shape: one CTA of 128 threads per 128 x 64 tile of T (cta_group::1, M = 128, N = 64).
+// Kernel shape: one CTA of 256 threads per 128 x 64 tile of T (cta_group::1, M = 128, N = 64).
 // Operands are pre-tiled in global memory by the split kernels in the tcgen05 no-swizzle K-major
-// layout (8-row x 16-byte core matrices), so each 128-byte-deep K tile of an operand is one
-// contiguous block moved by a single cp.async.bulk (no multicast) into a 6-stage ring of shared
-// memory, completion signalled on an mbarrier.  Thread 0 issues the copies, thread 32 the MMAs
-// (tcgen05.mma, one per 32-byte K step, then tcgen05.commit to free the stage); each product
-// (A piece, B piece) goes to its accumulator's 64 TMEM columns.  The epilogue loads the
-// accumulators with tcgen05.ld (warp w reads TMEM lanes 32w .. 32w + 31), rebuilds FP64 and
-// stores T in the [p][r][q][s] order of the build's T4 buffers.  Every mbarrier wait is bounded:
-// on a timeout the CTA records an error flag, stops issuing work, waits (bounded) for what it
-// issued, frees its tensor memory and returns.
+// layout (8-row x 16-byte core matrices, 64-byte-deep K tiles), so the K tile of one piece of an
+// operand is one contiguous block moved by a single cp.async.bulk (no multicast).  A pipeline
+// stage holds the K tile of EVERY piece of both operands (int8: 8 + 8 slices, 96 KB, two stages;
+// BF16: 3 + 3 pieces, 36 KB, five stages), so each slice is read from L2 once per tile and all
+// products of that K tile run from shared memory.  Thread 0 issues the copies, thread 32 the MMAs
+// (tcgen05.mma, two 32-byte K steps per product and stage, then tcgen05.commit to free the
+// stage); each product (A piece, B piece) goes to its accumulator's 64 TMEM columns.  All eight
+// warps run the epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 and columns 32 (w / 4) .. + 31
+// of every accumulator with one 32-column tcgen05.ld each, rebuilds FP64 (exact int32 -> FP64
+// conversion by the 2^52 + 2^31 offset, power-of-two scales built from the exponent bits) and
+// stores T in the [p][r][q][s] order of the build's T4 buffers, with the tile's column offsets
+// and exponents staged in shared memory.  Every mbarrier wait is bounded: on a timeout the CTA
+// records an error flag, stops issuing work, waits (bounded) for what it issued, frees its
+// tensor memory and returns.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -38,14 +43,25 @@
 namespace nw {
 namespace {
 
-constexpr int kTcThreads = 128;
+constexpr int kTcThreads = 256;
 constexpr int kTileM = 128, kTileN = 64;
-constexpr int kKBytes = 128;                      // bytes of K per stage tile row
-constexpr int kStages = 6;                       // 144 KB of stages: one CTA per SM
-constexpr uint32_t kTileABytes = kTileM * kKBytes;  // 16 KB
-constexpr uint32_t kTileBBytes = kTileN * kKBytes;  // 8 KB
+constexpr int kKBytes = 64;                         // bytes of K per tile row and stage
+constexpr uint32_t kBlockBytes = 64 * kKBytes;      // one pre-tiled 64-row block: 4 KB
+constexpr uint32_t kTileABytes = kTileM * kKBytes;  // 8 KB per piece (two adjacent blocks)
+constexpr uint32_t kTileBBytes = kTileN * kKBytes;  // 4 KB per piece
+constexpr uint32_t kSbo = 8 * 16 * (kKBytes / 16);  // 512: between 8-row groups of a block
 constexpr int kMaxAcc = 8;                          // accumulators of 64 columns (512 TMEM columns)
 constexpr uint32_t kWaitLimit = 1u << 24;           // try_wait rounds before a wait gives up
+
+template <int kKind>
+struct TcShape {
+  static constexpr int kPieces = kKind == 1 ? kOzakiSlices : 3;
+  static constexpr int kStages = kKind == 1 ? 2 : 5;
+  static constexpr uint32_t kStageA = kPieces * kTileABytes, kStageB = kPieces * kTileBBytes;
+  // ring, barriers (full, empty, done), TMEM slot + abort flag, column exponents and offsets
+  static constexpr size_t kSmem = 1024 + (size_t)kStages * (kStageA + kStageB) + 8 * (2 * kStages + 1) + 8 +
+                                  2 * kTileN * sizeof(int);
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -116,22 +132,35 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// 8 consecutive 32-bit columns of this thread's TMEM lane.
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+// 32 consecutive 32-bit columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
                : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// Exact int32 -> FP64: the low word of 2^52 + 2^31 + x, minus that offset (one DADD).
+__device__ __forceinline__ double i32_to_f64(uint32_t x) {
+  return __hiloint2double(0x43300000, (int)(x ^ 0x80000000u)) - 4503601774854144.0;
+}
+
+// v 2^e; a multiplication by the exact power of two when 2^e is a normal number (the same
+// single rounding as ldexp), ldexp otherwise.
+__device__ __forceinline__ double scale_pow2(double v, int e) {
+  if (e >= -1022 && e <= 1023) return v * __longlong_as_double((long long)(e + 1023) << 52);
+  return ldexp(v, e);
+}
+
 struct TcArgs {
-  const uint8_t* a;        // pre-tiled A pieces: [piece][k tile][64-row tile][8 KB]
+  const uint8_t* a;        // pre-tiled A pieces: [piece][k tile][64-row block][4 KB]
   const uint8_t* b;        // pre-tiled B pieces, same layout
   long long a_piece, b_piece;  // bytes per piece
   int nkt;                 // K tiles per piece
-  int nrt_a, nrt_b;        // 64-row tiles of each operand (rows padded to 128)
+  int nrt_a, nrt_b;        // 64-row blocks of each operand (rows padded to 128)
   int nprod;               // products
   int8_t pa[64], pb[64], pacc[64];  // per product: A piece, B piece, accumulator
+  int8_t pfirst[64];       // 1 for the first product of its accumulator (starts it at K tile 0)
   int nacc;
   double acc_scale[kMaxAcc];   // per accumulator: 2^(-7 (s + 2)) (int8) or 1 (bf16)
   const int* erow;         // per row / column power-of-two exponents (int8), or null
@@ -144,18 +173,22 @@ struct TcArgs {
 
 template <int kKind>
 __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_constant__ TcArgs g) {
+  using Sh = TcShape<kKind>;
+  constexpr int kPieces = Sh::kPieces, kStages = Sh::kStages;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  // 1024-byte aligned stage ring: A tiles then B tiles; barriers after them
+  // 1024-byte aligned stage rings (A tiles, then B tiles); barriers and column tables after them
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* sa = smem;
-  uint8_t* sb = smem + kStages * kTileABytes;
-  uint64_t* full = reinterpret_cast<uint64_t*>(sb + kStages * kTileBBytes);
+  uint8_t* sb = smem + kStages * Sh::kStageA;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sb + kStages * Sh::kStageB);
   uint64_t* empty = full + kStages;
   uint64_t* done = empty + kStages;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   volatile uint32_t* abort_flag = tmem_slot + 1;
+  int* col_exp = reinterpret_cast<int*>(tmem_slot + 2);
+  int* col_off = col_exp + kTileN;
 
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tm = blockIdx.y, tn = blockIdx.x;
   const uint32_t ncols = (uint32_t)g.nacc * kTileN <= 64 ? 64u
                          : (uint32_t)g.nacc * kTileN <= 128 ? 128u
@@ -169,6 +202,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  if (tid < kTileN) {
+    // column rs of T -> offset r n^2 + s of [p][r][q][s], and its exponent
+    const int col = tn * kTileN + tid;
+    const bool in = col < g.N;
+    col_off[tid] = in ? (col / g.n) * g.n * g.n + col % g.n : 0;
+    col_exp[tid] = in && g.ecol ? g.ecol[col] : 0;
+  }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(ncols)
@@ -179,10 +219,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int nsteps = g.nprod * g.nkt;
+  const int nsteps = g.nkt;
 
   if (tid == 0) {
-    // producer: one A tile and one B tile per step into the stage ring
+    // producer: the K tile of every piece of both operands per stage
     int issued = 0;
     for (int t = 0; t < nsteps; ++t) {
       const int s = t % kStages, use = t / kStages;
@@ -192,13 +232,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
         break;
       }
       if (*abort_flag) break;
-      const int p = t / g.nkt, kt = t % g.nkt;
-      // a 128-row A tile is the two adjacent 64-row tiles 2 tm, 2 tm + 1 of its K tile
-      const uint8_t* asrc = g.a + g.pa[p] * g.a_piece + ((long long)kt * g.nrt_a + 2 * tm) * kTileBBytes;
-      const uint8_t* bsrc = g.b + g.pb[p] * g.b_piece + ((long long)kt * g.nrt_b + tn) * kTileBBytes;
-      mbar_expect_tx(&full[s], kTileABytes + kTileBBytes);
-      bulk_g2s(sa + s * kTileABytes, asrc, kTileABytes, &full[s]);
-      bulk_g2s(sb + s * kTileBBytes, bsrc, kTileBBytes, &full[s]);
+      mbar_expect_tx(&full[s], Sh::kStageA + Sh::kStageB);
+      // a 128-row A tile is the two adjacent 64-row blocks 2 tm, 2 tm + 1 of its K tile
+      const long long aoff = ((long long)t * g.nrt_a + 2 * tm) * kBlockBytes;
+      const long long boff = ((long long)t * g.nrt_b + tn) * kBlockBytes;
+#pragma unroll
+      for (int i = 0; i < kPieces; ++i)
+        bulk_g2s(sa + s * Sh::kStageA + i * kTileABytes, g.a + i * g.a_piece + aoff, kTileABytes, &full[s]);
+#pragma unroll
+      for (int j = 0; j < kPieces; ++j)
+        bulk_g2s(sb + s * Sh::kStageB + j * kTileBBytes, g.b + j * g.b_piece + boff, kTileBBytes, &full[s]);
       ++issued;
     }
     // the copies of the last stages must have landed before the CTA may exit (on the normal
@@ -206,8 +249,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
     for (int t = issued - kStages < 0 ? 0 : issued - kStages; t < issued; ++t)
       if (!mbar_wait(&full[t % kStages], (uint32_t)(t / kStages) & 1u)) atomicOr(g.err, 8u);
   } else if (tid == 32) {
-    // MMA issuer: four 32-byte K steps per stage into the product's accumulator
-    int issued = 0;
+    // MMA issuer: every product of the stage, two 32-byte K steps each, into its accumulator
     for (int t = 0; t < nsteps; ++t) {
       const int s = t % kStages, use = t / kStages;
       if (!mbar_wait(&full[s], (uint32_t)use & 1u)) {
@@ -216,58 +258,53 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
         break;
       }
       tc_fence_after();
-      const int p = t / g.nkt, kt = t % g.nkt;
-      const uint32_t dcol = tmem + (uint32_t)g.pacc[p] * kTileN;
-      // first K tile of the first product of each accumulator starts it
-      bool first = kt == 0;
-      for (int q = 0; q < p && first; ++q) first = g.pacc[q] != g.pacc[p];
-      const uint32_t a0 = smem_u32(sa + s * kTileABytes), b0 = smem_u32(sb + s * kTileBBytes);
+      const uint32_t a_st = smem_u32(sa + s * Sh::kStageA), b_st = smem_u32(sb + s * Sh::kStageB);
+      for (int p = 0; p < g.nprod; ++p) {
+        const uint32_t dcol = tmem + (uint32_t)g.pacc[p] * kTileN;
+        const bool first = t == 0 && g.pfirst[p];
+        const uint32_t a0 = a_st + (uint32_t)g.pa[p] * kTileABytes, b0 = b_st + (uint32_t)g.pb[p] * kTileBBytes;
 #pragma unroll
-      for (int k = 0; k < kKBytes / 32; ++k) {
-        const uint64_t ad = smem_desc(a0 + k * 256, 128, 1024);
-        const uint64_t bd = smem_desc(b0 + k * 256, 128, 1024);
-        mma<kKind>(dcol, ad, bd, (first && k == 0) ? 0u : 1u);
+        for (int k = 0; k < kKBytes / 32; ++k)
+          mma<kKind>(dcol, smem_desc(a0 + k * 256, 128, kSbo), smem_desc(b0 + k * 256, 128, kSbo),
+                     (first && k == 0) ? 0u : 1u);
       }
       mma_commit(&empty[s]);
-      ++issued;
     }
     mma_commit(done);  // arrives once every MMA issued above has completed
-    (void)issued;
   }
   __syncwarp();
-  // epilogue: every thread owns row 32 warp + lane of the tile
+  // epilogue: warp w owns TMEM lanes (rows) 32 (w % 4) + lane and columns 32 (w / 4) .. + 31
   const bool ok = mbar_wait(done, 0);
   tc_fence_after();
-  if (!ok) atomicOr(g.err, 4u);
-  const int row = tm * kTileM + warp * 32 + (tid & 31);
+  if (!ok && lane == 0) atomicOr(g.err, 4u);
+  const int quad = warp & 3, half = warp >> 2;
+  const int row = tm * kTileM + quad * 32 + lane;
   // warp-uniform: tcgen05.ld is a whole-warp instruction
   if (__all_sync(0xFFFFFFFFu, ok && !*abort_flag)) {
-    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-    const int p = row / g.n, q = row % g.n;
-    const int er = g.erow && row < g.M ? g.erow[row] : 0;
-    for (int c8 = 0; c8 < kTileN; c8 += 8) {
-      double v[8];
+    const uint32_t base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * 32);
+    double v[32];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) v[j] = 0.0;
-      for (int a = 0; a < g.nacc; ++a) {
-        uint32_t r[8];
-        tmem_ld8(lane_base + (uint32_t)(a * kTileN + c8), r);
-        tmem_wait_ld();
+    for (int j = 0; j < 32; ++j) v[j] = 0.0;
+    for (int a = 0; a < g.nacc; ++a) {
+      uint32_t r[32];
+      tmem_ld32(base + (uint32_t)(a * kTileN), r);
+      tmem_wait_ld();
+      const double sc = g.acc_scale[a];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const double x = kKind == 0 ? (double)__uint_as_float(r[j]) : (double)(int32_t)r[j];
-          v[j] += g.acc_scale[a] * x;
-        }
+      for (int j = 0; j < 32; ++j) {
+        const double x = kKind == 0 ? (double)__uint_as_float(r[j]) : i32_to_f64(r[j]);
+        v[j] += sc * x;
       }
-      if (row < g.M) {
+    }
+    if (row < g.M) {
+      const int p = row / g.n, q = row % g.n;
+      const long long roff = (long long)p * g.n * g.n * g.n + (long long)q * g.n;
+      const int er = g.erow ? g.erow[row] : 0;
+      double* out = g.out + roff;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int col = tn * kTileN + c8 + j;
-          if (col >= g.N) break;
-          const int r = col / g.n, s = col % g.n;
-          const int ec = g.ecol ? g.ecol[col] : 0;
-          g.out[(((long long)p * g.n + r) * g.n + q) * g.n + s] = ldexp(v[j], er + ec);
-        }
+      for (int j = 0; j < 32; ++j) {
+        const int c = half * 32 + j;
+        if (tn * kTileN + c < g.N) out[col_off[c]] = scale_pow2(v[j], er + col_exp[c]);
       }
     }
   }
@@ -279,14 +316,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
 
 // ---------------------------------------------------------------------------------------
 // Split kernels: FP64 factor F[k][row] (k < K, row < R; the K-major rows of the product) into
-// pieces in one pre-tiled layout shared by both operands: piece c holds, for each 128-byte K
-// tile kt and each 64-row tile rt, 8 KB of core matrices [row group of 8][16-byte K chunk]
-// [8 rows][16 bytes] at ((c * nkt + kt) * nrt + rt) * 8 KB; rows are padded to a multiple of
-// 128 with zeros, so a 128-row A tile is two adjacent 64-row tiles.
+// pieces in one pre-tiled layout shared by both operands: piece c holds, for each 64-byte K
+// tile kt and each 64-row block rt, 4 KB of core matrices [row group of 8][16-byte K chunk]
+// [8 rows][16 bytes] at ((c * nkt + kt) * nrt + rt) * 4 KB; rows are padded to a multiple of
+// 128 with zeros, so a 128-row A tile is two adjacent 64-row blocks.
 // ---------------------------------------------------------------------------------------
 __device__ __forceinline__ long long chunk_offset(int row, int kc, int nrt) {
-  const int kt = kc >> 3, c = kc & 7;
-  return ((long long)kt * nrt + (row >> 6)) * kTileBBytes + ((row & 63) >> 3) * 1024 + c * 128 + (row & 7) * 16;
+  constexpr int kChunks = kKBytes / 16;
+  const int kt = kc / kChunks, c = kc % kChunks;
+  return ((long long)kt * nrt + (row >> 6)) * kBlockBytes + ((row & 63) >> 3) * kSbo + c * 128 + (row & 7) * 16;
 }
 
 // Per-row exponents e with max_k |F[k][row]| * 2^-e <= 1/2 (0 for an all-zero or padding row).
@@ -309,7 +347,7 @@ __global__ void row_exponent_kernel(const double* __restrict__ f, int K, int R, 
 // a signed byte, |a_i| <= 64); one 16-byte store per slice.
 __global__ void int8_slices_kernel(const double* __restrict__ f, int K, int R, int rpad, int nkt,
                                    const int* __restrict__ e, int S, long long piece_bytes, uint8_t* __restrict__ out) {
-  const long long total = (long long)rpad * nkt * 8;
+  const long long total = (long long)rpad * nkt * (kKBytes / 16);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const int row = (int)(t % rpad), kc = (int)(t / rpad);
@@ -339,7 +377,7 @@ __global__ void int8_slices_kernel(const double* __restrict__ f, int K, int R, i
 // of one row) per thread.
 __global__ void bf16_pieces_kernel(const double* __restrict__ f, int K, int R, int rpad, int nkt,
                                    long long piece_bytes, uint8_t* __restrict__ out) {
-  const long long total = (long long)rpad * nkt * 8;
+  const long long total = (long long)rpad * nkt * (kKBytes / 16);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const int row = (int)(t % rpad), kc = (int)(t / rpad);
@@ -371,7 +409,7 @@ int pieces_of(int mode) { return mode == NW_TRANSFORM_CHOL_INT8 ? kOzakiSlices :
 size_t split_factor_bytes(int mode, int naux, int R) {
   const int kbytes = mode == NW_TRANSFORM_CHOL_INT8 ? naux : 2 * naux;
   const int nkt = (kbytes + kKBytes - 1) / kKBytes, rpad = (R + kTileM - 1) / kTileM * kTileM;
-  return (size_t)pieces_of(mode) * nkt * (rpad / 64) * kTileBBytes + (size_t)rpad * sizeof(int) + 256;
+  return (size_t)pieces_of(mode) * nkt * (rpad / 64) * kBlockBytes + (size_t)rpad * sizeof(int) + 256;
 }
 
 cudaError_t split_factor(cudaStream_t st, int mode, const double* F, int naux, int R, void* buf, size_t bytes,
@@ -384,10 +422,10 @@ cudaError_t split_factor(cudaStream_t st, int mode, const double* F, int naux, i
   f.R = R;
   f.rpad = (R + kTileM - 1) / kTileM * kTileM;
   f.nkt = (kbytes + kKBytes - 1) / kKBytes;
-  f.piece_bytes = (long long)f.nkt * (f.rpad / 64) * kTileBBytes;
+  f.piece_bytes = (long long)f.nkt * (f.rpad / 64) * kBlockBytes;
   f.pieces = static_cast<uint8_t*>(buf);
   f.exps = reinterpret_cast<int*>(f.pieces + (size_t)pieces_of(mode) * f.piece_bytes);
-  const long long chunks = (long long)f.rpad * f.nkt * 8;
+  const long long chunks = (long long)f.rpad * f.nkt * (kKBytes / 16);
   const int blocks = (int)std::min<long long>((chunks + 255) / 256, 148 * 16);
   if (mode == NW_TRANSFORM_CHOL_INT8) {
     row_exponent_kernel<<<(f.rpad + 255) / 256, 256, 0, st>>>(F, naux, R, f.rpad, f.exps);
@@ -424,6 +462,7 @@ cudaError_t split_product(cudaStream_t st, const SplitFactor& A, const SplitFact
         ++np;
       }
     g.nprod = np;
+    for (int p = 0; p < np; ++p) g.pfirst[p] = g.pa[p] == 0;  // (0, s) opens accumulator s
     g.nacc = kOzakiSlices;
     for (int s = 0; s < kOzakiSlices; ++s) g.acc_scale[s] = ldexp(1.0, -7 * (s + 2));
     g.erow = A.exps;
@@ -435,6 +474,7 @@ cudaError_t split_product(cudaStream_t st, const SplitFactor& A, const SplitFact
       g.pa[i] = pa[i];
       g.pb[i] = pb[i];
       g.pacc[i] = 0;
+      g.pfirst[i] = i == 0;
     }
     g.nprod = 6;
     g.nacc = 1;
@@ -445,17 +485,16 @@ cudaError_t split_product(cudaStream_t st, const SplitFactor& A, const SplitFact
   g.n = n;
   g.out = out;
   g.err = err;
-  const size_t smem = kStages * (kTileABytes + kTileBBytes) + 1024 + 256;
   const dim3 grid((unsigned)(B.rpad / kTileN), (unsigned)(A.rpad / kTileM));
   cudaError_t e;
   if (A.mode == NW_TRANSFORM_CHOL_INT8) {
-    e = cudaFuncSetAttribute(tc_gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(tc_gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcShape<1>::kSmem);
     if (e != cudaSuccess) return e;
-    tc_gemm_kernel<1><<<grid, kTcThreads, smem, st>>>(g);
+    tc_gemm_kernel<1><<<grid, kTcThreads, TcShape<1>::kSmem, st>>>(g);
   } else {
-    e = cudaFuncSetAttribute(tc_gemm_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(tc_gemm_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcShape<0>::kSmem);
     if (e != cudaSuccess) return e;
-    tc_gemm_kernel<0><<<grid, kTcThreads, smem, st>>>(g);
+    tc_gemm_kernel<0><<<grid, kTcThreads, TcShape<0>::kSmem, st>>>(g);
   }
   return cudaGetLastError();
 }
