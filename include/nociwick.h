@@ -45,7 +45,8 @@ typedef enum {
     NW_ERR_ALLOC = 3,        /* device or pinned host allocation failed            */
     NW_ERR_UNSUPPORTED = 4,  /* input outside what this build supports             */
     NW_ERR_STATE = 5,        /* call out of order (e.g. evaluate before build)     */
-    NW_ERR_NO_DEVICE = 6     /* no usable CUDA device                              */
+    NW_ERR_NO_DEVICE = 6,    /* no usable CUDA device                              */
+    NW_ERR_IO = 7            /* a cache file could not be created, read or written  */
 } nw_status;
 
 /* Matrix-element conventions for reference pairs with zero-overlap orbital pairs (m > 0).
@@ -175,6 +176,31 @@ NW_API nw_status nw_transform_product(int32_t mode, const double* u, const doubl
 
 /* Zero-overlap counts (m_alpha, m_beta) of ordered pair x*nref + w, as planned by
  * plan_wicks_pairs (src/noci/wicks.rs:90-121).  m must hold 2*nref*nref ints. */
+/* Blocked (out-of-core) evaluation for systems whose intermediates exceed the device memory
+ * (at n = 64 each ordered reference pair without zero-overlap orbitals holds 0.4 GB, so about
+ * 20 references fill 180 GB): the ordered reference pairs are cut, in index order, into blocks
+ * whose slab fits slab_budget bytes (0: the free device memory less 8 GB); each block is built
+ * and the whole request evaluated against it, each block writing the (H, S) of its own
+ * reference pairs.  Results equal one full build's bit for bit.  Device buffers, synchronous;
+ * *nblocks (if not null) receives the number of blocks.  Afterwards the context holds the last
+ * block, and the other evaluation, matrix, QMC, PT2 and cache calls return NW_ERR_STATE until
+ * nw_build_intermediates (unless one block held every reference pair).  NW_ERR_ALLOC when one
+ * reference pair alone exceeds the budget. */
+NW_API nw_status nw_eval_hs_pairs_blocked(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* hs_dev,
+                                          uint64_t slab_budget, uint32_t* nblocks, void* stream);
+
+/* On-disk cache of the built intermediates (the counterpart of the reference's wicks.bin /
+ * wicks.meta, src/nonorthogonalwicks/storage.rs:19,164-240): nw_save_intermediates writes the
+ * slab (and the Fock basis the build keeps) to slab_path and the versioned per-reference-pair
+ * tables to meta_path; nw_load_intermediates restores them into a context created with the same
+ * system and options instead of nw_build_intermediates.  Loading checks the format version, the
+ * geometry, tol, convention, transform and a hash of every input of the build (S, h, the
+ * two-electron integrals or Cholesky vectors, the reference orbitals): a cache of another system
+ * gives NW_ERR_INVALID, an unreadable file NW_ERR_IO.  The format is this engine's own slab
+ * layout, not the reference's. */
+NW_API nw_status nw_save_intermediates(nw_ctx* ctx, const char* slab_path, const char* meta_path);
+NW_API nw_status nw_load_intermediates(nw_ctx* ctx, const char* slab_path, const char* meta_path);
+
 NW_API nw_status nw_pair_zero_counts(const nw_ctx* ctx, int32_t* m);
 
 /* Upload the determinant basis once (host array of ndet records); it stays resident.
@@ -510,9 +536,14 @@ NW_API nw_status nw_autotune(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs
  * recorded on its stream while timing is enabled: ms[0] classify, ms[1] scan, ms[2] scatter,
  * ms[3] the evaluators (the m = 0 classes and the m > 0 generic evaluator run concurrently on
  * forked streams, so they are timed together), ms[4] the m > 0 generic evaluator alone (events
- * on its forked stream; 0 when the call had no such pair).  nw_last_timings waits for that call. */
+ * on its forked stream; 0 when the call had no such pair).  nw_last_timings waits for that call.
+ * enable = 2 is a profiling mode: the class evaluators run one after another on the call's
+ * stream (same kernels and work, no overlap), and nw_last_class_timings gives each one's device
+ * time: ms[0] light, ms[1] medium, ms[2] heavy, ms[3] runtime rank, ms[4] the m > 0 generic
+ * evaluator (the F+S path has no medium and runtime-rank kernels: 0 there). */
 NW_API nw_status nw_set_timing(nw_ctx* ctx, int enable);
 NW_API nw_status nw_last_timings(nw_ctx* ctx, float* ms);
+NW_API nw_status nw_last_class_timings(nw_ctx* ctx, float* ms);
 
 NW_API nw_status nw_ctx_info(const nw_ctx* ctx, nw_info* out);
 NW_API nw_status nw_ctx_destroy(nw_ctx* ctx);

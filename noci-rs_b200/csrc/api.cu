@@ -191,6 +191,8 @@ const char* nw_status_string(nw_status st) {
       return "call out of order";
     case NW_ERR_NO_DEVICE:
       return "no CUDA device";
+    case NW_ERR_IO:
+      return "cache file input/output failed";
   }
   return "unknown status";
 }
@@ -347,7 +349,7 @@ nw_status nw_transform_product(int32_t mode, const double* u, const double* v, i
 nw_status nw_build_intermediates(nw_ctx* ctx) {
   if (!ctx) return NW_ERR_INVALID;
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
-  return nw::build_all(ctx);
+  return nw::build_all(ctx, nullptr);
 }
 
 nw_status nw_pair_zero_counts(const nw_ctx* ctx, int32_t* m) {
@@ -398,6 +400,15 @@ nw_status nw_set_basis(nw_ctx* ctx, const nw_det* basis, uint64_t ndet) {
   NW_CUDA(ctx, cudaMemcpy(ctx->d_desc, desc.data(), ndet * sizeof(uint16_t), cudaMemcpyHostToDevice));
   ctx->ndet = ndet;
   return NW_OK;
+}
+
+nw_status nw_eval_hs_pairs_blocked(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* hs_dev,
+                                   uint64_t slab_budget, uint32_t* nblocks, void* stream) {
+  if (!ctx || (npairs && (!pairs_dev || !hs_dev))) return NW_ERR_INVALID;
+  if (ctx->live_qmc > 0)
+    return nw::fail(ctx, NW_ERR_STATE, "a QMC object uses the intermediates (nw_qmc_destroy it first)");
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  return nw::eval_blocked(ctx, pairs_dev, npairs, hs_dev, slab_budget, static_cast<cudaStream_t>(stream), nblocks);
 }
 
 nw_status nw_eval_hs_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* hs_dev,
@@ -480,11 +491,26 @@ nw_status nw_sync(nw_ctx* ctx, void* stream) {
 nw_status nw_set_timing(nw_ctx* ctx, int enable) {
   if (!ctx) return NW_ERR_INVALID;
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (enable < 0 || enable > 2) return NW_ERR_INVALID;
   if (enable && !ctx->ev[0]) {
     for (int i = 0; i < 8; ++i) NW_CUDA(ctx, cudaEventCreate(&ctx->ev[i]));
   }
+  if (enable == 2 && !ctx->evc[0]) {
+    for (int i = 0; i < 6; ++i) NW_CUDA(ctx, cudaEventCreate(&ctx->evc[i]));
+  }
   ctx->timing = enable != 0;
+  ctx->serial_classes = enable == 2;
   ctx->timed_valid = false;
+  ctx->timed_classes = false;
+  return NW_OK;
+}
+
+nw_status nw_last_class_timings(nw_ctx* ctx, float* ms) {
+  if (!ctx || !ms) return NW_ERR_INVALID;
+  if (!ctx->timed_valid || !ctx->timed_classes)
+    return nw::fail(ctx, NW_ERR_STATE, "no serially timed evaluation recorded (nw_set_timing(ctx, 2))");
+  NW_CUDA(ctx, cudaEventSynchronize(ctx->evc[5]));
+  for (int i = 0; i < 5; ++i) NW_CUDA(ctx, cudaEventElapsedTime(&ms[i], ctx->evc[i], ctx->evc[i + 1]));
   return NW_OK;
 }
 
@@ -503,7 +529,7 @@ nw_status nw_ctx_info(const nw_ctx* ctx, nw_info* out) {
   std::memset(out, 0, sizeof(*out));
   out->nref = ctx->nref;
   out->nmo = ctx->nmo;
-  out->ngeneric = ctx->built ? ctx->nref * ctx->nref - ctx->nfast : 0;
+  out->ngeneric = ctx->built ? ctx->nresident - ctx->nfast : 0;
   out->slab_bytes = ctx->slab_bytes;
   out->ndet = ctx->ndet;
   return NW_OK;
@@ -540,6 +566,8 @@ nw_status nw_ctx_destroy(nw_ctx* ctx) {
   if (ctx->h_flag) cudaFreeHost(ctx->h_flag);
   for (int i = 0; i < 8; ++i)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+  for (int i = 0; i < 6; ++i)
+    if (ctx->evc[i]) cudaEventDestroy(ctx->evc[i]);
   for (cudaStream_t q : {ctx->s_in, ctx->s_comp, ctx->s_out, ctx->s_aux[0], ctx->s_aux[1], ctx->s_aux[2]})
     if (q) cudaStreamDestroy(q);
   for (cudaEvent_t e : {ctx->ev_start, ctx->ev_in[0], ctx->ev_in[1], ctx->ev_comp[0], ctx->ev_comp[1], ctx->ev_fork,

@@ -443,13 +443,20 @@ cudaError_t swap_qr(cudaStream_t st, const double* src, int n, double* dst) {
   return cudaGetLastError();
 }
 
-nw_status build_all(nw_ctx* ctx) {
+nw_status build_all(nw_ctx* ctx, const std::vector<char>* subset) {
   const int n = ctx->nmo, nao = ctx->nao, nref = ctx->nref;
   const int npair = nref * nref, nps = 2 * npair;
   const int oa = ctx->nocc_a, ob = ctx->nocc_b, omax = std::max(oa, ob);
   const size_t n2 = (size_t)n * n, n4 = n2 * n2;
   if (nao != n) return fail(ctx, NW_ERR_UNSUPPORTED, "this build requires nao == nmo");
+  if (subset && subset->size() != (size_t)npair) return fail(ctx, NW_ERR_INVALID, "reference-pair subset size");
   const cudaStream_t h = 0;  // the build runs on the legacy default stream
+  // a rebuild replaces the slab: nothing evaluates until it has completed
+  ctx->built = false;
+  ctx->partial = false;
+  // the ordered reference pairs whose slab pieces this build holds (all, or a block of a
+  // blocked evaluation); every per-pair scalar and the Fock basis cover all pairs
+  auto resident = [&](int p) { return !subset || (*subset)[p] != 0; };
 
   // ---------------- workspace ----------------
   const size_t per_ps = 2 * (size_t)nao * omax + omax + 2 * n2 /*M*/ + 4 * n2 /*rowc colc cxs cws*/ +
@@ -677,6 +684,7 @@ nw_status build_all(nw_ctx* ctx) {
   std::vector<FastOff> fo(npair);
   std::vector<GenOff> go(npair);
   for (int p = 0; p < npair; ++p) {
+    if (!resident(p)) continue;
     if (!generic[p]) {
       for (int s = 0; s < 2; ++s) {
         fo[p].recx[s] = reserve(2 * n2);
@@ -729,6 +737,7 @@ nw_status build_all(nw_ctx* ctx) {
   std::memset(hfast.data(), 0, sizeof(FastPair) * npair);
   std::memset(hgen.data(), 0, sizeof(GenPair) * npair);
   for (int p = 0; p < npair; ++p) {
+    if (!resident(p)) continue;
     const int psa = 2 * p, psb = 2 * p + 1;
     auto CX = [&](int ps, int m) { return cx + ((size_t)ps * 2 + m) * n2; };
     auto XC = [&](int ps, int m) { return xc + ((size_t)ps * 2 + m) * n2; };
@@ -845,13 +854,16 @@ nw_status build_all(nw_ctx* ctx) {
   }
 
   // ---------------- tables ----------------
-  ctx->order_host.assign(npair, 0);
+  // sort positions: the resident m = 0 pairs, then the resident others; -1 marks a pair whose
+  // slab pieces this build does not hold (its pairs are skipped by the evaluators)
+  ctx->order_host.assign(npair, -1);
   int pos = 0;
   for (int p = 0; p < npair; ++p)
-    if (!generic[p]) ctx->order_host[p] = pos++;
+    if (resident(p) && !generic[p]) ctx->order_host[p] = pos++;
   ctx->nfast = pos;
   for (int p = 0; p < npair; ++p)
-    if (generic[p]) ctx->order_host[p] = pos++;
+    if (resident(p) && generic[p]) ctx->order_host[p] = pos++;
+  ctx->nresident = pos;
   if (!ctx->d_fast) NW_CUDA(ctx, cudaMalloc(&ctx->d_fast, sizeof(FastPair) * npair));
   if (!ctx->d_gen) NW_CUDA(ctx, cudaMalloc(&ctx->d_gen, sizeof(GenPair) * npair));
   if (!ctx->d_order) NW_CUDA(ctx, cudaMalloc(&ctx->d_order, sizeof(int32_t) * npair));
@@ -882,7 +894,30 @@ nw_status build_all(nw_ctx* ctx) {
     if (err) return fail(ctx, NW_ERR_CUDA, "tcgen05 split product gave up waiting (flags " + std::to_string(err) + ")");
   }
   ctx->built = true;
+  ctx->partial = pos < npair;
   return NW_OK;
+}
+
+// Slab doubles of one ordered reference pair under the layout of build_all (the same rounding
+// of every piece to 256 bytes): the fast layout, or the reference-ordered one with the J and II
+// slots its zero-overlap counts (m_alpha, m_beta) need.
+size_t pair_slab_doubles(int n, int ma, int mb) {
+  const size_t n2 = (size_t)n * n, n4 = n2 * n2;
+  auto r = [](size_t d) { return ((d + 31) / 32) * 32; };
+  if (ma + mb == 0) return 2 * (2 * r(2 * n2) + r(n4)) + r(n4);
+  static const int br[10][4] = {{0, 0, 0, 0}, {0, 0, 0, 1}, {0, 0, 1, 0}, {0, 0, 1, 1}, {0, 1, 0, 1},
+                                {0, 1, 1, 0}, {0, 1, 1, 1}, {1, 0, 1, 0}, {1, 0, 1, 1}, {1, 1, 1, 1}};
+  size_t t = 0;
+  for (int ms : {ma, mb}) {
+    t += 4 * r(n2) + 4 * r(n2) + 8 * r(n2);
+    for (int sl = 0; sl < 10; ++sl) t += (br[sl][0] + br[sl][1] + br[sl][2] + br[sl][3] <= ms) ? r(n4) : 0;
+  }
+  t += 16 * r(n2);
+  for (int k = 0; k < 16; ++k) {
+    const int a0 = (k >> 3) & 1, az = (k >> 2) & 1, b0 = (k >> 1) & 1, by = k & 1;
+    t += (a0 + az <= ma && b0 + by <= mb) ? r(n4) : 0;
+  }
+  return t;
 }
 
 // Fock tables for the F + S path (update_wicks_fock, src/noci/wicks.rs:290-330, with

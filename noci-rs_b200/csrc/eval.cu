@@ -455,7 +455,9 @@ __global__ void __launch_bounds__(128) eval_s_kernel(EvalParams P, const uint32_
       continue;
     }
     const int p = (int)x.parent * P.nref + (int)w.parent;
-    const bool fast = __ldg(P.order + p) < P.nfast;
+    const int ord = __ldg(P.order + p);
+    if (ord < 0) continue;  // reference pair outside the resident block
+    const bool fast = ord < P.nfast;
     out[i] = eval_s_pair(fast ? P.fast + p : nullptr, fast ? nullptr : P.gen + p, x, w, P.n, P.nocc_a, P.nocc_b);
   }
 }
@@ -502,7 +504,7 @@ uint64_t plan_keys(const nw_ctx* ctx, EvalParams& P, uint64_t cap) {
   uint32_t nb = 1;
   P.shift = sort_key_shift(P.ndet, ctx->nref, cap, &nb);
   P.nbucket = nb;
-  const uint64_t ngen = (uint64_t)ctx->nref * ctx->nref - (uint64_t)ctx->nfast;
+  const uint64_t ngen = (uint64_t)ctx->nresident - (uint64_t)ctx->nfast;
   return (uint64_t)kClasses * nb + (uint64_t)kGenClasses * ngen;
 }
 
@@ -544,36 +546,62 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
   // medium, the heavy / runtime-rank and the zero-overlap generic classes run on streams forked
   // off the launching one, beside the light classes, and join before the call returns (also
   // inside a stream capture: the forked streams join the capture through the fork event).
-  const bool fast = ctx->nfast > 0, gen = ctx->nfast < ctx->nref * ctx->nref;
-  NW_CUDA(ctx, cudaEventRecord(ctx->ev_fork, stream));
-  for (int i = 0; i < 3; ++i) NW_CUDA(ctx, cudaStreamWaitEvent(ctx->s_aux[i], ctx->ev_fork, 0));
+  const bool fast = ctx->nfast > 0, gen = ctx->nfast < ctx->nresident;
+  // Serial per-class timing (a profiling mode, timing enabled): every class kernel on the
+  // launching stream, in the order light, medium, heavy, runtime rank, generic, each between two
+  // events; the kernels and their work are the same, only their overlap is given up.
+  const bool serial = ev != nullptr && ctx->serial_classes;
+  cudaStream_t sq[4] = {stream, ctx->s_aux[0], ctx->s_aux[1], ctx->s_aux[2]};
+  if (serial) {
+    for (int i = 1; i < 4; ++i) sq[i] = stream;
+    NW_CUDA(ctx, cudaEventRecord(ctx->evc[0], stream));
+  } else {
+    NW_CUDA(ctx, cudaEventRecord(ctx->ev_fork, stream));
+    for (int i = 0; i < 3; ++i) NW_CUDA(ctx, cudaStreamWaitEvent(ctx->s_aux[i], ctx->ev_fork, 0));
+  }
+  auto mark = [&](int i) -> cudaError_t { return serial ? cudaEventRecord(ctx->evc[i], stream) : cudaSuccess; };
   if (fast) {
     if (mode == EvalMode::kFS) {
-      eval_fs_light_kernel<<<grid_stride_blocks(npairs, 256, per_sm), 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
-      eval_fs_heavy_kernel<<<148 * 2, 256, 0, ctx->s_aux[0]>>>(P, pp, S.sidx, S.offsets, out);
+      eval_fs_light_kernel<<<grid_stride_blocks(npairs, 256, per_sm), 256, 0, sq[0]>>>(P, pp, S.sidx, S.offsets, out);
+      NW_CUDA(ctx, mark(1));
+      NW_CUDA(ctx, mark(2));
+      eval_fs_heavy_kernel<<<148 * 2, 256, 0, sq[1]>>>(P, pp, S.sidx, S.offsets, out);
+      NW_CUDA(ctx, mark(3));
+      NW_CUDA(ctx, mark(4));
     } else {
-      eval_light_kernel<<<grid_stride_blocks(npairs, 256, per_sm), 256, 0, stream>>>(P, pp, S.sidx, S.offsets, out);
-      eval_medium_kernel<<<148 * 2, 256, 0, ctx->s_aux[0]>>>(P, pp, S.sidx, S.offsets, out);
-      eval_heavy_kernel<<<148, 256, 0, ctx->s_aux[1]>>>(P, pp, S.sidx, S.offsets, out);
-      eval_rt_kernel<<<148 * 2, 128, 0, ctx->s_aux[1]>>>(P, pp, S.sidx, S.offsets, out);
+      eval_light_kernel<<<grid_stride_blocks(npairs, 256, per_sm), 256, 0, sq[0]>>>(P, pp, S.sidx, S.offsets, out);
+      NW_CUDA(ctx, mark(1));
+      eval_medium_kernel<<<148 * 2, 256, 0, sq[1]>>>(P, pp, S.sidx, S.offsets, out);
+      NW_CUDA(ctx, mark(2));
+      eval_heavy_kernel<<<148, 256, 0, sq[2]>>>(P, pp, S.sidx, S.offsets, out);
+      NW_CUDA(ctx, mark(3));
+      eval_rt_kernel<<<148 * 2, 128, 0, sq[2]>>>(P, pp, S.sidx, S.offsets, out);
+      NW_CUDA(ctx, mark(4));
     }
     NW_CUDA(ctx, cudaGetLastError());
+  } else {
+    for (int i = 1; i <= 4; ++i) NW_CUDA(ctx, mark(i));
   }
   if (gen) {
-    NW_CUDA(ctx, cudaMemsetAsync(S.work, 0, sizeof(uint32_t), ctx->s_aux[2]));
-    if (ev) NW_CUDA(ctx, cudaEventRecord(ev[6], ctx->s_aux[2]));
+    NW_CUDA(ctx, cudaMemsetAsync(S.work, 0, sizeof(uint32_t), sq[3]));
+    if (ev && !serial) NW_CUDA(ctx, cudaEventRecord(ev[6], sq[3]));
     if (mode == EvalMode::kFS)
-      eval_fs_gen_kernel<<<148 * 4, 128, 0, ctx->s_aux[2]>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out, S.work);
+      eval_fs_gen_kernel<<<148 * 4, 128, 0, sq[3]>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out, S.work);
     else
-      eval_gen_kernel<<<148 * 4, 128, 0, ctx->s_aux[2]>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out, S.work);
+      eval_gen_kernel<<<148 * 4, 128, 0, sq[3]>>>(P, pp, S.sidx, S.offsets, (int)nkeys, out, S.work);
     NW_CUDA(ctx, cudaGetLastError());
-    if (ev) NW_CUDA(ctx, cudaEventRecord(ev[7], ctx->s_aux[2]));
+    if (ev && !serial) NW_CUDA(ctx, cudaEventRecord(ev[7], sq[3]));
   }
-  if (ev) ctx->timed_gen = gen;
-  for (int i = 0; i < 3; ++i) {
-    NW_CUDA(ctx, cudaEventRecord(ctx->ev_join[i], ctx->s_aux[i]));
-    NW_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->ev_join[i], 0));
+  NW_CUDA(ctx, mark(5));
+  if (ev) {
+    ctx->timed_gen = gen && !serial;
+    ctx->timed_classes = serial;
   }
+  if (!serial)
+    for (int i = 0; i < 3; ++i) {
+      NW_CUDA(ctx, cudaEventRecord(ctx->ev_join[i], ctx->s_aux[i]));
+      NW_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->ev_join[i], 0));
+    }
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[4], stream));
   if (ev) NW_CUDA(ctx, cudaEventRecord(ev[5], stream));
   return NW_OK;
@@ -587,9 +615,80 @@ nw_status eval_pairs(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double
   return eval_pairs_on(ctx, make_params(ctx), pairs, npairs, out, mode, stream, clear_flag);
 }
 
+// Blocked evaluation for systems whose intermediates exceed the device memory: a build of no
+// slab (the pairing, every per-pair scalar and the zero-overlap counts) sizes each ordered
+// reference pair's slab pieces; the pairs are cut, in index order, into blocks whose slab fits
+// `budget` bytes (0: the free device memory less 8 GB for the evaluation and the build
+// workspace); each block is built and the whole request evaluated against it, every block
+// writing the elements of its own reference pairs (the others are skipped by classify).  The
+// results equal those of one full build bit for bit: every block computes its pairs'
+// intermediates with the same products.  The context keeps the last block afterwards
+// (`partial`): other evaluations refuse it until nw_build_intermediates.
+nw_status eval_blocked(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* hs, uint64_t budget,
+                       cudaStream_t stream, uint32_t* nblocks) {
+  if (nblocks) *nblocks = 0;
+  if (!ctx->d_dets) return fail(ctx, NW_ERR_STATE, "no determinant basis set");
+  const int npair = ctx->nref * ctx->nref, n = ctx->nmo;
+  if (budget == 0) {
+    size_t fr = 0, tot = 0;
+    NW_CUDA(ctx, cudaMemGetInfo(&fr, &tot));
+    const size_t reserve = 8ull << 30;
+    budget = fr > reserve ? fr - reserve : 0;
+    if (ctx->d_slab) budget += ctx->slab_bytes;  // the current slab is freed by the next build
+  }
+  std::vector<char> none(npair, 0);
+  nw_status st = build_all(ctx, &none);
+  if (st != NW_OK) return st;
+  std::vector<size_t> bytes(npair);
+  size_t total = 0;
+  for (int p = 0; p < npair; ++p) {
+    bytes[p] = pair_slab_doubles(n, ctx->m_counts[2 * p], ctx->m_counts[2 * p + 1]) * sizeof(double);
+    if (bytes[p] > budget)
+      return fail(ctx, NW_ERR_ALLOC, "one reference pair's intermediates exceed the blocked-evaluation budget");
+    total += bytes[p];
+  }
+  std::vector<std::vector<char>> blocks;
+  {
+    std::vector<char> cur(npair, 0);
+    size_t used = 0;
+    bool any = false;
+    for (int p = 0; p < npair; ++p) {
+      if (used + bytes[p] > budget && any) {
+        blocks.push_back(cur);
+        std::fill(cur.begin(), cur.end(), 0);
+        used = 0;
+        any = false;
+      }
+      cur[p] = 1;
+      used += bytes[p];
+      any = true;
+    }
+    if (any) blocks.push_back(cur);
+  }
+  (void)total;
+  for (size_t b = 0; b < blocks.size(); ++b) {
+    const bool all = blocks.size() == 1;
+    if ((st = build_all(ctx, all ? nullptr : &blocks[b])) != NW_OK) return st;
+    ctx->allow_partial = true;
+    st = eval_pairs_on(ctx, make_params(ctx), pairs, npairs, hs, EvalMode::kHS, stream, true);
+    ctx->allow_partial = false;
+    if (st != NW_OK) return st;
+    // the flag of out-of-range indices is read once per block: stop at the first report
+    uint32_t flag = 0;
+    NW_CUDA(ctx, cudaMemcpyAsync(ctx->h_flag, ctx->flag.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    NW_CUDA(ctx, cudaStreamSynchronize(stream));
+    flag = *ctx->h_flag;
+    if (flag) return fail(ctx, NW_ERR_INVALID, "pair index out of range of the determinant basis");
+  }
+  if (nblocks) *nblocks = (uint32_t)blocks.size();
+  return NW_OK;
+}
+
 nw_status eval_pairs_on(nw_ctx* ctx, EvalParams P, const uint32_t* pairs, uint64_t npairs, double* out, EvalMode mode,
                         cudaStream_t stream, bool clear_flag) {
   if (!ctx->built) return fail(ctx, NW_ERR_STATE, "intermediates not built");
+  if (ctx->partial && !ctx->allow_partial)
+    return fail(ctx, NW_ERR_STATE, "the intermediates hold one block of a blocked evaluation (rebuild them)");
   if (mode == EvalMode::kFS && !ctx->fock_ready) return fail(ctx, NW_ERR_STATE, "Fock tables not set (nw_update_fock)");
   const bool overlap_only = mode == EvalMode::kS;
   if (npairs == 0) return NW_OK;
@@ -693,6 +792,8 @@ nw_status noalloc_scratch(nw_ctx* ctx, unsigned char** out) {
 
 nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, cudaStream_t stream) {
   if (!ctx->built) return fail(ctx, NW_ERR_STATE, "intermediates not built");
+  if (ctx->partial && !ctx->allow_partial)
+    return fail(ctx, NW_ERR_STATE, "the intermediates hold one block of a blocked evaluation (rebuild them)");
   if (!ctx->d_dets) return fail(ctx, NW_ERR_STATE, "no determinant basis set");
   if (npairs > kNoallocMaxPairs)
     return fail(ctx, NW_ERR_UNSUPPORTED, "allocation-free evaluation takes at most " +
@@ -708,7 +809,7 @@ nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs
   if (st != NW_OK) return st;
   if (npairs == 0) return NW_OK;
   EvalParams P = make_params(ctx);
-  const uint64_t ngen = (uint64_t)ctx->nref * ctx->nref - (uint64_t)ctx->nfast;
+  const uint64_t ngen = (uint64_t)ctx->nresident - (uint64_t)ctx->nfast;
   // the same fine-key budget as the allocating path (nw_autotune's choice when there is one),
   // clamped to the keys the fixed array holds
   const uint64_t budget =

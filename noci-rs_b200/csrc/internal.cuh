@@ -70,6 +70,9 @@ struct nw_ctx {
   nw::GenPair* d_gen = nullptr;
   int32_t* d_order = nullptr;
   int nfast = 0;
+  int nresident = 0;               // ordered pairs whose slab pieces are built (sort positions)
+  bool partial = false;            // the slab holds one block of a blocked evaluation
+  bool allow_partial = false;      // set by the blocked evaluation while it evaluates a block
   std::vector<int32_t> m_counts;   // 2 per ordered pair
   std::vector<int32_t> order_host; // ordered pair -> sort position
 
@@ -109,8 +112,10 @@ struct nw_ctx {
   cusolverDnHandle_t solver = nullptr;  // created by the first generalised eigensolve
   std::string last_error;
 
-  // optional per-phase timing of the evaluation pipeline
+  // optional per-phase timing of the evaluation pipeline; serial_classes runs the class
+  // evaluators one after another on the launching stream, each between two of evc[0..5]
   bool timing = false;
+  bool serial_classes = false;
   // launch configuration chosen by nw_autotune (0: defaults)
   double tune_keys_per_pair = 0.0;  // fine sort-key budget of nw_eval_hs_pairs* per pair
   int live_qmc = 0;                 // QMC objects evaluating against the resident basis
@@ -120,6 +125,8 @@ struct nw_ctx {
   // phase events: ev[0..5] on the launching stream, ev[6] / ev[7] around the m > 0 evaluator on
   // its forked stream
   cudaEvent_t ev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t evc[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool timed_classes = false;       // the last timed call recorded evc (serial_classes)
 };
 
 namespace nw {
@@ -162,7 +169,17 @@ cudaError_t split_product_pqrs(cudaStream_t st, int mode, int slices, const doub
 cudaError_t swap_qr(cudaStream_t st, const double* src, int n, double* dst);
 
 // Build (build.cu).
-nw_status build_all(nw_ctx* ctx);
+// Build of the intermediates of every ordered reference pair, or of the pairs flagged in
+// `subset` (nref^2 flags; the others get sort position -1 and are skipped by the evaluators).
+nw_status build_all(nw_ctx* ctx, const std::vector<char>* subset = nullptr);
+// Slab doubles of one ordered reference pair with zero-overlap counts (ma, mb).
+size_t pair_slab_doubles(int n, int ma, int mb);
+// Blocked evaluation of (H, S) over blocks of reference pairs whose slab fits `budget` bytes.
+nw_status eval_blocked(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* hs, uint64_t budget,
+                       cudaStream_t stream, uint32_t* nblocks);
+// On-disk cache of the built intermediates (storage.cu).
+nw_status save_intermediates(nw_ctx* ctx, const char* slab_path, const char* meta_path);
+nw_status load_intermediates(nw_ctx* ctx, const char* slab_path, const char* meta_path);
 // Fock tables from AO Fock matrices (build.cu).
 nw_status update_fock(nw_ctx* ctx, const double* fa, const double* fb);
 

@@ -19,7 +19,10 @@
 //               A P^-1 with two Gram-Schmidt passes (here classical, as two matrix-vector
 //               products per pass, in place of the reference's two modified passes), Givens
 //               rotations, back substitution, restart from the true residual; convergence on
-//               |r| / sqrt(n) <= res_tol.
+//               |r| / sqrt(n) <= res_tol.  Each Arnoldi step runs on the device (own two-pass
+//               reduction kernels; the Hessenberg matrix, rotations and stopping rule in device
+//               memory); on the packed path the step is one CUDA graph, replayed for every step
+//               of a cycle without host synchronisation (one per restart cycle).
 //   precond   : Preconditioner::new / apply (src/snoci/types.rs:161-288): diagonal inverse with
 //               the reference's floor, and the Woodbury rank-2 correction for the projection.
 #include <cuda_runtime.h>
@@ -27,6 +30,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <new>
 #include <string>
 #include <vector>
@@ -64,7 +68,9 @@ __device__ inline void tile_of(uint64_t t, uint64_t nb, uint64_t* I, uint64_t* J
 constexpr int kSymvRows = 2;
 
 __global__ void __launch_bounds__(kTile, 2) packed_symv_kernel(const double* __restrict__ m, uint64_t n, uint64_t nb,
-                                                               const double* __restrict__ x, double* __restrict__ y) {
+                                                               const double* __restrict__ x, double* __restrict__ y,
+                                                               const int* __restrict__ skip) {
+  if (skip && *skip) return;  // a finished Arnoldi cycle (device-side GMRES)
   __shared__ double xrow[kTile];
   __shared__ double rowsum[kTile];
   __shared__ double colsum[kTileWarps][kTile];
@@ -215,6 +221,256 @@ __global__ void mul_kernel(const double* __restrict__ a, const double* __restric
 
 inline int grid_n(uint64_t n) { return (int)std::min<uint64_t>((n + 255) / 256, 148 * 16); }
 
+// ---------------------------------------------------------------------------------------
+// Device-side Arnoldi step of GMRES (one CUDA graph per solve on the packed path).  The
+// scalars of the cycle live on the device (ArnoldiState, the Hessenberg matrix, the Givens
+// rotations and the rotated right-hand side g); every reduction is two-pass and in a fixed
+// order (per-block partial sums, then one ordered sum), and every kernel returns at once when
+// the cycle is done, so the host can queue the `inner` steps of a cycle back to back and
+// synchronise once per cycle (gmres.rs:197-266 for the rotations and the stopping rule).
+// ---------------------------------------------------------------------------------------
+constexpr int kVB = 256;            // threads of the vector kernels
+constexpr int kVBlocks = 148 * 4;   // blocks of the vector kernels = partial sums per reduction
+
+struct ArnoldiState {
+  int k;        // current column
+  int inner;    // columns of this cycle
+  int done;     // the cycle has finished (converged, breakdown or k == inner)
+  int kfinal;   // columns completed
+  int col;      // column that receives w / h_{k+1,k}
+  int pad;
+  double tol;   // res_tol sqrt(n): the stopping bound on |g[k+1]|
+  double inv;   // 1 / h_{k+1,k} (0 on breakdown)
+};
+
+constexpr double kArnoldiSmall = 1e-14;
+
+// Sum over the block of v (thread 0 gets the total); sh holds 32 doubles.
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (wid == 0) {
+    t = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xFFFFFFFFu, t, o);
+  }
+  return t;
+}
+
+// Ordered sum of the kVBlocks partials part[b * stride + j] (every thread gets it).
+__device__ __forceinline__ double sum_partials(const double* __restrict__ part, int stride, int j, double* sh) {
+  double v = 0.0;
+  for (int b = threadIdx.x; b < kVBlocks; b += blockDim.x) v += part[(size_t)b * stride + j];
+  v = block_sum(v, sh);
+  if (threadIdx.x == 0) sh[32] = v;
+  __syncthreads();
+  v = sh[32];
+  __syncthreads();
+  return v;
+}
+
+// z = P^-1 q_k, diagonal part: z = dinv (.) q_k, with partial sums of (v0.z, v1.z) when the
+// Woodbury correction follows, else of (s_0a.z, f_0a.z) for the projection.
+__global__ void __launch_bounds__(kVB) arn_precond_kernel(const ArnoldiState* __restrict__ st, const double* __restrict__ Q,
+                                                          const double* __restrict__ dinv, const double* __restrict__ u0,
+                                                          const double* __restrict__ u1, uint64_t n, double* __restrict__ z,
+                                                          double* __restrict__ part) {
+  __shared__ double sh[33];
+  if (st->done) return;
+  const double* q = Q + (uint64_t)st->k * n;
+  double a0 = 0.0, a1 = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)kVB + threadIdx.x; i < n; i += (uint64_t)kVBlocks * kVB) {
+    const double v = q[i] * dinv[i];
+    z[i] = v;
+    a0 = fma(u0[i], v, a0);
+    a1 = fma(u1[i], v, a1);
+  }
+  a0 = block_sum(a0, sh);
+  a1 = block_sum(a1, sh);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = a0;
+    part[2 * blockIdx.x + 1] = a1;
+  }
+}
+
+// Woodbury correction z += c0 z0 + c1 z1, c = -W (v0.z, v1.z), then partial sums of
+// (s_0a.z, f_0a.z) into part_out.
+__global__ void __launch_bounds__(kVB) arn_woodbury_kernel(const ArnoldiState* __restrict__ st,
+                                                           const double* __restrict__ part_in, double w00, double w01,
+                                                           double w10, double w11, const double* __restrict__ z0,
+                                                           const double* __restrict__ z1, const double* __restrict__ s_0a,
+                                                           const double* __restrict__ f_0a, uint64_t n,
+                                                           double* __restrict__ z, double* __restrict__ part_out) {
+  __shared__ double sh[33];
+  if (st->done) return;
+  const double t0 = sum_partials(part_in, 2, 0, sh), t1 = sum_partials(part_in, 2, 1, sh);
+  const double c0 = -(w00 * t0 + w01 * t1), c1 = -(w10 * t0 + w11 * t1);
+  double a0 = 0.0, a1 = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)kVB + threadIdx.x; i < n; i += (uint64_t)kVBlocks * kVB) {
+    const double v = z[i] + c0 * z0[i] + c1 * z1[i];
+    z[i] = v;
+    a0 = fma(s_0a[i], v, a0);
+    a1 = fma(f_0a[i], v, a1);
+  }
+  a0 = block_sum(a0, sh);
+  a1 = block_sum(a1, sh);
+  if (threadIdx.x == 0) {
+    part_out[2 * blockIdx.x] = a0;
+    part_out[2 * blockIdx.x + 1] = a1;
+  }
+}
+
+__global__ void __launch_bounds__(kVB) arn_zero_kernel(const ArnoldiState* __restrict__ st, uint64_t n,
+                                                       double* __restrict__ w) {
+  if (st->done) return;
+  for (uint64_t i = blockIdx.x * (uint64_t)kVB + threadIdx.x; i < n; i += (uint64_t)kVBlocks * kVB) w[i] = 0.0;
+}
+
+// Projection of the product (apply_projection_correction): w += -sx f_a0 + (2 e0 sx - fx) s_a0
+// with (sx, fx) = (s_0a.z, f_0a.z); then partial sums of q_j.w for j <= k (first Gram-Schmidt
+// pass) into part[b * ld + j].
+__global__ void __launch_bounds__(kVB) arn_project_kernel(const ArnoldiState* __restrict__ st,
+                                                          const double* __restrict__ part_sf, double e0,
+                                                          const double* __restrict__ f_a0, const double* __restrict__ s_a0,
+                                                          const double* __restrict__ Q, uint64_t n, int ld,
+                                                          double* __restrict__ w, double* __restrict__ part) {
+  __shared__ double sh[33];
+  if (st->done) return;
+  const double sx = sum_partials(part_sf, 2, 0, sh), fx = sum_partials(part_sf, 2, 1, sh);
+  const double cf = -sx, cs = 2.0 * e0 * sx - fx;
+  for (uint64_t i = blockIdx.x * (uint64_t)kVB + threadIdx.x; i < n; i += (uint64_t)kVBlocks * kVB)
+    w[i] = w[i] + cf * f_a0[i] + cs * s_a0[i];
+  __syncthreads();
+  const int k = st->k;
+  for (int j = 0; j <= k; ++j) {
+    const double* q = Q + (uint64_t)j * n;
+    double a = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)kVB + threadIdx.x; i < n; i += (uint64_t)kVBlocks * kVB) a = fma(q[i], w[i], a);
+    a = block_sum(a, sh);
+    if (threadIdx.x == 0) part[(size_t)blockIdx.x * ld + j] = a;
+  }
+}
+
+// Gram-Schmidt coefficients c_j = sum of the partials (j <= k); hcol = c (first pass) or
+// hcol += c (second pass).  One block.
+__global__ void __launch_bounds__(kVB) arn_coef_kernel(const ArnoldiState* __restrict__ st, const double* __restrict__ part,
+                                                       int ld, int accumulate, double* __restrict__ coef,
+                                                       double* __restrict__ hcol) {
+  if (st->done) return;
+  const int k = st->k, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int j = wid; j <= k; j += kVB / 32) {
+    double v = 0.0;
+    for (int b = lane; b < kVBlocks; b += 32) v += part[(size_t)b * ld + j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    if (lane == 0) {
+      coef[j] = v;
+      hcol[j] = accumulate ? hcol[j] + v : v;
+    }
+  }
+}
+
+// w -= sum_{j <= k} q_j c_j; then the partial sums of the second pass (q_j.w into part) or,
+// after it, of |w|^2 (part[b * ld]).
+__global__ void __launch_bounds__(kVB) arn_orth_kernel(const ArnoldiState* __restrict__ st, const double* __restrict__ Q,
+                                                       const double* __restrict__ coef, uint64_t n, int ld, int norm,
+                                                       double* __restrict__ w, double* __restrict__ part) {
+  __shared__ double sh[33];
+  if (st->done) return;
+  const int k = st->k;
+  double a2 = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)kVB + threadIdx.x; i < n; i += (uint64_t)kVBlocks * kVB) {
+    double v = w[i];
+    for (int j = 0; j <= k; ++j) v -= Q[(uint64_t)j * n + i] * coef[j];
+    w[i] = v;
+    a2 = fma(v, v, a2);
+  }
+  if (norm) {
+    a2 = block_sum(a2, sh);
+    if (threadIdx.x == 0) part[(size_t)blockIdx.x * ld] = a2;
+    return;
+  }
+  __syncthreads();
+  for (int j = 0; j <= k; ++j) {
+    const double* q = Q + (uint64_t)j * n;
+    double a = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)kVB + threadIdx.x; i < n; i += (uint64_t)kVBlocks * kVB) a = fma(q[i], w[i], a);
+    a = block_sum(a, sh);
+    if (threadIdx.x == 0) part[(size_t)blockIdx.x * ld + j] = a;
+  }
+}
+
+// h_{k+1,k} = |w|, column k of the Hessenberg matrix, the earlier rotations and the new one,
+// the rotated right-hand side and the stopping rule (gmres.rs:197-266).  One block.
+__global__ void __launch_bounds__(kVB) arn_givens_kernel(ArnoldiState* __restrict__ st, const double* __restrict__ part,
+                                                         int ld, const double* __restrict__ hcol, int kmax,
+                                                         double* __restrict__ H, double* __restrict__ cs,
+                                                         double* __restrict__ sn, double* __restrict__ g) {
+  __shared__ double sh[33];
+  if (st->done) return;
+  double v = 0.0;
+  for (int b = threadIdx.x; b < kVBlocks; b += kVB) v += part[(size_t)b * ld];
+  v = block_sum(v, sh);
+  if (threadIdx.x != 0) return;
+  const int k = st->k;
+  const double hnext = sqrt(v);
+  auto Hh = [&](int i, int j) -> double& { return H[(size_t)i * kmax + j]; };
+  for (int j = 0; j <= k; ++j) Hh(j, k) = hcol[j];
+  Hh(k + 1, k) = hnext;
+  for (int j = 0; j < k; ++j) {
+    const double t = cs[j] * Hh(j, k) + sn[j] * Hh(j + 1, k);
+    Hh(j + 1, k) = -sn[j] * Hh(j, k) + cs[j] * Hh(j + 1, k);
+    Hh(j, k) = t;
+  }
+  const double a = Hh(k, k), bb = Hh(k + 1, k);
+  const double den = hypot(a, bb);
+  if (den > kArnoldiSmall) {
+    cs[k] = a / den;
+    sn[k] = bb / den;
+  } else {
+    cs[k] = 1.0;
+    sn[k] = 0.0;
+  }
+  Hh(k, k) = cs[k] * a + sn[k] * bb;
+  Hh(k + 1, k) = 0.0;
+  g[k + 1] = -sn[k] * g[k];
+  g[k] = cs[k] * g[k];
+  st->kfinal = k + 1;
+  st->col = k + 1;
+  st->inv = hnext > kArnoldiSmall ? 1.0 / hnext : 0.0;
+  st->k = k + 1;
+  if (fabs(g[k + 1]) <= st->tol || hnext <= kArnoldiSmall || k + 1 >= st->inner) st->done = 1;
+}
+
+// q_{k+1} = w / h_{k+1,k} (skipped once the cycle is done: no later step reads it).
+__global__ void __launch_bounds__(kVB) arn_next_kernel(const ArnoldiState* __restrict__ st, const double* __restrict__ w,
+                                                       uint64_t n, double* __restrict__ Q) {
+  if (st->done) return;
+  double* q = Q + (uint64_t)st->col * n;
+  const double inv = st->inv;
+  for (uint64_t i = blockIdx.x * (uint64_t)kVB + threadIdx.x; i < n; i += (uint64_t)kVBlocks * kVB) q[i] = w[i] * inv;
+}
+
+__global__ void arn_init_kernel(ArnoldiState* __restrict__ st, int inner, double tol, double beta, int kmax,
+                                double* __restrict__ H, double* __restrict__ g) {
+  for (int i = threadIdx.x; i < (kmax + 1) * kmax; i += blockDim.x) H[i] = 0.0;
+  for (int i = threadIdx.x; i <= kmax; i += blockDim.x) g[i] = i == 0 ? beta : 0.0;
+  if (threadIdx.x == 0) {
+    st->k = 0;
+    st->inner = inner;
+    st->done = inner <= 0;
+    st->kfinal = 0;
+    st->col = 0;
+    st->tol = tol;
+    st->inv = 0.0;
+  }
+}
+
 }  // namespace
 
 struct nw_pt2 {
@@ -261,7 +517,7 @@ nw_status symv(nw_pt2* p, const double* x, double* y) {
   NW_CUDA(p->ctx, cudaMemsetAsync(y, 0, sizeof(double) * n, nullptr));
   if (p->m) {
     const uint64_t ntiles = nb * (nb + 1) / 2;
-    packed_symv_kernel<<<(unsigned)ntiles, kTile>>>(p->m, n, nb, x, y);
+    packed_symv_kernel<<<(unsigned)ntiles, kTile>>>(p->m, n, nb, x, y, nullptr);
     NW_CUDA(p->ctx, cudaGetLastError());
     return NW_OK;
   }
@@ -543,68 +799,114 @@ nw_status nw_pt2_solve(nw_pt2* p, const nw_pt2_projection* proj, const double* r
   double res = beta / rms;
   int total = 0;
   bool converged = res <= opts->res_tol;
-  std::vector<double> H((size_t)(kmax + 1) * kmax), cs(kmax), sn(kmax), g(kmax + 1), hcol(kmax + 1), c(kmax + 1);
+  std::vector<double> H((size_t)(kmax + 1) * kmax), g(kmax + 1);
   auto Hh = [&](int i, int j) -> double& { return H[(size_t)i * kmax + j]; };
+
+  // device-side Arnoldi scratch: the cycle state, per-block partial sums, Gram-Schmidt
+  // coefficients, the Hessenberg matrix, rotations and g
+  const int ld = kmax + 1;
+  const size_t nscr = (size_t)kVBlocks * ld + 4 * (size_t)kVBlocks + 2 * (size_t)ld + (size_t)(kmax + 1) * kmax +
+                      2 * (size_t)kmax + (size_t)ld;
+  struct ArnoldiRes {
+    void* mem = nullptr;
+    cudaStream_t q = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~ArnoldiRes() {
+      if (exec) cudaGraphExecDestroy(exec);
+      if (q) cudaStreamDestroy(q);
+      if (mem) cudaFree(mem);
+    }
+  } ar;
+  if (cudaMalloc(&ar.mem, sizeof(ArnoldiState) + sizeof(double) * nscr) != cudaSuccess)
+    return pfail(p, NW_ERR_ALLOC, "GMRES Arnoldi scratch");
+  // a blocking stream: ordered with the legacy-stream work (products, cuBLAS) around it
+  NW_CUDA(ctx, cudaStreamCreate(&ar.q));
+  ArnoldiState* dst = static_cast<ArnoldiState*>(ar.mem);
+  double* part = reinterpret_cast<double*>(static_cast<char*>(ar.mem) + sizeof(ArnoldiState));
+  double* part_a = part + (size_t)kVBlocks * ld;      // 2 per block
+  double* part_b = part_a + 2 * (size_t)kVBlocks;     // 2 per block
+  double* coef = part_b + 2 * (size_t)kVBlocks;
+  double* hcol = coef + ld;
+  double* dH = hcol + ld;
+  double* dcs = dH + (size_t)(kmax + 1) * kmax;
+  double* dsn = dcs + kmax;
+  double* dg = dsn + kmax;
+  const int* done_flag = reinterpret_cast<const int*>(reinterpret_cast<const char*>(dst) + offsetof(ArnoldiState, done));
+  const uint64_t nb = (n + kTile - 1) / kTile;
+  // One Arnoldi step: z = P^-1 q_k, w = M^Omega z, two classical Gram-Schmidt passes, |w|, the
+  // Givens update and q_{k+1}; every kernel is a no-op once the cycle is done.
+  auto enqueue_step = [&](cudaStream_t q) -> nw_status {
+    arn_precond_kernel<<<kVBlocks, kVB, 0, q>>>(dst, Q, dinv, s_0a, f_0a, n, z, P.active ? part_a : part_b);
+    if (P.active)
+      arn_woodbury_kernel<<<kVBlocks, kVB, 0, q>>>(dst, part_a, P.w00, P.w01, P.w10, P.w11, z0, z1, s_0a, f_0a, n, z,
+                                                   part_b);
+    if (p->m) {
+      arn_zero_kernel<<<kVBlocks, kVB, 0, q>>>(dst, n, w);
+      packed_symv_kernel<<<(unsigned)(nb * (nb + 1) / 2), kTile, 0, q>>>(p->m, n, nb, z, w, done_flag);
+      NW_CUDA(ctx, cudaGetLastError());
+    } else {
+      // matrix-free: the (F, S) pair pipeline on the legacy stream (the host checks `done`
+      // before every step, so this runs only inside a live cycle)
+      nw_status st = symv(p, z, w);
+      if (st != NW_OK) return st;
+    }
+    arn_project_kernel<<<kVBlocks, kVB, 0, q>>>(dst, part_b, pr.e0, f_a0, s_a0, Q, n, ld, w, part);
+    arn_coef_kernel<<<1, kVB, 0, q>>>(dst, part, ld, 0, coef, hcol);
+    arn_orth_kernel<<<kVBlocks, kVB, 0, q>>>(dst, Q, coef, n, ld, 0, w, part);
+    arn_coef_kernel<<<1, kVB, 0, q>>>(dst, part, ld, 1, coef, hcol);
+    arn_orth_kernel<<<kVBlocks, kVB, 0, q>>>(dst, Q, coef, n, ld, 1, w, part);
+    arn_givens_kernel<<<1, kVB, 0, q>>>(dst, part, ld, hcol, kmax, dH, dcs, dsn, dg);
+    arn_next_kernel<<<kVBlocks, kVB, 0, q>>>(dst, w, n, Q);
+    NW_CUDA(ctx, cudaGetLastError());
+    return NW_OK;
+  };
+  if (p->m) {
+    // the packed path's step is one CUDA graph, captured once per solve and replayed per step
+    cudaGraph_t graph = nullptr;
+    NW_CUDA(ctx, cudaStreamBeginCapture(ar.q, cudaStreamCaptureModeThreadLocal));
+    const nw_status cst = enqueue_step(ar.q);
+    const cudaError_t ce = cudaStreamEndCapture(ar.q, &graph);
+    if (cst != NW_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return cst;
+    }
+    NW_CUDA(ctx, ce);
+    const cudaError_t ie = cudaGraphInstantiate(&ar.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    NW_CUDA(ctx, ie);
+  }
   while (!converged && total < opts->max_iter) {
     PT_BLAS(p, cublasDnrm2(h, (int)n, r, 1, &beta));
     if (beta <= kSmall) {
       res = beta / rms;
       break;
     }
-    // the Krylov dimension cannot exceed n (and r holds the k + 1 coefficients below)
+    // the Krylov dimension cannot exceed n
     const int inner = (int)std::min<uint64_t>(std::min(kmax, opts->max_iter - total), n);
-    std::fill(H.begin(), H.end(), 0.0);
-    std::fill(g.begin(), g.end(), 0.0);
-    g[0] = beta;
     const double inv = 1.0 / beta;
     NW_CUDA(ctx, cudaMemcpy(Q, r, vb, cudaMemcpyDeviceToDevice));
     PT_BLAS(p, cublasDscal(h, (int)n, &inv, Q, 1));
-    int kfinal = 0;
-    for (int k = 0; k < inner; ++k) {
-      const double* qk = Q + (uint64_t)k * n;
-      nw_status st = apply_precond(p, P, qk, z);
-      if (st == NW_OK) st = apply_omega(p, pr, z, w);
-      if (st != NW_OK) return st;
-      // two classical Gram-Schmidt passes against q_0..q_k; r is free during the cycle and
-      // holds the k + 1 <= n coefficients
-      std::fill(hcol.begin(), hcol.end(), 0.0);
-      for (int pass = 0; pass < 2; ++pass) {
-        PT_BLAS(p, cublasDgemv(h, CUBLAS_OP_T, (int)n, k + 1, &one, Q, (int)n, w, 1, &zero, r, 1));
-        PT_BLAS(p, cublasDgemv(h, CUBLAS_OP_N, (int)n, k + 1, &mone, Q, (int)n, r, 1, &one, w, 1));
-        NW_CUDA(ctx, cudaMemcpy(c.data(), r, sizeof(double) * (k + 1), cudaMemcpyDeviceToHost));
-        for (int j = 0; j <= k; ++j) hcol[j] += c[j];
+    arn_init_kernel<<<1, kVB, 0, ar.q>>>(dst, inner, opts->res_tol * rms, beta, kmax, dH, dg);
+    NW_CUDA(ctx, cudaGetLastError());
+    if (ar.exec) {
+      // every step of the cycle queued at once; the steps after the stopping point are no-ops
+      for (int k = 0; k < inner; ++k) NW_CUDA(ctx, cudaGraphLaunch(ar.exec, ar.q));
+    } else {
+      for (int k = 0; k < inner; ++k) {
+        nw_status st = enqueue_step(ar.q);
+        if (st != NW_OK) return st;
+        int done = 0;
+        NW_CUDA(ctx, cudaMemcpyAsync(&done, done_flag, sizeof(int), cudaMemcpyDeviceToHost, ar.q));
+        NW_CUDA(ctx, cudaStreamSynchronize(ar.q));
+        if (done) break;
       }
-      double hnext = 0.0;
-      PT_BLAS(p, cublasDnrm2(h, (int)n, w, 1, &hnext));
-      for (int j = 0; j <= k; ++j) Hh(j, k) = hcol[j];
-      Hh(k + 1, k) = hnext;
-      if (hnext > kSmall) {
-        const double s = 1.0 / hnext;
-        NW_CUDA(ctx, cudaMemcpy(Q + (uint64_t)(k + 1) * n, w, vb, cudaMemcpyDeviceToDevice));
-        PT_BLAS(p, cublasDscal(h, (int)n, &s, Q + (uint64_t)(k + 1) * n, 1));
-      }
-      // previous rotations, then the new one (gmres.rs:197-266)
-      for (int j = 0; j < k; ++j) {
-        const double t = cs[j] * Hh(j, k) + sn[j] * Hh(j + 1, k);
-        Hh(j + 1, k) = -sn[j] * Hh(j, k) + cs[j] * Hh(j + 1, k);
-        Hh(j, k) = t;
-      }
-      const double a = Hh(k, k), bb = Hh(k + 1, k);
-      const double den = std::hypot(a, bb);
-      if (den > kSmall) {
-        cs[k] = a / den;
-        sn[k] = bb / den;
-      } else {
-        cs[k] = 1.0;
-        sn[k] = 0.0;
-      }
-      Hh(k, k) = cs[k] * a + sn[k] * bb;
-      Hh(k + 1, k) = 0.0;
-      g[k + 1] = -sn[k] * g[k];
-      g[k] = cs[k] * g[k];
-      kfinal = k + 1;
-      if (std::fabs(g[k + 1]) / rms <= opts->res_tol || hnext <= kSmall) break;
     }
+    NW_CUDA(ctx, cudaStreamSynchronize(ar.q));
+    ArnoldiState hst;
+    NW_CUDA(ctx, cudaMemcpy(&hst, dst, sizeof(hst), cudaMemcpyDeviceToHost));
+    const int kfinal = hst.kfinal;
+    NW_CUDA(ctx, cudaMemcpy(H.data(), dH, sizeof(double) * H.size(), cudaMemcpyDeviceToHost));
+    NW_CUDA(ctx, cudaMemcpy(g.data(), dg, sizeof(double) * g.size(), cudaMemcpyDeviceToHost));
     // back substitution, then x += P^-1 Q y
     std::vector<double> yv(kfinal, 0.0);
     for (int ii = kfinal - 1; ii >= 0; --ii) {

@@ -749,6 +749,8 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
   *out = nullptr;
   if (!ctx || !opts || !c0 || (nref_idx && !ref_idx)) return NW_ERR_INVALID;
   if (!ctx->built) return nw::fail(ctx, NW_ERR_STATE, "intermediates not built");
+  if (ctx->partial)
+    return nw::fail(ctx, NW_ERR_STATE, "the intermediates hold one block of a blocked evaluation (rebuild them)");
   if (!ctx->d_dets || ctx->ndet < 2) return nw::fail(ctx, NW_ERR_STATE, "QMC needs a resident basis of >= 2 determinants");
   if (!(opts->dt > 0.0) || opts->ncycles < 1 || opts->propagator < 0 || opts->propagator > 4 ||
       !(opts->initial_population > 0.0) || !(opts->sampling_cutoff >= 0.0) || !(opts->spawn_cutoff >= 0.0) ||

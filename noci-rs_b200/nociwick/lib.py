@@ -26,7 +26,7 @@ _lib = None
 
 NW_OK = 0
 _STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "allocation failed", 4: "unsupported input",
-           5: "call out of order", 6: "no CUDA device"}
+           5: "call out of order", 6: "no CUDA device", 7: "cache file input/output failed"}
 CONVENTIONS = {"reference": 0, "exact": 1}
 NOALLOC_MAX_PAIRS = 1 << 20
 TRANSFORMS = {"fp64": 0, "chol_fp64": 1, "chol_int8": 2, "chol_bf16x6": 3}
@@ -124,7 +124,8 @@ class NwInfo(ctypes.Structure):
                 ("pad", ctypes.c_int32), ("slab_bytes", ctypes.c_uint64), ("ndet", ctypes.c_uint64)]
 
 
-EXPORTED = ("nw_ctx_create", "nw_ctx_create_cholesky", "nw_build_intermediates", "nw_pair_zero_counts",
+EXPORTED = ("nw_ctx_create", "nw_ctx_create_cholesky", "nw_build_intermediates", "nw_save_intermediates",
+            "nw_load_intermediates", "nw_eval_hs_pairs_blocked", "nw_pair_zero_counts",
             "nw_set_basis", "nw_eval_hs_pairs_device", "nw_eval_hs_pairs", "nw_eval_hs_pairs_noalloc",
             "nw_eval_hs_batched", "nw_eval_hs_batched_device", "nw_eval_s_pairs_device", "nw_eval_s_pairs", "nw_update_fock", "nw_eval_fs_pairs_device", "nw_eval_fs_pairs",
             "nw_build_hs_matrix", "nw_build_fs_matrix", "nw_general_evp",
@@ -134,7 +135,7 @@ EXPORTED = ("nw_ctx_create", "nw_ctx_create_cholesky", "nw_build_intermediates",
             "nw_qmc_proposal_probs", "nw_pt2_create", "nw_pt2_create_matrix_free", "nw_pt2_apply_m", "nw_pt2_last_apply_ms", "nw_pt2_solve",
             "nw_pt2_destroy", "nw_screen_create", "nw_screen_train", "nw_screen_predict", "nw_screen_destroy",
             "nw_autotune", "nw_dgemm", "nw_set_transform", "nw_transform_product", "nw_sync",
-            "nw_set_timing", "nw_last_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
+            "nw_set_timing", "nw_last_timings", "nw_last_class_timings", "nw_ctx_info", "nw_ctx_destroy", "nw_status_string",
             "nw_last_error")
 
 
@@ -154,6 +155,10 @@ def load(path: Optional[str] = None):
     L.nw_ctx_create_cholesky.argtypes = [ctypes.POINTER(NwSystemCd), ctypes.POINTER(NwRefs), ctypes.POINTER(NwOpts),
                                          ctypes.POINTER(vp)]
     L.nw_build_intermediates.argtypes = [vp]
+    L.nw_save_intermediates.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p]
+    L.nw_load_intermediates.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p]
+    L.nw_eval_hs_pairs_blocked.argtypes = [vp, vp, ctypes.c_uint64, vp, ctypes.c_uint64,
+                                           ctypes.POINTER(ctypes.c_uint32), vp]
     L.nw_eval_hs_batched.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_eval_hs_batched_device.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_eval_s_pairs.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
@@ -207,6 +212,7 @@ def load(path: Optional[str] = None):
     L.nw_transform_product.argtypes = [ctypes.c_int32, vp, vp, ctypes.c_int32, ctypes.c_int32, vp, vp]
     L.nw_set_timing.argtypes = [vp, ctypes.c_int]
     L.nw_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    L.nw_last_class_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     L.nw_ctx_info.argtypes = [vp, ctypes.POINTER(NwInfo)]
     L.nw_ctx_destroy.argtypes = [vp]
     L.nw_status_string.argtypes = [ctypes.c_int]
@@ -295,6 +301,18 @@ class WicksShared:
         self._check(self._lib.nw_build_intermediates(self._ctx), "nw_build_intermediates")
         return self
 
+    def save(self, slab_path, meta_path):
+        """Write the built intermediates to a slab file and a metadata file (nw_save_intermediates)."""
+        self._check(self._lib.nw_save_intermediates(self._ctx, str(slab_path).encode(), str(meta_path).encode()),
+                    "nw_save_intermediates")
+        return self
+
+    def load(self, slab_path, meta_path):
+        """Restore intermediates saved for this system instead of building them (nw_load_intermediates)."""
+        self._check(self._lib.nw_load_intermediates(self._ctx, str(slab_path).encode(), str(meta_path).encode()),
+                    "nw_load_intermediates")
+        return self
+
     def set_transform(self, mode: str):
         """Four-index transform of the next build: "fp64" (quarter transforms of the full
         tensor), or on a Cholesky context "chol_fp64", "chol_int8" (tcgen05 Ozaki slices,
@@ -357,6 +375,16 @@ class WicksShared:
         self._check(self._lib.nw_eval_s_pairs(self._ctx, pairs.ctypes.data, pairs.shape[0], out.ctypes.data,
                                               ctypes.c_void_p(stream)), "nw_eval_s_pairs")
         return out
+
+    def eval_pairs_blocked(self, pairs_ptr: int, npairs: int, out_ptr: int, slab_budget: int = 0,
+                           stream: int = 0) -> int:
+        """(H, S) of device pairs in blocks of reference pairs whose intermediates fit
+        slab_budget bytes (nw_eval_hs_pairs_blocked); returns the number of blocks."""
+        nb = ctypes.c_uint32(0)
+        self._check(self._lib.nw_eval_hs_pairs_blocked(self._ctx, ctypes.c_void_p(pairs_ptr), npairs,
+                                                       ctypes.c_void_p(out_ptr), int(slab_budget), ctypes.byref(nb),
+                                                       ctypes.c_void_p(stream)), "nw_eval_hs_pairs_blocked")
+        return int(nb.value)
 
     def eval_pairs_device(self, pairs_ptr: int, npairs: int, out_ptr: int, stream: int = 0):
         self._check(self._lib.nw_eval_hs_pairs_device(self._ctx, ctypes.c_void_p(pairs_ptr), npairs,
@@ -444,8 +472,17 @@ class WicksShared:
         (nw_pt2_create) or applied matrix-free (nw_pt2_create_matrix_free)."""
         return Pt2(self, candidates, e0, matrix_free=matrix_free)
 
-    def set_timing(self, enable: bool = True):
-        self._check(self._lib.nw_set_timing(self._ctx, 1 if enable else 0), "nw_set_timing")
+    def set_timing(self, enable: bool = True, serial_classes: bool = False):
+        """Phase timing of the following evaluations; serial_classes runs the class evaluators
+        one after another (a profiling mode, last_class_timings)."""
+        mode = (2 if serial_classes else 1) if enable else 0
+        self._check(self._lib.nw_set_timing(self._ctx, mode), "nw_set_timing")
+
+    def last_class_timings(self) -> dict:
+        """Device ms of each class evaluator of the last serially timed evaluation."""
+        ms = (ctypes.c_float * 5)()
+        self._check(self._lib.nw_last_class_timings(self._ctx, ms), "nw_last_class_timings")
+        return dict(zip(("light", "medium", "heavy", "rt", "gen"), [float(v) for v in ms]))
 
     def last_timings(self) -> dict:
         """Device ms of the phases of the last evaluation (CUDA events on its stream)."""

@@ -142,6 +142,33 @@ def test_autotune_keeps_every_result_bit():
     assert np.array_equal(before, after)
 
 
+def test_serial_class_timing_keeps_results():
+    """The serialised per-class timing mode (nw_set_timing(ctx, 2)) runs the same class kernels
+    one after another instead of on forked streams: results are bit-identical, and every class
+    present in the batch (m = 0 classes and the m > 0 generic one) reports a positive time."""
+    import torch
+    system = sy.make_system(12, 3, 3, 3, 24, seed=5, k_scale=0.3, zero_pairs=[(0, 1, 1, 0)], enuc=0.2)
+    basis = sy.sd_basis(12, 3, 3, 3, orders=(1, 2, 3, 4))
+    pairs = sy.sample_pairs(basis, 200000, seed=9, distinct_parents=False).astype(np.uint32)
+    with _engine(system) as w:
+        w.set_basis(basis)
+        stream = torch.cuda.current_stream().cuda_stream
+        dp = torch.from_numpy(pairs.view(np.int32)).cuda()
+        out = torch.empty((pairs.shape[0], 2), dtype=torch.float64, device="cuda")
+        w.eval_pairs_device(dp.data_ptr(), pairs.shape[0], out.data_ptr(), stream)
+        before = out.cpu().numpy()
+        w.set_timing(True, serial_classes=True)
+        out.fill_(np.nan)
+        w.eval_pairs_device(dp.data_ptr(), pairs.shape[0], out.data_ptr(), stream)
+        cls = w.last_class_timings()
+        phases = w.last_timings()
+        w.set_timing(False)
+        after = out.cpu().numpy()
+    assert np.array_equal(before, after)
+    assert cls["light"] > 0 and cls["gen"] > 0 and phases["eval_m0"] > 0
+    assert all(v >= 0 for v in cls.values())
+
+
 def test_pinned_host_entry_pipeline():
     """Page-locked host buffers take the chunked copy-in / evaluate / copy-out pipeline of
     nw_eval_hs_pairs; its results equal the device entry point's bit for bit, and an
