@@ -496,7 +496,8 @@ def snoci_leg(args, rank, world, local_rank, dist):
         # the same two iterations scored exhaustively: iteration 1's candidate M (3.7 TB packed)
         # is applied matrix-free, every GMRES product evaluating its 4.6e11 pairs again
         t0 = time.perf_counter()
-        res_x = sn.snoci(w, system, it_opts, screener=None)
+        res_x = sn.snoci(w, system, it_opts, screener=None,
+                         log=lambda msg: print(f"[snoci exhaustive] {msg}", file=sys.stderr, flush=True))
         exhaustive_loop = {"seconds": time.perf_counter() - t0, "energy": res_x.energy, "ept2": res_x.ept2,
                            "energy_plus_ept2": res_x.energy + res_x.ept2,
                            "learned_energy_plus_ept2": res.energy + res.ept2,

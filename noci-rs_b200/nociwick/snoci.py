@@ -350,10 +350,12 @@ def pt2_scores(wicks, m: int, cand: np.ndarray, c: np.ndarray, ecurrent: float, 
     return np.abs(amp * v_omega), ept2, e0, info
 
 
-def snoci(wicks, system, opts: SnociOptions, screener=None) -> SnociResult:
+def snoci(wicks, system, opts: SnociOptions, screener=None, log=None) -> SnociResult:
     """Iterate snoci_step (src/snoci/step.rs:178-550) from the reference space.  ``wicks`` is a
     built WicksShared of the system's references; its resident basis is replaced each
-    iteration by the selected space followed by the candidate pool."""
+    iteration by the selected space followed by the candidate pool.  ``log``, if given, is
+    called with a short progress message at each stage."""
+    say = log if log is not None else (lambda msg: None)
     nmo = system.nmo
     sel, sel_labels = reference_states(system.nref, system.nocc_a, system.nocc_b)
     pool: Optional[CandidatePool] = None
@@ -380,7 +382,10 @@ def snoci(wicks, system, opts: SnociOptions, screener=None) -> SnociResult:
         else:
             keep = np.arange(npool)
         cand = cand_all[keep]
+        say(f"iteration {it}: selected {m}, pool {npool}, scoring {cand.shape[0]}, E_current {ecurrent:.10f}, "
+            f"{time.perf_counter() - t0:.1f} s")
         kept_scores, ept2, e0, info = pt2_scores(wicks, m, cand, c, ecurrent, opts)
+        say(f"iteration {it}: E_PT2 {ept2:.10f}, GMRES {info}, {time.perf_counter() - t0:.1f} s")
         scores = np.zeros(npool)
         scores[keep] = kept_scores
         if screener is not None:
