@@ -76,7 +76,7 @@ def parse():
     ap.add_argument("--no-snoci", action="store_true", help="skip the selected-NOCI screening leg")
     ap.add_argument("--qmc-equil", type=int, default=40, help="QMC equilibration report blocks")
     ap.add_argument("--qmc-train-epochs", type=int, default=2, help="epochs of proposal training")
-    ap.add_argument("--qmc-seeds", type=int, default=3,
+    ap.add_argument("--qmc-seeds", type=int, default=5,
                     help="independent runs per generator in the uniform vs learned comparison (0: skip)")
     ap.add_argument("--qmc-max-seconds", type=float, default=30.0,
                     help="device-time cap of each run of the generator comparison")
@@ -567,7 +567,7 @@ def blocking_error(x):
     return best, bool(plateau)
 
 
-def run_to_target(q, target, chunk_reports=100, min_reports=200, max_seconds=30.0):
+def run_to_target(q, target, chunk_reports=100, min_reports=1000, max_seconds=30.0):
     """Run report blocks (10 steps each) until the blocking error of the projected energy over
     the measured blocks is at most `target` at a plateau, or the device time reaches
     max_seconds.  Returns the measured statistics; time is measured, not extrapolated."""
@@ -598,8 +598,10 @@ def compare_generators(w, c0, refs, e_ref, walkers, seeds, rank, target=1e-4, ep
     and then (learned arm) harvests attempts over `harvest_reports` blocks (2000 steps) with
     the uniform generator, trains the proposal on the GPU and switches to the learned mixture
     (uniform weight 0.1); both arms then run 100-block chunks until the blocking error of the
-    measured blocks is at most `target` at a plateau (at least 200 blocks), or until
-    `max_seconds` of device time.  The learned arm's time includes harvest and training."""
+    measured blocks is at most `target` at a plateau (at least 1000 blocks, so six blocking
+    levels), or until `max_seconds` of device time.  The learned arm's time includes harvest
+    and training.  The summary also checks the error bars against the runs themselves: the
+    spread of the seeds' projected energies against their mean error bar."""
     import nociwick
     arms = {"uniform": [], "learned": []}
     for k in range(seeds):
@@ -630,9 +632,14 @@ def compare_generators(w, c0, refs, e_ref, walkers, seeds, rank, target=1e-4, ep
     summary = {}
     for arm, runs in arms.items():
         t = np.array([r["seconds_to_0.1mEh"] for r in runs])
+        ep = np.array([r["eproj"] for r in runs])
+        eb = np.array([r["error_bar"] for r in runs])
         summary[arm] = {"mean_s": float(t.mean()), "min_s": float(t.min()), "max_s": float(t.max()),
                         "reached": int(sum(r["reached"] for r in runs)), "runs": len(runs),
-                        "walkers": float(np.mean([r["walkers_mean"] for r in runs]))}
+                        "walkers": float(np.mean([r["walkers_mean"] for r in runs])),
+                        "eproj_mean": float(ep.mean()),
+                        "eproj_seed_std": float(ep.std(ddof=1)) if len(runs) > 1 else None,
+                        "error_bar_mean": float(eb.mean())}
     summary["speedup_mean"] = summary["uniform"]["mean_s"] / max(summary["learned"]["mean_s"], 1e-9)
     return {"target_eh": target, "seeds": seeds, "runs": arms, "summary": summary,
             "note": "measured wall time (host clock around the graph launches, plus harvest and training for the "
@@ -895,7 +902,9 @@ def mixed_leg(args, system, basis, pairs, hs_ref, fp64_build_s, fp64_eval_ms, lo
     cond = smin[par[pairs[:, 0]] * len(system.refs) + par[pairs[:, 1]]]
     out = {"first_build": {"build_seconds": fp64_build_s, "eval_ms": fp64_eval_ms,
                            "note": "the config-3 leg's own FP64 build: the first on this process, so it includes "
-                                   "the allocation of the slab and the build buffers; fp64 below is a rebuild"}}
+                                   "the allocation of the slab and the build buffers; below, build_seconds is a "
+                                   "rebuild on the same context (slab and workspace reused), first_build_seconds "
+                                   "the first build of that context"}}
     for mode in ("fp64", "chol_fp64", "chol_int8", "chol_bf16x6"):
         if mode == "fp64":
             # four FP64 quarter transforms of the full Coulomb tensor (the default build)
@@ -906,6 +915,10 @@ def mixed_leg(args, system, basis, pairs, hs_ref, fp64_build_s, fp64_eval_ms, lo
                                        device=local_rank, chol=system.chol)
             eng.set_transform(mode)
         torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.build()
+        first_s = time.perf_counter() - t0
+        # a rebuild reuses the slab and the workspace: the build's own device work
         t0 = time.perf_counter()
         eng.build()
         build_s = time.perf_counter() - t0
@@ -929,7 +942,7 @@ def mixed_leg(args, system, basis, pairs, hs_ref, fp64_build_s, fp64_eval_ms, lo
             if sel.any():
                 buckets[nm] = {"pairs": int(sel.sum()), "max_abs_err_h": float(dh[sel].max()),
                                "rms_abs_err_h": float(np.sqrt(np.mean(dh[sel] ** 2)))}
-        out[mode] = {"build_seconds": build_s, "eval_ms": ms, "value": npairs / (ms / 1e3),
+        out[mode] = {"build_seconds": build_s, "first_build_seconds": first_s, "eval_ms": ms, "value": npairs / (ms / 1e3),
                      "one_shot_value": npairs / (build_s + ms / 1e3),
                      "max_abs_dh_vs_fp64": float(dh.max()), "rms_abs_dh_vs_fp64": float(np.sqrt(np.mean(dh ** 2))),
                      "max_abs_ds_vs_fp64": float(ds.max()), "by_reference_pair_conditioning": buckets}

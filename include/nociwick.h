@@ -486,7 +486,7 @@ typedef struct nw_pt2 nw_pt2;
 NW_API nw_status nw_pt2_create(nw_ctx* ctx, const uint32_t* cand, uint64_t n, double e0, nw_pt2** out);
 /* The same operator without storing M: every product (nw_pt2_apply_m, and each GMRES step of
  * nw_pt2_solve) evaluates the n (n + 1) / 2 upper-triangle (F, S) pairs again through the pair
- * pipeline in blocks of 2^24 and accumulates M x directly, so the device holds O(n) instead of
+ * pipeline in blocks of 2^26 and accumulates M x directly, so the device holds O(n) instead of
  * the n^2 / 2 doubles of the packed matrix.  Replaces apply_candidate_m without a cached matrix
  * (src/snoci/operators.rs:424-471). */
 NW_API nw_status nw_pt2_create_matrix_free(nw_ctx* ctx, const uint32_t* cand, uint64_t n, double e0, nw_pt2** out);

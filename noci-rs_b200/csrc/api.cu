@@ -550,6 +550,7 @@ nw_status nw_ctx_destroy(nw_ctx* ctx) {
   for (double* b : {ctx->d_fbase, ctx->d_fock, ctx->d_fslab})
     if (b) cudaFree(b);
   if (ctx->d_fockp) cudaFree(ctx->d_fockp);
+  free_buf(ctx->build_work);
   free_buf(ctx->bt_dets);
   free_buf(ctx->bt_desc);
   free_buf(ctx->bt_pairs);

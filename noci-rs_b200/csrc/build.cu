@@ -466,18 +466,15 @@ nw_status build_all(nw_ctx* ctx, const std::vector<char>* subset) {
                         4 * n2 /*JcXc*/ + 64;
   // 40 arena pieces, each rounded up to 256 bytes
   const size_t work_doubles = per_ps * nps + 5 * n4 + 40 * 32 + 4096;
+  // the workspace stays with the context, so rebuilds (blocked evaluation, transform changes)
+  // do not allocate it again
   Arena ar;
   {
-    void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, work_doubles * sizeof(double) + 256 * 64);
-    if (e != cudaSuccess) return fail(ctx, NW_ERR_ALLOC, "build workspace allocation failed");
-    ar.base = static_cast<char*>(p);
-    ar.cap = work_doubles * sizeof(double) + 256 * 64;
+    nw_status st = ensure(ctx, ctx->build_work, work_doubles * sizeof(double) + 256 * 64);
+    if (st != NW_OK) return fail(ctx, NW_ERR_ALLOC, "build workspace allocation failed");
+    ar.base = static_cast<char*>(ctx->build_work.p);
+    ar.cap = ctx->build_work.bytes;
   }
-  struct Free {
-    void* p;
-    ~Free() { cudaFree(p); }
-  } free_work{ar.base};
 
   double* ctx_t = ar.take((size_t)nps * nao * omax);
   double* ctw_t = ar.take((size_t)nps * nao * omax);
@@ -718,14 +715,23 @@ nw_status build_all(nw_ctx* ctx, const std::vector<char>* subset) {
       }
     }
   }
-  if (ctx->d_slab) {
+  // a slab at least as large is reused (rebuilds, the blocks of a blocked evaluation)
+  const size_t slab_need = std::max<size_t>(slab, 32) * sizeof(double);
+  if (ctx->d_slab && ctx->slab_capacity < slab_need) {
     cudaFree(ctx->d_slab);
     ctx->d_slab = nullptr;
+    ctx->slab_capacity = 0;
   }
   {
-    cudaError_t e = cudaMalloc(&ctx->d_slab, std::max<size_t>(slab, 32) * sizeof(double));
-    if (e != cudaSuccess) return fail(ctx, NW_ERR_ALLOC, "intermediate slab allocation failed (" +
-                                                             std::to_string(slab * 8 / (1 << 20)) + " MiB)");
+    if (!ctx->d_slab) {
+      cudaError_t e = cudaMalloc(&ctx->d_slab, slab_need);
+      if (e != cudaSuccess) {
+        ctx->d_slab = nullptr;
+        return fail(ctx, NW_ERR_ALLOC, "intermediate slab allocation failed (" +
+                                           std::to_string(slab * 8 / (1 << 20)) + " MiB)");
+      }
+      ctx->slab_capacity = slab_need;
+    }
     ctx->slab_bytes = slab * sizeof(double);
   }
   double* S0 = ctx->d_slab;

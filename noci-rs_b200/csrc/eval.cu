@@ -634,7 +634,7 @@ nw_status eval_blocked(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, doub
     NW_CUDA(ctx, cudaMemGetInfo(&fr, &tot));
     const size_t reserve = 8ull << 30;
     budget = fr > reserve ? fr - reserve : 0;
-    if (ctx->d_slab) budget += ctx->slab_bytes;  // the current slab is freed by the next build
+    if (ctx->d_slab) budget += ctx->slab_capacity;  // the current slab is reused or freed
   }
   std::vector<char> none(npair, 0);
   nw_status st = build_all(ctx, &none);

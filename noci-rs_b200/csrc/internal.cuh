@@ -66,6 +66,8 @@ struct nw_ctx {
   // intermediates
   double* d_slab = nullptr;
   size_t slab_bytes = 0;
+  size_t slab_capacity = 0;        // bytes allocated at d_slab (>= slab_bytes)
+  nw::DevBuf build_work;           // workspace of the build, kept for rebuilds
   nw::FastPair* d_fast = nullptr;
   nw::GenPair* d_gen = nullptr;
   int32_t* d_order = nullptr;

@@ -661,7 +661,9 @@ nw_status nw_pt2_create_matrix_free(nw_ctx* ctx, const uint32_t* cand, uint64_t 
   p->ctx = ctx;
   p->n = n;
   p->e0 = e0;
-  constexpr uint64_t kBlock = 1ull << 24;  // pairs per evaluation block
+  // pairs per evaluation block: 2^26 (1.6 GB of pairs and (F, S)) keeps the per-block cost of
+  // the sort (counter clear and scan) small next to the evaluation
+  constexpr uint64_t kBlock = 1ull << 26;
   p->blk = std::max(std::min(kBlock, n * (n + 1) / 2), n);  // a block also holds the n diagonal pairs
   auto cleanup = [&](nw_status st) {
     if (st != NW_OK) nw_pt2_destroy(p);

@@ -315,12 +315,14 @@ nw_status load_intermediates(nw_ctx* ctx, const char* slab_path, const char* met
   if (ctx->d_slab) cudaFree(ctx->d_slab);
   ctx->d_slab = nullptr;
   ctx->slab_bytes = 0;
+  ctx->slab_capacity = 0;
   if (ctx->d_fbase) cudaFree(ctx->d_fbase);
   ctx->d_fbase = nullptr;
   if (cudaMalloc(&ctx->d_slab, std::max<size_t>(hd.slab_bytes, 256)) != cudaSuccess) {
     ctx->d_slab = nullptr;
     return fail(ctx, NW_ERR_ALLOC, "intermediate slab allocation failed");
   }
+  ctx->slab_capacity = std::max<size_t>(hd.slab_bytes, 256);
   if (cudaMalloc(&ctx->d_fbase, fbase_bytes) != cudaSuccess) {
     ctx->d_fbase = nullptr;
     return fail(ctx, NW_ERR_ALLOC, "Fock basis allocation failed");
