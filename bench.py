@@ -69,6 +69,10 @@ def parse():
     ap.add_argument("--snoci-exhaustive", action="store_true",
                     help="also run the two SNOCI iterations exhaustively (matrix-free candidate M, minutes)")
     ap.add_argument("--config3-npairs", type=int, default=100_000_000, help="pairs of the config-3 H/S leg")
+    ap.add_argument("--no-beyond-hbm", action="store_true",
+                    help="skip the blocked evaluation of a system whose intermediates exceed HBM")
+    ap.add_argument("--beyond-hbm-nref", type=int, default=24, help="references of the beyond-HBM system")
+    ap.add_argument("--beyond-hbm-npairs", type=int, default=50_000_000, help="pairs of the beyond-HBM leg")
     ap.add_argument("--qmc-reports", type=int, default=30, help="timed QMC report blocks (10 steps each)")
     ap.add_argument("--no-pt2", action="store_true", help="skip the NOCI-PT2 mat-vec / GMRES leg")
     ap.add_argument("--pt2-ncand", type=int, default=0, help="PT2 candidates (0: all 125685 of the stand-in)")
@@ -954,6 +958,50 @@ def mixed_leg(args, system, basis, pairs, hs_ref, fp64_build_s, fp64_eval_ms, lo
     return out
 
 
+def beyond_hbm_leg(args, rank, local_rank):
+    """Blocked (out-of-core) evaluation: the config-3 stress system with `--beyond-hbm-nref`
+    references (24: 576 ordered reference pairs, 0.4 GB of intermediates each at n = 64, about
+    230 GB in all, more than the device holds).  nw_eval_hs_pairs_blocked cuts the reference
+    pairs into blocks that fit the free device memory, builds each block and evaluates the
+    whole request against it.  Reported: blocks, host-clock seconds of the whole call (builds
+    included), the pair rate over that time, and the device time of one block's evaluation for
+    comparison with the resident path."""
+    import torch
+    import nociwick
+    from nociwick import synthetic as sy
+    nref, npairs, nmo = args.beyond_hbm_nref, args.beyond_hbm_npairs, 64
+    system = sy.config3_system(nmo=nmo, nref=nref)
+    basis = sy.sd_basis(nmo, 6, 6, nref)
+    pairs = sy.sample_pairs_by_rank(basis, npairs, seed=rank_seed(4, rank)).astype(np.uint32)
+    eng = nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8,
+                               device=local_rank)
+    eng.set_basis(basis)
+    dp = torch.from_numpy(pairs.view(np.int32)).to(f"cuda:{local_rank}")
+    out = torch.empty((npairs, 2), dtype=torch.float64, device=f"cuda:{local_rank}")
+    sh = torch.cuda.current_stream().cuda_stream
+    free, total = torch.cuda.mem_get_info()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    nb = eng.eval_pairs_blocked(dp.data_ptr(), npairs, out.data_ptr(), 0, sh)
+    torch.cuda.synchronize()
+    seconds = time.perf_counter() - t0
+    hs = out.cpu().numpy()
+    block_bytes = eng.info()["slab_bytes"]
+    eng.close()
+    del dp, out
+    torch.cuda.empty_cache()
+    fast_pair_bytes = (2 * (2 * 2 * nmo * nmo * 8 + nmo ** 4 * 8) + nmo ** 4 * 8)
+    return {"workload": f"synthetic stress system with {nref} references: n={nmo}, 6a+6b electrons, "
+                        f"{nref * nref} ordered reference pairs, contraction rank 0-4 uniform",
+            "npairs": npairs, "ndet": int(basis.shape[0]),
+            "intermediates_gb_estimate": nref * nref * fast_pair_bytes / 1e9,
+            "device_memory_gb": total / 1e9, "free_before_gb": free / 1e9,
+            "blocks": nb, "last_block_slab_gb": block_bytes / 1e9,
+            "seconds": seconds, "value": npairs / seconds, "unit": "pair-elements/s",
+            "finite": bool(np.isfinite(hs).all()),
+            "timing": "host clock around nw_eval_hs_pairs_blocked (every block's build and evaluation)"}
+
+
 def tail_summary(line):
     """The figures a reader of the end of the output needs, in a few hundred bytes."""
     wl = "hs_config3" if line["config"]["workload"].startswith("synthetic stress") else "hs_config2"
@@ -971,6 +1019,10 @@ def tail_summary(line):
             out["mixed_config3"] = {m: {"build_s": v["build_seconds"], "one_shot": v.get("one_shot_value"),
                                         "max_dh": v.get("max_abs_dh_vs_fp64")}
                                     for m, v in mx.items() if isinstance(v, dict)}
+    b = line.get("beyond_hbm")
+    if b:
+        out["beyond_hbm"] = {"nref": b["workload"].split(" references")[0].split()[-1], "blocks": b["blocks"],
+                             "seconds": b["seconds"], "value": b["value"]}
     q = line.get("qmc")
     if q:
         out["qmc"] = {"steps_per_s": q["value"], "walkers": q["walkers_mean"]}
@@ -1010,6 +1062,7 @@ def run_ours(args, rank, world, local_rank):
                 c3["mixed"] = mixed_leg(args, system, basis, pairs, hs_host, c3["config"]["build_seconds"],
                                         c3["roofline"]["eval_ms"], local_rank)
         del system, basis, pairs, hs_host
+    beyond = None if (args.no_beyond_hbm or world > 1) else beyond_hbm_leg(args, rank, local_rank)
     qmc = None if args.no_qmc else qmc_leg(args, rank, world, local_rank, dist)
     if rank != 0:
         return
@@ -1028,6 +1081,8 @@ def run_ours(args, rank, world, local_rank):
         line["snoci"] = snoci_out
     if c3 is not None:
         line["config3"] = dict(c3, metric=METRIC, unit=UNIT, dtype="f64")
+    if beyond is not None:
+        line["beyond_hbm"] = beyond
     if qmc is not None:
         line["qmc"] = qmc
     line["tail_summary"] = tail_summary(line)

@@ -195,11 +195,21 @@ __global__ void qmc_spawn_kernel(QmcParams q, Proposal pr, nw::EvalParams P, con
   for (uint32_t w0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); w0 < n; w0 += gridDim.x * blockDim.x) {
     const uint32_t t = w0 + lane;
     uint32_t key = nw::kSkipKey;
-    if (t < n) {
-      // owners of this chunk's first attempt and of the next chunk's bound the search
-      const uint32_t c = t >> kChunkShift;
-      const uint64_t lo = cown[c];
-      const uint64_t hi = ((uint64_t)(c + 1) << kChunkShift) < n ? cown[c + 1] : q.ndet - 1;
+    // Owner of attempt t: the largest determinant a with off[a] <= t.  The owners of this
+    // chunk's first attempt and of the next chunk's bound it (a warp's 32 attempts lie in one
+    // chunk, so the bounds are warp-uniform); when they are fewer than 32 apart the warp loads
+    // their offsets once and each lane counts those <= t, else each lane bisects.
+    const uint32_t c = w0 >> kChunkShift;
+    const uint64_t lo = cown[c];
+    const uint64_t hi = ((uint64_t)(c + 1) << kChunkShift) < n ? cown[c + 1] : q.ndet - 1;
+    uint64_t owner = lo;
+    if (hi - lo < 32) {
+      const uint32_t o = lo + lane <= hi ? off[lo + lane] : 0xFFFFFFFFu;
+      uint32_t cnt = 0;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) cnt += __shfl_sync(0xFFFFFFFFu, o, j) <= t ? 1u : 0u;
+      owner = lo + (cnt > 0 ? cnt - 1 : 0);
+    } else if (t < n) {
       uint64_t a = lo, b = hi + 1;  // off[a] <= t < off[b]
       while (b - a > 1) {
         const uint64_t mid = (a + b) >> 1;
@@ -208,7 +218,10 @@ __global__ void qmc_spawn_kernel(QmcParams q, Proposal pr, nw::EvalParams P, con
         else
           b = mid;
       }
-      const uint64_t g = a;
+      owner = a;
+    }
+    if (t < n) {
+      const uint64_t g = owner;
       double u0, u1;
       nwq::uniform2(q.seed, cycle, t, nwq::kDrawChild, &u0, &u1);
       uint64_t lam;

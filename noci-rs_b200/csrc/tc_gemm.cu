@@ -16,22 +16,24 @@
 //     INT32 in tensor memory (one accumulator per s), and the result is rebuilt in FP64 as
 //     sum_s 2^(e_row + e_col - 7 (s + 2)) C_s.  With S = 8 the result is FP64-faithful.
 //
-// Kernel shape: one CTA of 256 threads per 128 x 64 tile of T (cta_group::1, M = 128, N = 64).
+// Kernel shape: persistent, one CTA of 320 threads per SM walking 128 x 64 tiles of T
+// (cta_group::1, M = 128, N = 64).
 // Operands are pre-tiled in global memory by the split kernels in the tcgen05 no-swizzle K-major
 // layout (8-row x 16-byte core matrices, 64-byte-deep K tiles), so the K tile of one piece of an
 // operand is one contiguous block moved by a single cp.async.bulk (no multicast).  A pipeline
 // stage holds the K tile of EVERY piece of both operands (int8: 8 + 8 slices, 96 KB, two stages;
 // BF16: 3 + 3 pieces, 36 KB, five stages), so each slice is read from L2 once per tile and all
-// products of that K tile run from shared memory.  Thread 0 issues the copies, thread 32 the MMAs
-// (tcgen05.mma, two 32-byte K steps per product and stage, then tcgen05.commit to free the
-// stage); each product (A piece, B piece) goes to its accumulator's 64 TMEM columns.  All eight
-// warps run the epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 and columns 32 (w / 4) .. + 31
-// of every accumulator with one 32-column tcgen05.ld each, rebuilds FP64 (exact int32 -> FP64
-// conversion by the 2^52 + 2^31 offset, power-of-two scales built from the exponent bits) and
-// stores T in the [p][r][q][s] order of the build's T4 buffers, with the tile's column offsets
-// and exponents staged in shared memory.  Every mbarrier wait is bounded: on a timeout the CTA
-// records an error flag, stops issuing work, waits (bounded) for what it issued, frees its
-// tensor memory and returns.
+// products of that K tile run from shared memory.  Warp 0 issues the copies (running ahead
+// across tile boundaries), warp 1 the MMAs (tcgen05.mma, two 32-byte K steps per product and
+// stage, then tcgen05.commit to free the stage; one more commit marks the tile's accumulators
+// complete); each product (A piece, B piece) goes to its accumulator's 64 TMEM columns.  Eight
+// epilogue warps (2..9) drain a tile: warp w reads TMEM lanes 32 (w % 4) .. + 31 and one half of
+// the columns of every accumulator with one 32-column tcgen05.ld each, releases the TMEM to the
+// next tile's MMAs, then rebuilds FP64 (exact int32 -> FP64 conversion by the 2^52 + 2^31
+// offset, power-of-two scales built from the exponent bits) and stores T in the [p][r][q][s]
+// order of the build's T4 buffers while the next tile is copied and multiplied.  Every
+// mbarrier wait is bounded: on a timeout the CTA records an error flag, stops issuing work,
+// waits (bounded) for what it issued, frees its tensor memory and returns.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -43,7 +45,9 @@
 namespace nw {
 namespace {
 
-constexpr int kTcThreads = 256;
+// warp 0: copies, warp 1: MMAs, warps 2..9: epilogue
+constexpr int kTcThreads = 320;
+constexpr int kEpiWarps = 8;
 constexpr int kTileM = 128, kTileN = 64;
 constexpr int kKBytes = 64;                         // bytes of K per tile row and stage
 constexpr uint32_t kBlockBytes = 64 * kKBytes;      // one pre-tiled 64-row block: 4 KB
@@ -58,9 +62,8 @@ struct TcShape {
   static constexpr int kPieces = kKind == 1 ? kOzakiSlices : 3;
   static constexpr int kStages = kKind == 1 ? 2 : 5;
   static constexpr uint32_t kStageA = kPieces * kTileABytes, kStageB = kPieces * kTileBBytes;
-  // ring, barriers (full, empty, done), TMEM slot + abort flag, column exponents and offsets
-  static constexpr size_t kSmem = 1024 + (size_t)kStages * (kStageA + kStageB) + 8 * (2 * kStages + 1) + 8 +
-                                  2 * kTileN * sizeof(int);
+  // ring, barriers (full and empty per stage, tmem_full, tmem_empty), TMEM slot + abort flag
+  static constexpr size_t kSmem = 1024 + (size_t)kStages * (kStageA + kStageB) + 8 * (2 * kStages + 2) + 8;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -167,29 +170,40 @@ struct TcArgs {
   const int* ecol;
   int M, N;                // rows (pq) and columns (rs) of T
   int n;                   // orbital count: T[pq][rs] is stored at [p][r][q][s]
+  int ntm, ntn;            // 128-row and 64-column tiles of T
   double* out;
   uint32_t* err;
 };
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Persistent kernel: each CTA takes tiles blockIdx.x, blockIdx.x + gridDim.x, ... (64-column
+// tiles fastest, so the CTAs working at one time share their A tiles).  The copy warp runs
+// ahead through the stage ring across tile boundaries; the MMA warp starts a tile once the
+// epilogue has read the previous tile's accumulators out of TMEM (tmem_empty), and signals a
+// finished tile with tcgen05.commit (tmem_full); the epilogue warps convert and store a tile
+// while the next tile's copies and MMAs proceed.
 template <int kKind>
 __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_constant__ TcArgs g) {
   using Sh = TcShape<kKind>;
   constexpr int kPieces = Sh::kPieces, kStages = Sh::kStages;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  // 1024-byte aligned stage rings (A tiles, then B tiles); barriers and column tables after them
+  // 1024-byte aligned stage rings (A tiles, then B tiles); barriers after them
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* sa = smem;
   uint8_t* sb = smem + kStages * Sh::kStageA;
   uint64_t* full = reinterpret_cast<uint64_t*>(sb + kStages * Sh::kStageB);
   uint64_t* empty = full + kStages;
-  uint64_t* done = empty + kStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  uint64_t* tmem_full = empty + kStages;
+  uint64_t* tmem_empty = tmem_full + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tmem_empty + 1);
   volatile uint32_t* abort_flag = tmem_slot + 1;
-  int* col_exp = reinterpret_cast<int*>(tmem_slot + 2);
-  int* col_off = col_exp + kTileN;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int tm = blockIdx.y, tn = blockIdx.x;
+  const int ntiles = g.ntm * g.ntn;
+  const int mytiles = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const uint32_t ncols = (uint32_t)g.nacc * kTileN <= 64 ? 64u
                          : (uint32_t)g.nacc * kTileN <= 128 ? 128u
                          : (uint32_t)g.nacc * kTileN <= 256 ? 256u : 512u;
@@ -198,16 +212,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(done, 1);
+    mbar_init(tmem_full, 1);
+    mbar_init(tmem_empty, kEpiWarps);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  if (tid < kTileN) {
-    // column rs of T -> offset r n^2 + s of [p][r][q][s], and its exponent
-    const int col = tn * kTileN + tid;
-    const bool in = col < g.N;
-    col_off[tid] = in ? (col / g.n) * g.n * g.n + col % g.n : 0;
-    col_exp[tid] = in && g.ecol ? g.ecol[col] : 0;
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -219,99 +227,141 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int nsteps = g.nkt;
 
-  if (tid == 0) {
-    // producer: the K tile of every piece of both operands per stage
-    int issued = 0;
-    for (int t = 0; t < nsteps; ++t) {
-      const int s = t % kStages, use = t / kStages;
-      if (use > 0 && !mbar_wait(&empty[s], (uint32_t)(use - 1) & 1u)) {
-        *abort_flag = 1;
-        atomicOr(g.err, 1u);
-        break;
+  if (warp == 0) {
+    if (lane == 0) {
+      // copies: the K tile of every piece of both operands per stage, tile after tile
+      int issued = 0;
+      for (int i = 0; i < mytiles && !*abort_flag; ++i) {
+        const int tile = (int)blockIdx.x + i * (int)gridDim.x;
+        const int tm = tile / g.ntn, tn = tile % g.ntn;
+        for (int kt = 0; kt < g.nkt; ++kt) {
+          const int t = i * g.nkt + kt;
+          const int s = t % kStages, use = t / kStages;
+          if (use > 0 && !mbar_wait(&empty[s], (uint32_t)(use - 1) & 1u)) {
+            *abort_flag = 1;
+            atomicOr(g.err, 1u);
+            break;
+          }
+          if (*abort_flag) break;
+          mbar_expect_tx(&full[s], Sh::kStageA + Sh::kStageB);
+          // a 128-row A tile is the two adjacent 64-row blocks 2 tm, 2 tm + 1 of its K tile
+          const long long aoff = ((long long)kt * g.nrt_a + 2 * tm) * kBlockBytes;
+          const long long boff = ((long long)kt * g.nrt_b + tn) * kBlockBytes;
+#pragma unroll
+          for (int p = 0; p < kPieces; ++p)
+            bulk_g2s(sa + s * Sh::kStageA + p * kTileABytes, g.a + p * g.a_piece + aoff, kTileABytes, &full[s]);
+#pragma unroll
+          for (int p = 0; p < kPieces; ++p)
+            bulk_g2s(sb + s * Sh::kStageB + p * kTileBBytes, g.b + p * g.b_piece + boff, kTileBBytes, &full[s]);
+          ++issued;
+        }
       }
-      if (*abort_flag) break;
-      mbar_expect_tx(&full[s], Sh::kStageA + Sh::kStageB);
-      // a 128-row A tile is the two adjacent 64-row blocks 2 tm, 2 tm + 1 of its K tile
-      const long long aoff = ((long long)t * g.nrt_a + 2 * tm) * kBlockBytes;
-      const long long boff = ((long long)t * g.nrt_b + tn) * kBlockBytes;
-#pragma unroll
-      for (int i = 0; i < kPieces; ++i)
-        bulk_g2s(sa + s * Sh::kStageA + i * kTileABytes, g.a + i * g.a_piece + aoff, kTileABytes, &full[s]);
-#pragma unroll
-      for (int j = 0; j < kPieces; ++j)
-        bulk_g2s(sb + s * Sh::kStageB + j * kTileBBytes, g.b + j * g.b_piece + boff, kTileBBytes, &full[s]);
-      ++issued;
+      // the copies of the last stages must have landed before the CTA may exit (on the normal
+      // path these phases completed long ago; after an abort they bound the wait for them)
+      for (int t = issued - kStages < 0 ? 0 : issued - kStages; t < issued; ++t)
+        if (!mbar_wait(&full[t % kStages], (uint32_t)(t / kStages) & 1u)) atomicOr(g.err, 8u);
     }
-    // the copies of the last stages must have landed before the CTA may exit (on the normal
-    // path these phases completed long ago; after an abort they bound the wait for them)
-    for (int t = issued - kStages < 0 ? 0 : issued - kStages; t < issued; ++t)
-      if (!mbar_wait(&full[t % kStages], (uint32_t)(t / kStages) & 1u)) atomicOr(g.err, 8u);
-  } else if (tid == 32) {
-    // MMA issuer: every product of the stage, two 32-byte K steps each, into its accumulator
-    for (int t = 0; t < nsteps; ++t) {
-      const int s = t % kStages, use = t / kStages;
-      if (!mbar_wait(&full[s], (uint32_t)use & 1u)) {
-        *abort_flag = 1;
-        atomicOr(g.err, 2u);
-        break;
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // MMAs: every product of each stage, two 32-byte K steps each, into its accumulator
+      for (int i = 0; i < mytiles && !*abort_flag; ++i) {
+        // the epilogue has read the previous tile's accumulators
+        if (i > 0 && !mbar_wait(tmem_empty, (uint32_t)(i - 1) & 1u)) {
+          *abort_flag = 1;
+          atomicOr(g.err, 16u);
+          break;
+        }
+        tc_fence_after();
+        bool ok = true;
+        for (int kt = 0; kt < g.nkt; ++kt) {
+          const int t = i * g.nkt + kt;
+          const int s = t % kStages, use = t / kStages;
+          if (!mbar_wait(&full[s], (uint32_t)use & 1u)) {
+            *abort_flag = 1;
+            atomicOr(g.err, 2u);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a_st = smem_u32(sa + s * Sh::kStageA), b_st = smem_u32(sb + s * Sh::kStageB);
+          for (int p = 0; p < g.nprod; ++p) {
+            const uint32_t dcol = tmem + (uint32_t)g.pacc[p] * kTileN;
+            const bool first = kt == 0 && g.pfirst[p];
+            const uint32_t a0 = a_st + (uint32_t)g.pa[p] * kTileABytes, b0 = b_st + (uint32_t)g.pb[p] * kTileBBytes;
+#pragma unroll
+            for (int k = 0; k < kKBytes / 32; ++k)
+              mma<kKind>(dcol, smem_desc(a0 + k * 256, 128, kSbo), smem_desc(b0 + k * 256, 128, kSbo),
+                         (first && k == 0) ? 0u : 1u);
+          }
+          mma_commit(&empty[s]);
+        }
+        if (!ok) break;
+        mma_commit(tmem_full);  // arrives once every MMA of the tile has completed
       }
+    }
+  } else {
+    // epilogue warps 2..9: warp w reads TMEM lanes 32 (w % 4) .. + 31 and columns 32 h .. + 31
+    const int ew = warp - 2, quad = warp & 3, half = ew >> 2;
+    for (int i = 0; i < mytiles; ++i) {
+      const int tile = (int)blockIdx.x + i * (int)gridDim.x;
+      const int tm = tile / g.ntn, tn = tile % g.ntn;
+      const bool ok = mbar_wait(tmem_full, (uint32_t)i & 1u);
       tc_fence_after();
-      const uint32_t a_st = smem_u32(sa + s * Sh::kStageA), b_st = smem_u32(sb + s * Sh::kStageB);
-      for (int p = 0; p < g.nprod; ++p) {
-        const uint32_t dcol = tmem + (uint32_t)g.pacc[p] * kTileN;
-        const bool first = t == 0 && g.pfirst[p];
-        const uint32_t a0 = a_st + (uint32_t)g.pa[p] * kTileABytes, b0 = b_st + (uint32_t)g.pb[p] * kTileBBytes;
-#pragma unroll
-        for (int k = 0; k < kKBytes / 32; ++k)
-          mma<kKind>(dcol, smem_desc(a0 + k * 256, 128, kSbo), smem_desc(b0 + k * 256, 128, kSbo),
-                     (first && k == 0) ? 0u : 1u);
+      // warp-uniform: tcgen05.ld is a whole-warp instruction
+      if (!__all_sync(0xFFFFFFFFu, ok && !*abort_flag)) {
+        if (lane == 0 && !ok) atomicOr(g.err, 4u);
+        break;
       }
-      mma_commit(&empty[s]);
-    }
-    mma_commit(done);  // arrives once every MMA issued above has completed
-  }
-  __syncwarp();
-  // epilogue: warp w owns TMEM lanes (rows) 32 (w % 4) + lane and columns 32 (w / 4) .. + 31
-  const bool ok = mbar_wait(done, 0);
-  tc_fence_after();
-  if (!ok && lane == 0) atomicOr(g.err, 4u);
-  const int quad = warp & 3, half = warp >> 2;
-  const int row = tm * kTileM + quad * 32 + lane;
-  // warp-uniform: tcgen05.ld is a whole-warp instruction
-  if (__all_sync(0xFFFFFFFFu, ok && !*abort_flag)) {
-    const uint32_t base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * 32);
-    double v[32];
+      __syncwarp();  // converged for the .sync.aligned TMEM loads
+      const uint32_t base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * 32);
+      double v[32];
 #pragma unroll
-    for (int j = 0; j < 32; ++j) v[j] = 0.0;
-    for (int a = 0; a < g.nacc; ++a) {
-      uint32_t r[32];
-      tmem_ld32(base + (uint32_t)(a * kTileN), r);
-      tmem_wait_ld();
-      const double sc = g.acc_scale[a];
+      for (int j = 0; j < 32; ++j) v[j] = 0.0;
+      for (int a = 0; a < g.nacc; ++a) {
+        uint32_t r[32];
+        tmem_ld32(base + (uint32_t)(a * kTileN), r);
+        tmem_wait_ld();
+        const double sc = g.acc_scale[a];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const double x = kKind == 0 ? (double)__uint_as_float(r[j]) : i32_to_f64(r[j]);
-        v[j] += sc * x;
+        for (int j = 0; j < 32; ++j) {
+          const double x = kKind == 0 ? (double)__uint_as_float(r[j]) : i32_to_f64(r[j]);
+          v[j] += sc * x;
+        }
       }
-    }
-    if (row < g.M) {
-      const int p = row / g.n, q = row % g.n;
-      const long long roff = (long long)p * g.n * g.n * g.n + (long long)q * g.n;
-      const int er = g.erow ? g.erow[row] : 0;
-      double* out = g.out + roff;
+      // the accumulators are in registers: the next tile's MMAs may overwrite them
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tmem_empty);
+      const int row = tm * kTileM + quad * 32 + lane;
+      if (row < g.M) {
+        const int p = row / g.n, q = row % g.n;
+        const int er = g.erow ? g.erow[row] : 0;
+        double* out = g.out + (long long)p * g.n * g.n * g.n + (long long)q * g.n;
+        // column rs of T -> offset r n^2 + s of [p][r][q][s], stepped from the first column
+        const int c0 = tn * kTileN + half * 32;
+        int r = c0 / g.n, sidx = c0 % g.n;
 #pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const int c = half * 32 + j;
-        if (tn * kTileN + c < g.N) out[col_off[c]] = scale_pow2(v[j], er + col_exp[c]);
+        for (int j = 0; j < 32; ++j) {
+          const int col = c0 + j;
+          if (col < g.N) {
+            const int ec = g.ecol ? __ldg(g.ecol + col) : 0;
+            out[(long long)r * g.n * g.n + sidx] = scale_pow2(v[j], er + ec);
+          }
+          if (++sidx == g.n) {
+            sidx = 0;
+            ++r;
+          }
+        }
       }
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0)
+  if (warp == 0) {
+    __syncwarp();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+  }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -485,7 +535,10 @@ cudaError_t split_product(cudaStream_t st, const SplitFactor& A, const SplitFact
   g.n = n;
   g.out = out;
   g.err = err;
-  const dim3 grid((unsigned)(B.rpad / kTileN), (unsigned)(A.rpad / kTileM));
+  g.ntm = A.rpad / kTileM;
+  g.ntn = B.rpad / kTileN;
+  const int ntiles = g.ntm * g.ntn;
+  const dim3 grid((unsigned)std::min(ntiles, 148));  // persistent: one CTA per SM
   cudaError_t e;
   if (A.mode == NW_TRANSFORM_CHOL_INT8) {
     e = cudaFuncSetAttribute(tc_gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcShape<1>::kSmem);
