@@ -640,12 +640,10 @@ nw_status eval_blocked(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, doub
   nw_status st = build_all(ctx, &none);
   if (st != NW_OK) return st;
   std::vector<size_t> bytes(npair);
-  size_t total = 0;
   for (int p = 0; p < npair; ++p) {
     bytes[p] = pair_slab_doubles(n, ctx->m_counts[2 * p], ctx->m_counts[2 * p + 1]) * sizeof(double);
     if (bytes[p] > budget)
       return fail(ctx, NW_ERR_ALLOC, "one reference pair's intermediates exceed the blocked-evaluation budget");
-    total += bytes[p];
   }
   std::vector<std::vector<char>> blocks;
   {
@@ -665,7 +663,6 @@ nw_status eval_blocked(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, doub
     }
     if (any) blocks.push_back(cur);
   }
-  (void)total;
   for (size_t b = 0; b < blocks.size(); ++b) {
     const bool all = blocks.size() == 1;
     if ((st = build_all(ctx, all ? nullptr : &blocks[b])) != NW_OK) return st;
@@ -674,11 +671,9 @@ nw_status eval_blocked(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, doub
     ctx->allow_partial = false;
     if (st != NW_OK) return st;
     // the flag of out-of-range indices is read once per block: stop at the first report
-    uint32_t flag = 0;
     NW_CUDA(ctx, cudaMemcpyAsync(ctx->h_flag, ctx->flag.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     NW_CUDA(ctx, cudaStreamSynchronize(stream));
-    flag = *ctx->h_flag;
-    if (flag) return fail(ctx, NW_ERR_INVALID, "pair index out of range of the determinant basis");
+    if (*ctx->h_flag) return fail(ctx, NW_ERR_INVALID, "pair index out of range of the determinant basis");
   }
   if (nblocks) *nblocks = (uint32_t)blocks.size();
   return NW_OK;
