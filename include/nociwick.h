@@ -267,6 +267,22 @@ NW_API nw_status nw_eval_hs_batched(nw_ctx* ctx, int32_t lp, int32_t gp, const n
 NW_API nw_status nw_eval_hs_batched_device(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x_dev,
                                            const nw_exc_cache* w_dev, const double* phase_dev, uint64_t npairs,
                                            double* hs_dev, void* stream);
+/* Overlap only for the same per-reference-pair request blocks: s_out[i] = S.  Replaces
+ * xw_overlap_same_f64_batched (src/nonorthogonalwicks/eval/overlap.rs:2572-2856) and
+ * xw_overlap (:42-65) with the excitation phases. */
+NW_API nw_status nw_eval_s_batched(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x, const nw_exc_cache* w,
+                                   const double* phase, uint64_t npairs, double* s_out, void* stream);
+NW_API nw_status nw_eval_s_batched_device(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x_dev,
+                                          const nw_exc_cache* w_dev, const double* phase_dev, uint64_t npairs,
+                                          double* s_dev, void* stream);
+/* Fock one-body element with the overlap for the same request blocks (after nw_update_fock):
+ * fs_out[2i] = F, fs_out[2i + 1] = S.  Replaces xw_f_overlap_prepared
+ * (src/nonorthogonalwicks/eval/prepareonebodyoverlap.rs:57) and xw_f (eval/onebody.rs:40). */
+NW_API nw_status nw_eval_fs_batched(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x, const nw_exc_cache* w,
+                                    const double* phase, uint64_t npairs, double* fs_out, void* stream);
+NW_API nw_status nw_eval_fs_batched_device(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x_dev,
+                                           const nw_exc_cache* w_dev, const double* phase_dev, uint64_t npairs,
+                                           double* fs_dev, void* stream);
 
 /* Fock tables for the (F, S) path from the AO Fock matrices of each spin (row-major nao x nao,
  * host memory): F^(mi,mj) = cx^(mi)^T F xc^(mj) and F_0^(m) = tr(M^(m) F) for every ordered

@@ -64,9 +64,10 @@ __global__ void pack_batched_kernel(uint32_t lp, uint32_t gp, const nw_exc_cache
   }
 }
 
-nw_status eval_batched(nw_ctx* ctx, int lp, int gp, const nw_exc_cache* x, const nw_exc_cache* w,
+nw_status eval_batched(nw_ctx* ctx, EvalMode mode, int lp, int gp, const nw_exc_cache* x, const nw_exc_cache* w,
                        const double* phase, uint64_t n, double* hs, cudaStream_t s) {
   if (!ctx->built) return fail(ctx, NW_ERR_STATE, "intermediates not built");
+  if (mode == EvalMode::kFS && !ctx->fock_ready) return fail(ctx, NW_ERR_STATE, "Fock tables not set (nw_update_fock)");
   if (lp < 0 || gp < 0 || lp >= ctx->nref || gp >= ctx->nref) return fail(ctx, NW_ERR_INVALID, "reference index out of range");
   if (n == 0) return NW_OK;
   if (n >= 0x7FFFFFFFull) return fail(ctx, NW_ERR_UNSUPPORTED, "at most 2^31 - 2 requests per call");
@@ -85,7 +86,38 @@ nw_status eval_batched(nw_ctx* ctx, int lp, int gp, const nw_exc_cache* x, const
   P.dets = dets;
   P.desc = desc;
   P.ndet = 2 * n;
-  return eval_pairs_on(ctx, P, reinterpret_cast<const uint32_t*>(pairs), n, hs, EvalMode::kHS, s);
+  return eval_pairs_on(ctx, P, reinterpret_cast<const uint32_t*>(pairs), n, hs, mode, s);
+}
+
+// Host-buffer form: stage the caches and phases, evaluate, copy the results back (width
+// doubles per request), synchronise and report invalid requests.
+nw_status eval_batched_host(nw_ctx* ctx, EvalMode mode, int lp, int gp, const nw_exc_cache* x, const nw_exc_cache* w,
+                            const double* phase, uint64_t npairs, double* out, cudaStream_t s) {
+  if (npairs == 0) return NW_OK;
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (npairs >= 0x7FFFFFFFull) return fail(ctx, NW_ERR_UNSUPPORTED, "at most 2^31 - 2 requests per call");
+  const int width = mode == EvalMode::kS ? 1 : 2;
+  // staging: x caches | w caches | phases (8-byte aligned) | results (16-byte aligned)
+  const size_t cache_bytes = npairs * sizeof(nw_exc_cache);
+  const size_t off_ph = (2 * cache_bytes + 15) / 16 * 16;
+  const size_t off_out = (off_ph + npairs * sizeof(double) + 15) / 16 * 16;
+  nw_status st = ensure(ctx, ctx->bt_in, off_out + npairs * width * sizeof(double));
+  if (st != NW_OK) return st;
+  if ((st = ensure(ctx, ctx->flag, 256)) != NW_OK) return st;
+  char* base = static_cast<char*>(ctx->bt_in.p);
+  nw_exc_cache* dx = reinterpret_cast<nw_exc_cache*>(base);
+  nw_exc_cache* dw = reinterpret_cast<nw_exc_cache*>(base + cache_bytes);
+  double* dph = reinterpret_cast<double*>(base + off_ph);
+  double* dout = reinterpret_cast<double*>(base + off_out);
+  NW_CUDA(ctx, cudaMemcpyAsync(dx, x, cache_bytes, cudaMemcpyHostToDevice, s));
+  NW_CUDA(ctx, cudaMemcpyAsync(dw, w, cache_bytes, cudaMemcpyHostToDevice, s));
+  NW_CUDA(ctx, cudaMemcpyAsync(dph, phase, npairs * sizeof(double), cudaMemcpyHostToDevice, s));
+  if ((st = eval_batched(ctx, mode, lp, gp, dx, dw, dph, npairs, dout, s)) != NW_OK) return st;
+  NW_CUDA(ctx, cudaMemcpyAsync(out, dout, npairs * width * sizeof(double), cudaMemcpyDeviceToHost, s));
+  NW_CUDA(ctx, cudaMemcpyAsync(ctx->h_flag, ctx->flag.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  NW_CUDA(ctx, cudaStreamSynchronize(s));
+  if (*ctx->h_flag) return fail(ctx, NW_ERR_INVALID, "invalid excitation cache or phase in a request");
+  return NW_OK;
 }
 
 }  // namespace
@@ -98,37 +130,47 @@ nw_status nw_eval_hs_batched_device(nw_ctx* ctx, int32_t lp, int32_t gp, const n
                                     double* hs_dev, void* stream) {
   if (!ctx || (npairs && (!x_dev || !w_dev || !phase_dev || !hs_dev))) return NW_ERR_INVALID;
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
-  return nw::eval_batched(ctx, lp, gp, x_dev, w_dev, phase_dev, npairs, hs_dev, static_cast<cudaStream_t>(stream));
+  return nw::eval_batched(ctx, nw::EvalMode::kHS, lp, gp, x_dev, w_dev, phase_dev, npairs, hs_dev,
+                          static_cast<cudaStream_t>(stream));
 }
 
 nw_status nw_eval_hs_batched(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x, const nw_exc_cache* w,
                              const double* phase, uint64_t npairs, double* hs_out, void* stream) {
   if (!ctx || (npairs && (!x || !w || !phase || !hs_out))) return NW_ERR_INVALID;
-  if (npairs == 0) return NW_OK;
-  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return nw::eval_batched_host(ctx, nw::EvalMode::kHS, lp, gp, x, w, phase, npairs, hs_out,
+                               static_cast<cudaStream_t>(stream));
+}
+
+nw_status nw_eval_s_batched_device(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x_dev,
+                                   const nw_exc_cache* w_dev, const double* phase_dev, uint64_t npairs, double* s_dev,
+                                   void* stream) {
+  if (!ctx || (npairs && (!x_dev || !w_dev || !phase_dev || !s_dev))) return NW_ERR_INVALID;
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
-  if (npairs >= 0x7FFFFFFFull) return nw::fail(ctx, NW_ERR_UNSUPPORTED, "at most 2^31 - 2 requests per call");
-  // staging: x caches | w caches | phases (8-byte aligned) | (H, S) (16-byte aligned)
-  const size_t cache_bytes = npairs * sizeof(nw_exc_cache);
-  const size_t off_ph = (2 * cache_bytes + 15) / 16 * 16;
-  const size_t off_hs = (off_ph + npairs * sizeof(double) + 15) / 16 * 16;
-  nw_status st = nw::ensure(ctx, ctx->bt_in, off_hs + npairs * 2 * sizeof(double));
-  if (st != NW_OK) return st;
-  if ((st = nw::ensure(ctx, ctx->flag, 256)) != NW_OK) return st;
-  char* base = static_cast<char*>(ctx->bt_in.p);
-  nw_exc_cache* dx = reinterpret_cast<nw_exc_cache*>(base);
-  nw_exc_cache* dw = reinterpret_cast<nw_exc_cache*>(base + cache_bytes);
-  double* dph = reinterpret_cast<double*>(base + off_ph);
-  double* dhs = reinterpret_cast<double*>(base + off_hs);
-  NW_CUDA(ctx, cudaMemcpyAsync(dx, x, cache_bytes, cudaMemcpyHostToDevice, s));
-  NW_CUDA(ctx, cudaMemcpyAsync(dw, w, cache_bytes, cudaMemcpyHostToDevice, s));
-  NW_CUDA(ctx, cudaMemcpyAsync(dph, phase, npairs * sizeof(double), cudaMemcpyHostToDevice, s));
-  if ((st = nw::eval_batched(ctx, lp, gp, dx, dw, dph, npairs, dhs, s)) != NW_OK) return st;
-  NW_CUDA(ctx, cudaMemcpyAsync(hs_out, dhs, npairs * 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
-  NW_CUDA(ctx, cudaMemcpyAsync(ctx->h_flag, ctx->flag.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  NW_CUDA(ctx, cudaStreamSynchronize(s));
-  if (*ctx->h_flag) return nw::fail(ctx, NW_ERR_INVALID, "invalid excitation cache or phase in a request");
-  return NW_OK;
+  return nw::eval_batched(ctx, nw::EvalMode::kS, lp, gp, x_dev, w_dev, phase_dev, npairs, s_dev,
+                          static_cast<cudaStream_t>(stream));
+}
+
+nw_status nw_eval_s_batched(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x, const nw_exc_cache* w,
+                            const double* phase, uint64_t npairs, double* s_out, void* stream) {
+  if (!ctx || (npairs && (!x || !w || !phase || !s_out))) return NW_ERR_INVALID;
+  return nw::eval_batched_host(ctx, nw::EvalMode::kS, lp, gp, x, w, phase, npairs, s_out,
+                               static_cast<cudaStream_t>(stream));
+}
+
+nw_status nw_eval_fs_batched_device(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x_dev,
+                                    const nw_exc_cache* w_dev, const double* phase_dev, uint64_t npairs,
+                                    double* fs_dev, void* stream) {
+  if (!ctx || (npairs && (!x_dev || !w_dev || !phase_dev || !fs_dev))) return NW_ERR_INVALID;
+  NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  return nw::eval_batched(ctx, nw::EvalMode::kFS, lp, gp, x_dev, w_dev, phase_dev, npairs, fs_dev,
+                          static_cast<cudaStream_t>(stream));
+}
+
+nw_status nw_eval_fs_batched(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x, const nw_exc_cache* w,
+                             const double* phase, uint64_t npairs, double* fs_out, void* stream) {
+  if (!ctx || (npairs && (!x || !w || !phase || !fs_out))) return NW_ERR_INVALID;
+  return nw::eval_batched_host(ctx, nw::EvalMode::kFS, lp, gp, x, w, phase, npairs, fs_out,
+                               static_cast<cudaStream_t>(stream));
 }
 
 nw_status nw_eval_s_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* s_host, void* stream) {

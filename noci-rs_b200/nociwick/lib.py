@@ -127,7 +127,8 @@ class NwInfo(ctypes.Structure):
 EXPORTED = ("nw_ctx_create", "nw_ctx_create_cholesky", "nw_build_intermediates", "nw_save_intermediates",
             "nw_load_intermediates", "nw_eval_hs_pairs_blocked", "nw_pair_zero_counts",
             "nw_set_basis", "nw_eval_hs_pairs_device", "nw_eval_hs_pairs", "nw_eval_hs_pairs_noalloc",
-            "nw_eval_hs_batched", "nw_eval_hs_batched_device", "nw_eval_s_pairs_device", "nw_eval_s_pairs", "nw_update_fock", "nw_eval_fs_pairs_device", "nw_eval_fs_pairs",
+            "nw_eval_hs_batched", "nw_eval_hs_batched_device", "nw_eval_s_batched", "nw_eval_s_batched_device",
+            "nw_eval_fs_batched", "nw_eval_fs_batched_device", "nw_eval_s_pairs_device", "nw_eval_s_pairs", "nw_update_fock", "nw_eval_fs_pairs_device", "nw_eval_fs_pairs",
             "nw_build_hs_matrix", "nw_build_fs_matrix", "nw_general_evp",
             "nw_qmc_create", "nw_qmc_run", "nw_qmc_set_shift", "nw_qmc_last_run_ms", "nw_qmc_populations", "nw_qmc_set_populations", "nw_qmc_cycle_delta",
             "nw_qmc_destroy", "nw_qmc_harvest", "nw_qmc_train_proposal", "nw_qmc_set_generator",
@@ -161,6 +162,8 @@ def load(path: Optional[str] = None):
                                            ctypes.POINTER(ctypes.c_uint32), vp]
     L.nw_eval_hs_batched.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_eval_hs_batched_device.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_uint64, vp, vp]
+    for name in ("nw_eval_s_batched", "nw_eval_s_batched_device", "nw_eval_fs_batched", "nw_eval_fs_batched_device"):
+        getattr(L, name).argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_eval_s_pairs.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_pair_zero_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
     L.nw_set_basis.argtypes = [vp, vp, ctypes.c_uint64]
@@ -352,20 +355,21 @@ class WicksShared:
         return out
 
     def eval_batched(self, lp: int, gp: int, x_caches: np.ndarray, w_caches: np.ndarray, phase: np.ndarray,
-                     stream: int = 0) -> np.ndarray:
-        """(H, S) of one ordered reference pair (lp, gp) from caller-held excitation caches
+                     stream: int = 0, kind: str = "hs") -> np.ndarray:
+        """One ordered reference pair (lp, gp) from caller-held excitation caches
         (xw_hamiltonian_overlap_prepared_batched): x_caches / w_caches of NW_EXC_CACHE_DTYPE,
-        phase the product of both excitation phases per request; returns (n, 2)."""
+        phase the product of both excitation phases per request.  kind "hs" returns (H, S) as
+        (n, 2), "s" the overlaps (n,), "fs" (F, S) as (n, 2) after update_fock."""
         x = np.ascontiguousarray(x_caches, dtype=NW_EXC_CACHE_DTYPE)
         w = np.ascontiguousarray(w_caches, dtype=NW_EXC_CACHE_DTYPE)
         ph = np.ascontiguousarray(phase, dtype=np.float64)
         n = x.shape[0]
         if w.shape[0] != n or ph.shape[0] != n:
             raise ValueError("x_caches, w_caches and phase must have one entry per request")
-        out = np.empty((n, 2), np.float64)
-        self._check(self._lib.nw_eval_hs_batched(self._ctx, int(lp), int(gp), x.ctypes.data, w.ctypes.data,
-                                                 ph.ctypes.data, n, out.ctypes.data, ctypes.c_void_p(stream)),
-                    "nw_eval_hs_batched")
+        fn = {"hs": "nw_eval_hs_batched", "s": "nw_eval_s_batched", "fs": "nw_eval_fs_batched"}[kind]
+        out = np.empty((n,) if kind == "s" else (n, 2), np.float64)
+        self._check(getattr(self._lib, fn)(self._ctx, int(lp), int(gp), x.ctypes.data, w.ctypes.data,
+                                           ph.ctypes.data, n, out.ctypes.data, ctypes.c_void_p(stream)), fn)
         return out
 
     def eval_overlap(self, pairs: np.ndarray, stream: int = 0) -> np.ndarray:

@@ -61,6 +61,39 @@ def test_batched_blocks_match_resident_pairs_and_oracle():
     assert far.any() and np.all(got[far] == 0.0)
 
 
+def test_batched_overlap_and_fock_blocks_match_resident_pairs():
+    """nw_eval_s_batched and nw_eval_fs_batched on the same per-reference-pair blocks equal the
+    resident-basis overlap and (F, S) calls, every block (zero-overlap ones included)."""
+    system = _system()
+    basis = sy.sd_basis(10, 3, 3, 3)
+    pairs = sy.sample_pairs(basis, 20_000, seed=9, distinct_parents=False, canonical=False).astype(np.int64)
+    caches = L.exc_caches(basis)
+    par = basis["parent"].astype(np.int64)
+    rng = np.random.default_rng(3)
+    fa = rng.standard_normal((10, 10))
+    fa = fa + fa.T
+    fb = fa + 0.2 * np.eye(10)
+    with nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs) as w:
+        w.build().set_basis(basis)
+        w.update_fock(fa, fb)
+        s_res = w.eval_overlap(pairs)
+        fs_res = w.eval_fs_pairs(pairs)
+        s_got = np.full(pairs.shape[0], np.nan)
+        fs_got = np.full((pairs.shape[0], 2), np.nan)
+        for lp in range(3):
+            for gp in range(3):
+                sel = np.nonzero((par[pairs[:, 0]] == lp) & (par[pairs[:, 1]] == gp))[0]
+                if sel.size == 0:
+                    continue
+                a, b = pairs[sel, 0], pairs[sel, 1]
+                ph = basis["phase"][a] * basis["phase"][b]
+                s_got[sel] = w.eval_batched(lp, gp, caches[a], caches[b], ph, kind="s")
+                fs_got[sel] = w.eval_batched(lp, gp, caches[a], caches[b], ph, kind="fs")
+    assert np.all(np.isfinite(s_got)) and np.all(np.isfinite(fs_got))
+    assert np.max(np.abs(s_got - s_res)) <= 1e-13
+    assert np.max(np.abs(fs_got - fs_res)) <= 1e-12
+
+
 def test_batched_rejects_invalid_caches():
     system = _system()
     basis = sy.sd_basis(10, 3, 3, 3)
