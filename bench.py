@@ -483,12 +483,8 @@ def snoci_leg(args, rank, world, local_rank, dist):
     pred = scr.predict(cand_all)
     nkeep = int(np.ceil(0.25 * npool))
     keep = np.sort(np.argsort(-pred, kind="stable")[:nkeep])
-    kept, ept2_kept, e0_kept, info_kept = sn.pt2_scores(w, m, cand_all[keep], c, ecur, opts)
+    kept, ept2_kept, _, info_kept = sn.pt2_scores(w, m, cand_all[keep], c, ecur, opts)
     screen_s = time.perf_counter() - t0
-    dropped = np.setdiff1d(cand_all, cand_all[keep], assume_unique=True)
-    t0 = time.perf_counter()
-    rem = sn.diagonal_pt2_remainder(w, m, dropped, c, ecur, e0_kept)
-    rem_s = time.perf_counter() - t0
     scr.close()
     # iteration 1 at full size: the pool grows by the excitations of the 20 selected
     # determinants; its exhaustive M would not fit in HBM, the learned screener keeps 10 %
@@ -509,8 +505,6 @@ def snoci_leg(args, rank, world, local_rank, dist):
         exhaustive_loop = {"seconds": time.perf_counter() - t0, "energy": res_x.energy, "ept2": res_x.ept2,
                            "energy_plus_ept2": res_x.energy + res_x.ept2,
                            "learned_energy_plus_ept2": res.energy + res.ept2,
-                           "learned_energy_plus_ept2_with_dropped_diagonal":
-                               res.energy + res.ept2 + (res.iterations[-1].ept2_remainder or 0.0),
                            "difference_mEh": 1e3 * ((res.energy + res.ept2) - (res_x.energy + res_x.ept2)),
                            "e_current_difference_mEh": 1e3 * (res.energy - res_x.energy),
                            "last_selection_overlap": len(set(res.added) & set(res_x.added)) / max(1, len(res_x.added)),
@@ -522,9 +516,6 @@ def snoci_leg(args, rank, world, local_rank, dist):
     w.close()
     iters = [{"iteration": it.it, "selected_space": it.nselected, "pool": it.npool, "scored": it.nscored,
               "screened": it.screened, "seconds": it.seconds, "e_current": it.ecurrent, "ept2": it.ept2,
-              "ept2_dropped_diagonal": it.ept2_remainder,
-              "ept2_kept_plus_dropped_diagonal": (it.ept2 + it.ept2_remainder) if it.ept2_remainder is not None
-              else None,
               "gmres": it.gmres,
               "packed_m_gb_scored": it.nscored * (it.nscored + 1) / 2 * 8 / 1e9,
               "packed_m_gb_exhaustive": it.npool * (it.npool + 1) / 2 * 8 / 1e9} for it in res.iterations]
@@ -542,8 +533,6 @@ def snoci_leg(args, rank, world, local_rank, dist):
             "prepare_seconds": prep_s,
             "exhaustive": {"seconds": full_s, "scored": int(npool), "ept2": ept2_full, "gmres": info_full},
             "learned": {"train_seconds": train_s, "seconds": screen_s, "scored": int(nkeep), "ept2": ept2_kept,
-                        "ept2_dropped_diagonal": rem, "ept2_kept_plus_dropped_diagonal": ept2_kept + rem,
-                        "remainder_seconds": rem_s,
                         "gmres": info_kept, "training": rep,
                         "selected_overlap": len(sel_full & sel_scr) / max(1, len(sel_full)),
                         "top200_recall": float(np.isin(top, keep).mean()),

@@ -280,7 +280,6 @@ class SnociOptions:
     min_keep: int = 64
     audit: bool = False             # screened iterations also score the whole pool (the referee)
     packed_m_max_bytes: float = 120e9   # above this the candidate M is applied matrix-free
-    pt2_remainder: bool = True      # screened iterations: diagonal PT2 estimate of the dropped candidates
 
 
 @dataclass
@@ -299,7 +298,6 @@ class SnociIteration:
     recall: Optional[float] = None        # audit: exhaustive top picks found among the kept
     best_kept: Optional[bool] = None       # audit: the exhaustive best candidate was kept
     same_selection: Optional[bool] = None  # audit: the screened step selected the same set
-    ept2_remainder: Optional[float] = None  # screened: diagonal estimate over the dropped candidates
 
 
 @dataclass
@@ -352,27 +350,6 @@ def pt2_scores(wicks, m: int, cand: np.ndarray, c: np.ndarray, ecurrent: float, 
     return np.abs(amp * v_omega), ept2, e0, info
 
 
-def diagonal_pt2_remainder(wicks, m: int, cand: np.ndarray, c: np.ndarray, ecurrent: float, e0: float) -> float:
-    """Second-order energy of candidates that the solve leaves out (the ones a screener drops):
-    sum_a -(V_a^Omega)^2 / M^Omega_aa with the projected diagonal of the Diag preconditioner
-    (Preconditioner::new, src/snoci/types.rs:161-251: M_aa - 2 f_a0 s_a0 + 2 E0 s_a0^2 for real
-    states), an Epstein-Nesbet-type estimate that needs only the candidates' couplings to the
-    current space and their diagonal elements, O(n) instead of the n^2 / 2 pairs of M."""
-    cand = np.ascontiguousarray(cand, dtype=np.uint32)
-    if cand.shape[0] == 0:
-        return 0.0
-    cur = np.arange(m, dtype=np.uint32)
-    h_ai, s_ai = wicks.build_hs_matrix(cand, cur, symmetric=False)
-    f_ai, _ = wicks.build_fs_matrix(cand, cur, symmetric=False)
-    s_a0 = s_ai @ c
-    f_a0 = f_ai @ c
-    v = h_ai @ c - ecurrent * s_a0
-    fs = wicks.eval_fs_pairs(np.stack([cand, cand], axis=1))
-    d = fs[:, 0] - e0 * fs[:, 1] - 2.0 * f_a0 * s_a0 + 2.0 * e0 * s_a0 * s_a0
-    keep = np.abs(d) > 1e-12
-    return float(-(v[keep] ** 2 / d[keep]).sum())
-
-
 def snoci(wicks, system, opts: SnociOptions, screener=None, log=None) -> SnociResult:
     """Iterate snoci_step (src/snoci/step.rs:178-550) from the reference space.  ``wicks`` is a
     built WicksShared of the system's references; its resident basis is replaced each
@@ -409,10 +386,6 @@ def snoci(wicks, system, opts: SnociOptions, screener=None, log=None) -> SnociRe
             f"{time.perf_counter() - t0:.1f} s")
         kept_scores, ept2, e0, info = pt2_scores(wicks, m, cand, c, ecurrent, opts)
         say(f"iteration {it}: E_PT2 {ept2:.10f}, GMRES {info}, {time.perf_counter() - t0:.1f} s")
-        remainder = None
-        if screened and opts.pt2_remainder:
-            dropped = np.setdiff1d(cand_all, cand, assume_unique=True)
-            remainder = diagonal_pt2_remainder(wicks, m, dropped, c, ecurrent, e0)
         scores = np.zeros(npool)
         scores[keep] = kept_scores
         if screener is not None:
@@ -428,7 +401,7 @@ def snoci(wicks, system, opts: SnociOptions, screener=None, log=None) -> SnociRe
             best = bool(np.isin(top[:1], keep).all())
             same = set(top.tolist()) == set(chosen.tolist())
         rec = SnociIteration(it, m, npool, int(cand.shape[0]), ecurrent, e0, ept2, info, int(chosen.shape[0]),
-                             seconds, screened, recall, best, same, remainder)
+                             seconds, screened, recall, best, same)
         result = SnociResult(ecurrent, ept2, c, sel, sel_labels,
                              ([] if result is None else result.iterations) + [rec],
                              added=[pool.labels[i] for i in chosen])
