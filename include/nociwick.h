@@ -19,8 +19,12 @@
  *  - Pair (a, b) puts determinant a in the bra and b in the ket; results are written as
  *    hs[2*i] = H, hs[2*i + 1] = S.
  *  - Every call returns an nw_status; NW_OK is 0.  Nothing aborts the process.
- *  - A context owns its device memory and is not thread-safe; calls on one context must be
- *    serialised by the caller (different contexts are independent).
+ *  - A context owns its device memory.  Its entry points may be called from several host
+ *    threads, each with its own stream: calls on one context are serialised (a per-context
+ *    lock while a call enqueues its work, and on the device each call's work waits for the
+ *    previous call's, since they share the context's scratch buffers); different contexts are
+ *    independent.  nw_ctx_destroy must not race with other calls on the context, and calls of
+ *    nw_eval_hs_pairs_noalloc must not overlap at all (its scratch is per process).
  */
 #ifndef NOCIWICK_H
 #define NOCIWICK_H

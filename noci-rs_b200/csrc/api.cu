@@ -245,6 +245,7 @@ nw_status create_base(int nao, int nmo, double enuc, const double* s, const doub
         cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming) != cudaSuccess)
       st = NW_ERR_CUDA;
   if (st == NW_OK && cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess) st = NW_ERR_CUDA;
+  if (st == NW_OK && cudaEventCreateWithFlags(&ctx->ev_free, cudaEventDisableTiming) != cudaSuccess) st = NW_ERR_CUDA;
   if (st != NW_OK) {
     nw_ctx_destroy(ctx);
     return st;
@@ -305,6 +306,7 @@ nw_status nw_ctx_create_cholesky(const nw_system_cd* sys, const nw_refs* refs, c
 
 nw_status nw_set_transform(nw_ctx* ctx, int32_t mode) {
   if (!ctx) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   if (mode < NW_TRANSFORM_FP64 || mode > NW_TRANSFORM_CHOL_BF16X6) return nw::fail(ctx, NW_ERR_INVALID, "unknown transform");
   if (mode != NW_TRANSFORM_FP64 && !ctx->d_chol)
     return nw::fail(ctx, NW_ERR_STATE, "Cholesky transforms need a context from nw_ctx_create_cholesky");
@@ -348,6 +350,7 @@ nw_status nw_transform_product(int32_t mode, const double* u, const double* v, i
 
 nw_status nw_build_intermediates(nw_ctx* ctx) {
   if (!ctx) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
   return nw::build_all(ctx, nullptr);
 }
@@ -361,6 +364,7 @@ nw_status nw_pair_zero_counts(const nw_ctx* ctx, int32_t* m) {
 
 nw_status nw_set_basis(nw_ctx* ctx, const nw_det* basis, uint64_t ndet) {
   if (!ctx || (!basis && ndet)) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   if (ndet >= 0xFFFFFFFFull) return nw::fail(ctx, NW_ERR_UNSUPPORTED, "at most 2^32 - 2 determinants");
   if (ctx->live_qmc > 0)
     return nw::fail(ctx, NW_ERR_STATE, "a QMC object uses the resident basis (nw_qmc_destroy it first)");
@@ -405,6 +409,7 @@ nw_status nw_set_basis(nw_ctx* ctx, const nw_det* basis, uint64_t ndet) {
 nw_status nw_eval_hs_pairs_blocked(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* hs_dev,
                                    uint64_t slab_budget, uint32_t* nblocks, void* stream) {
   if (!ctx || (npairs && (!pairs_dev || !hs_dev))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   if (ctx->live_qmc > 0)
     return nw::fail(ctx, NW_ERR_STATE, "a QMC object uses the intermediates (nw_qmc_destroy it first)");
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -414,27 +419,33 @@ nw_status nw_eval_hs_pairs_blocked(nw_ctx* ctx, const uint32_t* pairs_dev, uint6
 nw_status nw_eval_hs_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* hs_dev,
                                   void* stream) {
   if (!ctx || (npairs && (!pairs_dev || !hs_dev))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   return nw::eval_pairs(ctx, pairs_dev, npairs, hs_dev, nw::EvalMode::kHS, static_cast<cudaStream_t>(stream));
 }
 
 nw_status nw_eval_hs_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* hs_dev,
                                    void* stream) {
   if (!ctx || (npairs && (!pairs_dev || !hs_dev))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   return nw::eval_pairs_noalloc(ctx, pairs_dev, npairs, hs_dev, static_cast<cudaStream_t>(stream));
 }
 
 nw_status nw_eval_s_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* s_dev,
                                  void* stream) {
   if (!ctx || (npairs && (!pairs_dev || !s_dev))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   return nw::eval_pairs(ctx, pairs_dev, npairs, s_dev, nw::EvalMode::kS, static_cast<cudaStream_t>(stream));
 }
 
 nw_status nw_eval_hs_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* hs_host, void* stream) {
+  if (!ctx) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   return eval_host(ctx, nw::EvalMode::kHS, pairs_host, npairs, hs_host, stream);
 }
 
 nw_status nw_update_fock(nw_ctx* ctx, const double* fock_a, const double* fock_b) {
   if (!ctx || !fock_a || !fock_b) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   const size_t n2 = (size_t)ctx->nao * ctx->nao;
   if (!finite_all(fock_a, n2) || !finite_all(fock_b, n2)) return nw::fail(ctx, NW_ERR_INVALID, "non-finite Fock matrix");
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -444,22 +455,27 @@ nw_status nw_update_fock(nw_ctx* ctx, const double* fock_a, const double* fock_b
 nw_status nw_eval_fs_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, uint64_t npairs, double* fs_dev,
                                   void* stream) {
   if (!ctx || (npairs && (!pairs_dev || !fs_dev))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   return nw::eval_pairs(ctx, pairs_dev, npairs, fs_dev, nw::EvalMode::kFS, static_cast<cudaStream_t>(stream));
 }
 
 nw_status nw_eval_fs_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* fs_host, void* stream) {
+  if (!ctx) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   return eval_host(ctx, nw::EvalMode::kFS, pairs_host, npairs, fs_host, stream);
 }
 
 nw_status nw_build_hs_matrix(nw_ctx* ctx, const uint32_t* left, uint64_t nl, const uint32_t* right, uint64_t nr,
                              int symmetric, double* h_out, double* s_out) {
   if (!ctx || (nl && !left) || (nr && !right) || (nl && nr && (!h_out || !s_out))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   return nw::build_matrix(ctx, nw::EvalMode::kHS, left, nl, right, nr, symmetric != 0, h_out, s_out);
 }
 
 nw_status nw_build_fs_matrix(nw_ctx* ctx, const uint32_t* left, uint64_t nl, const uint32_t* right, uint64_t nr,
                              int symmetric, double* f_out, double* s_out) {
   if (!ctx || (nl && !left) || (nr && !right) || (nl && nr && (!f_out || !s_out))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   if (!ctx->fock_ready) return nw::fail(ctx, NW_ERR_STATE, "Fock tables not set (nw_update_fock)");
   return nw::build_matrix(ctx, nw::EvalMode::kFS, left, nl, right, nr, symmetric != 0, f_out, s_out);
 }
@@ -478,6 +494,7 @@ nw_status nw_general_evp(nw_ctx* ctx, int32_t n, const double* h, const double* 
 
 nw_status nw_sync(nw_ctx* ctx, void* stream) {
   if (!ctx) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
   if (ctx->flag.p) {
@@ -490,6 +507,7 @@ nw_status nw_sync(nw_ctx* ctx, void* stream) {
 
 nw_status nw_set_timing(nw_ctx* ctx, int enable) {
   if (!ctx) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
   if (enable < 0 || enable > 2) return NW_ERR_INVALID;
   if (enable && !ctx->ev[0]) {
@@ -507,6 +525,7 @@ nw_status nw_set_timing(nw_ctx* ctx, int enable) {
 
 nw_status nw_last_class_timings(nw_ctx* ctx, float* ms) {
   if (!ctx || !ms) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   if (!ctx->timed_valid || !ctx->timed_classes)
     return nw::fail(ctx, NW_ERR_STATE, "no serially timed evaluation recorded (nw_set_timing(ctx, 2))");
   NW_CUDA(ctx, cudaEventSynchronize(ctx->evc[5]));
@@ -516,6 +535,7 @@ nw_status nw_last_class_timings(nw_ctx* ctx, float* ms) {
 
 nw_status nw_last_timings(nw_ctx* ctx, float* ms) {
   if (!ctx || !ms) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   if (!ctx->timed_valid) return nw::fail(ctx, NW_ERR_STATE, "no timed evaluation recorded");
   NW_CUDA(ctx, cudaEventSynchronize(ctx->ev[5]));
   for (int i = 0; i < 4; ++i) NW_CUDA(ctx, cudaEventElapsedTime(&ms[i], ctx->ev[i], ctx->ev[i + 1]));
@@ -572,7 +592,7 @@ nw_status nw_ctx_destroy(nw_ctx* ctx) {
   for (cudaStream_t q : {ctx->s_in, ctx->s_comp, ctx->s_out, ctx->s_aux[0], ctx->s_aux[1], ctx->s_aux[2]})
     if (q) cudaStreamDestroy(q);
   for (cudaEvent_t e : {ctx->ev_start, ctx->ev_in[0], ctx->ev_in[1], ctx->ev_comp[0], ctx->ev_comp[1], ctx->ev_fork,
-                        ctx->ev_join[0], ctx->ev_join[1], ctx->ev_join[2]})
+                        ctx->ev_join[0], ctx->ev_join[1], ctx->ev_join[2], ctx->ev_free})
     if (e) cudaEventDestroy(e);
   if (ctx->blas) cublasDestroy(ctx->blas);
   if (ctx->solver) cusolverDnDestroy(ctx->solver);

@@ -129,6 +129,7 @@ nw_status nw_eval_hs_batched_device(nw_ctx* ctx, int32_t lp, int32_t gp, const n
                                     const nw_exc_cache* w_dev, const double* phase_dev, uint64_t npairs,
                                     double* hs_dev, void* stream) {
   if (!ctx || (npairs && (!x_dev || !w_dev || !phase_dev || !hs_dev))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
   return nw::eval_batched(ctx, nw::EvalMode::kHS, lp, gp, x_dev, w_dev, phase_dev, npairs, hs_dev,
                           static_cast<cudaStream_t>(stream));
@@ -137,6 +138,7 @@ nw_status nw_eval_hs_batched_device(nw_ctx* ctx, int32_t lp, int32_t gp, const n
 nw_status nw_eval_hs_batched(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x, const nw_exc_cache* w,
                              const double* phase, uint64_t npairs, double* hs_out, void* stream) {
   if (!ctx || (npairs && (!x || !w || !phase || !hs_out))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   return nw::eval_batched_host(ctx, nw::EvalMode::kHS, lp, gp, x, w, phase, npairs, hs_out,
                                static_cast<cudaStream_t>(stream));
 }
@@ -145,6 +147,7 @@ nw_status nw_eval_s_batched_device(nw_ctx* ctx, int32_t lp, int32_t gp, const nw
                                    const nw_exc_cache* w_dev, const double* phase_dev, uint64_t npairs, double* s_dev,
                                    void* stream) {
   if (!ctx || (npairs && (!x_dev || !w_dev || !phase_dev || !s_dev))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
   return nw::eval_batched(ctx, nw::EvalMode::kS, lp, gp, x_dev, w_dev, phase_dev, npairs, s_dev,
                           static_cast<cudaStream_t>(stream));
@@ -153,6 +156,7 @@ nw_status nw_eval_s_batched_device(nw_ctx* ctx, int32_t lp, int32_t gp, const nw
 nw_status nw_eval_s_batched(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x, const nw_exc_cache* w,
                             const double* phase, uint64_t npairs, double* s_out, void* stream) {
   if (!ctx || (npairs && (!x || !w || !phase || !s_out))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   return nw::eval_batched_host(ctx, nw::EvalMode::kS, lp, gp, x, w, phase, npairs, s_out,
                                static_cast<cudaStream_t>(stream));
 }
@@ -161,6 +165,7 @@ nw_status nw_eval_fs_batched_device(nw_ctx* ctx, int32_t lp, int32_t gp, const n
                                     const nw_exc_cache* w_dev, const double* phase_dev, uint64_t npairs,
                                     double* fs_dev, void* stream) {
   if (!ctx || (npairs && (!x_dev || !w_dev || !phase_dev || !fs_dev))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
   return nw::eval_batched(ctx, nw::EvalMode::kFS, lp, gp, x_dev, w_dev, phase_dev, npairs, fs_dev,
                           static_cast<cudaStream_t>(stream));
@@ -169,12 +174,14 @@ nw_status nw_eval_fs_batched_device(nw_ctx* ctx, int32_t lp, int32_t gp, const n
 nw_status nw_eval_fs_batched(nw_ctx* ctx, int32_t lp, int32_t gp, const nw_exc_cache* x, const nw_exc_cache* w,
                              const double* phase, uint64_t npairs, double* fs_out, void* stream) {
   if (!ctx || (npairs && (!x || !w || !phase || !fs_out))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   return nw::eval_batched_host(ctx, nw::EvalMode::kFS, lp, gp, x, w, phase, npairs, fs_out,
                                static_cast<cudaStream_t>(stream));
 }
 
 nw_status nw_eval_s_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* s_host, void* stream) {
   if (!ctx || (npairs && (!pairs_host || !s_host))) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   if (npairs == 0) return NW_OK;
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
   NW_CUDA(ctx, cudaSetDevice(ctx->device));

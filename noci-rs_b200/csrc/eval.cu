@@ -837,6 +837,7 @@ nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs
 extern "C" nw_status nw_autotune(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* hs, void* stream,
                                  nw_tune_report* rep) {
   if (!ctx || !pairs || !hs || !rep || npairs == 0) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, static_cast<cudaStream_t>(stream));
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
   static const uint64_t kBudgets[] = {1ull << 14, 1ull << 16, 1ull << 18, 1ull << 20, 1ull << 22, 1ull << 23};

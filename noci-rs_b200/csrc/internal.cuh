@@ -7,6 +7,8 @@
 #include <cusolverDn.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include <string>
 #include <vector>
 
@@ -97,6 +99,13 @@ struct nw_ctx {
   cudaStream_t s_aux[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t ev_fork = nullptr, ev_join[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t ev_start = nullptr;
+  // Calls on one context from several host threads (each on its own stream) are serialised:
+  // the guard holds mtx while a call enqueues its work, and the work of one call waits for the
+  // previous call's (ev_free, recorded on that call's stream), since both use the context's
+  // scratch buffers.
+  std::recursive_mutex mtx;
+  cudaEvent_t ev_free = nullptr;
+  bool ev_free_used = false;
   cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr};
 
   // Fock (F + S) path: per (pair, spin) [M^(0), M^(1), cx^(0), cx^(1), xc^(0), xc^(1)] kept
@@ -132,6 +141,25 @@ struct nw_ctx {
 };
 
 namespace nw {
+
+// Serialises one entry point's use of a context (see nw_ctx::mtx): the stream of the call first
+// waits for the work of the previous call on the context, and the call's end is recorded for
+// the next one.
+struct CtxGuard {
+  nw_ctx* ctx;
+  cudaStream_t stream;
+  CtxGuard(nw_ctx* c, cudaStream_t s) : ctx(c), stream(s) {
+    ctx->mtx.lock();
+    if (ctx->ev_free_used) cudaStreamWaitEvent(stream, ctx->ev_free, 0);
+  }
+  ~CtxGuard() {
+    if (ctx->ev_free && cudaEventRecord(ctx->ev_free, stream) == cudaSuccess) ctx->ev_free_used = true;
+    ctx->mtx.unlock();
+  }
+  CtxGuard(const CtxGuard&) = delete;
+  CtxGuard& operator=(const CtxGuard&) = delete;
+};
+
 
 // Pipelined host-buffer path: about kPipeChunks chunks of at least kPipeMinChunk pairs.
 constexpr uint64_t kPipeChunks = 16;

@@ -584,6 +584,7 @@ nw_status nw_pt2_create(nw_ctx* ctx, const uint32_t* cand, uint64_t n, double e0
   if (!out) return NW_ERR_INVALID;
   *out = nullptr;
   if (!ctx || !cand || n == 0 || !std::isfinite(e0)) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   if (!ctx->fock_ready) return nw::fail(ctx, NW_ERR_STATE, "Fock tables not set (nw_update_fock)");
   if (!ctx->d_dets) return nw::fail(ctx, NW_ERR_STATE, "no determinant basis set");
   if (n > 0x7FFFFFFFull) return nw::fail(ctx, NW_ERR_UNSUPPORTED, "too many candidates");
@@ -650,6 +651,7 @@ nw_status nw_pt2_create_matrix_free(nw_ctx* ctx, const uint32_t* cand, uint64_t 
   if (!out) return NW_ERR_INVALID;
   *out = nullptr;
   if (!ctx || !cand || n == 0 || !std::isfinite(e0)) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   if (!ctx->fock_ready) return nw::fail(ctx, NW_ERR_STATE, "Fock tables not set (nw_update_fock)");
   if (!ctx->d_dets) return nw::fail(ctx, NW_ERR_STATE, "no determinant basis set");
   if (n > 0x7FFFFFFFull) return nw::fail(ctx, NW_ERR_UNSUPPORTED, "too many candidates");
@@ -688,6 +690,7 @@ nw_status nw_pt2_create_matrix_free(nw_ctx* ctx, const uint32_t* cand, uint64_t 
 
 nw_status nw_pt2_apply_m(nw_pt2* p, const double* x, double* y) {
   if (!p || !x || !y) return NW_ERR_INVALID;
+  nw::CtxGuard guard(p->ctx, nullptr);
   nw_ctx* ctx = p->ctx;
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
   double *dx = nullptr, *dy = nullptr;
@@ -726,6 +729,7 @@ nw_status nw_pt2_solve(nw_pt2* p, const nw_pt2_projection* proj, const double* r
                        double* x_out, nw_gmres_info* info) {
   if (!p || !proj || !rhs || !opts || !x_out || !info) return NW_ERR_INVALID;
   if (!proj->s_a0 || !proj->s_0a || !proj->f_a0 || !proj->f_0a) return NW_ERR_INVALID;
+  nw::CtxGuard guard(p->ctx, nullptr);
   if (opts->max_iter < 0 || opts->restart < 1 || !(opts->res_tol >= 0.0)) return NW_ERR_INVALID;
   nw_ctx* ctx = p->ctx;
   NW_CUDA(ctx, cudaSetDevice(ctx->device));

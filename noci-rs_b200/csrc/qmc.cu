@@ -761,6 +761,7 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
   if (!out) return NW_ERR_INVALID;
   *out = nullptr;
   if (!ctx || !opts || !c0 || (nref_idx && !ref_idx)) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   if (!ctx->built) return nw::fail(ctx, NW_ERR_STATE, "intermediates not built");
   if (ctx->partial)
     return nw::fail(ctx, NW_ERR_STATE, "the intermediates hold one block of a blocked evaluation (rebuild them)");
@@ -952,6 +953,7 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
 
 nw_status nw_qmc_run(nw_qmc* q, int32_t nreports, nw_qmc_report* reports) {
   if (!q || nreports < 0 || (nreports && !reports)) return NW_ERR_INVALID;
+  nw::CtxGuard guard(q->ctx, q->stream);
   nw_ctx* ctx = q->ctx;
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
   if (!q->graph) {

@@ -367,12 +367,14 @@ extern "C" {
 
 nw_status nw_save_intermediates(nw_ctx* ctx, const char* slab_path, const char* meta_path) {
   if (!ctx || !slab_path || !meta_path) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
   return nw::save_intermediates(ctx, slab_path, meta_path);
 }
 
 nw_status nw_load_intermediates(nw_ctx* ctx, const char* slab_path, const char* meta_path) {
   if (!ctx || !slab_path || !meta_path) return NW_ERR_INVALID;
+  nw::CtxGuard guard(ctx, nullptr);
   if (ctx->live_qmc > 0)
     return nw::fail(ctx, NW_ERR_STATE, "a QMC object uses the intermediates (nw_qmc_destroy it first)");
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
