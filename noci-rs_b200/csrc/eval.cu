@@ -328,7 +328,10 @@ __device__ __forceinline__ void for_each_gen_pair(uint32_t begin, uint32_t end, 
     if (lane == 0) c = atomicAdd(work, 1u);
     c = __shfl_sync(0xffffffffu, c, 0);
     if (c >= nchunk) break;
-    const uint32_t t = begin + c * 32 + lane;
+    // chunks are handed out from the end of the range: within each reference pair the classes
+    // are keyed in increasing (L_alpha, L_beta), so the costliest chunks go first and the last
+    // ones, which set the kernel's tail, are the cheapest
+    const uint32_t t = begin + (nchunk - 1 - c) * 32 + lane;
     if (t < end) f(t);
   }
 }

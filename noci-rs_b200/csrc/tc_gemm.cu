@@ -19,13 +19,15 @@
 // Kernel shape: persistent, one CTA of 320 threads per SM walking 128 x 64 tiles of T
 // (cta_group::1, M = 128, N = 64).
 // Operands are pre-tiled in global memory by the split kernels in the tcgen05 no-swizzle K-major
-// layout (8-row x 16-byte core matrices, 64-byte-deep K tiles), so the K tile of one piece of an
-// operand is one contiguous block moved by a single cp.async.bulk (no multicast).  A pipeline
-// stage holds the K tile of EVERY piece of both operands (int8: 8 + 8 slices, 96 KB, two stages;
-// BF16: 3 + 3 pieces, 36 KB, five stages), so each slice is read from L2 once per tile and all
+// layout (8-row x 16-byte core matrices; 32-byte-deep K tiles for the int8 slices, 64-byte for
+// the BF16 pieces), so the K tile of one piece of an operand is one contiguous block moved by a
+// single cp.async.bulk (no multicast).  A pipeline stage holds the K tile of EVERY piece of both
+// operands (int8: 8 + 8 slices, 48 KB, four stages; BF16: 3 + 3 pieces, 36 KB, five stages), so
+// each slice is read from L2 once per tile and all
 // products of that K tile run from shared memory.  Warp 0 issues the copies (running ahead
-// across tile boundaries), warp 1 the MMAs (tcgen05.mma, two 32-byte K steps per product and
-// stage, then tcgen05.commit to free the stage; one more commit marks the tile's accumulators
+// across tile boundaries), warp 1 the MMAs (tcgen05.mma, one 32-byte K step per product and
+// stage for int8, two for BF16, then tcgen05.commit to free the stage; one more commit marks the
+// tile's accumulators
 // complete); each product (A piece, B piece) goes to its accumulator's 64 TMEM columns.  Eight
 // epilogue warps (2..9) drain a tile: warp w reads TMEM lanes 32 (w % 4) .. + 31 and one half of
 // the columns of every accumulator with one 32-column tcgen05.ld each, releases the TMEM to the
@@ -49,18 +51,24 @@ namespace {
 constexpr int kTcThreads = 320;
 constexpr int kEpiWarps = 8;
 constexpr int kTileM = 128, kTileN = 64;
-constexpr int kKBytes = 64;                         // bytes of K per tile row and stage
-constexpr uint32_t kBlockBytes = 64 * kKBytes;      // one pre-tiled 64-row block: 4 KB
-constexpr uint32_t kTileABytes = kTileM * kKBytes;  // 8 KB per piece (two adjacent blocks)
-constexpr uint32_t kTileBBytes = kTileN * kKBytes;  // 4 KB per piece
-constexpr uint32_t kSbo = 8 * 16 * (kKBytes / 16);  // 512: between 8-row groups of a block
+// Bytes of K per tile row and stage: 32 for the int8 slices (16 slices of a K tile take 48 KB,
+// four stages), 64 for the BF16 pieces (6 pieces, 36 KB, five stages).  A pre-tiled 64-row block
+// holds 64 x that many bytes, a 128-row A tile two adjacent blocks; consecutive 8-row groups
+// of a block are 8 x 16 x (K bytes / 16) bytes apart (the descriptor's stride offset).
+constexpr int kbytes_of(int kind) { return kind == 1 ? 32 : 64; }
+constexpr uint32_t block_bytes_of(int kind) { return 64u * (uint32_t)kbytes_of(kind); }
+constexpr uint32_t sbo_of(int kind) { return 8u * 16u * (uint32_t)(kbytes_of(kind) / 16); }
 constexpr int kMaxAcc = 8;                          // accumulators of 64 columns (512 TMEM columns)
 constexpr uint32_t kWaitLimit = 1u << 24;           // try_wait rounds before a wait gives up
 
 template <int kKind>
 struct TcShape {
   static constexpr int kPieces = kKind == 1 ? kOzakiSlices : 3;
-  static constexpr int kStages = kKind == 1 ? 2 : 5;
+  static constexpr int kStages = kKind == 1 ? 4 : 5;
+  static constexpr int kKBytes = kbytes_of(kKind);
+  static constexpr uint32_t kBlockBytes = block_bytes_of(kKind);
+  static constexpr uint32_t kTileABytes = kTileM * kKBytes, kTileBBytes = kTileN * kKBytes;
+  static constexpr uint32_t kSbo = sbo_of(kKind);
   static constexpr uint32_t kStageA = kPieces * kTileABytes, kStageB = kPieces * kTileBBytes;
   // ring, barriers (full and empty per stage, tmem_full, tmem_empty), TMEM slot + abort flag
   static constexpr size_t kSmem = 1024 + (size_t)kStages * (kStageA + kStageB) + 8 * (2 * kStages + 2) + 8;
@@ -246,14 +254,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
           if (*abort_flag) break;
           mbar_expect_tx(&full[s], Sh::kStageA + Sh::kStageB);
           // a 128-row A tile is the two adjacent 64-row blocks 2 tm, 2 tm + 1 of its K tile
-          const long long aoff = ((long long)kt * g.nrt_a + 2 * tm) * kBlockBytes;
-          const long long boff = ((long long)kt * g.nrt_b + tn) * kBlockBytes;
+          const long long aoff = ((long long)kt * g.nrt_a + 2 * tm) * Sh::kBlockBytes;
+          const long long boff = ((long long)kt * g.nrt_b + tn) * Sh::kBlockBytes;
 #pragma unroll
           for (int p = 0; p < kPieces; ++p)
-            bulk_g2s(sa + s * Sh::kStageA + p * kTileABytes, g.a + p * g.a_piece + aoff, kTileABytes, &full[s]);
+            bulk_g2s(sa + s * Sh::kStageA + p * Sh::kTileABytes, g.a + p * g.a_piece + aoff, Sh::kTileABytes,
+                     &full[s]);
 #pragma unroll
           for (int p = 0; p < kPieces; ++p)
-            bulk_g2s(sb + s * Sh::kStageB + p * kTileBBytes, g.b + p * g.b_piece + boff, kTileBBytes, &full[s]);
+            bulk_g2s(sb + s * Sh::kStageB + p * Sh::kTileBBytes, g.b + p * g.b_piece + boff, Sh::kTileBBytes,
+                     &full[s]);
           ++issued;
         }
       }
@@ -288,10 +298,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
           for (int p = 0; p < g.nprod; ++p) {
             const uint32_t dcol = tmem + (uint32_t)g.pacc[p] * kTileN;
             const bool first = kt == 0 && g.pfirst[p];
-            const uint32_t a0 = a_st + (uint32_t)g.pa[p] * kTileABytes, b0 = b_st + (uint32_t)g.pb[p] * kTileBBytes;
+            const uint32_t a0 = a_st + (uint32_t)g.pa[p] * Sh::kTileABytes;
+            const uint32_t b0 = b_st + (uint32_t)g.pb[p] * Sh::kTileBBytes;
 #pragma unroll
-            for (int k = 0; k < kKBytes / 32; ++k)
-              mma<kKind>(dcol, smem_desc(a0 + k * 256, 128, kSbo), smem_desc(b0 + k * 256, 128, kSbo),
+            for (int k = 0; k < Sh::kKBytes / 32; ++k)
+              mma<kKind>(dcol, smem_desc(a0 + k * 256, 128, Sh::kSbo), smem_desc(b0 + k * 256, 128, Sh::kSbo),
                          (first && k == 0) ? 0u : 1u);
           }
           mma_commit(&empty[s]);
@@ -366,15 +377,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
 
 // ---------------------------------------------------------------------------------------
 // Split kernels: FP64 factor F[k][row] (k < K, row < R; the K-major rows of the product) into
-// pieces in one pre-tiled layout shared by both operands: piece c holds, for each 64-byte K
-// tile kt and each 64-row block rt, 4 KB of core matrices [row group of 8][16-byte K chunk]
-// [8 rows][16 bytes] at ((c * nkt + kt) * nrt + rt) * 4 KB; rows are padded to a multiple of
-// 128 with zeros, so a 128-row A tile is two adjacent 64-row blocks.
+// pieces in one pre-tiled layout shared by both operands: piece c holds, for each K tile kt
+// (32 bytes for the int8 slices, 64 for the BF16 pieces) and each 64-row block rt, the block's
+// core matrices [row group of 8][16-byte K chunk][8 rows][16 bytes] at
+// ((c * nkt + kt) * nrt + rt) * block bytes; rows are padded to a multiple of 128 with zeros, so
+// a 128-row A tile is two adjacent 64-row blocks.
 // ---------------------------------------------------------------------------------------
+template <int kKind>
 __device__ __forceinline__ long long chunk_offset(int row, int kc, int nrt) {
-  constexpr int kChunks = kKBytes / 16;
+  constexpr int kChunks = kbytes_of(kKind) / 16;
   const int kt = kc / kChunks, c = kc % kChunks;
-  return ((long long)kt * nrt + (row >> 6)) * kBlockBytes + ((row & 63) >> 3) * kSbo + c * 128 + (row & 7) * 16;
+  return ((long long)kt * nrt + (row >> 6)) * block_bytes_of(kKind) + ((row & 63) >> 3) * sbo_of(kKind) + c * 128 +
+         (row & 7) * 16;
 }
 
 // Per-row exponents e with max_k |F[k][row]| * 2^-e <= 1/2 (0 for an all-zero or padding row).
@@ -397,7 +411,7 @@ __global__ void row_exponent_kernel(const double* __restrict__ f, int K, int R, 
 // a signed byte, |a_i| <= 64); one 16-byte store per slice.
 __global__ void int8_slices_kernel(const double* __restrict__ f, int K, int R, int rpad, int nkt,
                                    const int* __restrict__ e, int S, long long piece_bytes, uint8_t* __restrict__ out) {
-  const long long total = (long long)rpad * nkt * (kKBytes / 16);
+  const long long total = (long long)rpad * nkt * (kbytes_of(1) / 16);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const int row = (int)(t % rpad), kc = (int)(t / rpad);
@@ -408,7 +422,7 @@ __global__ void int8_slices_kernel(const double* __restrict__ f, int K, int R, i
       const int k = kc * 16 + j;
       x[j] = (row < R && k < K) ? ldexp(f[(long long)k * R + row], -ex) : 0.0;
     }
-    const long long off = chunk_offset(row, kc, rpad >> 6);
+    const long long off = chunk_offset<1>(row, kc, rpad >> 6);
     for (int c = 0; c < S; ++c) {
       uint32_t w[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
@@ -427,7 +441,7 @@ __global__ void int8_slices_kernel(const double* __restrict__ f, int K, int R, i
 // of one row) per thread.
 __global__ void bf16_pieces_kernel(const double* __restrict__ f, int K, int R, int rpad, int nkt,
                                    long long piece_bytes, uint8_t* __restrict__ out) {
-  const long long total = (long long)rpad * nkt * (kKBytes / 16);
+  const long long total = (long long)rpad * nkt * (kbytes_of(0) / 16);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const int row = (int)(t % rpad), kc = (int)(t / rpad);
@@ -437,7 +451,7 @@ __global__ void bf16_pieces_kernel(const double* __restrict__ f, int K, int R, i
       const int k = kc * 8 + j;
       x[j] = (row < R && k < K) ? f[(long long)k * R + row] : 0.0;
     }
-    const long long off = chunk_offset(row, kc, rpad >> 6);
+    const long long off = chunk_offset<0>(row, kc, rpad >> 6);
     for (int c = 0; c < 3; ++c) {
       uint32_t w[4];
 #pragma unroll
@@ -458,8 +472,9 @@ int pieces_of(int mode) { return mode == NW_TRANSFORM_CHOL_INT8 ? kOzakiSlices :
 
 size_t split_factor_bytes(int mode, int naux, int R) {
   const int kbytes = mode == NW_TRANSFORM_CHOL_INT8 ? naux : 2 * naux;
-  const int nkt = (kbytes + kKBytes - 1) / kKBytes, rpad = (R + kTileM - 1) / kTileM * kTileM;
-  return (size_t)pieces_of(mode) * nkt * (rpad / 64) * kBlockBytes + (size_t)rpad * sizeof(int) + 256;
+  const int kind = mode == NW_TRANSFORM_CHOL_INT8 ? 1 : 0, kb = kbytes_of(kind);
+  const int nkt = (kbytes + kb - 1) / kb, rpad = (R + kTileM - 1) / kTileM * kTileM;
+  return (size_t)pieces_of(mode) * nkt * (rpad / 64) * block_bytes_of(kind) + (size_t)rpad * sizeof(int) + 256;
 }
 
 cudaError_t split_factor(cudaStream_t st, int mode, const double* F, int naux, int R, void* buf, size_t bytes,
@@ -471,11 +486,12 @@ cudaError_t split_factor(cudaStream_t st, int mode, const double* F, int naux, i
   f.mode = mode;
   f.R = R;
   f.rpad = (R + kTileM - 1) / kTileM * kTileM;
-  f.nkt = (kbytes + kKBytes - 1) / kKBytes;
-  f.piece_bytes = (long long)f.nkt * (f.rpad / 64) * kBlockBytes;
+  const int kind = mode == NW_TRANSFORM_CHOL_INT8 ? 1 : 0, kb = kbytes_of(kind);
+  f.nkt = (kbytes + kb - 1) / kb;
+  f.piece_bytes = (long long)f.nkt * (f.rpad / 64) * block_bytes_of(kind);
   f.pieces = static_cast<uint8_t*>(buf);
   f.exps = reinterpret_cast<int*>(f.pieces + (size_t)pieces_of(mode) * f.piece_bytes);
-  const long long chunks = (long long)f.rpad * f.nkt * (kKBytes / 16);
+  const long long chunks = (long long)f.rpad * f.nkt * (kb / 16);
   const int blocks = (int)std::min<long long>((chunks + 255) / 256, 148 * 16);
   if (mode == NW_TRANSFORM_CHOL_INT8) {
     row_exponent_kernel<<<(f.rpad + 255) / 256, 256, 0, st>>>(F, naux, R, f.rpad, f.exps);
