@@ -109,6 +109,12 @@ def workload(name: str, npairs: int, rank: int, nmo: int = 64):
 PIPE_CHUNKS, PIPE_MIN_CHUNK = 16, 1 << 18  # chunking of the pinned-host entry (csrc/internal.cuh)
 # DRAM bytes (read + write) of one step's evaluator launches, from ncu captures of these workloads
 # (dram__bytes_read.sum + dram__bytes_write.sum; the summaries under profiles/ give the commands)
+# L1TEX throughput (fraction of peak) of the evaluators, the limiter of the L2-resident
+# workload, from the committed ncu capture of that workload
+EVAL_L1TEX = {
+    "config2": ({"eval_light_kernel": 0.757, "eval_medium_kernel": 0.743},
+                "profiles/eval_pipeline_config2_4Mpairs_ncu.md"),
+}
 EVAL_TRAFFIC = {
     ("config2", 10_000_000): (1_438_561_280, "profiles/eval_traffic_config2_10Mpairs.md"),
     ("config3", 100_000_000): (63_536_004_352, "profiles/eval_traffic_config3_100Mpairs.md"),
@@ -817,6 +823,8 @@ def hs_leg(args, name, npairs, rank, world, local_rank, dist):
                                       "(m > 0 pairs counted with the m = 0 bytes of their ranks: a lower bound)",
                      "eval_ms": ev_ms, "eval_gen_ms": class_ms["gen"], "phase_ms": phase_ms,
                      "class_ms_serial": class_ms,
+                     "l1tex_frac": EVAL_L1TEX.get(name, (None, None))[0],
+                     "l1tex_source": EVAL_L1TEX.get(name, (None, None))[1],
                      "dram_frac": (traffic / (ev_ms / 1e3) / 1e9 / peak) if traffic else None,
                      "note": "eval_ms: the class evaluators overlapped on forked streams (the timed step); "
                              "eval_gen_ms and class_ms_serial: each class kernel's own time with the classes "
