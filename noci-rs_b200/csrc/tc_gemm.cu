@@ -19,15 +19,13 @@
 // Kernel shape: persistent, one CTA of 320 threads per SM walking 128 x 64 tiles of T
 // (cta_group::1, M = 128, N = 64).
 // Operands are pre-tiled in global memory by the split kernels in the tcgen05 no-swizzle K-major
-// layout (8-row x 16-byte core matrices; 32-byte-deep K tiles for the int8 slices, 64-byte for
-// the BF16 pieces), so the K tile of one piece of an operand is one contiguous block moved by a
-// single cp.async.bulk (no multicast).  A pipeline stage holds the K tile of EVERY piece of both
-// operands (int8: 8 + 8 slices, 48 KB, four stages; BF16: 3 + 3 pieces, 36 KB, five stages), so
-// each slice is read from L2 once per tile and all
+// layout (8-row x 16-byte core matrices, 64-byte-deep K tiles), so the K tile of one piece of an
+// operand is one contiguous block moved by a single cp.async.bulk (no multicast).  A pipeline
+// stage holds the K tile of EVERY piece of both operands (int8: 8 + 8 slices, 96 KB, two stages;
+// BF16: 3 + 3 pieces, 36 KB, five stages), so each slice is read from L2 once per tile and all
 // products of that K tile run from shared memory.  Warp 0 issues the copies (running ahead
-// across tile boundaries), warp 1 the MMAs (tcgen05.mma, one 32-byte K step per product and
-// stage for int8, two for BF16, then tcgen05.commit to free the stage; one more commit marks the
-// tile's accumulators
+// across tile boundaries), warp 1 the MMAs (tcgen05.mma, two 32-byte K steps per product and
+// stage, then tcgen05.commit to free the stage; one more commit marks the tile's accumulators
 // complete); each product (A piece, B piece) goes to its accumulator's 64 TMEM columns.  Eight
 // epilogue warps (2..9) drain a tile: warp w reads TMEM lanes 32 (w % 4) .. + 31 and one half of
 // the columns of every accumulator with one 32-column tcgen05.ld each, releases the TMEM to the
@@ -51,11 +49,12 @@ namespace {
 constexpr int kTcThreads = 320;
 constexpr int kEpiWarps = 8;
 constexpr int kTileM = 128, kTileN = 64;
-// Bytes of K per tile row and stage: 32 for the int8 slices (16 slices of a K tile take 48 KB,
-// four stages), 64 for the BF16 pieces (6 pieces, 36 KB, five stages).  A pre-tiled 64-row block
+// Bytes of K per tile row and stage: 64 for both splits (int8: the 16 slices of a K tile take
+// 96 KB, two stages; BF16: 6 pieces, 36 KB, five stages; 32-byte int8 tiles in four stages
+// were measured slower, 336 against 279 us at n = 64, naux = 256).  A pre-tiled 64-row block
 // holds 64 x that many bytes, a 128-row A tile two adjacent blocks; consecutive 8-row groups
 // of a block are 8 x 16 x (K bytes / 16) bytes apart (the descriptor's stride offset).
-constexpr int kbytes_of(int kind) { return kind == 1 ? 32 : 64; }
+constexpr int kbytes_of(int kind) { return kind == 1 ? 64 : 64; }
 constexpr uint32_t block_bytes_of(int kind) { return 64u * (uint32_t)kbytes_of(kind); }
 constexpr uint32_t sbo_of(int kind) { return 8u * 16u * (uint32_t)(kbytes_of(kind) / 16); }
 constexpr int kMaxAcc = 8;                          // accumulators of 64 columns (512 TMEM columns)
@@ -64,7 +63,7 @@ constexpr uint32_t kWaitLimit = 1u << 24;           // try_wait rounds before a 
 template <int kKind>
 struct TcShape {
   static constexpr int kPieces = kKind == 1 ? kOzakiSlices : 3;
-  static constexpr int kStages = kKind == 1 ? 4 : 5;
+  static constexpr int kStages = kKind == 1 ? 2 : 5;
   static constexpr int kKBytes = kbytes_of(kKind);
   static constexpr uint32_t kBlockBytes = block_bytes_of(kKind);
   static constexpr uint32_t kTileABytes = kTileM * kKBytes, kTileBBytes = kTileN * kKBytes;
@@ -377,8 +376,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
 
 // ---------------------------------------------------------------------------------------
 // Split kernels: FP64 factor F[k][row] (k < K, row < R; the K-major rows of the product) into
-// pieces in one pre-tiled layout shared by both operands: piece c holds, for each K tile kt
-// (32 bytes for the int8 slices, 64 for the BF16 pieces) and each 64-row block rt, the block's
+// pieces in one pre-tiled layout shared by both operands: piece c holds, for each 64-byte K
+// tile kt and each 64-row block rt, the block's
 // core matrices [row group of 8][16-byte K chunk][8 rows][16 bytes] at
 // ((c * nkt + kt) * nrt + rt) * block bytes; rows are padded to a multiple of 128 with zeros, so
 // a 128-row A tile is two adjacent 64-row blocks.
