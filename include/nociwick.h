@@ -253,6 +253,21 @@ NW_API nw_status nw_eval_s_pairs_device(nw_ctx* ctx, const uint32_t* pairs_dev, 
 NW_API nw_status nw_eval_s_pairs(nw_ctx* ctx, const uint32_t* pairs_host, uint64_t npairs, double* s_host,
                                  void* stream);
 
+/* Overlap action over the resident basis: y_dev[w] += sum_x S_wx x_dev[x] for every determinant
+ * w (device buffers of ndet doubles; y_dev must not alias x_dev).  S_wx is the same overlap as
+ * nw_eval_s_pairs*, computed from single-spin factors: the determinants of one parent share their
+ * alpha and beta strings, S_wx = A[a_w][a_x] B[b_w][b_x] for parents Q != P with A, B the
+ * single-spin overlaps det(C_Q[:,occ]^T S C_P[:,occ]) of the two parents' strings, and the
+ * determinants of one parent are orthonormal.  The first call on a basis builds the factor tables
+ * (allocates about 8 (na_Q na_P + nb_Q nb_P) bytes per ordered pair of parents with na / nb
+ * distinct alpha / beta strings per parent, and synchronises the stream; call it once before any
+ * stream capture); later calls only launch kernels.  At most 16 occupied orbitals per spin.
+ * Needs the resident basis (nw_set_basis), not the built intermediates.
+ * Replaces SpinFactorisation::apply_overlap_sparse with build_overlap_factors
+ * (src/noci/factorise/overlap.rs:280-498), as applied by apply_overlap_population_changes
+ * (src/stochastic/metric.rs:97-232). */
+NW_API nw_status nw_apply_overlap_device(nw_ctx* ctx, const double* x_dev, double* y_dev, void* stream);
+
 /* (H, S) for npairs requests of one ordered reference pair (bra reference lp, ket reference gp)
  * from caller-held excitation caches: request i is the bra x[i] (a determinant of reference lp)
  * against the ket w[i] (of reference gp), with phase[i] the product of both determinants'
@@ -339,7 +354,9 @@ NW_API nw_status nw_general_evp(nw_ctx* ctx, int32_t n, const double* h, const d
  * Replaces qmc_step for the signed-walker propagators (src/stochastic/walkers.rs:101-441) with
  * propagate_iteration (src/stochastic/metric.rs:378-473), spawning / resolve_batched_spawning
  * with the uniform generator (src/stochastic/state.rs:537-726), sample_populations / fri
- * (metric.rs:579-699) and update_shift (metric.rs:729-751).  Random numbers come from a
+ * (metric.rs:579-699) and update_shift (metric.rs:729-751), and qmc_step of the direct-overlap
+ * propagator (metric.rs:766-1087: the same cycles, then N += S Phi(Delta) per report through the
+ * overlap action of nw_apply_overlap_device, inside the graph).  Random numbers come from a
  * counter-based Philox4x32-10 stream per (seed, cycle, index), so runs are reproducible for a
  * given seed but are not the reference's SmallRng sequence.
  * --------------------------------------------------------------------------------------- */
@@ -348,7 +365,10 @@ typedef enum nw_propagator {
     NW_PROP_SHIFTED = 1,         /* U = (1 + dt E_s) - dt (H - E_s S)           */
     NW_PROP_DOUBLY_SHIFTED = 2,  /* as SHIFTED with E_s = E_s^S (the default)   */
     NW_PROP_DDS_U1 = 3,          /* difference doubly shifted, variant 1        */
-    NW_PROP_DDS_U2 = 4           /* difference doubly shifted, variant 2        */
+    NW_PROP_DDS_U2 = 4,          /* difference doubly shifted, variant 2        */
+    NW_PROP_DIRECT_OVERLAP = 5   /* real metric population N (N_0 = S c_0 scaled), cycles as
+                                    UNSHIFTED, each report's change applied as N += S Phi(Delta)
+                                    (qmc_step of src/stochastic/metric.rs:766-1087)            */
 } nw_propagator;
 
 typedef struct nw_qmc_opts {
@@ -364,6 +384,9 @@ typedef struct nw_qmc_opts {
     uint64_t seed;
     uint64_t max_attempts;      /* spawning attempts one cycle can hold (0: 16 x the larger of
                                    the target and initial populations + 2 ndet + 2^20)        */
+    double update_cutoff;       /* NW_PROP_DIRECT_OVERLAP: FRI cutoff of a report's accumulated
+                                   change before the overlap is applied (sampling_cutoff2 of
+                                   noci-rs; 0: none); ignored by the other propagators        */
 } nw_qmc_opts;
 
 typedef struct nw_qmc_report {

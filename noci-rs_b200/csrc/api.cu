@@ -389,6 +389,8 @@ nw_status nw_set_basis(nw_ctx* ctx, const nw_det* basis, uint64_t ndet) {
     }
   }
   NW_CUDA(ctx, cudaSetDevice(ctx->device));
+  nw::overlap_plan_free(ctx->ovl);
+  ctx->ovl = nullptr;
   if (ctx->d_dets) cudaFree(ctx->d_dets);
   if (ctx->d_desc) cudaFree(ctx->d_desc);
   ctx->d_dets = nullptr;
@@ -567,6 +569,7 @@ nw_status nw_ctx_destroy(nw_ctx* ctx) {
   if (ctx->d_order) cudaFree(ctx->d_order);
   if (ctx->d_dets) cudaFree(ctx->d_dets);
   if (ctx->d_desc) cudaFree(ctx->d_desc);
+  nw::overlap_plan_free(ctx->ovl);
   for (double* b : {ctx->d_fbase, ctx->d_fock, ctx->d_fslab})
     if (b) cudaFree(b);
   if (ctx->d_fockp) cudaFree(ctx->d_fockp);

@@ -45,6 +45,9 @@ struct DevBuf {
   size_t bytes = 0;
 };
 
+// Spin-factorised overlap action over the resident basis (overlap.cu).
+struct OverlapPlan;
+
 }  // namespace nw
 
 struct nw_ctx {
@@ -84,6 +87,7 @@ struct nw_ctx {
   nw_det* d_dets = nullptr;
   uint16_t* d_desc = nullptr;      // det_desc of every record
   uint64_t ndet = 0;
+  nw::OverlapPlan* ovl = nullptr;  // factor tables of the overlap action, built on first use
 
   // evaluation scratch (grown on demand)
   nw::DevBuf keys, perm, counts, offsets, flag, ranks, tsum;
@@ -263,6 +267,13 @@ nw_status launch_sorted(nw_ctx* ctx, const EvalParams& P, uint64_t nkeys, const 
 // Exclusive scan of n counters into offsets[0..n] (offsets[n] = total); tsum holds n / 4096 + 1.
 nw_status scan_exclusive(nw_ctx* ctx, const uint32_t* counts, uint64_t n, uint32_t* offsets, uint32_t* tsum,
                          cudaStream_t stream);
+
+// Overlap action y += S x over the resident basis (overlap.cu): the plan (spin components,
+// factor tables, work buffers) is built on first use, allocates and synchronises `stream`, and
+// stays with the context until the basis changes; an apply only launches kernels.
+nw_status overlap_plan_get(nw_ctx* ctx, cudaStream_t stream, OverlapPlan** out);
+nw_status overlap_apply(nw_ctx* ctx, const OverlapPlan* plan, const double* x, double* y, cudaStream_t stream);
+void overlap_plan_free(OverlapPlan* plan);
 
 // Same evaluation with its scratch in a fixed device array (no device allocation).
 nw_status eval_pairs_noalloc(nw_ctx* ctx, const uint32_t* pairs, uint64_t npairs, double* out, cudaStream_t stream);

@@ -14,6 +14,10 @@
 // After ncycles: qmc_block_kernel adds delta to the populations (annihilation happens in the
 // dense accumulation) and reduces the statistics per block; qmc_finalize_kernel sums them in a
 // fixed order, updates the shift (update_shift, metric.rs:729-751) and writes the report.
+// The direct-overlap propagator (qmc_step, metric.rs:766-1087) keeps the real metric population
+// N instead: its report FRI-compresses delta with the update cutoff (fri_population_updates,
+// metric.rs:701-718), adds S delta through the overlap action (overlap.cu), and only then reduces
+// the statistics; its populations start from S c_0 (initialise_populations, init.rs:32-83).
 // Every per-run quantity (shift, cycle counter, attempt count) lives in device memory, so a
 // report block is captured once as a CUDA graph and replayed.
 #include <cuda_runtime.h>
@@ -71,6 +75,7 @@ struct QmcParams {
   uint32_t pad;
   uint64_t hcap;    // harvest buffer capacity
   double hkeep;     // probability of recording an attempt while harvesting
+  double c_update;  // direct overlap: FRI cutoff of a report's accumulated change
 };
 
 // One harvested attempt: parent, the child's bin and the weight |H - E^S S| / ((N - 1) pgen),
@@ -301,6 +306,15 @@ __global__ void qmc_apply_kernel(QmcParams q, Proposal pr, const QmcState* __res
 
 __global__ void qmc_next_cycle_kernel(QmcState* __restrict__ st) { st->cycle += 1; }
 
+// Direct overlap: Phi_c(delta) of the report's accumulated change, one stream per (seed, report).
+__global__ void qmc_update_fri_kernel(QmcParams q, const QmcState* __restrict__ st, double* __restrict__ delta) {
+  const uint64_t report = st->report;
+  for (uint64_t d = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; d < q.ndet; d += (uint64_t)gridDim.x * blockDim.x) {
+    const double x = delta[d];
+    if (x != 0.0) delta[d] = nwq::fri(x, q.c_update, nwq::uniform1(q.seed, report, d, nwq::kDrawUpdate));
+  }
+}
+
 // N += delta, delta = 0; per-block partial statistics in a fixed order.
 __global__ void __launch_bounds__(kBlockThreads) qmc_block_kernel(QmcParams q, double* __restrict__ pop,
                                                                   double* __restrict__ delta,
@@ -504,6 +518,7 @@ struct nw_qmc {
   double2* hs = nullptr;
   double* partial = nullptr;
   nw_qmc_report* ring = nullptr;
+  nw::OverlapPlan* ovl = nullptr;  // direct overlap: the context's overlap action
   // sort scratch for the attempts
   nw::EvalParams P{};
   uint64_t nkeys = 0;
@@ -559,8 +574,17 @@ nw_status enqueue_block(nw_qmc* q) {
     const nw_status st = enqueue_cycle(q);
     if (st != NW_OK) return st;
   }
+  int apply = 1;
+  if (q->q.prop == nwq::kDirectOverlap) {
+    // N += S Phi_c(delta), delta = 0
+    if (q->q.c_update > 0.0) qmc_update_fri_kernel<<<grid_for(q->q.ndet), kBlockThreads, 0, q->stream>>>(q->q, q->st, q->delta);
+    const nw_status st = nw::overlap_apply(q->ctx, q->ovl, q->delta, q->pop, q->stream);
+    if (st != NW_OK) return st;
+    NW_CUDA(q->ctx, cudaMemsetAsync(q->delta, 0, sizeof(double) * q->q.ndet, q->stream));
+    apply = 0;
+  }
   qmc_block_kernel<<<kStatBlocks, kBlockThreads, 0, q->stream>>>(q->q, q->pop, q->delta, q->sampled, q->refhs, q->isref,
-                                                                 1, q->partial);
+                                                                 apply, q->partial);
   qmc_finalize_kernel<<<1, 32, 0, q->stream>>>(q->q, q->st, q->partial, kStatBlocks, q->ring, 1);
   NW_CUDA(q->ctx, cudaGetLastError());
   return NW_OK;
@@ -766,8 +790,9 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
   if (ctx->partial)
     return nw::fail(ctx, NW_ERR_STATE, "the intermediates hold one block of a blocked evaluation (rebuild them)");
   if (!ctx->d_dets || ctx->ndet < 2) return nw::fail(ctx, NW_ERR_STATE, "QMC needs a resident basis of >= 2 determinants");
-  if (!(opts->dt > 0.0) || opts->ncycles < 1 || opts->propagator < 0 || opts->propagator > 4 ||
+  if (!(opts->dt > 0.0) || opts->ncycles < 1 || opts->propagator < 0 || opts->propagator > 5 ||
       !(opts->initial_population > 0.0) || !(opts->sampling_cutoff >= 0.0) || !(opts->spawn_cutoff >= 0.0) ||
+      !(opts->update_cutoff >= 0.0) || !std::isfinite(opts->update_cutoff) ||
       !std::isfinite(opts->initial_shift) || !std::isfinite(opts->shift_damping))
     return nw::fail(ctx, NW_ERR_INVALID, "invalid QMC options");
   const uint64_t nd = ctx->ndet;
@@ -808,7 +833,8 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
                    (uint32_t)ctx->nref * kRankBins,
                    0,
                    kHarvestCap,
-                   1.0};
+                   1.0,
+                   opts->update_cutoff};
   bool ok = true;
   auto take = [&](auto*& p, size_t count) {
     using T = std::remove_reference_t<decltype(*p)>;
@@ -927,9 +953,31 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
       qmc_axpy2_kernel<<<grid_for(nd), kBlockThreads, 0, q->stream>>>(nd, c0[i], q->hs, q->refhs);
     }
     if (st != NW_OK) break;
-    std::vector<double> pop(nd);
-    const double scale = opts->initial_population / norm;
-    for (uint64_t i = 0; i < nd; ++i) pop[i] = scale * c0[i];
+    std::vector<double> pop(c0, c0 + nd);
+    double pnorm = norm;
+    if (opts->propagator == nwq::kDirectOverlap) {
+      // N_0 = S c_0 through the overlap action (delta as the source, pop as the target)
+      if ((st = nw::overlap_plan_get(ctx, q->stream, &q->ovl)) != NW_OK) break;
+      if (cudaMemcpyAsync(q->delta, c0, sizeof(double) * nd, cudaMemcpyHostToDevice, q->stream) != cudaSuccess ||
+          cudaMemsetAsync(q->pop, 0, sizeof(double) * nd, q->stream) != cudaSuccess) {
+        st = nw::fail(ctx, NW_ERR_CUDA, "QMC initialisation copies failed");
+        break;
+      }
+      if ((st = nw::overlap_apply(ctx, q->ovl, q->delta, q->pop, q->stream)) != NW_OK) break;
+      if (cudaMemcpyAsync(pop.data(), q->pop, sizeof(double) * nd, cudaMemcpyDeviceToHost, q->stream) != cudaSuccess ||
+          cudaStreamSynchronize(q->stream) != cudaSuccess) {
+        st = nw::fail(ctx, NW_ERR_CUDA, "QMC initialisation copies failed");
+        break;
+      }
+      pnorm = 0.0;
+      for (uint64_t i = 0; i < nd; ++i) pnorm += std::fabs(pop[i]);
+      if (!(pnorm > 0.0) || !std::isfinite(pnorm)) {
+        st = nw::fail(ctx, NW_ERR_INVALID, "S c0 is zero or not finite");
+        break;
+      }
+    }
+    const double scale = opts->initial_population / pnorm;
+    for (uint64_t i = 0; i < nd; ++i) pop[i] *= scale;
     QmcState hst{};
     hst.shift = opts->initial_shift;
     if (cudaMemcpyAsync(q->isref, isref.data(), nd, cudaMemcpyHostToDevice, q->stream) != cudaSuccess ||

@@ -57,6 +57,7 @@ constexpr uint32_t kDrawSpawn = 3;   // FRI rounding of a spawned amplitude
 constexpr uint32_t kDrawChildBin = 4;  // bin and member of a learned-proposal attempt
 constexpr uint32_t kDrawTrain = 5;   // minibatch draws of the proposal training
 constexpr uint32_t kDrawHarvest = 6;  // thinning of the harvested attempts
+constexpr uint32_t kDrawUpdate = 7;   // FRI of a report's accumulated change (direct overlap)
 
 // Two uniform doubles in [0, 1) with 53 random bits each, for (seed, cycle, index, purpose).
 NWQ_HD void uniform2(uint64_t seed, uint64_t cycle, uint64_t index, uint32_t purpose, double* u0, double* u1) {
@@ -96,8 +97,9 @@ NWQ_HD uint64_t uniform_child(uint64_t gamma, uint64_t ndet, double u) {
   return l;
 }
 
-// Shifts of the signed-walker propagators (ShiftSpec, state.rs:80-162) with E_s = E_s^S = es.
-enum Propagator : int32_t { kUnshifted = 0, kShifted = 1, kDoublyShifted = 2, kDdsU1 = 3, kDdsU2 = 4 };
+// Shifts of the signed-walker propagators (ShiftSpec, state.rs:80-162) with E_s = E_s^S = es;
+// the direct-overlap propagator shifts only the overlap (ShiftSpec::direct_overlap, state.rs:95-101).
+enum Propagator : int32_t { kUnshifted = 0, kShifted = 1, kDoublyShifted = 2, kDdsU1 = 3, kDdsU2 = 4, kDirectOverlap = 5 };
 
 NWQ_HD double overlap_shift(int prop, double es) {
   (void)prop;

@@ -77,7 +77,7 @@ class NwQmcOpts(ctypes.Structure):
                 ("target_population", ctypes.c_double), ("sampling_cutoff", ctypes.c_double),
                 ("spawn_cutoff", ctypes.c_double), ("shift_damping", ctypes.c_double),
                 ("initial_shift", ctypes.c_double), ("ncycles", ctypes.c_int32), ("propagator", ctypes.c_int32),
-                ("seed", ctypes.c_uint64), ("max_attempts", ctypes.c_uint64)]
+                ("seed", ctypes.c_uint64), ("max_attempts", ctypes.c_uint64), ("update_cutoff", ctypes.c_double)]
 
 
 class NwQmcReport(ctypes.Structure):
@@ -87,7 +87,7 @@ class NwQmcReport(ctypes.Structure):
 
 
 PROPAGATORS = {"unshifted": 0, "shifted": 1, "doubly-shifted": 2, "difference-doubly-shifted-u1": 3,
-               "difference-doubly-shifted-u2": 4}
+               "difference-doubly-shifted-u2": 4, "direct-overlap": 5}
 
 
 class NwMlpOpts(ctypes.Structure):
@@ -128,7 +128,8 @@ EXPORTED = ("nw_ctx_create", "nw_ctx_create_cholesky", "nw_build_intermediates",
             "nw_load_intermediates", "nw_eval_hs_pairs_blocked", "nw_pair_zero_counts",
             "nw_set_basis", "nw_eval_hs_pairs_device", "nw_eval_hs_pairs", "nw_eval_hs_pairs_noalloc",
             "nw_eval_hs_batched", "nw_eval_hs_batched_device", "nw_eval_s_batched", "nw_eval_s_batched_device",
-            "nw_eval_fs_batched", "nw_eval_fs_batched_device", "nw_eval_s_pairs_device", "nw_eval_s_pairs", "nw_update_fock", "nw_eval_fs_pairs_device", "nw_eval_fs_pairs",
+            "nw_eval_fs_batched", "nw_eval_fs_batched_device", "nw_eval_s_pairs_device", "nw_eval_s_pairs",
+            "nw_apply_overlap_device", "nw_update_fock", "nw_eval_fs_pairs_device", "nw_eval_fs_pairs",
             "nw_build_hs_matrix", "nw_build_fs_matrix", "nw_general_evp",
             "nw_qmc_create", "nw_qmc_run", "nw_qmc_set_shift", "nw_qmc_last_run_ms", "nw_qmc_populations", "nw_qmc_set_populations", "nw_qmc_cycle_delta",
             "nw_qmc_destroy", "nw_qmc_harvest", "nw_qmc_train_proposal", "nw_qmc_set_generator",
@@ -165,6 +166,7 @@ def load(path: Optional[str] = None):
     for name in ("nw_eval_s_batched", "nw_eval_s_batched_device", "nw_eval_fs_batched", "nw_eval_fs_batched_device"):
         getattr(L, name).argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_uint64, vp, vp]
     L.nw_eval_s_pairs.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
+    L.nw_apply_overlap_device.argtypes = [vp, vp, vp, vp]
     L.nw_pair_zero_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
     L.nw_set_basis.argtypes = [vp, vp, ctypes.c_uint64]
     L.nw_eval_hs_pairs_device.argtypes = [vp, vp, ctypes.c_uint64, vp, vp]
@@ -402,6 +404,12 @@ class WicksShared:
                                                        ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream)),
                     "nw_eval_hs_pairs_noalloc")
 
+    def apply_overlap_device(self, x_ptr: int, y_ptr: int, stream: int = 0):
+        """y += S x over the resident basis (device buffers of ndet doubles; nw_apply_overlap_device).
+        The first call on a basis builds the spin-factor tables."""
+        self._check(self._lib.nw_apply_overlap_device(self._ctx, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
+                                                      ctypes.c_void_p(stream)), "nw_apply_overlap_device")
+
     def eval_overlap_device(self, pairs_ptr: int, npairs: int, out_ptr: int, stream: int = 0):
         self._check(self._lib.nw_eval_s_pairs_device(self._ctx, ctypes.c_void_p(pairs_ptr), npairs,
                                                      ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream)),
@@ -499,23 +507,25 @@ class WicksShared:
 
 
 class Qmc:
-    """NOCI-QMC with signed real walkers on the GPU (qmc_step of src/stochastic/walkers.rs with
-    the uniform generator).  ``c0`` has one coefficient per determinant of the resident basis;
-    ``ref_idx`` are the reference determinants used for the projected energy."""
+    """NOCI-QMC on the GPU: signed real walkers (qmc_step of src/stochastic/walkers.rs), or with
+    propagator="direct-overlap" the real metric population of qmc_step in src/stochastic/metric.rs
+    (N_0 = S c_0, each report's change applied through the overlap, FRI-compressed with
+    ``update_cutoff``), with the uniform generator.  ``c0`` has one coefficient per determinant of
+    the resident basis; ``ref_idx`` are the reference determinants used for the projected energy."""
 
     REPORT_FIELDS = ("shift", "eproj_num", "eproj_den", "nw", "nref", "sampled_norm", "nocc", "nattempts")
 
     def __init__(self, wicks: "WicksShared", c0, ref_idx, dt: float, initial_population: float = 100.0,
                  target_population: float = 1e5, sampling_cutoff: float = 0.0, spawn_cutoff: float = 0.0,
                  shift_damping: float = 5e-4, initial_shift: float = 0.0, ncycles: int = 10,
-                 propagator: str = "unshifted", seed: int = 1, max_attempts: int = 0):
+                 propagator: str = "unshifted", seed: int = 1, max_attempts: int = 0, update_cutoff: float = 0.0):
         self._w = wicks
         self._lib = wicks._lib
         c0 = np.ascontiguousarray(c0, dtype=np.float64)
         ref = np.ascontiguousarray(ref_idx, dtype=np.uint32)
         o = NwQmcOpts(dt, initial_population, target_population, sampling_cutoff, spawn_cutoff, shift_damping,
                       initial_shift, ncycles, PROPAGATORS[propagator] if isinstance(propagator, str) else propagator,
-                      seed, max_attempts)
+                      seed, max_attempts, update_cutoff)
         self._q = ctypes.c_void_p()
         self.ndet = c0.shape[0]
         wicks._check(self._lib.nw_qmc_create(wicks._ctx, ctypes.byref(o), c0.ctypes.data, ref.ctypes.data,

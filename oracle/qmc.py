@@ -9,13 +9,18 @@ change (state.rs:653-667), ceil|n| uniform spawning attempts per occupied determ
 the spawned amplitude with the spawn cutoff; after ncycles the accumulated change is added to
 the populations and the shift is updated (update_shift, metric.rs:729-751).  The random numbers
 are numpy's (the reference's SmallRng stream is not reproduced); comparisons are statistical.
+
+The direct-overlap propagator (qmc_step of src/stochastic/metric.rs:766-1087) runs the same cycles
+with no identity shift, starts from N_0 = S c_0 scaled to the initial 1-norm (init.rs:32-83) and
+applies each report's accumulated change through the overlap, N += S Phi_c(Delta), with the update
+cutoff c of fri_population_updates (metric.rs:701-718, :1030) -- so N stays in the range of S.
 """
 from __future__ import annotations
 
 import numpy as np
 
 PROPAGATORS = {"unshifted": 0, "shifted": 1, "doubly-shifted": 2, "difference-doubly-shifted-u1": 3,
-               "difference-doubly-shifted-u2": 4}
+               "difference-doubly-shifted-u2": 4, "direct-overlap": 5}
 
 
 def fri(x: np.ndarray, c: float, u: np.ndarray) -> np.ndarray:
@@ -32,7 +37,7 @@ def fri(x: np.ndarray, c: float, u: np.ndarray) -> np.ndarray:
 class OracleQmc:
     def __init__(self, orc, obasis, c0, ref_idx, dt, initial_population=100.0, target_population=1e5,
                  sampling_cutoff=0.0, spawn_cutoff=0.0, shift_damping=5e-4, initial_shift=0.0, ncycles=10,
-                 propagator="unshifted", seed=1, nthreads=0):
+                 propagator="unshifted", seed=1, nthreads=0, update_cutoff=0.0, overlap=None):
         self.orc, self.ob = orc, obasis
         self.n = obasis.shape[0]
         self.dt, self.target = dt, target_population
@@ -53,6 +58,11 @@ class OracleQmc:
                 hi, si = orc.eval_pairs(obasis, np.stack([np.full(self.n, i), g], 1), nthreads=nthreads)
                 self.refhs += c0[i] * np.stack([hi, si], 1)
         c0 = np.asarray(c0, float)
+        self.c_update, self.overlap = update_cutoff, overlap
+        if self.prop == 5:
+            if overlap is None:
+                raise ValueError("the direct-overlap propagator needs the overlap action S x")
+            c0 = overlap(c0)
         self.pop = initial_population / np.abs(c0).sum() * c0
         self.nw_prev = np.abs(self.pop).sum()
         self.reached = False
@@ -87,7 +97,10 @@ class OracleQmc:
         delta = np.zeros(self.n)
         for _ in range(self.ncycles):
             delta += self.cycle_delta()
-        self.pop += delta
+        if self.prop == 5:
+            self.pop += self.overlap(fri(delta, self.c_update, self.rng.random(self.n)))
+        else:
+            self.pop += delta
         a = np.abs(self.pop)
         nw = a.sum()
         if not self.reached and nw >= self.target:

@@ -352,15 +352,22 @@ FIXTURES = {
                             {"max_iter": 2, "max_add": 1, **GMRES_512}),
     "QMC_LiH_STO-3G_2_8_TRAJECTORY_DDS2": ("STO-3G", chain(2.8, (-0.5, 0.5), ["Li", "H"]), LIH_STATES, (1, 2), None),
     "QMC_LiH_6-31G_2_8_TRAJECTORY_DDS2": ("6-31G", chain(2.8, (-0.5, 0.5), ["Li", "H"]), LIH_STATES, (1, 2), None),
+    "QMC_LiH_STO-3G_2_8_TRAJECTORY_DIRECT_OVERLAP": ("STO-3G", chain(2.8, (-0.5, 0.5), ["Li", "H"]), LIH_STATES,
+                                                     (1, 2), None),
+    "QMC_LiH_6-31G_2_8_TRAJECTORY_DIRECT_OVERLAP": ("6-31G", chain(2.8, (-0.5, 0.5), ["Li", "H"]), LIH_STATES,
+                                                    (1, 2), None),
 }
 
 # qmc / prop blocks of the QMC trajectory fixtures' inputs (their expected.json stores only
 # trajectory bounds: an energy window, a minimum number of report energies, span and drop)
 QMC_OPTIONS = {
-    name: {"dt": 1e-2, "propagator": "difference-doubly-shifted-u2", "initial_population": 200,
+    name: {"dt": dt, "propagator": prop, "initial_population": 200,
            "target_population": 500, "ncycles": 1, "nreports": 80, "sampling_cutoff": 1.0, "spawn_cutoff": 0.25,
            "excitation_gen": "uniform", "seed": 1}
-    for name in ("QMC_LiH_STO-3G_2_8_TRAJECTORY_DDS2", "QMC_LiH_6-31G_2_8_TRAJECTORY_DDS2")
+    for name, prop, dt in (("QMC_LiH_STO-3G_2_8_TRAJECTORY_DDS2", "difference-doubly-shifted-u2", 1e-2),
+                           ("QMC_LiH_6-31G_2_8_TRAJECTORY_DDS2", "difference-doubly-shifted-u2", 1e-3),
+                           ("QMC_LiH_STO-3G_2_8_TRAJECTORY_DIRECT_OVERLAP", "direct-overlap", 1e-2),
+                           ("QMC_LiH_6-31G_2_8_TRAJECTORY_DIRECT_OVERLAP", "direct-overlap", 1e-3))
 }
 
 

@@ -57,11 +57,11 @@ def test_pt2_and_snoci_energies(name):
         assert abs(res.energy - expected["snoci_energy"]) < 1e-8, (res.energy, expected)
 
 
-@pytest.mark.parametrize("name", [n for n in NAMES if n.startswith("QMC_") and "TRAJECTORY_DDS2" in n])
+@pytest.mark.parametrize("name", [n for n in NAMES if n.startswith("QMC_") and "_TRAJECTORY_" in n])
 def test_qmc_trajectory_bounds(name):
-    """The reference's DDS-u2 trajectory fixtures (tests/qmc.rs:195-243, 499-545): a short
-    NOCI-QMC run with the fixture's qmc / prop blocks (uniform generator, 80 one-cycle reports
-    from 200 walkers towards 500) must give at least min_samples projected energies, all finite
+    """The reference's DDS-u2 and direct-overlap trajectory fixtures (tests/qmc.rs:195-243,
+    487-545): a short NOCI-QMC run with the fixture's qmc / prop blocks (uniform generator, 80
+    one-cycle reports from 200 walkers towards 500) must give at least min_samples projected energies, all finite
     and inside [min_energy, max_energy], spanning at least min_energy_span and ending at least
     min_final_drop below the first.  The engine's random stream is Philox, not the reference's
     SmallRng, so its trajectory for seed 1 is a different sample of the same process; with a few

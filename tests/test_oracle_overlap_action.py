@@ -1,0 +1,82 @@
+"""CPU checks of the oracle's spin-factorised overlap action (oracle/overlap_action.py) and of the
+direct-overlap report of the QMC oracle (oracle/qmc.py), the checkers of the GPU overlap action
+and of the direct-overlap propagator.
+
+* The factorised S (single-spin determinants of the two parents' strings, identity inside a
+  parent, r = record phase x canonical phase) equals the oracle's Wick overlap of every pair,
+  with and without zero-overlap reference pairs, with a duplicated determinant and with a
+  non-canonical record phase; the B-first contraction equals the dense product.
+* Direct overlap: the populations start at S c_0 scaled to the initial 1-norm, and a report adds
+  S times the report's accumulated change (here a fixed change) instead of the change itself.
+"""
+import numpy as np
+import pytest
+
+from nociwick import synthetic as sy
+from oracle.oracle import Oracle
+from oracle.overlap_action import OverlapFactorisation, canonical_phase, spin_key
+from oracle.qmc import OracleQmc
+
+
+def _all_pairs_overlap(system, basis):
+    orc = Oracle.from_system(system, tol=1e-8)
+    ob = orc.oracle_basis(basis)
+    g = np.arange(basis.shape[0])
+    pairs = np.stack(np.meshgrid(g, g, indexing="ij"), -1).reshape(-1, 2)
+    _, s = orc.eval_pairs(ob, pairs)
+    return s.reshape(basis.shape[0], basis.shape[0]), orc, ob
+
+
+@pytest.mark.parametrize("zero_pairs", [(), ((0, 1, 1, 0), (1, 2, 0, 2))])
+def test_factorised_overlap_equals_wick_overlap(zero_pairs):
+    system = sy.make_system(8, 2, 2, 3, 12, seed=7, k_scale=0.3, zero_pairs=list(zero_pairs), enuc=0.5)
+    basis = sy.sd_basis(8, 2, 2, 3)
+    s, _, _ = _all_pairs_overlap(system, basis)
+    f = OverlapFactorisation(system.s, system.refs, 2, 2, basis)
+    assert np.abs(f.r - 1.0).max() == 0.0       # sd_basis records carry the canonical phases
+    assert np.abs(f.dense() - s).max() < 1e-14
+    x = np.random.default_rng(1).standard_normal(basis.shape[0])
+    assert np.abs(f.apply(x) - s @ x).max() < 1e-13 * np.abs(x).sum()
+
+
+def test_factorised_overlap_duplicates_and_phases():
+    system = sy.make_system(8, 2, 2, 2, 12, seed=3, k_scale=0.3)
+    basis = sy.sd_basis(8, 2, 2, 2)
+    basis = np.concatenate([basis, basis[[4, 120]]])
+    basis["phase"][9] *= -1.0
+    s, _, _ = _all_pairs_overlap(system, basis)
+    f = OverlapFactorisation(system.s, system.refs, 2, 2, basis)
+    assert f.r[9] == -1.0
+    assert abs(s[4, basis.shape[0] - 2] - 1.0) < 1e-15
+    assert np.abs(f.dense() - s).max() < 1e-14
+    x = np.random.default_rng(4).standard_normal(basis.shape[0])
+    assert np.abs(f.apply(x) - s @ x).max() < 1e-13 * np.abs(x).sum()
+
+
+def test_canonical_phase_is_the_basis_phase():
+    basis = sy.sd_basis(9, 3, 2, 1, orders=(1, 2, 3, 4))
+    for d in basis[:: max(1, basis.shape[0] // 400)]:
+        ph = canonical_phase(3, spin_key(d["rank_a"], d["idx_a"])) * canonical_phase(2, spin_key(d["rank_b"], d["idx_b"]))
+        assert ph == d["phase"]
+
+
+def test_direct_overlap_report_applies_the_overlap():
+    system = sy.make_system(8, 2, 2, 2, 12, seed=5, k_scale=0.3)
+    basis = sy.sd_basis(8, 2, 2, 2)
+    s, orc, ob = _all_pairs_overlap(system, basis)
+    f = OverlapFactorisation(system.s, system.refs, 2, 2, basis)
+    refs = np.nonzero((basis["rank_a"] == 0) & (basis["rank_b"] == 0))[0]
+    c0 = np.zeros(basis.shape[0])
+    c0[refs] = [0.7, -0.4]
+    q = OracleQmc(orc, ob, c0, refs, dt=0.01, initial_population=200.0, ncycles=1, propagator="direct-overlap",
+                  overlap=f.apply, seed=3)
+    sc0 = s @ c0
+    assert np.abs(q.pop - 200.0 * sc0 / np.abs(sc0).sum()).max() < 1e-12
+    fixed = np.random.default_rng(8).standard_normal(basis.shape[0])
+    q.cycle_delta = lambda: fixed
+    before = q.pop.copy()
+    rep = q.report()
+    assert np.abs((q.pop - before) - s @ fixed).max() < 1e-12
+    assert abs(rep["nw"] - np.abs(q.pop).sum()) < 1e-9
+    with pytest.raises(ValueError):
+        OracleQmc(orc, ob, c0, refs, dt=0.01, propagator="direct-overlap")
