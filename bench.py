@@ -372,6 +372,7 @@ def qmc_leg(args, rank, world, local_rank, dist):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = qmc_cpu_baseline(system, basis, c0, refs, q, float(rep["shift"][-1]))
     q.close()
+    out["direct_overlap"] = direct_overlap_leg(args, w, c0, refs, float(er[0]), walkers, rank, local_rank, dist)
     if args.qmc_seeds > 0:
         out["generators"] = compare_generators(w, c0, refs, float(er[0]), walkers, args.qmc_seeds, rank,
                                                epochs=args.qmc_train_epochs, max_seconds=args.qmc_max_seconds,
@@ -1010,6 +1011,54 @@ def beyond_hbm_leg(args, rank, local_rank):
             "timing": "host clock around nw_eval_hs_pairs_blocked (every block's build and evaluation)"}
 
 
+def direct_overlap_leg(args, w, c0, refs, e_ref, walkers, rank, local_rank, dist):
+    """The direct-overlap propagator on the same system: steps/s of report blocks whose end
+    applies the overlap action N += S Phi(Delta), and the overlap action alone (y += S x over the
+    85755 determinants through the spin-factor tables; CUDA events around repeated applies)."""
+    import torch
+    import nociwick
+    nd = c0.shape[0]
+    dev = f"cuda:{local_rank}"
+    x = torch.randn(nd, dtype=torch.float64, device=dev)
+    y = torch.zeros(nd, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    w.apply_overlap_device(x.data_ptr(), y.data_ptr(), stream)      # builds the spin-factor tables
+    torch.cuda.synchronize(dev)
+    setup_s = time.perf_counter() - t0
+    for _ in range(3):
+        w.apply_overlap_device(x.data_ptr(), y.data_ptr(), stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 50
+    e0.record()
+    for _ in range(reps):
+        w.apply_overlap_device(x.data_ptr(), y.data_ptr(), stream)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    apply_ms = e0.elapsed_time(e1) / reps
+    q = nociwick.Qmc(w, c0, refs, dt=1e-3, initial_population=walkers, target_population=walkers,
+                     shift_damping=0.5, initial_shift=e_ref, ncycles=10, propagator="direct-overlap",
+                     seed=rank_seed(4343, rank), max_attempts=48_000_000)
+    q.run(args.qmc_equil)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    rep = q.run(args.qmc_reports)
+    ms = q.last_run_ms()
+    q.close()
+    (ms, apply_ms) = reduce_max([ms, apply_ms], dist, dev)
+    steps = args.qmc_reports * 10
+    return {"value": steps / (ms / 1e3), "unit": "steps/s", "ms_per_step": ms / steps,
+            "config": {"propagator": "direct-overlap", "ncycles": 10, "update_cutoff": 0.0},
+            "walkers_mean": float(rep["nw"].mean()),
+            "eproj_last": float(rep["eproj_num"][-1] / rep["eproj_den"][-1]),
+            "overlap_apply_ms": apply_ms, "overlap_setup_s": setup_s,
+            "overlap_elements_per_s": nd * nd / (apply_ms / 1e3),
+            "note": "one report = 10 cycles then N += S Delta; overlap_elements_per_s counts the ndet^2 "
+                    "overlaps a dense S x would need per apply"}
+
+
 def tail_summary(line):
     """The figures a reader of the end of the output needs, in a few hundred bytes."""
     wl = "hs_config3" if line["config"]["workload"].startswith("synthetic stress") else "hs_config2"
@@ -1034,6 +1083,9 @@ def tail_summary(line):
     q = line.get("qmc")
     if q:
         out["qmc"] = {"steps_per_s": q["value"], "walkers": q["walkers_mean"]}
+        do = q.get("direct_overlap")
+        if do:
+            out["qmc"]["direct_overlap"] = {"steps_per_s": do["value"], "overlap_apply_ms": do["overlap_apply_ms"]}
         if "cpu_baseline" in q:
             out["qmc"]["cpu_steps_per_s"] = q["cpu_baseline"]["value"]
         g = q.get("generators")

@@ -17,9 +17,11 @@
 // the same (a, b) pair (the determinant itself in a basis without duplicates).  Per ordered pair
 // the work is nnz(x_P) nb_Q + ndet_Q na_P multiply-adds instead of ndet_Q ndet_P overlaps.
 //
-// Layout: the determinants sorted by (parent, alpha component, beta component); stage 1 is one
-// block per source alpha component (its sorted run of sources) and 256 target beta components per
-// block, reading rows of B^{QP} stored source-major (coalesced over bbar); stage 2 is one thread
+// Layout: the determinants sorted by (parent, alpha component, beta component); stage 1 takes
+// the sorted sources of each alpha component in chunks of at most 32 (a long row, such as the
+// parent's own alpha string with every beta string, is spread over many blocks that add into its
+// U row) with 256 target beta components per block, reading rows of B^{QP} stored source-major
+// (coalesced over bbar) with four independent loads in flight per thread; stage 2 is one thread
 // per target in sorted order, so the lanes of a warp share a_w (broadcast A reads) and read
 // neighbouring b_w of U (coalesced), with the (P, a) sum split into segments whose partial sums a
 // finishing kernel adds in a fixed order.  No allocation and no host synchronisation per apply,
@@ -39,19 +41,33 @@
 
 namespace nw {
 
-// One stage-1 row: a source alpha component of P for target parent Q.
-struct RowDesc {
-  uint64_t comp;  // global alpha component index (rowstart)
+// Stage 1 works on chunks of at most kOvlChunk sources of one row (a source alpha component a of
+// P for target parent Q): U^{QP}[a][.] is stored by the row's only chunk, or added atomically by
+// each chunk of a longer row (whose U row is cleared first).  A block takes a group of consecutive
+// chunks of one source parent (at most kOvlGroup sources), staged in shared memory.
+struct OvlChunk {
   uint64_t bt;    // B^{QP} (source-major, nb_P x nb_Q) in the factor buffer
   uint64_t urow;  // row a of U^{QP} in the work buffer
+  uint32_t t0, t1;  // sorted source positions
+  uint32_t atomic;  // the row has several chunks
+  uint32_t pad;
+};
+struct OvlGroup {
+  uint32_t c0, c1;  // chunks
+  uint32_t t0, t1;  // their sources
 };
 
 namespace {
 
 constexpr int kOvlMaxOcc = 16;    // occupied orbitals per spin of the factor kernel
 constexpr int kOvlThreads = 256;
-constexpr uint64_t kOvlThreadTarget = 148ull * 2048;  // stage-2 threads to aim for (segments)
+constexpr uint64_t kOvlThreadTarget = 148ull * 2048 * 4;  // stage-2 threads to aim for (segments): 4 waves
+constexpr uint32_t kOvlChunk = 32;   // sources per stage-1 chunk
+constexpr uint32_t kOvlGroup = 64;   // sources per stage-1 block
 
+// One entry of a single-spin factor table per thread; MAXO bounds nocc (the LU scratch lives in
+// the thread's stack frame, MAXO^2 doubles).
+template <int MAXO>
 __global__ void __launch_bounds__(kOvlThreads) ovl_factor_kernel(const double* __restrict__ o, int nmo,
                                                                   const uint8_t* __restrict__ occ_t,
                                                                   const uint8_t* __restrict__ occ_s, int nocc,
@@ -62,7 +78,7 @@ __global__ void __launch_bounds__(kOvlThreads) ovl_factor_kernel(const double* _
     const uint32_t i = (uint32_t)(e / ns), j = (uint32_t)(e % ns);
     const uint8_t* oi = occ_t + (uint64_t)i * nocc;
     const uint8_t* oj = occ_s + (uint64_t)j * nocc;
-    double m[kOvlMaxOcc * kOvlMaxOcc];
+    double m[MAXO * MAXO];
     for (int r = 0; r < nocc; ++r)
       for (int c = 0; c < nocc; ++c) m[r * nocc + c] = o[(uint64_t)oi[r] * nmo + oj[c]];
     const double d = det_lu_inplace(m, nocc);
@@ -78,34 +94,53 @@ __global__ void __launch_bounds__(kOvlThreads) ovl_gather_kernel(uint64_t ndet, 
     xs[t] = ord_r[t] * x[ord_det[t]];
 }
 
-// U^{QP}[a][bbar] for every row (P, a) of target parent Q; blockIdx.x = row, blockIdx.y = chunk
-// of 256 target beta components.  The sources of a row are uniform over the block.
-__global__ void __launch_bounds__(kOvlThreads) ovl_stage1_kernel(const RowDesc* __restrict__ rows,
-                                                                  const uint64_t* __restrict__ rowstart,
+// Clears the U rows that several chunks add into (blockIdx.x = row, blockIdx.y = 256 columns).
+__global__ void __launch_bounds__(kOvlThreads) ovl_zero_kernel(const uint64_t* __restrict__ urows, uint32_t nbq,
+                                                                double* __restrict__ u) {
+  const uint32_t b = blockIdx.y * blockDim.x + threadIdx.x;
+  if (b < nbq) u[urows[blockIdx.x] + b] = 0.0;
+}
+
+// U^{QP}[a][bbar] for the chunks of one group (blockIdx.x) and 256 target beta components
+// (blockIdx.y): every thread sums its column over the group's staged sources; the loads of one
+// chunk are independent (four in flight per step).
+__global__ void __launch_bounds__(kOvlThreads) ovl_stage1_kernel(const OvlGroup* __restrict__ groups,
+                                                                  const OvlChunk* __restrict__ chunks,
                                                                   const uint32_t* __restrict__ ord_b,
                                                                   const double* __restrict__ xs,
                                                                   const double* __restrict__ fac, uint32_t nbq,
                                                                   double* __restrict__ u) {
-  const RowDesc rd = rows[blockIdx.x];
+  __shared__ double sx[kOvlGroup];
+  __shared__ uint32_t sb[kOvlGroup];
+  const OvlGroup g = groups[blockIdx.x];
+  for (uint32_t i = threadIdx.x; i < g.t1 - g.t0; i += blockDim.x) {
+    sx[i] = xs[g.t0 + i];
+    sb[i] = ord_b[g.t0 + i];
+  }
+  __syncthreads();
   const uint32_t bbar = blockIdx.y * blockDim.x + threadIdx.x;
-  const bool live = bbar < nbq;
-  const uint64_t t0 = rowstart[rd.comp], t1 = rowstart[rd.comp + 1];
-  const double* bt = fac + rd.bt + bbar;
-  double acc0 = 0.0, acc1 = 0.0;
-  uint64_t t = t0;
-  for (; t + 2 <= t1; t += 2) {
-    const double v0 = xs[t], v1 = xs[t + 1];
-    const uint32_t b0 = ord_b[t], b1 = ord_b[t + 1];
-    if (live) {
-      if (v0 != 0.0) acc0 += v0 * __ldg(bt + (uint64_t)b0 * nbq);
-      if (v1 != 0.0) acc1 += v1 * __ldg(bt + (uint64_t)b1 * nbq);
+  if (bbar >= nbq) return;
+  for (uint32_t c = g.c0; c < g.c1; ++c) {
+    const OvlChunk ch = chunks[c];
+    const double* bt = fac + ch.bt + bbar;
+    const uint32_t k1 = ch.t1 - g.t0;
+    uint32_t k = ch.t0 - g.t0;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    for (; k + 4 <= k1; k += 4) {
+      const double b0 = __ldg(bt + (uint64_t)sb[k] * nbq), b1 = __ldg(bt + (uint64_t)sb[k + 1] * nbq);
+      const double b2 = __ldg(bt + (uint64_t)sb[k + 2] * nbq), b3 = __ldg(bt + (uint64_t)sb[k + 3] * nbq);
+      a0 += sx[k] * b0;
+      a1 += sx[k + 1] * b1;
+      a2 += sx[k + 2] * b2;
+      a3 += sx[k + 3] * b3;
     }
+    for (; k < k1; ++k) a0 += sx[k] * __ldg(bt + (uint64_t)sb[k] * nbq);
+    const double sum = (a0 + a1) + (a2 + a3);
+    if (ch.atomic)
+      atomicAdd(u + ch.urow + bbar, sum);
+    else
+      u[ch.urow + bbar] = sum;
   }
-  if (t < t1 && live) {
-    const double v0 = xs[t];
-    if (v0 != 0.0) acc0 += v0 * __ldg(bt + (uint64_t)ord_b[t] * nbq);
-  }
-  if (live) u[rd.urow + bbar] = acc0 + acc1;
 }
 
 // Partial sums over segment blockIdx.y of the (P, a) index of every target t in [t0, t1) of
@@ -123,7 +158,7 @@ __global__ void __launch_bounds__(kOvlThreads) ovl_stage2_kernel(int q, int nref
   if (t >= t1) return;
   const uint64_t k0 = (uint64_t)blockIdx.y * seglen, k1 = k0 + seglen;
   const uint32_t at = ord_a[t], bq = ord_b[t];
-  double acc0 = 0.0, acc1 = 0.0;
+  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
   uint64_t kbase = 0;
   for (int p = 0; p < nref; ++p) {
     if (p == q) continue;
@@ -136,15 +171,19 @@ __global__ void __launch_bounds__(kOvlThreads) ovl_stage2_kernel(int q, int nref
       const double* ucol = u + u_off[(uint64_t)q * nref + p] + bq;
       const uint64_t a1 = hi - kbase;
       uint64_t a = lo - kbase;
-      for (; a + 2 <= a1; a += 2) {
-        acc0 += __ldg(arow + a) * __ldg(ucol + a * nbq);
-        acc1 += __ldg(arow + a + 1) * __ldg(ucol + (a + 1) * nbq);
+      for (; a + 4 <= a1; a += 4) {
+        const double u0 = __ldg(ucol + a * nbq), u1 = __ldg(ucol + (a + 1) * nbq);
+        const double u2 = __ldg(ucol + (a + 2) * nbq), u3 = __ldg(ucol + (a + 3) * nbq);
+        acc0 += __ldg(arow + a) * u0;
+        acc1 += __ldg(arow + a + 1) * u1;
+        acc2 += __ldg(arow + a + 2) * u2;
+        acc3 += __ldg(arow + a + 3) * u3;
       }
-      if (a < a1) acc0 += __ldg(arow + a) * __ldg(ucol + a * nbq);
+      for (; a < a1; ++a) acc0 += __ldg(arow + a) * __ldg(ucol + a * nbq);
     }
     kbase += n;
   }
-  part[(uint64_t)blockIdx.y * ndet + t] = acc0 + acc1;
+  part[(uint64_t)blockIdx.y * ndet + t] = (acc0 + acc1) + (acc2 + acc3);
 }
 
 __global__ void __launch_bounds__(kOvlThreads) ovl_finish_kernel(uint64_t ndet, int nseg, int cross,
@@ -216,17 +255,19 @@ struct OverlapPlan {
   int nseg = 1;
   std::vector<uint32_t> na, nb;
   std::vector<uint64_t> pstart;         // per parent: first sorted position (nref + 1)
-  std::vector<uint64_t> nrows, rows_off;  // per target parent: stage-1 rows
+  std::vector<uint64_t> ngroups, groups_off;  // per target parent: stage-1 groups
+  std::vector<uint64_t> nzero, zero_off;      // per target parent: U rows cleared before stage 1
   std::vector<uint64_t> seglen;         // per target parent
   void* mem = nullptr;
   uint32_t* ord_det = nullptr;
   uint32_t* ord_a = nullptr;
   uint32_t* ord_b = nullptr;
   double* ord_r = nullptr;
-  uint64_t* rowstart = nullptr;
   uint32_t* run_lo = nullptr;  // null when every (parent, a, b) is a single determinant
   uint32_t* run_hi = nullptr;
-  RowDesc* rows = nullptr;
+  OvlGroup* groups = nullptr;
+  OvlChunk* chunks = nullptr;
+  uint64_t* zero_rows = nullptr;
   uint64_t* d_a_off = nullptr;
   uint64_t* d_u_off = nullptr;
   uint32_t* d_na = nullptr;
@@ -342,16 +383,21 @@ nw_status overlap_plan_get(nw_ctx* ctx, cudaStream_t stream, OverlapPlan** out) 
   // factor tables, U offsets and stage-1 rows
   std::vector<uint64_t> a_off((size_t)nref * nref, 0), bt_off((size_t)nref * nref, 0), u_off((size_t)nref * nref, 0);
   uint64_t nfac = 0, nu = 0;
-  std::vector<RowDesc> rows;
-  pl->nrows.assign(nref, 0);
-  pl->rows_off.assign(nref, 0);
+  std::vector<OvlGroup> groups;
+  std::vector<OvlChunk> chunks;
+  std::vector<uint64_t> zero_rows;
+  pl->ngroups.assign(nref, 0);
+  pl->groups_off.assign(nref, 0);
+  pl->nzero.assign(nref, 0);
+  pl->zero_off.assign(nref, 0);
   pl->seglen.assign(nref, 1);
   uint64_t max_targets = 1;
   for (int q = 0; q < nref; ++q) max_targets = std::max<uint64_t>(max_targets, pl->pstart[q + 1] - pl->pstart[q]);
   pl->nseg = (int)std::max<uint64_t>(1, std::min<uint64_t>(64, (kOvlThreadTarget + max_targets - 1) / max_targets));
   for (int q = 0; q < nref; ++q) {
     uint64_t uq = 0, kq = 0;
-    pl->rows_off[q] = rows.size();
+    pl->groups_off[q] = groups.size();
+    pl->zero_off[q] = zero_rows.size();
     for (int p = 0; p < nref; ++p) {
       if (p == q) continue;
       const size_t i = (size_t)q * nref + p;
@@ -360,11 +406,29 @@ nw_status overlap_plan_get(nw_ctx* ctx, cudaStream_t stream, OverlapPlan** out) 
       bt_off[i] = nfac;
       nfac += (uint64_t)pl->nb[p] * pl->nb[q];
       u_off[i] = uq;
-      for (uint32_t a = 0; a < pl->na[p]; ++a) rows.push_back(RowDesc{ca_off[p] + a, bt_off[i], uq + (uint64_t)a * pl->nb[q]});
+      // chunks of the rows of P in sorted order, grouped (a group never spans two parents)
+      bool open = false;
+      for (uint32_t a = 0; a < pl->na[p]; ++a) {
+        const uint64_t r0 = rowstart[ca_off[p] + a], r1 = rowstart[ca_off[p] + a + 1];
+        const uint64_t urow = uq + (uint64_t)a * pl->nb[q];
+        const bool multi = r1 - r0 > kOvlChunk;
+        if (multi) zero_rows.push_back(urow);
+        for (uint64_t c0 = r0; c0 < r1; c0 += kOvlChunk) {
+          const uint64_t c1 = std::min<uint64_t>(r1, c0 + kOvlChunk);
+          if (!open || c1 - groups.back().t0 > kOvlGroup) {
+            groups.push_back(OvlGroup{(uint32_t)chunks.size(), (uint32_t)chunks.size(), (uint32_t)c0, (uint32_t)c0});
+            open = true;
+          }
+          chunks.push_back(OvlChunk{bt_off[i], urow, (uint32_t)c0, (uint32_t)c1, multi ? 1u : 0u, 0u});
+          groups.back().c1 = (uint32_t)chunks.size();
+          groups.back().t1 = (uint32_t)c1;
+        }
+      }
       uq += (uint64_t)pl->na[p] * pl->nb[q];
       kq += pl->na[p];
     }
-    pl->nrows[q] = rows.size() - pl->rows_off[q];
+    pl->ngroups[q] = groups.size() - pl->groups_off[q];
+    pl->nzero[q] = zero_rows.size() - pl->zero_off[q];
     pl->seglen[q] = std::max<uint64_t>(1, (kq + pl->nseg - 1) / pl->nseg);
     nu = std::max(nu, uq);
   }
@@ -378,9 +442,10 @@ nw_status overlap_plan_get(nw_ctx* ctx, cudaStream_t stream, OverlapPlan** out) 
     return at;
   };
   const size_t o_det = carve(nd * 4), o_a_ = carve(nd * 4), o_b_ = carve(nd * 4), o_r_ = carve(nd * 8);
-  const size_t o_rs = carve(rowstart.size() * 8);
   const size_t o_lo = dups ? carve(nd * 4) : 0, o_hi = dups ? carve(nd * 4) : 0;
-  const size_t o_rows = carve(std::max<size_t>(1, rows.size()) * sizeof(RowDesc));
+  const size_t o_groups = carve(std::max<size_t>(1, groups.size()) * sizeof(OvlGroup));
+  const size_t o_chunks = carve(std::max<size_t>(1, chunks.size()) * sizeof(OvlChunk));
+  const size_t o_zero = carve(std::max<size_t>(1, zero_rows.size()) * 8);
   const size_t o_aoff = carve(nrr * 8), o_uoff = carve(nrr * 8), o_na = carve(nref * 4);
   const size_t o_occa = carve(occ_a.size()), o_occb = carve(occ_b.size());
   const size_t o_fac = carve(std::max<uint64_t>(1, nfac) * 8), o_u = carve(std::max<uint64_t>(1, nu) * 8);
@@ -402,10 +467,11 @@ nw_status overlap_plan_get(nw_ctx* ctx, cudaStream_t stream, OverlapPlan** out) 
   pl->ord_a = reinterpret_cast<uint32_t*>(base + o_a_);
   pl->ord_b = reinterpret_cast<uint32_t*>(base + o_b_);
   pl->ord_r = reinterpret_cast<double*>(base + o_r_);
-  pl->rowstart = reinterpret_cast<uint64_t*>(base + o_rs);
   pl->run_lo = dups ? reinterpret_cast<uint32_t*>(base + o_lo) : nullptr;
   pl->run_hi = dups ? reinterpret_cast<uint32_t*>(base + o_hi) : nullptr;
-  pl->rows = reinterpret_cast<RowDesc*>(base + o_rows);
+  pl->groups = reinterpret_cast<OvlGroup*>(base + o_groups);
+  pl->chunks = reinterpret_cast<OvlChunk*>(base + o_chunks);
+  pl->zero_rows = reinterpret_cast<uint64_t*>(base + o_zero);
   pl->d_a_off = reinterpret_cast<uint64_t*>(base + o_aoff);
   pl->d_u_off = reinterpret_cast<uint64_t*>(base + o_uoff);
   pl->d_na = reinterpret_cast<uint32_t*>(base + o_na);
@@ -422,7 +488,9 @@ nw_status overlap_plan_get(nw_ctx* ctx, cudaStream_t stream, OverlapPlan** out) 
   };
   bool ok = up(pl->ord_det, order.data(), nd * 4) && up(pl->ord_a, o_a.data(), nd * 4) &&
             up(pl->ord_b, o_b.data(), nd * 4) && up(pl->ord_r, o_r.data(), nd * 8) &&
-            up(pl->rowstart, rowstart.data(), rowstart.size() * 8) && up(pl->rows, rows.data(), rows.size() * sizeof(RowDesc)) &&
+            up(pl->groups, groups.data(), groups.size() * sizeof(OvlGroup)) &&
+            up(pl->chunks, chunks.data(), chunks.size() * sizeof(OvlChunk)) &&
+            up(pl->zero_rows, zero_rows.data(), zero_rows.size() * 8) &&
             up(pl->d_a_off, a_off.data(), nrr * 8) && up(pl->d_u_off, u_off.data(), nrr * 8) &&
             up(pl->d_na, pl->na.data(), nref * 4) && up(d_occa, occ_a.data(), occ_a.size()) &&
             up(d_occb, occ_b.data(), occ_b.size());
@@ -437,19 +505,26 @@ nw_status overlap_plan_get(nw_ctx* ctx, cudaStream_t stream, OverlapPlan** out) 
       ok = dgemm_strided(stream, true, false, nmo, nmo, nao, 1.0, c + q * cs, nmo, 0, d_t, nmo, cs, 0.0,
                          d_o + ((size_t)spin * nrr + (size_t)q * nref) * n2, nmo, (long long)n2, nref) == cudaSuccess;
   }
+  auto factors = [&](const double* o, const uint8_t* ot, const uint8_t* os, int nocc, uint32_t nt, uint32_t ns,
+                     int source_major, double* out) {
+    const uint64_t e = (uint64_t)nt * ns;
+    if (e == 0) return;
+    if (nocc <= 4)
+      ovl_factor_kernel<4><<<grid_of(e), kOvlThreads, 0, stream>>>(o, nmo, ot, os, nocc, nt, ns, source_major, out);
+    else if (nocc <= 8)
+      ovl_factor_kernel<8><<<grid_of(e), kOvlThreads, 0, stream>>>(o, nmo, ot, os, nocc, nt, ns, source_major, out);
+    else
+      ovl_factor_kernel<kOvlMaxOcc><<<grid_of(e), kOvlThreads, 0, stream>>>(o, nmo, ot, os, nocc, nt, ns, source_major,
+                                                                            out);
+  };
   for (int q = 0; ok && q < nref; ++q)
     for (int p = 0; ok && p < nref; ++p) {
       if (p == q) continue;
       const size_t i = (size_t)q * nref + p;
-      const uint64_t ea = (uint64_t)pl->na[q] * pl->na[p], eb = (uint64_t)pl->nb[q] * pl->nb[p];
-      if (ea)
-        ovl_factor_kernel<<<grid_of(ea), kOvlThreads, 0, stream>>>(d_o + i * n2, nmo, d_occa + ca_off[q] * pl->oa,
-                                                                   d_occa + ca_off[p] * pl->oa, pl->oa, pl->na[q],
-                                                                   pl->na[p], 0, pl->fac + a_off[i]);
-      if (eb)
-        ovl_factor_kernel<<<grid_of(eb), kOvlThreads, 0, stream>>>(d_o + (nrr + i) * n2, nmo, d_occb + cb_off[q] * pl->ob,
-                                                                   d_occb + cb_off[p] * pl->ob, pl->ob, pl->nb[q],
-                                                                   pl->nb[p], 1, pl->fac + bt_off[i]);
+      factors(d_o + i * n2, d_occa + ca_off[q] * pl->oa, d_occa + ca_off[p] * pl->oa, pl->oa, pl->na[q], pl->na[p], 0,
+              pl->fac + a_off[i]);
+      factors(d_o + (nrr + i) * n2, d_occb + cb_off[q] * pl->ob, d_occb + cb_off[p] * pl->ob, pl->ob, pl->nb[q],
+              pl->nb[p], 1, pl->fac + bt_off[i]);
       ok = cudaGetLastError() == cudaSuccess;
     }
   if (ok) ok = cudaStreamSynchronize(stream) == cudaSuccess;
@@ -470,11 +545,13 @@ nw_status overlap_apply(nw_ctx* ctx, const OverlapPlan* pl, const double* x, dou
     const uint64_t t0 = pl->pstart[q], t1 = pl->pstart[q + 1];
     if (t1 == t0) continue;
     const uint32_t nbq = pl->nb[q];
-    if (pl->nrows[q] > 0) {
-      const dim3 g((unsigned)pl->nrows[q], (nbq + kOvlThreads - 1) / kOvlThreads);
-      ovl_stage1_kernel<<<g, kOvlThreads, 0, stream>>>(pl->rows + pl->rows_off[q], pl->rowstart, pl->ord_b, pl->xs,
-                                                       pl->fac, nbq, pl->u);
-    }
+    const unsigned ycols = (nbq + kOvlThreads - 1) / kOvlThreads;
+    if (pl->nzero[q] > 0)
+      ovl_zero_kernel<<<dim3((unsigned)pl->nzero[q], ycols), kOvlThreads, 0, stream>>>(pl->zero_rows + pl->zero_off[q],
+                                                                                      nbq, pl->u);
+    if (pl->ngroups[q] > 0)
+      ovl_stage1_kernel<<<dim3((unsigned)pl->ngroups[q], ycols), kOvlThreads, 0, stream>>>(
+          pl->groups + pl->groups_off[q], pl->chunks, pl->ord_b, pl->xs, pl->fac, nbq, pl->u);
     const dim3 g2((unsigned)((t1 - t0 + kOvlThreads - 1) / kOvlThreads), (unsigned)pl->nseg);
     ovl_stage2_kernel<<<g2, kOvlThreads, 0, stream>>>(q, pl->nref, t0, t1, pl->seglen[q], pl->ord_a, pl->ord_b,
                                                       pl->d_na, pl->d_a_off, pl->d_u_off, nbq, pl->fac, pl->u, nd,
