@@ -11,8 +11,9 @@
 //               off the diagonal, its column sums to y[cols] (FP64 atomics, 512 per tile).  The
 //               triangle is streamed from HBM once per product.  Without a stored matrix
 //               (nw_pt2_create_matrix_free, operators.rs:424-471) every product evaluates the
-//               upper-triangle (F, S) pairs again through the sorted pair pipeline, block by
-//               block, and accumulates them into y directly: no n^2 storage.
+//               upper-triangle (F, S) pairs again through the sorted pair pipeline in blocks of
+//               whole 256 x 256 tiles and accumulates each tile into y as the stored product
+//               does (row and column sums, 512 atomics per tile): no n^2 storage.
 //   projected : apply_omega_m / apply_projection_correction (operators.rs:696-955):
 //               y = M x - f_a0 (s_0a.x) - s_a0 (f_0a.x) + 2 E0 s_a0 (s_0a.x).
 //   GMRES     : gmres / run_arnoldi_cycle (src/snoci/gmres.rs:268-544): zero start, Arnoldi on
@@ -140,66 +141,114 @@ __global__ void packed_diag_kernel(const double* __restrict__ m, uint64_t n, dou
     d[a] = m[row_start(a, n)];
 }
 
-// Pair k of a block is packed entry base + k; its (row, col) by a search over the rows >= r0.
-__global__ void upper_pairs_kernel(const uint32_t* __restrict__ cand, uint64_t n, uint64_t r0, uint64_t base,
-                                   uint64_t count, uint2* __restrict__ pairs) {
+// Row of packed entry p: the largest a with row_start(a) <= p, from the root of the quadratic
+// row_start(a) = p (FP64, within one of the answer) and an exact integer fix-up.
+__device__ inline uint64_t row_of(uint64_t p, uint64_t n) {
+  const double b = 2.0 * (double)n + 1.0;
+  const double g = floor((b - sqrt(b * b - 8.0 * (double)p)) / 2.0);
+  uint64_t a = g < 0.0 ? 0 : (uint64_t)g;
+  if (a >= n) a = n - 1;
+  while (a > 0 && row_start(a, n) > p) --a;
+  while (a + 1 < n && row_start(a + 1, n) <= p) ++a;
+  return a;
+}
+
+// Pair k of a block is packed entry base + k (the packed build's row-major order).
+__global__ void upper_pairs_kernel(const uint32_t* __restrict__ cand, uint64_t n, uint64_t base, uint64_t count,
+                                   uint2* __restrict__ pairs) {
   for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < count; k += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t p = base + k;
-    uint64_t lo = r0, hi = n;  // largest a with row_start(a) <= p
-    while (hi - lo > 1) {
-      const uint64_t mid = (lo + hi) >> 1;
-      if (row_start(mid, n) <= p)
-        lo = mid;
-      else
-        hi = mid;
-    }
-    const uint64_t b = lo + (p - row_start(lo, n));
-    pairs[k] = make_uint2(cand[lo], cand[b]);
+    const uint64_t a = row_of(p, n);
+    const uint64_t b = a + (p - row_start(a, n));
+    pairs[k] = make_uint2(cand[a], cand[b]);
   }
 }
 
-// Matrix-free product of one block of upper-triangle entries base .. base + count (rows from
-// r0): M_ab = F_ab - e0 S_ab, y[a] += M_ab x[b] and, off the diagonal, y[b] += M_ab x[a]
-// (apply_candidate_m without a cached matrix, src/snoci/operators.rs:424-471).  Each thread
-// takes kMfRun consecutive entries, which lie in one row except at row ends, and adds its row
-// sum with one atomic per row it touches; the column terms go out one atomic each.
-constexpr int kMfRun = 8;
+// Matrix-free products go over the upper triangle in 256 x 256 tiles (I <= J), 65536 pair slots
+// per tile in row-major (i, j) order; slots outside the triangle (b < a on a diagonal tile, or
+// past the last candidate) get the pair (cand[0], cand[0]) and are ignored by the product.
+constexpr uint64_t kTileSlots = (uint64_t)kTile * kTile;
 
-__global__ void mf_apply_kernel(const double2* __restrict__ fs, uint64_t n, uint64_t r0, uint64_t base,
-                                uint64_t count, double e0, const double* __restrict__ x, double* __restrict__ y) {
-  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t k0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) * kMfRun; k0 < count; k0 += nthreads * kMfRun) {
-    const uint64_t p0 = base + k0;
-    uint64_t lo = r0, hi = n;  // row of entry p0: largest a with row_start(a) <= p0
-    while (hi - lo > 1) {
-      const uint64_t mid = (lo + hi) >> 1;
-      if (row_start(mid, n) <= p0)
-        lo = mid;
-      else
-        hi = mid;
-    }
-    uint64_t a = lo, b = lo + (p0 - row_start(lo, n));
-    double xa = x[a], rowsum = 0.0;
-    const uint64_t kend = k0 + kMfRun < count ? k0 + kMfRun : count;
-    for (uint64_t k = k0; k < kend; ++k) {
-      if (b >= n) {  // next row
-        if (rowsum != 0.0) atomicAdd(y + a, rowsum);
-        ++a;
-        b = a;
-        xa = x[a];
-        rowsum = 0.0;
-      }
-      const double2 v = fs[k];
-      const double m = v.x - e0 * v.y;
-      rowsum = fma(m, x[b], rowsum);
-      if (b != a) {
-        const double cy = m * xa;
-        if (cy != 0.0) atomicAdd(y + b, cy);
-      }
-      ++b;
-    }
-    if (rowsum != 0.0) atomicAdd(y + a, rowsum);
+__global__ void tile_pairs_kernel(const uint32_t* __restrict__ cand, uint64_t n, uint64_t nb, uint64_t t0,
+                                  uint64_t nslots, uint2* __restrict__ pairs) {
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nslots; s += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t I, J;
+    tile_of(t0 + s / kTileSlots, nb, &I, &J);
+    const uint64_t k = s % kTileSlots;
+    const uint64_t a = I * kTile + k / kTile, b = J * kTile + k % kTile;
+    const bool live = a < n && b < n && b >= a;
+    pairs[s] = live ? make_uint2(cand[a], cand[b]) : make_uint2(cand[0], cand[0]);
   }
+}
+
+// y += M x over the tiles t0 .. t0 + gridDim.x of a block of evaluated (F, S) slots, M = F - e0 S:
+// the structure of packed_symv_kernel (8 warps x 32 rows, a lane holds 8 columns; row sums to
+// y[rows], strictly-upper column sums to y[cols], 512 atomics per tile) with the tile's entries
+// read from its 65536 contiguous (F, S) slots.
+__global__ void __launch_bounds__(kTile, 2) mf_tile_apply_kernel(const double2* __restrict__ fs, uint64_t n,
+                                                                 uint64_t nb, uint64_t t0, double e0,
+                                                                 const double* __restrict__ x,
+                                                                 double* __restrict__ y) {
+  __shared__ double xrow[kTile];
+  __shared__ double rowsum[kTile];
+  __shared__ double colsum[kTileWarps][kTile];
+  uint64_t I, J;
+  tile_of(t0 + blockIdx.x, nb, &I, &J);
+  const double2* tile = fs + (uint64_t)blockIdx.x * kTileSlots;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t r0 = I * kTile, c0 = J * kTile;
+  xrow[threadIdx.x] = r0 + threadIdx.x < n ? x[r0 + threadIdx.x] : 0.0;
+  double xc[kColsPerLane], cacc[kColsPerLane];
+#pragma unroll
+  for (int k = 0; k < kColsPerLane; ++k) {
+    const uint64_t b = c0 + lane + 32 * k;
+    xc[k] = b < n ? x[b] : 0.0;
+    cacc[k] = 0.0;
+  }
+  __syncthreads();
+  for (int rr = 0; rr < kRowsPerWarp; rr += kSymvRows) {
+    double v[kSymvRows][kColsPerLane];
+#pragma unroll
+    for (int g = 0; g < kSymvRows; ++g) {
+      const int rl = warp * kRowsPerWarp + rr + g;
+      const uint64_t a = r0 + rl;
+#pragma unroll
+      for (int k = 0; k < kColsPerLane; ++k) {
+        const int cl = lane + 32 * k;
+        const uint64_t b = c0 + cl;
+        double m = 0.0;
+        if (a < n && b < n && b >= a) {
+          const double2 e = __ldcs(tile + rl * kTile + cl);
+          m = e.x - e0 * e.y;
+        }
+        v[g][k] = m;
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < kSymvRows; ++g) {
+      const int rl = warp * kRowsPerWarp + rr + g;
+      const uint64_t a = r0 + rl;
+      const double xa = xrow[rl];
+      double rs = 0.0;
+#pragma unroll
+      for (int k = 0; k < kColsPerLane; ++k) {
+        rs = fma(v[g][k], xc[k], rs);
+        if (c0 + lane + 32 * k != a) cacc[k] = fma(v[g][k], xa, cacc[k]);
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) rs += __shfl_xor_sync(0xFFFFFFFFu, rs, off);
+      if (lane == 0) rowsum[rl] = rs;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kColsPerLane; ++k) colsum[warp][lane + 32 * k] = cacc[k];
+  __syncthreads();
+  const int t = threadIdx.x;
+  if (r0 + t < n && rowsum[t] != 0.0) atomicAdd(y + r0 + t, rowsum[t]);
+  double cs = 0.0;
+#pragma unroll
+  for (int w = 0; w < kTileWarps; ++w) cs += colsum[w][t];
+  if (c0 + t < n && cs != 0.0) atomicAdd(y + c0 + t, cs);
 }
 
 // diagonal pairs (cand[a], cand[a])
@@ -497,18 +546,6 @@ nw_status pfail(nw_pt2* p, nw_status s, const std::string& m) { return nw::fail(
     if (s_ != CUBLAS_STATUS_SUCCESS) return pfail(p, NW_ERR_CUDA, std::string(#call) + " failed"); \
   } while (0)
 
-// First row of the packed entry `base`: largest r with row_start(r) <= base.
-uint64_t first_row(uint64_t base, uint64_t n) {
-  uint64_t lo = 0, hi = n;
-  while (hi - lo > 1) {
-    const uint64_t mid = (lo + hi) >> 1;
-    if (row_start(mid, n) <= base)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  return lo;
-}
 
 // y = M x (device vectors, legacy stream): one pass over the packed triangle, or, matrix-free,
 // every upper-triangle pair evaluated again through the (F, S) pipeline block by block.
@@ -521,15 +558,14 @@ nw_status symv(nw_pt2* p, const double* x, double* y) {
     NW_CUDA(p->ctx, cudaGetLastError());
     return NW_OK;
   }
-  const uint64_t len = n * (n + 1) / 2;
-  for (uint64_t base = 0; base < len; base += p->blk) {
-    const uint64_t count = std::min(p->blk, len - base);
-    const uint64_t r0 = first_row(base, n);
-    upper_pairs_kernel<<<grid_n(count), 256>>>(p->dcand, n, r0, base, count, p->pairs);
-    nw_status st = nw::eval_pairs(p->ctx, reinterpret_cast<const uint32_t*>(p->pairs), count,
+  const uint64_t ntiles = nb * (nb + 1) / 2, per_block = p->blk / kTileSlots;
+  for (uint64_t t0 = 0; t0 < ntiles; t0 += per_block) {
+    const uint64_t nt = std::min(per_block, ntiles - t0), nslots = nt * kTileSlots;
+    tile_pairs_kernel<<<grid_n(nslots), 256>>>(p->dcand, n, nb, t0, nslots, p->pairs);
+    nw_status st = nw::eval_pairs(p->ctx, reinterpret_cast<const uint32_t*>(p->pairs), nslots,
                                   reinterpret_cast<double*>(p->fs), nw::EvalMode::kFS, nullptr);
     if (st != NW_OK) return st;
-    mf_apply_kernel<<<grid_n((count + kMfRun - 1) / kMfRun), 256>>>(p->fs, n, r0, base, count, p->e0, x, y);
+    mf_tile_apply_kernel<<<(unsigned)nt, kTile>>>(p->fs, n, nb, t0, p->e0, x, y);
     NW_CUDA(p->ctx, cudaGetLastError());
   }
   return NW_OK;
@@ -625,16 +661,7 @@ nw_status nw_pt2_create(nw_ctx* ctx, const uint32_t* cand, uint64_t n, double e0
     return cleanup(nw::fail(ctx, NW_ERR_CUDA, "candidate upload"));
   for (uint64_t base = 0; base < len; base += blk) {
     const uint64_t count = std::min(blk, len - base);
-    // first row of the block: largest r with row_start(r) <= base
-    uint64_t lo = 0, hi = n;
-    while (hi - lo > 1) {
-      const uint64_t mid = (lo + hi) >> 1;
-      if (row_start(mid, n) <= base)
-        lo = mid;
-      else
-        hi = mid;
-    }
-    upper_pairs_kernel<<<grid_n(count), 256>>>(dcand, n, lo, base, count, pairs);
+    upper_pairs_kernel<<<grid_n(count), 256>>>(dcand, n, base, count, pairs);
     nw_status st = nw::eval_pairs(ctx, reinterpret_cast<const uint32_t*>(pairs), count, reinterpret_cast<double*>(fs),
                                   nw::EvalMode::kFS, nullptr);
     if (st != NW_OK) return cleanup(st);
@@ -666,7 +693,9 @@ nw_status nw_pt2_create_matrix_free(nw_ctx* ctx, const uint32_t* cand, uint64_t 
   // pairs per evaluation block: 2^26 (1.6 GB of pairs and (F, S)) keeps the per-block cost of
   // the sort (counter clear and scan) small next to the evaluation
   constexpr uint64_t kBlock = 1ull << 26;
-  p->blk = std::max(std::min(kBlock, n * (n + 1) / 2), n);  // a block also holds the n diagonal pairs
+  const uint64_t nb = (n + kTile - 1) / kTile;
+  p->blk = std::min(kBlock, nb * (nb + 1) / 2 * kTileSlots);  // whole tiles
+  p->blk = std::max(p->blk, ((n + kTileSlots - 1) / kTileSlots) * kTileSlots);  // it also holds the n diagonal pairs
   auto cleanup = [&](nw_status st) {
     if (st != NW_OK) nw_pt2_destroy(p);
     return st;

@@ -117,3 +117,25 @@ def test_matrix_free_operator_matches_packed(snoci_system):
     assert np.all(np.abs(y_mf - y_pk) <= 1e-12 * scale + 1e-14)
     assert info_mf["converged"] and info_pk["converged"]
     assert np.max(np.abs(a_mf - a_pk)) <= 1e-8 * max(1.0, np.max(np.abs(a_pk)))
+
+
+def test_matrix_free_tiles_match_packed_and_dense():
+    """Candidates spanning several 256 x 256 tiles (diagonal, off-diagonal and partial edge
+    tiles of the matrix-free product): the matrix-free M x equals the packed product and the
+    dense F - E0 S from nw_build_fs_matrix."""
+    system = sy.make_system(10, 3, 3, 3, 16, seed=8, k_scale=0.3)
+    basis = sy.sd_basis(10, 3, 3, 3)
+    cand = np.nonzero((basis["rank_a"] + basis["rank_b"]) > 0)[0].astype(np.uint32)
+    assert cand.shape[0] > 5 * 256
+    e0 = -3.7
+    xv = np.random.default_rng(4).normal(size=cand.shape[0])
+    with nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8).build() as w:
+        w.set_basis(basis)
+        w.update_fock(system.h, system.h)
+        f, s = w.build_fs_matrix(cand, cand)
+        with nociwick.Pt2(w, cand, e0) as pk, nociwick.Pt2(w, cand, e0, matrix_free=True) as mf:
+            y_pk, y_mf = pk.apply_m(xv), mf.apply_m(xv)
+    m = f - e0 * s
+    scale = np.abs(m) @ np.abs(xv)
+    assert np.all(np.abs(y_mf - m @ xv) <= 1e-12 * scale + 1e-14)
+    assert np.all(np.abs(y_mf - y_pk) <= 1e-12 * scale + 1e-14)
