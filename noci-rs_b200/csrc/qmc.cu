@@ -58,8 +58,11 @@ struct QmcState {
   int32_t pad;
   // 64-bit sum of the current cycle's attempts, added up by the sample kernel (the 32-bit
   // per-determinant counts and their scan would wrap beyond 2^32 - 1), read and cleared by the
-  // count kernel
+  // owners kernel
   unsigned long long cycle_total;
+  // the cycle whose attempts are being spawned and applied: the sample kernel draws with
+  // `cycle`, the owners kernel copies it here and advances `cycle` for the next cycle
+  uint64_t cycle_cur;
 };
 
 struct QmcParams {
@@ -145,40 +148,33 @@ __global__ void qmc_sample_kernel(QmcParams q, QmcState* __restrict__ st, const 
   if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&st->cycle_total, sum);
 }
 
-// The 32-bit attempt offsets are valid only while the cycle's 64-bit total fits the buffers
-// (cap < 2^32); otherwise the cycle is flagged and the run fails on the host.
-__global__ void qmc_count_kernel(QmcParams q, QmcState* __restrict__ st, const uint32_t* __restrict__ off) {
-  const unsigned long long total64 = st->cycle_total;
-  st->cycle_total = 0ull;
-  const uint64_t total = total64 <= q.cap ? (uint64_t)off[q.ndet] : (uint64_t)total64;
-  const uint64_t held = total < q.cap ? total : q.cap;
-  if (total64 > q.cap) st->overflow = 1;
-  st->npairs = (uint32_t)held;
-  st->attempts += total;
-}
-
-// Largest g with off[g] <= t (off non-decreasing, off[0] = 0, t < off[ndet]).
-__device__ __forceinline__ uint64_t owner_of(const uint32_t* __restrict__ off, uint64_t ndet, uint32_t t) {
-  uint64_t lo = 0, hi = ndet;  // invariant: off[lo] <= t < off[hi]
-  while (hi - lo > 1) {
-    const uint64_t mid = (lo + hi) >> 1;
-    if (off[mid] <= t)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  return lo;
-}
-
 // Attempts are grouped in chunks of 2^kChunkShift; cown[c] = owner of the chunk's first attempt.
 constexpr int kChunkShift = 8;
 
-__global__ void qmc_chunk_kernel(QmcParams q, const QmcState* __restrict__ st, const uint32_t* __restrict__ off,
-                                 uint32_t* __restrict__ cown) {
-  const uint32_t n = st->npairs;
-  const uint32_t nchunk = (n + (1u << kChunkShift) - 1) >> kChunkShift;
-  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunk; c += gridDim.x * blockDim.x)
-    cown[c] = (uint32_t)owner_of(off, q.ndet, c << kChunkShift);
+// After the scan of the attempt counts: every determinant with attempts writes itself as the
+// owner of the chunks whose first attempt it holds (off[d] <= c 2^kChunkShift < off[d + 1]);
+// thread 0 also settles the cycle's totals -- the 32-bit offsets are valid only while the
+// cycle's 64-bit total fits the buffers (cap < 2^32), otherwise the cycle is flagged and the run
+// fails on the host -- and moves the cycle counter on (spawn and apply use cycle_cur).
+__global__ void qmc_owners_kernel(QmcParams q, QmcState* __restrict__ st, const uint32_t* __restrict__ off,
+                                  uint32_t* __restrict__ cown) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned long long total64 = st->cycle_total;
+    st->cycle_total = 0ull;
+    const uint64_t total = total64 <= q.cap ? (uint64_t)off[q.ndet] : (uint64_t)total64;
+    const uint64_t held = total < q.cap ? total : q.cap;
+    if (total64 > q.cap) st->overflow = 1;
+    st->npairs = (uint32_t)held;
+    st->attempts += total;
+    st->cycle_cur = st->cycle;
+    st->cycle += 1;
+  }
+  const uint64_t last = q.cap >> kChunkShift;  // cown holds chunks 0 .. last (+1 spare)
+  for (uint64_t d = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; d < q.ndet; d += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t lo = off[d], hi = off[d + 1];
+    for (uint64_t c = (lo + (1u << kChunkShift) - 1) >> kChunkShift; (c << kChunkShift) < hi && c <= last; ++c)
+      cown[c] = (uint32_t)d;
+  }
 }
 
 // Spawn attempts and classify their pairs for the sorted evaluation in one pass: the child
@@ -194,7 +190,7 @@ __global__ void qmc_spawn_kernel(QmcParams q, Proposal pr, nw::EvalParams P, con
                                  uint32_t* __restrict__ keys, uint32_t* __restrict__ ranks,
                                  uint32_t* __restrict__ counts, double* __restrict__ hs, uint32_t* __restrict__ flag) {
   const uint32_t n = st->npairs;
-  const uint64_t cycle = st->cycle;
+  const uint64_t cycle = st->cycle_cur;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t lanes_below = (1u << lane) - 1u;
   for (uint32_t w0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); w0 < n; w0 += gridDim.x * blockDim.x) {
@@ -281,7 +277,7 @@ __global__ void qmc_apply_kernel(QmcParams q, Proposal pr, const QmcState* __res
                                  const uint32_t* __restrict__ parent, const double* __restrict__ amp,
                                  const double* __restrict__ pg, double* __restrict__ delta) {
   const uint32_t n = st->npairs;
-  const uint64_t cycle = st->cycle;
+  const uint64_t cycle = st->cycle_cur;
   const double es = st->shift;
   const double pu = 1.0 / (double)(q.ndet - 1);
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
@@ -303,8 +299,6 @@ __global__ void qmc_apply_kernel(QmcParams q, Proposal pr, const QmcState* __res
     }
   }
 }
-
-__global__ void qmc_next_cycle_kernel(QmcState* __restrict__ st) { st->cycle += 1; }
 
 // Direct overlap: Phi_c(delta) of the report's accumulated change, one stream per (seed, report).
 __global__ void qmc_update_fri_kernel(QmcParams q, const QmcState* __restrict__ st, double* __restrict__ delta) {
@@ -552,8 +546,7 @@ nw_status enqueue_cycle(nw_qmc* q) {
   NW_CUDA(ctx, cudaGetLastError());
   nw_status st = nw::scan_exclusive(ctx, q->na, nd, q->off, q->tsum, s);
   if (st != NW_OK) return st;
-  qmc_count_kernel<<<1, 1, 0, s>>>(q->q, q->st, q->off);
-  qmc_chunk_kernel<<<grid_for((q->q.cap >> kChunkShift) + 1), kBlockThreads, 0, s>>>(q->q, q->st, q->off, q->cown);
+  qmc_owners_kernel<<<grid_for(nd), kBlockThreads, 0, s>>>(q->q, q->st, q->off, q->cown);
   NW_CUDA(ctx, cudaMemsetAsync(q->S.counts, 0, sizeof(uint32_t) * q->nkeys, s));
   qmc_spawn_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(
       q->q, q->pr, q->P, q->st, q->off, q->cown, q->sampled, q->na, q->pairs, q->child, q->parent, q->amp, q->pg,
@@ -564,7 +557,6 @@ nw_status enqueue_cycle(nw_qmc* q) {
   if (st != NW_OK) return st;
   qmc_apply_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(q->q, q->pr, q->st, q->hs, q->child, q->parent,
                                                                 q->amp, q->pg, q->delta);
-  qmc_next_cycle_kernel<<<1, 1, 0, s>>>(q->st);
   NW_CUDA(ctx, cudaGetLastError());
   return NW_OK;
 }

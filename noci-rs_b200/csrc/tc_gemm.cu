@@ -391,11 +391,21 @@ __device__ __forceinline__ long long chunk_offset(int row, int kc, int nrt) {
 }
 
 // Per-row exponents e with max_k |F[k][row]| * 2^-e <= 1/2 (0 for an all-zero or padding row).
-__global__ void row_exponent_kernel(const double* __restrict__ f, int K, int R, int rpad, int* __restrict__ e) {
-  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < rpad; row += gridDim.x * blockDim.x) {
-    double mx = 0.0;
-    if (row < R)
-      for (int k = 0; k < K; ++k) mx = fmax(mx, fabs(f[(long long)k * R + row]));
+// A block takes 32 rows (one per lane, coalesced loads) and splits the K range over its 8
+// warps; the per-warp maxima meet in shared memory.
+__global__ void __launch_bounds__(256) row_exponent_kernel(const double* __restrict__ f, int K, int R, int rpad,
+                                                           int* __restrict__ e) {
+  __shared__ double part[8][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int row = blockIdx.x * 32 + lane;
+  double mx = 0.0;
+  if (row < R)
+    for (int k = warp; k < K; k += 8) mx = fmax(mx, fabs(f[(long long)k * R + row]));
+  part[warp][lane] = mx;
+  __syncthreads();
+  if (warp == 0 && row < rpad) {
+#pragma unroll
+    for (int w = 1; w < 8; ++w) mx = fmax(mx, part[w][lane]);
     int ex = 0;
     if (mx > 0.0) {
       frexp(mx, &ex);   // mx = m 2^ex, m in [1/2, 1)
@@ -493,7 +503,7 @@ cudaError_t split_factor(cudaStream_t st, int mode, const double* F, int naux, i
   const long long chunks = (long long)f.rpad * f.nkt * (kb / 16);
   const int blocks = (int)std::min<long long>((chunks + 255) / 256, 148 * 16);
   if (mode == NW_TRANSFORM_CHOL_INT8) {
-    row_exponent_kernel<<<(f.rpad + 255) / 256, 256, 0, st>>>(F, naux, R, f.rpad, f.exps);
+    row_exponent_kernel<<<(f.rpad + 31) / 32, 256, 0, st>>>(F, naux, R, f.rpad, f.exps);
     int8_slices_kernel<<<blocks, 256, 0, st>>>(F, naux, R, f.rpad, f.nkt, f.exps, kOzakiSlices, f.piece_bytes,
                                                f.pieces);
   } else {
