@@ -48,7 +48,7 @@ __device__ __forceinline__ uint32_t classify_one(const EvalParams& P, uint2 ab, 
   const int la = (int)((dx >> 8) & 15) + (int)((dw >> 8) & 15), lb = (int)(dx >> 12) + (int)(dw >> 12);
   const int ord = __ldg(P.order + px * P.nref + pw);
   if (ord < 0) return kSkipKey;  // reference pair outside the resident block: left unwritten
-  return pair_sort_key(la, lb, ab.x, pw, ord, P.nfast, P.nref, P.nbucket, P.shift);
+  return pair_sort_key(la, lb, ab.x, pw, ord, P.nfast, P.ndet, P.nbucket, P.shift);
 }
 
 

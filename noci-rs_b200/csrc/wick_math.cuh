@@ -907,10 +907,13 @@ NW_HD int rank_class(int la, int lb) { return (la <= 4 && lb <= 4) ? la * 5 + lb
 
 // ---------------------------------------------------------------------------------------
 // Sort keys of the evaluation pipeline.  A pair of a fast reference pair (no zero-overlap
-// orbitals) gets  cls * nbucket + ((bra * nref + ket_parent) >> shift):  class-major, so each
-// evaluator kernel walks one contiguous range per class, and inside a class the pairs of one
-// bra determinant (and ket reference) lie together, so the lanes of a warp share the bra's
-// rows of the intermediates.  Pairs of reference pairs with zero-overlap orbitals follow,
+// orbitals) gets  cls * nbucket + ((ket_parent * ndet + bra) >> shift):  class-major, so each
+// evaluator kernel walks one contiguous range per class; inside a class the pairs of one ket
+// reference come together, ordered by bra (bras are numbered parent by parent), so the pairs
+// of one bra determinant lie together (the lanes of a warp share the bra's rows of the
+// intermediates) and the grid's window over the class stays inside one ordered reference pair
+// (x, w) at a time instead of spreading over the nref pairs (x, *) of the bra's parent -- a
+// working set nref times smaller in L2.  Pairs of reference pairs with zero-overlap orbitals follow,
 // keyed by (sort position - nfast, L_alpha, L_beta) with the full ranks 0..kML: their
 // distribution sums cost about L^7 per spin, so a warp whose lanes mixed ranks would run every
 // lane at the pace of its largest L.  Keys are < kRankClasses * nbucket + kGenClasses *
@@ -919,11 +922,11 @@ NW_HD int rank_class(int la, int lb) { return (la <= 4 && lb <= 4) ? la * 5 + lb
 constexpr int kRankClasses = 26;
 constexpr int kGenClasses = (kML + 1) * (kML + 1);
 
-NW_HD uint32_t pair_sort_key(int la, int lb, uint32_t bra, int ket_parent, int ord, int nfast, int nref,
+NW_HD uint32_t pair_sort_key(int la, int lb, uint32_t bra, int ket_parent, int ord, int nfast, uint64_t ndet,
                              uint32_t nbucket, int shift) {
   if (ord < nfast)
     return (uint32_t)rank_class(la, lb) * nbucket +
-           (uint32_t)((((uint64_t)bra * (uint64_t)nref) + ket_parent) >> shift);
+           (uint32_t)((((uint64_t)ket_parent * ndet) + bra) >> shift);
   return (uint32_t)kRankClasses * nbucket + (uint32_t)((ord - nfast) * kGenClasses + la * (kML + 1) + lb);
 }
 

@@ -133,7 +133,7 @@ uint64_t mir_sort_keys(const void* dets, uint64_t ndet, int nref, const int32_t*
       continue;
     }
     const int la = (int)((dx >> 8) & 15) + (int)((dw >> 8) & 15), lb = (int)(dx >> 12) + (int)(dw >> 12);
-    keys[i] = pair_sort_key(la, lb, pairs[2 * i], pw, order[px * nref + pw], nfast, nref, nb, s);
+    keys[i] = pair_sort_key(la, lb, pairs[2 * i], pw, order[px * nref + pw], nfast, ndet, nb, s);
   }
   return (uint64_t)kRankClasses * nb + (uint64_t)kGenClasses * ((uint64_t)nref * nref - nfast);
 }
