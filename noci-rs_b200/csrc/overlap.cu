@@ -22,9 +22,10 @@
 // parent's own alpha string with every beta string, is spread over many blocks that add into its
 // U row) with 256 target beta components per block, reading rows of B^{QP} stored source-major
 // (coalesced over bbar) with four independent loads in flight per thread; stage 2 is one thread
-// per target in sorted order, so the lanes of a warp share a_w (broadcast A reads) and read
-// neighbouring b_w of U (coalesced), with the (P, a) sum split into segments whose partial sums a
-// finishing kernel adds in a fixed order.  No allocation and no host synchronisation per apply,
+// per target in sorted order, reading A^{QP} stored source-major too, so for each source string a
+// the lanes of a warp read equal or neighbouring a_w of A and b_w of U (broadcast or coalesced),
+// with the (P, a) sum split into segments whose partial sums a finishing kernel adds in a fixed
+// order.  No allocation and no host synchronisation per apply,
 // so the QMC report block keeps it inside its CUDA graph.
 #include <cuda_runtime.h>
 
@@ -72,7 +73,7 @@ __global__ void __launch_bounds__(kOvlThreads) ovl_factor_kernel(const double* _
                                                                   const uint8_t* __restrict__ occ_t,
                                                                   const uint8_t* __restrict__ occ_s, int nocc,
                                                                   uint32_t nt, uint32_t ns, int source_major,
-                                                                  double* __restrict__ out) {
+                                                                  uint32_t ld, double* __restrict__ out) {
   const uint64_t total = (uint64_t)nt * ns;
   for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t i = (uint32_t)(e / ns), j = (uint32_t)(e % ns);
@@ -82,7 +83,7 @@ __global__ void __launch_bounds__(kOvlThreads) ovl_factor_kernel(const double* _
     for (int r = 0; r < nocc; ++r)
       for (int c = 0; c < nocc; ++c) m[r * nocc + c] = o[(uint64_t)oi[r] * nmo + oj[c]];
     const double d = det_lu_inplace(m, nocc);
-    out[source_major ? (uint64_t)j * nt + i : (uint64_t)i * ns + j] = d;
+    out[source_major ? (uint64_t)j * ld + i : (uint64_t)i * ns + j] = d;
   }
 }
 
@@ -95,20 +96,21 @@ __global__ void __launch_bounds__(kOvlThreads) ovl_gather_kernel(uint64_t ndet, 
 }
 
 // Clears the U rows that several chunks add into (blockIdx.x = row, blockIdx.y = 256 columns).
-__global__ void __launch_bounds__(kOvlThreads) ovl_zero_kernel(const uint64_t* __restrict__ urows, uint32_t nbq,
+__global__ void __launch_bounds__(kOvlThreads) ovl_zero_kernel(const uint64_t* __restrict__ urows, uint32_t ldb,
                                                                 double* __restrict__ u) {
   const uint32_t b = blockIdx.y * blockDim.x + threadIdx.x;
-  if (b < nbq) u[urows[blockIdx.x] + b] = 0.0;
+  if (b < ldb) u[urows[blockIdx.x] + b] = 0.0;
 }
 
-// U^{QP}[a][bbar] for the chunks of one group (blockIdx.x) and 256 target beta components
-// (blockIdx.y): every thread sums its column over the group's staged sources; the loads of one
-// chunk are independent (four in flight per step).
+// U^{QP}[a][bbar] for the chunks of one group (blockIdx.x) and 512 target beta components
+// (blockIdx.y), two neighbouring columns per thread (16-byte loads of rows of B^{QP} padded to an
+// even length ldb): every thread sums its columns over the group's staged sources; the loads of
+// one chunk are independent (four in flight per step).
 __global__ void __launch_bounds__(kOvlThreads) ovl_stage1_kernel(const OvlGroup* __restrict__ groups,
                                                                   const OvlChunk* __restrict__ chunks,
                                                                   const uint32_t* __restrict__ ord_b,
                                                                   const double* __restrict__ xs,
-                                                                  const double* __restrict__ fac, uint32_t nbq,
+                                                                  const double* __restrict__ fac, uint32_t ldb,
                                                                   double* __restrict__ u) {
   __shared__ double sx[kOvlGroup];
   __shared__ uint32_t sb[kOvlGroup];
@@ -118,40 +120,54 @@ __global__ void __launch_bounds__(kOvlThreads) ovl_stage1_kernel(const OvlGroup*
     sb[i] = ord_b[g.t0 + i];
   }
   __syncthreads();
-  const uint32_t bbar = blockIdx.y * blockDim.x + threadIdx.x;
-  if (bbar >= nbq) return;
+  const uint32_t col = 2 * (blockIdx.y * blockDim.x + threadIdx.x);
+  if (col >= ldb) return;
   for (uint32_t c = g.c0; c < g.c1; ++c) {
     const OvlChunk ch = chunks[c];
-    const double* bt = fac + ch.bt + bbar;
+    const double* bt = fac + ch.bt + col;
+    auto row = [&](uint32_t k) { return __ldg(reinterpret_cast<const double2*>(bt + (uint64_t)sb[k] * ldb)); };
     const uint32_t k1 = ch.t1 - g.t0;
     uint32_t k = ch.t0 - g.t0;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    double2 a0 = make_double2(0.0, 0.0), a1 = a0, a2 = a0, a3 = a0;
     for (; k + 4 <= k1; k += 4) {
-      const double b0 = __ldg(bt + (uint64_t)sb[k] * nbq), b1 = __ldg(bt + (uint64_t)sb[k + 1] * nbq);
-      const double b2 = __ldg(bt + (uint64_t)sb[k + 2] * nbq), b3 = __ldg(bt + (uint64_t)sb[k + 3] * nbq);
-      a0 += sx[k] * b0;
-      a1 += sx[k + 1] * b1;
-      a2 += sx[k + 2] * b2;
-      a3 += sx[k + 3] * b3;
+      const double2 b0 = row(k), b1 = row(k + 1), b2 = row(k + 2), b3 = row(k + 3);
+      a0.x += sx[k] * b0.x;
+      a0.y += sx[k] * b0.y;
+      a1.x += sx[k + 1] * b1.x;
+      a1.y += sx[k + 1] * b1.y;
+      a2.x += sx[k + 2] * b2.x;
+      a2.y += sx[k + 2] * b2.y;
+      a3.x += sx[k + 3] * b3.x;
+      a3.y += sx[k + 3] * b3.y;
     }
-    for (; k < k1; ++k) a0 += sx[k] * __ldg(bt + (uint64_t)sb[k] * nbq);
-    const double sum = (a0 + a1) + (a2 + a3);
-    if (ch.atomic)
-      atomicAdd(u + ch.urow + bbar, sum);
-    else
-      u[ch.urow + bbar] = sum;
+    for (; k < k1; ++k) {
+      const double2 b0 = row(k);
+      a0.x += sx[k] * b0.x;
+      a0.y += sx[k] * b0.y;
+    }
+    const double s0 = (a0.x + a1.x) + (a2.x + a3.x), s1 = (a0.y + a1.y) + (a2.y + a3.y);
+    double* dst = u + ch.urow + col;
+    if (ch.atomic) {
+      atomicAdd(dst, s0);
+      atomicAdd(dst + 1, s1);
+    } else {
+      *reinterpret_cast<double2*>(dst) = make_double2(s0, s1);
+    }
   }
 }
 
 // Partial sums over segment blockIdx.y of the (P, a) index of every target t in [t0, t1) of
-// parent q: part[seg][t] = sum A^{qP}[a_t][a] U^{qP}[a][b_t].
+// parent q: part[seg][t] = sum A^{qP}[a_t][a] U^{qP}[a][b_t].  A is stored source-major
+// (row a holds the na_q targets' strings), so for a fixed a the lanes of a warp read
+// neighbouring or equal a_t (one run of a string's targets, or the doubly excited strings one
+// target each) as they read neighbouring or equal b_t of U: both loads coalesce or broadcast.
 __global__ void __launch_bounds__(kOvlThreads) ovl_stage2_kernel(int q, int nref, uint64_t t0, uint64_t t1,
                                                                   uint64_t seglen, const uint32_t* __restrict__ ord_a,
                                                                   const uint32_t* __restrict__ ord_b,
                                                                   const uint32_t* __restrict__ na,
                                                                   const uint64_t* __restrict__ a_off,
-                                                                  const uint64_t* __restrict__ u_off, uint32_t nbq,
-                                                                  const double* __restrict__ fac,
+                                                                  const uint64_t* __restrict__ u_off, uint32_t naq,
+                                                                  uint32_t ldb, const double* __restrict__ fac,
                                                                   const double* __restrict__ u, uint64_t ndet,
                                                                   double* __restrict__ part) {
   const uint64_t t = t0 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -167,19 +183,19 @@ __global__ void __launch_bounds__(kOvlThreads) ovl_stage2_kernel(int q, int nref
     const uint64_t hi = k1 < kbase + n ? k1 : kbase + n;
     if (lo < hi) {
       // a = k - kbase runs over [lo - kbase, hi - kbase) of this parent's alpha components
-      const double* arow = fac + a_off[(uint64_t)q * nref + p] + (uint64_t)at * n;
+      const double* acol = fac + a_off[(uint64_t)q * nref + p] + at;
       const double* ucol = u + u_off[(uint64_t)q * nref + p] + bq;
       const uint64_t a1 = hi - kbase;
       uint64_t a = lo - kbase;
       for (; a + 4 <= a1; a += 4) {
-        const double u0 = __ldg(ucol + a * nbq), u1 = __ldg(ucol + (a + 1) * nbq);
-        const double u2 = __ldg(ucol + (a + 2) * nbq), u3 = __ldg(ucol + (a + 3) * nbq);
-        acc0 += __ldg(arow + a) * u0;
-        acc1 += __ldg(arow + a + 1) * u1;
-        acc2 += __ldg(arow + a + 2) * u2;
-        acc3 += __ldg(arow + a + 3) * u3;
+        const double u0 = __ldg(ucol + a * ldb), u1 = __ldg(ucol + (a + 1) * ldb);
+        const double u2 = __ldg(ucol + (a + 2) * ldb), u3 = __ldg(ucol + (a + 3) * ldb);
+        acc0 += __ldg(acol + a * naq) * u0;
+        acc1 += __ldg(acol + (a + 1) * naq) * u1;
+        acc2 += __ldg(acol + (a + 2) * naq) * u2;
+        acc3 += __ldg(acol + (a + 3) * naq) * u3;
       }
-      for (; a < a1; ++a) acc0 += __ldg(arow + a) * __ldg(ucol + a * nbq);
+      for (; a < a1; ++a) acc0 += __ldg(acol + a * naq) * __ldg(ucol + a * ldb);
     }
     kbase += n;
   }
@@ -254,6 +270,7 @@ struct OverlapPlan {
   uint64_t ndet = 0;
   int nseg = 1;
   std::vector<uint32_t> na, nb;
+  std::vector<uint32_t> ldb;            // beta strings per parent rounded up to even: row stride of B and U
   std::vector<uint64_t> pstart;         // per parent: first sorted position (nref + 1)
   std::vector<uint64_t> ngroups, groups_off;  // per target parent: stage-1 groups
   std::vector<uint64_t> nzero, zero_off;      // per target parent: U rows cleared before stage 1
@@ -319,10 +336,12 @@ nw_status overlap_plan_get(nw_ctx* ctx, cudaStream_t stream, OverlapPlan** out) 
   }
   pl->na.resize(nref);
   pl->nb.resize(nref);
+  pl->ldb.resize(nref);
   std::vector<uint64_t> ca_off(nref + 1, 0), cb_off(nref + 1, 0);
   for (int p = 0; p < nref; ++p) {
     pl->na[p] = (uint32_t)ca[p].size();
     pl->nb[p] = (uint32_t)cb[p].size();
+    pl->ldb[p] = (pl->nb[p] + 1) & ~1u;
     ca_off[p + 1] = ca_off[p] + pl->na[p];
     cb_off[p + 1] = cb_off[p] + pl->nb[p];
   }
@@ -403,14 +422,15 @@ nw_status overlap_plan_get(nw_ctx* ctx, cudaStream_t stream, OverlapPlan** out) 
       const size_t i = (size_t)q * nref + p;
       a_off[i] = nfac;
       nfac += (uint64_t)pl->na[q] * pl->na[p];
+      nfac = (nfac + 1) & ~1ull;  // 16-byte aligned rows of B
       bt_off[i] = nfac;
-      nfac += (uint64_t)pl->nb[p] * pl->nb[q];
+      nfac += (uint64_t)pl->nb[p] * pl->ldb[q];
       u_off[i] = uq;
       // chunks of the rows of P in sorted order, grouped (a group never spans two parents)
       bool open = false;
       for (uint32_t a = 0; a < pl->na[p]; ++a) {
         const uint64_t r0 = rowstart[ca_off[p] + a], r1 = rowstart[ca_off[p] + a + 1];
-        const uint64_t urow = uq + (uint64_t)a * pl->nb[q];
+        const uint64_t urow = uq + (uint64_t)a * pl->ldb[q];
         const bool multi = r1 - r0 > kOvlChunk;
         if (multi) zero_rows.push_back(urow);
         for (uint64_t c0 = r0; c0 < r1; c0 += kOvlChunk) {
@@ -424,7 +444,7 @@ nw_status overlap_plan_get(nw_ctx* ctx, cudaStream_t stream, OverlapPlan** out) 
           groups.back().t1 = (uint32_t)c1;
         }
       }
-      uq += (uint64_t)pl->na[p] * pl->nb[q];
+      uq += (uint64_t)pl->na[p] * pl->ldb[q];
       kq += pl->na[p];
     }
     pl->ngroups[q] = groups.size() - pl->groups_off[q];
@@ -486,7 +506,9 @@ nw_status overlap_plan_get(nw_ctx* ctx, cudaStream_t stream, OverlapPlan** out) 
   auto up = [&](void* dst, const void* src, size_t bytes) {
     return bytes == 0 || cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream) == cudaSuccess;
   };
-  bool ok = up(pl->ord_det, order.data(), nd * 4) && up(pl->ord_a, o_a.data(), nd * 4) &&
+  // the padding column of an odd-length B row is summed by stage 1 into a U column nobody reads
+  bool ok = cudaMemsetAsync(pl->fac, 0, std::max<uint64_t>(1, nfac) * 8, stream) == cudaSuccess &&
+            up(pl->ord_det, order.data(), nd * 4) && up(pl->ord_a, o_a.data(), nd * 4) &&
             up(pl->ord_b, o_b.data(), nd * 4) && up(pl->ord_r, o_r.data(), nd * 8) &&
             up(pl->groups, groups.data(), groups.size() * sizeof(OvlGroup)) &&
             up(pl->chunks, chunks.data(), chunks.size() * sizeof(OvlChunk)) &&
@@ -506,25 +528,24 @@ nw_status overlap_plan_get(nw_ctx* ctx, cudaStream_t stream, OverlapPlan** out) 
                          d_o + ((size_t)spin * nrr + (size_t)q * nref) * n2, nmo, (long long)n2, nref) == cudaSuccess;
   }
   auto factors = [&](const double* o, const uint8_t* ot, const uint8_t* os, int nocc, uint32_t nt, uint32_t ns,
-                     int source_major, double* out) {
+                     uint32_t ld, double* out) {
     const uint64_t e = (uint64_t)nt * ns;
     if (e == 0) return;
     if (nocc <= 4)
-      ovl_factor_kernel<4><<<grid_of(e), kOvlThreads, 0, stream>>>(o, nmo, ot, os, nocc, nt, ns, source_major, out);
+      ovl_factor_kernel<4><<<grid_of(e), kOvlThreads, 0, stream>>>(o, nmo, ot, os, nocc, nt, ns, 1, ld, out);
     else if (nocc <= 8)
-      ovl_factor_kernel<8><<<grid_of(e), kOvlThreads, 0, stream>>>(o, nmo, ot, os, nocc, nt, ns, source_major, out);
+      ovl_factor_kernel<8><<<grid_of(e), kOvlThreads, 0, stream>>>(o, nmo, ot, os, nocc, nt, ns, 1, ld, out);
     else
-      ovl_factor_kernel<kOvlMaxOcc><<<grid_of(e), kOvlThreads, 0, stream>>>(o, nmo, ot, os, nocc, nt, ns, source_major,
-                                                                            out);
+      ovl_factor_kernel<kOvlMaxOcc><<<grid_of(e), kOvlThreads, 0, stream>>>(o, nmo, ot, os, nocc, nt, ns, 1, ld, out);
   };
   for (int q = 0; ok && q < nref; ++q)
     for (int p = 0; ok && p < nref; ++p) {
       if (p == q) continue;
       const size_t i = (size_t)q * nref + p;
-      factors(d_o + i * n2, d_occa + ca_off[q] * pl->oa, d_occa + ca_off[p] * pl->oa, pl->oa, pl->na[q], pl->na[p], 0,
-              pl->fac + a_off[i]);
+      factors(d_o + i * n2, d_occa + ca_off[q] * pl->oa, d_occa + ca_off[p] * pl->oa, pl->oa, pl->na[q], pl->na[p],
+              pl->na[q], pl->fac + a_off[i]);
       factors(d_o + (nrr + i) * n2, d_occb + cb_off[q] * pl->ob, d_occb + cb_off[p] * pl->ob, pl->ob, pl->nb[q],
-              pl->nb[p], 1, pl->fac + bt_off[i]);
+              pl->nb[p], pl->ldb[q], pl->fac + bt_off[i]);
       ok = cudaGetLastError() == cudaSuccess;
     }
   if (ok) ok = cudaStreamSynchronize(stream) == cudaSuccess;
@@ -544,17 +565,17 @@ nw_status overlap_apply(nw_ctx* ctx, const OverlapPlan* pl, const double* x, dou
   for (int q = 0; cross && q < pl->nref; ++q) {
     const uint64_t t0 = pl->pstart[q], t1 = pl->pstart[q + 1];
     if (t1 == t0) continue;
-    const uint32_t nbq = pl->nb[q];
-    const unsigned ycols = (nbq + kOvlThreads - 1) / kOvlThreads;
+    const uint32_t ldb = pl->ldb[q];
     if (pl->nzero[q] > 0)
-      ovl_zero_kernel<<<dim3((unsigned)pl->nzero[q], ycols), kOvlThreads, 0, stream>>>(pl->zero_rows + pl->zero_off[q],
-                                                                                      nbq, pl->u);
+      ovl_zero_kernel<<<dim3((unsigned)pl->nzero[q], (ldb + kOvlThreads - 1) / kOvlThreads), kOvlThreads, 0, stream>>>(
+          pl->zero_rows + pl->zero_off[q], ldb, pl->u);
     if (pl->ngroups[q] > 0)
-      ovl_stage1_kernel<<<dim3((unsigned)pl->ngroups[q], ycols), kOvlThreads, 0, stream>>>(
-          pl->groups + pl->groups_off[q], pl->chunks, pl->ord_b, pl->xs, pl->fac, nbq, pl->u);
+      ovl_stage1_kernel<<<dim3((unsigned)pl->ngroups[q], (ldb + 2 * kOvlThreads - 1) / (2 * kOvlThreads)), kOvlThreads, 0,
+                          stream>>>(pl->groups + pl->groups_off[q], pl->chunks, pl->ord_b, pl->xs, pl->fac, ldb, pl->u);
     const dim3 g2((unsigned)((t1 - t0 + kOvlThreads - 1) / kOvlThreads), (unsigned)pl->nseg);
     ovl_stage2_kernel<<<g2, kOvlThreads, 0, stream>>>(q, pl->nref, t0, t1, pl->seglen[q], pl->ord_a, pl->ord_b,
-                                                      pl->d_na, pl->d_a_off, pl->d_u_off, nbq, pl->fac, pl->u, nd,
+                                                      pl->d_na, pl->d_a_off, pl->d_u_off, pl->na[q], ldb, pl->fac,
+                                                      pl->u, nd,
                                                       pl->part);
   }
   ovl_finish_kernel<<<grid_of(nd), kOvlThreads, 0, stream>>>(nd, pl->nseg, cross, pl->ord_det, pl->ord_r, pl->run_lo,

@@ -206,3 +206,25 @@ def test_direct_overlap_run_approaches_ground_state():
     mean = rep["eproj_num"][tail].sum() / rep["eproj_den"][tail].sum()
     err = blocks.std(ddof=1) / np.sqrt(len(blocks))
     assert abs(mean - e_det) < 5 * err + 5e-4, (mean, e_det, e0, err)
+
+
+def test_overlap_action_single_parent_and_missing_parent():
+    """One reference (only the orthonormal same-parent block) and a basis in which a middle
+    reference has no determinants (empty parent blocks on both sides of the contraction)."""
+    rng = np.random.default_rng(5)
+    one = sy.make_system(8, 2, 2, 1, 12, seed=2, k_scale=0.3)
+    b1 = sy.sd_basis(8, 2, 2, 1)
+    with nociwick.WicksShared(one.s, one.h, one.eri, one.enuc, one.refs, tol=1e-8) as w:
+        w.build().set_basis(b1)
+        x = rng.standard_normal(b1.shape[0])
+        y = _apply(w, x)
+    assert np.abs(y - x).max() <= 1e-15 * np.abs(x).max()
+    three = sy.make_system(8, 2, 2, 3, 12, seed=9, k_scale=0.3)
+    b3 = sy.sd_basis(8, 2, 2, 3)
+    b3 = b3[b3["parent"] != 1]
+    with nociwick.WicksShared(three.s, three.h, three.eri, three.enuc, three.refs, tol=1e-8) as w:
+        w.build().set_basis(b3)
+        _, s = w.build_hs_matrix()
+        x = rng.standard_normal(b3.shape[0])
+        y = _apply(w, x)
+    assert np.abs(y - s @ x).max() <= 1e-13 * np.abs(s).max() * np.abs(x).sum()
