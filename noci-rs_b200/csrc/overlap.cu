@@ -76,7 +76,9 @@ __global__ void __launch_bounds__(kOvlThreads) ovl_factor_kernel(const double* _
                                                                   uint32_t ld, double* __restrict__ out) {
   const uint64_t total = (uint64_t)nt * ns;
   for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t i = (uint32_t)(e / ns), j = (uint32_t)(e % ns);
+    // consecutive threads write consecutive entries of the output row
+    const uint32_t i = source_major ? (uint32_t)(e % nt) : (uint32_t)(e / ns);
+    const uint32_t j = source_major ? (uint32_t)(e / nt) : (uint32_t)(e % ns);
     const uint8_t* oi = occ_t + (uint64_t)i * nocc;
     const uint8_t* oj = occ_s + (uint64_t)j * nocc;
     double m[MAXO * MAXO];
