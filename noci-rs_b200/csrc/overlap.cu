@@ -234,9 +234,9 @@ inline int grid_of(uint64_t work) {
 // Fermionic sign of the excitation (excitation_phase_bits, src/basis/excitation.rs:110-146):
 // holes removed from the highest down, particles added from the lowest up, each contributing
 // the parity of the occupied orbitals below it.
-double excitation_sign(int nocc, int nmo, int rank, const uint8_t* idx) {
-  std::vector<char> occ(std::max(nmo, nocc) + 1, 0);
-  for (int i = 0; i < nocc; ++i) occ[i] = 1;
+double excitation_sign(int nocc, int rank, const uint8_t* idx) {
+  char occ[256] = {};  // orbital indices are bytes
+  for (int i = 0; i < nocc && i < 256; ++i) occ[i] = 1;
   auto below = [&](int p) {
     int c = 0;
     for (int i = 0; i < p; ++i) c += occ[i];
@@ -333,8 +333,7 @@ nw_status overlap_plan_get(nw_ctx* ctx, cudaStream_t stream, OverlapPlan** out) 
     auto ib = cb[r.parent].emplace(kb, (uint32_t)cb[r.parent].size()).first;
     aid[d] = ia->second;
     bid[d] = ib->second;
-    rr[d] = r.phase * excitation_sign(ctx->nocc_a, nmo, r.rank_a, r.idx_a) *
-            excitation_sign(ctx->nocc_b, nmo, r.rank_b, r.idx_b);
+    rr[d] = r.phase * excitation_sign(ctx->nocc_a, r.rank_a, r.idx_a) * excitation_sign(ctx->nocc_b, r.rank_b, r.idx_b);
   }
   pl->na.resize(nref);
   pl->nb.resize(nref);

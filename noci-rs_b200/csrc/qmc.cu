@@ -169,11 +169,24 @@ __global__ void qmc_owners_kernel(QmcParams q, QmcState* __restrict__ st, const 
     st->cycle_cur = st->cycle;
     st->cycle += 1;
   }
+  // a warp takes 32 determinants and writes each one's chunk range with all its lanes, so a
+  // determinant holding many chunks (a heavily populated reference) is not one thread's loop
   const uint64_t last = q.cap >> kChunkShift;  // cown holds chunks 0 .. last (+1 spare)
-  for (uint64_t d = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; d < q.ndet; d += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t lo = off[d], hi = off[d + 1];
-    for (uint64_t c = (lo + (1u << kChunkShift) - 1) >> kChunkShift; (c << kChunkShift) < hi && c <= last; ++c)
-      cown[c] = (uint32_t)d;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t base = ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5) << 5; base < q.ndet;
+       base += nwarps << 5) {
+    const uint64_t d = base + lane;
+    uint64_t c0 = 0, c1 = 0;  // chunks c with off[d] <= c 2^kChunkShift < off[d + 1]
+    if (d < q.ndet) {
+      c0 = ((uint64_t)off[d] + (1u << kChunkShift) - 1) >> kChunkShift;
+      c1 = ((uint64_t)off[d + 1] + (1u << kChunkShift) - 1) >> kChunkShift;
+      if (c1 > last + 1) c1 = last + 1;
+    }
+    for (int j = 0; j < 32; ++j) {
+      const uint64_t a = __shfl_sync(0xFFFFFFFFu, c0, j), b = __shfl_sync(0xFFFFFFFFu, c1, j);
+      for (uint64_t c = a + lane; c < b; c += 32) cown[c] = (uint32_t)(base + j);
+    }
   }
 }
 
