@@ -20,6 +20,7 @@ namespace {
 constexpr int kT = 64;   // output tile
 constexpr int kL = 16;   // reduction chunk
 constexpr int kSplitMax = 32;  // k-split blocks of a weight-gradient product
+constexpr int kPrefetch = 8;   // reduction chunks whose panels one block loads at once
 
 __device__ __forceinline__ float to_f(float v) { return v; }
 __device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
@@ -66,14 +67,32 @@ __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int L, const fl
   for (int j = 0; j < 4; ++j)
 #pragma unroll
     for (int e = 0; e < 4; ++e) acc[j][e] = 0.0f;
-  for (int l0 = lbeg; l0 < lend; l0 += kL) {
-    for (int e = threadIdx.x; e < kT * kL; e += 256) {
-      const int r = e / kL, c = e % kL, gr = row0 + r, gc = l0 + c;
-      As[c][r] = (gr < M && gc < lend) ? A[gr * asr + gc * asc] : 0.0f;
+  // The panels of up to kPrefetch chunks are loaded into registers at once (every load in
+  // flight together: one memory latency per kPrefetch chunks instead of one per chunk, which
+  // set the pace of these small products), then staged chunk by chunk.
+  constexpr int kPer = kT * kL / 256;  // elements of a panel per thread and chunk (4)
+  for (int p0 = lbeg; p0 < lend; p0 += kL * kPrefetch) {
+    float ra[kPrefetch][kPer], rb[kPrefetch][kPer];
+#pragma unroll
+    for (int ch = 0; ch < kPrefetch; ++ch) {
+      const int l0 = p0 + ch * kL;
+#pragma unroll
+      for (int i = 0; i < kPer; ++i) {
+        const int e = threadIdx.x + 256 * i;
+        const int ar = e / kL, ac = e % kL, agr = row0 + ar, agc = l0 + ac;
+        ra[ch][i] = (agr < M && agc < lend) ? A[agr * asr + agc * asc] : 0.0f;
+        const int br = e / kT, bc = e % kT, bgr = l0 + br, bgc = col0 + bc;
+        rb[ch][i] = (bgr < lend && bgc < N) ? to_f(B[bgr * bsr + bgc * bsc]) : 0.0f;
+      }
     }
-    for (int e = threadIdx.x; e < kT * kL; e += 256) {
-      const int r = e / kT, c = e % kT, gr = l0 + r, gc = col0 + c;
-      Bs[r][c] = (gr < lend && gc < N) ? to_f(B[gr * bsr + gc * bsc]) : 0.0f;
+#pragma unroll
+    for (int ch = 0; ch < kPrefetch; ++ch) {
+    if (p0 + ch * kL >= lend) break;  // block-uniform
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int e = threadIdx.x + 256 * i;
+      As[e % kL][e / kL] = ra[ch][i];
+      Bs[e / kT][e % kT] = rb[ch][i];
     }
     __syncthreads();
 #pragma unroll
@@ -94,6 +113,7 @@ __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int L, const fl
       }
     }
     __syncthreads();
+    }
   }
 #pragma unroll
   for (int j = 0; j < 4; ++j)
