@@ -117,7 +117,7 @@ EVAL_L1TEX = {
 }
 EVAL_TRAFFIC = {
     ("config2", 10_000_000): (1_438_561_280, "profiles/eval_traffic_config2_10Mpairs.md"),
-    ("config3", 100_000_000): (63_536_004_352, "profiles/eval_traffic_config3_100Mpairs.md"),
+    ("config3", 100_000_000): (59_238_853_120, "profiles/eval_traffic_config3_100Mpairs.md"),
 }
 
 
