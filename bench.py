@@ -116,7 +116,7 @@ EVAL_L1TEX = {
                 "profiles/eval_pipeline_config2_4Mpairs_ncu.md"),
 }
 EVAL_TRAFFIC = {
-    ("config2", 10_000_000): (1_438_561_280, "profiles/eval_traffic_config2_10Mpairs.md"),
+    ("config2", 10_000_000): (1_446_515_712, "profiles/eval_traffic_config2_10Mpairs.md"),
     ("config3", 100_000_000): (59_238_853_120, "profiles/eval_traffic_config3_100Mpairs.md"),
 }
 
