@@ -3,8 +3,8 @@
 // Pipeline for one request batch (all on one stream, no host synchronisation):
 //   1. classify: read each pair's two 16-bit determinant descriptors (the full 32-byte records
 //      only for same-parent pairs, which get exact zeros when more than a double excitation
-//      apart, noci-rs hs.rs:96-101), key every other pair by (contraction-rank class, bra
-//      determinant, ket reference) -- pair_sort_key -- and take its rank within the key from a
+//      apart, noci-rs hs.rs:96-101), key every other pair by (contraction-rank class, ket
+//      reference, bra determinant) -- pair_sort_key -- and take its rank within the key from a
 //      global per-key counter;
 //   2. scan the per-key counts (two passes over tiles);
 //   3. scatter each pair's request index to offsets[key] + rank;
