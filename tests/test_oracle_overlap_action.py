@@ -80,3 +80,38 @@ def test_direct_overlap_report_applies_the_overlap():
     assert abs(rep["nw"] - np.abs(q.pop).sum()) < 1e-9
     with pytest.raises(ValueError):
         OracleQmc(orc, ob, c0, refs, dt=0.01, propagator="direct-overlap")
+
+
+def test_direct_overlap_report_is_unbiased_in_the_oracle():
+    """The oracle's direct-overlap report from fixed populations N changes them, on average over
+    independent reports, by S (-dt (H - E_s S) N): FRI sampling, uniform spawning, spawn
+    rounding and the FRI-compressed update all keep the expectation (z < 6 per determinant)."""
+    system = sy.make_system(6, 2, 2, 2, 10, seed=4, k_scale=0.3)
+    basis = sy.sd_basis(6, 2, 2, 2)
+    n = basis.shape[0]
+    orc = Oracle.from_system(system, tol=1e-8)
+    ob = orc.oracle_basis(basis)
+    g = np.arange(n)
+    pairs = np.stack(np.meshgrid(g, g, indexing="ij"), -1).reshape(-1, 2)
+    h, s = orc.eval_pairs(ob, pairs)
+    h, s = h.reshape(n, n), s.reshape(n, n)
+    f = OverlapFactorisation(system.s, system.refs, 2, 2, basis)
+    refs = np.nonzero((basis["rank_a"] == 0) & (basis["rank_b"] == 0))[0]
+    c0 = np.zeros(n)
+    c0[refs] = 1.0
+    es, dt = -2.0, 0.01
+    q = OracleQmc(orc, ob, c0, refs, dt=dt, initial_population=60.0, sampling_cutoff=0.5, spawn_cutoff=0.05,
+                  initial_shift=es, ncycles=1, propagator="direct-overlap", overlap=f.apply, seed=11,
+                  update_cutoff=0.05, target_population=1e9)
+    pop = np.random.default_rng(3).normal(0.0, 1.0, n) * (np.random.default_rng(4).random(n) < 0.4)
+    reps = 1500
+    d = np.empty((reps, n))
+    for k in range(reps):
+        q.pop = pop.copy()
+        q.report()
+        d[k] = q.pop - pop
+    expected = s @ (-dt * (h - es * s) @ pop)
+    mean, se = d.mean(axis=0), d.std(axis=0, ddof=1) / np.sqrt(reps)
+    live = se > 1e-12
+    assert np.all(np.abs(mean[~live] - expected[~live]) < 1e-12)
+    assert np.max(np.abs(mean[live] - expected[live]) / se[live]) < 6.0
