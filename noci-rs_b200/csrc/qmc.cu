@@ -124,9 +124,12 @@ T* dalloc(size_t count, bool* ok) {
   return static_cast<T*>(p);
 }
 
+// Per determinant: the sampled population, its attempt count and the amplitude n~ / attempts
+// that each of its attempts carries (one division per determinant, read by the apply kernel
+// through the attempt's parent).
 __global__ void qmc_sample_kernel(QmcParams q, QmcState* __restrict__ st, const double* __restrict__ pop,
                                   const double2* __restrict__ diag, double* __restrict__ sampled,
-                                  uint32_t* __restrict__ na, double* __restrict__ delta) {
+                                  uint32_t* __restrict__ na, double* __restrict__ amp, double* __restrict__ delta) {
   const uint64_t cycle = st->cycle;
   const double es = st->shift;
   unsigned long long sum = 0ull;
@@ -136,7 +139,9 @@ __global__ void qmc_sample_kernel(QmcParams q, QmcState* __restrict__ st, const 
     if (p != 0.0) n = nwq::fri(p, q.c_sample, nwq::uniform1(q.seed, cycle, d, nwq::kDrawSample));
     sampled[d] = n;
     const uint64_t a = nwq::attempts(n);
-    na[d] = a > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)a;
+    const uint32_t a32 = a > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)a;
+    na[d] = a32;
+    amp[d] = n != 0.0 ? n / (double)a32 : 0.0;
     sum += a;
     if (n != 0.0) {
       const double2 hs = diag[d];
@@ -191,15 +196,14 @@ __global__ void qmc_owners_kernel(QmcParams q, QmcState* __restrict__ st, const 
 }
 
 // Spawn attempts and classify their pairs for the sorted evaluation in one pass: the child
-// of every attempt, its pair, amplitude and generation probability, then the pair's sort key
+// of every attempt, its pair, parent and generation probability, then the pair's sort key
 // (nw::classify_one) and its rank within the key, taken warp-aggregated from the per-key
 // counters (attempts of one parent share keys).  The loop is warp-uniform (its trip count
 // depends on the warp's first attempt only), so every lane reaches the full-mask intrinsics.
 __global__ void qmc_spawn_kernel(QmcParams q, Proposal pr, nw::EvalParams P, const QmcState* __restrict__ st,
                                  const uint32_t* __restrict__ off, const uint32_t* __restrict__ cown,
-                                 const double* __restrict__ sampled,
-                                 const uint32_t* __restrict__ na, uint2* __restrict__ pairs, uint32_t* __restrict__ child,
-                                 uint32_t* __restrict__ parent, double* __restrict__ amp, double* __restrict__ pg,
+                                 uint2* __restrict__ pairs, uint32_t* __restrict__ child,
+                                 uint32_t* __restrict__ parent, double* __restrict__ pg,
                                  uint32_t* __restrict__ keys, uint32_t* __restrict__ ranks,
                                  uint32_t* __restrict__ counts, double* __restrict__ hs, uint32_t* __restrict__ flag) {
   const uint32_t n = st->npairs;
@@ -270,7 +274,6 @@ __global__ void qmc_spawn_kernel(QmcParams q, Proposal pr, nw::EvalParams P, con
       pairs[t] = ab;
       child[t] = (uint32_t)lam;
       parent[t] = (uint32_t)g;
-      amp[t] = sampled[g] / (double)na[g];
       key = nw::classify_one(P, ab, t, hs, 2, flag);
     }
     const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
@@ -296,7 +299,7 @@ __global__ void qmc_apply_kernel(QmcParams q, Proposal pr, const QmcState* __res
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const double2 v = hs[t];
     const double pgen = q.gen == 0 ? pu : pg[t];
-    const double raw = nwq::spawn_amplitude(q.prop, q.dt, es, v.x, v.y, amp[t], pgen);
+    const double raw = nwq::spawn_amplitude(q.prop, q.dt, es, v.x, v.y, amp[parent[t]], pgen);
     const double dn = nwq::fri(raw, q.c_spawn, nwq::uniform1(q.seed, cycle, t, nwq::kDrawSpawn));
     if (dn != 0.0) atomicAdd(delta + child[t], dn);
     if (q.harvest && (q.hkeep >= 1.0 || nwq::uniform1(q.seed, cycle, t, nwq::kDrawHarvest) < q.hkeep)) {
@@ -519,7 +522,7 @@ struct nw_qmc {
   uint8_t* isref = nullptr;
   uint2* pairs = nullptr;
   uint32_t* child = nullptr;
-  double* amp = nullptr;
+  double* amp = nullptr;     // per determinant: n~ / attempts of the current cycle
   uint32_t* parent = nullptr;
   double* pg = nullptr;
   double2* hs = nullptr;
@@ -555,14 +558,15 @@ nw_status enqueue_cycle(nw_qmc* q) {
   nw_ctx* ctx = q->ctx;
   const cudaStream_t s = q->stream;
   const uint64_t nd = q->q.ndet;
-  qmc_sample_kernel<<<grid_for(nd), kBlockThreads, 0, s>>>(q->q, q->st, q->pop, q->diag, q->sampled, q->na, q->delta);
+  qmc_sample_kernel<<<grid_for(nd), kBlockThreads, 0, s>>>(q->q, q->st, q->pop, q->diag, q->sampled, q->na, q->amp,
+                                                          q->delta);
   NW_CUDA(ctx, cudaGetLastError());
   nw_status st = nw::scan_exclusive(ctx, q->na, nd, q->off, q->tsum, s);
   if (st != NW_OK) return st;
   qmc_owners_kernel<<<grid_for(nd), kBlockThreads, 0, s>>>(q->q, q->st, q->off, q->cown);
   NW_CUDA(ctx, cudaMemsetAsync(q->S.counts, 0, sizeof(uint32_t) * q->nkeys, s));
   qmc_spawn_kernel<<<grid_for(q->q.cap), kBlockThreads, 0, s>>>(
-      q->q, q->pr, q->P, q->st, q->off, q->cown, q->sampled, q->na, q->pairs, q->child, q->parent, q->amp, q->pg,
+      q->q, q->pr, q->P, q->st, q->off, q->cown, q->pairs, q->child, q->parent, q->pg,
       q->S.keys, q->S.ranks, q->S.counts, reinterpret_cast<double*>(q->hs), q->S.flag);
   NW_CUDA(ctx, cudaGetLastError());
   st = nw::launch_sorted(ctx, q->P, q->nkeys, reinterpret_cast<const uint32_t*>(q->pairs), q->q.cap,
@@ -859,7 +863,7 @@ nw_status nw_qmc_create(nw_ctx* ctx, const nw_qmc_opts* opts, const double* c0, 
   take(q->isref, nd);
   take(q->pairs, std::max<uint64_t>(cap, nd));
   take(q->child, cap);
-  take(q->amp, cap);
+  take(q->amp, nd);
   take(q->parent, cap);
   take(q->pg, cap);
   take(q->hs, std::max<uint64_t>(cap, nd));
