@@ -85,6 +85,12 @@ class WicksShared {
     return out;
   }
 
+  // y += S x over the resident basis (device buffers of ndet doubles; the first call on a basis
+  // builds the spin-factor tables; apply_overlap_sparse, src/noci/factorise/overlap.rs:434-498).
+  void apply_overlap_device(const double* x_dev, double* y_dev, void* stream) {
+    check(nw_apply_overlap_device(ctx_, x_dev, y_dev, stream), "nw_apply_overlap_device");
+  }
+
   std::vector<int32_t> zero_counts(int nref) const {
     std::vector<int32_t> m(2 * (size_t)nref * nref);
     check(nw_pair_zero_counts(ctx_, m.data()), "nw_pair_zero_counts");
