@@ -1019,7 +1019,7 @@ def direct_overlap_leg(args, w, c0, refs, e_ref, walkers, rank, local_rank, dist
     import nociwick
     nd = c0.shape[0]
     dev = f"cuda:{local_rank}"
-    x = torch.randn(nd, dtype=torch.float64, device=dev)
+    x = torch.randn(nd, dtype=torch.float64, device=dev, generator=torch.Generator(device=dev).manual_seed(rank_seed(77, rank)))
     y = torch.zeros(nd, dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
     torch.cuda.synchronize(dev)
