@@ -429,13 +429,13 @@ __global__ void gather_batch_kernel(const HarvestSample* __restrict__ samples, u
   w[r] = h.w;
 }
 
-__global__ void sum_kernel(const float* __restrict__ w, int B, float* __restrict__ out) {
-  __shared__ float red[256];
+__global__ void __launch_bounds__(1024) sum_kernel(const float* __restrict__ w, int B, float* __restrict__ out) {
+  __shared__ float red[1024];
   float a = 0.0f;
   for (int r = threadIdx.x; r < B; r += blockDim.x) a += w[r];
   red[threadIdx.x] = a;
   __syncthreads();
-  for (int k = 128; k > 0; k >>= 1) {
+  for (int k = 512; k > 0; k >>= 1) {
     if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
     __syncthreads();
   }
@@ -443,27 +443,48 @@ __global__ void sum_kernel(const float* __restrict__ w, int B, float* __restrict
 }
 
 // Softmax over the bins that hold a child of the row's parent; in place, z becomes
-// dL/dz of L = -sum_r w_r log p(bin_r | parent_r) / sum_r w_r.
-__global__ void ce_kernel(float* __restrict__ z, int B, int K, const uint32_t* __restrict__ rows,
-                          const uint32_t* __restrict__ tbin, const float* __restrict__ w,
-                          const float* __restrict__ wsum, Proposal pr, double* __restrict__ loss) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= B) return;
-  float* zr = z + (size_t)r * K;
-  const uint32_t g = rows[r];
-  float mx = -INFINITY;
-  for (int k = 0; k < K; ++k)
-    if (bin_size_without(pr, (uint32_t)k, g) > 0) mx = fmaxf(mx, zr[k]);
-  float se = 0.0f;
-  for (int k = 0; k < K; ++k)
-    if (bin_size_without(pr, (uint32_t)k, g) > 0) se += __expf(zr[k] - mx);
-  const float scale = w[r] / *wsum;
-  const uint32_t t = tbin[r];
-  atomicAdd(loss, -(double)scale * (double)(zr[t] - mx - __logf(se)));
-  for (int k = 0; k < K; ++k) {
-    const bool valid = bin_size_without(pr, (uint32_t)k, g) > 0;
-    const float p = valid ? __expf(zr[k] - mx) / se : 0.0f;
-    zr[k] = valid ? scale * (p - (k == (int)t ? 1.0f : 0.0f)) : 0.0f;
+// dL/dz of L = -sum_r w_r log p(bin_r | parent_r) / sum_r w_r.  One warp per row (lanes over the
+// bins, coalesced row access, shuffle reductions); the rows' loss terms are added per block and
+// reach `loss` with one atomic per block.
+constexpr int kCeRowsPerBlock = 32;  // 8 warps x 4 rows
+
+__global__ void __launch_bounds__(256) ce_kernel(float* __restrict__ z, int B, int K, const uint32_t* __restrict__ rows,
+                                                 const uint32_t* __restrict__ tbin, const float* __restrict__ w,
+                                                 const float* __restrict__ wsum, Proposal pr,
+                                                 double* __restrict__ loss) {
+  __shared__ double part[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double acc = 0.0;
+  for (int j = 0; j < kCeRowsPerBlock / 8; ++j) {
+    const int r = blockIdx.x * kCeRowsPerBlock + j * 8 + warp;
+    if (r >= B) break;  // warp-uniform
+    float* zr = z + (size_t)r * K;
+    const uint32_t g = rows[r];
+    float mx = -INFINITY;
+    for (int k = lane; k < K; k += 32)
+      if (bin_size_without(pr, (uint32_t)k, g) > 0) mx = fmaxf(mx, zr[k]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+    float se = 0.0f;
+    for (int k = lane; k < K; k += 32)
+      if (bin_size_without(pr, (uint32_t)k, g) > 0) se += __expf(zr[k] - mx);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xFFFFFFFFu, se, o);
+    const float scale = w[r] / *wsum;
+    const uint32_t t = tbin[r];
+    if (lane == 0) acc += -(double)scale * (double)(zr[t] - mx - __logf(se));
+    for (int k = lane; k < K; k += 32) {
+      const bool valid = bin_size_without(pr, (uint32_t)k, g) > 0;
+      const float p = valid ? __expf(zr[k] - mx) / se : 0.0f;
+      zr[k] = valid ? scale * (p - (k == (int)t ? 1.0f : 0.0f)) : 0.0f;
+    }
+  }
+  if (lane == 0) part[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < 8; ++i) s += part[i];
+    atomicAdd(loss, s);
   }
 }
 
@@ -632,9 +653,10 @@ nw_status batch_loss_grad(nw_qmc* q, int B, double* loss_out) {
   if (st != NW_OK) return st;
   st = nw::mlp_forward(ctx, &m, B, s);
   if (st != NW_OK) return st;
-  sum_kernel<<<1, 256, 0, s>>>(q->tw, B, q->twsum);
+  sum_kernel<<<1, 1024, 0, s>>>(q->tw, B, q->twsum);
   NW_CUDA(ctx, cudaMemsetAsync(q->tloss, 0, sizeof(double), s));
-  ce_kernel<<<(B + 127) / 128, 128, 0, s>>>(m.z, B, m.nout, q->trows, q->tbin, q->tw, q->twsum, q->pr, q->tloss);
+  ce_kernel<<<(B + kCeRowsPerBlock - 1) / kCeRowsPerBlock, 256, 0, s>>>(m.z, B, m.nout, q->trows, q->tbin, q->tw,
+                                                                         q->twsum, q->pr, q->tloss);
   NW_CUDA(ctx, cudaGetLastError());
   if ((st = nw::mlp_backward(ctx, &m, B, s)) != NW_OK) return st;
   if (loss_out) {
