@@ -228,3 +228,20 @@ def test_overlap_action_single_parent_and_missing_parent():
         x = rng.standard_normal(b3.shape[0])
         y = _apply(w, x)
     assert np.abs(y - s @ x).max() <= 1e-13 * np.abs(s).max() * np.abs(x).sum()
+
+
+@pytest.mark.parametrize("nocc", [6, 9])
+def test_overlap_action_more_occupied_orbitals(nocc):
+    """Single-spin determinants of 6 and 9 occupied orbitals (the factor kernel's larger LU
+    scratch variants), singles and doubles of three references."""
+    n = nocc + 5
+    system = sy.make_system(n, nocc, nocc, 3, 16, seed=nocc, k_scale=0.2)
+    basis = sy.sd_basis(n, nocc, nocc, 3)
+    rng = np.random.default_rng(nocc)
+    with nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8) as w:
+        w.build().set_basis(basis)
+        _, s = w.build_hs_matrix()
+        x = rng.standard_normal(basis.shape[0])
+        y = _apply(w, x)
+    scale = np.abs(s).max() * np.abs(x).sum()
+    assert np.abs(y - s @ x).max() <= 1e-12 * scale, np.abs(y - s @ x).max() / scale

@@ -139,3 +139,22 @@ def test_matrix_free_tiles_match_packed_and_dense():
     scale = np.abs(m) @ np.abs(xv)
     assert np.all(np.abs(y_mf - m @ xv) <= 1e-12 * scale + 1e-14)
     assert np.all(np.abs(y_mf - y_pk) <= 1e-12 * scale + 1e-14)
+
+
+def test_matrix_free_blocks_match_packed():
+    """More candidates than one block of 1024 tiles (13022 candidates: 1128 tiles, two blocks of
+    the matrix-free product): matrix-free and packed M x agree."""
+    system = sy.make_system(18, 4, 4, 3, 16, seed=12, k_scale=0.3)
+    basis = sy.sd_basis(18, 4, 4, 3)
+    cand = np.nonzero((basis["rank_a"] + basis["rank_b"]) > 0)[0].astype(np.uint32)
+    nb = (cand.shape[0] + 255) // 256
+    assert nb * (nb + 1) // 2 > 1024
+    e0 = -5.1
+    xv = np.random.default_rng(6).normal(size=cand.shape[0])
+    with nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8).build() as w:
+        w.set_basis(basis)
+        w.update_fock(system.h, system.h)
+        with nociwick.Pt2(w, cand, e0) as pk, nociwick.Pt2(w, cand, e0, matrix_free=True) as mf:
+            y_pk, y_mf = pk.apply_m(xv), mf.apply_m(xv)
+    scale = np.abs(y_pk).max() + np.abs(xv).max()
+    assert np.abs(y_mf - y_pk).max() <= 1e-11 * scale, np.abs(y_mf - y_pk).max() / scale
