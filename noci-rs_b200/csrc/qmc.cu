@@ -2,11 +2,13 @@
 //
 // One cycle (propagate_iteration, src/stochastic/metric.rs:378-473, for the uniform generator):
 //   1. qmc_sample_kernel   per determinant: sampled population n~ = Phi_c1(N) (FRI), the
-//                          diagonal change -dt (H_gg - E^S S_gg - E^I) n~ into delta, and the
-//                          number of spawning attempts max(1, ceil|n~|);
-//   2. scan of the attempts -> the attempt slots of every determinant;
-//   3. qmc_spawn_kernel    per attempt: its parent (binary search over the slots), a uniform
-//                          child != parent, the canonical pair (min, max);
+//                          diagonal change -dt (H_gg - E^S S_gg - E^I) n~ into delta, the
+//                          number of spawning attempts max(1, ceil|n~|) and n~ / attempts;
+//   2. scan of the attempts -> the attempt slots of every determinant; qmc_owners_kernel: the
+//      cycle's totals and the owner of every 256th attempt slot;
+//   3. qmc_spawn_kernel    per attempt: its parent (search inside its 256-slot chunk), a
+//                          child != parent from the uniform or learned generator, the
+//                          canonical pair (min, max) with its sort key;
 //   4. (H, S) of all attempts through the engine's sorted pair pipeline, with the number of
 //      attempts read on the device;
 //   5. qmc_apply_kernel    per attempt: -dt (H - E^S S) (n~ / attempts) (N - 1), FRI-rounded
