@@ -115,3 +115,17 @@ def test_direct_overlap_report_is_unbiased_in_the_oracle():
     live = se > 1e-12
     assert np.all(np.abs(mean[~live] - expected[~live]) < 1e-12)
     assert np.max(np.abs(mean[live] - expected[live]) / se[live]) < 6.0
+
+
+def test_factorised_overlap_on_a_reference_fixture():
+    """The reference's direct-overlap LiH 6-31G fixture (its integrals and UHF states rebuilt by
+    tests/golden/make_reference_fixtures.py): the factorised S x equals the oracle's Wick S x over
+    the 866 singles and doubles of the two references."""
+    import reffix
+    system, meta = reffix.load("QMC_LiH_6-31G_2_8_TRAJECTORY_DIRECT_OVERLAP")
+    basis = sy.sd_basis(system.nmo, system.nocc_a, system.nocc_b, len(system.refs), orders=(1, 2))
+    s, _, _ = _all_pairs_overlap(system, basis)
+    f = OverlapFactorisation(system.s, system.refs, system.nocc_a, system.nocc_b, basis)
+    x = np.random.default_rng(5).standard_normal(basis.shape[0])
+    assert basis.shape[0] == 866
+    assert np.abs(f.apply(x) - s @ x).max() < 1e-12 * np.abs(x).sum()
