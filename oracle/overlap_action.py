@@ -118,16 +118,21 @@ class OverlapFactorisation:
                 y[tq] += np.einsum("ta,at->t", a_tab[self.aid[tq]], u[:, self.bid[tq]])
         return self.r * y
 
-    def dense(self) -> np.ndarray:
-        """The full overlap matrix S_wick of the basis from the factor tables."""
-        s = np.zeros((self.ndet, self.ndet))
-        for w in range(self.ndet):
-            q = int(self.parent[w])
-            for x in range(self.ndet):
-                p = int(self.parent[x])
+    def dense(self, rows=None) -> np.ndarray:
+        """Rows of the overlap matrix S_wick of the basis from the factor tables (all rows when
+        rows is None), filled one (bra parent, ket parent) block at a time."""
+        rows = np.arange(self.ndet) if rows is None else np.asarray(rows, np.int64)
+        s = np.zeros((rows.shape[0], self.ndet))
+        for q in range(self.nref):
+            wi = np.nonzero(self.parent[rows] == q)[0]
+            w = rows[wi]
+            for p in range(self.nref):
+                xs = np.nonzero(self.parent == p)[0]
                 if q == p:
-                    v = 1.0 if (self.aid[w] == self.aid[x] and self.bid[w] == self.bid[x]) else 0.0
+                    v = ((self.aid[w][:, None] == self.aid[xs][None, :])
+                         & (self.bid[w][:, None] == self.bid[xs][None, :])).astype(float)
                 else:
-                    v = self.fac[(q, p, 0)][self.aid[w], self.aid[x]] * self.fac[(q, p, 1)][self.bid[w], self.bid[x]]
-                s[w, x] = self.r[w] * self.r[x] * v
-        return s
+                    v = (self.fac[(q, p, 0)][np.ix_(self.aid[w], self.aid[xs])]
+                         * self.fac[(q, p, 1)][np.ix_(self.bid[w], self.bid[xs])])
+                s[np.ix_(wi, xs)] = v
+        return self.r[rows][:, None] * s * self.r[None, :]

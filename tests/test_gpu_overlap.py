@@ -4,7 +4,8 @@ direct-overlap NOCI-QMC propagator built on it (qmc_step of src/stochastic/metri
 * The action equals the engine's own overlap matrix (nw_build_hs_matrix, itself checked against
   the oracle) times x, and the oracle's restatement of the spin-factorised contraction
   (oracle/overlap_action.py), on systems with and without zero-overlap reference pairs, with a
-  duplicated determinant and with a record whose phase is not the canonical one.
+  duplicated determinant, with a record whose phase is not the canonical one and through
+  quadruple excitations in one spin.
 * Direct overlap: the populations start at S c_0 scaled to the initial 1-norm; one report of one
   cycle changes them by exactly S times that cycle's change; they stay in the range of S on an
   overcomplete basis; the mean over independent runs follows the deterministic recursion; and a
@@ -245,3 +246,21 @@ def test_overlap_action_more_occupied_orbitals(nocc):
         y = _apply(w, x)
     scale = np.abs(s).max() * np.abs(x).sum()
     assert np.abs(y - s @ x).max() <= 1e-12 * scale, np.abs(y - s @ x).max() / scale
+
+
+def test_overlap_action_through_quadruple_excitations():
+    """Singles to quadruples of two references with 4 alpha and 3 beta electrons (single-spin
+    strings of rank 3 and 4): the action equals the engine's S times x and the oracle's
+    factorised contraction."""
+    system = sy.make_system(8, 4, 3, 2, 12, seed=12, k_scale=0.3)
+    basis = sy.sd_basis(8, 4, 3, 2, orders=(1, 2, 3, 4))
+    rng = np.random.default_rng(13)
+    with nociwick.WicksShared(system.s, system.h, system.eri, system.enuc, system.refs, tol=1e-8) as w:
+        w.build().set_basis(basis)
+        _, s = w.build_hs_matrix()
+        x = rng.standard_normal(basis.shape[0])
+        y = _apply(w, x)
+    scale = np.abs(s).max() * np.abs(x).sum()
+    assert np.abs(y - s @ x).max() <= 1e-13 * scale, np.abs(y - s @ x).max() / scale
+    f = OverlapFactorisation(system.s, system.refs, 4, 3, basis)
+    assert np.abs(y - f.apply(x)).max() <= 1e-13 * scale

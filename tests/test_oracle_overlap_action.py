@@ -5,7 +5,8 @@ and of the direct-overlap propagator.
 * The factorised S (single-spin determinants of the two parents' strings, identity inside a
   parent, r = record phase x canonical phase) equals the oracle's Wick overlap of every pair,
   with and without zero-overlap reference pairs, with a duplicated determinant and with a
-  non-canonical record phase; the B-first contraction equals the dense product.
+  non-canonical record phase, on the reference's LiH 6-31G fixture and through quadruple
+  excitations in one spin; the B-first contraction equals the dense product.
 * Direct overlap: the populations start at S c_0 scaled to the initial 1-norm, and a report adds
   S times the report's accumulated change (here a fixed change) instead of the change itself.
 """
@@ -129,3 +130,19 @@ def test_factorised_overlap_on_a_reference_fixture():
     x = np.random.default_rng(5).standard_normal(basis.shape[0])
     assert basis.shape[0] == 866
     assert np.abs(f.apply(x) - s @ x).max() < 1e-12 * np.abs(x).sum()
+
+
+def test_factorised_overlap_through_quadruple_excitations():
+    """Triple and quadruple excitations in one spin (spin keys of rank 3 and 4, unequal occupied
+    counts 4 and 3): 64 rows of the factorised S equal the oracle's Wick overlaps."""
+    system = sy.make_system(8, 4, 3, 2, 12, seed=12, k_scale=0.3)
+    basis = sy.sd_basis(8, 4, 3, 2, orders=(1, 2, 3, 4))
+    assert basis["rank_a"].max() == 4
+    orc = Oracle.from_system(system, tol=1e-8)
+    ob = orc.oracle_basis(basis)
+    n = basis.shape[0]
+    rows = np.random.default_rng(0).choice(n, 64, replace=False)
+    pairs = np.stack(np.meshgrid(rows, np.arange(n), indexing="ij"), -1).reshape(-1, 2)
+    _, s = orc.eval_pairs(ob, pairs)
+    f = OverlapFactorisation(system.s, system.refs, 4, 3, basis)
+    assert np.abs(f.dense(rows) - s.reshape(len(rows), n)).max() < 1e-14
