@@ -897,7 +897,7 @@ def config3_check(system, basis, pairs, gpu_hs, seconds: float, ngroups: int = 1
 
 
 def mixed_leg(args, system, basis, pairs, hs_ref, fp64_build_s, fp64_eval_ms, local_rank):
-    """Mixed precision on the config-3 system (north_star's split products on tensor cores): the
+    """Mixed precision on the config-3 system (split-precision products on tensor cores): the
     Cholesky route of the J and II tensors, T[pq][rs] = sum_P U[P][pq] V[P][rs], built
     (a) in FP64 on the FP64 tensor cores, (b) as int8 Ozaki slices on tcgen05 (exact int32 sums,
     FP64-faithful), (c) as three BF16 pieces on tcgen05 (FP32 accumulation).  Per mode: build
